@@ -1,0 +1,142 @@
+/*
+ * libnative_fp2_gpu.so -- B200 (sm_100a) GKR Fp2 prover core, C ABI.
+ *
+ * Drop-in for the reference library loaded by
+ * TruePix-main/libTruePix/native_fp2_bridge.py:116-183 from
+ * TruePix-main/native_fp2/lib/. The first 14 declarations keep the reference
+ * prototypes (TruePix-main/native_fp2/native_fp2.cpp:11-160,
+ * TruePix-main/native_fp2/native_fp2.cu:824-1022) and meaning:
+ *   - field p = 2^61 - 1, Fp2 = Fp[i]/(i^2+1), canonical limbs in [0, p);
+ *   - host arrays are caller-owned SoA real[]/imag[]; inputs are consumed and
+ *     outputs written before the call returns;
+ *   - session handles are opaque and freed by native_fp2_early_destroy.
+ * Differences: there is no host fallback. A void entry point that fails leaves
+ * its outputs untouched and sets tp_last_error_code() != 0; session calls
+ * return -1 / NULL as the reference does. Wire indices used by a gate must lie
+ * in [0, n_wires) and challenges must be canonical, else the call fails.
+ *
+ * The tp_* entry points are extensions: error reporting and device-buffer
+ * variants whose Fp2 buffers are packed {re, im} pairs of uint64 (16 bytes per
+ * element, 16-byte aligned) in device memory, asynchronous on `stream`
+ * (a cudaStream_t; NULL selects the library's own stream).
+ */
+#ifndef TRUEPIX_NATIVE_FP2_H
+#define TRUEPIX_NATIVE_FP2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* native_fp2.cu:826-829 -- initialise; 0 = ok (also without a device) */
+int native_fp2_init(void);
+/* native_fp2.cu:831-834 -- 1 when a CUDA device is usable */
+int native_fp2_cuda_available(void);
+
+/* native_fp2.cu:836-848 (core.hpp:53-64): out[i] = in[2i] + r (in[2i+1] - in[2i]) */
+void native_fp2_fold(const uint64_t* in_real, const uint64_t* in_imag, size_t n_out,
+                     uint64_t r_real, uint64_t r_imag, uint64_t* out_real, uint64_t* out_imag);
+
+/* native_fp2.cu:850-862 (core.hpp:66-80): out[i*ncopies + j] = in[i] */
+void native_fp2_expand(const uint64_t* in_real, const uint64_t* in_imag, size_t n_src,
+                       size_t ncopies, uint64_t* out_real, uint64_t* out_imag);
+
+/* native_fp2.cu:864-893 (core.hpp:82-137): early-round claim at t = 0, 1, -1, 2 with
+ * caller-supplied -1/2 tables; out8 = [re0, im0, re1, im1, re-1, im-1, re2, im2] */
+void native_fp2_sumcheck_early(int n_gates, const int* gate_type, const int* in0, const int* in1,
+                               const uint64_t* z1_real, const uint64_t* z1_imag, int n_copies,
+                               int n_wires, const uint64_t* values_real,
+                               const uint64_t* values_imag, const uint64_t* fact0_real,
+                               const uint64_t* fact0_imag, const uint64_t* fact1_real,
+                               const uint64_t* fact1_imag, const uint64_t* beta_real,
+                               const uint64_t* beta_imag, const uint64_t* beta_f0_real,
+                               const uint64_t* beta_f0_imag, const uint64_t* beta_f1_real,
+                               const uint64_t* beta_f1_imag, uint64_t out8[8]);
+
+/* native_fp2.cu:895-907 (core.hpp:139-161): out[i] = init * prod_j (bit_j(i) ? z_j : 1 - z_j) */
+void native_fp2_compute_beta(const uint64_t* z_real, const uint64_t* z_imag, int n_z,
+                             uint64_t init_real, uint64_t init_imag, uint64_t* out_real,
+                             uint64_t* out_imag);
+
+/* native_fp2.cu:909-921 (core.hpp:300-366): MLE of 2^n_z base-field inputs at z (LSB first) */
+void native_fp2_mle_eval_base(const uint64_t* inputs, const uint64_t* z_real,
+                              const uint64_t* z_imag, int n_z, uint64_t* out_real,
+                              uint64_t* out_imag);
+
+/* native_fp2.cu:923-952 (core.hpp:173-198): resident early-round session; NULL on failure.
+ * values: n_wires x n_copies, wire-major; n_copies a power of two >= 2. */
+void* native_fp2_early_create(int n_gates, const int* gate_type, const int* in0, const int* in1,
+                              const uint64_t* z1_real, const uint64_t* z1_imag, int n_copies,
+                              int n_wires, const uint64_t* values_real,
+                              const uint64_t* values_imag, const uint64_t* beta_real,
+                              const uint64_t* beta_imag);
+/* native_fp2.cu:954-963 (core.hpp:200-248): claim of the current round; 0 ok, -1 error */
+int native_fp2_early_claim(void* handle, uint64_t out8[8]);
+/* native_fp2.cu:965-974 (core.hpp:250-279): fold every wire and beta by r; 0 ok, -1 error */
+int native_fp2_early_fold(void* handle, uint64_t r_real, uint64_t r_imag);
+/* native_fp2.cu:976-989 (core.hpp:281-296): wire[w] = V[w][0], beta = beta[0] */
+int native_fp2_early_finish(void* handle, uint64_t* wire_real, uint64_t* wire_imag,
+                            uint64_t* beta_real, uint64_t* beta_imag);
+/* native_fp2.cu:991-1005 */
+int native_fp2_early_n_copies(void* handle);
+int native_fp2_early_n_wires(void* handle);
+/* native_fp2.cu:1007-1020 */
+void native_fp2_early_destroy(void* handle);
+
+/* ---- extensions (no counterpart in the reference) ---- */
+
+/* error state of the calling thread: 0 = ok; text describes the last failure */
+int tp_last_error_code(void);
+const char* tp_last_error(void);
+void tp_clear_error(void);
+/* kernels launched by the last batch entry point */
+int tp_last_launch_count(void);
+
+/* Host-only: the per-layer linear form the claim kernels use,
+ *   sum_g z1[g] gate_g(V[in0], V[in1]) = K0 + sum_w L[w] V[w] + sum_t c_t V[a_t] V[b_t].
+ * Writes k0[2], lin[2*n_wires] (re, im pairs) and up to max_terms product terms
+ * (term_ab[2i] = a, term_ab[2i+1] = b, term_c[2i..2i+1] = c); returns the number of
+ * terms, or -1 on a bad wire index. Needs no GPU. */
+int tp_gate_form(int n_gates, const int* gate_type, const int* in0, const int* in1,
+                 const uint64_t* z1_real, const uint64_t* z1_imag, int n_wires, uint64_t* k0,
+                 uint64_t* lin, int max_terms, int* term_ab, uint64_t* term_c);
+
+/* Session over a packed device table d_values (n_wires x n_copies Fp2) and packed
+ * d_beta (n_copies Fp2). borrow != 0 adopts d_values as working storage (the caller
+ * keeps it alive until destroy; its contents are overwritten); otherwise it is copied. */
+void* tp_early_create_dev(int n_gates, const int* gate_type, const int* in0, const int* in1,
+                          const uint64_t* z1_real, const uint64_t* z1_imag, int n_copies,
+                          int n_wires, const void* d_values, const void* d_beta, int borrow,
+                          void* stream);
+/* claim into 8 x uint64 of device memory, without synchronising */
+int tp_early_claim_dev(void* handle, void* d_out8);
+/* wires into n_wires packed Fp2 and beta[0] into one packed Fp2, device memory, async */
+int tp_early_finish_dev(void* handle, void* d_wires, void* d_beta);
+/* kernels launched so far by a session */
+int tp_early_launches(void* handle);
+
+/* packed-buffer variants of fold / compute_beta / mle_eval_base (asynchronous) */
+int tp_fold_dev(const void* d_in, size_t n_out, uint64_t r_real, uint64_t r_imag, void* d_out,
+                void* stream);
+int tp_compute_beta_dev(const void* d_z, int n_z, uint64_t init_real, uint64_t init_imag,
+                        void* d_out, void* stream);
+int tp_mle_eval_base_dev(const void* d_inputs, const void* d_z, int n_z, void* d_out,
+                         void* stream);
+
+/* Input layer from a uint8 frame: n_copies rows of copy_size bytes (copy-major)
+ * -> d_table, the packed wire-major table [n_wires][n_copies_padded] used by the
+ * early session, and/or d_inputs, the copy-major base-field vector
+ * x[c * n_wires + w] used by mle_eval_base (either may be NULL). Wire const_idx
+ * holds const_val (const_idx < 0: none); other wires and padded copies are zero.
+ * Layout of TruePix-main/Orion/Orion_nonzk/include/truepix/truepix_gkr.h:11-18
+ * (copy-major-384-const128-pad512-v1). Asynchronous. */
+int tp_table_from_pixels(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size,
+                         int n_wires, int const_idx, uint64_t const_val, void* d_table,
+                         void* d_inputs, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,53 @@
+// Process-wide device context for the prover core: one CUDA device per process
+// (the device current at first use), one library stream, a stream-ordered
+// caching memory pool, and a thread-local error state that the C ABI reports
+// through tp_last_error()/tp_last_error_code().
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace tp {
+
+struct Ctx {
+    int device = -1;
+    int n_sm = 0;
+    cudaStream_t stream = nullptr;   // library stream (non-blocking)
+    cudaMemPool_t pool = nullptr;    // stream-ordered pool, memory kept cached
+};
+
+// Initialise once; returns nullptr (and sets the error) when no device is usable.
+Ctx* ctx();
+bool device_present();
+
+// error state -----------------------------------------------------------
+enum ErrCode { TP_OK = 0, TP_ERR_ARG = 1, TP_ERR_CUDA = 2, TP_ERR_NODEV = 3, TP_ERR_OOM = 4 };
+void set_error(int code, const char* fmt, ...);
+void clear_error();
+int error_code();
+const char* error_text();
+// record a CUDA failure; returns true when `e` is an error
+bool cuda_failed(cudaError_t e, const char* what);
+
+// stream-ordered allocation from the library pool ------------------------
+void* dev_alloc(size_t bytes, cudaStream_t s);
+void dev_free(void* p, cudaStream_t s);
+
+// Asynchronous host->device upload of a small host buffer through a pinned
+// staging ring (64 slots of 256 KB, each reused only after its previous copy has
+// completed). The host buffer may be reused as soon as the call returns. Larger
+// uploads are copied synchronously.
+bool upload_async(void* d_dst, const void* h_src, size_t bytes, cudaStream_t s);
+
+// grid sizing helpers ----------------------------------------------------
+inline unsigned blocks_for(size_t n, unsigned threads)
+{
+    return (unsigned)((n + threads - 1) / threads);
+}
+
+}  // namespace tp
+
+#define TP_CUDA_OK(expr, what)                   \
+    do {                                         \
+        if (::tp::cuda_failed((expr), (what)))   \
+            return false;                        \
+    } while (0)

@@ -1,0 +1,90 @@
+"""Loader and ctypes prototypes for the in-tree CUDA libraries.
+
+`gkr()` returns libnative_fp2_gpu.so with every entry point of
+include/native_fp2.h bound. It raises if the library is missing or no CUDA
+device is usable: there is no CPU fallback anywhere in the product path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.realpath(__file__))
+LIBDIR = os.path.join(HERE, "lib")
+
+_U64 = ctypes.c_uint64
+_I32 = ctypes.c_int
+_SZ = ctypes.c_size_t
+_VP = ctypes.c_void_p
+_PU64 = ctypes.POINTER(_U64)
+_PI32 = ctypes.POINTER(_I32)
+
+GKR_SIGNATURES = {
+    "native_fp2_init": (_I32, []),
+    "native_fp2_cuda_available": (_I32, []),
+    "native_fp2_fold": (None, [_PU64, _PU64, _SZ, _U64, _U64, _PU64, _PU64]),
+    "native_fp2_expand": (None, [_PU64, _PU64, _SZ, _SZ, _PU64, _PU64]),
+    "native_fp2_sumcheck_early": (None, [_I32, _PI32, _PI32, _PI32, _PU64, _PU64, _I32, _I32]
+                                  + [_PU64] * 13),
+    "native_fp2_compute_beta": (None, [_PU64, _PU64, _I32, _U64, _U64, _PU64, _PU64]),
+    "native_fp2_mle_eval_base": (None, [_PU64, _PU64, _PU64, _I32, _PU64, _PU64]),
+    "native_fp2_early_create": (_VP, [_I32, _PI32, _PI32, _PI32, _PU64, _PU64, _I32, _I32,
+                                      _PU64, _PU64, _PU64, _PU64]),
+    "native_fp2_early_claim": (_I32, [_VP, _PU64]),
+    "native_fp2_early_fold": (_I32, [_VP, _U64, _U64]),
+    "native_fp2_early_finish": (_I32, [_VP, _PU64, _PU64, _PU64, _PU64]),
+    "native_fp2_early_n_copies": (_I32, [_VP]),
+    "native_fp2_early_n_wires": (_I32, [_VP]),
+    "native_fp2_early_destroy": (None, [_VP]),
+    "tp_last_error_code": (_I32, []),
+    "tp_last_error": (ctypes.c_char_p, []),
+    "tp_clear_error": (None, []),
+    "tp_last_launch_count": (_I32, []),
+    "tp_gate_form": (_I32, [_I32, _PI32, _PI32, _PI32, _PU64, _PU64, _I32, _PU64, _PU64, _I32,
+                            _PI32, _PU64]),
+    "tp_early_create_dev": (_VP, [_I32, _VP, _VP, _VP, _VP, _VP, _I32, _I32, _VP, _VP, _I32, _VP]),
+    "tp_early_claim_dev": (_I32, [_VP, _VP]),
+    "tp_early_finish_dev": (_I32, [_VP, _VP, _VP]),
+    "tp_early_launches": (_I32, [_VP]),
+    "tp_fold_dev": (_I32, [_VP, _SZ, _U64, _U64, _VP, _VP]),
+    "tp_compute_beta_dev": (_I32, [_VP, _I32, _U64, _U64, _VP, _VP]),
+    "tp_mle_eval_base_dev": (_I32, [_VP, _VP, _I32, _VP, _VP]),
+    "tp_table_from_pixels": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
+}
+
+_cache = {}
+
+
+def _bind(path: str, sigs: dict):
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in sigs.items():
+        if hasattr(lib, name):
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    return lib
+
+
+def lib_path(name: str) -> str:
+    return os.path.join(LIBDIR, name)
+
+
+def gkr(require_device: bool = True):
+    """libnative_fp2_gpu.so, bound; raises when unusable."""
+    if "gkr" not in _cache:
+        path = os.environ.get("TRUEPIX_NATIVE_FP2_GPU_LIB", lib_path("libnative_fp2_gpu.so"))
+        if not os.path.isfile(path):
+            raise RuntimeError(f"CUDA library missing: {path} (run python -m truepix_b200.build)")
+        _cache["gkr"] = _bind(path, GKR_SIGNATURES)
+    lib = _cache["gkr"]
+    if require_device:
+        lib.native_fp2_init()
+        if not lib.native_fp2_cuda_available():
+            raise RuntimeError("no usable CUDA device: " + lib.tp_last_error().decode())
+    return lib
+
+
+def check(lib, rc=0, what="call"):
+    """Raise with the library's message when rc is an error or an error is recorded."""
+    if (rc is not None and rc != 0) or lib.tp_last_error_code() != 0:
+        raise RuntimeError(f"{what} failed: {lib.tp_last_error().decode()}")
