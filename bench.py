@@ -141,45 +141,56 @@ def reference_arm(args, rank, world):
 # --------------------------------------------------------------------------
 
 class ClockSampler:
+    """nvidia-smi samples (50 ms) kept only inside [t_begin, t_end] of the timed region."""
+
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.out = ""
+        self.t0 = self.t1 = None
 
-    def __enter__(self):
-        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    def start(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + q,
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
-        return self
+        time.sleep(0.3)
 
-    def __exit__(self, *exc):
-        self.out = ""
+    def stop(self):
         if self.proc:
             self.proc.terminate()
             try:
                 self.out, _ = self.proc.communicate(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                self.out = ""
 
     def summary(self):
+        import datetime
         rows = []
         for line in (self.out or "").splitlines():
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 7 and parts[0].isdigit():
-                rows.append(parts)
+            if len(parts) < 7 or not parts[1].isdigit():
+                continue
+            try:
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                ts = None
+            if ts is not None and self.t0 is not None and not (self.t0 - 0.05 <= ts <= self.t1 + 0.05):
+                continue
+            rows.append(parts)
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = sorted(int(r[0]) for r in rows)
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[3 + i]})
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": int(rows[0][1]), "reasons": reasons,
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = sorted(int(r[1]) for r in rows)
+        reasons = sorted({self.NAMES[i] for r in rows for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": int(rows[0][2]), "reasons": reasons,
                 "samples": len(rows)}
 
 
@@ -203,7 +214,35 @@ def profiled_traffic():
     return None
 
 
+def kernel_groups(ms, tags, layout):
+    """Per claim-kernel kind: launches, total time and algorithmic bytes.
+    tag = 1000*(reads pixels) + 100*(fold fused) + log2(copies claimed)."""
+    rows = layout.const_idx + 1 if layout.const_idx >= 0 else layout.copy_size
+    pix_bytes = layout.copies * layout.copy_size
+    groups = {}
+    for t, tag in zip(ms, tags):
+        pix, fold, lg = tag // 1000, (tag // 100) % 10, tag % 100
+        n = 1 << lg                                    # copies claimed
+        if pix and not fold:
+            name, byt = "claim_pixels_kernel", pix_bytes + 16 * n
+        elif pix and fold:
+            name, byt = "fold_claim_pixels_kernel", pix_bytes + 16 * rows * n + 48 * n
+        elif fold:
+            name, byt = "claim_kernel<FOLD_CLAIM>", 48 * rows * n + 48 * n
+        else:
+            name, byt = "claim_kernel<CLAIM>", 16 * rows * n + 16 * n
+        g = groups.setdefault(name, {"launches": 0, "ms": 0.0, "bytes": 0.0, "by_copies": {}})
+        g["launches"] += 1
+        g["ms"] += t
+        g["bytes"] += byt
+        bc = g["by_copies"].setdefault(n, [0, 0.0])
+        bc[0] += 1
+        bc[1] += t
+    return groups
+
+
 def ours_arm(args, rank, world, local_rank):
+    import ctypes
     import torch
     import torch.distributed as dist
     from truepix_b200 import native
@@ -221,40 +260,41 @@ def ours_arm(args, rank, world, local_rank):
     pt_dev = torch.from_numpy(pack_fp2(point[:, 0], point[:, 1])).to(dev)
     stream = torch.cuda.Stream(dev)
     prover = GkrInputLayerProver(layout, gt, i0, i1, device=local_rank, stream=stream)
+    lib = native.gkr()
     nb = layout.n_copy_bits
-    Wn, C = layout.n_wires, layout.padded_copies
-
-    # per-launch events around the fused fold+claim kernel (rounds 1..nb-1)
-    ev = {}
-
-    def hook(k, when):
-        if k == 0:
-            return
-        e = torch.cuda.Event(enable_timing=True)
-        e.record(stream)
-        ev.setdefault(k, []).append(e)
 
     with torch.cuda.stream(stream):
         for i in range(args.warmup):
             prover.prove(pix[i % n_frames], z1, z2_dev, pt_dev, chal)
     torch.cuda.synchronize()
+    native.check(lib, lib.tp_timer_enable(args.steps * nb + 16), "timer")
+    clk = ClockSampler(local_rank)
+    clk.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    lib.tp_timer_reset()
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     launches = 0
-    with ClockSampler(local_rank) as clk:
-        with torch.cuda.stream(stream):
-            start.record(stream)
-            for i in range(args.steps):
-                prover.prove(pix[i % n_frames], z1, z2_dev, pt_dev, chal, claim_hook=hook)
-                launches += prover.launches_last
-            end.record(stream)
-        torch.cuda.synchronize()
+    clk.t0 = time.time()
+    with torch.cuda.stream(stream):
+        start.record(stream)
+        for i in range(args.steps):
+            prover.prove(pix[i % n_frames], z1, z2_dev, pt_dev, chal)
+            launches += prover.launches_last
+        end.record(stream)
+    torch.cuda.synchronize()
+    clk.t1 = time.time()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    clk.stop()
+    npairs = args.steps * nb + 16
+    tms = (ctypes.c_float * npairs)()
+    ttags = (ctypes.c_int * npairs)()
+    got = lib.tp_timer_read(tms, ttags, npairs)
+    lib.tp_timer_disable()
     ms = start.elapsed_time(end)
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -262,26 +302,30 @@ def ours_arm(args, rank, world, local_rank):
     ms = float(t.item())
     value = world * args.steps / (ms / 1e3)
 
-    # roofline of the fused fold+claim kernel
-    alg_bytes, dur_ms, n_l = 0.0, 0.0, 0
-    for k, lst in ev.items():
-        n_in = C >> (k - 1)
-        per = 48.0 * (Wn + 1) * (n_in // 2)
-        for j in range(0, len(lst) - 1, 2):
-            dur_ms += lst[j].elapsed_time(lst[j + 1])
-            alg_bytes += per
-            n_l += 1
+    groups = kernel_groups(list(tms[:max(0, got)]), list(ttags[:max(0, got)]), layout)
     peak, peak_kind = peaks()
-    achieved = alg_bytes / (dur_ms / 1e3) / 1e9 if dur_ms > 0 else None
+    kernels = []
+    for name, g in sorted(groups.items(), key=lambda kv: -kv[1]["ms"]):
+        ach = g["bytes"] / (g["ms"] / 1e3) / 1e9 if g["ms"] > 0 else None
+        kernels.append({"kernel": name, "launches": g["launches"], "total_ms": g["ms"],
+                        "share_of_step": g["ms"] / ms, "achieved_gbs": ach,
+                        "avg_us_by_copies": {str(k): round(1e3 * v[1] / v[0], 2)
+                                             for k, v in sorted(g["by_copies"].items())}})
+    top = kernels[0] if kernels else None
     traffic = profiled_traffic()
-    roof = {"kernel": "claim_kernel<FOLD_CLAIM> (fused fold + next claim)", "bound": "hbm",
-            "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
-            "algorithmic_bytes_per_launch": alg_bytes / max(1, n_l),
-            "avg_launch_us": 1e3 * dur_ms / max(1, n_l), "launches_timed": n_l,
-            "traffic": traffic.get("dram_bytes_per_launch_avg") if traffic else None}
+    roof = None
+    if top:
+        g = groups[top["kernel"]]
+        roof = {"kernel": top["kernel"], "bound": "hbm", "achieved": top["achieved_gbs"],
+                "peak": peak, "unit": "GB/s",
+                "frac": top["achieved_gbs"] / peak if top["achieved_gbs"] else None,
+                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6650 GB/s",
+                "algorithmic_bytes_per_launch": g["bytes"] / g["launches"],
+                "avg_launch_us": 1e3 * g["ms"] / g["launches"], "launches_timed": g["launches"],
+                "traffic": (traffic or {}).get(top["kernel"]),
+                "all_claim_kernels": kernels}
 
-    # correctness of what was timed: the last frame against the oracle's first claim
     res_ok = None
     if rank == 0:
         c, w, b, m = prover.results()
@@ -290,9 +334,8 @@ def ours_arm(args, rank, world, local_rank):
     e2e = None
     cpu = None
     if rank == 0 and not args.skip_e2e:
-        e2e = e2e_c_abi(args, native.gkr(), frames[0], layout, gt, i0, i1, z1, z2, point, chal)
+        e2e = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
     if rank == 0 and world == 1 and not args.skip_cpu:
-        t0 = time.perf_counter()
         secs, kind = _cpu_worker((0, 1))
         cpu = {"value": 1.0 / secs, "unit": UNIT, "cores": 1, "kind": kind,
                "sample": "1 frame of the same workload (compute_beta + 14 early rounds + finish "
@@ -304,9 +347,11 @@ def ours_arm(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u64 (Fp2 over 2^61-1)", "data": "synthetic",
             "config": {"workload": "gkr_input_layer_gray_1080p", "frame": [H, Wd, 3],
-                       "copies": layout.copies, "padded_copies": C, "wires": C * Wn,
-                       "rounds": nb, "circuit": "gray.pws", "l2": "inputs > L2 (128 MiB table "
-                       "+ 64 MiB input vector per frame, 4 frames cycled)",
+                       "copies": layout.copies, "padded_copies": layout.padded_copies,
+                       "wires": layout.padded_copies * layout.n_wires, "rounds": nb,
+                       "circuit": "gray.pws", "path": "pixels (tp_early_create_pixels)",
+                       "l2": "inputs > L2: 4 distinct frames cycled; the folded table of "
+                             "round 1 (47 MiB) is rewritten every frame",
                        "parallelism": f"replicas x{world}"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
@@ -361,7 +406,7 @@ def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
 
     for _ in range(max(1, min(args.warmup, 3))):
         one()
-    steps = max(1, min(args.steps, 10))
+    steps = max(3, min(args.steps // 100, 20))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -379,8 +424,8 @@ def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")

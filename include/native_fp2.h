@@ -136,6 +136,38 @@ int tp_table_from_pixels(const void* d_pixels, int n_copies, int n_copies_padded
                          int n_wires, int const_idx, uint64_t const_val, void* d_table,
                          void* d_inputs, void* stream);
 
+/* Early session whose input table is the implicit table of a uint8 frame in
+ * device memory (the layout of tp_table_from_pixels), read directly from the
+ * bytes: the first claim and the first fold never materialise the
+ * n_wires x n_copies_padded Fp2 table, and only rows [0, copy_size) and the
+ * constant row are stored afterwards (the other wires are zero). d_beta: packed
+ * Fp2 [n_copies_padded] (copied). Claims, folds, finish and destroy as for any
+ * session; the pixels must stay unchanged until the first fold has run. */
+void* tp_early_create_pixels(int n_gates, const int* gate_type, const int* in0, const int* in1,
+                             const uint64_t* z1_real, const uint64_t* z1_imag,
+                             const void* d_pixels, int n_copies, int n_copies_padded,
+                             int copy_size, int n_wires, int const_idx, uint64_t const_val,
+                             const void* d_beta, void* stream);
+/* mle_eval_base of the copy-major input vector of that frame (x[c * n_wires + w])
+ * at the packed Fp2 point d_z (log2(n_wires) + log2(n_copies_padded) coordinates,
+ * LSB first), computed from the bytes. n_wires <= 512, powers of two. Async. */
+int tp_mle_eval_pixels(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size,
+                       int n_wires, int const_idx, uint64_t const_val, const void* d_z,
+                       void* d_out, void* stream);
+
+/* n_rounds x (claim into d_claims[8k..8k+7] on the device, fold by challenges[2k],
+ * challenges[2k+1]) without returning to the caller in between: for callers that
+ * already hold the challenges (replay, benchmarking). Asynchronous. */
+int tp_early_rounds_dev(void* handle, int n_rounds, const uint64_t* challenges, void* d_claims);
+
+/* Claim-kernel timer: when enabled, every session claim records a CUDA event pair
+ * with tag 1000*(reads pixels) + 100*(fold fused) + log2(copies claimed).
+ * tp_timer_read (after a synchronise) returns the number of pairs and their ms. */
+int tp_timer_enable(int max_pairs);
+void tp_timer_disable(void);
+void tp_timer_reset(void);
+int tp_timer_read(float* ms, int* tags, int max_pairs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -278,14 +278,19 @@ def test_device_buffer_api(gpu_lib, oracle_lib, circuits):
     assert (int(f[W, 0]), int(f[W, 1])) == want[3]
 
 
-@pytest.mark.parametrize("name,hw", [("gray", (1080, 1920)), ("Crop", (240, 426))])
-def test_frame_prover_vs_oracle(oracle_lib, circuits, name, hw):
-    """The device-resident frame path (pixels -> table -> beta -> rounds -> MLE)."""
+@pytest.mark.parametrize("name,hw,mode", [
+    ("gray", (1080, 1920), "pixels"), ("gray", (1080, 1920), "table"),
+    ("Crop", (240, 426), "pixels"), ("Crop", (240, 426), "table"),
+    ("inv", (360, 640), "pixels"), ("mask", (8, 8), "pixels"), ("gray", (4, 8), "pixels"),
+    ("Crop", (2, 64), "pixels"), ("gray", (720, 1280), "pixels")])
+def test_frame_prover_vs_oracle(oracle_lib, circuits, name, hw, mode):
+    """The device-resident frame path (bytes -> beta -> rounds -> MLE) in both modes:
+    straight from the bytes, and through the materialised table."""
     import torch
     from truepix_b200.frame import FrameLayout, GkrInputLayerProver, pack_fp2
     rng = np.random.default_rng(4242)
-    const = {"gray": (384, 128), "Crop": (385, 128)}[name]
-    cs = 384 if name == "gray" else 385
+    const = {"gray": (384, 128), "Crop": (385, 128), "inv": (384, 255), "mask": (-1, 0)}[name]
+    cs = 385 if name == "Crop" else 384
     layout = FrameLayout.for_frame(hw[0], hw[1], copy_size=cs, const_idx=const[0],
                                    const_val=const[1])
     gt, i0, i1 = (circuits[name + "_" + k] for k in ("type", "in0", "in1"))
@@ -296,7 +301,7 @@ def test_frame_prover_vs_oracle(oracle_lib, circuits, name, hw):
     point = np.stack([rand_fp(rng, nb + 9), rand_fp(rng, nb + 9)], axis=1)
     chal = np.stack([rand_fp(rng, nb), rand_fp(rng, nb)], axis=1)
     dev = torch.device("cuda", 0)
-    prover = GkrInputLayerProver(layout, gt, i0, i1)
+    prover = GkrInputLayerProver(layout, gt, i0, i1, mode=mode)
     prover.prove(torch.from_numpy(pix).to(dev), z1,
                  torch.from_numpy(pack_fp2(z2[:, 0], z2[:, 1])).to(dev),
                  torch.from_numpy(pack_fp2(point[:, 0], point[:, 1])).to(dev), chal)
@@ -305,7 +310,8 @@ def test_frame_prover_vs_oracle(oracle_lib, circuits, name, hw):
     # oracle on the same inputs
     vals = np.zeros((C, W), np.uint64)
     vals[:layout.copies, :cs] = pix.reshape(layout.copies, cs)
-    vals[:layout.copies, const[0]] = const[1]
+    if const[0] >= 0:
+        vals[:layout.copies, const[0]] = const[1]
     table = np.ascontiguousarray(vals.T).reshape(-1)
     bre, bim = oracle_lib.compute_beta(np.ascontiguousarray(z2[:, 0]),
                                        np.ascontiguousarray(z2[:, 1]), (1, 0))

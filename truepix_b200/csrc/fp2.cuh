@@ -55,6 +55,53 @@ TP_HD u64 fmul(u64 a, u64 b)
 #endif
 }
 
+// ---- lazy ("nearly canonical") arithmetic --------------------------------
+// Values v < 2^61 + 8 stand for v mod p. Inputs of lmul may be < 2^62 + 64,
+// so a sum of two nearly canonical values is a valid operand. Nothing is made
+// canonical until a value leaves the kernel (canon61).
+TP_HD u64 fold61(u64 x) { return (x & P61) + (x >> 61); }   // any x -> < 2^61 + 8
+TP_HD u64 canon61(u64 x)
+{
+    const u64 f = fold61(x);
+    return f >= P61 ? f - P61 : f;
+}
+
+#if defined(__CUDA_ARCH__)
+// a, b < 2^62 + 64  ->  a*b mod p, < 2^61 + 8.
+// T = a*b < 2^125 is formed as four 32-bit words with one carry chain, then
+// T mod p = (T mod 2^61) + (T >> 61), folded once more.
+__device__ __forceinline__ u64 lmul(u64 a, u64 b)
+{
+    const u32 a0 = (u32)a, a1 = (u32)(a >> 32), b0 = (u32)b, b1 = (u32)(b >> 32);
+    const u64 p00 = (u64)a0 * b0;
+    const u64 mid = (u64)a0 * b1 + (u64)a1 * b0;   // < 2^64 for these bounds
+    const u64 p11 = (u64)a1 * b1;
+    u32 w1, w2, w3, q0, q1, s0, s1;
+    asm("add.cc.u32 %0, %3, %4;\n\t"
+        "addc.cc.u32 %1, %5, %6;\n\t"
+        "addc.u32 %2, %7, 0;"
+        : "=r"(w1), "=r"(w2), "=r"(w3)
+        : "r"((u32)(p00 >> 32)), "r"((u32)mid), "r"((u32)p11), "r"((u32)(mid >> 32)),
+          "r"((u32)(p11 >> 32)));
+    asm("shf.r.clamp.b32 %0, %1, %2, 29;" : "=r"(q0) : "r"(w1), "r"(w2));
+    asm("shf.r.clamp.b32 %0, %1, %2, 29;" : "=r"(q1) : "r"(w2), "r"(w3));
+    asm("add.cc.u32 %0, %2, %3;\n\t"
+        "addc.u32 %1, %4, %5;"
+        : "=r"(s0), "=r"(s1)
+        : "r"((u32)p00), "r"(q0), "r"(w1 & 0x1FFFFFFFu), "r"(q1));
+    return fold61(((u64)s1 << 32) | s0);
+}
+#else
+inline u64 lmul(u64 a, u64 b)
+{
+    const unsigned __int128 t = (unsigned __int128)a * b;
+    return fold61(((u64)t & P61) + (u64)(t >> 61));
+}
+#endif
+// nearly canonical a, b -> nearly canonical
+TP_HD u64 ladd(u64 a, u64 b) { return fold61(a + b); }
+TP_HD u64 lsub(u64 a, u64 b) { return fold61(a + (2 * P61 - b)); }   // b <= 2P
+
 TP_HD fp2 mk(u64 re, u64 im) { fp2 r; r.re = re; r.im = im; return r; }
 TP_HD fp2 f2zero() { return mk(0, 0); }
 TP_HD bool f2is0(fp2 a) { return (a.re | a.im) == 0; }
@@ -76,6 +123,22 @@ TP_HD fp2 f2fold(fp2 a, fp2 b, fp2 r) { return f2add(a, f2mul(r, f2sub(b, a))); 
 // the same line at -1 and at 2
 TP_HD fp2 f2at_m1(fp2 a, fp2 b) { return f2sub(f2dbl(a), b); }
 TP_HD fp2 f2at_2(fp2 a, fp2 b) { return f2sub(f2dbl(b), a); }
+// lazy Fp2 (limbs nearly canonical in and out)
+TP_HD fp2 l2add(fp2 a, fp2 b) { return mk(ladd(a.re, b.re), ladd(a.im, b.im)); }
+TP_HD fp2 l2sub(fp2 a, fp2 b) { return mk(lsub(a.re, b.re), lsub(a.im, b.im)); }
+TP_HD fp2 l2mul(fp2 a, fp2 b)
+{
+    const u64 ac = lmul(a.re, b.re);
+    const u64 bd = lmul(a.im, b.im);
+    const u64 s = lmul(a.re + a.im, b.re + b.im);
+    return mk(fold61(ac + (2 * P61 - bd)), fold61(s + (4 * P61 - ac - bd)));
+}
+TP_HD fp2 l2canon(fp2 a) { return mk(canon61(a.re), canon61(a.im)); }
+// a + r (b - a)
+TP_HD fp2 l2fold(fp2 a, fp2 b, fp2 r) { return l2add(a, l2mul(r, l2sub(b, a))); }
+TP_HD fp2 l2at_m1(fp2 a, fp2 b) { return l2sub(l2add(a, a), b); }
+TP_HD fp2 l2at_2(fp2 a, fp2 b) { return l2sub(l2add(b, b), a); }
+
 // small signed integer -> field
 TP_HD u64 from_small(int k) { return k >= 0 ? (u64)k : P61 - (u64)(-k); }
 

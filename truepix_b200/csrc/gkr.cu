@@ -20,6 +20,7 @@
 //    shared memory -> last-block grid reduction (ticket), leaving the 8 u64 claim
 //    on the device.
 #include "gkr.h"
+#include "gkr_internal.cuh"
 #include "runtime.h"
 
 #include <algorithm>
@@ -34,94 +35,6 @@ namespace {
 constexpr int kThreads = 256;
 thread_local int t_launches = 0;
 
-__device__ __forceinline__ fp2 ld2(const fp2* p)
-{
-    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p));
-    return mk(v.x, v.y);
-}
-__device__ __forceinline__ fp2 ldcg2(const fp2* p)
-{
-    const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(p));
-    return mk(v.x, v.y);
-}
-__device__ __forceinline__ void st2(fp2* p, fp2 v)
-{
-    *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(v.re, v.im);
-}
-__device__ __forceinline__ void stcg2(fp2* p, fp2 v)
-{
-    __stcg(reinterpret_cast<ulonglong2*>(p), make_ulonglong2(v.re, v.im));
-}
-
-__device__ __forceinline__ fp2 warp_sum(fp2 v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const u64 r = __shfl_xor_sync(0xffffffffu, v.re, o);
-        const u64 i = __shfl_xor_sync(0xffffffffu, v.im, o);
-        v = f2add(v, mk(r, i));
-    }
-    return v;
-}
-
-// Sum NV Fp2 values over the whole grid. Every thread of every block must call
-// it. Per-block partials go to `partials`; the last block to finish (ticket)
-// adds them up, writes out[2*NV] and re-arms the ticket.
-template <int NV>
-__device__ void grid_reduce(fp2 (&acc)[NV], fp2* partials, unsigned* ticket, u64* out)
-{
-    __shared__ fp2 sm[kThreads / 32][NV];
-    __shared__ bool s_last;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int t = 0; t < NV; ++t) acc[t] = warp_sum(acc[t]);
-    if (lane == 0)
-#pragma unroll
-        for (int t = 0; t < NV; ++t) sm[warp][t] = acc[t];
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int t = 0; t < NV; ++t) {
-            fp2 v = lane < nw ? sm[lane][t] : f2zero();
-            v = warp_sum(v);
-            if (lane == 0) stcg2(partials + (size_t)blockIdx.x * NV + t, v);
-        }
-    }
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned prev = atomicAdd(ticket, 1u);
-        s_last = (prev == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    fp2 tot[NV];
-#pragma unroll
-    for (int t = 0; t < NV; ++t) tot[t] = f2zero();
-    for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
-#pragma unroll
-        for (int t = 0; t < NV; ++t) tot[t] = f2add(tot[t], ldcg2(partials + (size_t)i * NV + t));
-#pragma unroll
-    for (int t = 0; t < NV; ++t) tot[t] = warp_sum(tot[t]);
-    __syncthreads();
-    if (lane == 0)
-#pragma unroll
-        for (int t = 0; t < NV; ++t) sm[warp][t] = tot[t];
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int t = 0; t < NV; ++t) {
-            fp2 v = lane < nw ? sm[lane][t] : f2zero();
-            v = warp_sum(v);
-            if (lane == 0) {
-                out[2 * t] = v.re;
-                out[2 * t + 1] = v.im;
-            }
-        }
-    }
-    if (threadIdx.x == 0) *ticket = 0u;
-}
-
 enum { MODE_CLAIM = 0, MODE_FOLD_CLAIM = 1, MODE_EXPLICIT = 2 };
 
 struct ClaimArgs {
@@ -132,7 +45,7 @@ struct ClaimArgs {
     fp2 r;             // pending fold challenge
     int n_in;
     int n_pairs;       // claim pairs
-    int W, n_slices, wc, tc;
+    int W, n_slices, wc, tc;   // W = rows stored; rows >= W are identically zero
     fp2 K0;
     const fp2* L;
     const int2* ab;
@@ -148,6 +61,10 @@ template <int MODE>
 __device__ __forceinline__ void load_01(const ClaimArgs& a, int w, int p, fp2& x0, fp2& x1,
                                         bool store)
 {
+    if (w >= a.W) {  // a known-zero row (frame padding wires)
+        x0 = x1 = f2zero();
+        return;
+    }
     const fp2* row = a.A + (size_t)w * (size_t)a.n_in;
     if (MODE == MODE_CLAIM) {
         x0 = ld2(row + 2 * (size_t)p);
@@ -155,8 +72,8 @@ __device__ __forceinline__ void load_01(const ClaimArgs& a, int w, int p, fp2& x
     } else {
         const fp2* q = row + 4 * (size_t)p;
         const fp2 a0 = ld2(q), a1 = ld2(q + 1), a2 = ld2(q + 2), a3 = ld2(q + 3);
-        x0 = f2fold(a0, a1, a.r);
-        x1 = f2fold(a2, a3, a.r);
+        x0 = l2fold(a0, a1, a.r);
+        x1 = l2fold(a2, a3, a.r);
         if (store) {
             fp2* o = a.Aout + (size_t)w * (size_t)(a.n_in >> 1) + 2 * (size_t)p;
             st2(o, x0);
@@ -190,8 +107,8 @@ __global__ void __launch_bounds__(kThreads) claim_kernel(const ClaimArgs a)
             bt[1] = ld2(a.beta + 2 * (size_t)p + 1);
         } else if (MODE == MODE_FOLD_CLAIM) {
             const fp2* q = a.beta + 4 * (size_t)p;
-            bt[0] = f2fold(ld2(q), ld2(q + 1), a.r);
-            bt[1] = f2fold(ld2(q + 2), ld2(q + 3), a.r);
+            bt[0] = l2fold(ld2(q), ld2(q + 1), a.r);
+            bt[1] = l2fold(ld2(q + 2), ld2(q + 3), a.r);
             if (y == 0) {
                 st2(a.beta_out + 2 * (size_t)p, bt[0]);
                 st2(a.beta_out + 2 * (size_t)p + 1, bt[1]);
@@ -203,27 +120,38 @@ __global__ void __launch_bounds__(kThreads) claim_kernel(const ClaimArgs a)
             bt[3] = mk(a.t[10][p], a.t[11][p]);
         }
         if (MODE != MODE_EXPLICIT) {
-            bt[2] = f2at_m1(bt[0], bt[1]);
-            bt[3] = f2at_2(bt[0], bt[1]);
+            bt[2] = l2at_m1(bt[0], bt[1]);
+            bt[3] = l2at_2(bt[0], bt[1]);
         }
 
-        // linear part over this slice's wires
+        // linear part over this slice's wires. Products are nearly canonical
+        // (< 2^61 + 8); raw sums of up to 5 of them stay below 2^64, so the
+        // accumulators are folded once every 4 wires.
         const int w0 = y * a.wc, w1 = min(a.W, w0 + a.wc);
         if (MODE != MODE_EXPLICIT) {
             fp2 S0 = f2zero(), S1 = f2zero();
+            int pending = 0;
             for (int w = w0; w < w1; ++w) {
                 fp2 x0, x1;
                 load_01<MODE>(a, w, p, x0, x1, true);
                 const fp2 l = ld2(a.L + w);
                 if (!f2is0(l)) {
-                    S0 = f2add(S0, f2mul(l, x0));
-                    S1 = f2add(S1, f2mul(l, x1));
+                    const fp2 m0 = l2mul(l, x0), m1 = l2mul(l, x1);
+                    S0.re += m0.re; S0.im += m0.im;
+                    S1.re += m1.re; S1.im += m1.im;
+                    if (++pending == 4) {
+                        S0 = mk(fold61(S0.re), fold61(S0.im));
+                        S1 = mk(fold61(S1.re), fold61(S1.im));
+                        pending = 0;
+                    }
                 }
             }
+            S0 = mk(fold61(S0.re), fold61(S0.im));
+            S1 = mk(fold61(S1.re), fold61(S1.im));
             S[0] = S0;
             S[1] = S1;
-            S[2] = f2at_m1(S0, S1);
-            S[3] = f2at_2(S0, S1);
+            S[2] = l2at_m1(S0, S1);
+            S[3] = l2at_2(S0, S1);
         } else {
 #pragma unroll
             for (int t = 0; t < 4; ++t) S[t] = f2zero();
@@ -233,12 +161,12 @@ __global__ void __launch_bounds__(kThreads) claim_kernel(const ClaimArgs a)
                 fp2 x[4];
                 load_explicit(a, w, p, x);
 #pragma unroll
-                for (int t = 0; t < 4; ++t) S[t] = f2add(S[t], f2mul(l, x[t]));
+                for (int t = 0; t < 4; ++t) S[t] = l2add(S[t], l2mul(l, x[t]));
             }
         }
         if (y == 0)
 #pragma unroll
-            for (int t = 0; t < 4; ++t) S[t] = f2add(S[t], a.K0);
+            for (int t = 0; t < 4; ++t) S[t] = l2add(S[t], a.K0);
 
         // product terms c*V[a]*V[b] of this slice, grouped by b
         const int e0 = y * a.tc, e1 = min(a.n_terms, e0 + a.tc);
@@ -251,16 +179,16 @@ __global__ void __launch_bounds__(kThreads) claim_kernel(const ClaimArgs a)
                     fp2 xb[4];
                     if (MODE != MODE_EXPLICIT) {
                         load_01<MODE>(a, cur_b, p, xb[0], xb[1], false);
-                        xb[2] = f2at_m1(xb[0], xb[1]);
-                        xb[3] = f2at_2(xb[0], xb[1]);
-                        M[2] = f2at_m1(M[0], M[1]);
-                        M[3] = f2at_2(M[0], M[1]);
+                        xb[2] = l2at_m1(xb[0], xb[1]);
+                        xb[3] = l2at_2(xb[0], xb[1]);
+                        M[2] = l2at_m1(M[0], M[1]);
+                        M[3] = l2at_2(M[0], M[1]);
                     } else {
                         load_explicit(a, cur_b, p, xb);
                     }
 #pragma unroll
                     for (int t = 0; t < 4; ++t) {
-                        S[t] = f2add(S[t], f2mul(xb[t], M[t]));
+                        S[t] = l2add(S[t], l2mul(xb[t], M[t]));
                         M[t] = f2zero();
                     }
                     if (e == e1) break;
@@ -270,18 +198,19 @@ __global__ void __launch_bounds__(kThreads) claim_kernel(const ClaimArgs a)
                 if (MODE != MODE_EXPLICIT) {
                     fp2 x0, x1;
                     load_01<MODE>(a, a.ab[e].x, p, x0, x1, false);
-                    M[0] = f2add(M[0], f2mul(c, x0));
-                    M[1] = f2add(M[1], f2mul(c, x1));
+                    M[0] = l2add(M[0], l2mul(c, x0));
+                    M[1] = l2add(M[1], l2mul(c, x1));
                 } else {
                     fp2 x[4];
                     load_explicit(a, a.ab[e].x, p, x);
 #pragma unroll
-                    for (int t = 0; t < 4; ++t) M[t] = f2add(M[t], f2mul(c, x[t]));
+                    for (int t = 0; t < 4; ++t) M[t] = l2add(M[t], l2mul(c, x[t]));
                 }
             }
         }
+        // canonical before the exact (canonical) grid reduction
 #pragma unroll
-        for (int t = 0; t < 4; ++t) acc[t] = f2mul(bt[t], S[t]);
+        for (int t = 0; t < 4; ++t) acc[t] = l2canon(l2mul(bt[t], S[t]));
     }
     grid_reduce<4>(acc, a.partials, a.ticket, a.out8);
 }
@@ -298,17 +227,18 @@ __global__ void __launch_bounds__(kThreads)
     const int w = (int)(item / n_out);
     const fp2* src = w < W ? A + (size_t)w * n_in : beta;
     fp2* dst = w < W ? Aout + (size_t)w * n_out : beta_out;
-    st2(dst + i, f2fold(ld2(src + 2 * (size_t)i), ld2(src + 2 * (size_t)i + 1), r));
+    st2(dst + i, l2fold(ld2(src + 2 * (size_t)i), ld2(src + 2 * (size_t)i + 1), r));
 }
 
 // fin[w] = V[w][0] for every wire, fin[W] = beta[0]
-__global__ void gather_first_kernel(const fp2* __restrict__ A, int n_phys, int W,
+__global__ void gather_first_kernel(const fp2* __restrict__ A, int n_phys, int W_rows, int W,
                                     const fp2* __restrict__ beta, fp2* __restrict__ fin,
                                     fp2* __restrict__ fin_beta)
 {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w < W) st2(fin + w, ld2(A + (size_t)w * n_phys));
-    if (w == W) st2(fin_beta, ld2(beta));
+    // session tables hold nearly canonical limbs; outputs are canonical
+    if (w < W) st2(fin + w, w < W_rows ? l2canon(ld2(A + (size_t)w * n_phys)) : f2zero());
+    if (w == W) st2(fin_beta, l2canon(ld2(beta)));
 }
 
 // One block per 64 copies: stage the copies' copy_size bytes in shared memory,
@@ -448,20 +378,26 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
             for (int j = 0; j < 4; ++j) v[j] = __ldg(src + j);
             const fp2* l = lo + (base & fmask);
+            // 8 products < 2^61 + 8 each: fold the raw sum after four of them
             fp2 s = f2zero();
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                s = f2add(s, f2scale(ld2(l + 2 * j), reduce64(v[j].x)));
-                s = f2add(s, f2scale(ld2(l + 2 * j + 1), reduce64(v[j].y)));
+                const fp2 l0 = ld2(l + 2 * j), l1 = ld2(l + 2 * j + 1);
+                const u64 x0 = fold61(v[j].x), x1 = fold61(v[j].y);
+                s.re += lmul(l0.re, x0) + lmul(l1.re, x1);
+                s.im += lmul(l0.im, x0) + lmul(l1.im, x1);
+                if (j & 1) s = mk(fold61(s.re), fold61(s.im));
             }
-            acc[0] = f2add(acc[0], f2mul(s, ld2(hi + (base >> h))));
+            acc[0] = l2add(acc[0], l2mul(s, ld2(hi + (base >> h))));
         }
     } else {
         for (size_t i = tid; i < n; i += stride) {
-            const fp2 w = f2mul(ld2(hi + (i >> h)), ld2(lo + (i & fmask)));
-            acc[0] = f2add(acc[0], f2scale(w, reduce64(__ldg(x + i))));
+            const fp2 w = l2mul(ld2(hi + (i >> h)), ld2(lo + (i & fmask)));
+            const u64 xv = fold61(__ldg(x + i));
+            acc[0] = l2add(acc[0], mk(lmul(w.re, xv), lmul(w.im, xv)));
         }
     }
+    acc[0] = l2canon(acc[0]);
     grid_reduce<1>(acc, partials, ticket, out);
 }
 
@@ -494,6 +430,12 @@ void orient_terms(std::map<std::pair<int, int>, fp2>& terms, GateForm& out)
 }  // namespace
 
 int last_launch_count() { return t_launches; }
+
+void launch_eq_tables(const fp2* d_z, int h, int hb, fp2 init, fp2* lo, fp2* hi, cudaStream_t s)
+{
+    const size_t nt = ((size_t)1 << h) + ((size_t)1 << hb);
+    eq_tables_kernel<<<blocks_for(nt, kThreads), kThreads, 0, s>>>(d_z, h, hb, init, lo, hi);
+}
 
 bool build_gate_form(int n_gates, const int* type, const int* in0, const int* in1,
                      const u64* z_re, const u64* z_im, int n_wires, GateForm& out)
@@ -666,6 +608,22 @@ bool launch_claim_explicit(const DevGateForm& g, int n_copies, const u64* const*
 // ---------------------------------------------------------------------------
 // session
 
+namespace {
+
+bool session_alloc(EarlySession* S, size_t rows0, size_t rows1, cudaStream_t s)
+{
+    const size_t n = (size_t)S->n_copies0;
+    if (rows0) S->buf[0] = (fp2*)dev_alloc(sizeof(fp2) * rows0, s);
+    S->buf[1] = (fp2*)dev_alloc(sizeof(fp2) * rows1, s);
+    S->beta[0] = (fp2*)dev_alloc(sizeof(fp2) * n, s);
+    S->beta[1] = (fp2*)dev_alloc(sizeof(fp2) * n, s);
+    S->fin = (fp2*)dev_alloc(sizeof(fp2) * ((size_t)S->n_wires + 1), s);
+    return (!rows0 || S->buf[0]) && S->buf[1] && S->beta[0] && S->beta[1] && S->fin &&
+           workspace_init(S->ws, 1024, s);
+}
+
+}  // namespace
+
 EarlySession* session_create(int n_gates, const int* type, const int* in0, const int* in1,
                              const u64* z_re, const u64* z_im, int n_copies, int n_wires,
                              cudaStream_t s)
@@ -680,20 +638,12 @@ EarlySession* session_create(int n_gates, const int* type, const int* in0, const
     if (!build_gate_form(n_gates, type, in0, in1, z_re, z_im, n_wires, g)) return nullptr;
     EarlySession* S = new EarlySession();
     S->n_gates = n_gates;
-    S->n_wires = n_wires;
+    S->n_wires = S->W_rows = n_wires;
     S->n_copies = S->n_phys = S->n_copies0 = n_copies;
     S->stream = s;
+    S->Lc = f2zero();
+    S->L_host = g.L;
     if (!upload_gate_form(g, S->form, s)) {
-        session_destroy(S);
-        return nullptr;
-    }
-    const size_t vn = (size_t)n_wires * (size_t)n_copies;
-    S->buf[1] = (fp2*)dev_alloc(sizeof(fp2) * (vn / 2), s);
-    S->beta[0] = (fp2*)dev_alloc(sizeof(fp2) * (size_t)n_copies, s);
-    S->beta[1] = (fp2*)dev_alloc(sizeof(fp2) * (size_t)n_copies, s);
-    S->fin = (fp2*)dev_alloc(sizeof(fp2) * ((size_t)n_wires + 1), s);
-    if (!S->buf[1] || !S->beta[0] || !S->beta[1] || !S->fin ||
-        !workspace_init(S->ws, 1024, s)) {
         session_destroy(S);
         return nullptr;
     }
@@ -705,8 +655,7 @@ bool session_load_host(EarlySession* S, const u64* v_re, const u64* v_im, const 
 {
     const size_t vn = (size_t)S->n_wires * (size_t)S->n_copies0;
     cudaStream_t s = S->stream;
-    S->buf[0] = (fp2*)dev_alloc(sizeof(fp2) * vn, s);
-    if (!S->buf[0]) return false;
+    if (!session_alloc(S, vn, vn / 2, s)) return false;
     // the half-size ping buffer holds exactly one SoA limb array
     u64* stage_re = reinterpret_cast<u64*>(S->buf[1]);
     u64* stage_im = (u64*)dev_alloc(sizeof(u64) * vn, s);
@@ -718,9 +667,9 @@ bool session_load_host(EarlySession* S, const u64* v_re, const u64* v_im, const 
         S->launches++;
         ok = !cuda_failed(cudaGetLastError(), "pack values");
     }
-    // beta: stage through the finish buffer area of the second beta table
+    // beta: the second beta table (16 B x n) holds both limb arrays while packing
     const size_t n = (size_t)S->n_copies0;
-    u64* bst = reinterpret_cast<u64*>(S->beta[1]);  // 16 B x n holds both limbs
+    u64* bst = reinterpret_cast<u64*>(S->beta[1]);
     if (ok)
         ok = !cuda_failed(cudaMemcpyAsync(bst, b_re, 8 * n, cudaMemcpyHostToDevice, s), "H2D beta") &&
              !cuda_failed(cudaMemcpyAsync(bst + n, b_im, 8 * n, cudaMemcpyHostToDevice, s), "H2D beta");
@@ -739,12 +688,11 @@ bool session_load_device(EarlySession* S, const fp2* d_values, const fp2* d_beta
 {
     const size_t vn = (size_t)S->n_wires * (size_t)S->n_copies0;
     cudaStream_t s = S->stream;
+    if (!session_alloc(S, borrow ? 0 : vn, vn / 2, s)) return false;
     if (borrow) {
         S->buf[0] = const_cast<fp2*>(d_values);
         S->borrowed0 = true;
     } else {
-        S->buf[0] = (fp2*)dev_alloc(sizeof(fp2) * vn, s);
-        if (!S->buf[0]) return false;
         TP_CUDA_OK(cudaMemcpyAsync(S->buf[0], d_values, sizeof(fp2) * vn, cudaMemcpyDeviceToDevice, s),
                    "copy values");
     }
@@ -753,21 +701,46 @@ bool session_load_device(EarlySession* S, const fp2* d_values, const fp2* d_beta
     return true;
 }
 
+bool session_load_pixels(EarlySession* S, const PixSrc& px, const fp2* d_beta)
+{
+    if (!pixsrc_valid(px, S->n_copies0, S->n_wires)) return false;
+    cudaStream_t s = S->stream;
+    S->px = px;
+    S->pix_mode = true;
+    S->W_rows = pixsrc_rows(px);
+    const size_t C = (size_t)S->n_copies0, R = (size_t)S->W_rows;
+    // first fold writes rows x C/2 into buf[1]; later folds alternate with buf[0]
+    if (!session_alloc(S, R * std::max<size_t>(1, C / 4), R * (C / 2), s)) return false;
+    if (px.const_idx >= 0) S->Lc = f2scale(S->L_host[(size_t)px.const_idx], px.const_val);
+    TP_CUDA_OK(cudaMemcpyAsync(S->beta[0], d_beta, sizeof(fp2) * C, cudaMemcpyDeviceToDevice, s),
+               "copy beta");
+    return true;
+}
+
 static bool apply_pending_fold(EarlySession* S)
 {
     const int n_out = S->n_phys >> 1;
-    const int nxt = S->cur ^ 1;
-    const size_t items = (size_t)(S->n_wires + 1) * (size_t)n_out;
-    fold_rows_kernel<<<blocks_for(items, kThreads), kThreads, 0, S->stream>>>(
-        S->buf[S->cur], S->n_phys, S->buf[nxt], S->n_wires, S->beta[S->cur], S->beta[nxt],
-        S->pending_r);
-    S->launches++;
-    if (cuda_failed(cudaGetLastError(), "fold kernel launch")) return false;
+    const int nxt = S->pix_mode ? 1 : (S->cur ^ 1);
+    if (S->pix_mode) {
+        if (!launch_fold_pixels(S->px, S->W_rows, n_out, S->pending_r, S->buf[1], S->beta[0],
+                                S->beta[1], S->stream, &S->launches))
+            return false;
+        S->pix_mode = false;
+    } else {
+        const size_t items = (size_t)(S->W_rows + 1) * (size_t)n_out;
+        fold_rows_kernel<<<blocks_for(items, kThreads), kThreads, 0, S->stream>>>(
+            S->buf[S->cur], S->n_phys, S->buf[nxt], S->W_rows, S->beta[S->cur], S->beta[nxt],
+            S->pending_r);
+        S->launches++;
+        if (cuda_failed(cudaGetLastError(), "fold kernel launch")) return false;
+    }
     S->cur = nxt;
     S->n_phys = n_out;
     S->pending = false;
     return true;
 }
+
+static bool session_claim_launch(EarlySession* S, u64* d_out8);
 
 bool session_claim_async(EarlySession* S, u64* d_out8)
 {
@@ -775,7 +748,51 @@ bool session_claim_async(EarlySession* S, u64* d_out8)
         set_error(TP_ERR_ARG, "claim needs at least 2 copies (have %d)", S->n_copies);
         return false;
     }
-    ClaimArgs a = base_args(S->form, S->n_wires, S->n_copies / 2, S->ws);
+    // timer tag: 1000 * (pixel source) + 100 * (fold fused) + log2(copies claimed)
+    int lg = 0;
+    while ((1 << lg) < S->n_copies) ++lg;
+    timer_begin(S->stream, 1000 * (S->pix_mode ? 1 : 0) + 100 * (S->pending ? 1 : 0) + lg);
+    const bool ok = session_claim_launch(S, d_out8);
+    timer_end(S->stream);
+    return ok;
+}
+
+static bool session_claim_launch(EarlySession* S, u64* d_out8)
+{
+    if (S->pix_mode) {
+        const bool fold = S->pending;
+        PixClaimArgs a;
+        memset(&a, 0, sizeof(a));
+        a.px = S->px;
+        a.W_rows = S->W_rows;
+        a.n_pad = S->n_copies0;
+        a.n_out = S->n_copies0 / 2;
+        a.L = S->form.L;
+        a.K0 = S->form.K0;
+        a.Lc = S->Lc;
+        a.ab = S->form.ab;
+        a.cf = S->form.c;
+        a.n_terms = S->form.n_terms;
+        a.beta = S->beta[0];
+        a.beta_out = S->beta[1];
+        a.Aout = S->buf[1];
+        a.r = S->pending_r;
+        const unsigned blocks = fold ? (unsigned)((S->n_copies0 / 2 + 31) / 32)
+                                     : (unsigned)((S->n_copies0 + 63) / 64);
+        if (!workspace_init(S->ws, blocks, S->stream)) return false;
+        a.partials = S->ws.partials;
+        a.ticket = S->ws.ticket;
+        a.out8 = d_out8 ? d_out8 : S->ws.out8;
+        if (!launch_claim_pixels(a, fold, S->stream, &S->launches)) return false;
+        if (fold) {
+            S->pix_mode = false;
+            S->pending = false;
+            S->cur = 1;
+            S->n_phys = S->n_copies0 / 2;
+        }
+        return true;
+    }
+    ClaimArgs a = base_args(S->form, S->W_rows, S->n_copies / 2, S->ws);
     a.A = S->buf[S->cur];
     a.n_in = S->n_phys;
     a.beta = S->beta[S->cur];
@@ -827,8 +844,11 @@ bool session_fold(EarlySession* S, fp2 r)
 bool session_finish_async(EarlySession* S, fp2* d_wires, fp2* d_beta)
 {
     if (S->pending && !apply_pending_fold(S)) return false;
+    if (S->pix_mode)
+        return launch_gather_pixels(S->px, S->n_wires, S->beta[0], d_wires, d_beta, S->stream,
+                                    &S->launches);
     gather_first_kernel<<<blocks_for((size_t)S->n_wires + 1, kThreads), kThreads, 0, S->stream>>>(
-        S->buf[S->cur], S->n_phys, S->n_wires, S->beta[S->cur], d_wires, d_beta);
+        S->buf[S->cur], S->n_phys, S->W_rows, S->n_wires, S->beta[S->cur], d_wires, d_beta);
     S->launches++;
     return !cuda_failed(cudaGetLastError(), "finish kernel launch");
 }

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "fp2.cuh"
+#include "gkr_internal.cuh"
 
 namespace tp {
 
@@ -61,9 +62,13 @@ struct EarlySession {
     DevGateForm form;
     ClaimWorkspace ws;
     fp2* fin = nullptr;    // finish staging [n_wires + 1]
-    u64* host8 = nullptr;  // pinned 8 x u64
+    std::vector<fp2> L_host;  // the linear coefficients, kept for the constant wire
     cudaStream_t stream = nullptr;
     int launches = 0;      // kernels launched by this session
+    int W_rows = 0;        // rows stored; rows >= W_rows are identically zero
+    bool pix_mode = false; // the current table is the implicit table of a uint8 frame
+    PixSrc px;
+    fp2 Lc;                // L[const_idx] * const_val (pixel mode)
 };
 
 EarlySession* session_create(int n_gates, const int* type, const int* in0, const int* in1,
@@ -72,6 +77,8 @@ EarlySession* session_create(int n_gates, const int* type, const int* in0, const
 // fill from host SoA tables (reference ABI)
 bool session_load_host(EarlySession* S, const u64* v_re, const u64* v_im, const u64* b_re,
                        const u64* b_im);
+// the table of a uint8 frame, read from device bytes (d_beta: packed, copied)
+bool session_load_pixels(EarlySession* S, const PixSrc& px, const fp2* d_beta);
 // fill from device packed tables; borrow=true adopts d_values as the first buffer
 bool session_load_device(EarlySession* S, const fp2* d_values, const fp2* d_beta, bool borrow);
 // claim; d_out8 receives the 4 Fp2 (0, 1, -1, 2) on device

@@ -415,4 +415,65 @@ int tp_table_from_pixels(const void* d_pixels, int n_copies, int n_copies_padded
                                         pick(stream, c)) ? 0 : -1;
 }
 
+void* tp_early_create_pixels(int n_gates, const int* gate_type, const int* in0, const int* in1,
+                             const uint64_t* z1_real, const uint64_t* z1_imag,
+                             const void* d_pixels, int n_copies, int n_copies_padded,
+                             int copy_size, int n_wires, int const_idx, uint64_t const_val,
+                             const void* d_beta, void* stream)
+{
+    tp::clear_error();
+    tp::Ctx* c = tp::ctx();
+    if (!c) return nullptr;
+    tp::EarlySession* S = tp::session_create(n_gates, gate_type, in0, in1, U(z1_real), U(z1_imag),
+                                             n_copies_padded, n_wires, pick(stream, c));
+    if (!S) return nullptr;
+    tp::PixSrc px;
+    px.pix = static_cast<const unsigned char*>(d_pixels);
+    px.n_real = n_copies;
+    px.cs = copy_size;
+    px.const_idx = const_idx;
+    px.const_val = const_val;
+    if (!tp::session_load_pixels(S, px, static_cast<const fp2*>(d_beta))) {
+        tp::session_destroy(S);
+        return nullptr;
+    }
+    return S;
+}
+
+int tp_mle_eval_pixels(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size,
+                       int n_wires, int const_idx, uint64_t const_val, const void* d_z,
+                       void* d_out, void* stream)
+{
+    tp::clear_error();
+    tp::Ctx* c = tp::ctx();
+    if (!c) return -1;
+    tp::PixSrc px;
+    px.pix = static_cast<const unsigned char*>(d_pixels);
+    px.n_real = n_copies;
+    px.cs = copy_size;
+    px.const_idx = const_idx;
+    px.const_val = const_val;
+    int launches = 0;
+    return tp::launch_mle_pixels(px, n_copies_padded, n_wires, static_cast<const fp2*>(d_z),
+                                 static_cast<fp2*>(d_out), pick(stream, c), &launches) ? 0 : -1;
+}
+
+int tp_early_rounds_dev(void* handle, int n_rounds, const uint64_t* challenges, void* d_claims)
+{
+    tp::clear_error();
+    if (!handle || n_rounds < 0) return -1;
+    tp::EarlySession* S = static_cast<tp::EarlySession*>(handle);
+    u64* out = static_cast<u64*>(d_claims);
+    for (int k = 0; k < n_rounds; ++k) {
+        if (!tp::session_claim_async(S, out ? out + 8 * (size_t)k : nullptr)) return -1;
+        if (!tp::session_fold(S, mk(challenges[2 * k], challenges[2 * k + 1]))) return -1;
+    }
+    return 0;
+}
+
+int tp_timer_enable(int max_pairs) { return tp::timer_enable(max_pairs) ? 0 : -1; }
+void tp_timer_disable(void) { tp::timer_disable(); }
+void tp_timer_reset(void) { tp::timer_reset(); }
+int tp_timer_read(float* ms, int* tags, int max_pairs) { return tp::timer_read(ms, tags, max_pairs); }
+
 }  // extern "C"

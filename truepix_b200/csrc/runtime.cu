@@ -5,7 +5,9 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
+#include <vector>
 
 namespace tp {
 
@@ -141,6 +143,54 @@ bool upload_async(void* d_dst, const void* h_src, size_t bytes, cudaStream_t s)
         return false;
     g_ring_used[slot] = true;
     return !cuda_failed(cudaEventRecord(g_ring_ev[slot], s), "staging record");
+}
+
+namespace {
+std::vector<cudaEvent_t> g_tev;
+std::vector<int> g_ttag;
+int g_tn = 0;      // events recorded
+bool g_ton = false;
+}  // namespace
+
+bool timer_enable(int max_pairs)
+{
+    if (!ctx()) return false;
+    while ((int)g_tev.size() < 2 * max_pairs) {
+        cudaEvent_t e;
+        if (cuda_failed(cudaEventCreate(&e), "timer event")) return false;
+        g_tev.push_back(e);
+    }
+    g_ttag.assign((size_t)max_pairs, 0);
+    g_tn = 0;
+    g_ton = true;
+    return true;
+}
+void timer_disable() { g_ton = false; }
+void timer_reset() { g_tn = 0; }
+bool timer_on() { return g_ton; }
+void timer_begin(cudaStream_t s, int tag)
+{
+    if (!g_ton || g_tn + 2 > (int)g_tev.size()) return;
+    g_ttag[(size_t)(g_tn / 2)] = tag;
+    cudaEventRecord(g_tev[(size_t)g_tn++], s);
+}
+void timer_end(cudaStream_t s)
+{
+    if (!g_ton || (g_tn & 1) == 0) return;
+    cudaEventRecord(g_tev[(size_t)g_tn++], s);
+}
+int timer_read(float* ms, int* tags, int max_pairs)
+{
+    const int n = std::min(g_tn / 2, max_pairs);
+    for (int i = 0; i < n; ++i) {
+        float t = 0.f;
+        if (cuda_failed(cudaEventElapsedTime(&t, g_tev[(size_t)2 * i], g_tev[(size_t)2 * i + 1]),
+                        "timer read"))
+            return -1;
+        ms[i] = t;
+        tags[i] = g_ttag[(size_t)i];
+    }
+    return n;
 }
 
 }  // namespace tp

@@ -38,6 +38,16 @@ void dev_free(void* p, cudaStream_t s);
 // uploads are copied synchronously.
 bool upload_async(void* d_dst, const void* h_src, size_t bytes, cudaStream_t s);
 
+// Kernel timer: when enabled, kernels that support it record a CUDA event pair
+// around their launch with an integer tag; read back after synchronising.
+bool timer_enable(int max_pairs);
+void timer_disable();
+void timer_reset();
+bool timer_on();
+void timer_begin(cudaStream_t s, int tag);
+void timer_end(cudaStream_t s);
+int timer_read(float* ms, int* tags, int max_pairs);
+
 // grid sizing helpers ----------------------------------------------------
 inline unsigned blocks_for(size_t n, unsigned threads)
 {

@@ -7,13 +7,17 @@ of copy c is byte c*384 + w, wire `const_idx` holds the circuit constant, wires
 up to 512 and padded copies are zero. For one frame the prover runs, on one
 stream and without host synchronisation:
 
-  1. tp_table_from_pixels  -> wire-major Fp2 table V[512][C] + copy-major inputs
-  2. tp_compute_beta_dev   -> beta over the copy challenges z2
-  3. early session: nCopyBits x (claim, fold)  (TruePix-main/libTruePix/
-     layerprover.py:144-290 drives the same calls through the bridge)
-  4. tp_early_finish_dev   -> the 512 folded wire values and beta
-  5. tp_mle_eval_base_dev  -> MLE of the input vector at the final input point
-     (TruePix-main/libTruePix/circuitnizkvec_vole.py:489-498)
+  1. tp_compute_beta_dev     -> beta over the copy challenges z2
+  2. tp_early_create_pixels  -> early session over the frame's bytes
+  3. nCopyBits x (claim, fold)  (TruePix-main/libTruePix/layerprover.py:144-290
+     drives the same calls through the bridge); rounds 0 and 1 read the bytes,
+     later rounds the folded Fp2 table in HBM
+  4. tp_early_finish_dev     -> the 512 folded wire values and beta
+  5. tp_mle_eval_pixels      -> MLE of the input vector at the final input point
+     (TruePix-main/libTruePix/circuitnizkvec_vole.py:489-498), from the bytes
+
+mode="table" instead materialises the 2^23-entry table and the copy-major input
+vector first (tp_table_from_pixels) and runs the generic table kernels.
 
 Challenges come from the host transcript in TruePix; here they are arguments.
 """
@@ -66,11 +70,14 @@ def pack_fp2(re: np.ndarray, im: np.ndarray) -> np.ndarray:
 class GkrInputLayerProver:
     """Holds device buffers for one frame size and proves frames into them."""
 
-    def __init__(self, layout: FrameLayout, gate_type, in0, in1, device: int = 0, stream=None):
+    def __init__(self, layout: FrameLayout, gate_type, in0, in1, device: int = 0, stream=None,
+                 mode: str = "pixels"):
         import torch
+        assert mode in ("pixels", "table")
         self.torch = torch
         self.lib = native.gkr()
         self.L = layout
+        self.mode = mode
         self.dev = torch.device("cuda", device)
         self.gt = np.ascontiguousarray(gate_type, np.int32)
         self.i0 = np.ascontiguousarray(in0, np.int32)
@@ -78,8 +85,9 @@ class GkrInputLayerProver:
         C, W = layout.padded_copies, layout.n_wires
         self.stream = stream
         i64 = torch.int64
-        self.table = torch.empty(2 * W * C, dtype=i64, device=self.dev)
-        self.inputs = torch.empty(W * C, dtype=i64, device=self.dev)
+        if mode == "table":
+            self.table = torch.empty(2 * W * C, dtype=i64, device=self.dev)
+            self.inputs = torch.empty(W * C, dtype=i64, device=self.dev)
         self.beta = torch.empty(2 * C, dtype=i64, device=self.dev)
         self.claims = torch.zeros(8 * layout.n_copy_bits, dtype=i64, device=self.dev)
         self.wires = torch.zeros(2 * (W + 1), dtype=i64, device=self.dev)
@@ -99,29 +107,38 @@ class GkrInputLayerProver:
         lib, L, s = self.lib, self.L, self._s()
         C, W, nb = L.padded_copies, L.n_wires, L.n_copy_bits
         launches = 0
-        native.check(lib, lib.tp_table_from_pixels(pixels.data_ptr(), L.copies, C, L.copy_size, W,
-                                                    L.const_idx, L.const_val,
-                                                    self.table.data_ptr(),
-                                                    self.inputs.data_ptr(), s), "table")
-        launches += 1
+        if self.mode == "table":
+            native.check(lib, lib.tp_table_from_pixels(pixels.data_ptr(), L.copies, C,
+                                                        L.copy_size, W, L.const_idx, L.const_val,
+                                                        self.table.data_ptr(),
+                                                        self.inputs.data_ptr(), s), "table")
+            launches += 1
         native.check(lib, lib.tp_compute_beta_dev(z2_dev.data_ptr(), nb, 1, 0,
                                                   self.beta.data_ptr(), s), "beta")
         launches += 2
         z1r = np.ascontiguousarray(z1[0], np.uint64)
         z1i = np.ascontiguousarray(z1[1], np.uint64)
-        h = lib.tp_early_create_dev(self.gt.size, self.gt.ctypes.data, self.i0.ctypes.data,
-                                    self.i1.ctypes.data, z1r.ctypes.data, z1i.ctypes.data, C, W,
-                                    self.table.data_ptr(), self.beta.data_ptr(), 1, s)
+        if self.mode == "table":
+            h = lib.tp_early_create_dev(self.gt.size, self.gt.ctypes.data, self.i0.ctypes.data,
+                                        self.i1.ctypes.data, z1r.ctypes.data, z1i.ctypes.data, C,
+                                        W, self.table.data_ptr(), self.beta.data_ptr(), 1, s)
+        else:
+            h = lib.tp_early_create_pixels(self.gt.size, self.gt.ctypes.data, self.i0.ctypes.data,
+                                           self.i1.ctypes.data, z1r.ctypes.data, z1i.ctypes.data,
+                                           pixels.data_ptr(), L.copies, C, L.copy_size, W,
+                                           L.const_idx, L.const_val, self.beta.data_ptr(), s)
         if not h:
             native.check(lib, -1, "early_create")
         try:
             base = self.claims.data_ptr()
-            for k in range(nb):
-                if claim_hook is not None:
-                    claim_hook(k, "pre")
+            if claim_hook is None:
+                ch = np.ascontiguousarray(challenges, np.uint64).reshape(-1)
+                native.check(lib, lib.tp_early_rounds_dev(
+                    h, nb, ch.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), base), "rounds")
+            for k in range(nb if claim_hook is not None else 0):
+                claim_hook(k, "pre")
                 native.check(lib, lib.tp_early_claim_dev(h, base + 64 * k), "claim")
-                if claim_hook is not None:
-                    claim_hook(k, "post")
+                claim_hook(k, "post")
                 native.check(lib, lib.native_fp2_early_fold(h, int(challenges[k][0]),
                                                             int(challenges[k][1])), "fold")
             wp = self.wires.data_ptr()
@@ -129,8 +146,15 @@ class GkrInputLayerProver:
             launches += lib.tp_early_launches(h)
         finally:
             lib.native_fp2_early_destroy(h)
-        native.check(lib, lib.tp_mle_eval_base_dev(self.inputs.data_ptr(), point_dev.data_ptr(),
-                                                   L.n_in_bits + nb, self.mle.data_ptr(), s), "mle")
+        if self.mode == "table":
+            native.check(lib, lib.tp_mle_eval_base_dev(self.inputs.data_ptr(),
+                                                       point_dev.data_ptr(), L.n_in_bits + nb,
+                                                       self.mle.data_ptr(), s), "mle")
+        else:
+            native.check(lib, lib.tp_mle_eval_pixels(pixels.data_ptr(), L.copies, C, L.copy_size,
+                                                     W, L.const_idx, L.const_val,
+                                                     point_dev.data_ptr(), self.mle.data_ptr(),
+                                                     s), "mle")
         launches += 2
         self.launches_last = launches
 

@@ -50,6 +50,14 @@ GKR_SIGNATURES = {
     "tp_compute_beta_dev": (_I32, [_VP, _I32, _U64, _U64, _VP, _VP]),
     "tp_mle_eval_base_dev": (_I32, [_VP, _VP, _I32, _VP, _VP]),
     "tp_table_from_pixels": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
+    "tp_early_create_pixels": (_VP, [_I32, _VP, _VP, _VP, _VP, _VP, _VP, _I32, _I32, _I32, _I32,
+                                     _I32, _U64, _VP, _VP]),
+    "tp_mle_eval_pixels": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
+    "tp_early_rounds_dev": (_I32, [_VP, _I32, _PU64, _VP]),
+    "tp_timer_enable": (_I32, [_I32]),
+    "tp_timer_disable": (None, []),
+    "tp_timer_reset": (None, []),
+    "tp_timer_read": (_I32, [ctypes.POINTER(ctypes.c_float), _PI32, _I32]),
 }
 
 _cache = {}
