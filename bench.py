@@ -1,20 +1,29 @@
 """Benchmark: proved 1080p frames/s on one B200 (GKR input layer of the gray circuit).
 
-Workload (one "step" = one frame): a seeded 1920x1080x3 uint8 frame, 16,200
-copies of 384 bytes padded to 16,384 x 512 input wires (2^23), proven by the
-device-resident path in truepix_b200.frame: table build from the pixels, beta
-over the 14 copy challenges, 14 early sumcheck rounds (claim + fold), finish,
-and the MLE of the 2^23-entry input vector at the final point. Inputs stay in
-HBM (every frame's table, 128 MiB, and input vector, 64 MiB, exceed the 126 MB
-L2, so no flush is needed).
+Workload: seeded 1920x1080x3 uint8 frames; each frame is 16,200 copies of 384
+bytes padded to 16,384 x 512 input wires (2^23) and is proven by the
+device-resident path (truepix_b200.frame): beta over the 14 copy challenges, 14
+early sumcheck rounds (claim + fold; rounds 0 and 1 read the frame's bytes),
+finish, and the MLE of the 2^23-entry input vector at the final point.
 
-  value      frames/s over all ranks, device time (CUDA events), inputs resident
-  e2e        frames/s through the reference C ABI (native_fp2_*) with pinned
-             host buffers: H2D of the tables and D2H of every claim inside
-  roofline   the fused fold+claim kernel: algorithmic bytes (48 B per folded
-             element) / its event-timed duration, against MEASURED_PEAKS.json
+One step = one batch of B frames (default 64) proven together, one kernel
+launch per round for the whole batch (BatchFrameProver). Inputs stay in HBM:
+B distinct frames (400 MB of bytes) and their folded tables (~4.8 GB) are far
+larger than the 126 MB L2, so no flush is needed.
+
+  value         frames/s over all ranks, device time (CUDA events), batched
+  plain         frames/s of single-frame proofs (one session per frame), same
+                device timing -- the batched/plain ratio is reported
+  e2e           the batched path from pinned host frames: H2D of the bytes, and
+                every round a D2H of all claims with a synchronise (the host
+                needs them for its transcript) inside the timed region
+  e2e_reference_abi  one frame through the reference C ABI (native_fp2_*) with
+                pinned host SoA tables
+  roofline      the claim kernel with the largest share: algorithmic bytes (per
+                launch kind, see kernel_groups) / its event-timed duration,
+                against MEASURED_PEAKS.json
   cpu_baseline  the reference CPU library (built from the reference's source)
-             proving one frame of the same workload on one host core
+                proving one frame of the same workload on one host core
 
 `--impl reference` times that reference CPU library on all host cores instead
 (one frame per worker process per step) and prints the same metric.
@@ -214,9 +223,11 @@ def profiled_traffic():
     return None
 
 
-def kernel_groups(ms, tags, layout):
-    """Per claim-kernel kind: launches, total time and algorithmic bytes.
-    tag = 1000*(reads pixels) + 100*(fold fused) + log2(copies claimed)."""
+def kernel_groups(ms, tags, layout, batch=1):
+    """Per claim-kernel kind: launches, total time, algorithmic bytes, folded elements.
+    tag = 1000*(reads bytes) + 100*(fold fused) + log2(copies claimed per frame).
+    Algorithmic bytes per frame: bytes read once + folded Fp2 rows written (16 B
+    per element) + table rows read (16 B per element) + beta."""
     rows = layout.const_idx + 1 if layout.const_idx >= 0 else layout.copy_size
     pix_bytes = layout.copies * layout.copy_size
     groups = {}
@@ -224,17 +235,19 @@ def kernel_groups(ms, tags, layout):
         pix, fold, lg = tag // 1000, (tag // 100) % 10, tag % 100
         n = 1 << lg                                    # copies claimed
         if pix and not fold:
-            name, byt = "claim_pixels_kernel", pix_bytes + 16 * n
+            name, byt, el = "pix_claim_kernel", pix_bytes + 16 * n, 0
         elif pix and fold:
-            name, byt = "fold_claim_pixels_kernel", pix_bytes + 16 * rows * n + 48 * n
+            name, byt, el = "pix_fold_claim_kernel", pix_bytes + 16 * rows * n + 48 * n, rows * n
         elif fold:
-            name, byt = "claim_kernel<FOLD_CLAIM>", 48 * rows * n + 48 * n
+            name, byt, el = "table_round_kernel<fold>", 48 * rows * n + 48 * n, rows * n
         else:
-            name, byt = "claim_kernel<CLAIM>", 16 * rows * n + 16 * n
-        g = groups.setdefault(name, {"launches": 0, "ms": 0.0, "bytes": 0.0, "by_copies": {}})
+            name, byt, el = "table_round_kernel<claim>", 16 * rows * n + 16 * n, 0
+        g = groups.setdefault(name, {"launches": 0, "ms": 0.0, "bytes": 0.0, "folded": 0,
+                                     "by_copies": {}})
         g["launches"] += 1
         g["ms"] += t
-        g["bytes"] += byt
+        g["bytes"] += byt * batch
+        g["folded"] += el * batch
         bc = g["by_copies"].setdefault(n, [0, 0.0])
         bc[0] += 1
         bc[1] += t
@@ -246,63 +259,89 @@ def ours_arm(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
     from truepix_b200 import native
-    from truepix_b200.frame import FrameLayout, GkrInputLayerProver, pack_fp2
+    from truepix_b200.frame import BatchFrameProver, FrameLayout, GkrInputLayerProver, pack_fp2
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     layout = FrameLayout.for_frame(H, Wd)
     gt, i0, i1 = circuit()
+    B = args.batch
+    nb = layout.n_copy_bits
     rng = np.random.default_rng(SEED + 101 * rank)
-    n_frames = 4
-    frames, z1, z2, point, chal = make_inputs(rng, layout, n_frames)
+    frames, z1, z2, point, chal = make_inputs(rng, layout, B)
     pix = [torch.from_numpy(f).to(dev) for f in frames]
     z2_dev = torch.from_numpy(pack_fp2(z2[:, 0], z2[:, 1])).to(dev)
     pt_dev = torch.from_numpy(pack_fp2(point[:, 0], point[:, 1])).to(dev)
+    chal_b = np.ascontiguousarray(np.broadcast_to(chal[:, None, :], (nb, B, 2)))
     stream = torch.cuda.Stream(dev)
-    prover = GkrInputLayerProver(layout, gt, i0, i1, device=local_rank, stream=stream)
     lib = native.gkr()
-    nb = layout.n_copy_bits
+    bprover = BatchFrameProver([layout] * B, gt, i0, i1, device=local_rank, stream=stream)
+    z1s = [z1] * B
+    z2s = z2_dev.repeat(B)      # packed [B][nb]
+    pts = pt_dev.repeat(B)      # packed [B][9 + nb]
 
+    def run_batch(hook=None):
+        bprover.prove(pix, z1s, z2s, pts, chal_b, round_hook=hook)
+
+    # ---- plain single-frame proofs (the baseline of the batched/plain ratio)
+    plain = GkrInputLayerProver(layout, gt, i0, i1, device=local_rank, stream=stream)
+    n_plain = 0 if args.no_plain else max(10, min(200, 4 * B))
+    plain_fps = None
+    if n_plain:
+        with torch.cuda.stream(stream):
+            for i in range(5):
+                plain.prove(pix[i % B], z1, z2_dev, pt_dev, chal)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for i in range(n_plain):
+                plain.prove(pix[i % B], z1, z2_dev, pt_dev, chal)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        plain_fps = n_plain / (e0.elapsed_time(e1) / 1e3)
+
+    # ---- batched: the timed region
     with torch.cuda.stream(stream):
         for i in range(args.warmup):
-            prover.prove(pix[i % n_frames], z1, z2_dev, pt_dev, chal)
+            run_batch()
     torch.cuda.synchronize()
-    native.check(lib, lib.tp_timer_enable(args.steps * nb + 16), "timer")
+    native.check(lib, lib.tp_timer_enable(args.steps * nb * 2 + 16), "timer")
     clk = ClockSampler(local_rank)
     clk.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     lib.tp_timer_reset()
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     launches = 0
     clk.t0 = time.time()
     with torch.cuda.stream(stream):
-        start.record(stream)
+        evs[0].record(stream)
         for i in range(args.steps):
-            prover.prove(pix[i % n_frames], z1, z2_dev, pt_dev, chal)
-            launches += prover.launches_last
-        end.record(stream)
+            run_batch()
+            launches += bprover.launches_last
+            evs[i + 1].record(stream)
     torch.cuda.synchronize()
     clk.t1 = time.time()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     clk.stop()
-    npairs = args.steps * nb + 16
+    npairs = args.steps * nb * 2 + 16
     tms = (ctypes.c_float * npairs)()
     ttags = (ctypes.c_int * npairs)()
     got = lib.tp_timer_read(tms, ttags, npairs)
     lib.tp_timer_disable()
-    ms = start.elapsed_time(end)
+    ms = evs[0].elapsed_time(evs[-1])
+    per_batch = sorted(evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps))
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
-    value = world * args.steps / (ms / 1e3)
+    frames_done = args.steps * B
+    value = world * frames_done / (ms / 1e3)
 
-    groups = kernel_groups(list(tms[:max(0, got)]), list(ttags[:max(0, got)]), layout)
+    groups = kernel_groups(list(tms[:max(0, got)]), list(ttags[:max(0, got)]), layout, B)
     peak, peak_kind = peaks()
     kernels = []
     for name, g in sorted(groups.items(), key=lambda kv: -kv[1]["ms"]):
@@ -311,30 +350,31 @@ def ours_arm(args, rank, world, local_rank):
                         "share_of_step": g["ms"] / ms, "achieved_gbs": ach,
                         "avg_us_by_copies": {str(k): round(1e3 * v[1] / v[0], 2)
                                              for k, v in sorted(g["by_copies"].items())}})
-    top = kernels[0] if kernels else None
-    traffic = profiled_traffic()
     roof = None
-    if top:
+    traffic = profiled_traffic()
+    if kernels:
+        top = kernels[0]
         g = groups[top["kernel"]]
         roof = {"kernel": top["kernel"], "bound": "hbm", "achieved": top["achieved_gbs"],
                 "peak": peak, "unit": "GB/s",
                 "frac": top["achieved_gbs"] / peak if top["achieved_gbs"] else None,
-                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                "peak_source": (peak_kind + " hbm_gbs (MEASURED_PEAKS.json)") if peak_kind == "measured"
                 else "fallback 6650 GB/s",
                 "algorithmic_bytes_per_launch": g["bytes"] / g["launches"],
                 "avg_launch_us": 1e3 * g["ms"] / g["launches"], "launches_timed": g["launches"],
                 "traffic": (traffic or {}).get(top["kernel"]),
                 "all_claim_kernels": kernels}
+    folded = sum(g["folded"] for g in groups.values())
 
     res_ok = None
     if rank == 0:
-        c, w, b, m = prover.results()
+        c, w, b, m = bprover.results(B - 1)
         res_ok = bool(c.any() and w.any() and m != (0, 0))
 
-    e2e = None
-    cpu = None
+    e2e = e2e_ref = cpu = None
     if rank == 0 and not args.skip_e2e:
-        e2e = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
+        e2e = e2e_batched(args, bprover, frames, z1s, z2s, pts, chal_b, stream, dev)
+        e2e_ref = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
     if rank == 0 and world == 1 and not args.skip_cpu:
         secs, kind = _cpu_worker((0, 1))
         cpu = {"value": 1.0 / secs, "unit": UNIT, "cores": 1, "kind": kind,
@@ -349,14 +389,61 @@ def ours_arm(args, rank, world, local_rank):
             "config": {"workload": "gkr_input_layer_gray_1080p", "frame": [H, Wd, 3],
                        "copies": layout.copies, "padded_copies": layout.padded_copies,
                        "wires": layout.padded_copies * layout.n_wires, "rounds": nb,
-                       "circuit": "gray.pws", "path": "pixels (tp_early_create_pixels)",
-                       "l2": "inputs > L2: 4 distinct frames cycled; the folded table of "
-                             "round 1 (47 MiB) is rewritten every frame",
+                       "circuit": "gray.pws", "batch": B, "step": f"one batch of {B} frames",
+                       "path": "bytes -> batched rounds (tp_batch_*)",
+                       "l2": "inputs > L2: B distinct frames (0.4 GB) and their folded "
+                             "tables (~4.8 GB) per step",
                        "parallelism": f"replicas x{world}"},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "plain": {"value": plain_fps, "unit": UNIT, "frames": n_plain,
+                      "what": "single-frame sessions back to back, same device timing"},
+            "batched_over_plain": (value / world / plain_fps) if plain_fps else None,
+            "fp2_elem_per_s": folded / (ms / 1e3),
+            "latency_ms_per_batch": {"p50": per_batch[len(per_batch) // 2],
+                                     "p99": per_batch[min(len(per_batch) - 1,
+                                                          int(0.99 * len(per_batch)))]},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
             "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
         }
         print(json.dumps(line), flush=True)
+
+
+def e2e_batched(args, bprover, frames, z1s, z2s, pts, chal_b, stream, dev):
+    """The batched path from pinned host frames: H2D of every frame's bytes, a D2H
+    of all claims after every round with a synchronise, D2H of wires and MLEs."""
+    import torch
+    B = bprover.B
+    host = [torch.from_numpy(f).pin_memory() for f in frames]
+    dpix = [torch.empty_like(h, device=dev) for h in host]
+    R = bprover.max_rounds
+    claims_h = torch.zeros(B * 8, dtype=torch.int64).pin_memory()
+    wires_h = torch.zeros_like(bprover.wires, device="cpu").pin_memory()
+    mle_h = torch.zeros_like(bprover.mle, device="cpu").pin_memory()
+
+    def hook(k):
+        claims_h.copy_(bprover.claims[k * B * 8:(k + 1) * B * 8], non_blocking=True)
+        stream.synchronize()
+
+    def one():
+        with torch.cuda.stream(stream):
+            for d, h in zip(dpix, host):
+                d.copy_(h, non_blocking=True)
+            bprover.prove(dpix, z1s, z2s, pts, chal_b, round_hook=hook)
+            wires_h.copy_(bprover.wires, non_blocking=True)
+            mle_h.copy_(bprover.mle, non_blocking=True)
+        stream.synchronize()
+
+    one()
+    steps = max(2, min(args.steps, 8))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    wall = time.perf_counter() - t0
+    h2d = sum(f.nbytes for f in frames)
+    d2h = R * B * 64 + bprover.wires.numel() * 8 + bprover.mle.numel() * 8
+    return {"value": steps * B / wall, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "steps": steps, "frames_per_step": B,
+            "timer": "host wall clock", "path": "tp_batch_* from pinned host frames, "
+            "claims read back every round"}
 
 
 def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
@@ -406,7 +493,7 @@ def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
 
     for _ in range(max(1, min(args.warmup, 3))):
         one()
-    steps = max(3, min(args.steps // 100, 20))
+    steps = max(3, min(args.steps, 20))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -424,8 +511,10 @@ def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3000)
-    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--no-plain", action="store_true", help="skip the single-frame measurement")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")

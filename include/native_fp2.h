@@ -18,7 +18,7 @@
  * The tp_* entry points are extensions: error reporting and device-buffer
  * variants whose Fp2 buffers are packed {re, im} pairs of uint64 (16 bytes per
  * element, 16-byte aligned) in device memory, asynchronous on `stream`
- * (a cudaStream_t; NULL selects the library's own stream).
+ * (a cudaStream_t; NULL is the CUDA default stream).
  */
 #ifndef TRUEPIX_NATIVE_FP2_H
 #define TRUEPIX_NATIVE_FP2_H
@@ -159,6 +159,47 @@ int tp_mle_eval_pixels(const void* d_pixels, int n_copies, int n_copies_padded, 
  * challenges[2k+1]) without returning to the caller in between: for callers that
  * already hold the challenges (replay, benchmarking). Asynchronous. */
 int tp_early_rounds_dev(void* handle, int n_rounds, const uint64_t* challenges, void* d_claims);
+
+/* ---- batches: one kernel launch per round for many frames ----
+ * A batch holds n_frames independent early sessions (own table, beta, gate
+ * weights z1, challenges; sizes may differ). tp_batch_claim evaluates the claim
+ * of every frame that still has at least 2 copies, with one launch per source
+ * kind present; frames whose early rounds are over are skipped and their claim
+ * slots left untouched. Asynchronous on the batch's stream. */
+void* tp_batch_create(int n_frames, void* stream);
+/* frame i from a uint8 frame in device memory (layout of tp_table_from_pixels) */
+int tp_batch_set_pixels(void* batch, int i, int n_gates, const int* gate_type, const int* in0,
+                        const int* in1, const uint64_t* z1_real, const uint64_t* z1_imag,
+                        const void* d_pixels, int n_copies, int n_copies_padded, int copy_size,
+                        int n_wires, int const_idx, uint64_t const_val, const void* d_beta);
+/* frame i from a packed device table (borrow as in tp_early_create_dev) */
+int tp_batch_set_table(void* batch, int i, int n_gates, const int* gate_type, const int* in0,
+                       const int* in1, const uint64_t* z1_real, const uint64_t* z1_imag,
+                       int n_copies, int n_wires, const void* d_values, const void* d_beta,
+                       int borrow);
+/* claims into d_claims[8 * i .. 8 * i + 7] (device, u64) */
+int tp_batch_claim(void* batch, void* d_claims);
+/* fold every frame that has >= 2 copies by (challenges[2i], challenges[2i+1]) (host array) */
+int tp_batch_fold(void* batch, const uint64_t* challenges);
+int tp_batch_n_copies(void* batch, int i);
+/* d_wires: frame i at d_wires + 16 * (sum of n_wires of frames < i) bytes -- with equal
+ * n_wires simply [n_frames][n_wires] packed Fp2; d_beta: [n_frames] packed Fp2 */
+int tp_batch_finish(void* batch, void* d_wires, void* d_beta);
+int tp_batch_launches(void* batch);
+/* forget every frame's configuration (tp_batch_set_* may be called again) while
+ * keeping the device buffers for the next batch of the same or smaller sizes */
+void tp_batch_reset(void* batch);
+void tp_batch_destroy(void* batch);
+
+/* beta tables of n_frames frames in one pass: d_z packed Fp2 [n_frames][n_z],
+ * d_out packed Fp2 [n_frames][2^n_z] (compute_beta with init 1). Async. */
+int tp_compute_beta_batch_dev(const void* d_z, int n_z, int n_frames, void* d_out, void* stream);
+/* tp_mle_eval_pixels for n_frames frames of one padded size in one pass:
+ * d_pixels / n_copies host arrays [n_frames]; d_points packed Fp2
+ * [n_frames][log2 n_wires + log2 n_copies_padded]; d_out packed Fp2 [n_frames]. */
+int tp_mle_eval_pixels_batch(int n_frames, const void* const* d_pixels, const int* n_copies,
+                             int n_copies_padded, int copy_size, int n_wires, int const_idx,
+                             uint64_t const_val, const void* d_points, void* d_out, void* stream);
 
 /* Claim-kernel timer: when enabled, every session claim records a CUDA event pair
  * with tag 1000*(reads pixels) + 100*(fold fused) + log2(copies claimed).

@@ -322,3 +322,66 @@ def test_frame_prover_vs_oracle(oracle_lib, circuits, name, hw, mode):
     assert np.array_equal(claims, oc)
     assert np.array_equal(wires[:, 0], wre) and np.array_equal(wires[:, 1], wim)
     assert beta == ob and mle == om
+
+
+def _oracle_frame(oracle_lib, gt, i0, i1, layout, pix, z1, z2, point, chal):
+    C, W, cs = layout.padded_copies, layout.n_wires, layout.copy_size
+    vals = np.zeros((C, W), np.uint64)
+    vals[:layout.copies, :cs] = pix.reshape(layout.copies, cs)
+    if layout.const_idx >= 0:
+        vals[:layout.copies, layout.const_idx] = layout.const_val
+    table = np.ascontiguousarray(vals.T).reshape(-1)
+    bre, bim = oracle_lib.compute_beta(np.ascontiguousarray(z2[:, 0]),
+                                       np.ascontiguousarray(z2[:, 1]), (1, 0))
+    oc, wre, wim, ob, _ = run_session(oracle_lib, gt, i0, i1, z1[0].copy(), z1[1].copy(), C, W,
+                                      table, np.zeros_like(table), bre, bim, chal)
+    om = oracle_lib.mle_eval_base(vals.reshape(-1).copy(), np.ascontiguousarray(point[:, 0]),
+                                  np.ascontiguousarray(point[:, 1]))
+    return oc, wre, wim, ob, om
+
+
+@pytest.mark.parametrize("name", ["gray", "Crop"])
+def test_batch_uneven_frames_vs_oracle(oracle_lib, circuits, name):
+    """A batch of frames of uneven size (1 to 16,200 copies): every frame's claims,
+    wires, beta and MLE equal the oracle's for that frame alone."""
+    import torch
+    from truepix_b200.frame import BatchFrameProver, FrameLayout, pack_fp2
+    rng = np.random.default_rng(77)
+    cs = 385 if name == "Crop" else 384
+    const = (385, 128) if name == "Crop" else (384, 128)
+    copies = [1, 2, 5, 100, 1000, 3000, 16200] if name == "gray" else [1, 7, 64, 700]
+    layouts = [FrameLayout(copies=c, copy_size=cs, const_idx=const[0], const_val=const[1])
+               for c in copies]
+    gt, i0, i1 = (circuits[name + "_" + k] for k in ("type", "in0", "in1"))
+    dev = torch.device("cuda", 0)
+    prover = BatchFrameProver(layouts, gt, i0, i1)
+    R, B = prover.max_rounds, len(layouts)
+    for rep in range(2):   # the same batch object serves consecutive batches
+        pix, z1s, z2s, pts = [], [], [], []
+        for L in layouts:
+            pix.append(rng.integers(0, 256, size=L.copies * cs, dtype=np.uint8))
+            z1s.append(np.stack([rand_fp(rng, gt.size), rand_fp(rng, gt.size)]))
+            nb = L.n_copy_bits
+            z2s.append(np.stack([rand_fp(rng, nb), rand_fp(rng, nb)], axis=1))
+            pts.append(np.stack([rand_fp(rng, nb + 9), rand_fp(rng, nb + 9)], axis=1))
+        chal = rng.integers(0, P61, size=(R, B, 2), dtype=np.uint64)
+        z2d, ptd = {}, {}
+        for C, fs in prover.groups.items():
+            z2d[C] = torch.from_numpy(np.concatenate(
+                [pack_fp2(z2s[f][:, 0], z2s[f][:, 1]) for f in fs])).to(dev)
+            ptd[C] = torch.from_numpy(np.concatenate(
+                [pack_fp2(pts[f][:, 0], pts[f][:, 1]) for f in fs])).to(dev)
+        prover.prove([torch.from_numpy(p).to(dev) for p in pix], z1s, z2d, ptd, chal)
+        torch.cuda.synchronize()
+        _check_batch(oracle_lib, gt, i0, i1, layouts, prover, pix, z1s, z2s, pts, chal)
+
+
+def _check_batch(oracle_lib, gt, i0, i1, layouts, prover, pix, z1s, z2s, pts, chal):
+    for f, L in enumerate(layouts):
+        claims, wires, beta, mle = prover.results(f)
+        nb = L.n_copy_bits
+        oc, wre, wim, ob, om = _oracle_frame(oracle_lib, gt, i0, i1, L, pix[f], z1s[f], z2s[f],
+                                             pts[f], chal[:nb, f])
+        assert np.array_equal(claims, oc), f"frame {f} ({L.copies} copies): claims"
+        assert np.array_equal(wires[:, 0], wre) and np.array_equal(wires[:, 1], wim), f"frame {f}"
+        assert beta == ob and mle == om, f"frame {f}"

@@ -22,7 +22,8 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
          "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
 
 LIBS = {
-    "libnative_fp2_gpu.so": ["runtime.cu", "gkr.cu", "gkr_pixels.cu", "native_fp2_abi.cu"],
+    "libnative_fp2_gpu.so": ["runtime.cu", "gkr.cu", "gkr_pixels.cu", "gkr_batch.cu", "gkr_session.cu",
+                             "native_fp2_abi.cu"],
 }
 
 

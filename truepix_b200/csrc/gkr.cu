@@ -230,17 +230,6 @@ __global__ void __launch_bounds__(kThreads)
     st2(dst + i, l2fold(ld2(src + 2 * (size_t)i), ld2(src + 2 * (size_t)i + 1), r));
 }
 
-// fin[w] = V[w][0] for every wire, fin[W] = beta[0]
-__global__ void gather_first_kernel(const fp2* __restrict__ A, int n_phys, int W_rows, int W,
-                                    const fp2* __restrict__ beta, fp2* __restrict__ fin,
-                                    fp2* __restrict__ fin_beta)
-{
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    // session tables hold nearly canonical limbs; outputs are canonical
-    if (w < W) st2(fin + w, w < W_rows ? l2canon(ld2(A + (size_t)w * n_phys)) : f2zero());
-    if (w == W) st2(fin_beta, l2canon(ld2(beta)));
-}
-
 // One block per 64 copies: stage the copies' copy_size bytes in shared memory,
 // then write the wire-major packed table V[w][c] (1 KB contiguous per wire) and
 // the copy-major base-field input vector x[c * W + w].
@@ -356,6 +345,40 @@ __global__ void beta_expand_kernel(const fp2* __restrict__ lo, const fp2* __rest
         out_re[i] = v.re;
         out_im[i] = v.im;
     }
+}
+
+// Batched eq tables: frame blockIdx.y, z at d_z + frame * z_stride, tables at
+// tabs + frame * (2^h + 2^hb) (lo first, then hi with `init` folded in).
+__global__ void eq_tables_batch_kernel(const fp2* __restrict__ d_z, int z_stride, int h, int hb,
+                                       fp2 init, fp2* __restrict__ tabs)
+{
+    const long long nlo = 1ll << h, nhi = 1ll << hb;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nlo + nhi) return;
+    const fp2* z = d_z + (size_t)blockIdx.y * z_stride;
+    fp2* t = tabs + (size_t)blockIdx.y * (size_t)(nlo + nhi);
+    const fp2 one = mk(1, 0);
+    fp2 v = idx < nlo ? one : init;
+    const long long bits = idx < nlo ? idx : idx - nlo;
+    const int n = idx < nlo ? h : hb, off = idx < nlo ? 0 : h;
+    for (int j = 0; j < n; ++j) {
+        const fp2 zj = ld2(z + off + j);
+        v = f2mul(v, ((bits >> j) & 1) ? zj : f2sub(one, zj));
+    }
+    st2(t + idx, v);
+}
+
+__global__ void beta_expand_batch_kernel(const fp2* __restrict__ tabs, int h, int hb,
+                                         fp2* __restrict__ out, size_t out_stride)
+{
+    const size_t n = (size_t)1 << (h + hb);
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const fp2* t = tabs + (size_t)blockIdx.y * (((size_t)1 << h) + ((size_t)1 << hb));
+    const fp2* lo = t;
+    const fp2* hi = t + ((size_t)1 << h);
+    st2(out + (size_t)blockIdx.y * out_stride + i,
+        f2mul(ld2(hi + (i >> h)), ld2(lo + (i & (((size_t)1 << h) - 1)))));
 }
 
 // sum_i reduce(x[i]) * hi[i >> h] * lo[i & (2^h - 1)]. For h >= 3 every thread takes
@@ -605,282 +628,26 @@ bool launch_claim_explicit(const DevGateForm& g, int n_copies, const u64* const*
     return launch_claim<MODE_EXPLICIT>(a, ws, s);
 }
 
+bool launch_pack(const u64* re, const u64* im, size_t n, fp2* out, cudaStream_t s, int* launches)
+{
+    if (n == 0) return true;
+    pack_kernel<<<blocks_for(n, kThreads), kThreads, 0, s>>>(re, im, n, out);
+    ++*launches;
+    return !cuda_failed(cudaGetLastError(), "pack launch");
+}
+
 // ---------------------------------------------------------------------------
-// session
+// fold without a claim (table source): every row [0, W_rows) and beta
 
-namespace {
-
-bool session_alloc(EarlySession* S, size_t rows0, size_t rows1, cudaStream_t s)
+bool launch_fold_rows(const fp2* A, int n_in, fp2* Aout, int W_rows, const fp2* beta,
+                      fp2* beta_out, fp2 r, cudaStream_t s, int* launches)
 {
-    const size_t n = (size_t)S->n_copies0;
-    if (rows0) S->buf[0] = (fp2*)dev_alloc(sizeof(fp2) * rows0, s);
-    S->buf[1] = (fp2*)dev_alloc(sizeof(fp2) * rows1, s);
-    S->beta[0] = (fp2*)dev_alloc(sizeof(fp2) * n, s);
-    S->beta[1] = (fp2*)dev_alloc(sizeof(fp2) * n, s);
-    S->fin = (fp2*)dev_alloc(sizeof(fp2) * ((size_t)S->n_wires + 1), s);
-    return (!rows0 || S->buf[0]) && S->buf[1] && S->beta[0] && S->beta[1] && S->fin &&
-           workspace_init(S->ws, 1024, s);
-}
-
-}  // namespace
-
-EarlySession* session_create(int n_gates, const int* type, const int* in0, const int* in1,
-                             const u64* z_re, const u64* z_im, int n_copies, int n_wires,
-                             cudaStream_t s)
-{
-    if (n_gates <= 0 || n_wires <= 0 || n_copies < 2 || (n_copies & (n_copies - 1)) != 0) {
-        set_error(TP_ERR_ARG, "early session needs n_gates > 0, n_wires > 0 and n_copies a "
-                              "power of two >= 2 (got %d, %d, %d)", n_gates, n_wires, n_copies);
-        return nullptr;
-    }
-    if (!ctx()) return nullptr;
-    GateForm g;
-    if (!build_gate_form(n_gates, type, in0, in1, z_re, z_im, n_wires, g)) return nullptr;
-    EarlySession* S = new EarlySession();
-    S->n_gates = n_gates;
-    S->n_wires = S->W_rows = n_wires;
-    S->n_copies = S->n_phys = S->n_copies0 = n_copies;
-    S->stream = s;
-    S->Lc = f2zero();
-    S->L_host = g.L;
-    if (!upload_gate_form(g, S->form, s)) {
-        session_destroy(S);
-        return nullptr;
-    }
-    return S;
-}
-
-bool session_load_host(EarlySession* S, const u64* v_re, const u64* v_im, const u64* b_re,
-                       const u64* b_im)
-{
-    const size_t vn = (size_t)S->n_wires * (size_t)S->n_copies0;
-    cudaStream_t s = S->stream;
-    if (!session_alloc(S, vn, vn / 2, s)) return false;
-    // the half-size ping buffer holds exactly one SoA limb array
-    u64* stage_re = reinterpret_cast<u64*>(S->buf[1]);
-    u64* stage_im = (u64*)dev_alloc(sizeof(u64) * vn, s);
-    if (!stage_im) return false;
-    bool ok = !cuda_failed(cudaMemcpyAsync(stage_re, v_re, 8 * vn, cudaMemcpyHostToDevice, s), "H2D values") &&
-              !cuda_failed(cudaMemcpyAsync(stage_im, v_im, 8 * vn, cudaMemcpyHostToDevice, s), "H2D values");
-    if (ok) {
-        pack_kernel<<<blocks_for(vn, kThreads), kThreads, 0, s>>>(stage_re, stage_im, vn, S->buf[0]);
-        S->launches++;
-        ok = !cuda_failed(cudaGetLastError(), "pack values");
-    }
-    // beta: the second beta table (16 B x n) holds both limb arrays while packing
-    const size_t n = (size_t)S->n_copies0;
-    u64* bst = reinterpret_cast<u64*>(S->beta[1]);
-    if (ok)
-        ok = !cuda_failed(cudaMemcpyAsync(bst, b_re, 8 * n, cudaMemcpyHostToDevice, s), "H2D beta") &&
-             !cuda_failed(cudaMemcpyAsync(bst + n, b_im, 8 * n, cudaMemcpyHostToDevice, s), "H2D beta");
-    if (ok) {
-        pack_kernel<<<blocks_for(n, kThreads), kThreads, 0, s>>>(bst, bst + n, n, S->beta[0]);
-        S->launches++;
-        ok = !cuda_failed(cudaGetLastError(), "pack beta");
-    }
-    dev_free(stage_im, s);
-    // the reference contract: inputs are consumed before the call returns
-    if (ok) ok = !cuda_failed(cudaStreamSynchronize(s), "load tables");
-    return ok;
-}
-
-bool session_load_device(EarlySession* S, const fp2* d_values, const fp2* d_beta, bool borrow)
-{
-    const size_t vn = (size_t)S->n_wires * (size_t)S->n_copies0;
-    cudaStream_t s = S->stream;
-    if (!session_alloc(S, borrow ? 0 : vn, vn / 2, s)) return false;
-    if (borrow) {
-        S->buf[0] = const_cast<fp2*>(d_values);
-        S->borrowed0 = true;
-    } else {
-        TP_CUDA_OK(cudaMemcpyAsync(S->buf[0], d_values, sizeof(fp2) * vn, cudaMemcpyDeviceToDevice, s),
-                   "copy values");
-    }
-    TP_CUDA_OK(cudaMemcpyAsync(S->beta[0], d_beta, sizeof(fp2) * (size_t)S->n_copies0,
-                               cudaMemcpyDeviceToDevice, s), "copy beta");
-    return true;
-}
-
-bool session_load_pixels(EarlySession* S, const PixSrc& px, const fp2* d_beta)
-{
-    if (!pixsrc_valid(px, S->n_copies0, S->n_wires)) return false;
-    cudaStream_t s = S->stream;
-    S->px = px;
-    S->pix_mode = true;
-    S->W_rows = pixsrc_rows(px);
-    const size_t C = (size_t)S->n_copies0, R = (size_t)S->W_rows;
-    // first fold writes rows x C/2 into buf[1]; later folds alternate with buf[0]
-    if (!session_alloc(S, R * std::max<size_t>(1, C / 4), R * (C / 2), s)) return false;
-    if (px.const_idx >= 0) S->Lc = f2scale(S->L_host[(size_t)px.const_idx], px.const_val);
-    TP_CUDA_OK(cudaMemcpyAsync(S->beta[0], d_beta, sizeof(fp2) * C, cudaMemcpyDeviceToDevice, s),
-               "copy beta");
-    return true;
-}
-
-static bool apply_pending_fold(EarlySession* S)
-{
-    const int n_out = S->n_phys >> 1;
-    const int nxt = S->pix_mode ? 1 : (S->cur ^ 1);
-    if (S->pix_mode) {
-        if (!launch_fold_pixels(S->px, S->W_rows, n_out, S->pending_r, S->buf[1], S->beta[0],
-                                S->beta[1], S->stream, &S->launches))
-            return false;
-        S->pix_mode = false;
-    } else {
-        const size_t items = (size_t)(S->W_rows + 1) * (size_t)n_out;
-        fold_rows_kernel<<<blocks_for(items, kThreads), kThreads, 0, S->stream>>>(
-            S->buf[S->cur], S->n_phys, S->buf[nxt], S->W_rows, S->beta[S->cur], S->beta[nxt],
-            S->pending_r);
-        S->launches++;
-        if (cuda_failed(cudaGetLastError(), "fold kernel launch")) return false;
-    }
-    S->cur = nxt;
-    S->n_phys = n_out;
-    S->pending = false;
-    return true;
-}
-
-static bool session_claim_launch(EarlySession* S, u64* d_out8);
-
-bool session_claim_async(EarlySession* S, u64* d_out8)
-{
-    if (S->n_copies < 2) {
-        set_error(TP_ERR_ARG, "claim needs at least 2 copies (have %d)", S->n_copies);
-        return false;
-    }
-    // timer tag: 1000 * (pixel source) + 100 * (fold fused) + log2(copies claimed)
-    int lg = 0;
-    while ((1 << lg) < S->n_copies) ++lg;
-    timer_begin(S->stream, 1000 * (S->pix_mode ? 1 : 0) + 100 * (S->pending ? 1 : 0) + lg);
-    const bool ok = session_claim_launch(S, d_out8);
-    timer_end(S->stream);
-    return ok;
-}
-
-static bool session_claim_launch(EarlySession* S, u64* d_out8)
-{
-    if (S->pix_mode) {
-        const bool fold = S->pending;
-        PixClaimArgs a;
-        memset(&a, 0, sizeof(a));
-        a.px = S->px;
-        a.W_rows = S->W_rows;
-        a.n_pad = S->n_copies0;
-        a.n_out = S->n_copies0 / 2;
-        a.L = S->form.L;
-        a.K0 = S->form.K0;
-        a.Lc = S->Lc;
-        a.ab = S->form.ab;
-        a.cf = S->form.c;
-        a.n_terms = S->form.n_terms;
-        a.beta = S->beta[0];
-        a.beta_out = S->beta[1];
-        a.Aout = S->buf[1];
-        a.r = S->pending_r;
-        const unsigned blocks = fold ? (unsigned)((S->n_copies0 / 2 + 31) / 32)
-                                     : (unsigned)((S->n_copies0 + 63) / 64);
-        if (!workspace_init(S->ws, blocks, S->stream)) return false;
-        a.partials = S->ws.partials;
-        a.ticket = S->ws.ticket;
-        a.out8 = d_out8 ? d_out8 : S->ws.out8;
-        if (!launch_claim_pixels(a, fold, S->stream, &S->launches)) return false;
-        if (fold) {
-            S->pix_mode = false;
-            S->pending = false;
-            S->cur = 1;
-            S->n_phys = S->n_copies0 / 2;
-        }
-        return true;
-    }
-    ClaimArgs a = base_args(S->form, S->W_rows, S->n_copies / 2, S->ws);
-    a.A = S->buf[S->cur];
-    a.n_in = S->n_phys;
-    a.beta = S->beta[S->cur];
-    a.r = S->pending_r;
-    a.out8 = d_out8;  // nullptr: the session's own slot
-    bool ok;
-    if (S->pending) {
-        const int nxt = S->cur ^ 1;
-        a.Aout = S->buf[nxt];
-        a.beta_out = S->beta[nxt];
-        ok = launch_claim<MODE_FOLD_CLAIM>(a, S->ws, S->stream);
-        if (ok) {
-            S->cur = nxt;
-            S->n_phys >>= 1;
-            S->pending = false;
-        }
-    } else {
-        ok = launch_claim<MODE_CLAIM>(a, S->ws, S->stream);
-    }
-    S->launches++;
-    return ok;
-}
-
-bool session_claim(EarlySession* S, u64 out8[8])
-{
-    if (!session_claim_async(S, nullptr)) return false;
-    TP_CUDA_OK(cudaMemcpyAsync(out8, S->ws.out8, 64, cudaMemcpyDeviceToHost, S->stream), "D2H claim");
-    TP_CUDA_OK(cudaStreamSynchronize(S->stream), "claim");
-    return true;
-}
-
-bool session_fold(EarlySession* S, fp2 r)
-{
-    if (S->n_copies < 2) {
-        set_error(TP_ERR_ARG, "fold needs at least 2 copies (have %d)", S->n_copies);
-        return false;
-    }
-    if (r.re >= P61 || r.im >= P61) {
-        set_error(TP_ERR_ARG, "fold challenge is not a canonical field element");
-        return false;
-    }
-    if (S->pending && !apply_pending_fold(S)) return false;
-    S->pending = true;
-    S->pending_r = r;
-    S->n_copies >>= 1;
-    return true;
-}
-
-bool session_finish_async(EarlySession* S, fp2* d_wires, fp2* d_beta)
-{
-    if (S->pending && !apply_pending_fold(S)) return false;
-    if (S->pix_mode)
-        return launch_gather_pixels(S->px, S->n_wires, S->beta[0], d_wires, d_beta, S->stream,
-                                    &S->launches);
-    gather_first_kernel<<<blocks_for((size_t)S->n_wires + 1, kThreads), kThreads, 0, S->stream>>>(
-        S->buf[S->cur], S->n_phys, S->W_rows, S->n_wires, S->beta[S->cur], d_wires, d_beta);
-    S->launches++;
-    return !cuda_failed(cudaGetLastError(), "finish kernel launch");
-}
-
-bool session_finish(EarlySession* S, u64* w_re, u64* w_im, u64* b_re, u64* b_im)
-{
-    if (!session_finish_async(S, S->fin, S->fin + S->n_wires)) return false;
-    std::vector<fp2> h((size_t)S->n_wires + 1);
-    TP_CUDA_OK(cudaMemcpyAsync(h.data(), S->fin, sizeof(fp2) * h.size(), cudaMemcpyDeviceToHost,
-                               S->stream), "D2H finish");
-    TP_CUDA_OK(cudaStreamSynchronize(S->stream), "finish");
-    for (int w = 0; w < S->n_wires; ++w) {
-        w_re[w] = h[w].re;
-        w_im[w] = h[w].im;
-    }
-    *b_re = h[S->n_wires].re;
-    *b_im = h[S->n_wires].im;
-    return true;
-}
-
-void session_destroy(EarlySession* S)
-{
-    if (!S) return;
-    cudaStream_t s = S->stream;
-    if (!S->borrowed0) dev_free(S->buf[0], s);
-    dev_free(S->buf[1], s);
-    dev_free(S->beta[0], s);
-    dev_free(S->beta[1], s);
-    dev_free(S->fin, s);
-    free_gate_form(S->form, s);
-    workspace_free(S->ws, s);
-    delete S;
+    const int n_out = n_in >> 1;
+    const size_t items = (size_t)(W_rows + 1) * (size_t)n_out;
+    fold_rows_kernel<<<blocks_for(items, kThreads), kThreads, 0, s>>>(A, n_in, Aout, W_rows, beta,
+                                                                        beta_out, r);
+    ++*launches;
+    return !cuda_failed(cudaGetLastError(), "fold kernel launch");
 }
 
 // ---------------------------------------------------------------------------
@@ -955,6 +722,30 @@ bool launch_table_from_pixels(const unsigned char* d_pix, int n_real, int n_pad,
                                                             const_idx, const_val, d_table, d_inputs);
     t_launches = 1;
     return !cuda_failed(cudaGetLastError(), "table_from_pixels launch");
+}
+
+void launch_eq_tables_batch(const fp2* d_z, int z_stride, int h, int hb, fp2 init, fp2* tabs,
+                            int n, cudaStream_t s)
+{
+    const size_t nt = ((size_t)1 << h) + ((size_t)1 << hb);
+    eq_tables_batch_kernel<<<dim3(blocks_for(nt, kThreads), n), kThreads, 0, s>>>(d_z, z_stride, h, hb,
+                                                                               init, tabs);
+}
+
+bool launch_beta_batch(const fp2* d_z, int n_z, int n, fp2* d_out, cudaStream_t s, int* launches)
+{
+    if (n <= 0 || n_z <= 0) return true;
+    const int h = n_z / 2, hb = n_z - h;
+    const size_t nt = ((size_t)1 << h) + ((size_t)1 << hb);
+    fp2* tabs = (fp2*)dev_alloc(sizeof(fp2) * nt * n, s);
+    if (!tabs) return false;
+    launch_eq_tables_batch(d_z, n_z, h, hb, mk(1, 0), tabs, n, s);
+    const size_t m = (size_t)1 << n_z;
+    beta_expand_batch_kernel<<<dim3(blocks_for(m, kThreads), n), kThreads, 0, s>>>(tabs, h, hb,
+                                                                                 d_out, m);
+    *launches += 2;
+    dev_free(tabs, s);
+    return !cuda_failed(cudaGetLastError(), "beta batch launch");
 }
 
 bool launch_mle_base(const u64* d_in, const fp2* d_z, int n_z, fp2* d_out, cudaStream_t s)

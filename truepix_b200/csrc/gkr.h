@@ -47,47 +47,68 @@ struct ClaimWorkspace {
 bool workspace_init(ClaimWorkspace& w, size_t blocks, cudaStream_t s);
 void workspace_free(ClaimWorkspace& w, cudaStream_t s);
 
-// Early-round session over a wire-major table V[w][c] of packed Fp2 (16 B).
-struct EarlySession {
-    int n_gates = 0, n_wires = 0;
+// One frame (early-round session) of a batch: its table source, ping-pong
+// buffers, beta, gate form and round state.
+struct Frame {
+    int n_wires = 0, W_rows = 0;
+    int n_copies0 = 0;     // copies of the input table (a power of two >= 2)
     int n_copies = 0;      // logical copies (after a recorded fold)
-    int n_phys = 0;        // copies held by buf[cur]
-    int n_copies0 = 0;
-    bool pending = false;  // fold recorded, applied by the next claim/fold/finish
-    fp2 pending_r;
+    int n_phys = 0;        // copies held by the current source
+    int cur = 0;           // table buffer holding the current source
+    bool pix_cur = false;  // the current source is the frame's bytes
+    PixSrc px;
+    bool pending = false;  // fold recorded, applied by the next claim / fold / finish
+    fp2 r;
+    DevGateForm form;
+    std::vector<fp2> L_host;
+    fp2 Lc;                // L[const_idx] * const_val (byte source)
     fp2* buf[2] = {nullptr, nullptr};
     bool borrowed0 = false;
     fp2* beta[2] = {nullptr, nullptr};
-    int cur = 0;
-    DevGateForm form;
-    ClaimWorkspace ws;
-    fp2* fin = nullptr;    // finish staging [n_wires + 1]
-    std::vector<fp2> L_host;  // the linear coefficients, kept for the constant wire
-    cudaStream_t stream = nullptr;
-    int launches = 0;      // kernels launched by this session
-    int W_rows = 0;        // rows stored; rows >= W_rows are identically zero
-    bool pix_mode = false; // the current table is the implicit table of a uint8 frame
-    PixSrc px;
-    fp2 Lc;                // L[const_idx] * const_val (pixel mode)
+    fp2* fin = nullptr;    // [n_wires + 1]: wires, then beta
+    u64* out8 = nullptr;   // default claim slot
+    bool configured = false;
+    size_t cap0 = 0, cap1 = 0, capb = 0, capfin = 0;  // element capacities kept across resets
 };
 
-EarlySession* session_create(int n_gates, const int* type, const int* in0, const int* in1,
-                             const u64* z_re, const u64* z_im, int n_copies, int n_wires,
-                             cudaStream_t s);
-// fill from host SoA tables (reference ABI)
-bool session_load_host(EarlySession* S, const u64* v_re, const u64* v_im, const u64* b_re,
-                       const u64* b_im);
-// the table of a uint8 frame, read from device bytes (d_beta: packed, copied)
-bool session_load_pixels(EarlySession* S, const PixSrc& px, const fp2* d_beta);
-// fill from device packed tables; borrow=true adopts d_values as the first buffer
-bool session_load_device(EarlySession* S, const fp2* d_values, const fp2* d_beta, bool borrow);
-// claim; d_out8 receives the 4 Fp2 (0, 1, -1, 2) on device
-bool session_claim_async(EarlySession* S, u64* d_out8);
-bool session_claim(EarlySession* S, u64 out8[8]);
-bool session_fold(EarlySession* S, fp2 r);
-bool session_finish_async(EarlySession* S, fp2* d_wires, fp2* d_beta);
-bool session_finish(EarlySession* S, u64* w_re, u64* w_im, u64* b_re, u64* b_im);
-void session_destroy(EarlySession* S);
+// A batch of frames advanced together: one launch per round for all frames
+// whose early rounds are not finished.
+struct Batch {
+    std::vector<Frame*> frames;
+    cudaStream_t stream = nullptr;
+    Job* d_jobs = nullptr;
+    size_t cap_jobs = 0;
+    fp2* partials = nullptr;
+    size_t cap_partials = 0;  // in CTAs (4 fp2 each)
+    unsigned* tickets = nullptr;
+    size_t cap_tickets = 0;
+    int launches = 0;
+};
+
+Batch* batch_create(int n_frames, cudaStream_t s);
+// configure frame i (gate form from z1; tables from host SoA, device packed, or bytes)
+bool batch_set_gates(Batch* B, int i, int n_gates, const int* type, const int* in0,
+                     const int* in1, const u64* z_re, const u64* z_im, int n_copies, int n_wires);
+bool batch_load_host(Batch* B, int i, const u64* v_re, const u64* v_im, const u64* b_re,
+                     const u64* b_im);
+bool batch_load_device(Batch* B, int i, const fp2* d_values, const fp2* d_beta, bool borrow);
+bool batch_load_pixels(Batch* B, int i, const PixSrc& px, const fp2* d_beta);
+// claims of all unfinished frames; d_claims[i] (8 u64, device) or the frame's slot
+bool batch_claim(Batch* B, u64* const* d_claims);
+bool batch_fold(Batch* B, int i, fp2 r);
+// wires / beta of every frame into d_wires[i] (n_wires packed) / d_beta[i] (1 packed);
+// nullptr destinations use the frame's own staging buffer
+bool batch_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta);
+void batch_destroy(Batch* B);
+// forget every frame's configuration but keep its device buffers for reuse
+void batch_reset(Batch* B);
+
+// single-frame views used by the reference ABI
+Batch* session_create(int n_gates, const int* type, const int* in0, const int* in1,
+                      const u64* z_re, const u64* z_im, int n_copies, int n_wires,
+                      cudaStream_t s);
+bool session_claim(Batch* B, u64 out8[8]);
+bool session_finish(Batch* B, u64* w_re, u64* w_im, u64* b_re, u64* b_im);
 
 // ---- batch operations on device buffers (all asynchronous on stream s) ----
 bool launch_fold_soa(const u64* in_re, const u64* in_im, size_t n_out, fp2 r, u64* out_re,

@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "fp2.cuh"
 
 namespace tp {
@@ -110,37 +112,62 @@ struct PixSrc {
     u64 const_val;
 };
 
-struct PixClaimArgs {
-    PixSrc px;
-    int pw;          // padded 32-bit words per staged copy
-    int W_rows;      // rows kept in the folded table (private wires + constant)
-    int n_pad;       // copies of the implicit table
-    int n_out;       // folded copies (fold kernel)
-    const fp2* L;    // canonical linear coefficients [n_wires]
-    fp2 K0;
-    fp2 Lc;          // L[const_idx] * const_val
-    const int2* ab;  // product terms, grouped by b
-    const fp2* cf;
-    int n_terms, tc;
+
+// One frame's work in a batched round launch (device memory). Table source
+// when A != nullptr, frame bytes when pix != nullptr.
+struct Job {
+    const fp2* A;           // table [W_rows][n_in]
+    fp2* Aout;              // folded table [W_rows][n_in / 2]
+    const unsigned char* pix;
     const fp2* beta;
     fp2* beta_out;
-    fp2* Aout;       // folded rows, stride n_out
-    fp2 r;
-    fp2* partials;
+    const fp2* L;           // canonical linear coefficients [W]
+    const int2* ab;         // product terms grouped by b
+    const fp2* cf;
+    fp2* partials;          // [tiles * groups][4]
     unsigned* ticket;
     u64* out8;
+    fp2* fin;               // finish: wires [W]
+    fp2* fin_beta;          // finish: beta [1]
+    fp2 K0, Lc, r;
+    u64 const_val;
+    int kind;               // 0 table claim, 1 table fold+claim, 2 bytes claim, 3 bytes fold+claim
+    int n_in;               // copies of the source
+    int n_pairs;            // claim pairs
+    int W, W_rows;
+    int n_real, cs, const_idx;
+    int n_terms, tiles, groups, wpg, tpg, pw, cta0, pad_;
 };
+
+void plan_job(Job& j, int target_ctas);
+bool launch_round(const Job* d_jobs, const std::vector<Job>& jobs, int kind, cudaStream_t s,
+                  int* launches);
+bool launch_finish(const Job* d_jobs, int n_jobs, int max_w, cudaStream_t s, int* launches);
 
 // host-side launchers implemented in gkr_pixels.cu / gkr.cu
 bool pixsrc_valid(const PixSrc& px, int n_pad, int W);
 int pixsrc_rows(const PixSrc& px);
-bool launch_claim_pixels(PixClaimArgs a, bool fold, cudaStream_t s, int* launches);
 bool launch_fold_pixels(const PixSrc& px, int W_rows, int n_out, fp2 r, fp2* Aout,
                         const fp2* beta, fp2* beta_out, cudaStream_t s, int* launches);
-bool launch_gather_pixels(const PixSrc& px, int W, const fp2* beta, fp2* fin, fp2* fin_beta,
-                          cudaStream_t s, int* launches);
+bool launch_pack(const u64* re, const u64* im, size_t n, fp2* out, cudaStream_t s, int* launches);
+bool launch_fold_rows(const fp2* A, int n_in, fp2* Aout, int W_rows, const fp2* beta,
+                      fp2* beta_out, fp2 r, cudaStream_t s, int* launches);
 bool launch_mle_pixels(const PixSrc& px, int n_pad, int W, const fp2* d_z, fp2* d_out,
                        cudaStream_t s, int* launches);
 void launch_eq_tables(const fp2* d_z, int h, int hb, fp2 init, fp2* lo, fp2* hi, cudaStream_t s);
+void launch_eq_tables_batch(const fp2* d_z, int z_stride, int h, int hb, fp2 init, fp2* tabs,
+                            int n, cudaStream_t s);
+// beta tables of n frames: d_z packed [n][n_z], d_out packed [n][2^n_z]
+bool launch_beta_batch(const fp2* d_z, int n_z, int n, fp2* d_out, cudaStream_t s, int* launches);
+// MLE of n frames' input vectors (same padded size) from their bytes:
+// frames[i] = {pix, n_real}; points packed [n][log2 W + log2 n_pad]; out packed [n]
+struct MleFrame {
+    const unsigned char* pix;
+    int n_real;
+    int pad_;
+};
+bool launch_mle_pixels_batch(const MleFrame* h_frames, int n, int n_pad, int cs, int W,
+                             int const_idx, u64 const_val, const fp2* d_points, fp2* d_out,
+                             cudaStream_t s, int* launches);
 
 }  // namespace tp

@@ -55,9 +55,12 @@ bool d2h(void* h, const void* d, size_t bytes, cudaStream_t s)
 }
 bool sync(cudaStream_t s) { return !tp::cuda_failed(cudaStreamSynchronize(s), "synchronize"); }
 
-cudaStream_t pick(void* stream, tp::Ctx* c)
+// NULL is the CUDA default stream, as everywhere in CUDA; callers that mix these
+// entry points with other work on that stream (torch's default stream, for one)
+// stay ordered with it
+cudaStream_t pick(void* stream, tp::Ctx*)
 {
-    return stream ? reinterpret_cast<cudaStream_t>(stream) : c->stream;
+    return reinterpret_cast<cudaStream_t>(stream);
 }
 
 // uint64_t (unsigned long) and tp::u64 (unsigned long long) have the same layout
@@ -251,11 +254,11 @@ void* native_fp2_early_create(int n_gates, const int* gate_type, const int* in0,
     tp::clear_error();
     tp::Ctx* c = tp::ctx();
     if (!c) return nullptr;
-    tp::EarlySession* S = tp::session_create(n_gates, gate_type, in0, in1, U(z1_real), U(z1_imag),
-                                             n_copies, n_wires, c->stream);
+    tp::Batch* S = tp::session_create(n_gates, gate_type, in0, in1, U(z1_real), U(z1_imag),
+                                      n_copies, n_wires, c->stream);
     if (!S) return nullptr;
-    if (!tp::session_load_host(S, U(values_real), U(values_imag), U(beta_real), U(beta_imag))) {
-        tp::session_destroy(S);
+    if (!tp::batch_load_host(S, 0, U(values_real), U(values_imag), U(beta_real), U(beta_imag))) {
+        tp::batch_destroy(S);
         return nullptr;
     }
     return S;
@@ -265,14 +268,14 @@ int native_fp2_early_claim(void* handle, uint64_t out8[8])
 {
     tp::clear_error();
     if (!handle) return -1;
-    return tp::session_claim(static_cast<tp::EarlySession*>(handle), U(out8)) ? 0 : -1;
+    return tp::session_claim(static_cast<tp::Batch*>(handle), U(out8)) ? 0 : -1;
 }
 
 int native_fp2_early_fold(void* handle, uint64_t r_real, uint64_t r_imag)
 {
     tp::clear_error();
     if (!handle) return -1;
-    return tp::session_fold(static_cast<tp::EarlySession*>(handle), mk(r_real, r_imag)) ? 0 : -1;
+    return tp::batch_fold(static_cast<tp::Batch*>(handle), 0, mk(r_real, r_imag)) ? 0 : -1;
 }
 
 int native_fp2_early_finish(void* handle, uint64_t* wire_real, uint64_t* wire_imag,
@@ -280,24 +283,21 @@ int native_fp2_early_finish(void* handle, uint64_t* wire_real, uint64_t* wire_im
 {
     tp::clear_error();
     if (!handle) return -1;
-    return tp::session_finish(static_cast<tp::EarlySession*>(handle), U(wire_real), U(wire_imag),
+    return tp::session_finish(static_cast<tp::Batch*>(handle), U(wire_real), U(wire_imag),
                               U(beta_real), U(beta_imag)) ? 0 : -1;
 }
 
 int native_fp2_early_n_copies(void* handle)
 {
-    return handle ? static_cast<tp::EarlySession*>(handle)->n_copies : 0;
+    return handle ? static_cast<tp::Batch*>(handle)->frames[0]->n_copies : 0;
 }
 
 int native_fp2_early_n_wires(void* handle)
 {
-    return handle ? static_cast<tp::EarlySession*>(handle)->n_wires : 0;
+    return handle ? static_cast<tp::Batch*>(handle)->frames[0]->n_wires : 0;
 }
 
-void native_fp2_early_destroy(void* handle)
-{
-    tp::session_destroy(static_cast<tp::EarlySession*>(handle));
-}
+void native_fp2_early_destroy(void* handle) { tp::batch_destroy(static_cast<tp::Batch*>(handle)); }
 
 // ---- host-only inspection ----------------------------------------------------
 
@@ -336,12 +336,12 @@ void* tp_early_create_dev(int n_gates, const int* gate_type, const int* in0, con
     tp::clear_error();
     tp::Ctx* c = tp::ctx();
     if (!c) return nullptr;
-    tp::EarlySession* S = tp::session_create(n_gates, gate_type, in0, in1, U(z1_real), U(z1_imag),
-                                             n_copies, n_wires, pick(stream, c));
+    tp::Batch* S = tp::session_create(n_gates, gate_type, in0, in1, U(z1_real), U(z1_imag),
+                                      n_copies, n_wires, pick(stream, c));
     if (!S) return nullptr;
-    if (!tp::session_load_device(S, static_cast<const fp2*>(d_values),
-                                 static_cast<const fp2*>(d_beta), borrow != 0)) {
-        tp::session_destroy(S);
+    if (!tp::batch_load_device(S, 0, static_cast<const fp2*>(d_values),
+                               static_cast<const fp2*>(d_beta), borrow != 0)) {
+        tp::batch_destroy(S);
         return nullptr;
     }
     return S;
@@ -351,21 +351,22 @@ int tp_early_claim_dev(void* handle, void* d_out8)
 {
     tp::clear_error();
     if (!handle) return -1;
-    return tp::session_claim_async(static_cast<tp::EarlySession*>(handle),
-                                   static_cast<u64*>(d_out8)) ? 0 : -1;
+    u64* p = static_cast<u64*>(d_out8);
+    return tp::batch_claim(static_cast<tp::Batch*>(handle), &p) ? 0 : -1;
 }
 
 int tp_early_finish_dev(void* handle, void* d_wires, void* d_beta)
 {
     tp::clear_error();
     if (!handle) return -1;
-    return tp::session_finish_async(static_cast<tp::EarlySession*>(handle),
-                                    static_cast<fp2*>(d_wires), static_cast<fp2*>(d_beta)) ? 0 : -1;
+    fp2* w = static_cast<fp2*>(d_wires);
+    fp2* b = static_cast<fp2*>(d_beta);
+    return tp::batch_finish(static_cast<tp::Batch*>(handle), &w, &b) ? 0 : -1;
 }
 
 int tp_early_launches(void* handle)
 {
-    return handle ? static_cast<tp::EarlySession*>(handle)->launches : 0;
+    return handle ? static_cast<tp::Batch*>(handle)->launches : 0;
 }
 
 int tp_fold_dev(const void* d_in, size_t n_out, uint64_t r_real, uint64_t r_imag, void* d_out,
@@ -424,8 +425,8 @@ void* tp_early_create_pixels(int n_gates, const int* gate_type, const int* in0, 
     tp::clear_error();
     tp::Ctx* c = tp::ctx();
     if (!c) return nullptr;
-    tp::EarlySession* S = tp::session_create(n_gates, gate_type, in0, in1, U(z1_real), U(z1_imag),
-                                             n_copies_padded, n_wires, pick(stream, c));
+    tp::Batch* S = tp::session_create(n_gates, gate_type, in0, in1, U(z1_real), U(z1_imag),
+                                      n_copies_padded, n_wires, pick(stream, c));
     if (!S) return nullptr;
     tp::PixSrc px;
     px.pix = static_cast<const unsigned char*>(d_pixels);
@@ -433,8 +434,8 @@ void* tp_early_create_pixels(int n_gates, const int* gate_type, const int* in0, 
     px.cs = copy_size;
     px.const_idx = const_idx;
     px.const_val = const_val;
-    if (!tp::session_load_pixels(S, px, static_cast<const fp2*>(d_beta))) {
-        tp::session_destroy(S);
+    if (!tp::batch_load_pixels(S, 0, px, static_cast<const fp2*>(d_beta))) {
+        tp::batch_destroy(S);
         return nullptr;
     }
     return S;
@@ -462,18 +463,151 @@ int tp_early_rounds_dev(void* handle, int n_rounds, const uint64_t* challenges, 
 {
     tp::clear_error();
     if (!handle || n_rounds < 0) return -1;
-    tp::EarlySession* S = static_cast<tp::EarlySession*>(handle);
+    tp::Batch* S = static_cast<tp::Batch*>(handle);
     u64* out = static_cast<u64*>(d_claims);
     for (int k = 0; k < n_rounds; ++k) {
-        if (!tp::session_claim_async(S, out ? out + 8 * (size_t)k : nullptr)) return -1;
-        if (!tp::session_fold(S, mk(challenges[2 * k], challenges[2 * k + 1]))) return -1;
+        u64* p = out ? out + 8 * (size_t)k : nullptr;
+        if (!tp::batch_claim(S, &p)) return -1;
+        if (!tp::batch_fold(S, 0, mk(challenges[2 * k], challenges[2 * k + 1]))) return -1;
     }
     return 0;
 }
+
+// ---- batches of frames -------------------------------------------------------
+
+void* tp_batch_create(int n_frames, void* stream)
+{
+    tp::clear_error();
+    tp::Ctx* c = tp::ctx();
+    if (!c) return nullptr;
+    return tp::batch_create(n_frames, pick(stream, c));
+}
+
+int tp_batch_set_pixels(void* batch, int i, int n_gates, const int* gate_type, const int* in0,
+                        const int* in1, const uint64_t* z1_real, const uint64_t* z1_imag,
+                        const void* d_pixels, int n_copies, int n_copies_padded, int copy_size,
+                        int n_wires, int const_idx, uint64_t const_val, const void* d_beta)
+{
+    tp::clear_error();
+    if (!batch) return -1;
+    tp::Batch* B = static_cast<tp::Batch*>(batch);
+    if (!tp::batch_set_gates(B, i, n_gates, gate_type, in0, in1, U(z1_real), U(z1_imag),
+                             n_copies_padded, n_wires))
+        return -1;
+    tp::PixSrc px;
+    px.pix = static_cast<const unsigned char*>(d_pixels);
+    px.n_real = n_copies;
+    px.cs = copy_size;
+    px.const_idx = const_idx;
+    px.const_val = const_val;
+    return tp::batch_load_pixels(B, i, px, static_cast<const fp2*>(d_beta)) ? 0 : -1;
+}
+
+int tp_batch_set_table(void* batch, int i, int n_gates, const int* gate_type, const int* in0,
+                       const int* in1, const uint64_t* z1_real, const uint64_t* z1_imag,
+                       int n_copies, int n_wires, const void* d_values, const void* d_beta,
+                       int borrow)
+{
+    tp::clear_error();
+    if (!batch) return -1;
+    tp::Batch* B = static_cast<tp::Batch*>(batch);
+    if (!tp::batch_set_gates(B, i, n_gates, gate_type, in0, in1, U(z1_real), U(z1_imag), n_copies,
+                             n_wires))
+        return -1;
+    return tp::batch_load_device(B, i, static_cast<const fp2*>(d_values),
+                                 static_cast<const fp2*>(d_beta), borrow != 0) ? 0 : -1;
+}
+
+int tp_batch_claim(void* batch, void* d_claims)
+{
+    tp::clear_error();
+    if (!batch) return -1;
+    tp::Batch* B = static_cast<tp::Batch*>(batch);
+    std::vector<u64*> ptrs(B->frames.size(), nullptr);
+    if (d_claims)
+        for (size_t i = 0; i < ptrs.size(); ++i) ptrs[i] = static_cast<u64*>(d_claims) + 8 * i;
+    return tp::batch_claim(B, ptrs.data()) ? 0 : -1;
+}
+
+int tp_batch_fold(void* batch, const uint64_t* challenges)
+{
+    tp::clear_error();
+    if (!batch) return -1;
+    tp::Batch* B = static_cast<tp::Batch*>(batch);
+    for (size_t i = 0; i < B->frames.size(); ++i) {
+        if (B->frames[i]->n_copies < 2) continue;
+        if (!tp::batch_fold(B, (int)i, mk(challenges[2 * i], challenges[2 * i + 1]))) return -1;
+    }
+    return 0;
+}
+
+int tp_batch_n_copies(void* batch, int i)
+{
+    if (!batch) return 0;
+    tp::Batch* B = static_cast<tp::Batch*>(batch);
+    if (i < 0 || i >= (int)B->frames.size()) return 0;
+    return B->frames[(size_t)i]->n_copies;
+}
+
+int tp_batch_finish(void* batch, void* d_wires, void* d_beta)
+{
+    tp::clear_error();
+    if (!batch) return -1;
+    tp::Batch* B = static_cast<tp::Batch*>(batch);
+    const size_t n = B->frames.size();
+    std::vector<fp2*> w(n, nullptr), b(n, nullptr);
+    for (size_t i = 0; i < n; ++i) {
+        if (d_wires) w[i] = static_cast<fp2*>(d_wires) + i * (size_t)B->frames[i]->n_wires;
+        if (d_beta) b[i] = static_cast<fp2*>(d_beta) + i;
+    }
+    return tp::batch_finish(B, w.data(), b.data()) ? 0 : -1;
+}
+
+int tp_batch_launches(void* batch) { return batch ? static_cast<tp::Batch*>(batch)->launches : 0; }
+
+void tp_batch_destroy(void* batch) { tp::batch_destroy(static_cast<tp::Batch*>(batch)); }
 
 int tp_timer_enable(int max_pairs) { return tp::timer_enable(max_pairs) ? 0 : -1; }
 void tp_timer_disable(void) { tp::timer_disable(); }
 void tp_timer_reset(void) { tp::timer_reset(); }
 int tp_timer_read(float* ms, int* tags, int max_pairs) { return tp::timer_read(ms, tags, max_pairs); }
+
+void tp_batch_reset(void* batch)
+{
+    if (batch) tp::batch_reset(static_cast<tp::Batch*>(batch));
+}
+
+int tp_compute_beta_batch_dev(const void* d_z, int n_z, int n_frames, void* d_out, void* stream)
+{
+    tp::clear_error();
+    tp::Ctx* c = tp::ctx();
+    if (!c) return -1;
+    if (n_z <= 0 || n_z > 30 || n_frames <= 0) {
+        tp::set_error(tp::TP_ERR_ARG, "beta batch: n_z %d, frames %d", n_z, n_frames);
+        return -1;
+    }
+    int launches = 0;
+    return tp::launch_beta_batch(static_cast<const fp2*>(d_z), n_z, n_frames,
+                                 static_cast<fp2*>(d_out), pick(stream, c), &launches) ? 0 : -1;
+}
+
+int tp_mle_eval_pixels_batch(int n_frames, const void* const* d_pixels, const int* n_copies,
+                             int n_copies_padded, int copy_size, int n_wires, int const_idx,
+                             uint64_t const_val, const void* d_points, void* d_out, void* stream)
+{
+    tp::clear_error();
+    tp::Ctx* c = tp::ctx();
+    if (!c) return -1;
+    std::vector<tp::MleFrame> fr((size_t)std::max(0, n_frames));
+    for (int i = 0; i < n_frames; ++i) {
+        fr[(size_t)i].pix = static_cast<const unsigned char*>(d_pixels[i]);
+        fr[(size_t)i].n_real = n_copies[i];
+        fr[(size_t)i].pad_ = 0;
+    }
+    int launches = 0;
+    return tp::launch_mle_pixels_batch(fr.data(), n_frames, n_copies_padded, copy_size, n_wires,
+                                       const_idx, const_val, static_cast<const fp2*>(d_points),
+                                       static_cast<fp2*>(d_out), pick(stream, c), &launches) ? 0 : -1;
+}
 
 }  // extern "C"

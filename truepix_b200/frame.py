@@ -165,3 +165,126 @@ class GkrInputLayerProver:
         w = self.wires.cpu().numpy().view(np.uint64).reshape(W + 1, 2)
         m = self.mle.cpu().numpy().view(np.uint64)
         return c, w[:W], (int(w[W, 0]), int(w[W, 1])), (int(m[0]), int(m[1]))
+
+
+class BatchFrameProver:
+    """Many frames (sizes may differ) proven together: one kernel launch per
+    sumcheck round serves every frame that still has early rounds left
+    (tp_batch_*); beta tables and input MLEs are computed in one launch per
+    group of frames with the same padded size. The batch object and its device
+    buffers persist across prove() calls."""
+
+    def __init__(self, layouts, gate_type, in0, in1, device: int = 0, stream=None):
+        import torch
+        self.torch = torch
+        self.lib = native.gkr()
+        self.layouts = list(layouts)
+        self.B = len(self.layouts)
+        self.dev = torch.device("cuda", device)
+        self.stream = stream
+        self.gt = np.ascontiguousarray(gate_type, np.int32)
+        self.i0 = np.ascontiguousarray(in0, np.int32)
+        self.i1 = np.ascontiguousarray(in1, np.int32)
+        W = self.layouts[0].n_wires
+        L0 = self.layouts[0]
+        assert all((L.n_wires, L.copy_size, L.const_idx, L.const_val) ==
+                   (W, L0.copy_size, L0.const_idx, L0.const_val) for L in self.layouts), \
+            "one circuit layout per batch (copy counts may differ)"
+        self.W = W
+        self.max_rounds = max(L.n_copy_bits for L in self.layouts)
+        i64 = torch.int64
+        # frames grouped by padded size: one beta / MLE launch per group
+        self.groups = {}
+        for f, L in enumerate(self.layouts):
+            self.groups.setdefault(L.padded_copies, []).append(f)
+        self.betas = {C: torch.empty(len(fs) * 2 * C, dtype=i64, device=self.dev)
+                      for C, fs in self.groups.items()}
+        self.claims = torch.zeros(self.max_rounds * self.B * 8, dtype=i64, device=self.dev)
+        self.wires = torch.zeros(self.B * W * 2, dtype=i64, device=self.dev)
+        self.fin_beta = torch.zeros(self.B * 2, dtype=i64, device=self.dev)
+        self.mle = torch.zeros(self.B * 2, dtype=i64, device=self.dev)
+        self.launches_last = 0
+        self.handle = self.lib.tp_batch_create(self.B, self._s())
+        if not self.handle:
+            native.check(self.lib, -1, "batch_create")
+
+    def __del__(self):
+        try:
+            if self.handle:
+                self.lib.tp_batch_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+    def _s(self):
+        return self.stream.cuda_stream if self.stream is not None else \
+            self.torch.cuda.current_stream(self.dev).cuda_stream
+
+    def prove(self, pixels, z1s, z2s_dev, points_dev, challenges: np.ndarray,
+              round_hook=None) -> None:
+        """pixels: one uint8 device tensor per frame; z1s: uint64 [2, n_gates] per
+        frame; z2s_dev / points_dev: per padded size C, a packed Fp2 device tensor
+        [frames of size C][log2 C] / [..][log2 W + log2 C], frames in batch order
+        (dicts keyed by C; a single tensor is accepted when all frames share C);
+        challenges: uint64 [max_rounds, B, 2]. round_hook(k) runs after round k's
+        claims are queued (where a prover reads them back for its transcript)."""
+        lib, s, b = self.lib, self._s(), self.handle
+        if not isinstance(z2s_dev, dict):
+            assert len(self.groups) == 1
+            C = next(iter(self.groups))
+            z2s_dev, points_dev = {C: z2s_dev}, {C: points_dev}
+        launches = 0
+        beta_of = {}
+        for C, fs in self.groups.items():
+            nb = int(math.log2(C))
+            native.check(lib, lib.tp_compute_beta_batch_dev(z2s_dev[C].data_ptr(), nb, len(fs),
+                                                            self.betas[C].data_ptr(), s), "beta")
+            launches += 2
+            for q, f in enumerate(fs):
+                beta_of[f] = self.betas[C].data_ptr() + 16 * C * q
+        lib.tp_batch_reset(b)
+        keep = []
+        for f, L in enumerate(self.layouts):
+            z1r = np.ascontiguousarray(z1s[f][0], np.uint64)
+            z1i = np.ascontiguousarray(z1s[f][1], np.uint64)
+            keep += [z1r, z1i]
+            native.check(lib, lib.tp_batch_set_pixels(
+                b, f, self.gt.size, self.gt.ctypes.data, self.i0.ctypes.data, self.i1.ctypes.data,
+                z1r.ctypes.data, z1i.ctypes.data, pixels[f].data_ptr(), L.copies, L.padded_copies,
+                L.copy_size, L.n_wires, L.const_idx, L.const_val, beta_of[f]), "batch_set_pixels")
+        ch = np.ascontiguousarray(challenges, np.uint64)
+        base = self.claims.data_ptr()
+        l0 = lib.tp_batch_launches(b)
+        for k in range(self.max_rounds):
+            native.check(lib, lib.tp_batch_claim(b, base + 64 * self.B * k), "batch_claim")
+            if round_hook is not None:
+                round_hook(k)
+            native.check(lib, lib.tp_batch_fold(
+                b, ch[k].reshape(-1).ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))), "batch_fold")
+        native.check(lib, lib.tp_batch_finish(b, self.wires.data_ptr(), self.fin_beta.data_ptr()),
+                     "batch_finish")
+        launches += lib.tp_batch_launches(b) - l0
+        L0 = self.layouts[0]
+        for C, fs in self.groups.items():
+            ptrs = (ctypes.c_void_p * len(fs))(*[pixels[f].data_ptr() for f in fs])
+            ncop = (ctypes.c_int * len(fs))(*[self.layouts[f].copies for f in fs])
+            out = self.torch.empty(2 * len(fs), dtype=self.torch.int64, device=self.dev)
+            native.check(lib, lib.tp_mle_eval_pixels_batch(
+                len(fs), ptrs, ncop, C, L0.copy_size, L0.n_wires, L0.const_idx, L0.const_val,
+                points_dev[C].data_ptr(), out.data_ptr(), s), "mle")
+            launches += 2
+            if len(self.groups) == 1:
+                self.mle.copy_(out)
+            else:
+                for q, f in enumerate(fs):
+                    self.mle[2 * f:2 * f + 2].copy_(out[2 * q:2 * q + 2])
+        self.launches_last = launches
+
+    def results(self, f: int):
+        """Frame f: (claims [n_copy_bits, 8], wires [W, 2], beta, mle)."""
+        nb = self.layouts[f].n_copy_bits
+        c = self.claims.cpu().numpy().view(np.uint64).reshape(self.max_rounds, self.B, 8)[:nb, f]
+        w = self.wires.cpu().numpy().view(np.uint64).reshape(self.B, self.W, 2)[f]
+        b = self.fin_beta.cpu().numpy().view(np.uint64).reshape(self.B, 2)[f]
+        m = self.mle.cpu().numpy().view(np.uint64).reshape(self.B, 2)[f]
+        return c, w, (int(b[0]), int(b[1])), (int(m[0]), int(m[1]))

@@ -54,6 +54,21 @@ GKR_SIGNATURES = {
                                      _I32, _U64, _VP, _VP]),
     "tp_mle_eval_pixels": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
     "tp_early_rounds_dev": (_I32, [_VP, _I32, _PU64, _VP]),
+    "tp_batch_create": (_VP, [_I32, _VP]),
+    "tp_batch_set_pixels": (_I32, [_VP, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP, _I32, _I32, _I32,
+                                   _I32, _I32, _U64, _VP]),
+    "tp_batch_set_table": (_I32, [_VP, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _I32, _I32, _VP, _VP,
+                                  _I32]),
+    "tp_batch_claim": (_I32, [_VP, _VP]),
+    "tp_batch_fold": (_I32, [_VP, _PU64]),
+    "tp_batch_n_copies": (_I32, [_VP, _I32]),
+    "tp_batch_finish": (_I32, [_VP, _VP, _VP]),
+    "tp_batch_launches": (_I32, [_VP]),
+    "tp_batch_destroy": (None, [_VP]),
+    "tp_batch_reset": (None, [_VP]),
+    "tp_compute_beta_batch_dev": (_I32, [_VP, _I32, _I32, _VP, _VP]),
+    "tp_mle_eval_pixels_batch": (_I32, [_I32, ctypes.POINTER(_VP), _PI32, _I32, _I32, _I32, _I32,
+                                        _U64, _VP, _VP, _VP]),
     "tp_timer_enable": (_I32, [_I32]),
     "tp_timer_disable": (None, []),
     "tp_timer_reset": (None, []),
