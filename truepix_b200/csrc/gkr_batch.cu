@@ -70,28 +70,54 @@ __device__ __forceinline__ u32 pbyte(const u32* tile, int pw, int row, int w)
 // Stage `rows` copies from copy c0 as words; copies >= n_real read as zero.
 // With split_pairs, copy c0 + 2i goes to row i and c0 + 2i + 1 to row rows/2 + i,
 // so the two copies a lane folds sit in different banks (pw is odd).
+// Byte rows that are a multiple of 16 bytes are loaded as 16-byte vectors, all
+// of a thread's loads issued before the first shared-memory store.
+__device__ __forceinline__ int row_of(int r, int rows, bool split_pairs)
+{
+    return split_pairs ? ((r & 1) ? (rows >> 1) + (r >> 1) : (r >> 1)) : r;
+}
+
 __device__ void stage_rows(const Job& J, int c0, int rows, int pw, u32* tile, bool split_pairs = false)
 {
-    auto row_of = [&](int r) { return split_pairs ? ((r & 1) ? (rows >> 1) + (r >> 1) : (r >> 1)) : r; };
     const int cs = J.cs;
+    if ((cs & 15) == 0 && ((reinterpret_cast<size_t>(J.pix) & 15) == 0) && rows * cs <= 8 * 16 * kBT) {
+        const int per = cs >> 4;                       // 16-byte vectors per row
+        const int nv = rows * per;
+        const uint4* src = reinterpret_cast<const uint4*>(J.pix + (size_t)c0 * cs);
+        uint4 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int q = threadIdx.x + k * kBT;
+            v[k] = make_uint4(0, 0, 0, 0);
+            if (q < nv && c0 + q / per < J.n_real) v[k] = __ldg(src + q);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int q = threadIdx.x + k * kBT;
+            if (q < nv) {
+                const int r = q / per, j = 4 * (q - r * per);
+                u32* d = tile + row_of(r, rows, split_pairs) * pw + j;
+                d[0] = v[k].x;
+                d[1] = v[k].y;
+                d[2] = v[k].z;
+                d[3] = v[k].w;
+            }
+        }
+        const int wpr = cs >> 2;
+        for (int i = threadIdx.x; i < rows * (pw - wpr); i += kBT) {
+            const int r = i / (pw - wpr);
+            tile[r * pw + wpr + (i - r * (pw - wpr))] = 0u;
+        }
+        return;
+    }
     const long long nbytes = (long long)J.n_real * cs;
     const long long g0 = (long long)c0 * cs;
-    if ((cs & 3) == 0 && ((reinterpret_cast<size_t>(J.pix) & 3) == 0)) {
-        const int wpr = cs >> 2;
-        const u32* src = reinterpret_cast<const u32*>(J.pix) + (g0 >> 2);
-        const long long wreal = nbytes >> 2;
-        for (int i = threadIdx.x; i < rows * pw; i += blockDim.x) {
-            const int r = i / pw, j = i - r * pw;
-            const long long gi = (g0 >> 2) + (long long)r * wpr + j;
-            tile[row_of(r) * pw + j] = (j < wpr && gi < wreal) ? __ldg(src + (long long)r * wpr + j) : 0u;
-        }
-    } else {
-        unsigned char* tb = reinterpret_cast<unsigned char*>(tile);
-        for (int i = threadIdx.x; i < rows * pw * 4; i += blockDim.x) {
-            const int r = i / (pw * 4), j = i - r * pw * 4;
-            const long long g = g0 + (long long)r * cs + j;
-            tb[(size_t)row_of(r) * pw * 4 + j] = (j < cs && g < nbytes) ? J.pix[g] : (unsigned char)0;
-        }
+    unsigned char* tb = reinterpret_cast<unsigned char*>(tile);
+    for (int i = threadIdx.x; i < rows * pw * 4; i += blockDim.x) {
+        const int r = i / (pw * 4), j = i - r * pw * 4;
+        const long long g = g0 + (long long)r * cs + j;
+        tb[(size_t)row_of(r, rows, split_pairs) * pw * 4 + j] =
+            (j < cs && g < nbytes) ? J.pix[g] : (unsigned char)0;
     }
 }
 
@@ -211,7 +237,7 @@ __device__ __forceinline__ void trow(const Job& J, int w, int p, fp2& x0, fp2& x
 }
 
 template <bool FOLD>
-__global__ void __launch_bounds__(kBT) table_round_kernel(const Job* __restrict__ jobs)
+__global__ void __launch_bounds__(kBT, 4) table_round_kernel(const Job* __restrict__ jobs)
 {
     __shared__ __align__(16) Job J;
     __shared__ __align__(16) fp2 red[kWarps * 32 * 4];
