@@ -209,6 +209,18 @@ void tp_timer_disable(void);
 void tp_timer_reset(void);
 int tp_timer_read(float* ms, int* tags, int max_pairs);
 
+/* No counterpart in the reference. tp_mle_eval_base_dev for callers that cannot
+ * allocate device memory (their GPU memory belongs to another allocator, or a
+ * time-critical loop cannot afford cudaMalloc/cudaFree): it calls no allocator
+ * and uses a fixed 339 KB scratch array compiled into the library, which every
+ * GPU that loads the library keeps until exit. Inputs up to 2^26 base-field
+ * values (n_z <= 26); larger n_z is rejected with an error (-1). All calls share
+ * the scratch: calls that overlap on the GPU race, order them. The first call
+ * on a device looks up the scratch's device address; make it before any stream
+ * capture. d_inputs: 2^n_z u64; d_z: n_z packed Fp2; d_out: 1 packed Fp2. Async. */
+int tp_mle_eval_base_noalloc(const void* d_inputs, const void* d_z, int n_z, void* d_out,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -748,6 +748,23 @@ bool launch_beta_batch(const fp2* d_z, int n_z, int n, fp2* d_out, cudaStream_t 
     return !cuda_failed(cudaGetLastError(), "beta batch launch");
 }
 
+bool launch_mle_base_into(const u64* d_in, const fp2* d_z, int n_z, fp2* d_out, fp2* tabs,
+                          fp2* partials, unsigned* ticket, unsigned max_blocks, cudaStream_t s)
+{
+    const int h = std::min(n_z, 12), hb = n_z - h;
+    const size_t nt = ((size_t)1 << h) + ((size_t)1 << hb);
+    fp2* lo = tabs;
+    fp2* hi = tabs + ((size_t)1 << h);
+    eq_tables_kernel<<<blocks_for(nt, kThreads), kThreads, 0, s>>>(d_z, h, hb, mk(1, 0), lo, hi);
+    const size_t n = (size_t)1 << n_z;
+    const size_t work = h >= 3 ? (n >> 3) : n;
+    const unsigned blocks = (unsigned)std::max<size_t>(
+        1, std::min<size_t>(blocks_for(work, kThreads), (size_t)max_blocks));
+    mle_kernel<<<blocks, kThreads, 0, s>>>(d_in, n, h, lo, hi, partials, ticket,
+                                           reinterpret_cast<u64*>(d_out));
+    return !cuda_failed(cudaGetLastError(), "mle launch");
+}
+
 bool launch_mle_base(const u64* d_in, const fp2* d_z, int n_z, fp2* d_out, cudaStream_t s)
 {
     t_launches = 0;

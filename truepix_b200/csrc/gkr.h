@@ -122,6 +122,10 @@ bool launch_claim_explicit(const DevGateForm& g, int n_copies, const u64* const*
 // eq table: out[i] = init * prod_j (bit_j(i) ? z_j : 1 - z_j), SoA or packed
 bool launch_beta(const fp2* d_z, int n_z, fp2 init, u64* out_re, u64* out_im, fp2* out_aos,
                  cudaStream_t s);
+// The same MLE with caller-provided scratch: tabs (2^min(n_z,12) + 2^(n_z-12) Fp2),
+// partials (max_blocks Fp2) and a zeroed ticket; launches at most max_blocks blocks.
+bool launch_mle_base_into(const u64* d_in, const fp2* d_z, int n_z, fp2* d_out, fp2* tabs,
+                          fp2* partials, unsigned* ticket, unsigned max_blocks, cudaStream_t s);
 // MLE of base-field inputs (2^n_z u64) at the Fp2 point z -> d_out (1 fp2)
 bool launch_mle_base(const u64* d_in, const fp2* d_z, int n_z, fp2* d_out, cudaStream_t s);
 // uint8 frame (n_real copies x copy_size bytes, copy-major) -> packed wire-major

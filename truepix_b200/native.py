@@ -69,6 +69,7 @@ GKR_SIGNATURES = {
     "tp_compute_beta_batch_dev": (_I32, [_VP, _I32, _I32, _VP, _VP]),
     "tp_mle_eval_pixels_batch": (_I32, [_I32, ctypes.POINTER(_VP), _PI32, _I32, _I32, _I32, _I32,
                                         _U64, _VP, _VP, _VP]),
+    "tp_mle_eval_base_noalloc": (_I32, [_VP, _VP, _I32, _VP, _VP]),
     "tp_timer_enable": (_I32, [_I32]),
     "tp_timer_disable": (None, []),
     "tp_timer_reset": (None, []),
