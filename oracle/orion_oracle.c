@@ -1,0 +1,448 @@
+/*
+ * CPU oracle for the Orion commitment (expander encode + SHA-256 Merkle tree)
+ * -- TEST INFRASTRUCTURE ONLY. Only tests/ and bench.py's cpu_baseline leg
+ * load it; the shipped library never links or calls it.
+ *
+ * Restates, in plain C:
+ *   - glibc rand() (TYPE_3 additive feedback generator, the published glibc
+ *     algorithm: 34-word state seeded by the 16807 LCG, 310 discarded outputs,
+ *     r[i] = r[i-31] + r[i-3], output r[i] >> 1); the reference never seeds it,
+ *     so its stream starts from seed 1 (TruePix-main/Orion/Orion_nonzk/include/
+ *     linear_code/expanders.h:19-60 is its first consumer);
+ *   - the expander graphs (expanders.h:19-60, parameter.h: alpha 0.238, r 1.72,
+ *     degrees 10 / 20, distance threshold 13) and the recursive encoder
+ *     (include/linear_code/linear_code_encode.h:8-72);
+ *   - SHA-256 (FIPS 180-4) of one 64-byte block, as my_hhash
+ *     (include/infrastructure/my_hhash.h:46-54 over flo-shani);
+ *   - commit (src/VPD/linearPC.cpp:97-197): 128 columns of N/128 elements, row
+ *     leaves chained over the 64 column pairs, h <- SHA256(h || x || y) with
+ *     field elements as LE64(img) || LE64(real); padded rows use the zero-element
+ *     chain; Merkle tree in heap order (src/infrastructure/merkle_tree.cpp:28-84).
+ *
+ * Parity pin: tests/golden/orion_golden.npz holds roots produced by the
+ * reference sources themselves (oracle/orion_ref_harness.cpp, built by
+ * `make -C oracle ref`), checked by tests/test_oracle.py.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef uint64_t u64;
+typedef uint32_t u32;
+typedef unsigned __int128 u128;
+#define P61 ((u64)0x1FFFFFFFFFFFFFFFull)
+
+/* ---- field (Fp2 = Fp[i]/(i^2+1)), elements stored as (img, real) ---- */
+static inline u64 canon(u64 x) { return x >= P61 ? x - P61 : x; }
+static inline u64 fadd(u64 a, u64 b) { return canon(a + b); }
+static inline u64 fmul(u64 a, u64 b)
+{
+    u128 t = (u128)a * b;
+    return canon(((u64)t & P61) + (u64)(t >> 61));
+}
+typedef struct { u64 img, real; } fe;
+static inline fe feadd(fe a, fe b) { fe r = {fadd(a.img, b.img), fadd(a.real, b.real)}; return r; }
+static inline fe femul(fe a, fe b)
+{
+    fe r;
+    r.real = canon(fmul(a.real, b.real) + (P61 - fmul(a.img, b.img)));
+    r.img = fadd(fmul(a.real, b.img), fmul(a.img, b.real));
+    return r;
+}
+
+/* ---- glibc rand() ---- */
+typedef struct { u32 r[34]; int i; } grand;
+
+void oracle_glibc_seed(grand* g, u32 seed)
+{
+    int32_t r[34];
+    r[0] = (int32_t)seed;
+    for (int i = 1; i < 31; ++i) {
+        long long v = (16807LL * r[i - 1]) % 2147483647LL;
+        if (v < 0) v += 2147483647LL;
+        r[i] = (int32_t)v;
+    }
+    for (int i = 31; i < 34; ++i) r[i] = r[i - 31];
+    for (int i = 0; i < 34; ++i) g->r[i] = (u32)r[i];
+    g->i = 34;
+    /* discard 310 outputs */
+    for (int k = 0; k < 310; ++k) {
+        u32 v = g->r[(g->i - 31) % 34] + g->r[(g->i - 3) % 34];
+        g->r[g->i % 34] = v;
+        g->i++;
+    }
+}
+
+static inline int grand_next(grand* g)
+{
+    u32 v = g->r[(g->i - 31) % 34] + g->r[(g->i - 3) % 34];
+    g->r[g->i % 34] = v;
+    g->i++;
+    return (int)(v >> 1);
+}
+
+void oracle_glibc_stream(u32 seed, int n, int* out)
+{
+    grand g;
+    oracle_glibc_seed(&g, seed);
+    for (int i = 0; i < n; ++i) out[i] = grand_next(&g);
+}
+
+/* ---- expander graphs and encoder ---- */
+#define CN 10
+#define DN 20
+#define THRESH 13
+typedef struct { long long L, R; int degree; long long* nb; fe* w; } graph;
+typedef struct { graph C[64], D[64]; int depth; } expanders;
+
+static void gen_graph(grand* g, graph* gr, long long L, long long R, int d)
+{
+    gr->L = L;
+    gr->R = R;
+    gr->degree = d;
+    gr->nb = (long long*)malloc(sizeof(long long) * (size_t)(L * d > 0 ? L * d : 1));
+    gr->w = (fe*)malloc(sizeof(fe) * (size_t)(L * d > 0 ? L * d : 1));
+    for (long long i = 0; i < L; ++i)
+        for (int j = 0; j < d; ++j) {
+            long long t = (long long)grand_next(g) % R;
+            fe w;
+            w.real = (u64)grand_next(g) % P61;
+            w.img = (u64)grand_next(g) % P61;
+            gr->nb[i * d + j] = t;
+            gr->w[i * d + j] = w;
+        }
+}
+
+static long long exp_init(grand* g, expanders* E, long long n, int dep)
+{
+    if (n <= THRESH) {
+        if (dep > E->depth) E->depth = dep;
+        return n;
+    }
+    long long R = (long long)(0.238 * (double)n);
+    gen_graph(g, &E->C[dep], n, R, CN);
+    long long L = exp_init(g, E, R, dep + 1);
+    long long RD = (long long)((double)n * (1.72 - 1) - (double)L);
+    gen_graph(g, &E->D[dep], L, RD, DN);
+    return n + L + RD;
+}
+
+static long long enc_len(const expanders* E, long long n, int dep)
+{
+    if (n <= THRESH) return n;
+    long long R = (long long)(0.238 * (double)n);
+    long long L = enc_len(E, R, dep + 1);
+    return n + L + E->D[dep].R;
+}
+
+static long long encode(const expanders* E, const fe* src, fe* dst, long long n, int dep)
+{
+    if (n <= THRESH) {
+        memcpy(dst, src, sizeof(fe) * (size_t)n);
+        return n;
+    }
+    const graph* C = &E->C[dep];
+    const graph* D = &E->D[dep];
+    long long R = (long long)(0.238 * (double)n);
+    fe* y = (fe*)calloc((size_t)R + 1, sizeof(fe));
+    for (long long i = 0; i < n; ++i)
+        for (int d = 0; d < C->degree; ++d) {
+            long long t = C->nb[i * C->degree + d];
+            y[t] = feadd(y[t], femul(C->w[i * C->degree + d], src[i]));
+        }
+    memcpy(dst, src, sizeof(fe) * (size_t)n);
+    long long L = encode(E, y, dst + n, R, dep + 1);
+    free(y);
+    fe* out = dst + n + L;
+    memset(out, 0, sizeof(fe) * (size_t)D->R);
+    for (long long i = 0; i < L; ++i)
+        for (int d = 0; d < D->degree; ++d) {
+            long long t = D->nb[i * D->degree + d];
+            out[t] = feadd(out[t], femul(dst[n + i], D->w[i * D->degree + d]));
+        }
+    return n + L + D->R;
+}
+
+static void free_expanders(expanders* E)
+{
+    for (int d = 0; d < 64; ++d) {
+        free(E->C[d].nb); free(E->C[d].w);
+        free(E->D[d].nb); free(E->D[d].w);
+    }
+}
+
+/* ---- SHA-256 (FIPS 180-4) of one 64-byte message ---- */
+static const u32 K256[64] = {
+    0x428a2f98, 0x71374491, 0xb5c0fbcf, 0xe9b5dba5, 0x3956c25b, 0x59f111f1, 0x923f82a4, 0xab1c5ed5,
+    0xd807aa98, 0x12835b01, 0x243185be, 0x550c7dc3, 0x72be5d74, 0x80deb1fe, 0x9bdc06a7, 0xc19bf174,
+    0xe49b69c1, 0xefbe4786, 0x0fc19dc6, 0x240ca1cc, 0x2de92c6f, 0x4a7484aa, 0x5cb0a9dc, 0x76f988da,
+    0x983e5152, 0xa831c66d, 0xb00327c8, 0xbf597fc7, 0xc6e00bf3, 0xd5a79147, 0x06ca6351, 0x14292967,
+    0x27b70a85, 0x2e1b2138, 0x4d2c6dfc, 0x53380d13, 0x650a7354, 0x766a0abb, 0x81c2c92e, 0x92722c85,
+    0xa2bfe8a1, 0xa81a664b, 0xc24b8b70, 0xc76c51a3, 0xd192e819, 0xd6990624, 0xf40e3585, 0x106aa070,
+    0x19a4c116, 0x1e376c08, 0x2748774c, 0x34b0bcb5, 0x391c0cb3, 0x4ed8aa4a, 0x5b9cca4f, 0x682e6ff3,
+    0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7, 0xc67178f2};
+#define ROR(x, n) (((x) >> (n)) | ((x) << (32 - (n))))
+
+static void sha_block(u32 st[8], const unsigned char* blk)
+{
+    u32 w[64];
+    for (int t = 0; t < 16; ++t)
+        w[t] = ((u32)blk[4 * t] << 24) | ((u32)blk[4 * t + 1] << 16) | ((u32)blk[4 * t + 2] << 8) |
+               blk[4 * t + 3];
+    for (int t = 16; t < 64; ++t) {
+        u32 s0 = ROR(w[t - 15], 7) ^ ROR(w[t - 15], 18) ^ (w[t - 15] >> 3);
+        u32 s1 = ROR(w[t - 2], 17) ^ ROR(w[t - 2], 19) ^ (w[t - 2] >> 10);
+        w[t] = w[t - 16] + s0 + w[t - 7] + s1;
+    }
+    u32 a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
+    for (int t = 0; t < 64; ++t) {
+        u32 t1 = h + (ROR(e, 6) ^ ROR(e, 11) ^ ROR(e, 25)) + ((e & f) ^ (~e & g)) + K256[t] + w[t];
+        u32 t2 = (ROR(a, 2) ^ ROR(a, 13) ^ ROR(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+        h = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
+    }
+    st[0] += a; st[1] += b; st[2] += c; st[3] += d; st[4] += e; st[5] += f; st[6] += g; st[7] += h;
+}
+
+void oracle_sha256_64(const unsigned char* in, unsigned char* out)
+{
+    u32 st[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
+                 0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+    unsigned char pad[64];
+    memset(pad, 0, 64);
+    pad[0] = 0x80;
+    pad[62] = 0x02;  /* 512 bits, big-endian length */
+    sha_block(st, in);
+    sha_block(st, pad);
+    for (int i = 0; i < 8; ++i) {
+        out[4 * i] = (unsigned char)(st[i] >> 24);
+        out[4 * i + 1] = (unsigned char)(st[i] >> 16);
+        out[4 * i + 2] = (unsigned char)(st[i] >> 8);
+        out[4 * i + 3] = (unsigned char)st[i];
+    }
+}
+
+static void put_fe(unsigned char* p, fe x)
+{
+    for (int i = 0; i < 8; ++i) p[i] = (unsigned char)(x.img >> (8 * i));
+    for (int i = 0; i < 8; ++i) p[8 + i] = (unsigned char)(x.real >> (8 * i));
+}
+
+/* ---- commit ---- */
+long long oracle_encode_len(long long col_len)
+{
+    grand g;
+    expanders E;
+    memset(&E, 0, sizeof(E));
+    oracle_glibc_seed(&g, 1);
+    long long n = exp_init(&g, &E, col_len, 0);
+    free_expanders(&E);
+    return n;
+}
+
+/* codeword of one column of n elements (graphs from the default seed); dst
+ * holds oracle_encode_len(n) elements. Returns that length. */
+long long oracle_encode(const u64* src, long long n, u64* dst)
+{
+    grand g;
+    expanders E;
+    memset(&E, 0, sizeof(E));
+    oracle_glibc_seed(&g, 1);
+    exp_init(&g, &E, n, 0);
+    long long len = encode(&E, (const fe*)src, (fe*)dst, n, 0);
+    free_expanders(&E);
+    return len;
+}
+
+/* src: N elements as (img, real) u64 pairs; writes the 32-byte root. Optionally
+ * returns the leaves (rows x 32 bytes) when leaves != NULL. */
+int oracle_orion_commit(const u64* src, long long N, unsigned char* root, unsigned char* leaves)
+{
+    if (N % 128 != 0) return -1;
+    const long long col_len = N / 128, rows = 2 * col_len;
+    grand g;
+    expanders E;
+    memset(&E, 0, sizeof(E));
+    oracle_glibc_seed(&g, 1);
+    const long long cw_len = exp_init(&g, &E, col_len, 0);
+    if (cw_len != enc_len(&E, col_len, 0)) return -2;
+    fe* cw = (fe*)calloc((size_t)(128 * (cw_len + 1)), sizeof(fe));
+    for (int c = 0; c < 128; ++c)
+        encode(&E, (const fe*)src + (size_t)c * col_len, cw + (size_t)c * cw_len, col_len, 0);
+    unsigned char* stash = (unsigned char*)calloc((size_t)rows, 32);
+    unsigned char blk[64];
+    for (long long r = 0; r < cw_len; ++r) {
+        unsigned char* h = stash + 32 * r;
+        for (int j = 0; j < 64; ++j) {
+            memcpy(blk, h, 32);
+            put_fe(blk + 32, cw[(size_t)(2 * j) * cw_len + r]);
+            put_fe(blk + 48, cw[(size_t)(2 * j + 1) * cw_len + r]);
+            oracle_sha256_64(blk, h);
+        }
+    }
+    unsigned char zl[32];
+    memset(zl, 0, 32);
+    for (int j = 0; j < 64; ++j) {
+        memcpy(blk, zl, 32);
+        memset(blk + 32, 0, 32);
+        oracle_sha256_64(blk, zl);
+    }
+    for (long long r = cw_len; r < rows; ++r) memcpy(stash + 32 * r, zl, 32);
+    if (leaves) memcpy(leaves, stash, (size_t)rows * 32);
+    long long size = 1;
+    while (size < rows) size *= 2;
+    unsigned char* tree = (unsigned char*)calloc((size_t)(2 * size), 32);
+    memcpy(tree + 32 * size, stash, (size_t)rows * 32);
+    for (long long i = rows; i < size; ++i) {  /* padded leaves: SHA256(0^64) */
+        memset(blk, 0, 64);
+        oracle_sha256_64(blk, tree + 32 * (size + i));
+    }
+    for (long long k = size - 1; k >= 1; --k) {
+        memcpy(blk, tree + 32 * (2 * k), 32);
+        memcpy(blk + 32, tree + 32 * (2 * k + 1), 32);
+        oracle_sha256_64(blk, tree + 32 * k);
+    }
+    memcpy(root, tree + 32, 32);
+    free(tree);
+    free(stash);
+    free(cw);
+    free_expanders(&E);
+    return 0;
+}
+
+/* ---- Fp2 NTT (TruePix-main/Orion/Orion_nonzk/src/infrastructure/RS_polynomial.cpp:46-206) ----
+ * fft: result[i] = P(w^i), i < order, P given by coef_len coefficients, w the
+ * order-th root of unity of get_root_of_unity (src/linear_gkr/prime_field.cpp:60-73:
+ * g = (real 2147483648, img 1033321771269002680) squared 62 - log2(order) times).
+ * ifft: the coef_len coefficients whose evaluations on the coef_len-th roots of
+ * unity are evals[i * (order / coef_len)]. Any exact transform gives the same
+ * values; this one splits the order points into order/coef_len cosets. */
+static fe fe_pow(fe a, u64 e)
+{
+    fe r = {0, 1};
+    while (e) {
+        if (e & 1) r = femul(r, a);
+        a = femul(a, a);
+        e >>= 1;
+    }
+    return r;
+}
+
+static fe root_of_unity(int lg)
+{
+    fe g = {1033321771269002680ull, 2147483648ull};
+    for (int i = 0; i < 62 - lg; ++i) g = femul(g, g);
+    return g;
+}
+
+static int ilog2(long long n)
+{
+    int k = 0;
+    while ((1LL << k) < n) ++k;
+    return k;
+}
+
+/* in-place radix-2 DFT of length m = 2^k: a[t] <- sum_j a[j] w^(jt) */
+static void dft_inplace(fe* a, long long m, fe w)
+{
+    int k = ilog2(m);
+    for (long long i = 1, j = 0; i < m; ++i) {
+        long long bit = m >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) { fe t = a[i]; a[i] = a[j]; a[j] = t; }
+    }
+    for (int s = 1; s <= k; ++s) {
+        long long len = 1LL << s, half = len >> 1;
+        fe wl = fe_pow(w, (u64)(m / len));
+        for (long long b = 0; b < m; b += len) {
+            fe x = {0, 1};
+            for (long long j = 0; j < half; ++j) {
+                fe u = a[b + j], v = femul(a[b + j + half], x);
+                a[b + j] = feadd(u, v);
+                fe nv = {canon(P61 - v.img), canon(P61 - v.real)};
+                a[b + j + half] = feadd(u, nv);
+                x = femul(x, wl);
+            }
+        }
+    }
+}
+
+int oracle_fft(const u64* coef, long long coef_len, long long order, u64* result)
+{
+    if (coef_len < 1 || order < coef_len || (coef_len & (coef_len - 1)) || (order & (order - 1)) ||
+        order > (1LL << 27))
+        return -1;
+    const fe* c = (const fe*)coef;
+    fe* out = (fe*)result;
+    const fe w = root_of_unity(ilog2(order));
+    const long long b = order / coef_len;
+    const fe wb = fe_pow(w, (u64)b);
+    fe* t = (fe*)malloc(sizeof(fe) * (size_t)coef_len);
+    for (long long s = 0; s < b; ++s) {
+        fe ws = fe_pow(w, (u64)s), x = {0, 1};
+        for (long long j = 0; j < coef_len; ++j) { t[j] = femul(c[j], x); x = femul(x, ws); }
+        dft_inplace(t, coef_len, wb);
+        for (long long q = 0; q < coef_len; ++q) out[s + b * q] = t[q];
+    }
+    free(t);
+    return 0;
+}
+
+int oracle_ifft(const u64* evals, long long coef_len, long long order, u64* result)
+{
+    if (coef_len < 1 || order < coef_len || (coef_len & (coef_len - 1)) || (order & (order - 1)) ||
+        order > (1LL << 27))
+        return -1;
+    const fe* e = (const fe*)evals;
+    fe* out = (fe*)result;
+    const long long b = order / coef_len;
+    for (long long i = 0; i < coef_len; ++i) out[i] = e[i * b];
+    const int k = ilog2(coef_len);
+    fe wi = fe_pow(root_of_unity(k), (u64)(coef_len - 1));  /* inverse root */
+    dft_inplace(out, coef_len, wi);
+    const fe inv_n = {0, k ? (1ull << (61 - k)) : 1ull};     /* 2^-k = 2^(61-k) mod p */
+    for (long long i = 0; i < coef_len; ++i) out[i] = femul(out[i], inv_n);
+    return 0;
+}
+
+/* ---- RS commit (include/poly_commitment/poly_commit.h:42-96 + src/VPD/fri.cpp:36-123) ----
+ * 64 slices of 2^(L-6) elements; slice i -> IFFT -> FFT onto 2^(L-1) points
+ * (l_eval[i][.]); codeword interleaved as w[(j << 7) | (i << 1) | h] =
+ * l_eval[i][j + h * 2^(L-2)]; leaf j = chain over its 64 pairs of
+ * h <- SHA256(x || y || h) from zero; Merkle tree over the 2^(L-2) leaves. */
+int oracle_rs_commit(const u64* src, int log_len, unsigned char* root, u64* l_eval_out)
+{
+    if (log_len < 6 || log_len > 28) return -1;
+    const long long real_cnt = 1LL << (log_len - 6), slice = 1LL << (log_len - 1);
+    const long long total = slice * 64, n_leaves = slice / 2;
+    fe* lev = (fe*)malloc(sizeof(fe) * (size_t)total);
+    fe* tmp = (fe*)malloc(sizeof(fe) * (size_t)real_cnt);
+    for (int i = 0; i < 64; ++i) {
+        oracle_ifft(src + 2 * i * real_cnt, real_cnt, real_cnt, (u64*)tmp);
+        oracle_fft((const u64*)tmp, real_cnt, slice, (u64*)(lev + i * slice));
+    }
+    free(tmp);
+    if (l_eval_out) memcpy(l_eval_out, lev, sizeof(fe) * (size_t)total);
+    unsigned char* tree = (unsigned char*)calloc((size_t)(2 * n_leaves), 32);
+    unsigned char blk[64];
+    for (long long j = 0; j < n_leaves; ++j) {
+        unsigned char h[32];
+        memset(h, 0, 32);
+        for (int i = 0; i < 64; ++i) {
+            put_fe(blk, lev[i * slice + j]);
+            put_fe(blk + 16, lev[i * slice + j + n_leaves]);
+            memcpy(blk + 32, h, 32);
+            oracle_sha256_64(blk, h);
+        }
+        memcpy(tree + 32 * (n_leaves + j), h, 32);
+    }
+    for (long long k = n_leaves - 1; k >= 1; --k) {
+        memcpy(blk, tree + 32 * (2 * k), 32);
+        memcpy(blk + 32, tree + 32 * (2 * k + 1), 32);
+        oracle_sha256_64(blk, tree + 32 * k);
+    }
+    memcpy(root, tree + 32, 32);
+    free(tree);
+    free(lev);
+    return 0;
+}

@@ -1,0 +1,111 @@
+// C entry points over the reference's own Orion sources (TEST INFRASTRUCTURE).
+//
+// Compiled by `make -C oracle ref` together with the unmodified reference files
+// under TruePix-main/Orion/Orion_nonzk (their own sources, compiled in place)
+// into oracle/_ref/liborion_ref.so. The golden generator and the CPU baseline
+// call these; the shipped library never links them.
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+
+#include "infrastructure/RS_polynomial.h"
+#include "infrastructure/merkle_tree.h"
+#include "infrastructure/my_hhash.h"
+#include "linear_code/linear_code_encode.h"
+#include "linear_gkr/prime_field.h"
+#include "poly_commitment/poly_commit.h"
+#include "VPD/linearPC.h"
+#include "truepix/truepix_gkr.h"
+
+extern "C" {
+
+// SHA-256 of one 64-byte block exactly as Orion hashes it (my_hhash)
+void ref_hhash64(const unsigned char* in, unsigned char* out32)
+{
+    my_hhash(in, out32);
+}
+
+// element pairs are (img, real), the reference's memory order
+static_assert(sizeof(prime_field::field_element) == 16, "field_element layout");
+
+// result[i] = P(w^i), w = get_root_of_unity(log2 order), P given by coef_len coefficients
+void ref_fft(const uint64_t* coef, int coef_len, int order, uint64_t* result)
+{
+    prime_field::init();
+    init_scratch_pad(order);
+    const int lg = __builtin_ctz((unsigned)order);
+    fast_fourier_transform(reinterpret_cast<const prime_field::field_element*>(coef), coef_len,
+                           order, prime_field::get_root_of_unity(lg),
+                           reinterpret_cast<prime_field::field_element*>(result));
+    delete_scratch_pad();
+}
+
+// coefficients (coef_len of them) of the polynomial whose evaluations on the
+// order-th roots of unity are `evals` (sub-sampled when coef_len < order)
+void ref_ifft(const uint64_t* evals, int coef_len, int order, uint64_t* result)
+{
+    prime_field::init();
+    init_scratch_pad(order);
+    const int lg = __builtin_ctz((unsigned)order);
+    prime_field::field_element* e = new prime_field::field_element[order];
+    memcpy(e, evals, 16 * (size_t)order);
+    inverse_fast_fourier_transform(e, coef_len, order, prime_field::get_root_of_unity(lg),
+                                   reinterpret_cast<prime_field::field_element*>(result));
+    delete[] e;
+    delete_scratch_pad();
+}
+
+// Orion commit of N field elements (N a multiple of 128) exactly as
+// linearPC_multi_commit does it in a fresh process (glibc rand() from its
+// default seed drives expander_init). Writes the 32-byte root and its hex form
+// (truepix::root_hex). Call once per process: the reference keeps encoder state.
+void ref_commit(const uint64_t* src, long long N, unsigned char* root32, char* hex65)
+{
+    prime_field::init();
+    srand(1);
+    expander_init(N / column_size);
+    set_retain_encoded_codeword(true);
+    __hhash_digest* h = commit(reinterpret_cast<const prime_field::field_element*>(src), N);
+    memcpy(root32, &h[1], 32);
+    const std::string hx = truepix::root_hex(h[1]);
+    memcpy(hex65, hx.c_str(), 65);
+}
+
+// Reed-Solomon commit of 2^log_len elements exactly as
+// poly_commit_prover::commit_private_array does it: 64 slices, each an IFFT of
+// 2^(log_len-6) evaluations followed by an FFT onto 2^(log_len-1) points (rate
+// 2^-5), then fri::request_init_commit's interleave, leaf chains and Merkle
+// tree. Writes the root and, when l_eval != NULL, the 2^(log_len+5) codeword
+// elements (slice-major). Call once per process.
+void ref_rs_commit(const uint64_t* src, int log_len, unsigned char* root32, uint64_t* l_eval)
+{
+    prime_field::init();
+    const size_t n = (size_t)1 << log_len;
+    prime_field::field_element* a = new prime_field::field_element[n];
+    memcpy(a, src, 16 * n);
+    poly_commit::poly_commit_prover p;
+    __hhash_digest h = p.commit_private_array(a, log_len);
+    memcpy(root32, &h, 32);
+    if (l_eval) memcpy(l_eval, poly_commit::l_eval, 16 * (n << rs_code_rate));
+    delete[] a;
+}
+
+// encoded length of a column of n elements (graphs generated from the default seed)
+long long ref_encode_len(long long n)
+{
+    srand(1);
+    expander_init(n);
+    return encode_output_len(n);
+}
+
+// the codeword of one column of n elements: dst must hold ref_encode_len(n) elements
+void ref_encode(const uint64_t* src, long long n, uint64_t* dst)
+{
+    prime_field::init();
+    srand(1);
+    expander_init(n);
+    encode(reinterpret_cast<const prime_field::field_element*>(src),
+           reinterpret_cast<prime_field::field_element*>(dst), n);
+}
+
+}  // extern "C"

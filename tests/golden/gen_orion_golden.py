@@ -1,0 +1,131 @@
+"""Generate the golden fixtures for the Orion side of the path from the reference.
+
+Runs the reference's own Orion sources, compiled by `make -C oracle ref` into
+oracle/_ref/liborion_ref.so (TruePix-main/Orion/Orion_nonzk sources + the C
+harness oracle/orion_ref_harness.cpp), on seeded inputs (tests/orionlib.py
+`elements`, splitmix64-based) and stores the outputs in
+tests/golden/orion_golden.npz:
+
+  commit_<case>   32-byte Merkle roots of the Orion commit (linearPC.cpp:97-197)
+  encode_<n>      SHA-256 digest of the expander codeword of one column
+                  (linear_code_encode.h:17-72); full codeword for n = 64
+  fft_<m>_<o>     digest of P(w^i), i < o, for m seeded coefficients
+                  (RS_polynomial.cpp:46-130)
+  ifft_<m>_<o>    digest of the m coefficients from o seeded evaluations
+                  (RS_polynomial.cpp:132-206)
+  rs_<L>          Merkle root and codeword digest of the rate-2^-5 RS commit
+                  of 2^L elements (poly_commit.h:42-96, fri.cpp:36-123)
+
+Every reference call runs in a fresh spawned process: the reference keeps
+global scratch state sized by its first call.
+
+Run here (needs the reference checkout and `make -C oracle ref`):
+    python tests/golden/gen_orion_golden.py
+"""
+from __future__ import annotations
+
+import ctypes
+import multiprocessing as mp
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+from orionlib import ORION_REF_LIB, digest, elements  # noqa: E402
+
+V = ctypes.c_void_p
+
+COMMIT_CASES = [  # (name, log2 N, seed, kind)
+    ("r13", 13, 1, "random"), ("zero13", 13, 0, "zero"), ("max13", 13, 0, "max"),
+    ("small14", 14, 7, "small"), ("r14", 14, 2, "random"), ("r15", 15, 3, "random"),
+    ("r16", 16, 4, "random"), ("r18", 18, 5, "random"), ("r20", 20, 6, "random"),
+]
+ENCODE_CASES = [1, 13, 14, 64, 100, 1000, 8192, 65536]
+FFT_CASES = [(1, 1), (1, 8), (2, 2), (8, 8), (4, 16), (16, 256), (1024, 1024), (256, 4096),
+             (1 << 12, 1 << 17), (1 << 16, 1 << 16), (1 << 20, 1 << 20)]
+RS_CASES = [6, 7, 10, 13, 16, 18]
+
+
+def _ref():
+    lib = ctypes.CDLL(ORION_REF_LIB)
+    lib.ref_commit.argtypes = [V, ctypes.c_longlong, V, V]
+    lib.ref_fft.argtypes = [V, ctypes.c_int, ctypes.c_int, V]
+    lib.ref_ifft.argtypes = [V, ctypes.c_int, ctypes.c_int, V]
+    lib.ref_rs_commit.argtypes = [V, ctypes.c_int, V, V]
+    lib.ref_encode.argtypes = [V, ctypes.c_longlong, V]
+    lib.ref_encode_len.argtypes = [ctypes.c_longlong]
+    lib.ref_encode_len.restype = ctypes.c_longlong
+    return lib
+
+
+def _commit(args):
+    lg, seed, kind = args
+    src = elements(seed, 1 << lg, kind)
+    root = ctypes.create_string_buffer(32)
+    hx = ctypes.create_string_buffer(80)
+    _ref().ref_commit(V(src.ctypes.data), 1 << lg, root, hx)
+    return root.raw, hx.value
+
+
+def _encode(n):
+    lib = _ref()
+    src = elements(100 + n, n)
+    out = np.zeros(2 * lib.ref_encode_len(n), np.uint64)
+    lib.ref_encode(V(src.ctypes.data), n, V(out.ctypes.data))
+    return out
+
+
+def _fft(args):
+    m, o = args
+    src = elements(200 + m + o, m)
+    out = np.zeros(2 * o, np.uint64)
+    _ref().ref_fft(V(src.ctypes.data), m, o, V(out.ctypes.data))
+    return out
+
+
+def _ifft(args):
+    m, o = args
+    src = elements(300 + m + o, o)
+    out = np.zeros(2 * m, np.uint64)
+    _ref().ref_ifft(V(src.ctypes.data), m, o, V(out.ctypes.data))
+    return out
+
+
+def _rs(lg):
+    src = elements(400 + lg, 1 << lg)
+    root = ctypes.create_string_buffer(32)
+    cw = np.zeros(2 << (lg + 5), np.uint64)
+    _ref().ref_rs_commit(V(src.ctypes.data), lg, root, V(cw.ctypes.data))
+    return root.raw, digest(cw)
+
+
+def main():
+    ctx = mp.get_context("spawn")
+    out = {}
+    with ctx.Pool(8, maxtasksperchild=1) as pool:
+        for (name, lg, seed, kind), (root, hx) in zip(
+                COMMIT_CASES, pool.map(_commit, [c[1:] for c in COMMIT_CASES], chunksize=1)):
+            out["commit_" + name] = np.frombuffer(root, np.uint8)
+            out["commithex_" + name] = np.frombuffer(hx, np.uint8)
+            out["commitcase_" + name] = np.array([lg, seed, ["random", "zero", "max", "small"].index(kind)])
+        for n, cw in zip(ENCODE_CASES, pool.map(_encode, ENCODE_CASES, chunksize=1)):
+            out["encode_%d" % n] = np.frombuffer(digest(cw), np.uint8)
+            out["encodelen_%d" % n] = np.array([cw.size // 2])
+            if n == 64:
+                out["encodefull_64"] = cw
+        for (m, o), r in zip(FFT_CASES, pool.map(_fft, FFT_CASES, chunksize=1)):
+            out["fft_%d_%d" % (m, o)] = np.frombuffer(digest(r), np.uint8)
+            out["ffthead_%d_%d" % (m, o)] = r[:16].copy()
+        for (m, o), r in zip(FFT_CASES, pool.map(_ifft, FFT_CASES, chunksize=1)):
+            out["ifft_%d_%d" % (m, o)] = np.frombuffer(digest(r), np.uint8)
+        for lg, (root, d) in zip(RS_CASES, pool.map(_rs, RS_CASES, chunksize=1)):
+            out["rs_%d" % lg] = np.frombuffer(root, np.uint8)
+            out["rscw_%d" % lg] = np.frombuffer(d, np.uint8)
+    np.savez_compressed(os.path.join(HERE, "orion_golden.npz"), **out)
+    print("wrote", len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()

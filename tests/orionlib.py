@@ -1,0 +1,119 @@
+"""Helpers shared by the Orion tests, the golden generator and the bench.
+
+Field elements are 16 bytes in the reference's memory order: u64 img, then
+u64 real (TruePix-main/Orion/Orion_nonzk/include/linear_gkr/prime_field.h).
+Arrays of n elements are numpy uint64 arrays of 2n words [img0, re0, img1, ...].
+
+`elements(seed, n)` makes seeded inputs without depending on numpy's
+generator streams (splitmix64 of seed:index), so fixtures stay valid across
+numpy versions.
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import os
+
+import numpy as np
+
+P61 = (1 << 61) - 1
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORION_ORACLE_LIB = os.path.join(ROOT, "oracle", "liborion_oracle.so")
+ORION_REF_LIB = os.path.join(ROOT, "oracle", "_ref", "liborion_ref.so")
+
+_V = ctypes.c_void_p
+_LL = ctypes.c_longlong
+_I = ctypes.c_int
+
+
+def splitmix64(x: np.ndarray) -> np.ndarray:
+    with np.errstate(over="ignore"):
+        z = x + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def elements(seed: int, n: int, kind: str = "random") -> np.ndarray:
+    """n canonical Fp2 elements (2n u64 words). kind: random | zero | max | small."""
+    if kind == "zero":
+        return np.zeros(2 * n, np.uint64)
+    if kind == "max":
+        return np.full(2 * n, P61 - 1, np.uint64)
+    idx = np.arange(2 * n, dtype=np.uint64) + (np.uint64(seed) << np.uint64(40))
+    v = splitmix64(idx)
+    if kind == "small":
+        return v & np.uint64(0xFF)
+    return (v >> np.uint64(3)) % np.uint64(P61)
+
+
+def digest(a: np.ndarray) -> bytes:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest()
+
+
+def _vp(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class OrionOracle:
+    """ctypes view of oracle/orion_oracle.c (the C restatement)."""
+
+    def __init__(self, path: str = ORION_ORACLE_LIB):
+        L = self.lib = ctypes.CDLL(path)
+        L.oracle_sha256_64.argtypes = [ctypes.c_char_p, _V]
+        L.oracle_glibc_stream.argtypes = [ctypes.c_uint32, _I, _V]
+        L.oracle_encode_len.argtypes = [_LL]
+        L.oracle_encode_len.restype = _LL
+        L.oracle_orion_commit.argtypes = [_V, _LL, _V, _V]
+        L.oracle_fft.argtypes = [_V, _LL, _LL, _V]
+        L.oracle_ifft.argtypes = [_V, _LL, _LL, _V]
+        L.oracle_rs_commit.argtypes = [_V, _I, _V, _V]
+        L.oracle_encode.argtypes = [_V, _LL, _V]
+        L.oracle_encode.restype = _LL
+
+    def sha256_64(self, msg: bytes) -> bytes:
+        assert len(msg) == 64
+        out = ctypes.create_string_buffer(32)
+        self.lib.oracle_sha256_64(msg, out)
+        return out.raw
+
+    def glibc_rand(self, seed: int, n: int) -> list:
+        out = (ctypes.c_int * n)()
+        self.lib.oracle_glibc_stream(seed, n, out)
+        return list(out)
+
+    def encode_len(self, n: int) -> int:
+        return self.lib.oracle_encode_len(n)
+
+    def encode(self, src: np.ndarray) -> np.ndarray:
+        n = src.size // 2
+        out = np.zeros(2 * self.encode_len(n), np.uint64)
+        assert self.lib.oracle_encode(_vp(src), n, _vp(out)) == out.size // 2
+        return out
+
+    def commit(self, src: np.ndarray, leaves: bool = False):
+        n = src.size // 2
+        root = ctypes.create_string_buffer(32)
+        lv = np.zeros(2 * (n // 128) * 32, np.uint8) if leaves else None
+        rc = self.lib.oracle_orion_commit(_vp(src), n, root, _vp(lv) if leaves else None)
+        if rc != 0:
+            raise ValueError("oracle_orion_commit: %d" % rc)
+        return (root.raw, lv.reshape(-1, 32)) if leaves else root.raw
+
+    def fft(self, coef: np.ndarray, order: int) -> np.ndarray:
+        out = np.zeros(2 * order, np.uint64)
+        assert self.lib.oracle_fft(_vp(coef), coef.size // 2, order, _vp(out)) == 0
+        return out
+
+    def ifft(self, evals: np.ndarray, coef_len: int) -> np.ndarray:
+        out = np.zeros(2 * coef_len, np.uint64)
+        assert self.lib.oracle_ifft(_vp(evals), coef_len, evals.size // 2, _vp(out)) == 0
+        return out
+
+    def rs_commit(self, src: np.ndarray, log_len: int, want_codeword: bool = False):
+        root = ctypes.create_string_buffer(32)
+        cw = np.zeros(2 << (log_len + 5), np.uint64) if want_codeword else None
+        rc = self.lib.oracle_rs_commit(_vp(src), log_len, root, _vp(cw) if want_codeword else None)
+        assert rc == 0
+        return (root.raw, cw) if want_codeword else root.raw

@@ -1,0 +1,107 @@
+"""The Orion oracle (oracle/orion_oracle.c) against the reference's own outputs.
+
+tests/golden/orion_golden.npz was produced by the reference sources
+(tests/golden/gen_orion_golden.py); these tests pin the C restatement to it so
+that the GPU tests may use the oracle as their checker. CPU only.
+"""
+import ctypes
+import hashlib
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from orionlib import ORION_ORACLE_LIB, P61, ROOT, OrionOracle, digest, elements
+
+KINDS = ["random", "zero", "max", "small"]
+
+
+@pytest.fixture(scope="module")
+def orc():
+    if not os.path.exists(ORION_ORACLE_LIB):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"])
+    return OrionOracle()
+
+
+@pytest.fixture(scope="module")
+def og():
+    return np.load(os.path.join(ROOT, "tests", "golden", "orion_golden.npz"))
+
+
+def test_sha256_matches_hashlib(orc):
+    rng = np.random.default_rng(0)
+    for msg in (bytes(64), bytes(range(64)), b"\xff" * 64, rng.bytes(64), rng.bytes(64)):
+        assert orc.sha256_64(msg) == hashlib.sha256(msg).digest()
+
+
+def test_glibc_rand_matches_libc(orc):
+    libc = ctypes.CDLL("libc.so.6")
+    for seed in (1, 2, 12345):
+        libc.srand(seed)
+        want = [libc.rand() for _ in range(2000)]
+        assert orc.glibc_rand(seed, 2000) == want
+
+
+def test_commit_roots(orc, og):
+    for k in og.files:
+        if not k.startswith("commit_"):
+            continue
+        name = k[len("commit_"):]
+        lg, seed, kind = (int(v) for v in og["commitcase_" + name])
+        root = orc.commit(elements(seed, 1 << lg, KINDS[kind]))
+        assert root == og[k].tobytes(), name
+
+
+def test_commit_root_hex_format(orc, og):
+    # root_hex (truepix_gkr.h) prints h0.hi, h0.lo, h1.hi, h1.lo as %016llx of
+    # the little-endian 64-bit words of the digest
+    root = og["commit_r13"].tobytes()
+    w = np.frombuffer(root, np.uint64)
+    hx = "%016x%016x%016x%016x" % (w[1], w[0], w[3], w[2])
+    assert hx.encode() == og["commithex_r13"].tobytes()
+
+
+def test_encode(orc, og):
+    for k in og.files:
+        if not k.startswith("encode_"):
+            continue
+        n = int(k.split("_")[1])
+        cw = orc.encode(elements(100 + n, n))
+        assert cw.size // 2 == int(og["encodelen_%d" % n][0]) == orc.encode_len(n)
+        assert digest(cw) == og[k].tobytes(), n
+    np.testing.assert_array_equal(orc.encode(elements(164, 64)), og["encodefull_64"])
+
+
+def test_fft_ifft(orc, og):
+    for k in og.files:
+        if not k.startswith("fft_"):
+            continue
+        m, o = (int(v) for v in k.split("_")[1:])
+        r = orc.fft(elements(200 + m + o, m), o)
+        assert digest(r) == og[k].tobytes(), (m, o)
+        ri = orc.ifft(elements(300 + m + o, o), m)
+        assert digest(ri) == og["ifft_%d_%d" % (m, o)].tobytes(), (m, o)
+
+
+def test_fft_then_ifft_is_identity(orc):
+    a = elements(9, 1 << 12)
+    np.testing.assert_array_equal(orc.ifft(orc.fft(a, 1 << 12), 1 << 12), a)
+    # evaluations on a larger domain sub-sample back to the coefficients
+    np.testing.assert_array_equal(orc.ifft(orc.fft(a, 1 << 15), 1 << 12), a)
+
+
+def test_rs_commit(orc, og):
+    for k in og.files:
+        if not k.startswith("rs_"):
+            continue
+        lg = int(k.split("_")[1])
+        root, cw = orc.rs_commit(elements(400 + lg, 1 << lg), lg, want_codeword=True)
+        assert digest(cw) == og["rscw_%d" % lg].tobytes(), lg
+        assert root == og[k].tobytes(), lg
+
+
+def test_elements_are_canonical():
+    for kind in KINDS:
+        e = elements(3, 1000, kind)
+        assert e.dtype == np.uint64 and e.size == 2000 and int(e.max()) < P61
