@@ -210,6 +210,87 @@ __device__ void cta_finish(const Job& J, fp2* red, int pairs, int pair0, int loc
     if (threadIdx.x == 0) *J.ticket = 0u;
 }
 
+// Epilogue of one warp: lane = claim pair p with 4-point values V (nearly
+// canonical). Adds K0 (group 0), multiplies by beta at the four points (beta is
+// folded by r first for fold kinds; group 0 stores the folded pair), sums over
+// the warp. CTA level: the 8 warp sums go through shared memory to one partial
+// per CTA; the job's last CTA (ticket) writes the job's 8 u64.
+__device__ void warp_claim(const Job& J, fp2 (&V)[4], int p, bool live, int g, bool fold,
+                           fp2 (&acc)[4])
+{
+#pragma unroll
+    for (int t = 0; t < 4; ++t) acc[t] = f2zero();
+    if (live) {
+        fp2 b4[4];
+        if (fold) {
+            const fp2* q = J.beta + 4 * (size_t)p;
+            const fp2 b0 = l2fold(ld2(q), ld2(q + 1), J.r), b1 = l2fold(ld2(q + 2), ld2(q + 3), J.r);
+            if (g == 0) {
+                st2(J.beta_out + 2 * (size_t)p, b0);
+                st2(J.beta_out + 2 * (size_t)p + 1, b1);
+            }
+            four4(b0, b1, b4);
+        } else {
+            four4(ld2(J.beta + 2 * (size_t)p), ld2(J.beta + 2 * (size_t)p + 1), b4);
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const fp2 v = g == 0 ? l2add(V[t], J.K0) : V[t];
+            acc[t] = l2canon(l2mul(b4[t], v));
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t) acc[t] = warp_sum(acc[t]);
+}
+
+__device__ void cta_combine(const Job& J, const fp2 (&acc)[4], int local)
+{
+    __shared__ fp2 ws[kWarps][4];
+    __shared__ bool s_last;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) ws[warp][t] = acc[t];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        fp2 tot[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            tot[t] = ws[0][t];
+            for (int w = 1; w < kWarps; ++w) tot[t] = f2add(tot[t], ws[w][t]);
+            stcg2(J.partials + (size_t)local * 4 + t, tot[t]);
+        }
+        __threadfence();
+        const unsigned prev = atomicAdd(J.ticket, 1u);
+        s_last = (prev == (unsigned)(J.tiles * J.groups - 1));
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const int n = J.tiles * J.groups;
+    fp2 tot[4] = {f2zero(), f2zero(), f2zero(), f2zero()};
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) tot[t] = f2add(tot[t], ldcg2(J.partials + (size_t)i * 4 + t));
+#pragma unroll
+    for (int t = 0; t < 4; ++t) tot[t] = warp_sum(tot[t]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) ws[warp][t] = tot[t];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            fp2 v = ws[0][t];
+            for (int w = 1; w < kWarps; ++w) v = f2add(v, ws[w][t]);
+            J.out8[2 * t] = v.re;
+            J.out8[2 * t + 1] = v.im;
+        }
+        *J.ticket = 0u;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // kinds 0/1: table source. lane = claim pair, warp = slice of the group's rows
 template <bool FOLD>
@@ -312,89 +393,97 @@ __global__ void __launch_bounds__(kBT, 4) table_round_kernel(const Job* __restri
 }
 
 // ---------------------------------------------------------------------------
-// kind 2: claim over the frame bytes. lane = copy (pairs are lane pairs),
-// warp = slice of the group's byte words
-__global__ void __launch_bounds__(kBT) pix_claim_kernel(const Job* __restrict__ jobs)
+// byte rows: the 16 bytes of vector q of copy c (zero past n_real)
+__device__ __forceinline__ uint4 prow16(const Job& J, int c, int q)
+{
+    if (c >= J.n_real) return make_uint4(0, 0, 0, 0);
+    return __ldg(reinterpret_cast<const uint4*>(J.pix + (size_t)c * J.cs) + q);
+}
+__device__ __forceinline__ u32 vbyte(const uint4& v, int k)
+{
+    const u32 word = k < 8 ? (k < 4 ? v.x : v.y) : (k < 12 ? v.z : v.w);
+    return (word >> (8 * (k & 3))) & 0xFFu;
+}
+__device__ __forceinline__ u64 gval(const Job& J, int c, int w)
+{
+    if (c >= J.n_real) return 0;
+    if (w < J.cs) return J.pix[(size_t)c * J.cs + w];
+    return w == J.const_idx ? J.const_val : 0;
+}
+
+// kind 2: claim over the frame bytes. CTA = 256 claim pairs x one group of
+// 16-wire units; lane = pair (copies 2p, 2p+1 read with 16-byte loads).
+__global__ void __launch_bounds__(kBT, 4) pix_claim_kernel(const Job* __restrict__ jobs)
 {
     __shared__ __align__(16) Job J;
-    __shared__ __align__(16) fp2 red[kWarps * 32 * 4];
-    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ uint4 Ls[512];
     if (!load_job(jobs, J)) return;
     const int local = blockIdx.x;
     const int tile = local / J.groups, g = local - tile * J.groups;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cs = J.cs, pw = J.pw;
-    const int nw = (cs + 3) >> 2;
-    const int gw0 = g * J.wpg, gw1 = min(nw, gw0 + J.wpg);   // word range of the group
-    uint4* Ls = reinterpret_cast<uint4*>(dsm);                // [4 * wpg] wires of the group
-    u32* tile_w = reinterpret_cast<u32*>(Ls + 4 * J.wpg);     // [32][pw]
-    for (int i = threadIdx.x; i < 4 * (gw1 - gw0); i += blockDim.x) {
-        const int w = 4 * gw0 + i;
-        Ls[i] = w < cs ? split4b(ld2(J.L + w)) : make_uint4(0, 0, 0, 0);
-    }
-    const int c0 = tile * 32;
-    stage_rows(J, c0, 32, pw, tile_w);
+    const int cs = J.cs;
+    const int w0 = 16 * g * J.wpg, w1 = min(cs, w0 + 16 * J.wpg);
+    for (int w = w0 + threadIdx.x; w < w1; w += blockDim.x) Ls[w - w0] = split4b(ld2(J.L + w));
     __syncthreads();
-
-    const int c = c0 + lane;
-    const int per = (gw1 - gw0 + kWarps - 1) / kWarps;
-    const int j0 = gw0 + warp * per, j1 = min(gw1, j0 + per);
-    u64 A0 = 0, A1 = 0, A2 = 0, A3 = 0;
-    for (int j = j0; j < j1; ++j) {
-        const u32 v = tile_w[lane * pw + j];
+    const int p = tile * kBT + warp * 32 + lane;
+    const bool live = p < J.n_pairs;
+    const int ca = 2 * p, cb = ca + 1;
+    u64 A0 = 0, A1 = 0, A2 = 0, A3 = 0, B0 = 0, B1 = 0, B2 = 0, B3 = 0;
+    if (J.vec) {
+        for (int q = w0 >> 4; q < (w1 + 15) >> 4; ++q) {
+            const uint4 va = prow16(J, live ? ca : J.n_real, q);
+            const uint4 vb = prow16(J, live ? cb : J.n_real, q);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const u32 x = (v >> (8 * k)) & 0xFFu;
-            const uint4 l = Ls[4 * (j - gw0) + k];
-            A0 += (u64)l.x * x;
-            A1 += (u64)l.y * x;
-            A2 += (u64)l.z * x;
-            A3 += (u64)l.w * x;
+            for (int k = 0; k < 16; ++k) {
+                const u32 xa = vbyte(va, k), xb = vbyte(vb, k);
+                const uint4 l = Ls[16 * q + k - w0];
+                A0 += (u64)l.x * xa; A1 += (u64)l.y * xa; A2 += (u64)l.z * xa; A3 += (u64)l.w * xa;
+                B0 += (u64)l.x * xb; B1 += (u64)l.y * xb; B2 += (u64)l.z * xb; B3 += (u64)l.w * xb;
+            }
+        }
+    } else {
+        for (int w = w0; w < w1; ++w) {
+            const u32 xa = live ? (u32)gval(J, ca, w) : 0u, xb = live ? (u32)gval(J, cb, w) : 0u;
+            const uint4 l = Ls[w - w0];
+            A0 += (u64)l.x * xa; A1 += (u64)l.y * xa; A2 += (u64)l.z * xa; A3 += (u64)l.w * xa;
+            B0 += (u64)l.x * xb; B1 += (u64)l.y * xb; B2 += (u64)l.z * xb; B3 += (u64)l.w * xb;
         }
     }
-    fp2 S = mk(combine2(A0, A1), combine2(A2, A3));
-    if (g == 0 && warp == 0 && c < J.n_real && J.const_idx >= 0) S = l2add(S, J.Lc);
-
-    fp2 P[4] = {f2zero(), f2zero(), f2zero(), f2zero()};
-    const int tper = (J.tpg + kWarps - 1) / kWarps;
-    const int e0 = min(J.n_terms, g * J.tpg + warp * tper);
-    const int e1 = min(J.n_terms, min(g * J.tpg + J.tpg, e0 + tper));
-    if (e0 < e1) {
-        fp2 M = f2zero();
+    fp2 S0 = mk(combine2(A0, A1), combine2(A2, A3));
+    fp2 S1 = mk(combine2(B0, B1), combine2(B2, B3));
+    if (g == 0 && J.const_idx >= 0) {
+        if (ca < J.n_real) S0 = l2add(S0, J.Lc);
+        if (cb < J.n_real) S1 = l2add(S1, J.Lc);
+    }
+    fp2 V[4];
+    four4(S0, S1, V);
+    const int e0 = min(J.n_terms, g * J.tpg), e1 = min(J.n_terms, e0 + J.tpg);
+    if (e0 < e1 && live) {
+        fp2 M0 = f2zero(), M1 = f2zero();
         int cur_b = J.ab[e0].y;
         for (int e = e0; e <= e1; ++e) {
             if (e == e1 || J.ab[e].y != cur_b) {
-                const u64 xb = bval(J, tile_w, pw, lane, c, cur_b);
-                const fp2 Mo = partner2(M);
-                const u64 xbo = __shfl_xor_sync(0xffffffffu, xb, 1);
-                if ((lane & 1) == 0) {
-                    fp2 m4[4];
-                    four4(M, Mo, m4);
-                    const u64 x4[4] = {xb, xbo, lsub(xb + xb, xbo), lsub(xbo + xbo, xb)};
+                const u64 xb0 = gval(J, ca, cur_b), xb1 = gval(J, cb, cur_b);
+                fp2 m4[4];
+                four4(M0, M1, m4);
+                const u64 x4[4] = {xb0, xb1, lsub(xb0 + xb0, xb1), lsub(xb1 + xb1, xb0)};
 #pragma unroll
-                    for (int t = 0; t < 4; ++t)
-                        P[t] = l2add(P[t], mk(lmul(m4[t].re, x4[t]), lmul(m4[t].im, x4[t])));
-                }
-                M = f2zero();
+                for (int t = 0; t < 4; ++t)
+                    V[t] = l2add(V[t], mk(lmul(m4[t].re, x4[t]), lmul(m4[t].im, x4[t])));
+                M0 = M1 = f2zero();
                 if (e == e1) break;
                 cur_b = J.ab[e].y;
             }
             const fp2 cf = ld2(J.cf + e);
-            const u64 xa = bval(J, tile_w, pw, lane, c, J.ab[e].x);
-            M = l2add(M, mk(lmul(cf.re, xa), lmul(cf.im, xa)));
+            const int w = J.ab[e].x;
+            const u64 xa0 = gval(J, ca, w), xa1 = gval(J, cb, w);
+            M0 = l2add(M0, mk(lmul(cf.re, xa0), lmul(cf.im, xa0)));
+            M1 = l2add(M1, mk(lmul(cf.re, xa1), lmul(cf.im, xa1)));
         }
     }
-    const fp2 So = partner2(S);
-    if ((lane & 1) == 0) {
-        fp2 V[4];
-        four4(S, So, V);
-#pragma unroll
-        for (int t = 0; t < 4; ++t) red[((size_t)warp * 32 + (lane >> 1)) * 4 + t] = l2add(V[t], P[t]);
-    } else {
-#pragma unroll
-        for (int t = 0; t < 4; ++t) red[((size_t)warp * 32 + 16 + (lane >> 1)) * 4 + t] = f2zero();
-    }
-    cta_finish(J, red, 16, tile * 16, local, g, false, nullptr);
+    fp2 acc[4];
+    warp_claim(J, V, p, live, g, false, acc);
+    cta_combine(J, acc, local);
 }
 
 // ---------------------------------------------------------------------------
@@ -558,7 +647,6 @@ __global__ void __launch_bounds__(kBT) finish_kernel(const Job* __restrict__ job
     st2(J.fin + w, l2canon(v));
 }
 
-size_t pix_claim_smem(int wpg, int pw) { return 16 * 4 * (size_t)wpg + 4 * 32 * (size_t)pw; }
 size_t pix_fold_smem(int wpg, int pw)
 {
     return 32 * 4 * (size_t)wpg + 16 * 511 + 4 * 64 * (size_t)pw;
@@ -575,8 +663,6 @@ bool set_attrs()
 {
     if (g_attrs) return true;
     const int big = 160 * 1024;
-    TP_CUDA_OK(cudaFuncSetAttribute(pix_claim_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    big), "smem attr");
     TP_CUDA_OK(cudaFuncSetAttribute(pix_fold_claim_kernel,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, big), "smem attr");
     g_attrs = true;
@@ -590,24 +676,30 @@ bool set_attrs()
 
 void plan_job(Job& j, int target_ctas)
 {
-    const int kind = j.kind;
-    if (kind <= 1) {
+    if (j.kind <= 1) {
         j.tiles = (j.n_pairs + 31) / 32;
         int groups = std::max(1, (target_ctas + j.tiles - 1) / j.tiles);
         groups = std::min(groups, std::max(1, (j.W_rows + kWarps - 1) / kWarps));
         j.wpg = (j.W_rows + groups - 1) / groups;
         j.groups = (j.W_rows + j.wpg - 1) / j.wpg;
+    } else if (j.kind == 2) {
+        j.tiles = (j.n_pairs + kBT - 1) / kBT;   // 256 claim pairs per CTA
+        const int units = (j.cs + 15) / 16;      // 16-wire units
+        int groups = std::max(1, (target_ctas + j.tiles - 1) / j.tiles);
+        groups = std::min(groups, units);
+        j.wpg = (units + groups - 1) / groups;
+        j.groups = (units + j.wpg - 1) / j.wpg;
     } else {
-        const int copies = kind == 2 ? j.n_in : (j.n_in >> 1);
-        j.tiles = (copies + 31) / 32;
+        j.tiles = ((j.n_in >> 1) + 31) / 32;     // 32 output copies per CTA
         const int nw = (j.cs + 3) / 4;
         int groups = std::max(1, (target_ctas + j.tiles - 1) / j.tiles);
         groups = std::min(groups, std::max(1, (nw + kWarps - 1) / kWarps));
         j.wpg = (nw + groups - 1) / groups;
         j.groups = (nw + j.wpg - 1) / j.wpg;
-        j.pw = pad_words_b(j.cs);
     }
+    j.pw = pad_words_b(j.cs);
     j.tpg = j.n_terms ? (j.n_terms + j.groups - 1) / j.groups : 0;
+    j.vec = (j.kind >= 2 && (j.cs & 15) == 0 && (reinterpret_cast<size_t>(j.pix) & 15) == 0) ? 1 : 0;
 }
 
 bool launch_round(const Job* d_jobs, const std::vector<Job>& jobs, int kind, cudaStream_t s,
@@ -624,9 +716,8 @@ bool launch_round(const Job* d_jobs, const std::vector<Job>& jobs, int kind, cud
         table_round_kernel<true><<<grid, kBT, 0, s>>>(d_jobs);
     } else {
         size_t smem = 0;
-        for (const Job& j : jobs)
-            smem = std::max(smem, kind == 2 ? pix_claim_smem(j.wpg, j.pw) : pix_fold_smem(j.wpg, j.pw));
-        if (kind == 2) pix_claim_kernel<<<grid, kBT, smem, s>>>(d_jobs);
+        for (const Job& j : jobs) smem = std::max(smem, pix_fold_smem(j.wpg, j.pw));
+        if (kind == 2) pix_claim_kernel<<<grid, kBT, 0, s>>>(d_jobs);
         else pix_fold_claim_kernel<<<grid, kBT, smem, s>>>(d_jobs);
     }
     ++*launches;

@@ -136,7 +136,8 @@ struct Job {
     int n_pairs;            // claim pairs
     int W, W_rows;
     int n_real, cs, const_idx;
-    int n_terms, tiles, groups, wpg, tpg, pw, cta0, pad_;
+    int n_terms, tiles, groups, wpg, tpg, pw, cta0;
+    int vec;                // byte rows are whole 16-byte vectors (copy_size % 16 == 0, aligned)
 };
 
 void plan_job(Job& j, int target_ctas);

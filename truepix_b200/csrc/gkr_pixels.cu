@@ -240,7 +240,7 @@ bool launch_mle_pixels_batch(const MleFrame* h_frames, int n, int n_pad, int cs,
 
 bool pixsrc_valid(const PixSrc& px, int n_pad, int W)
 {
-    if (!px.pix || px.n_real < 0 || px.n_real > n_pad || px.cs <= 0 || px.cs > W || W > 4096 ||
+    if (!px.pix || px.n_real < 0 || px.n_real > n_pad || px.cs <= 0 || px.cs > W || px.cs > 512 ||
         px.const_idx >= W || (px.const_idx >= 0 && px.const_idx < px.cs) || px.const_val >= P61) {
         set_error(TP_ERR_ARG, "pixel layout: copies %d/%d, copy_size %d, wires %d, const %d",
                   px.n_real, n_pad, px.cs, W, px.const_idx);
