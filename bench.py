@@ -212,9 +212,10 @@ def peaks():
 
 
 def profiled_traffic():
-    """DRAM bytes per fold+claim launch of the 1080p round 1, from the committed
-    ncu summary (profiles/claim_kernel_fold_1080p.json), scaled like `achieved`."""
-    p = os.path.join(ROOT, "profiles", "claim_kernel_fold_1080p.json")
+    """DRAM bytes (read + write) per launch of each round kernel of the 64-frame
+    1080p step, from the committed ncu summary (profiles/gkr_batch_1080p_traffic.json;
+    measured at 4 frames per launch and scaled by the frames per launch)."""
+    p = os.path.join(ROOT, "profiles", "gkr_batch_1080p_traffic.json")
     if os.path.exists(p):
         try:
             return json.load(open(p))
