@@ -1,0 +1,68 @@
+/*
+ * Orion input-layer commitment on the GPU (libnative_fp2_gpu.so).
+ *
+ * The reference runs these steps on the CPU inside its Orion binaries
+ * (TruePix-main/Orion/Orion_nonzk, driven by examples/multivariate_PC_test_*.cpp
+ * through `linearPC_multi_{commit,prove,open}`); a rebuilt driver calls the
+ * entry points below instead. Field elements are 16 bytes in the reference's
+ * memory order (u64 img, then u64 real; include/linear_gkr/prime_field.h),
+ * canonical in [0, 2^61 - 1). Digests are 32 bytes exactly as __hhash_digest
+ * stores them (the SHA-256 output bytes).
+ *
+ * Return value: 0 on success, -1 on failure with tp_last_error_code() /
+ * tp_last_error() set (native_fp2.h). Host-buffer entry points run on the
+ * library stream and return when their outputs are written; *_dev entry points
+ * take device pointers and a cudaStream_t (NULL = the CUDA default stream) and
+ * return once the work is queued.
+ */
+#ifndef TRUEPIX_B200_ORION_GPU_H
+#define TRUEPIX_B200_ORION_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* encode_output_len(col_len): codeword length of one column
+ * (include/linear_code/linear_code_encode.h:8-15 after expander_init(col_len),
+ * include/linear_code/expanders.h:47-60). */
+long long tp_orion_codeword_len(long long col_len);
+
+/* Merkle leaves after padding for an N-element commit: the power of two >=
+ * 2 * N / 128 (merkle_tree.cpp:30-32); the tree holds 2 * leaves digests. */
+long long tp_orion_tree_leaves(long long N);
+
+/* Replaces commit(src, N) (src/VPD/linearPC.cpp:97-197) with the encoder state of
+ * expander_init(N / 128) drawn from glibc rand() in its unseeded state, as the
+ * reference's drivers do. src: N elements, column c = src[c * N/128 ...].
+ * tree_out: 2 * tp_orion_tree_leaves(N) digests, heap order (root at index 1,
+ * index 0 zero) -- the array commit() returns. codeword_out: NULL, or
+ * 128 * tp_orion_codeword_len(N/128) elements, column-major like the reference's
+ * encoded_codeword[c][r] when set_retain_encoded_codeword(true). N % 128 == 0,
+ * N / 128 <= 2^22. */
+int tp_orion_commit(const uint64_t* src, long long N, unsigned char* tree_out, uint64_t* codeword_out);
+
+/* Device form of tp_orion_commit. d_src: N elements, column-major as above.
+ * d_rows: scratch and output, cw_len x 128 elements, ROW-major (row r holds
+ * element r of every column). d_tree: 2 * tp_orion_tree_leaves(N) digests. */
+int tp_orion_commit_dev(const void* d_src, long long N, void* d_rows, void* d_tree, void* stream);
+
+/* Commit of a frame read from its uint8 bytes in TruePix's layout
+ * (include/truepix/truepix_gkr.h:107-206: element copy * n_wires + wire is
+ * pixel[copy * copy_size + wire] for wire < copy_size, const_val at const_idx,
+ * zero elsewhere and for copies >= n_copies). N = n_copies_padded * n_wires.
+ * No N-element input vector is materialised. */
+int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size,
+                               int n_wires, int const_idx, uint64_t const_val, void* d_rows,
+                               void* d_tree, void* stream);
+
+/* Row-major codeword (as written by the commits above) -> column-major
+ * (encoded_codeword[c][r]); d_cols holds 128 * cw_len elements. */
+int tp_orion_rows_to_columns_dev(const void* d_rows, long long cw_len, void* d_cols, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -6,7 +6,8 @@ harness oracle/orion_ref_harness.cpp), on seeded inputs (tests/orionlib.py
 `elements`, splitmix64-based) and stores the outputs in
 tests/golden/orion_golden.npz:
 
-  commit_<case>   32-byte Merkle roots of the Orion commit (linearPC.cpp:97-197)
+  commit_<case>   32-byte Merkle roots of the Orion commit (linearPC.cpp:97-197),
+                  incl. one 1080p frame in TruePix's layout (frameroot_1080)
   encode_<n>      SHA-256 digest of the expander codeword of one column
                   (linear_code_encode.h:17-72); full codeword for n = 64
   fft_<m>_<o>     digest of P(w^i), i < o, for m seeded coefficients
@@ -33,15 +34,20 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
-from orionlib import ORION_REF_LIB, digest, elements  # noqa: E402
+from orionlib import ORION_REF_LIB, digest, elements, frame_bytes, frame_elements  # noqa: E402
 
 V = ctypes.c_void_p
 
-COMMIT_CASES = [  # (name, log2 N, seed, kind)
-    ("r13", 13, 1, "random"), ("zero13", 13, 0, "zero"), ("max13", 13, 0, "max"),
-    ("small14", 14, 7, "small"), ("r14", 14, 2, "random"), ("r15", 15, 3, "random"),
-    ("r16", 16, 4, "random"), ("r18", 18, 5, "random"), ("r20", 20, 6, "random"),
+COMMIT_CASES = [  # (name, N, seed, kind)
+    ("r13", 1 << 13, 1, "random"), ("zero13", 1 << 13, 0, "zero"), ("max13", 1 << 13, 0, "max"),
+    ("small14", 1 << 14, 7, "small"), ("r14", 1 << 14, 2, "random"), ("r15", 1 << 15, 3, "random"),
+    ("r16", 1 << 16, 4, "random"), ("r18", 1 << 18, 5, "random"), ("r20", 1 << 20, 6, "random"),
+    ("c100", 128 * 100, 8, "random"), ("c13", 128 * 13, 9, "random"), ("c1", 128, 10, "random"),
+    ("c1000", 128 * 1000, 11, "random"),
 ]
+# one 1080p frame (TruePix layout: 16,200 copies of 384 bytes, gray constant 128
+# at wire 384, 512 wires, padded to 16,384 copies -> N = 2^23)
+FRAME = dict(copies=16200, cs=384, W=512, const_idx=384, const_val=128, padded=16384, seed=12)
 ENCODE_CASES = [1, 13, 14, 64, 100, 1000, 8192, 65536]
 FFT_CASES = [(1, 1), (1, 8), (2, 2), (8, 8), (4, 16), (16, 256), (1024, 1024), (256, 4096),
              (1 << 12, 1 << 17), (1 << 16, 1 << 16), (1 << 20, 1 << 20)]
@@ -61,12 +67,21 @@ def _ref():
 
 
 def _commit(args):
-    lg, seed, kind = args
-    src = elements(seed, 1 << lg, kind)
+    n, seed, kind = args
+    src = elements(seed, n, kind)
     root = ctypes.create_string_buffer(32)
     hx = ctypes.create_string_buffer(80)
-    _ref().ref_commit(V(src.ctypes.data), 1 << lg, root, hx)
+    _ref().ref_commit(V(src.ctypes.data), n, root, hx)
     return root.raw, hx.value
+
+
+def _commit_frame(_):
+    src = frame_elements(frame_bytes(FRAME["seed"], FRAME["copies"] * FRAME["cs"]), **{
+        k: FRAME[k] for k in ("copies", "cs", "W", "const_idx", "const_val", "padded")})
+    root = ctypes.create_string_buffer(32)
+    hx = ctypes.create_string_buffer(80)
+    _ref().ref_commit(V(src.ctypes.data), src.size // 2, root, hx)
+    return root.raw
 
 
 def _encode(n):
@@ -105,11 +120,14 @@ def main():
     ctx = mp.get_context("spawn")
     out = {}
     with ctx.Pool(8, maxtasksperchild=1) as pool:
-        for (name, lg, seed, kind), (root, hx) in zip(
+        for (name, n, seed, kind), (root, hx) in zip(
                 COMMIT_CASES, pool.map(_commit, [c[1:] for c in COMMIT_CASES], chunksize=1)):
             out["commit_" + name] = np.frombuffer(root, np.uint8)
             out["commithex_" + name] = np.frombuffer(hx, np.uint8)
-            out["commitcase_" + name] = np.array([lg, seed, ["random", "zero", "max", "small"].index(kind)])
+            out["commitcase_" + name] = np.array([n, seed, ["random", "zero", "max", "small"].index(kind)])
+        out["frameroot_1080"] = np.frombuffer(pool.apply(_commit_frame, (0,)), np.uint8)
+        out["frame1080"] = np.array([FRAME[k] for k in ("copies", "cs", "W", "const_idx", "const_val",
+                                                         "padded", "seed")])
         for n, cw in zip(ENCODE_CASES, pool.map(_encode, ENCODE_CASES, chunksize=1)):
             out["encode_%d" % n] = np.frombuffer(digest(cw), np.uint8)
             out["encodelen_%d" % n] = np.array([cw.size // 2])

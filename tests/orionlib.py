@@ -47,6 +47,26 @@ def elements(seed: int, n: int, kind: str = "random") -> np.ndarray:
     return (v >> np.uint64(3)) % np.uint64(P61)
 
 
+def frame_bytes(seed: int, n: int) -> np.ndarray:
+    """n seeded uniform bytes (splitmix64 of seed:index)."""
+    idx = np.arange((n + 7) // 8, dtype=np.uint64) + (np.uint64(seed) << np.uint64(40))
+    return splitmix64(idx).view(np.uint8)[:n].copy()
+
+
+def frame_elements(pix: np.ndarray, copies: int, cs: int, W: int, const_idx: int, const_val: int,
+                   padded: int) -> np.ndarray:
+    """The commit input of a frame (include/truepix/truepix_gkr.h:154-206): element
+    copy * W + wire = pixel for wire < cs, const_val at const_idx, zero elsewhere;
+    real part only (img 0)."""
+    v = np.zeros((padded, W), np.uint64)
+    v[:copies, :cs] = pix.reshape(copies, cs)
+    if const_idx >= 0:
+        v[:copies, const_idx] = const_val
+    out = np.zeros(2 * padded * W, np.uint64)
+    out[1::2] = v.reshape(-1)
+    return out
+
+
 def digest(a: np.ndarray) -> bytes:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest()
 

@@ -175,3 +175,17 @@ def test_bridge_without_device_fails_loudly():
         br.compute_beta([1, 2, 3])
     with pytest.raises(RuntimeError):
         br.early_session_create([12], [0], [0], [1], 2, 1, [[1, 2]], [1, 1])
+
+
+def test_orion_sizes_without_device():
+    """tp_orion_codeword_len / tp_orion_tree_leaves are host arithmetic: they
+    match the oracle's encode_output_len and the tree padding with no GPU."""
+    from orionlib import OrionOracle
+    from truepix_b200 import native
+    lib = native.gkr(require_device=False)
+    orc = OrionOracle()
+    for n in (1, 2, 13, 14, 64, 100, 1000, 8192, 65536, 1 << 18):
+        assert lib.tp_orion_codeword_len(n) == orc.encode_len(n), n
+    assert lib.tp_orion_tree_leaves(128 * 100) == 256
+    assert lib.tp_orion_tree_leaves(1 << 23) == 1 << 17
+    assert lib.tp_orion_tree_leaves(100) == 0

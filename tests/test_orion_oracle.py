@@ -48,8 +48,8 @@ def test_commit_roots(orc, og):
         if not k.startswith("commit_"):
             continue
         name = k[len("commit_"):]
-        lg, seed, kind = (int(v) for v in og["commitcase_" + name])
-        root = orc.commit(elements(seed, 1 << lg, KINDS[kind]))
+        n, seed, kind = (int(v) for v in og["commitcase_" + name])
+        root = orc.commit(elements(seed, n, KINDS[kind]))
         assert root == og[k].tobytes(), name
 
 
@@ -105,3 +105,11 @@ def test_elements_are_canonical():
     for kind in KINDS:
         e = elements(3, 1000, kind)
         assert e.dtype == np.uint64 and e.size == 2000 and int(e.max()) < P61
+
+
+def test_commit_root_of_a_1080p_frame(orc, og):
+    from orionlib import frame_bytes, frame_elements
+    copies, cs, W, ci, cv, padded, seed = (int(x) for x in og["frame1080"])
+    src = frame_elements(frame_bytes(seed, copies * cs), copies, cs, W, ci, cv, padded)
+    assert src.size == 2 << 23
+    assert orc.commit(src) == og["frameroot_1080"].tobytes()

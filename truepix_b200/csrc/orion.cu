@@ -1,0 +1,534 @@
+// Orion commit on the device: expander encode (gathers over target-sorted
+// graphs) and the SHA-256 Merkle tree. See orion.h for the layout.
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "fp2.cuh"
+#include "orion.h"
+#include "runtime.h"
+#include "sha256.cuh"
+
+namespace tp {
+namespace orion {
+
+namespace {
+
+thread_local int g_launches = 0;
+
+// glibc rand(): the TYPE_3 additive generator (degree 31, separation 3) that
+// glibc uses by default. Seeded like srand(seed): r[0] = seed, r[i] = 16807 *
+// r[i-1] mod (2^31 - 1) for i < 31, r[31..33] = r[0..2], then 310 outputs are
+// discarded; each output is o[i] = o[i-31] + o[i-3] (mod 2^32), returned >> 1.
+// The reference never seeds it, so its stream is that of seed 1.
+class GlibcRand {
+public:
+    explicit GlibcRand(uint32_t seed)
+    {
+        int64_t v = seed;
+        s_[0] = (uint32_t)v;
+        for (int i = 1; i < 31; ++i) {
+            v = (16807 * v) % 2147483647;
+            if (v < 0) v += 2147483647;
+            s_[i] = (uint32_t)v;
+        }
+        for (int i = 31; i < 34; ++i) s_[i] = s_[i - 31];
+        pos_ = 34;
+        for (int i = 0; i < 310; ++i) step();
+    }
+    int next() { return (int)(step() >> 1); }
+
+private:
+    uint32_t step()
+    {
+        const uint32_t o = s_[(pos_ - 31) % 34] + s_[(pos_ - 3) % 34];
+        s_[pos_ % 34] = o;
+        ++pos_;
+        return o;
+    }
+    uint32_t s_[34];
+    long long pos_;
+};
+
+long long c_targets(long long n) { return (long long)(0.238 * (double)n); }
+long long d_targets(long long n, long long L) { return (long long)((double)n * (1.72 - 1) - (double)L); }
+
+// encode_output_len (linear_code_encode.h:8-15) with D[dep].R from expander_init
+long long cw_len_rec(long long n)
+{
+    if (n <= kThreshold) return n;
+    const long long L = cw_len_rec(c_targets(n));
+    return n + L + d_targets(n, L);
+}
+
+struct HostGraph {
+    long long L, R;
+    std::vector<unsigned> ptr;       // R + 1
+    std::vector<unsigned> src;       // edges, grouped by target
+    std::vector<ulonglong2> w;
+};
+
+// generate_random_expander (expanders.h:19-45): for each source i, d draws of
+// (target = rand() % R, weight = (real rand() % p, img rand() % p)); stored by target
+HostGraph gen_graph(GlibcRand& g, long long L, long long R, int d)
+{
+    HostGraph h;
+    h.L = L;
+    h.R = R;
+    std::vector<unsigned> tgt((size_t)(L * d));
+    std::vector<ulonglong2> wt((size_t)(L * d));
+    std::vector<unsigned> cnt((size_t)R + 1, 0);
+    for (long long i = 0; i < L; ++i)
+        for (int j = 0; j < d; ++j) {
+            const long long t = (long long)g.next() % R;
+            const uint64_t re = (uint64_t)g.next() % P61;
+            const uint64_t im = (uint64_t)g.next() % P61;
+            tgt[(size_t)(i * d + j)] = (unsigned)t;
+            wt[(size_t)(i * d + j)] = make_ulonglong2(im, re);
+            cnt[(size_t)t + 1]++;
+        }
+    h.ptr.assign((size_t)R + 1, 0);
+    for (long long t = 0; t < R; ++t) h.ptr[(size_t)t + 1] = h.ptr[(size_t)t] + cnt[(size_t)t + 1];
+    h.src.resize((size_t)(L * d));
+    h.w.resize((size_t)(L * d));
+    std::vector<unsigned> fill(h.ptr.begin(), h.ptr.end() - 1);
+    for (long long i = 0; i < L; ++i)
+        for (int j = 0; j < d; ++j) {
+            const unsigned t = tgt[(size_t)(i * d + j)];
+            const unsigned e = fill[t]++;
+            h.src[e] = (unsigned)i;
+            h.w[e] = wt[(size_t)(i * d + j)];
+        }
+    return h;
+}
+
+// expander_init (expanders.h:47-60): C[dep], recurse, D[dep]
+long long init_rec(GlibcRand& g, long long n, int dep, std::vector<HostGraph>& C, std::vector<HostGraph>& D)
+{
+    if (n <= kThreshold) return n;
+    const long long R = c_targets(n);
+    C.push_back(gen_graph(g, n, R, kCDegree));
+    const long long L = init_rec(g, R, dep + 1, C, D);
+    const long long RD = d_targets(n, L);
+    HostGraph dg = gen_graph(g, L, RD, kDDegree);
+    if ((long long)D.size() <= dep) D.resize(dep + 1);
+    D[dep] = std::move(dg);
+    return n + L + RD;
+}
+
+std::mutex g_mu;
+std::map<std::pair<int, long long>, Encoder*> g_cache;
+
+void state_to_bytes(const uint32_t st[8], unsigned char out[32])
+{
+    for (int i = 0; i < 8; ++i) {
+        out[4 * i] = (unsigned char)(st[i] >> 24);
+        out[4 * i + 1] = (unsigned char)(st[i] >> 16);
+        out[4 * i + 2] = (unsigned char)(st[i] >> 8);
+        out[4 * i + 3] = (unsigned char)st[i];
+    }
+}
+
+// ---- kernels --------------------------------------------------------------
+
+__device__ __forceinline__ ulonglong2 ldg16(const ulonglong2* p) { return __ldg(p); }
+
+__device__ __forceinline__ fp2 as_fp2(ulonglong2 v) { return mk(v.y, v.x); }   // {img, real}
+__device__ __forceinline__ ulonglong2 from_fp2(fp2 a) { return make_ulonglong2(a.im, a.re); }
+
+// out[c][r] = in[r][c] for in [n_r][n_c] (16-byte elements), 32 x 32 tiles,
+// one tile per CTA in a 1-D grid
+__global__ void __launch_bounds__(256) transpose_kernel(const ulonglong2* __restrict__ in,
+                                                        ulonglong2* __restrict__ out,
+                                                        long long n_r, long long n_c)
+{
+    __shared__ ulonglong2 tile[32][33];
+    const long long tiles_c = (n_c + 31) / 32;
+    const long long r0 = ((long long)blockIdx.x / tiles_c) * 32, c0 = ((long long)blockIdx.x % tiles_c) * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const long long r = r0 + ty + k, c = c0 + tx;
+        if (r < n_r && c < n_c) tile[ty + k][tx] = ldg16(in + r * n_c + c);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const long long c = c0 + ty + k, r = r0 + tx;
+        if (r < n_r && c < n_c) out[c * n_r + r] = tile[tx][ty + k];
+    }
+}
+
+// rows[r][c] = input element c * col_len + r of a frame (PixelInput layout)
+__global__ void __launch_bounds__(256) pixel_rows_kernel(PixelInput px, long long col_len, int w_shift,
+                                                         ulonglong2* __restrict__ rows)
+{
+    const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (i >= col_len * kColumns) return;
+    const long long r = i >> 7, c = i & 127;
+    const long long f = c * col_len + r;
+    const long long copy = f >> w_shift;
+    const int wire = (int)(f & ((1LL << w_shift) - 1));
+    uint64_t v = 0;
+    if (copy < px.copies) {
+        if (wire < px.cs)
+            v = px.pix[copy * px.cs + wire];
+        else if (wire == px.const_idx)
+            v = px.const_val;
+    }
+    rows[i] = make_ulonglong2(0, v);
+}
+
+// One warp per target row t of a graph: rows[dst + t][c] = sum over in-edges
+// (s, w) of w * rows[src + s][c]. Lane l owns columns l, l + 32, l + 64, l + 96
+// (each edge reads one 2 KB row, 512 contiguous bytes per load instruction).
+// Edge metadata is read 32 at a time, one edge per lane, and broadcast.
+__global__ void __launch_bounds__(256) gather_kernel(ulonglong2* __restrict__ rows, long long src_row,
+                                                     long long dst_row, long long n_targets,
+                                                     const unsigned* __restrict__ ptr,
+                                                     const unsigned* __restrict__ esrc,
+                                                     const ulonglong2* __restrict__ ew)
+{
+    const long long t = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (t >= n_targets) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned e0 = ptr[t], e1 = ptr[t + 1];
+    const ulonglong2* src = rows + src_row * kColumns + lane;
+    fp2 acc[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc[k] = f2zero();
+    for (unsigned eb = e0; eb < e1; eb += 32) {
+        const int cnt = (int)min(32u, e1 - eb);
+        unsigned my_s = 0;
+        ulonglong2 my_w = make_ulonglong2(0, 0);
+        if (lane < cnt) {
+            my_s = esrc[eb + lane];
+            my_w = ew[eb + lane];
+        }
+        int j = 0;
+        for (; j + 2 <= cnt; j += 2) {
+            const unsigned s0 = __shfl_sync(0xffffffffu, my_s, j);
+            const unsigned s1 = __shfl_sync(0xffffffffu, my_s, j + 1);
+            const fp2 w0 = mk(__shfl_sync(0xffffffffu, my_w.y, j), __shfl_sync(0xffffffffu, my_w.x, j));
+            const fp2 w1 = mk(__shfl_sync(0xffffffffu, my_w.y, j + 1), __shfl_sync(0xffffffffu, my_w.x, j + 1));
+            const ulonglong2* p0 = src + (long long)s0 * kColumns;
+            const ulonglong2* p1 = src + (long long)s1 * kColumns;
+            ulonglong2 v0[4], v1[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                v0[k] = ldg16(p0 + 32 * k);
+                v1[k] = ldg16(p1 + 32 * k);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                acc[k] = l2add(acc[k], l2mul(w0, as_fp2(v0[k])));
+                acc[k] = l2add(acc[k], l2mul(w1, as_fp2(v1[k])));
+            }
+        }
+        if (j < cnt) {
+            const unsigned s0 = __shfl_sync(0xffffffffu, my_s, j);
+            const fp2 w0 = mk(__shfl_sync(0xffffffffu, my_w.y, j), __shfl_sync(0xffffffffu, my_w.x, j));
+            const ulonglong2* p0 = src + (long long)s0 * kColumns;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[k] = l2add(acc[k], l2mul(w0, as_fp2(ldg16(p0 + 32 * k))));
+        }
+    }
+    ulonglong2* dst = rows + (dst_row + t) * kColumns + lane;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dst[32 * k] = from_fp2(l2canon(acc[k]));
+}
+
+constexpr int kLeafRows = 128;     // rows (threads) per CTA
+constexpr int kLeafPairs = 4;      // column pairs staged per chunk
+
+__device__ __forceinline__ void store_digest(unsigned char* tree, long long node, const uint32_t st[8])
+{
+    uint4 a, b;
+    a.x = sha::bswap32(st[0]); a.y = sha::bswap32(st[1]); a.z = sha::bswap32(st[2]); a.w = sha::bswap32(st[3]);
+    b.x = sha::bswap32(st[4]); b.y = sha::bswap32(st[5]); b.z = sha::bswap32(st[6]); b.w = sha::bswap32(st[7]);
+    uint4* p = reinterpret_cast<uint4*>(tree + node * 32);
+    p[0] = a;
+    p[1] = b;
+}
+
+__device__ __forceinline__ void load_digest(const unsigned char* tree, long long node, uint32_t* w)
+{
+    const uint4* p = reinterpret_cast<const uint4*>(tree + node * 32);
+    const uint4 a = p[0], b = p[1];
+    w[0] = sha::bswap32(a.x); w[1] = sha::bswap32(a.y); w[2] = sha::bswap32(a.z); w[3] = sha::bswap32(a.w);
+    w[4] = sha::bswap32(b.x); w[5] = sha::bswap32(b.y); w[6] = sha::bswap32(b.z); w[7] = sha::bswap32(b.w);
+}
+
+// Row leaves (linearPC.cpp:61-95,145-168): for row r < cw_len,
+// h <- SHA256(h || rows[r][2j] || rows[r][2j+1]) for j = 0..63 from h = 0.
+// One thread per row; the CTA stages 128 rows x 8 columns (padded to 9, so
+// that 16-byte reads of consecutive rows fall in distinct banks) at a time.
+__global__ void __launch_bounds__(kLeafRows) leaf_kernel(const ulonglong2* __restrict__ rows, long long cw_len,
+                                                         unsigned char* __restrict__ tree, long long leaf0)
+{
+    __shared__ ulonglong2 tile[kLeafRows][2 * kLeafPairs + 1];
+    const long long r0 = (long long)blockIdx.x * kLeafRows;
+    const int tid = threadIdx.x;
+    uint32_t st[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) st[i] = 0;
+    for (int pair = 0; pair < kColumns / 2; pair += kLeafPairs) {
+#pragma unroll
+        for (int k = 0; k < 2 * kLeafPairs; ++k) {
+            const int i = tid + k * kLeafRows;
+            const int rr = i >> 3, cc = i & 7;
+            const long long r = r0 + rr;
+            tile[rr][cc] = r < cw_len ? ldg16(rows + r * kColumns + 2 * pair + cc) : make_ulonglong2(0, 0);
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int p = 0; p < kLeafPairs; ++p) {
+            uint32_t w[16];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) w[i] = st[i];
+            const ulonglong2 x = tile[tid][2 * p], y = tile[tid][2 * p + 1];
+            sha::fe_words(x.x, x.y, w + 8);
+            sha::fe_words(y.x, y.y, w + 12);
+            sha::hash64(w, st);
+        }
+        __syncthreads();
+    }
+    if (r0 + tid < cw_len) store_digest(tree, leaf0 + r0 + tid, st);
+}
+
+// tree[leaf0 + i] for i in [from, to): `a` below `split`, `b` from there on
+__global__ void fill_leaves_kernel(unsigned char* __restrict__ tree, long long leaf0, long long from,
+                                   long long split, long long to, ulonglong2 a0, ulonglong2 a1,
+                                   ulonglong2 b0, ulonglong2 b1)
+{
+    const long long i = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= to) return;
+    ulonglong2* p = reinterpret_cast<ulonglong2*>(tree + (leaf0 + i) * 32);
+    p[0] = i < split ? a0 : b0;
+    p[1] = i < split ? a1 : b1;
+}
+
+// `levels` tree levels above the n_in nodes at heap positions [n_in, 2 n_in):
+// CTA b reduces the 2^levels nodes from n_in + b * 2^levels to one node
+// (merkle_tree.cpp:64-83: node k = SHA256(node 2k || node 2k + 1)).
+__global__ void __launch_bounds__(256) tree_kernel(unsigned char* __restrict__ tree, long long n_in, int levels)
+{
+    __shared__ uint32_t s[256][9];
+    const int t = threadIdx.x;
+    long long base = n_in + ((long long)blockIdx.x << levels);   // first child of this level
+    int cnt = 1 << (levels - 1);                                  // parents at this level
+    uint32_t st[8];
+    if (t < cnt) {
+        uint32_t w[16];
+        load_digest(tree, base + 2 * t, w);
+        load_digest(tree, base + 2 * t + 1, w + 8);
+        sha::hash64(w, st);
+        store_digest(tree, (base >> 1) + t, st);
+    }
+    for (int lv = 1; lv < levels; ++lv) {
+        if (t < cnt) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) s[t][i] = st[i];
+        }
+        __syncthreads();
+        base >>= 1;
+        cnt >>= 1;
+        if (t < cnt) {
+            uint32_t w[16];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                w[i] = s[2 * t][i];
+                w[8 + i] = s[2 * t + 1][i];
+            }
+            sha::hash64(w, st);
+            store_digest(tree, (base >> 1) + t, st);
+        }
+        __syncthreads();
+    }
+}
+
+bool launch_ok(const char* what)
+{
+    ++g_launches;
+    return !cuda_failed(cudaGetLastError(), what);
+}
+
+}  // namespace
+
+long long codeword_len(long long col_len) { return cw_len_rec(col_len); }
+
+long long tree_leaves(long long col_len)
+{
+    long long s = 1;
+    while (s < 2 * col_len) s *= 2;
+    return s;
+}
+
+void zero_row_leaf(unsigned char out[32])
+{
+    uint32_t st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = 0; j < kColumns / 2; ++j) {
+        uint32_t w[16];
+        for (int i = 0; i < 8; ++i) w[i] = st[i];
+        for (int i = 8; i < 16; ++i) w[i] = 0;
+        sha::hash64(w, st);
+    }
+    state_to_bytes(st, out);
+}
+
+void zero_block_hash(unsigned char out[32])
+{
+    uint32_t w[16] = {0}, st[8];
+    sha::hash64(w, st);
+    state_to_bytes(st, out);
+}
+
+const Encoder* encoder(long long col_len)
+{
+    Ctx* c = ctx();
+    if (!c) return nullptr;
+    if (col_len < 1 || col_len > (1LL << 26)) {
+        set_error(TP_ERR_ARG, "orion: column length %lld out of range [1, 2^26]", col_len);
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto key = std::make_pair(c->device, col_len);
+    auto it = g_cache.find(key);
+    if (it != g_cache.end()) return it->second;
+
+    GlibcRand g(1);
+    std::vector<HostGraph> C, D;
+    const long long cw = init_rec(g, col_len, 0, C, D);
+    Encoder* e = new Encoder();
+    e->device = c->device;
+    e->col_len = col_len;
+    e->cw_len = cw;
+    std::vector<unsigned> ptr, src;
+    std::vector<ulonglong2> w;
+    long long off = 0, n = col_len;
+    for (size_t k = 0; k < C.size(); ++k) {
+        Level lv;
+        lv.n = n;
+        lv.R = C[k].R;
+        lv.L = D[k].L;
+        lv.RD = D[k].R;
+        lv.off = off;
+        lv.c_ptr = (long long)ptr.size();
+        lv.c_edge = (long long)src.size();
+        ptr.insert(ptr.end(), C[k].ptr.begin(), C[k].ptr.end());
+        src.insert(src.end(), C[k].src.begin(), C[k].src.end());
+        w.insert(w.end(), C[k].w.begin(), C[k].w.end());
+        lv.d_ptr = (long long)ptr.size();
+        lv.d_edge = (long long)src.size();
+        ptr.insert(ptr.end(), D[k].ptr.begin(), D[k].ptr.end());
+        src.insert(src.end(), D[k].src.begin(), D[k].src.end());
+        w.insert(w.end(), D[k].w.begin(), D[k].w.end());
+        e->levels.push_back(lv);
+        off += n;
+        n = lv.R;
+    }
+    e->n_ptr = (long long)ptr.size();
+    e->n_edges = (long long)src.size();
+    bool ok = true;
+    if (e->n_ptr) ok = !cuda_failed(cudaMalloc(&e->d_ptr, sizeof(unsigned) * ptr.size()), "orion graph alloc");
+    if (ok && e->n_edges) {
+        ok = !cuda_failed(cudaMalloc(&e->d_src, sizeof(unsigned) * src.size()), "orion graph alloc") &&
+             !cuda_failed(cudaMalloc(&e->d_w, sizeof(ulonglong2) * w.size()), "orion graph alloc");
+    }
+    if (ok && e->n_ptr)
+        ok = !cuda_failed(cudaMemcpy(e->d_ptr, ptr.data(), sizeof(unsigned) * ptr.size(), cudaMemcpyHostToDevice),
+                          "orion graph upload");
+    if (ok && e->n_edges)
+        ok = !cuda_failed(cudaMemcpy(e->d_src, src.data(), sizeof(unsigned) * src.size(), cudaMemcpyHostToDevice),
+                          "orion graph upload") &&
+             !cuda_failed(cudaMemcpy(e->d_w, w.data(), sizeof(ulonglong2) * w.size(), cudaMemcpyHostToDevice),
+                          "orion graph upload");
+    if (!ok) {
+        cudaFree(e->d_ptr);
+        cudaFree(e->d_src);
+        cudaFree(e->d_w);
+        delete e;
+        return nullptr;
+    }
+    g_cache[key] = e;
+    return e;
+}
+
+int last_launches() { return g_launches; }
+
+unsigned transpose_grid(long long n_r, long long n_c) { return (unsigned)(((n_r + 31) / 32) * ((n_c + 31) / 32)); }
+
+bool rows_to_columns(const ulonglong2* rows, long long cw_len, ulonglong2* cols, cudaStream_t s)
+{
+    transpose_kernel<<<transpose_grid(cw_len, kColumns), 256, 0, s>>>(rows, cols, cw_len, kColumns);
+    return launch_ok("orion rows_to_columns");
+}
+
+bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulonglong2* rows,
+            unsigned char* tree, cudaStream_t s)
+{
+    g_launches = 0;
+    const long long col_len = enc.col_len, cw_len = enc.cw_len;
+    const long long n_rows = 2 * col_len, size = tree_leaves(col_len);
+    // node 0 of the heap is unused; the reference leaves it zero
+    if (cuda_failed(cudaMemsetAsync(tree, 0, 32, s), "orion tree clear")) return false;
+    // 1. the message: column-major input -> rows [0, col_len)
+    if (src) {
+        transpose_kernel<<<transpose_grid(kColumns, col_len), 256, 0, s>>>(src, rows, kColumns, col_len);
+        if (!launch_ok("orion load columns")) return false;
+    } else {
+        int w_shift = 0;
+        while ((1 << w_shift) < px->W) ++w_shift;
+        const long long n = col_len * kColumns;
+        pixel_rows_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(*px, col_len, w_shift, rows);
+        if (!launch_ok("orion load pixels")) return false;
+    }
+    // 2. C multiplications, outermost depth first
+    for (const Level& lv : enc.levels) {
+        if (lv.R == 0) continue;
+        gather_kernel<<<(unsigned)((lv.R + 7) / 8), 256, 0, s>>>(rows, lv.off, lv.off + lv.n, lv.R,
+                                                                  enc.d_ptr + lv.c_ptr, enc.d_src + lv.c_edge,
+                                                                  enc.d_w + lv.c_edge);
+        if (!launch_ok("orion C gather")) return false;
+    }
+    // 3. D multiplications, innermost depth first
+    for (auto it = enc.levels.rbegin(); it != enc.levels.rend(); ++it) {
+        const Level& lv = *it;
+        if (lv.RD == 0) continue;
+        const long long next = lv.off + lv.n;
+        gather_kernel<<<(unsigned)((lv.RD + 7) / 8), 256, 0, s>>>(rows, next, next + lv.L, lv.RD,
+                                                                   enc.d_ptr + lv.d_ptr, enc.d_src + lv.d_edge,
+                                                                   enc.d_w + lv.d_edge);
+        if (!launch_ok("orion D gather")) return false;
+    }
+    // 4. row leaves, constant leaves for the zero rows and the tree padding
+    leaf_kernel<<<(unsigned)((cw_len + kLeafRows - 1) / kLeafRows), kLeafRows, 0, s>>>(rows, cw_len, tree, size);
+    if (!launch_ok("orion leaves")) return false;
+    if (size > cw_len) {
+        unsigned char zr[32], zb[32];
+        zero_row_leaf(zr);
+        zero_block_hash(zb);
+        ulonglong2 a[2], b[2];
+        memcpy(a, zr, 32);
+        memcpy(b, zb, 32);
+        const long long n = size - cw_len;
+        fill_leaves_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(tree, size, cw_len, n_rows, size, a[0],
+                                                                       a[1], b[0], b[1]);
+        if (!launch_ok("orion fill leaves")) return false;
+    }
+    // 5. the tree, nine levels per launch
+    long long n_in = size;
+    while (n_in > 1) {
+        int levels = 0;
+        while (levels < 9 && (1LL << (levels + 1)) <= n_in) ++levels;
+        const long long blocks = n_in >> levels;
+        tree_kernel<<<(unsigned)blocks, 1 << (levels - 1), 0, s>>>(tree, n_in, levels);
+        if (!launch_ok("orion tree")) return false;
+        n_in >>= levels;
+    }
+    return true;
+}
+
+}  // namespace orion
+}  // namespace tp

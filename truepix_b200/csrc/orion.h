@@ -1,0 +1,88 @@
+// Orion input-layer commitment on the device: expander encode of 128 columns
+// and the SHA-256 Merkle tree over the codeword rows.
+//
+// Reference: TruePix-main/Orion/Orion_nonzk -- commit() src/VPD/linearPC.cpp:97-197,
+// encode() include/linear_code/linear_code_encode.h:17-72, graphs
+// include/linear_code/expanders.h:19-60, tree src/infrastructure/merkle_tree.cpp:28-84.
+//
+// Device layout (ours): the codeword of all 128 columns is one row-major matrix
+// rows[r][c] of 16-byte field elements {u64 img, u64 real} (the reference's element
+// memory order), r < cw_len. A row is 2 KB: the expander gathers of one row and
+// the leaf hash of one row both read it contiguously. The encoder's levels live
+// in that one matrix: level k's message starts at row off_k, its codeword is
+// [message | codeword of level k+1 | D-part], and level k+1's message starts at
+// off_k + n_k, so no level needs a copy.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+namespace tp {
+namespace orion {
+
+constexpr int kColumns = 128;     // column_size (include/linear_code/parameter.h)
+constexpr int kThreshold = 13;    // distance_threshold = (int)(1 / 0.07) - 1
+constexpr int kCDegree = 10;      // cn
+constexpr int kDDegree = 20;      // dn
+
+struct Level {
+    long long n;     // message length at this depth
+    long long R;     // C targets  = (long long)(0.238 * n)
+    long long L;     // codeword length of the next depth
+    long long RD;    // D targets  = (long long)(n * 0.72 - L)
+    long long off;   // first row of this depth's message in the codeword matrix
+    long long c_ptr, c_edge;   // offsets of this depth's C graph in the CSR arrays
+    long long d_ptr, d_edge;   // same for the D graph
+};
+
+// Graphs of one column length, transposed to CSR by target on the host and kept
+// on the device (the reference draws them from glibc rand() in its default seed
+// state; the same draws are replayed here).
+struct Encoder {
+    int device = -1;
+    long long col_len = 0;
+    long long cw_len = 0;
+    std::vector<Level> levels;         // depths with n > kThreshold, outermost first
+    long long n_ptr = 0, n_edges = 0;
+    unsigned* d_ptr = nullptr;         // [n_ptr] first edge of each target (per graph, + 1 end)
+    unsigned* d_src = nullptr;         // [n_edges] source row within the graph's source range
+    ulonglong2* d_w = nullptr;         // [n_edges] weights {img, real}, canonical
+};
+
+// cached per (device, col_len); nullptr and the error set on failure
+const Encoder* encoder(long long col_len);
+// encode_output_len(col_len), computed without building graphs
+long long codeword_len(long long col_len);
+// power of two >= 2 * col_len (the Merkle tree has 2 * leaves() digests)
+long long tree_leaves(long long col_len);
+
+// Host-side SHA-256 constants of the commit: the chain of a row of zeros and
+// SHA-256 of 64 zero bytes (padded tree leaves), as digest bytes.
+void zero_row_leaf(unsigned char out[32]);
+void zero_block_hash(unsigned char out[32]);
+
+// Frame bytes as the commit's input vector (TruePix layout, truepix_gkr.h:107-206):
+// element f = copy * W + wire is pixel[copy * cs + wire] for wire < cs and copy < copies,
+// const_val at wire == const_idx (copy < copies), zero elsewhere (real part; img 0).
+struct PixelInput {
+    const unsigned char* pix;
+    int copies, cs, W, const_idx;
+    uint64_t const_val;
+};
+
+// Full commit into caller buffers: rows (cw_len x 128 elements) and tree
+// (2 * tree_leaves digests of 32 bytes, heap order, root at index 1).
+// src is the reference's column-major input (column c = src[c * col_len ..]),
+// or pixels when src == nullptr.
+bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulonglong2* rows,
+            unsigned char* tree, cudaStream_t s);
+
+// rows -> column-major codeword (the reference's encoded_codeword[c][r])
+bool rows_to_columns(const ulonglong2* rows, long long cw_len, ulonglong2* cols, cudaStream_t s);
+
+// launches issued by the last commit() on this thread
+int last_launches();
+
+}  // namespace orion
+}  // namespace tp

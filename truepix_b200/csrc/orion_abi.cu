@@ -1,0 +1,157 @@
+// C ABI of the Orion commitment (include/orion_gpu.h).
+#include <stdint.h>
+#include <string.h>
+
+#include "fp2.cuh"
+#include "orion.h"
+#include "runtime.h"
+#include "../../include/orion_gpu.h"
+
+namespace {
+
+constexpr long long kMaxColLen = 1LL << 22;
+
+bool check_n(long long N, const char* who)
+{
+    if (N <= 0 || N % tp::orion::kColumns != 0 || N / tp::orion::kColumns > kMaxColLen) {
+        tp::set_error(tp::TP_ERR_ARG, "%s: N = %lld must be a positive multiple of 128 with N/128 <= 2^22",
+                      who, N);
+        return false;
+    }
+    return true;
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    cudaStream_t s;
+    explicit DevBuf(size_t bytes, cudaStream_t st) : s(st) { p = tp::dev_alloc(bytes, st); }
+    ~DevBuf()
+    {
+        if (p) tp::dev_free(p, s);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+long long tp_orion_codeword_len(long long col_len)
+{
+    if (col_len <= 0) return 0;
+    return tp::orion::codeword_len(col_len);
+}
+
+long long tp_orion_tree_leaves(long long N)
+{
+    if (N <= 0 || N % tp::orion::kColumns) return 0;
+    return tp::orion::tree_leaves(N / tp::orion::kColumns);
+}
+
+int tp_orion_commit_dev(const void* d_src, long long N, void* d_rows, void* d_tree, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!check_n(N, "tp_orion_commit_dev")) return -1;
+    if (!d_src || !d_rows || !d_tree) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_commit_dev: null buffer");
+        return -1;
+    }
+    const tp::orion::Encoder* e = tp::orion::encoder(N / tp::orion::kColumns);
+    if (!e) return -1;
+    return tp::orion::commit(*e, static_cast<const ulonglong2*>(d_src), nullptr, static_cast<ulonglong2*>(d_rows),
+                             static_cast<unsigned char*>(d_tree), reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size,
+                               int n_wires, int const_idx, uint64_t const_val, void* d_rows, void* d_tree,
+                               void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!d_pixels || !d_rows || !d_tree || n_copies < 0 || n_copies > n_copies_padded || copy_size <= 0 ||
+        copy_size > n_wires || n_wires <= 0 || (n_wires & (n_wires - 1)) || n_copies_padded <= 0 ||
+        const_idx >= n_wires || (const_idx >= 0 && const_idx < copy_size) || const_val >= tp::P61) {
+        tp::set_error(tp::TP_ERR_ARG,
+                      "tp_orion_commit_pixels_dev: layout copies %d/%d, copy_size %d, wires %d, const %d",
+                      n_copies, n_copies_padded, copy_size, n_wires, const_idx);
+        return -1;
+    }
+    const long long N = (long long)n_copies_padded * n_wires;
+    if (!check_n(N, "tp_orion_commit_pixels_dev")) return -1;
+    const tp::orion::Encoder* e = tp::orion::encoder(N / tp::orion::kColumns);
+    if (!e) return -1;
+    tp::orion::PixelInput px;
+    px.pix = static_cast<const unsigned char*>(d_pixels);
+    px.copies = n_copies;
+    px.cs = copy_size;
+    px.W = n_wires;
+    px.const_idx = const_idx;
+    px.const_val = const_val;
+    return tp::orion::commit(*e, nullptr, &px, static_cast<ulonglong2*>(d_rows),
+                             static_cast<unsigned char*>(d_tree), reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_orion_rows_to_columns_dev(const void* d_rows, long long cw_len, void* d_cols, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!d_rows || !d_cols || cw_len <= 0) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_rows_to_columns_dev: bad arguments");
+        return -1;
+    }
+    return tp::orion::rows_to_columns(static_cast<const ulonglong2*>(d_rows), cw_len,
+                                      static_cast<ulonglong2*>(d_cols), reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_orion_commit(const uint64_t* src, long long N, unsigned char* tree_out, uint64_t* codeword_out)
+{
+    tp::clear_error();
+    tp::Ctx* c = tp::ctx();
+    if (!c) return -1;
+    if (!check_n(N, "tp_orion_commit")) return -1;
+    if (!src || !tree_out) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_commit: null buffer");
+        return -1;
+    }
+    for (long long i = 0; i < 2 * N; ++i)
+        if (src[i] >= tp::P61) {
+            tp::set_error(tp::TP_ERR_ARG, "tp_orion_commit: element %lld is not canonical", i / 2);
+            return -1;
+        }
+    const long long col_len = N / tp::orion::kColumns;
+    const tp::orion::Encoder* e = tp::orion::encoder(col_len);
+    if (!e) return -1;
+    const long long cw_len = e->cw_len, leaves = tp::orion::tree_leaves(col_len);
+    cudaStream_t s = c->stream;
+    DevBuf d_src(16 * (size_t)N, s), d_rows(16 * (size_t)cw_len * tp::orion::kColumns, s),
+        d_tree(64 * (size_t)leaves, s);
+    if (!d_src.p || !d_rows.p || !d_tree.p) return -1;
+    if (tp::cuda_failed(cudaMemcpyAsync(d_src.p, src, 16 * (size_t)N, cudaMemcpyHostToDevice, s), "H2D"))
+        return -1;
+    if (!tp::orion::commit(*e, static_cast<const ulonglong2*>(d_src.p), nullptr, static_cast<ulonglong2*>(d_rows.p),
+                           static_cast<unsigned char*>(d_tree.p), s))
+        return -1;
+    if (tp::cuda_failed(cudaMemcpyAsync(tree_out, d_tree.p, 64 * (size_t)leaves, cudaMemcpyDeviceToHost, s), "D2H"))
+        return -1;
+    if (codeword_out) {
+        DevBuf d_cols(16 * (size_t)cw_len * tp::orion::kColumns, s);
+        if (!d_cols.p) return -1;
+        if (!tp::orion::rows_to_columns(static_cast<const ulonglong2*>(d_rows.p), cw_len,
+                                        static_cast<ulonglong2*>(d_cols.p), s))
+            return -1;
+        if (tp::cuda_failed(cudaMemcpyAsync(codeword_out, d_cols.p, 16 * (size_t)cw_len * tp::orion::kColumns,
+                                            cudaMemcpyDeviceToHost, s),
+                            "D2H"))
+            return -1;
+        if (tp::cuda_failed(cudaStreamSynchronize(s), "synchronize")) return -1;
+    }
+    return tp::cuda_failed(cudaStreamSynchronize(s), "synchronize") ? -1 : 0;
+}
+
+}  // extern "C"

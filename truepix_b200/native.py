@@ -1,7 +1,7 @@
 """Loader and ctypes prototypes for the in-tree CUDA libraries.
 
 `gkr()` returns libnative_fp2_gpu.so with every entry point of
-include/native_fp2.h bound. It raises if the library is missing or no CUDA
+include/native_fp2.h and include/orion_gpu.h bound. It raises if the library is missing or no CUDA
 device is usable: there is no CPU fallback anywhere in the product path.
 """
 from __future__ import annotations
@@ -74,6 +74,13 @@ GKR_SIGNATURES = {
     "tp_timer_disable": (None, []),
     "tp_timer_reset": (None, []),
     "tp_timer_read": (_I32, [ctypes.POINTER(ctypes.c_float), _PI32, _I32]),
+    # Orion commitment (include/orion_gpu.h)
+    "tp_orion_codeword_len": (ctypes.c_longlong, [ctypes.c_longlong]),
+    "tp_orion_tree_leaves": (ctypes.c_longlong, [ctypes.c_longlong]),
+    "tp_orion_commit": (_I32, [_VP, ctypes.c_longlong, _VP, _VP]),
+    "tp_orion_commit_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP, _VP]),
+    "tp_orion_commit_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
+    "tp_orion_rows_to_columns_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP]),
 }
 
 _cache = {}
