@@ -1,5 +1,6 @@
 /*
- * Orion input-layer commitment on the GPU (libnative_fp2_gpu.so).
+ * Orion input-layer commitment, Fp2 NTT and Reed-Solomon commit on the GPU
+ * (libnative_fp2_gpu.so).
  *
  * The reference runs these steps on the CPU inside its Orion binaries
  * (TruePix-main/Orion/Orion_nonzk, driven by examples/multivariate_PC_test_*.cpp
@@ -60,6 +61,38 @@ int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_
 /* Row-major codeword (as written by the commits above) -> column-major
  * (encoded_codeword[c][r]); d_cols holds 128 * cw_len elements. */
 int tp_orion_rows_to_columns_dev(const void* d_rows, long long cw_len, void* d_cols, void* stream);
+
+/* ---- Fp2 NTT (src/infrastructure/RS_polynomial.cpp) ------------------------ */
+
+/* Replaces fast_fourier_transform(coef, coef_len, order, root, result)
+ * (RS_polynomial.cpp:46-130) with root = get_root_of_unity(log2 order)
+ * (src/linear_gkr/prime_field.cpp:60-73): result[i] = P(w^i), i < order, for the
+ * coef_len coefficients of P. Powers of two, coef_len <= order <= 2^28. */
+int tp_fft(const uint64_t* coef, int coef_len, int order, uint64_t* result);
+
+/* Replaces inverse_fast_fourier_transform(evals, coef_len, order, root, result)
+ * (RS_polynomial.cpp:132-206): the coef_len coefficients whose values on the
+ * coef_len-th roots of unity are evals[i * (order / coef_len)]. */
+int tp_ifft(const uint64_t* evals, int coef_len, int order, uint64_t* result);
+
+/* Device forms; `batch` transforms, transform b reading d_in + b * in_stride and
+ * writing d_out + b * out_stride (strides in elements). d_in == d_out only for
+ * batch 1. */
+int tp_fft_dev(const void* d_coef, long long coef_len, long long order, void* d_out, int batch,
+               long long in_stride, long long out_stride, void* stream);
+int tp_ifft_dev(const void* d_evals, long long coef_len, long long order, void* d_out, int batch,
+                long long in_stride, long long out_stride, void* stream);
+
+/* Replaces poly_commit_prover::commit_private_array(src, log_len)
+ * (include/poly_commitment/poly_commit.h:42-96) together with the
+ * fri::request_init_commit(log_len, 0) it ends in (src/VPD/fri.cpp:36-123):
+ * Reed-Solomon code at rate 2^-5 over 64 slices and the Merkle tree of the
+ * interleaved codeword. src: 2^log_len elements, 6 <= log_len <= 25.
+ * l_eval_out: NULL or 2^(log_len+5) elements (poly_commit::l_eval, slice-major).
+ * tree_out: 2^(log_len-1) digests (fri::witness_merkle[0]); the root (the
+ * function's return value in the reference) is tree_out[1]. */
+int tp_rs_commit(const uint64_t* src, int log_len, uint64_t* l_eval_out, unsigned char* tree_out);
+int tp_rs_commit_dev(const void* d_src, int log_len, void* d_l_eval, void* d_tree, void* stream);
 
 #ifdef __cplusplus
 }

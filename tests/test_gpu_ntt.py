@@ -1,0 +1,156 @@
+"""Fp2 NTT / IFFT and the Reed-Solomon commit on the GPU (include/orion_gpu.h)
+against the reference's outputs (tests/golden/orion_golden.npz) and the oracle,
+bit for bit; full-size transforms through round trips and linearity."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from orionlib import P61, ROOT, OrionOracle, digest, elements
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from truepix_b200 import native
+    return native.gkr()
+
+
+@pytest.fixture(scope="module")
+def orc():
+    return OrionOracle()
+
+
+@pytest.fixture(scope="module")
+def og():
+    return np.load(os.path.join(ROOT, "tests", "golden", "orion_golden.npz"))
+
+
+def vp(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def fft(lib, coef, order):
+    out = np.zeros(2 * order, np.uint64)
+    assert lib.tp_fft(vp(coef), coef.size // 2, order, vp(out)) == 0, lib.tp_last_error()
+    return out
+
+
+def ifft(lib, evals, coef_len):
+    out = np.zeros(2 * coef_len, np.uint64)
+    assert lib.tp_ifft(vp(evals), coef_len, evals.size // 2, vp(out)) == 0, lib.tp_last_error()
+    return out
+
+
+def test_fft_ifft_match_reference(lib, og):
+    for k in og.files:
+        if not k.startswith("fft_"):
+            continue
+        m, o = (int(v) for v in k.split("_")[1:])
+        r = fft(lib, elements(200 + m + o, m), o)
+        np.testing.assert_array_equal(r[:16], og["ffthead_%d_%d" % (m, o)][:r[:16].size])
+        assert digest(r) == og[k].tobytes(), (m, o)
+        ri = ifft(lib, elements(300 + m + o, o), m)
+        assert digest(ri) == og["ifft_%d_%d" % (m, o)].tobytes(), (m, o)
+
+
+@pytest.mark.parametrize("m,o", [(1 << 10, 1 << 11), (1 << 11, 1 << 11), (1 << 7, 1 << 13), (1 << 15, 1 << 20),
+                                 (1 << 21, 1 << 21), (1 << 16, 1 << 22)])
+def test_fft_ifft_match_oracle(lib, orc, m, o):
+    coef = elements(m + 3 * o, m)
+    np.testing.assert_array_equal(fft(lib, coef, o), orc.fft(coef, o))
+    ev = elements(m + 5 * o, o)
+    np.testing.assert_array_equal(ifft(lib, ev, m), orc.ifft(ev, m))
+
+
+def test_edge_values(lib, orc):
+    for kind in ("zero", "max", "small"):
+        a = elements(4, 1 << 12, kind)
+        np.testing.assert_array_equal(fft(lib, a, 1 << 14), orc.fft(a, 1 << 14))
+
+
+def test_size_2_24_round_trip_and_linearity(lib):
+    """2^24 (the largest transform of the microbenchmark): ifft(fft(a)) == a, and
+    fft(a + b) == fft(a) + fft(b), on the device."""
+    import torch
+    n = 1 << 24
+    dev = torch.device("cuda", 0)
+    a = torch.from_numpy(elements(31, n).view(np.int64)).to(dev)
+    b = torch.from_numpy(elements(32, n).view(np.int64)).to(dev)
+    s = torch.cuda.current_stream().cuda_stream
+    fa, fb, fab, back = (torch.empty_like(a) for _ in range(4))
+    for x, y in ((a, fa), (b, fb)):
+        assert lib.tp_fft_dev(x.data_ptr(), n, n, y.data_ptr(), 1, 0, 0, s) == 0, lib.tp_last_error()
+    assert lib.tp_ifft_dev(fa.data_ptr(), n, n, back.data_ptr(), 1, 0, 0, s) == 0
+    torch.cuda.synchronize()
+    an, bn = a.cpu().numpy().view(np.uint64), b.cpu().numpy().view(np.uint64)
+    np.testing.assert_array_equal(back.cpu().numpy().view(np.uint64), an)
+    abn = (an + bn) % np.uint64(P61)
+    dab = torch.from_numpy(abn.view(np.int64)).to(dev)
+    assert lib.tp_fft_dev(dab.data_ptr(), n, n, fab.data_ptr(), 1, 0, 0, s) == 0
+    torch.cuda.synchronize()
+    got = fab.cpu().numpy().view(np.uint64)
+    want = (fa.cpu().numpy().view(np.uint64) + fb.cpu().numpy().view(np.uint64)) % np.uint64(P61)
+    np.testing.assert_array_equal(got, want)
+    assert int(got.max()) < P61
+
+
+def test_batched_device_transforms(lib, orc):
+    import torch
+    m, o, batch = 1 << 8, 1 << 13, 64
+    src = elements(41, m * batch)
+    dev = torch.device("cuda", 0)
+    d_in = torch.from_numpy(src.view(np.int64)).to(dev)
+    d_out = torch.empty(2 * o * batch, dtype=torch.int64, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib.tp_fft_dev(d_in.data_ptr(), m, o, d_out.data_ptr(), batch, m, o, s) == 0
+    torch.cuda.synchronize()
+    out = d_out.cpu().numpy().view(np.uint64).reshape(batch, 2 * o)
+    for b in (0, 1, 37, 63):
+        np.testing.assert_array_equal(out[b], orc.fft(np.ascontiguousarray(src.reshape(batch, 2 * m)[b]), o))
+
+
+def test_rs_commit_matches_reference(lib, og):
+    for k in og.files:
+        if not k.startswith("rs_"):
+            continue
+        lg = int(k.split("_")[1])
+        src = elements(400 + lg, 1 << lg)
+        cw = np.zeros(2 << (lg + 5), np.uint64)
+        tree = np.zeros((1 << (lg - 1), 32), np.uint8)
+        assert lib.tp_rs_commit(vp(src), lg, vp(cw), vp(tree)) == 0, lib.tp_last_error()
+        assert digest(cw) == og["rscw_%d" % lg].tobytes(), lg
+        assert tree[1].tobytes() == og[k].tobytes(), lg
+        assert not tree[0].any()
+
+
+def test_rs_codeword_contains_the_input_at_2_22(lib):
+    """Rate 2^-5: slice i's evaluations on every 32nd point of its 2^(L-1)-point
+    domain are the slice's own inputs (the original domain is a subgroup)."""
+    import torch
+    lg = 22
+    n, real_cnt, slice_len = 1 << lg, 1 << (lg - 6), 1 << (lg - 1)
+    dev = torch.device("cuda", 0)
+    src = torch.from_numpy(elements(9, n).view(np.int64)).to(dev)
+    cw = torch.empty(2 << (lg + 5), dtype=torch.int64, device=dev)
+    tree = torch.empty(32 << (lg - 1), dtype=torch.uint8, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib.tp_rs_commit_dev(src.data_ptr(), lg, cw.data_ptr(), tree.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    sub = cw.view(64, slice_len, 2)[:, ::32, :]
+    assert torch.equal(sub, src.view(64, real_cnt, 2))
+    assert bool(((cw >= 0) & (cw < P61)).all())
+
+
+def test_transform_argument_errors(lib):
+    a = elements(1, 16)
+    out = np.zeros(64, np.uint64)
+    assert lib.tp_fft(vp(a), 3, 16, vp(out)) == -1
+    assert lib.tp_fft(vp(a), 32, 16, vp(out)) == -1
+    bad = a.copy()
+    bad[3] = P61
+    assert lib.tp_fft(vp(bad), 8, 16, vp(out)) == -1
+    assert b"canonical" in lib.tp_last_error()
+    assert lib.tp_rs_commit(vp(a), 5, None, vp(out)) == -1

@@ -1,0 +1,317 @@
+// Fp2 NTT passes (see ntt.h for the decomposition).
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "ntt.h"
+#include "runtime.h"
+
+namespace tp {
+namespace ntt {
+
+namespace {
+
+thread_local int g_launches = 0;
+
+constexpr int kThreads = 256;
+constexpr int kMaxLogR = 10;
+constexpr int kTileElems = 4096;   // R * G elements staged per CTA (64 KB)
+
+// w^t (t < 2^h) and w^(t 2^h) (t < n / 2^h) of one transform size and direction
+struct Tables {
+    fp2* lo = nullptr;
+    fp2* hi = nullptr;
+    int h = 0;
+};
+
+std::mutex g_mu;
+std::map<std::tuple<int, int, int>, Tables> g_tables;   // (device, log n, inverse)
+bool g_attr_set[64] = {};
+
+struct Pass {
+    int log_r, log_g, logn, log_s;
+    int first, last;
+    long long in_len, in_step;        // first pass: elements present, read stride
+    long long src_batch, dst_batch;   // element strides between transforms
+    u64 scale;                        // last pass: multiply by this base-field scalar (0: none)
+    int n_dig;                        // last pass: the earlier digits
+    int dig_bits[3];
+    int dig_shift[3];
+};
+
+__device__ __forceinline__ fp2 ld_fe(const ulonglong2* p) { const ulonglong2 v = *p; return mk(v.y, v.x); }
+__device__ __forceinline__ void st_fe(ulonglong2* p, fp2 a) { *p = make_ulonglong2(a.im, a.re); }
+
+__device__ __forceinline__ fp2 tw_pow(const fp2* __restrict__ lo, const fp2* __restrict__ hi, int h,
+                                      unsigned long long e)
+{
+    const fp2 a = lo[e & ((1ull << h) - 1)];
+    const unsigned long long q = e >> h;
+    return q ? l2mul(a, hi[q]) : a;
+}
+
+__device__ __forceinline__ int bitrev(int j, int bits) { return bits ? (int)(__brev((unsigned)j) >> (32 - bits)) : 0; }
+
+// One pass: a CTA transforms G = 2^log_g columns of R = 2^log_r elements.
+// src and dst may be the same buffer (in-place middle pass): every CTA reads its
+// own columns completely before it writes them, and no other CTA touches them.
+__global__ void __launch_bounds__(kThreads) pass_kernel(const ulonglong2* src, ulonglong2* dst, Pass p,
+                                                        const fp2* __restrict__ lo,
+                                                        const fp2* __restrict__ hi, int h)
+{
+    extern __shared__ fp2 sm[];
+    const int R = 1 << p.log_r, G = 1 << p.log_g;
+    fp2* tws = sm + (R << p.log_g);
+    const int tid = threadIdx.x;
+    src += (long long)blockIdx.y * p.src_batch;
+    dst += (long long)blockIdx.y * p.dst_batch;
+    const long long S = 1LL << p.log_s;
+
+    // twiddles of the R-point DFT: w_R^t = w_n^(t n / R), t < R / 2
+    for (int t = tid; t < R / 2; t += kThreads) tws[t] = tw_pow(lo, hi, h, (unsigned long long)t << (p.logn - p.log_r));
+
+    // columns of this CTA
+    long long col_base = 0, s0 = 0, c0 = 0;
+    if (!p.last) {
+        const long long groups = S >> p.log_g;   // column groups per outer index
+        const long long a = blockIdx.x / groups;
+        s0 = (blockIdx.x % groups) << p.log_g;
+        col_base = a * ((long long)R << p.log_s) + s0;
+    } else {
+        c0 = (long long)blockIdx.x << p.log_g;
+    }
+
+    // load (bit-reversed into shared memory)
+    for (int idx = tid; idx < (R << p.log_g); idx += kThreads) {
+        int c, j;
+        long long pos;
+        if (!p.last) {
+            c = idx & (G - 1);
+            j = idx >> p.log_g;
+            pos = col_base + c + (long long)j * S;
+        } else {
+            j = idx & (R - 1);
+            c = idx >> p.log_r;
+            const long long cc = c0 + c;
+            long long base = 0;
+            int sh = 0;
+            for (int t = 0; t < p.n_dig; ++t) {
+                base += ((cc >> sh) & ((1LL << p.dig_bits[t]) - 1)) << p.dig_shift[t];
+                sh += p.dig_bits[t];
+            }
+            pos = base + j;
+        }
+        fp2 v;
+        if (p.first)
+            v = pos < p.in_len ? ld_fe(src + pos * p.in_step) : f2zero();
+        else
+            v = ld_fe(src + pos);
+        sm[(bitrev(j, p.log_r) << p.log_g) + c] = v;
+    }
+    __syncthreads();
+
+    // radix-2 stages, natural-order output
+    for (int lh = 0; lh < p.log_r; ++lh) {
+        const int half = 1 << lh;
+        for (int bi = tid; bi < ((R / 2) << p.log_g); bi += kThreads) {
+            const int c = bi & (G - 1);
+            const int q = bi >> p.log_g;
+            const int pin = q & (half - 1);
+            const int u = ((q >> lh) << (lh + 1)) + pin;
+            const int v = u + half;
+            const fp2 w = tws[pin << (p.log_r - 1 - lh)];
+            const fp2 x = sm[(u << p.log_g) + c];
+            const fp2 y = l2mul(w, sm[(v << p.log_g) + c]);
+            sm[(u << p.log_g) + c] = l2add(x, y);
+            sm[(v << p.log_g) + c] = l2sub(x, y);
+        }
+        __syncthreads();
+    }
+
+    // store
+    for (int idx = tid; idx < (R << p.log_g); idx += kThreads) {
+        const int c = idx & (G - 1);
+        const int k = idx >> p.log_g;
+        fp2 val = sm[(k << p.log_g) + c];
+        if (!p.last) {
+            // w_{R S}^(k s) = w_n^((k s mod R S) n / (R S))
+            const unsigned long long e =
+                (((unsigned long long)k * (unsigned long long)(s0 + c)) & ((1ull << (p.log_r + p.log_s)) - 1))
+                << (p.logn - p.log_r - p.log_s);
+            if (e) val = l2mul(val, tw_pow(lo, hi, h, e));
+            st_fe(dst + col_base + c + (long long)k * S, val);
+        } else {
+            if (p.scale) val = mk(lmul(val.re, p.scale), lmul(val.im, p.scale));
+            st_fe(dst + (c0 + c) + ((long long)k << (p.logn - p.log_r)), l2canon(val));
+        }
+    }
+}
+
+fp2 f2pow(fp2 a, unsigned long long e)
+{
+    fp2 r = mk(1, 0);
+    while (e) {
+        if (e & 1) r = f2mul(r, a);
+        a = f2mul(a, a);
+        e >>= 1;
+    }
+    return r;
+}
+
+int ilog2(long long n)
+{
+    int k = 0;
+    while ((1LL << k) < n) ++k;
+    return k;
+}
+
+bool is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
+
+const Tables* tables(int logn, bool inv)
+{
+    Ctx* c = ctx();
+    if (!c) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto key = std::make_tuple(c->device, logn, inv ? 1 : 0);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end()) return &it->second;
+    fp2 w = root_of_unity(logn);
+    if (inv) w = f2pow(w, (1ull << logn) - 1);
+    Tables t;
+    t.h = (logn + 1) / 2;
+    const size_t nlo = (size_t)1 << t.h, nhi = (size_t)1 << (logn - t.h);
+    std::vector<fp2> lo(nlo), hi(nhi);
+    lo[0] = mk(1, 0);
+    for (size_t i = 1; i < nlo; ++i) lo[i] = f2mul(lo[i - 1], w);
+    const fp2 step = nlo < ((size_t)1 << logn) ? f2mul(lo[nlo - 1], w) : mk(1, 0);   // w^(2^h)
+    hi[0] = mk(1, 0);
+    for (size_t i = 1; i < nhi; ++i) hi[i] = f2mul(hi[i - 1], step);
+    if (cuda_failed(cudaMalloc(&t.lo, sizeof(fp2) * nlo), "ntt twiddle alloc") ||
+        cuda_failed(cudaMalloc(&t.hi, sizeof(fp2) * nhi), "ntt twiddle alloc") ||
+        cuda_failed(cudaMemcpy(t.lo, lo.data(), sizeof(fp2) * nlo, cudaMemcpyHostToDevice), "ntt twiddle upload") ||
+        cuda_failed(cudaMemcpy(t.hi, hi.data(), sizeof(fp2) * nhi, cudaMemcpyHostToDevice), "ntt twiddle upload")) {
+        cudaFree(t.lo);
+        cudaFree(t.hi);
+        return nullptr;
+    }
+    return &(g_tables[key] = t);
+}
+
+// digit split of a 2^logn transform: at most 10 bits per pass
+std::vector<int> split(int logn)
+{
+    const int P = logn <= kMaxLogR ? 1 : (logn + kMaxLogR - 1) / kMaxLogR;
+    std::vector<int> d(P, logn / P);
+    for (int i = 0; i < logn % P; ++i) d[i]++;
+    return d;
+}
+
+// n-point DFT (direction by tables) of the first-pass input `in`
+bool run(const ulonglong2* in, long long in_len, long long in_step, int logn, bool inv, ulonglong2* out,
+         int batch, long long in_batch, long long out_batch, ulonglong2* scratch, u64 scale, cudaStream_t s)
+{
+    const Tables* tb = tables(logn, inv);
+    if (!tb) return false;
+    Ctx* c = ctx();
+    if (c->device >= 0 && c->device < 64 && !g_attr_set[c->device]) {
+        if (cuda_failed(cudaFuncSetAttribute(pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (kTileElems + (1 << kMaxLogR) / 2) * (int)sizeof(fp2)),
+                        "ntt smem attribute"))
+            return false;
+        g_attr_set[c->device] = true;
+    }
+    const std::vector<int> d = split(logn);
+    const int P = (int)d.size();
+    const long long n = 1LL << logn;
+    ulonglong2* tmp = scratch;
+    bool own = false;
+    if (P > 1 && !tmp) {
+        tmp = static_cast<ulonglong2*>(dev_alloc(sizeof(ulonglong2) * (size_t)n * batch, s));
+        if (!tmp) return false;
+        own = true;
+    }
+    bool ok = true;
+    int rest = logn;
+    for (int t = 0; t < P && ok; ++t) {
+        Pass p = {};
+        p.log_r = d[t];
+        p.logn = logn;
+        rest -= d[t];
+        p.log_s = rest;
+        p.first = t == 0;
+        p.last = t == P - 1;
+        p.in_len = in_len;
+        p.in_step = in_step;
+        p.scale = p.last ? scale : 0;
+        const ulonglong2* src = t == 0 ? in : tmp;
+        ulonglong2* dst = p.last ? out : tmp;
+        p.src_batch = t == 0 ? in_batch : n;
+        p.dst_batch = p.last ? out_batch : n;
+        int log_g = ilog2(kTileElems) - p.log_r;
+        if (log_g > 4) log_g = 4;
+        if (!p.last && log_g > p.log_s) log_g = p.log_s;
+        if (p.last && log_g > logn - p.log_r) log_g = logn - p.log_r;
+        p.log_g = log_g;
+        if (p.last) {
+            p.n_dig = P - 1;
+            int shift = logn;
+            for (int u = 0; u < P - 1; ++u) {
+                shift -= d[u];
+                p.dig_bits[u] = d[u];
+                p.dig_shift[u] = shift;
+            }
+        }
+        const long long ctas = n >> (p.log_r + p.log_g);
+        const size_t smem = sizeof(fp2) * (((size_t)1 << (p.log_r + p.log_g)) + ((size_t)1 << p.log_r) / 2);
+        pass_kernel<<<dim3((unsigned)ctas, (unsigned)batch), kThreads, smem, s>>>(src, dst, p, tb->lo, tb->hi, tb->h);
+        ++g_launches;
+        ok = !cuda_failed(cudaGetLastError(), "ntt pass");
+    }
+    if (own) dev_free(tmp, s);
+    return ok;
+}
+
+bool check_sizes(long long m, long long n, int batch, const char* who)
+{
+    if (!is_pow2(m) || !is_pow2(n) || m > n || n > (1LL << kMaxLog) || batch < 1 || batch > 65535) {
+        set_error(TP_ERR_ARG, "%s: need powers of two coef_len %lld <= order %lld <= 2^%d, batch %d", who, m, n,
+                  kMaxLog, batch);
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+fp2 root_of_unity(int lg)
+{
+    fp2 g = mk(2147483648ull, 1033321771269002680ull);
+    for (int i = 0; i < 62 - lg; ++i) g = f2mul(g, g);
+    return g;
+}
+
+int passes(long long n) { return (int)split(ilog2(n)).size(); }
+
+int last_launches() { return g_launches; }
+
+bool forward(const ulonglong2* in, long long m, long long n, ulonglong2* out, int batch, long long in_batch,
+             long long out_batch, ulonglong2* scratch, cudaStream_t s)
+{
+    g_launches = 0;
+    if (!check_sizes(m, n, batch, "fft")) return false;
+    return run(in, m, 1, ilog2(n), false, out, batch, in_batch, out_batch, scratch, 0, s);
+}
+
+bool inverse(const ulonglong2* in, long long m, long long n, ulonglong2* out, int batch, long long in_batch,
+             long long out_batch, ulonglong2* scratch, cudaStream_t s)
+{
+    g_launches = 0;
+    if (!check_sizes(m, n, batch, "ifft")) return false;
+    const int lm = ilog2(m);
+    const u64 inv_m = lm ? (1ull << (61 - lm)) : 1ull;   // 2^-lm = 2^(61 - lm) mod 2^61 - 1
+    return run(in, m, n / m, lm, true, out, batch, in_batch, out_batch, scratch, inv_m, s);
+}
+
+}  // namespace ntt
+}  // namespace tp

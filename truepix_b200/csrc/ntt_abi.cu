@@ -1,0 +1,145 @@
+// C ABI of the Fp2 NTT and the Reed-Solomon commit (include/orion_gpu.h).
+#include <stdint.h>
+
+#include "ntt.h"
+#include "runtime.h"
+#include "../../include/orion_gpu.h"
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    cudaStream_t s;
+    explicit DevBuf(size_t bytes, cudaStream_t st) : s(st) { p = tp::dev_alloc(bytes, st); }
+    ~DevBuf()
+    {
+        if (p) tp::dev_free(p, s);
+    }
+};
+
+bool canonical(const uint64_t* a, long long words, const char* who)
+{
+    for (long long i = 0; i < words; ++i)
+        if (a[i] >= tp::P61) {
+            tp::set_error(tp::TP_ERR_ARG, "%s: element %lld is not canonical", who, i / 2);
+            return false;
+        }
+    return true;
+}
+
+bool pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
+
+int host_transform(const uint64_t* in, int coef_len, int order, uint64_t* out, bool inv)
+{
+    tp::clear_error();
+    tp::Ctx* c = tp::ctx();
+    if (!c) return -1;
+    const char* who = inv ? "tp_ifft" : "tp_fft";
+    if (!in || !out || !pow2(coef_len) || !pow2(order) || coef_len > order || order > (1 << tp::ntt::kMaxLog)) {
+        tp::set_error(tp::TP_ERR_ARG, "%s: need powers of two coef_len %d <= order %d <= 2^%d", who, coef_len,
+                      order, tp::ntt::kMaxLog);
+        return -1;
+    }
+    const long long n_in = inv ? order : coef_len, n_out = inv ? coef_len : order;
+    if (!canonical(in, 2 * n_in, who)) return -1;
+    cudaStream_t s = c->stream;
+    DevBuf d_in(16 * (size_t)n_in, s), d_out(16 * (size_t)n_out, s);
+    if (!d_in.p || !d_out.p) return -1;
+    if (tp::cuda_failed(cudaMemcpyAsync(d_in.p, in, 16 * (size_t)n_in, cudaMemcpyHostToDevice, s), "H2D")) return -1;
+    const ulonglong2* di = static_cast<const ulonglong2*>(d_in.p);
+    ulonglong2* dout = static_cast<ulonglong2*>(d_out.p);
+    const bool ok = inv ? tp::ntt::inverse(di, coef_len, order, dout, 1, 0, 0, nullptr, s)
+                        : tp::ntt::forward(di, coef_len, order, dout, 1, 0, 0, nullptr, s);
+    if (!ok) return -1;
+    if (tp::cuda_failed(cudaMemcpyAsync(out, d_out.p, 16 * (size_t)n_out, cudaMemcpyDeviceToHost, s), "D2H"))
+        return -1;
+    return tp::cuda_failed(cudaStreamSynchronize(s), "synchronize") ? -1 : 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tp_fft(const uint64_t* coef, int coef_len, int order, uint64_t* result)
+{
+    return host_transform(coef, coef_len, order, result, false);
+}
+
+int tp_ifft(const uint64_t* evals, int coef_len, int order, uint64_t* result)
+{
+    return host_transform(evals, coef_len, order, result, true);
+}
+
+int tp_fft_dev(const void* d_coef, long long coef_len, long long order, void* d_out, int batch,
+               long long in_stride, long long out_stride, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!d_coef || !d_out) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_fft_dev: null buffer");
+        return -1;
+    }
+    return tp::ntt::forward(static_cast<const ulonglong2*>(d_coef), coef_len, order, static_cast<ulonglong2*>(d_out),
+                            batch, in_stride, out_stride, nullptr, reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_ifft_dev(const void* d_evals, long long coef_len, long long order, void* d_out, int batch,
+                long long in_stride, long long out_stride, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!d_evals || !d_out) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_ifft_dev: null buffer");
+        return -1;
+    }
+    return tp::ntt::inverse(static_cast<const ulonglong2*>(d_evals), coef_len, order, static_cast<ulonglong2*>(d_out),
+                            batch, in_stride, out_stride, nullptr, reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_rs_commit_dev(const void* d_src, int log_len, void* d_l_eval, void* d_tree, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!d_src || !d_l_eval || !d_tree) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_rs_commit_dev: null buffer");
+        return -1;
+    }
+    return tp::rs::commit(static_cast<const ulonglong2*>(d_src), log_len, static_cast<ulonglong2*>(d_l_eval),
+                          static_cast<unsigned char*>(d_tree), reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_rs_commit(const uint64_t* src, int log_len, uint64_t* l_eval_out, unsigned char* tree_out)
+{
+    tp::clear_error();
+    tp::Ctx* c = tp::ctx();
+    if (!c) return -1;
+    if (!src || !tree_out || log_len < tp::rs::kMinLog || log_len > tp::rs::kMaxLog) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_rs_commit: need src, tree_out and %d <= log_len <= %d", tp::rs::kMinLog,
+                      tp::rs::kMaxLog);
+        return -1;
+    }
+    const long long n = 1LL << log_len, n_eval = n << 5, n_tree = n >> 1;
+    if (!canonical(src, 2 * n, "tp_rs_commit")) return -1;
+    cudaStream_t s = c->stream;
+    DevBuf d_src(16 * (size_t)n, s), d_eval(16 * (size_t)n_eval, s), d_tree(32 * (size_t)n_tree, s);
+    if (!d_src.p || !d_eval.p || !d_tree.p) return -1;
+    if (tp::cuda_failed(cudaMemcpyAsync(d_src.p, src, 16 * (size_t)n, cudaMemcpyHostToDevice, s), "H2D")) return -1;
+    if (!tp::rs::commit(static_cast<const ulonglong2*>(d_src.p), log_len, static_cast<ulonglong2*>(d_eval.p),
+                        static_cast<unsigned char*>(d_tree.p), s))
+        return -1;
+    if (tp::cuda_failed(cudaMemcpyAsync(tree_out, d_tree.p, 32 * (size_t)n_tree, cudaMemcpyDeviceToHost, s), "D2H"))
+        return -1;
+    if (l_eval_out && tp::cuda_failed(cudaMemcpyAsync(l_eval_out, d_eval.p, 16 * (size_t)n_eval,
+                                                      cudaMemcpyDeviceToHost, s),
+                                      "D2H"))
+        return -1;
+    return tp::cuda_failed(cudaStreamSynchronize(s), "synchronize") ? -1 : 0;
+}
+
+}  // extern "C"

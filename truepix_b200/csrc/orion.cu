@@ -517,14 +517,20 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
                                                                        a[1], b[0], b[1]);
         if (!launch_ok("orion fill leaves")) return false;
     }
-    // 5. the tree, nine levels per launch
-    long long n_in = size;
+    // 5. the tree
+    return build_tree(tree, size, s);
+}
+
+bool build_tree(unsigned char* tree, long long leaves, cudaStream_t s)
+{
+    // nine levels per launch
+    long long n_in = leaves;
     while (n_in > 1) {
         int levels = 0;
         while (levels < 9 && (1LL << (levels + 1)) <= n_in) ++levels;
         const long long blocks = n_in >> levels;
         tree_kernel<<<(unsigned)blocks, 1 << (levels - 1), 0, s>>>(tree, n_in, levels);
-        if (!launch_ok("orion tree")) return false;
+        if (!launch_ok("merkle tree")) return false;
         n_in >>= levels;
     }
     return true;

@@ -78,10 +78,15 @@ struct PixelInput {
 bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulonglong2* rows,
             unsigned char* tree, cudaStream_t s);
 
+// Merkle tree over `leaves` (a power of two) digests already stored at heap
+// positions [leaves, 2 leaves) of `tree`: node k = SHA256(node 2k || node 2k + 1)
+// (src/infrastructure/merkle_tree.cpp:64-83), root at 1.
+bool build_tree(unsigned char* tree, long long leaves, cudaStream_t s);
+
 // rows -> column-major codeword (the reference's encoded_codeword[c][r])
 bool rows_to_columns(const ulonglong2* rows, long long cw_len, ulonglong2* cols, cudaStream_t s);
 
-// launches issued by the last commit() on this thread
+// launches issued by commit() / build_tree() on this thread since the last commit()
 int last_launches();
 
 }  // namespace orion
