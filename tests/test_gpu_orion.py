@@ -124,6 +124,8 @@ def _pixel_commit(lib, pix, copies, cs, W, ci, cv, padded):
     (64, 384, -1, 0, 64),          # mask-like: no constant
     (30, 385, -1, 0, 32),          # crop: 385 inputs
     (3, 384, 384, 255, 4),         # inv constant, tiny
+    (5, 384, 384, 1000, 8),        # constant >= 256: no byte path for depth 0
+    (200, 384, 384, 128, 256),     # byte path with more targets than one CTA row
 ])
 def test_commit_from_pixels_matches_materialised_input(lib, orc, copies, cs, ci, cv, padded):
     pix = frame_bytes(copies + cs, copies * cs)

@@ -1,5 +1,6 @@
 // Orion commit on the device: expander encode (gathers over target-sorted
 // graphs) and the SHA-256 Merkle tree. See orion.h for the layout.
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -161,8 +162,11 @@ __global__ void __launch_bounds__(256) transpose_kernel(const ulonglong2* __rest
 }
 
 // rows[r][c] = input element c * col_len + r of a frame (PixelInput layout)
+// (and, when `bytes` is set, the same values as a row-major byte matrix
+// bytes[r][c]: every value of a frame is < 256 when its constant is)
 __global__ void __launch_bounds__(256) pixel_rows_kernel(PixelInput px, long long col_len, int w_shift,
-                                                         ulonglong2* __restrict__ rows)
+                                                         ulonglong2* __restrict__ rows,
+                                                         unsigned char* __restrict__ bytes)
 {
     const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
     if (i >= col_len * kColumns) return;
@@ -178,6 +182,66 @@ __global__ void __launch_bounds__(256) pixel_rows_kernel(PixelInput px, long lon
             v = px.const_val;
     }
     rows[i] = make_ulonglong2(0, v);
+    if (bytes) bytes[i] = (unsigned char)v;
+}
+
+// The depth-0 C multiplication of a frame, from its byte matrix: every source
+// value v is < 2^8 with zero imaginary part, so w * v needs no field
+// multiplication. With w = w1 * 2^32 + w0 (w0 < 2^32, w1 < 2^29), the sums
+// S0 = sum w0 v < 2^(40 + 16) and S1 = sum w1 v stay exact in 64 bits for up to
+// 2^16 in-edges (checked on the host), and S0 + S1 * 2^32 is reduced once per
+// target. One warp per target row; lane l owns columns 4l .. 4l + 3, one 32-bit
+// load (4 bytes) per edge.
+__global__ void __launch_bounds__(256) gather_bytes_kernel(const unsigned char* __restrict__ bytes,
+                                                           ulonglong2* __restrict__ rows, long long dst_row,
+                                                           long long n_targets,
+                                                           const unsigned* __restrict__ ptr,
+                                                           const unsigned* __restrict__ esrc,
+                                                           const ulonglong2* __restrict__ ew)
+{
+    const long long t = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (t >= n_targets) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned e0 = ptr[t], e1 = ptr[t + 1];
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(bytes) + lane;
+    // [column][re lo, re hi, im lo, im hi]
+    u64 acc[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[k][q] = 0;
+    for (unsigned eb = e0; eb < e1; eb += 32) {
+        const int cnt = (int)min(32u, e1 - eb);
+        unsigned my_s = 0;
+        ulonglong2 my_w = make_ulonglong2(0, 0);
+        if (lane < cnt) {
+            my_s = esrc[eb + lane];
+            my_w = ew[eb + lane];
+        }
+        for (int j = 0; j < cnt; ++j) {
+            const unsigned sj = __shfl_sync(0xffffffffu, my_s, j);
+            const uint32_t wr0 = __shfl_sync(0xffffffffu, (uint32_t)my_w.y, j);
+            const uint32_t wr1 = __shfl_sync(0xffffffffu, (uint32_t)(my_w.y >> 32), j);
+            const uint32_t wi0 = __shfl_sync(0xffffffffu, (uint32_t)my_w.x, j);
+            const uint32_t wi1 = __shfl_sync(0xffffffffu, (uint32_t)(my_w.x >> 32), j);
+            const uint32_t word = __ldg(src + (long long)sj * (kColumns / 4));
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t v = (word >> (8 * k)) & 0xFFu;
+                acc[k][0] += (u64)wr0 * v;
+                acc[k][1] += (u64)wr1 * v;
+                acc[k][2] += (u64)wi0 * v;
+                acc[k][3] += (u64)wi1 * v;
+            }
+        }
+    }
+    ulonglong2* dst = rows + (dst_row + t) * kColumns + 4 * lane;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const u64 re = acc[k][0] + ((acc[k][1] & 0x1FFFFFFFull) << 32) + (acc[k][1] >> 29);
+        const u64 im = acc[k][2] + ((acc[k][3] & 0x1FFFFFFFull) << 32) + (acc[k][3] >> 29);
+        dst[k] = make_ulonglong2(canon61(im), canon61(re));
+    }
 }
 
 // One warp per target row t of a graph: rows[dst + t][c] = sum over in-edges
@@ -265,7 +329,8 @@ __device__ __forceinline__ void load_digest(const unsigned char* tree, long long
 // One thread per row; the CTA stages 128 rows x 8 columns (padded to 9, so
 // that 16-byte reads of consecutive rows fall in distinct banks) at a time.
 __global__ void __launch_bounds__(kLeafRows) leaf_kernel(const ulonglong2* __restrict__ rows, long long cw_len,
-                                                         unsigned char* __restrict__ tree, long long leaf0)
+                                                         unsigned char* __restrict__ tree, long long leaf0,
+                                                         uint32_t one)
 {
     __shared__ ulonglong2 tile[kLeafRows][2 * kLeafPairs + 1];
     const long long r0 = (long long)blockIdx.x * kLeafRows;
@@ -290,7 +355,7 @@ __global__ void __launch_bounds__(kLeafRows) leaf_kernel(const ulonglong2* __res
             const ulonglong2 x = tile[tid][2 * p], y = tile[tid][2 * p + 1];
             sha::fe_words(x.x, x.y, w + 8);
             sha::fe_words(y.x, y.y, w + 12);
-            sha::hash64(w, st);
+            sha::hash64(w, st, sha::AddMad{one});
         }
         __syncthreads();
     }
@@ -312,7 +377,8 @@ __global__ void fill_leaves_kernel(unsigned char* __restrict__ tree, long long l
 // `levels` tree levels above the n_in nodes at heap positions [n_in, 2 n_in):
 // CTA b reduces the 2^levels nodes from n_in + b * 2^levels to one node
 // (merkle_tree.cpp:64-83: node k = SHA256(node 2k || node 2k + 1)).
-__global__ void __launch_bounds__(256) tree_kernel(unsigned char* __restrict__ tree, long long n_in, int levels)
+__global__ void __launch_bounds__(256) tree_kernel(unsigned char* __restrict__ tree, long long n_in, int levels,
+                                                   uint32_t one)
 {
     __shared__ uint32_t s[256][9];
     const int t = threadIdx.x;
@@ -323,7 +389,7 @@ __global__ void __launch_bounds__(256) tree_kernel(unsigned char* __restrict__ t
         uint32_t w[16];
         load_digest(tree, base + 2 * t, w);
         load_digest(tree, base + 2 * t + 1, w + 8);
-        sha::hash64(w, st);
+        sha::hash64(w, st, sha::AddMad{one});
         store_digest(tree, (base >> 1) + t, st);
     }
     for (int lv = 1; lv < levels; ++lv) {
@@ -341,7 +407,7 @@ __global__ void __launch_bounds__(256) tree_kernel(unsigned char* __restrict__ t
                 w[i] = s[2 * t][i];
                 w[8 + i] = s[2 * t + 1][i];
             }
-            sha::hash64(w, st);
+            sha::hash64(w, st, sha::AddMad{one});
             store_digest(tree, (base >> 1) + t, st);
         }
         __syncthreads();
@@ -428,6 +494,11 @@ const Encoder* encoder(long long col_len)
         off += n;
         n = lv.R;
     }
+    if (!C.empty()) {
+        unsigned mx = 0;
+        for (size_t t = 0; t + 1 < C[0].ptr.size(); ++t) mx = std::max(mx, C[0].ptr[t + 1] - C[0].ptr[t]);
+        e->max_c0_in_degree = mx;
+    }
     e->n_ptr = (long long)ptr.size();
     e->n_edges = (long long)src.size();
     bool ok = true;
@@ -474,6 +545,7 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
     // node 0 of the heap is unused; the reference leaves it zero
     if (cuda_failed(cudaMemsetAsync(tree, 0, 32, s), "orion tree clear")) return false;
     // 1. the message: column-major input -> rows [0, col_len)
+    unsigned char* bytes = nullptr;
     if (src) {
         transpose_kernel<<<transpose_grid(kColumns, col_len), 256, 0, s>>>(src, rows, kColumns, col_len);
         if (!launch_ok("orion load columns")) return false;
@@ -481,17 +553,34 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
         int w_shift = 0;
         while ((1 << w_shift) < px->W) ++w_shift;
         const long long n = col_len * kColumns;
-        pixel_rows_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(*px, col_len, w_shift, rows);
-        if (!launch_ok("orion load pixels")) return false;
+        // byte path of the depth-0 C multiplication: values < 2^8, in-degree < 2^16
+        if (px->const_val < 256 && !enc.levels.empty() && enc.max_c0_in_degree < (1u << 16)) {
+            bytes = static_cast<unsigned char*>(dev_alloc((size_t)n, s));
+            if (!bytes) return false;
+        }
+        pixel_rows_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(*px, col_len, w_shift, rows, bytes);
+        if (!launch_ok("orion load pixels")) {
+            if (bytes) dev_free(bytes, s);
+            return false;
+        }
     }
     // 2. C multiplications, outermost depth first
     for (const Level& lv : enc.levels) {
         if (lv.R == 0) continue;
+        if (bytes && lv.off == 0) {
+            gather_bytes_kernel<<<(unsigned)((lv.R + 7) / 8), 256, 0, s>>>(
+                bytes, rows, lv.n, lv.R, enc.d_ptr + lv.c_ptr, enc.d_src + lv.c_edge, enc.d_w + lv.c_edge);
+            dev_free(bytes, s);
+            bytes = nullptr;
+            if (!launch_ok("orion C gather (bytes)")) return false;
+            continue;
+        }
         gather_kernel<<<(unsigned)((lv.R + 7) / 8), 256, 0, s>>>(rows, lv.off, lv.off + lv.n, lv.R,
                                                                   enc.d_ptr + lv.c_ptr, enc.d_src + lv.c_edge,
                                                                   enc.d_w + lv.c_edge);
         if (!launch_ok("orion C gather")) return false;
     }
+    if (bytes) dev_free(bytes, s);
     // 3. D multiplications, innermost depth first
     for (auto it = enc.levels.rbegin(); it != enc.levels.rend(); ++it) {
         const Level& lv = *it;
@@ -503,7 +592,7 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
         if (!launch_ok("orion D gather")) return false;
     }
     // 4. row leaves, constant leaves for the zero rows and the tree padding
-    leaf_kernel<<<(unsigned)((cw_len + kLeafRows - 1) / kLeafRows), kLeafRows, 0, s>>>(rows, cw_len, tree, size);
+    leaf_kernel<<<(unsigned)((cw_len + kLeafRows - 1) / kLeafRows), kLeafRows, 0, s>>>(rows, cw_len, tree, size, 1u);
     if (!launch_ok("orion leaves")) return false;
     if (size > cw_len) {
         unsigned char zr[32], zb[32];
@@ -529,7 +618,7 @@ bool build_tree(unsigned char* tree, long long leaves, cudaStream_t s)
         int levels = 0;
         while (levels < 9 && (1LL << (levels + 1)) <= n_in) ++levels;
         const long long blocks = n_in >> levels;
-        tree_kernel<<<(unsigned)blocks, 1 << (levels - 1), 0, s>>>(tree, n_in, levels);
+        tree_kernel<<<(unsigned)blocks, 1 << (levels - 1), 0, s>>>(tree, n_in, levels, 1u);
         if (!launch_ok("merkle tree")) return false;
         n_in >>= levels;
     }

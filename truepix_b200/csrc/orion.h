@@ -45,6 +45,7 @@ struct Encoder {
     long long cw_len = 0;
     std::vector<Level> levels;         // depths with n > kThreshold, outermost first
     long long n_ptr = 0, n_edges = 0;
+    unsigned max_c0_in_degree = 0;     // largest in-degree of the depth-0 C graph
     unsigned* d_ptr = nullptr;         // [n_ptr] first edge of each target (per graph, + 1 end)
     unsigned* d_src = nullptr;         // [n_edges] source row within the graph's source range
     ulonglong2* d_w = nullptr;         // [n_edges] weights {img, real}, canonical

@@ -14,7 +14,7 @@ constexpr int kSlices = 64;   // 2^log_slice_number (include/infrastructure/cons
 // leaf j: h <- SHA256(x || y || h) over the 64 slices (fri.cpp:96-110: the pair
 // first, the running digest second -- the opposite order of the Orion row leaves)
 __global__ void __launch_bounds__(256) fri_leaf_kernel(const ulonglong2* __restrict__ l_eval, long long slice,
-                                                       unsigned char* __restrict__ tree)
+                                                       unsigned char* __restrict__ tree, uint32_t one)
 {
     const long long half = slice >> 1;
     const long long j = (long long)blockIdx.x * 256 + threadIdx.x;
@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(256) fri_leaf_kernel(const ulonglong2* __restr
         sha::fe_words(y.x, y.y, w + 4);
 #pragma unroll
         for (int k = 0; k < 8; ++k) w[8 + k] = st[k];
-        sha::hash64(w, st);
+        sha::hash64(w, st, sha::AddMad{one});
     }
     uint4 a, b;
     a.x = sha::bswap32(st[0]); a.y = sha::bswap32(st[1]); a.z = sha::bswap32(st[2]); a.w = sha::bswap32(st[3]);
@@ -59,7 +59,7 @@ bool commit(const ulonglong2* src, int log_len, ulonglong2* l_eval, unsigned cha
     if (!ok) return false;
     if (cuda_failed(cudaMemsetAsync(tree, 0, 32, s), "rs tree clear")) return false;
     const long long half = slice >> 1;
-    fri_leaf_kernel<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(l_eval, slice, tree);
+    fri_leaf_kernel<<<(unsigned)((half + 255) / 256), 256, 0, s>>>(l_eval, slice, tree, 1u);
     if (cuda_failed(cudaGetLastError(), "rs leaves")) return false;
     return orion::build_tree(tree, half, s);
 }

@@ -72,19 +72,33 @@ __host__ __device__ __forceinline__ void init(uint32_t st[8])
     st[4] = 0x510e527fu; st[5] = 0x9b05688cu; st[6] = 0x1f83d9abu; st[7] = 0x5be0cd19u;
 }
 
+// Additions. On the device the SHA-256 rounds are bound by the integer ALU pipe
+// (funnel shifts and LOP3 for the sigma/choice/majority functions); routing the
+// additions through the multiply-add pipe as x * one + y, with `one` == 1 known
+// only at run time, takes them off that pipe. The host adds directly.
+struct AddAlu {
+    __host__ __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const { return a + b; }
+};
+struct AddMad {
+    uint32_t one;   // 1, passed in at run time
+    __host__ __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const { return a * one + b; }
+};
+
 #define TP_SHA_ROUND(a, b, c, d, e, f, g, h, kw)                                          \
     do {                                                                                  \
-        const uint32_t t1 = h + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) +                \
-                            ((e & f) ^ (~e & g)) + (kw);                                  \
-        const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) +                    \
-                            ((a & b) ^ (a & c) ^ (b & c));                                \
-        d += t1;                                                                          \
-        h = t1 + t2;                                                                      \
+        const uint32_t s1 = rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25);                       \
+        const uint32_t ch = (e & f) ^ (~e & g);                                           \
+        const uint32_t t1 = add(add(add(h, s1), ch), (kw));                               \
+        const uint32_t s0 = rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22);                       \
+        const uint32_t mj = (a & b) ^ (a & c) ^ (b & c);                                  \
+        d = add(d, t1);                                                                   \
+        h = add(t1, add(s0, mj));                                                         \
     } while (0)
 
 // one compression of the message block w[16] into st[8] (w is consumed as the
 // rolling schedule)
-__host__ __device__ __forceinline__ void compress(uint32_t st[8], uint32_t w[16])
+template <class Add>
+__host__ __device__ __forceinline__ void compress(uint32_t st[8], uint32_t w[16], Add add)
 {
     constexpr Tables T = make_tables();
     uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
@@ -95,25 +109,26 @@ __host__ __device__ __forceinline__ void compress(uint32_t st[8], uint32_t w[16]
             for (int j = 0; j < 8; ++j) {
                 const int t = i + j;
                 const uint32_t x = w[(t - 15) & 15], y = w[(t - 2) & 15];
-                w[t & 15] += (rotr(x, 7) ^ rotr(x, 18) ^ (x >> 3)) + w[(t - 7) & 15] +
-                             (rotr(y, 17) ^ rotr(y, 19) ^ (y >> 10));
+                w[t & 15] = add(add(w[t & 15], rotr(x, 7) ^ rotr(x, 18) ^ (x >> 3)),
+                                add(w[(t - 7) & 15], rotr(y, 17) ^ rotr(y, 19) ^ (y >> 10)));
             }
         }
-        TP_SHA_ROUND(a, b, c, d, e, f, g, h, T.k[i + 0] + w[(i + 0) & 15]);
-        TP_SHA_ROUND(h, a, b, c, d, e, f, g, T.k[i + 1] + w[(i + 1) & 15]);
-        TP_SHA_ROUND(g, h, a, b, c, d, e, f, T.k[i + 2] + w[(i + 2) & 15]);
-        TP_SHA_ROUND(f, g, h, a, b, c, d, e, T.k[i + 3] + w[(i + 3) & 15]);
-        TP_SHA_ROUND(e, f, g, h, a, b, c, d, T.k[i + 4] + w[(i + 4) & 15]);
-        TP_SHA_ROUND(d, e, f, g, h, a, b, c, T.k[i + 5] + w[(i + 5) & 15]);
-        TP_SHA_ROUND(c, d, e, f, g, h, a, b, T.k[i + 6] + w[(i + 6) & 15]);
-        TP_SHA_ROUND(b, c, d, e, f, g, h, a, T.k[i + 7] + w[(i + 7) & 15]);
+        TP_SHA_ROUND(a, b, c, d, e, f, g, h, add(w[(i + 0) & 15], T.k[i + 0]));
+        TP_SHA_ROUND(h, a, b, c, d, e, f, g, add(w[(i + 1) & 15], T.k[i + 1]));
+        TP_SHA_ROUND(g, h, a, b, c, d, e, f, add(w[(i + 2) & 15], T.k[i + 2]));
+        TP_SHA_ROUND(f, g, h, a, b, c, d, e, add(w[(i + 3) & 15], T.k[i + 3]));
+        TP_SHA_ROUND(e, f, g, h, a, b, c, d, add(w[(i + 4) & 15], T.k[i + 4]));
+        TP_SHA_ROUND(d, e, f, g, h, a, b, c, add(w[(i + 5) & 15], T.k[i + 5]));
+        TP_SHA_ROUND(c, d, e, f, g, h, a, b, add(w[(i + 6) & 15], T.k[i + 6]));
+        TP_SHA_ROUND(b, c, d, e, f, g, h, a, add(w[(i + 7) & 15], T.k[i + 7]));
     }
-    st[0] += a; st[1] += b; st[2] += c; st[3] += d;
-    st[4] += e; st[5] += f; st[6] += g; st[7] += h;
+    st[0] = add(st[0], a); st[1] = add(st[1], b); st[2] = add(st[2], c); st[3] = add(st[3], d);
+    st[4] = add(st[4], e); st[5] = add(st[5], f); st[6] = add(st[6], g); st[7] = add(st[7], h);
 }
 
 // the second compression of a 64-byte message: constant block, constant schedule
-__host__ __device__ __forceinline__ void compress_pad64(uint32_t st[8])
+template <class Add>
+__host__ __device__ __forceinline__ void compress_pad64(uint32_t st[8], Add add)
 {
     constexpr Tables T = make_tables();
     uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
@@ -128,16 +143,17 @@ __host__ __device__ __forceinline__ void compress_pad64(uint32_t st[8])
         TP_SHA_ROUND(c, d, e, f, g, h, a, b, T.pad_kw[i + 6]);
         TP_SHA_ROUND(b, c, d, e, f, g, h, a, T.pad_kw[i + 7]);
     }
-    st[0] += a; st[1] += b; st[2] += c; st[3] += d;
-    st[4] += e; st[5] += f; st[6] += g; st[7] += h;
+    st[0] = add(st[0], a); st[1] = add(st[1], b); st[2] = add(st[2], c); st[3] = add(st[3], d);
+    st[4] = add(st[4], e); st[5] = add(st[5], f); st[6] = add(st[6], g); st[7] = add(st[7], h);
 }
 
 // SHA-256 of the 64-byte message given as 16 big-endian words; out = state words
-__host__ __device__ __forceinline__ void hash64(uint32_t w[16], uint32_t out[8])
+template <class Add = AddAlu>
+__host__ __device__ __forceinline__ void hash64(uint32_t w[16], uint32_t out[8], Add add = Add())
 {
     init(out);
-    compress(out, w);
-    compress_pad64(out);
+    compress(out, w, add);
+    compress_pad64(out, add);
 }
 
 // The message words of a field element (16 bytes: u64 img then u64 real, both
