@@ -58,9 +58,19 @@ int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_
                                int n_wires, int const_idx, uint64_t const_val, void* d_rows,
                                void* d_tree, void* stream);
 
+/* Kernels launched by the calling thread's last commit (any of the three forms). */
+int tp_orion_last_launches(void);
+
 /* Row-major codeword (as written by the commits above) -> column-major
  * (encoded_codeword[c][r]); d_cols holds 128 * cw_len elements. */
 int tp_orion_rows_to_columns_dev(const void* d_rows, long long cw_len, void* d_cols, void* stream);
+
+/* Measurement entry point, no counterpart in the reference: the register-only
+ * throughput of the library's SHA-256 code. blocks x 128 threads each chain
+ * `iters` SHA-256 of a 64-byte message (2 compressions each) and XOR their last
+ * digest word into *d_out (4 bytes, device). Used as the compute roof of the
+ * Merkle leaf kernels. */
+int tp_sha256_peak_dev(int blocks, int iters, void* d_out, void* stream);
 
 /* ---- Fp2 NTT (src/infrastructure/RS_polynomial.cpp) ------------------------ */
 

@@ -18,6 +18,9 @@ namespace {
 
 thread_local int g_launches = 0;
 
+// kernel-timer tags (runtime.h timer_*): commit kernels are 9100 + kind
+constexpr int kTagLoad = 9100, kTagGatherBytes = 9101, kTagGather = 9102, kTagLeaf = 9103, kTagTree = 9104;
+
 // glibc rand(): the TYPE_3 additive generator (degree 31, separation 3) that
 // glibc uses by default. Seeded like srand(seed): r[0] = seed, r[i] = 16807 *
 // r[i-1] mod (2^31 - 1) for i < 31, r[31..33] = r[0..2], then 310 outputs are
@@ -414,6 +417,27 @@ __global__ void __launch_bounds__(256) tree_kernel(unsigned char* __restrict__ t
     }
 }
 
+// Register-only throughput of the same SHA-256 code (the compute roof of the
+// leaf kernels): every thread chains `iters` hashes of a 64-byte message made of
+// its previous digest and a counter, no memory traffic.
+__global__ void __launch_bounds__(kLeafRows) sha_peak_kernel(int iters, uint32_t one, uint32_t* out)
+{
+    uint32_t st[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) st[i] = threadIdx.x + 977u * blockIdx.x + i;
+#pragma unroll 1
+    for (int it = 0; it < iters; ++it) {
+        uint32_t w[16];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            w[i] = st[i];
+            w[8 + i] = st[i] ^ (uint32_t)it;
+        }
+        sha::hash64(w, st, sha::AddMad{one});
+    }
+    atomicXor(out, st[0] ^ st[1] ^ st[2] ^ st[3] ^ st[4] ^ st[5] ^ st[6] ^ st[7]);
+}
+
 bool launch_ok(const char* what)
 {
     ++g_launches;
@@ -528,6 +552,12 @@ const Encoder* encoder(long long col_len)
 
 int last_launches() { return g_launches; }
 
+bool sha_peak(int blocks, int iters, uint32_t* out, cudaStream_t s)
+{
+    sha_peak_kernel<<<blocks, kLeafRows, 0, s>>>(iters, 1u, out);
+    return launch_ok("sha256 peak");
+}
+
 unsigned transpose_grid(long long n_r, long long n_c) { return (unsigned)(((n_r + 31) / 32) * ((n_c + 31) / 32)); }
 
 bool rows_to_columns(const ulonglong2* rows, long long cw_len, ulonglong2* cols, cudaStream_t s)
@@ -547,7 +577,9 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
     // 1. the message: column-major input -> rows [0, col_len)
     unsigned char* bytes = nullptr;
     if (src) {
+        timer_begin(s, kTagLoad);
         transpose_kernel<<<transpose_grid(kColumns, col_len), 256, 0, s>>>(src, rows, kColumns, col_len);
+        timer_end(s);
         if (!launch_ok("orion load columns")) return false;
     } else {
         int w_shift = 0;
@@ -558,7 +590,9 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
             bytes = static_cast<unsigned char*>(dev_alloc((size_t)n, s));
             if (!bytes) return false;
         }
+        timer_begin(s, kTagLoad);
         pixel_rows_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(*px, col_len, w_shift, rows, bytes);
+        timer_end(s);
         if (!launch_ok("orion load pixels")) {
             if (bytes) dev_free(bytes, s);
             return false;
@@ -568,16 +602,20 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
     for (const Level& lv : enc.levels) {
         if (lv.R == 0) continue;
         if (bytes && lv.off == 0) {
+            timer_begin(s, kTagGatherBytes);
             gather_bytes_kernel<<<(unsigned)((lv.R + 7) / 8), 256, 0, s>>>(
                 bytes, rows, lv.n, lv.R, enc.d_ptr + lv.c_ptr, enc.d_src + lv.c_edge, enc.d_w + lv.c_edge);
+            timer_end(s);
             dev_free(bytes, s);
             bytes = nullptr;
             if (!launch_ok("orion C gather (bytes)")) return false;
             continue;
         }
+        timer_begin(s, kTagGather);
         gather_kernel<<<(unsigned)((lv.R + 7) / 8), 256, 0, s>>>(rows, lv.off, lv.off + lv.n, lv.R,
                                                                   enc.d_ptr + lv.c_ptr, enc.d_src + lv.c_edge,
                                                                   enc.d_w + lv.c_edge);
+        timer_end(s);
         if (!launch_ok("orion C gather")) return false;
     }
     if (bytes) dev_free(bytes, s);
@@ -586,13 +624,17 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
         const Level& lv = *it;
         if (lv.RD == 0) continue;
         const long long next = lv.off + lv.n;
+        timer_begin(s, kTagGather);
         gather_kernel<<<(unsigned)((lv.RD + 7) / 8), 256, 0, s>>>(rows, next, next + lv.L, lv.RD,
                                                                    enc.d_ptr + lv.d_ptr, enc.d_src + lv.d_edge,
                                                                    enc.d_w + lv.d_edge);
+        timer_end(s);
         if (!launch_ok("orion D gather")) return false;
     }
     // 4. row leaves, constant leaves for the zero rows and the tree padding
+    timer_begin(s, kTagLeaf);
     leaf_kernel<<<(unsigned)((cw_len + kLeafRows - 1) / kLeafRows), kLeafRows, 0, s>>>(rows, cw_len, tree, size, 1u);
+    timer_end(s);
     if (!launch_ok("orion leaves")) return false;
     if (size > cw_len) {
         unsigned char zr[32], zb[32];
@@ -618,7 +660,9 @@ bool build_tree(unsigned char* tree, long long leaves, cudaStream_t s)
         int levels = 0;
         while (levels < 9 && (1LL << (levels + 1)) <= n_in) ++levels;
         const long long blocks = n_in >> levels;
+        timer_begin(s, kTagTree);
         tree_kernel<<<(unsigned)blocks, 1 << (levels - 1), 0, s>>>(tree, n_in, levels, 1u);
+        timer_end(s);
         if (!launch_ok("merkle tree")) return false;
         n_in >>= levels;
     }

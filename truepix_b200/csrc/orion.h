@@ -87,6 +87,10 @@ bool build_tree(unsigned char* tree, long long leaves, cudaStream_t s);
 // rows -> column-major codeword (the reference's encoded_codeword[c][r])
 bool rows_to_columns(const ulonglong2* rows, long long cw_len, ulonglong2* cols, cudaStream_t s);
 
+// `blocks` CTAs of 128 threads, each thread chaining `iters` SHA-256 of 64 bytes
+// in registers (2 compressions each); XORs its last digest into *out
+bool sha_peak(int blocks, int iters, uint32_t* out, cudaStream_t s);
+
 // launches issued by commit() / build_tree() on this thread since the last commit()
 int last_launches();
 

@@ -95,6 +95,21 @@ int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_
                : -1;
 }
 
+int tp_orion_last_launches(void) { return tp::orion::last_launches(); }
+
+int tp_sha256_peak_dev(int blocks, int iters, void* d_out, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (blocks <= 0 || iters <= 0 || !d_out) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_sha256_peak_dev: bad arguments");
+        return -1;
+    }
+    return tp::orion::sha_peak(blocks, iters, static_cast<uint32_t*>(d_out), reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
 int tp_orion_rows_to_columns_dev(const void* d_rows, long long cw_len, void* d_cols, void* stream)
 {
     tp::clear_error();

@@ -81,6 +81,8 @@ GKR_SIGNATURES = {
     "tp_orion_commit_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP, _VP]),
     "tp_orion_commit_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
     "tp_orion_rows_to_columns_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP]),
+    "tp_orion_last_launches": (_I32, []),
+    "tp_sha256_peak_dev": (_I32, [_I32, _I32, _VP, _VP]),
     "tp_fft": (_I32, [_VP, _I32, _I32, _VP]),
     "tp_ifft": (_I32, [_VP, _I32, _I32, _VP]),
     "tp_fft_dev": (_I32, [_VP, ctypes.c_longlong, ctypes.c_longlong, _VP, _I32, ctypes.c_longlong,

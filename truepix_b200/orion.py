@@ -1,0 +1,63 @@
+"""Orion input-layer commitment of frames on the device (include/orion_gpu.h).
+
+The reference commits a frame in its `linearPC_multi_commit` process
+(TruePix-main/Orion/Orion_nonzk/examples/multivariate_PC_test_commit.cpp:120-155):
+load the 2^(9 + nCopyBits) input vector in TruePix's layout
+(include/truepix/truepix_gkr.h:107-206), expander_init, commit() -> Merkle tree,
+root printed by root_hex. Here each frame is committed straight from its uint8
+bytes on the GPU; the codeword (kept for the opening, as the reference's
+set_retain_encoded_codeword(true) keeps it) and the tree stay in HBM.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import native
+
+
+class FrameCommitter:
+    """Commits frames of the given layouts (truepix_b200.frame.FrameLayout) from
+    their device bytes. One codeword (cw_len x 128 elements, row-major) and one
+    tree (2 * leaves digests) per frame, allocated once and reused."""
+
+    def __init__(self, layouts, device: int = 0, stream=None):
+        import torch
+        self.torch = torch
+        self.lib = native.gkr()
+        self.layouts = list(layouts)
+        self.dev = torch.device("cuda", device)
+        self.stream = stream
+        self.rows, self.trees, self.cw_len, self.leaves = [], [], [], []
+        for L in self.layouts:
+            n = L.padded_copies * L.n_wires
+            cw = self.lib.tp_orion_codeword_len(n // 128)
+            lv = self.lib.tp_orion_tree_leaves(n)
+            self.cw_len.append(cw)
+            self.leaves.append(lv)
+            self.rows.append(torch.empty(2 * 128 * cw, dtype=torch.int64, device=self.dev))
+            self.trees.append(torch.empty(64 * lv, dtype=torch.uint8, device=self.dev))
+        self.launches_last = 0
+
+    def _s(self):
+        return self.stream.cuda_stream if self.stream is not None else \
+            self.torch.cuda.current_stream(self.dev).cuda_stream
+
+    def commit(self, pixels) -> None:
+        """Queue the commits of all frames (pixels: one uint8 device tensor each)."""
+        lib, s = self.lib, self._s()
+        launches = 0
+        for f, L in enumerate(self.layouts):
+            native.check(lib, lib.tp_orion_commit_pixels_dev(
+                pixels[f].data_ptr(), L.copies, L.padded_copies, L.copy_size, L.n_wires,
+                L.const_idx, L.const_val, self.rows[f].data_ptr(), self.trees[f].data_ptr(), s),
+                "orion commit")
+            launches += lib.tp_orion_last_launches()
+        self.launches_last = launches
+
+    def root(self, f: int) -> bytes:
+        return self.trees[f][32:64].cpu().numpy().tobytes()
+
+    def root_hex(self, f: int) -> str:
+        """truepix::root_hex: the digest's little-endian u64 words as hi(h0) lo(h0) hi(h1) lo(h1)."""
+        w = np.frombuffer(self.root(f), np.uint64)
+        return "%016x%016x%016x%016x" % (w[1], w[0], w[3], w[2])
