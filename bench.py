@@ -1,32 +1,41 @@
-"""Benchmark: proved 1080p frames/s on one B200 (GKR input layer of the gray circuit).
+"""Benchmark: proved 1080p frames/s on one B200 (device prover core of TruePix).
 
 Workload: seeded 1920x1080x3 uint8 frames; each frame is 16,200 copies of 384
-bytes padded to 16,384 x 512 input wires (2^23) and is proven by the
-device-resident path (truepix_b200.frame): beta over the 14 copy challenges, 14
-early sumcheck rounds (claim + fold; rounds 0 and 1 read the frame's bytes),
-finish, and the MLE of the 2^23-entry input vector at the final point.
+bytes padded to 16,384 x 512 input wires (2^23). One frame's device work:
 
-One step = one batch of B frames (default 64) proven together, one kernel
-launch per round for the whole batch (BatchFrameProver). Inputs stay in HBM:
-B distinct frames (400 MB of bytes) and their folded tables (~4.8 GB) are far
-larger than the 126 MB L2, so no flush is needed.
+  GKR input layer (truepix_b200.frame): beta over the 14 copy challenges, 14
+    early sumcheck rounds (claim + fold; rounds 0 and 1 read the frame's bytes),
+    finish, and the MLE of the 2^23-entry input vector at the final point;
+  Orion input commitment (truepix_b200.orion): expander encode of the 128
+    columns and the SHA-256 Merkle tree over the 2^17 codeword rows, read from
+    the bytes; codeword and tree stay in HBM for the opening.
 
-  value         frames/s over all ranks, device time (CUDA events), batched
-  plain         frames/s of single-frame proofs (one session per frame), same
-                device timing -- the batched/plain ratio is reported
-  e2e           the batched path from pinned host frames: H2D of the bytes, and
-                every round a D2H of all claims with a synchronise (the host
-                needs them for its transcript) inside the timed region
-  e2e_reference_abi  one frame through the reference C ABI (native_fp2_*) with
-                pinned host SoA tables
-  roofline      the claim kernel with the largest share: algorithmic bytes (per
-                launch kind, see kernel_groups) / its event-timed duration,
-                against MEASURED_PEAKS.json
-  cpu_baseline  the reference CPU library (built from the reference's source)
-                proving one frame of the same workload on one host core
+One step = one batch of B frames (default 64): one kernel launch per sumcheck
+round for the whole batch (BatchFrameProver), then the B commits. Inputs stay
+in HBM: B frames (400 MB of bytes), their folded tables (~4.8 GB) and
+codewords (14.8 GB) are far larger than the 126 MB L2, so no flush is needed.
 
-`--impl reference` times that reference CPU library on all host cores instead
-(one frame per worker process per step) and prints the same metric.
+  value         frames/s over all ranks, device time (CUDA events)
+  breakdown     the step split into its GKR part and its commit part, and the
+                GKR part alone batched vs one frame at a time (`plain`)
+  kernels       every kernel kind of the step: launches, time share, algorithmic
+                bytes, achieved GB/s (the library's kernel timer, CUDA events)
+  roofline      the kernel with the largest share, against MEASURED_PEAKS.json;
+                for the SHA-256 leaf kernel also compressions/s against the
+                register-only throughput of the same SHA-256 code
+  ntt           the Fp2 NTT / IFFT / rate-2^-5 RS commit microbenchmark at
+                2^16, 2^20, 2^24 points
+  e2e           the batched path from pinned host frames: H2D of the bytes, a
+                D2H of all claims after every round with a synchronise (the host
+                transcript needs them), D2H of wires, MLEs and commitment roots
+  e2e_reference_abi  one frame through the reference-facing C ABI with host
+                buffers (native_fp2_* and tp_orion_commit)
+  cpu_baseline  the reference CPU implementation (native_fp2.cpp and the Orion
+                sources, built from the reference by oracle/Makefile) proving one
+                frame of the same workload on one host core
+
+`--impl reference` times that reference CPU implementation on all host cores
+instead (one frame per worker process per step) and prints the same metric.
 """
 from __future__ import annotations
 
@@ -41,8 +50,10 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+from truepix_b200 import native  # noqa: E402
 
-METRIC = "1080p proved frames/s (GKR input layer, gray circuit)"
+METRIC = "1080p proved frames/s (GKR input-layer sumcheck + input MLE + Orion input commitment, gray circuit)"
+WORKLOAD = "prover_core_gray_1080p"
 UNIT = "frames/s"
 H, Wd = 1080, 1920
 P61 = (1 << 61) - 1
@@ -79,8 +90,9 @@ def host_tables(pix, layout):
 
 
 # --------------------------------------------------------------------------
-# CPU side: reference library (oracle/_ref, built from the reference source) or
-# the oracle port when that build is absent.
+# CPU side: the reference implementation (oracle/_ref, built from the reference
+# sources: native_fp2.cpp and the Orion commit) or the oracle ports when those
+# builds are absent.
 
 def cpu_lib():
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -92,13 +104,44 @@ def cpu_lib():
     return Fp2Lib(ORACLE_LIB, "oracle_fp2_"), "port"
 
 
-def cpu_prove_frame(lib, gt, i0, i1, z1, z2, point, chal, table, inputs, layout):
+def cpu_commit_fn():
+    """fn(elements) -> 32-byte root: the reference's commit() (ref_commit of
+    oracle/_ref/liborion_ref.so) or the oracle's restatement."""
+    import ctypes
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from orionlib import ORION_REF_LIB, ORION_ORACLE_LIB, OrionOracle
+    V = ctypes.c_void_p
+    if os.path.exists(ORION_REF_LIB):
+        lib = ctypes.CDLL(ORION_REF_LIB)
+        lib.ref_commit.argtypes = [V, ctypes.c_longlong, V, V]
+
+        def fn(src):
+            root, hx = ctypes.create_string_buffer(32), ctypes.create_string_buffer(80)
+            lib.ref_commit(V(src.ctypes.data), src.size // 2, root, hx)
+            return root.raw
+        return fn, "reference"
+    if not os.path.exists(ORION_ORACLE_LIB):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"])
+    orc = OrionOracle()
+    return orc.commit, "port"
+
+
+def cpu_prove_frame(lib, commit, gt, i0, i1, z1, z2, point, chal, table, inputs, elems, layout):
     from fp2lib import run_session
     C, W = layout.padded_copies, layout.n_wires
     bre, bim = lib.compute_beta(np.ascontiguousarray(z2[:, 0]), np.ascontiguousarray(z2[:, 1]),
                                 (1, 0))
     run_session(lib, gt, i0, i1, z1[0], z1[1], C, W, table, np.zeros_like(table), bre, bim, chal)
     lib.mle_eval_base(inputs, np.ascontiguousarray(point[:, 0]), np.ascontiguousarray(point[:, 1]))
+    return commit(elems)
+
+
+def frame_elements(pix, layout):
+    """The commit input of a frame: element copy * W + wire (img 0, real value)."""
+    _, inputs = host_tables(pix, layout)
+    out = np.zeros(2 * inputs.size, np.uint64)
+    out[1::2] = inputs
+    return out
 
 
 def _cpu_worker(args):
@@ -108,39 +151,52 @@ def _cpu_worker(args):
     rng = np.random.default_rng(SEED + idx)
     frames, z1, z2, point, chal = make_inputs(rng, layout, 1)
     table, inputs = host_tables(frames[0], layout)
+    elems = frame_elements(frames[0], layout)
     lib, kind = cpu_lib()
+    commit, ckind = cpu_commit_fn()
     gt, i0, i1 = circuit()
     t0 = time.perf_counter()
     for _ in range(n_frames):
-        cpu_prove_frame(lib, gt, i0, i1, z1, z2, point, chal, table, inputs, layout)
-    return time.perf_counter() - t0, kind
+        cpu_prove_frame(lib, commit, gt, i0, i1, z1, z2, point, chal, table, inputs, elems, layout)
+    return time.perf_counter() - t0, kind if kind == ckind else kind + "+" + ckind
 
 
 def reference_arm(args, rank, world):
-    """The reference CPU implementation on all host cores (rank 0 only)."""
+    """The reference CPU implementation on all host cores (rank 0 only). One step
+    = one frame per worker process; at most 6 timed frames per worker (a frame
+    takes ~7 s on one core), so the run ends within a few minutes."""
     if rank != 0:
         return
     import multiprocessing as mp
     workers = max(1, min(os.cpu_count() or 1, 64))
+    try:
+        import psutil
+        workers = max(1, min(workers, int(psutil.virtual_memory().available / 1.2e9)))
+    except Exception:
+        pass
+    per_worker = max(1, min(args.steps, 6))
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers) as pool:
-        for _ in range(args.warmup and 1):      # one warm-up frame per worker
-            pool.map(_cpu_worker, [(i, 1) for i in range(workers)])
+        pool.map(_cpu_worker, [(i, 1) for i in range(workers)])     # warm-up frame
         t0 = time.perf_counter()
-        res = pool.map(_cpu_worker, [(i, args.steps) for i in range(workers)])
+        res = pool.map(_cpu_worker, [(i, per_worker) for i in range(workers)])
         wall = time.perf_counter() - t0
     kind = res[0][1]
-    frames = workers * args.steps
+    frames = workers * per_worker
     value = frames / wall
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / per_worker,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Fp2)",
         "data": "synthetic",
-        "config": {"workload": "gkr_input_layer_gray_1080p", "frame": [H, Wd, 3],
-                   "copies": 16200, "wires": 1 << 23, "circuit": "gray.pws"},
+        "config": {"workload": WORKLOAD, "frame": [H, Wd, 3],
+                   "copies": 16200, "wires": 1 << 23, "circuit": "gray.pws",
+                   "per_frame": "compute_beta + 14 early rounds + finish + MLE over 2^23 inputs "
+                                "(native_fp2.cpp) + Orion commit of the 2^23 inputs (commit(), "
+                                "expander_init in the same process)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": kind,
-                         "sample": f"{args.steps} frames per worker process x {workers} processes"},
+                         "sample": f"{per_worker} timed frames per worker process x {workers} "
+                                   f"processes after one warm-up frame each"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
     }
@@ -224,43 +280,150 @@ def profiled_traffic():
     return None
 
 
-def kernel_groups(ms, tags, layout, batch=1):
-    """Per claim-kernel kind: launches, total time, algorithmic bytes, folded elements.
-    tag = 1000*(reads bytes) + 100*(fold fused) + log2(copies claimed per frame).
-    Algorithmic bytes per frame: bytes read once + folded Fp2 rows written (16 B
-    per element) + table rows read (16 B per element) + beta."""
+COMMIT_TAGS = {9100: "pixel_rows_kernel", 9101: "gather_bytes_kernel", 9102: "gather_kernel",
+               9103: "leaf_kernel", 9104: "tree_kernel"}
+
+
+def kernel_groups(ms, tags, layout, batch=1, cw_len=0, leaves=0):
+    """Per kernel kind: launches, total time, algorithmic bytes, folded elements,
+    SHA-256 compressions.
+    Claim kernels: tag = 1000*(reads bytes) + 100*(fold fused) + log2(copies
+    claimed per frame); algorithmic bytes per frame = bytes read once + folded Fp2
+    rows written (16 B per element) + table rows read (16 B per element) + beta.
+    Commit kernels (tags 9100-9104), per frame: pixel rows = bytes read + 16 B per
+    codeword-message element written; leaves = 2 KB read + 32 B written per
+    codeword row, 128 compressions per row; tree = 64 B read + 32 B written and 2
+    compressions per node; gathers: see ntt/commit notes (one 2 KB row read per
+    edge, L2-resident), their bytes are the rows written."""
     rows = layout.const_idx + 1 if layout.const_idx >= 0 else layout.copy_size
     pix_bytes = layout.copies * layout.copy_size
+    col_len = layout.padded_copies * layout.n_wires // 128
     groups = {}
     for t, tag in zip(ms, tags):
-        pix, fold, lg = tag // 1000, (tag // 100) % 10, tag % 100
-        n = 1 << lg                                    # copies claimed
-        if pix and not fold:
-            name, byt, el = "pix_claim_kernel", pix_bytes + 16 * n, 0
-        elif pix and fold:
-            name, byt, el = "pix_fold_claim_kernel", pix_bytes + 16 * rows * n + 48 * n, rows * n
-        elif fold:
-            name, byt, el = "table_round_kernel<fold>", 48 * rows * n + 48 * n, rows * n
+        comp = 0
+        n = 0
+        if tag >= 9000:
+            name = COMMIT_TAGS.get(tag, "commit_kernel_%d" % tag)
+            if name == "pixel_rows_kernel":
+                byt, el = pix_bytes + 16 * 128 * col_len + 128 * col_len, 0
+            elif name == "leaf_kernel":
+                byt, el, comp = 2048 * cw_len + 32 * cw_len, 0, 128 * cw_len
+            elif name == "tree_kernel":
+                byt, el, comp = 0, 0, 0          # attributed below per frame
+            else:
+                byt, el = 0, 0
         else:
-            name, byt, el = "table_round_kernel<claim>", 16 * rows * n + 16 * n, 0
+            pix, fold, lg = tag // 1000, (tag // 100) % 10, tag % 100
+            n = 1 << lg                                    # copies claimed
+            if pix and not fold:
+                name, byt, el = "pix_claim_kernel", pix_bytes + 16 * n, 0
+            elif pix and fold:
+                name, byt, el = "pix_fold_claim_kernel", pix_bytes + 16 * rows * n + 48 * n, rows * n
+            elif fold:
+                name, byt, el = "table_round_kernel<fold>", 48 * rows * n + 48 * n, rows * n
+            else:
+                name, byt, el = "table_round_kernel<claim>", 16 * rows * n + 16 * n, 0
         g = groups.setdefault(name, {"launches": 0, "ms": 0.0, "bytes": 0.0, "folded": 0,
-                                     "by_copies": {}})
+                                     "compressions": 0.0, "by_copies": {}})
+        per_launch = batch if tag < 9000 else 1    # a claim launch serves the whole batch
         g["launches"] += 1
         g["ms"] += t
-        g["bytes"] += byt * batch
-        g["folded"] += el * batch
-        bc = g["by_copies"].setdefault(n, [0, 0.0])
-        bc[0] += 1
-        bc[1] += t
+        g["bytes"] += byt * per_launch
+        g["folded"] += el * per_launch
+        g["compressions"] += comp
+        if n:
+            bc = g["by_copies"].setdefault(n, [0, 0.0])
+            bc[0] += 1
+            bc[1] += t
+    if "tree_kernel" in groups and leaves:
+        g = groups["tree_kernel"]
+        frames = g["launches"] / max(1, tree_launches(leaves))
+        g["bytes"] = frames * 96 * (leaves - 1)
+        g["compressions"] = frames * 2 * (leaves - 1)
     return groups
+
+
+def tree_launches(leaves):
+    n, k = leaves, 0
+    while n > 1:
+        lv = 0
+        while lv < 9 and (1 << (lv + 1)) <= n:
+            lv += 1
+        n >>= lv
+        k += 1
+    return k
+
+
+def sha_peak(lib, dev, stream):
+    """G compressions/s of the library's SHA-256 code in registers, full device."""
+    import torch
+    out = torch.zeros(1, dtype=torch.int32, device=dev)
+    blocks, iters = 148 * 16, 256
+    s = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        native.check(lib, lib.tp_sha256_peak_dev(blocks, 16, out.data_ptr(), s), "sha peak")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        native.check(lib, lib.tp_sha256_peak_dev(blocks, iters, out.data_ptr(), s), "sha peak")
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return blocks * 128 * iters * 2 / (ms / 1e3) / 1e9
+
+
+def ntt_bench(lib, dev, stream, reps=5):
+    """Config-2 microbenchmark: forward NTT, inverse NTT and the rate-2^-5 RS
+    commit (IFFT + FFT per slice, FRI leaf chains, Merkle tree) at 2^16, 2^20, 2^24."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from orionlib import elements
+    s = stream.cuda_stream
+    out = {}
+    for lg in (16, 20, 24):
+        n = 1 << lg
+        a = torch.from_numpy(elements(lg, n).view(np.int64)).to(dev)
+        f = torch.empty_like(a)
+        back = torch.empty_like(a)
+        cw = torch.empty(2 << (lg + 5), dtype=torch.int64, device=dev)
+        tree = torch.empty(32 << (lg - 1), dtype=torch.uint8, device=dev)
+
+        def timed(fn):
+            with torch.cuda.stream(stream):
+                fn()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(reps):
+                    fn()
+                e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+
+        t_f = timed(lambda: native.check(lib, lib.tp_fft_dev(a.data_ptr(), n, n, f.data_ptr(), 1, 0, 0, s)))
+        t_i = timed(lambda: native.check(lib, lib.tp_ifft_dev(f.data_ptr(), n, n, back.data_ptr(), 1, 0, 0, s)))
+        t_rs = timed(lambda: native.check(lib, lib.tp_rs_commit_dev(a.data_ptr(), lg, cw.data_ptr(),
+                                                                      tree.data_ptr(), s)))
+        ok = bool(torch.equal(back, a))
+        leaves = 1 << (lg - 2)
+        comp = leaves * 64 * 2 + (leaves - 1) * 2
+        passes = 1 if lg <= 10 else (2 if lg <= 20 else 3)
+        out["2^%d" % lg] = {
+            "fft_ms": t_f, "ifft_ms": t_i, "round_trip_exact": ok,
+            "fft_elem_per_s": n / (t_f / 1e3), "butterflies_per_s": n / 2 * lg / (t_f / 1e3),
+            "fft_hbm_gbs": passes * 32 * n / (t_f / 1e3) / 1e9,
+            "rs_commit_ms": t_rs, "rs_codeword_elements": n << 5,
+            "rs_sha256_compressions_per_s": comp / (t_rs / 1e3)}
+        del a, f, back, cw, tree
+        torch.cuda.empty_cache()
+    return out
 
 
 def ours_arm(args, rank, world, local_rank):
     import ctypes
     import torch
     import torch.distributed as dist
-    from truepix_b200 import native
     from truepix_b200.frame import BatchFrameProver, FrameLayout, GkrInputLayerProver, pack_fp2
+    from truepix_b200.orion import FrameCommitter
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -277,36 +440,55 @@ def ours_arm(args, rank, world, local_rank):
     stream = torch.cuda.Stream(dev)
     lib = native.gkr()
     bprover = BatchFrameProver([layout] * B, gt, i0, i1, device=local_rank, stream=stream)
+    committer = FrameCommitter([layout] * B, device=local_rank, stream=stream)
+    cw_len, leaves = committer.cw_len[0], committer.leaves[0]
     z1s = [z1] * B
     z2s = z2_dev.repeat(B)      # packed [B][nb]
     pts = pt_dev.repeat(B)      # packed [B][9 + nb]
 
-    def run_batch(hook=None):
-        bprover.prove(pix, z1s, z2s, pts, chal_b, round_hook=hook)
+    def run_batch(marks=None):
+        bprover.prove(pix, z1s, z2s, pts, chal_b)
+        if marks is not None:
+            marks.record(stream)
+        committer.commit(pix)
 
-    # ---- plain single-frame proofs (the baseline of the batched/plain ratio)
+    # ---- one frame at a time (the plain baseline of the GKR part, and of the step)
     plain = GkrInputLayerProver(layout, gt, i0, i1, device=local_rank, stream=stream)
-    n_plain = 0 if args.no_plain else max(10, min(200, 4 * B))
-    plain_fps = None
+    pcommit = FrameCommitter([layout], device=local_rank, stream=stream)
+    n_plain = 0 if args.no_plain else max(8, min(64, B))
+    plain_gkr_fps = plain_fps = None
     if n_plain:
         with torch.cuda.stream(stream):
-            for i in range(5):
+            for i in range(4):
                 plain.prove(pix[i % B], z1, z2_dev, pt_dev, chal)
+                pcommit.commit([pix[i % B]])
             torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            ev[0].record(stream)
             for i in range(n_plain):
                 plain.prove(pix[i % B], z1, z2_dev, pt_dev, chal)
-            e1.record(stream)
+            ev[1].record(stream)
+            for i in range(n_plain):
+                plain.prove(pix[i % B], z1, z2_dev, pt_dev, chal)
+                pcommit.commit([pix[i % B]])
+            ev[2].record(stream)
         torch.cuda.synchronize()
-        plain_fps = n_plain / (e0.elapsed_time(e1) / 1e3)
+        plain_gkr_fps = n_plain / (ev[0].elapsed_time(ev[1]) / 1e3)
+        plain_fps = n_plain / (ev[1].elapsed_time(ev[2]) / 1e3)
+    del pcommit
+    torch.cuda.empty_cache()
+
+    # ---- compute roof of the SHA-256 leaf kernels
+    sha_gcs = sha_peak(lib, dev, stream)
 
     # ---- batched: the timed region
     with torch.cuda.stream(stream):
         for i in range(args.warmup):
             run_batch()
     torch.cuda.synchronize()
-    native.check(lib, lib.tp_timer_enable(args.steps * nb * 2 + 16), "timer")
+    per_step_pairs = nb * 2 + 24 * B + 16
+    npairs = args.steps * per_step_pairs
+    native.check(lib, lib.tp_timer_enable(npairs), "timer")
     clk = ClockSampler(local_rank)
     clk.start()
     if world > 1:
@@ -314,13 +496,14 @@ def ours_arm(args, rank, world, local_rank):
     torch.cuda.synchronize()
     lib.tp_timer_reset()
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    mids = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     launches = 0
     clk.t0 = time.time()
     with torch.cuda.stream(stream):
         evs[0].record(stream)
         for i in range(args.steps):
-            run_batch()
-            launches += bprover.launches_last
+            run_batch(mids[i])
+            launches += bprover.launches_last + committer.launches_last
             evs[i + 1].record(stream)
     torch.cuda.synchronize()
     clk.t1 = time.time()
@@ -328,13 +511,13 @@ def ours_arm(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     clk.stop()
-    npairs = args.steps * nb * 2 + 16
     tms = (ctypes.c_float * npairs)()
     ttags = (ctypes.c_int * npairs)()
     got = lib.tp_timer_read(tms, ttags, npairs)
     lib.tp_timer_disable()
     ms = evs[0].elapsed_time(evs[-1])
     per_batch = sorted(evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps))
+    gkr_ms = sum(evs[i].elapsed_time(mids[i]) for i in range(args.steps))
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -342,75 +525,101 @@ def ours_arm(args, rank, world, local_rank):
     frames_done = args.steps * B
     value = world * frames_done / (ms / 1e3)
 
-    groups = kernel_groups(list(tms[:max(0, got)]), list(ttags[:max(0, got)]), layout, B)
+    groups = kernel_groups(list(tms[:max(0, got)]), list(ttags[:max(0, got)]), layout, B,
+                           cw_len, leaves)
     peak, peak_kind = peaks()
     kernels = []
     for name, g in sorted(groups.items(), key=lambda kv: -kv[1]["ms"]):
-        ach = g["bytes"] / (g["ms"] / 1e3) / 1e9 if g["ms"] > 0 else None
-        kernels.append({"kernel": name, "launches": g["launches"], "total_ms": g["ms"],
-                        "share_of_step": g["ms"] / ms, "achieved_gbs": ach,
-                        "avg_us_by_copies": {str(k): round(1e3 * v[1] / v[0], 2)
-                                             for k, v in sorted(g["by_copies"].items())}})
-    roof = None
-    traffic = profiled_traffic()
-    if kernels:
-        top = kernels[0]
-        g = groups[top["kernel"]]
-        roof = {"kernel": top["kernel"], "bound": "hbm", "achieved": top["achieved_gbs"],
-                "peak": peak, "unit": "GB/s",
-                "frac": top["achieved_gbs"] / peak if top["achieved_gbs"] else None,
-                "peak_source": (peak_kind + " hbm_gbs (MEASURED_PEAKS.json)") if peak_kind == "measured"
-                else "fallback 6650 GB/s",
-                "algorithmic_bytes_per_launch": g["bytes"] / g["launches"],
-                "avg_launch_us": 1e3 * g["ms"] / g["launches"], "launches_timed": g["launches"],
-                "traffic": (traffic or {}).get(top["kernel"]),
-                "all_claim_kernels": kernels}
+        ach = g["bytes"] / (g["ms"] / 1e3) / 1e9 if g["ms"] > 0 and g["bytes"] else None
+        k = {"kernel": name, "launches": g["launches"], "total_ms": g["ms"],
+             "share_of_step": g["ms"] / ms, "achieved_gbs": ach}
+        if g["compressions"]:
+            k["g_compressions_per_s"] = g["compressions"] / (g["ms"] / 1e3) / 1e9
+        if g["by_copies"]:
+            k["avg_us_by_copies"] = {str(c): round(1e3 * v[1] / v[0], 2)
+                                     for c, v in sorted(g["by_copies"].items())}
+        kernels.append(k)
+    traffic = profiled_traffic() or {}
+
+    def roof_of(k):
+        g = groups[k["kernel"]]
+        r = {"kernel": k["kernel"], "bound": "hbm", "achieved": k["achieved_gbs"], "peak": peak,
+             "unit": "GB/s",
+             "frac": k["achieved_gbs"] / peak if k["achieved_gbs"] else None,
+             "peak_source": (peak_kind + " hbm_gbs (MEASURED_PEAKS.json)") if peak_kind == "measured"
+             else "fallback 6650 GB/s",
+             "algorithmic_bytes_per_launch": g["bytes"] / g["launches"],
+             "avg_launch_us": 1e3 * g["ms"] / g["launches"], "launches_timed": g["launches"],
+             "traffic": traffic.get(k["kernel"])}
+        if k.get("g_compressions_per_s"):
+            r["compute"] = {"unit": "G SHA-256 compressions/s", "achieved": k["g_compressions_per_s"],
+                            "peak": sha_gcs, "frac": k["g_compressions_per_s"] / sha_gcs,
+                            "peak_source": "register-only throughput of the same SHA-256 code on "
+                                           "this GPU (tp_sha256_peak_dev, measured in this run)"}
+        return r
+
+    roof = roof_of(kernels[0]) if kernels else None
+    hbm_kernel = next((k for k in kernels if k["kernel"] == "table_round_kernel<fold>"), None)
+    roof_fold = roof_of(hbm_kernel) if hbm_kernel else None
     folded = sum(g["folded"] for g in groups.values())
 
     res_ok = None
     if rank == 0:
         c, w, b, m = bprover.results(B - 1)
-        res_ok = bool(c.any() and w.any() and m != (0, 0))
+        res_ok = bool(c.any() and w.any() and m != (0, 0) and any(committer.root(B - 1)))
 
-    e2e = e2e_ref = cpu = None
+    ntt = e2e = e2e_ref = cpu = None
+    if rank == 0 and not args.skip_ntt:
+        ntt = ntt_bench(lib, dev, stream)
     if rank == 0 and not args.skip_e2e:
-        e2e = e2e_batched(args, bprover, frames, z1s, z2s, pts, chal_b, stream, dev)
+        e2e = e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream, dev)
         e2e_ref = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
     if rank == 0 and world == 1 and not args.skip_cpu:
         secs, kind = _cpu_worker((0, 1))
         cpu = {"value": 1.0 / secs, "unit": UNIT, "cores": 1, "kind": kind,
                "sample": "1 frame of the same workload (compute_beta + 14 early rounds + finish "
-                         "+ MLE over 2^23 inputs), library calls only, one process"}
+                         "+ MLE over 2^23 inputs + Orion commit of the 2^23 inputs), library "
+                         "calls only, one process"}
     if rank == 0:
+        commit_ms = ms - gkr_ms
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u64 (Fp2 over 2^61-1)", "data": "synthetic",
-            "config": {"workload": "gkr_input_layer_gray_1080p", "frame": [H, Wd, 3],
+            "config": {"workload": WORKLOAD, "frame": [H, Wd, 3],
                        "copies": layout.copies, "padded_copies": layout.padded_copies,
                        "wires": layout.padded_copies * layout.n_wires, "rounds": nb,
                        "circuit": "gray.pws", "batch": B, "step": f"one batch of {B} frames",
-                       "path": "bytes -> batched rounds (tp_batch_*)",
-                       "l2": "inputs > L2: B distinct frames (0.4 GB) and their folded "
-                             "tables (~4.8 GB) per step",
+                       "path": "bytes -> batched rounds (tp_batch_*) -> Orion commits from bytes",
+                       "orion": {"columns": 128, "codeword_rows": cw_len, "tree_leaves": leaves},
+                       "l2": "inputs > L2: B distinct frames (0.4 GB), their folded tables "
+                             "(~4.8 GB) and codewords (14.8 GB) per step",
                        "parallelism": f"replicas x{world}"},
-            "plain": {"value": plain_fps, "unit": UNIT, "frames": n_plain,
-                      "what": "single-frame sessions back to back, same device timing"},
-            "batched_over_plain": (value / world / plain_fps) if plain_fps else None,
+            "breakdown": {
+                "gkr_ms_per_step": gkr_ms / args.steps, "commit_ms_per_step": commit_ms / args.steps,
+                "gkr_frames_per_s": frames_done / (gkr_ms / 1e3),
+                "commit_frames_per_s": frames_done / (commit_ms / 1e3),
+                "plain_frames_per_s": plain_fps, "plain_gkr_frames_per_s": plain_gkr_fps,
+                "batched_over_plain": (value / world / plain_fps) if plain_fps else None,
+                "gkr_batched_over_plain": (frames_done / (gkr_ms / 1e3) / plain_gkr_fps)
+                if plain_gkr_fps else None,
+                "plain": f"{n_plain} single-frame sessions (GKR, then GKR + commit) back to back"},
             "fp2_elem_per_s": folded / (ms / 1e3),
             "latency_ms_per_batch": {"p50": per_batch[len(per_batch) // 2],
                                      "p99": per_batch[min(len(per_batch) - 1,
                                                           int(0.99 * len(per_batch)))]},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
+            "roofline": roof, "roofline_fold_kernel": roof_fold, "kernels": kernels,
+            "ntt": ntt, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
             "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
         }
         print(json.dumps(line), flush=True)
 
 
-def e2e_batched(args, bprover, frames, z1s, z2s, pts, chal_b, stream, dev):
+def e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream, dev):
     """The batched path from pinned host frames: H2D of every frame's bytes, a D2H
-    of all claims after every round with a synchronise, D2H of wires and MLEs."""
+    of all claims after every round with a synchronise, the commits, D2H of wires,
+    MLEs and commitment roots."""
     import torch
     B = bprover.B
     host = [torch.from_numpy(f).pin_memory() for f in frames]
@@ -419,6 +628,8 @@ def e2e_batched(args, bprover, frames, z1s, z2s, pts, chal_b, stream, dev):
     claims_h = torch.zeros(B * 8, dtype=torch.int64).pin_memory()
     wires_h = torch.zeros_like(bprover.wires, device="cpu").pin_memory()
     mle_h = torch.zeros_like(bprover.mle, device="cpu").pin_memory()
+    roots_h = torch.zeros(B * 32, dtype=torch.uint8).pin_memory()
+    roots_d = torch.zeros(B * 32, dtype=torch.uint8, device=dev)
 
     def hook(k):
         claims_h.copy_(bprover.claims[k * B * 8:(k + 1) * B * 8], non_blocking=True)
@@ -429,22 +640,26 @@ def e2e_batched(args, bprover, frames, z1s, z2s, pts, chal_b, stream, dev):
             for d, h in zip(dpix, host):
                 d.copy_(h, non_blocking=True)
             bprover.prove(dpix, z1s, z2s, pts, chal_b, round_hook=hook)
+            committer.commit(dpix)
+            for f in range(B):
+                roots_d[32 * f:32 * f + 32].copy_(committer.trees[f][32:64])
             wires_h.copy_(bprover.wires, non_blocking=True)
             mle_h.copy_(bprover.mle, non_blocking=True)
+            roots_h.copy_(roots_d, non_blocking=True)
         stream.synchronize()
 
     one()
-    steps = max(2, min(args.steps, 8))
+    steps = max(2, min(args.steps, 5))
     t0 = time.perf_counter()
     for _ in range(steps):
         one()
     wall = time.perf_counter() - t0
     h2d = sum(f.nbytes for f in frames)
-    d2h = R * B * 64 + bprover.wires.numel() * 8 + bprover.mle.numel() * 8
+    d2h = R * B * 64 + bprover.wires.numel() * 8 + bprover.mle.numel() * 8 + 32 * B
     return {"value": steps * B / wall, "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": steps, "frames_per_step": B,
-            "timer": "host wall clock", "path": "tp_batch_* from pinned host frames, "
-            "claims read back every round"}
+            "timer": "host wall clock", "path": "tp_batch_* + tp_orion_commit_pixels_dev from "
+            "pinned host frames, claims read back every round, roots at the end"}
 
 
 def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
@@ -476,6 +691,10 @@ def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
     pr, pim = np.ascontiguousarray(point[:, 0]), np.ascontiguousarray(point[:, 1])
     mr, mi = ctypes.c_uint64(), ctypes.c_uint64()
     br1, bi1 = ctypes.c_uint64(), ctypes.c_uint64()
+    elems = pinned(frame_elements(pix, layout))            # commit input, {img, real}
+    n_el = C * W
+    leaves = lib.tp_orion_tree_leaves(n_el)
+    tree_h = torch.zeros(64 * leaves, dtype=torch.uint8).pin_memory()
 
     def one():
         lib.native_fp2_compute_beta(arr(z2r), arr(z2i), nb, 1, 0, P(b_re), P(b_im))
@@ -491,22 +710,24 @@ def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
         lib.native_fp2_mle_eval_base(P(t_in), arr(pr), arr(pim), pr.size, ctypes.byref(mr),
                                      ctypes.byref(mi))
         assert lib.tp_last_error_code() == 0, lib.tp_last_error()
+        assert lib.tp_orion_commit(elems.data_ptr(), n_el, tree_h.data_ptr(), None) == 0, \
+            lib.tp_last_error()
 
     for _ in range(max(1, min(args.warmup, 3))):
         one()
-    steps = max(3, min(args.steps, 20))
+    steps = max(3, min(args.steps, 10))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(steps):
         one()
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
-    h2d = 16 * W * C + 16 * C + 8 * W * C + 16 * (nb + point.shape[0] + z1.shape[1])
-    d2h = 16 * C + 64 * nb + 16 * (W + 1) + 16
+    h2d = 16 * W * C + 16 * C + 8 * W * C + 16 * (nb + point.shape[0] + z1.shape[1]) + 16 * n_el
+    d2h = 16 * C + 64 * nb + 16 * (W + 1) + 16 + 64 * leaves
     return {"value": steps / wall, "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": steps, "timer": "host wall clock (synchronous API)",
-            "path": "native_fp2_compute_beta/early_create/claim/fold/finish/mle_eval_base, "
-                    "pinned host buffers"}
+            "path": "native_fp2_compute_beta/early_create/claim/fold/finish/mle_eval_base + "
+                    "tp_orion_commit (the whole tree back), pinned host buffers"}
 
 
 def main():
@@ -519,6 +740,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-ntt", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
