@@ -446,3 +446,56 @@ int oracle_rs_commit(const u64* src, int log_len, unsigned char* root, u64* l_ev
     free(lev);
     return 0;
 }
+
+/* ---- tensor-product opening, prover side (src/VPD/linearPC.cpp:480-531,569-571) ----
+ * combined[t] = sum_j r0[j] * codeword_j[t] (t < cw_len; its first N/128 entries
+ * are combined_message); leaves i < 2 N/128 = SHA256(combined[i] || 0^48) (zero
+ * element beyond cw_len; merkle_tree.cpp:5-13), tree as in the commit;
+ * answer = sum_{i < N/128} r1[i] * combined[i]. r0: 128 elements, r1: N/128. */
+int oracle_orion_combine(const u64* src, long long N, const u64* r0, const u64* r1, u64* combined_out,
+                         unsigned char* root, u64* answer)
+{
+    if (N % 128 != 0) return -1;
+    const long long col_len = N / 128, rows = 2 * col_len;
+    grand g;
+    expanders E;
+    memset(&E, 0, sizeof(E));
+    oracle_glibc_seed(&g, 1);
+    const long long cw_len = exp_init(&g, &E, col_len, 0);
+    fe* cw = (fe*)calloc((size_t)(cw_len + 1), sizeof(fe));
+    fe* comb = (fe*)calloc((size_t)(cw_len + 1), sizeof(fe));
+    for (int c = 0; c < 128; ++c) {
+        encode(&E, (const fe*)src + (size_t)c * col_len, cw, col_len, 0);
+        const fe r = ((const fe*)r0)[c];
+        for (long long t = 0; t < cw_len; ++t) comb[t] = feadd(comb[t], femul(r, cw[t]));
+    }
+    if (combined_out) memcpy(combined_out, comb, sizeof(fe) * (size_t)cw_len);
+    fe ans = {0, 0};
+    for (long long i = 0; i < col_len; ++i) ans = feadd(ans, femul(((const fe*)r1)[i], comb[i]));
+    answer[0] = ans.img;
+    answer[1] = ans.real;
+    long long size = 1;
+    while (size < rows) size *= 2;
+    unsigned char* tree = (unsigned char*)calloc((size_t)(2 * size), 32);
+    unsigned char blk[64];
+    for (long long i = 0; i < size; ++i) {
+        memset(blk, 0, 64);
+        if (i < rows) {
+            fe x = {0, 0};
+            if (i < cw_len) x = comb[i];
+            put_fe(blk, x);
+        }
+        oracle_sha256_64(blk, tree + 32 * (size + i));
+    }
+    for (long long k = size - 1; k >= 1; --k) {
+        memcpy(blk, tree + 32 * (2 * k), 32);
+        memcpy(blk + 32, tree + 32 * (2 * k + 1), 32);
+        oracle_sha256_64(blk, tree + 32 * k);
+    }
+    memcpy(root, tree + 32, 32);
+    free(tree);
+    free(comb);
+    free(cw);
+    free_expanders(&E);
+    return 0;
+}

@@ -17,6 +17,9 @@
 #include "VPD/linearPC.h"
 #include "truepix/truepix_gkr.h"
 
+// the codeword commit() retains (defined in src/VPD/linearPC.cpp)
+extern prime_field::field_element** encoded_codeword;
+
 extern "C" {
 
 // SHA-256 of one 64-byte block exactly as Orion hashes it (my_hhash)
@@ -88,6 +91,44 @@ void ref_rs_commit(const uint64_t* src, int log_len, unsigned char* root32, uint
     memcpy(root32, &h, 32);
     if (l_eval) memcpy(l_eval, poly_commit::l_eval, 16 * (n << rs_code_rate));
     delete[] a;
+}
+
+// The prover-side passes of tensor_product_protocol (src/VPD/linearPC.cpp:480-531,
+// 569-571) over the codeword that commit() retains, with the reference's own
+// primitives: combined[t] = sum_j r0[j] * encoded_codeword[j][t]; leaves
+// merkle_tree::hash_single_field_element(combined[i] or 0), i < 2 N/128, tree by
+// create_tree; answer = sum_i r1[i] * combined[i], i < N/128. Call once per process.
+void ref_combine(const uint64_t* src, long long N, const uint64_t* r0, const uint64_t* r1,
+                 uint64_t* combined_out, unsigned char* root32, uint64_t* answer)
+{
+    typedef prime_field::field_element F;
+    prime_field::init();
+    srand(1);
+    expander_init(N / column_size);
+    set_retain_encoded_codeword(true);
+    commit(reinterpret_cast<const F*>(src), N);
+    const long long msg_len = N / column_size, cw_len = encode_output_len(msg_len);
+    const F* R0 = reinterpret_cast<const F*>(r0);
+    const F* R1 = reinterpret_cast<const F*>(r1);
+    F* comb = new F[cw_len];
+    for (long long t = 0; t < cw_len; ++t) comb[t] = F(0ULL);
+    for (int j = 0; j < column_size; ++j)
+        for (long long t = 0; t < cw_len; ++t) comb[t] = comb[t] + R0[j] * encoded_codeword[j][t];
+    F ans = F(0ULL);
+    for (long long i = 0; i < msg_len; ++i) ans = ans + R1[i] * comb[i];
+    memcpy(answer, &ans, 16);
+    memcpy(combined_out, comb, 16 * (size_t)cw_len);
+    __hhash_digest* leaves = new __hhash_digest[msg_len * 2];
+    F zero;
+    memset(&zero, 0, sizeof(zero));
+    for (long long i = 0; i < msg_len * 2; ++i)
+        leaves[i] = merkle_tree::hash_single_field_element(i < cw_len ? comb[i] : zero);
+    __hhash_digest* mt = nullptr;
+    merkle_tree::merkle_tree_prover::create_tree(leaves, msg_len * 2, mt, sizeof(__hhash_digest), true);
+    memcpy(root32, &mt[1], 32);
+    free(mt);
+    delete[] leaves;
+    delete[] comb;
 }
 
 // encoded length of a column of n elements (graphs generated from the default seed)

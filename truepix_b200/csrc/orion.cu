@@ -138,8 +138,6 @@ void state_to_bytes(const uint32_t st[8], unsigned char out[32])
 
 __device__ __forceinline__ ulonglong2 ldg16(const ulonglong2* p) { return __ldg(p); }
 
-__device__ __forceinline__ fp2 as_fp2(ulonglong2 v) { return mk(v.y, v.x); }   // {img, real}
-__device__ __forceinline__ ulonglong2 from_fp2(fp2 a) { return make_ulonglong2(a.im, a.re); }
 
 // out[c][r] = in[r][c] for in [n_r][n_c] (16-byte elements), 32 x 32 tiles,
 // one tile per CTA in a 1-D grid
@@ -251,6 +249,9 @@ __global__ void __launch_bounds__(256) gather_bytes_kernel(const unsigned char* 
 // (s, w) of w * rows[src + s][c]. Lane l owns columns l, l + 32, l + 64, l + 96
 // (each edge reads one 2 KB row, 512 contiguous bytes per load instruction).
 // Edge metadata is read 32 at a time, one edge per lane, and broadcast.
+// The Fp2 products are accumulated as their three Karatsuba parts
+// (sum xr wr, sum xi wi, sum (xr + xi)(wr + wi)), folded once per two edges,
+// and combined into re = AC - BD, im = S - AC - BD once per target.
 __global__ void __launch_bounds__(256) gather_kernel(ulonglong2* __restrict__ rows, long long src_row,
                                                      long long dst_row, long long n_targets,
                                                      const unsigned* __restrict__ ptr,
@@ -262,9 +263,9 @@ __global__ void __launch_bounds__(256) gather_kernel(ulonglong2* __restrict__ ro
     const int lane = threadIdx.x & 31;
     const unsigned e0 = ptr[t], e1 = ptr[t + 1];
     const ulonglong2* src = rows + src_row * kColumns + lane;
-    fp2 acc[4];
+    u64 ac[4], bd[4], sm[4];   // nearly canonical (< 2^61 + 8)
 #pragma unroll
-    for (int k = 0; k < 4; ++k) acc[k] = f2zero();
+    for (int k = 0; k < 4; ++k) ac[k] = bd[k] = sm[k] = 0;
     for (unsigned eb = e0; eb < e1; eb += 32) {
         const int cnt = (int)min(32u, e1 - eb);
         unsigned my_s = 0;
@@ -277,8 +278,9 @@ __global__ void __launch_bounds__(256) gather_kernel(ulonglong2* __restrict__ ro
         for (; j + 2 <= cnt; j += 2) {
             const unsigned s0 = __shfl_sync(0xffffffffu, my_s, j);
             const unsigned s1 = __shfl_sync(0xffffffffu, my_s, j + 1);
-            const fp2 w0 = mk(__shfl_sync(0xffffffffu, my_w.y, j), __shfl_sync(0xffffffffu, my_w.x, j));
-            const fp2 w1 = mk(__shfl_sync(0xffffffffu, my_w.y, j + 1), __shfl_sync(0xffffffffu, my_w.x, j + 1));
+            const u64 w0r = __shfl_sync(0xffffffffu, my_w.y, j), w0i = __shfl_sync(0xffffffffu, my_w.x, j);
+            const u64 w1r = __shfl_sync(0xffffffffu, my_w.y, j + 1), w1i = __shfl_sync(0xffffffffu, my_w.x, j + 1);
+            const u64 w0s = w0r + w0i, w1s = w1r + w1i;   // < 2^62
             const ulonglong2* p0 = src + (long long)s0 * kColumns;
             const ulonglong2* p1 = src + (long long)s1 * kColumns;
             ulonglong2 v0[4], v1[4];
@@ -289,21 +291,33 @@ __global__ void __launch_bounds__(256) gather_kernel(ulonglong2* __restrict__ ro
             }
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                acc[k] = l2add(acc[k], l2mul(w0, as_fp2(v0[k])));
-                acc[k] = l2add(acc[k], l2mul(w1, as_fp2(v1[k])));
+                // three terms below 2^61 + 8 each: the sum stays below 2^63
+                ac[k] = fold61(ac[k] + lmul(v0[k].y, w0r) + lmul(v1[k].y, w1r));
+                bd[k] = fold61(bd[k] + lmul(v0[k].x, w0i) + lmul(v1[k].x, w1i));
+                sm[k] = fold61(sm[k] + lmul(v0[k].y + v0[k].x, w0s) + lmul(v1[k].y + v1[k].x, w1s));
             }
         }
         if (j < cnt) {
             const unsigned s0 = __shfl_sync(0xffffffffu, my_s, j);
-            const fp2 w0 = mk(__shfl_sync(0xffffffffu, my_w.y, j), __shfl_sync(0xffffffffu, my_w.x, j));
+            const u64 w0r = __shfl_sync(0xffffffffu, my_w.y, j), w0i = __shfl_sync(0xffffffffu, my_w.x, j);
+            const u64 w0s = w0r + w0i;
             const ulonglong2* p0 = src + (long long)s0 * kColumns;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) acc[k] = l2add(acc[k], l2mul(w0, as_fp2(ldg16(p0 + 32 * k))));
+            for (int k = 0; k < 4; ++k) {
+                const ulonglong2 v = ldg16(p0 + 32 * k);
+                ac[k] = fold61(ac[k] + lmul(v.y, w0r));
+                bd[k] = fold61(bd[k] + lmul(v.x, w0i));
+                sm[k] = fold61(sm[k] + lmul(v.y + v.x, w0s));
+            }
         }
     }
     ulonglong2* dst = rows + (dst_row + t) * kColumns + lane;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) dst[32 * k] = from_fp2(l2canon(acc[k]));
+    for (int k = 0; k < 4; ++k) {
+        const u64 re = fold61(ac[k] + (2 * P61 - bd[k]));
+        const u64 im = fold61(sm[k] + (4 * P61 - ac[k] - bd[k]));
+        dst[32 * k] = make_ulonglong2(canon61(im), canon61(re));
+    }
 }
 
 constexpr int kLeafRows = 128;     // rows (threads) per CTA
