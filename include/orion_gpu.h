@@ -58,6 +58,27 @@ int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_
                                int n_wires, int const_idx, uint64_t const_val, void* d_rows,
                                void* d_tree, void* stream);
 
+/* Prover-side passes of tensor_product_protocol (src/VPD/linearPC.cpp:480-531,
+ * 569-571) over the ROW-major codeword d_rows that a commit above left on the
+ * device. d_r0: 128 elements (the column weights r0). d_combined: cw_len
+ * elements, combined_codeword (its first N/128 entries are combined_message).
+ * d_ctree: NULL, or 2 * tp_orion_tree_leaves(N) digests: combined_codeword_mt,
+ * leaves merkle_tree::hash_single_field_element(combined[i]) (zero element past
+ * cw_len), root at 1. */
+int tp_orion_combine_dev(const void* d_rows, long long N, const void* d_r0, void* d_combined, void* d_ctree,
+                         void* stream);
+
+/* queried_cols[i][j] = encoded_codeword[j][col_q[i]] for i < count: d_q holds
+ * count int64 row indices (< cw_len, checked), d_out count * 128 elements.
+ * Synchronises the stream. */
+int tp_orion_query_columns_dev(const void* d_rows, long long N, const void* d_q, int count, void* d_out,
+                               void* stream);
+
+/* answer = sum_{i < msg_len} r1[i] * combined_message[i] (linearPC.cpp:569-571);
+ * d_answer: one element. */
+int tp_orion_answer_dev(const void* d_combined, long long msg_len, const void* d_r1, void* d_answer,
+                        void* stream);
+
 /* Kernels launched by the calling thread's last commit (any of the three forms). */
 int tp_orion_last_launches(void);
 
@@ -103,6 +124,19 @@ int tp_ifft_dev(const void* d_evals, long long coef_len, long long order, void* 
  * function's return value in the reference) is tree_out[1]. */
 int tp_rs_commit(const uint64_t* src, int log_len, uint64_t* l_eval_out, unsigned char* tree_out);
 int tp_rs_commit_dev(const void* d_src, int log_len, void* d_l_eval, void* d_tree, void* stream);
+
+/* ---- Virgo (linear GKR) sumcheck (src/linear_gkr/prover.cpp) --------------- */
+
+/* Replaces zk_prover::sumcheck_phase1_update and sumcheck_phase2_update
+ * (prover.cpp:576-644, 935-1006; one computation): the tables V_mult_add,
+ * addV_array, add_mult_sum (total_uv linear_poly entries {a, b} each, 32 bytes)
+ * are folded with previous_random (or, for current_bit == 0, without it) into
+ * d_*_out (total_uv / 2 entries each; the reference swaps them in), and d_ret gets
+ * the returned quadratic_poly {a, b, c} (48 bytes). total_uv even and >= 2;
+ * tables and previous_random canonical. */
+int tp_virgo_sumcheck_update_dev(const void* d_vma, const void* d_addv, const void* d_ams, long long total_uv,
+                                 uint64_t r_real, uint64_t r_imag, int current_bit, void* d_vma_out,
+                                 void* d_addv_out, void* d_ams_out, void* d_ret, void* stream);
 
 #ifdef __cplusplus
 }

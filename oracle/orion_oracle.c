@@ -499,3 +499,47 @@ int oracle_orion_combine(const u64* src, long long N, const u64* r0, const u64* 
     free_expanders(&E);
     return 0;
 }
+
+/* ---- Virgo sumcheck round (src/linear_gkr/prover.cpp:576-644, 935-1006) ----
+ * tables of n linear_poly {a, b} (two elements each); folded into n/2 entries;
+ * ret = {a, b, c} of the round polynomial over the folded tables. */
+static void fold_lp(const fe* t, long long i, fe r, int bit, fe* ya, fe* yb)
+{
+    const fe a0 = t[4 * i], b0 = t[4 * i + 1], a1 = t[4 * i + 2], b1 = t[4 * i + 3];
+    fe neg;
+    if (!bit) {
+        *yb = b0;
+        neg.img = canon(P61 - b0.img);
+        neg.real = canon(P61 - b0.real);
+        *ya = feadd(b1, neg);
+    } else {
+        *yb = feadd(femul(a0, r), b0);
+        neg.img = canon(P61 - yb->img);
+        neg.real = canon(P61 - yb->real);
+        *ya = feadd(feadd(femul(a1, r), b1), neg);
+    }
+}
+
+int oracle_virgo_update(const u64* vma, const u64* addv, const u64* ams, long long n, const u64* r, int bit,
+                        u64* vma_out, u64* addv_out, u64* ams_out, u64* ret)
+{
+    if (n < 2 || (n & 1)) return -1;
+    const fe R = {r[0], r[1]};
+    fe qa = {0, 0}, qb = {0, 0}, qc = {0, 0};
+    for (long long i = 0; i < n / 2; ++i) {
+        fe va, vb, da, db, ma, mb;
+        fold_lp((const fe*)vma, i, R, bit, &va, &vb);
+        fold_lp((const fe*)addv, i, R, bit, &da, &db);
+        fold_lp((const fe*)ams, i, R, bit, &ma, &mb);
+        ((fe*)vma_out)[2 * i] = va; ((fe*)vma_out)[2 * i + 1] = vb;
+        ((fe*)addv_out)[2 * i] = da; ((fe*)addv_out)[2 * i + 1] = db;
+        ((fe*)ams_out)[2 * i] = ma; ((fe*)ams_out)[2 * i + 1] = mb;
+        qa = feadd(qa, femul(ma, va));
+        qb = feadd(qb, feadd(feadd(femul(ma, vb), femul(mb, va)), da));
+        qc = feadd(qc, feadd(femul(mb, vb), db));
+    }
+    ret[0] = qa.img; ret[1] = qa.real;
+    ret[2] = qb.img; ret[3] = qb.real;
+    ret[4] = qc.img; ret[5] = qc.real;
+    return 0;
+}

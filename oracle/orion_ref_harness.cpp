@@ -13,6 +13,7 @@
 #include "infrastructure/my_hhash.h"
 #include "linear_code/linear_code_encode.h"
 #include "linear_gkr/prime_field.h"
+#include "linear_gkr/prover.h"
 #include "poly_commitment/poly_commit.h"
 #include "VPD/linearPC.h"
 #include "truepix/truepix_gkr.h"
@@ -129,6 +130,38 @@ void ref_combine(const uint64_t* src, long long N, const uint64_t* r0, const uin
     free(mt);
     delete[] leaves;
     delete[] comb;
+}
+
+// One Virgo sumcheck update (zk_prover::sumcheck_phase1_update when phase == 1,
+// sumcheck_phase2_update when phase == 2; src/linear_gkr/prover.cpp:576-644,
+// 935-1006) on tables given as linear_poly arrays of n entries {a, b}: the folded
+// tables (n / 2 entries each) and the returned quadratic_poly {a, b, c}.
+void ref_virgo_update(int phase, const uint64_t* vma, const uint64_t* addv, const uint64_t* ams, int n,
+                      const uint64_t* r, int current_bit, uint64_t* vma_out, uint64_t* addv_out,
+                      uint64_t* ams_out, uint64_t* ret)
+{
+    prime_field::init();
+    int bits = 0;
+    while ((1 << bits) < n) ++bits;
+    zk_prover* p = new zk_prover();
+    p->init_array(bits);
+    memcpy(p->V_mult_add, vma, 32 * (size_t)n);
+    memcpy(p->addV_array, addv, 32 * (size_t)n);
+    memcpy(p->add_mult_sum, ams, 32 * (size_t)n);
+    p->total_uv = n;
+    prime_field::field_element pr;
+    memcpy(&pr, r, 16);
+    quadratic_poly q = phase == 1 ? p->sumcheck_phase1_update(pr, current_bit)
+                                  : p->sumcheck_phase2_update(pr, current_bit);
+    memcpy(vma_out, p->V_mult_add, 16 * (size_t)n);
+    memcpy(addv_out, p->addV_array, 16 * (size_t)n);
+    memcpy(ams_out, p->add_mult_sum, 16 * (size_t)n);
+    memcpy(ret, &q, 48);
+    layered_circuit none;     // delete_self frees circuit_value[0 .. C->total_depth)
+    none.total_depth = 0;
+    p->C = &none;
+    p->delete_self();
+    delete p;
 }
 
 // encoded length of a column of n elements (graphs generated from the default seed)

@@ -16,6 +16,12 @@ tests/golden/orion_golden.npz:
                   (RS_polynomial.cpp:132-206)
   rs_<L>          Merkle root and codeword digest of the rate-2^-5 RS commit
                   of 2^L elements (poly_commit.h:42-96, fri.cpp:36-123)
+  virgo*_<p>_<n>_<bit>  one Virgo sumcheck update (zk_prover::sumcheck_phase<p>_update,
+                  prover.cpp:576-644, 935-1006) of three seeded linear_poly
+                  tables: digests of the folded tables and the round polynomial
+  combine*_<N>    the tensor-product opening passes (linearPC.cpp:480-531,
+                  569-571) run with the reference's primitives on its retained
+                  codeword: combined codeword digest, its Merkle root, answer
 
 Every reference call runs in a fresh spawned process: the reference keeps
 global scratch state sized by its first call.
@@ -34,7 +40,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
-from orionlib import ORION_REF_LIB, digest, elements, frame_bytes, frame_elements  # noqa: E402
+from orionlib import (ORION_REF_LIB, digest, elements, frame_bytes, frame_elements,  # noqa: E402
+                      virgo_inputs)
 
 V = ctypes.c_void_p
 
@@ -52,6 +59,9 @@ ENCODE_CASES = [1, 13, 14, 64, 100, 1000, 8192, 65536]
 FFT_CASES = [(1, 1), (1, 8), (2, 2), (8, 8), (4, 16), (16, 256), (1024, 1024), (256, 4096),
              (1 << 12, 1 << 17), (1 << 16, 1 << 16), (1 << 20, 1 << 20)]
 RS_CASES = [6, 7, 10, 13, 16, 18]
+COMBINE_CASES = [(1 << 14, 21), (128 * 100, 22), (1 << 18, 23)]   # (N, seed)
+VIRGO_CASES = [(1, 2, 0, 31), (1, 2, 1, 32), (1, 16, 1, 33), (2, 16, 0, 34), (1, 1 << 10, 1, 35),
+               (2, 1 << 14, 1, 36), (1, 1 << 18, 1, 37), (2, 1 << 18, 0, 38)]   # (phase, total_uv, bit, seed)
 
 
 def _ref():
@@ -61,6 +71,8 @@ def _ref():
     lib.ref_ifft.argtypes = [V, ctypes.c_int, ctypes.c_int, V]
     lib.ref_rs_commit.argtypes = [V, ctypes.c_int, V, V]
     lib.ref_encode.argtypes = [V, ctypes.c_longlong, V]
+    lib.ref_combine.argtypes = [V, ctypes.c_longlong, V, V, V, V, V]
+    lib.ref_virgo_update.argtypes = [ctypes.c_int, V, V, V, ctypes.c_int, V, ctypes.c_int, V, V, V, V]
     lib.ref_encode_len.argtypes = [ctypes.c_longlong]
     lib.ref_encode_len.restype = ctypes.c_longlong
     return lib
@@ -108,6 +120,29 @@ def _ifft(args):
     return out
 
 
+def _combine(args):
+    n, seed = args
+    lib = _ref()
+    src = elements(seed, n)
+    r0, r1 = elements(seed + 1000, 128), elements(seed + 2000, n // 128)
+    comb = np.zeros(2 * lib.ref_encode_len(n // 128), np.uint64)
+    root = ctypes.create_string_buffer(32)
+    ans = np.zeros(2, np.uint64)
+    lib.ref_combine(V(src.ctypes.data), n, V(r0.ctypes.data), V(r1.ctypes.data), V(comb.ctypes.data),
+                    root, V(ans.ctypes.data))
+    return digest(comb), root.raw, ans
+
+
+def _virgo(args):
+    phase, n, bit, seed = args
+    vma, addv, ams, r = virgo_inputs(n, seed)
+    outs = [np.zeros(2 * n, np.uint64) for _ in range(3)]
+    ret = np.zeros(6, np.uint64)
+    _ref().ref_virgo_update(phase, V(vma.ctypes.data), V(addv.ctypes.data), V(ams.ctypes.data), n,
+                            V(r.ctypes.data), bit, *[V(o.ctypes.data) for o in outs], V(ret.ctypes.data))
+    return [digest(o) for o in outs], ret
+
+
 def _rs(lg):
     src = elements(400 + lg, 1 << lg)
     root = ctypes.create_string_buffer(32)
@@ -141,6 +176,16 @@ def main():
         for lg, (root, d) in zip(RS_CASES, pool.map(_rs, RS_CASES, chunksize=1)):
             out["rs_%d" % lg] = np.frombuffer(root, np.uint8)
             out["rscw_%d" % lg] = np.frombuffer(d, np.uint8)
+        for (n, seed), (d, root, ans) in zip(COMBINE_CASES, pool.map(_combine, COMBINE_CASES, chunksize=1)):
+            out["combine_%d" % n] = np.frombuffer(d, np.uint8)
+            out["combineroot_%d" % n] = np.frombuffer(root, np.uint8)
+            out["combineanswer_%d" % n] = ans
+            out["combinecase_%d" % n] = np.array([n, seed])
+        for (phase, n, bit, seed), (ds, ret) in zip(VIRGO_CASES, pool.map(_virgo, VIRGO_CASES, chunksize=1)):
+            key = "%d_%d_%d" % (phase, n, bit)
+            out["virgocase_" + key] = np.array([phase, n, bit, seed])
+            out["virgotables_" + key] = np.frombuffer(b"".join(ds), np.uint8)
+            out["virgoret_" + key] = ret
     np.savez_compressed(os.path.join(HERE, "orion_golden.npz"), **out)
     print("wrote", len(out), "arrays")
 

@@ -67,6 +67,12 @@ def frame_elements(pix: np.ndarray, copies: int, cs: int, W: int, const_idx: int
     return out
 
 
+def virgo_inputs(n: int, seed: int):
+    """Three linear_poly tables of n entries {a, b} (4 words each) and a random."""
+    return (elements(seed, 2 * n), elements(seed + 1, 2 * n), elements(seed + 2, 2 * n),
+            elements(seed + 3, 1))
+
+
 def digest(a: np.ndarray) -> bytes:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest()
 
@@ -91,6 +97,8 @@ class OrionOracle:
         L.oracle_rs_commit.argtypes = [_V, _I, _V, _V]
         L.oracle_encode.argtypes = [_V, _LL, _V]
         L.oracle_encode.restype = _LL
+        L.oracle_orion_combine.argtypes = [_V, _LL, _V, _V, _V, _V, _V]
+        L.oracle_virgo_update.argtypes = [_V, _V, _V, _LL, _V, _I, _V, _V, _V, _V]
 
     def sha256_64(self, msg: bytes) -> bytes:
         assert len(msg) == 64
@@ -120,6 +128,26 @@ class OrionOracle:
         if rc != 0:
             raise ValueError("oracle_orion_commit: %d" % rc)
         return (root.raw, lv.reshape(-1, 32)) if leaves else root.raw
+
+    def combine(self, src: np.ndarray, r0: np.ndarray, r1: np.ndarray):
+        """(combined codeword, root of its tree, answer) of the opening passes."""
+        n = src.size // 2
+        comb = np.zeros(2 * self.encode_len(n // 128), np.uint64)
+        root = ctypes.create_string_buffer(32)
+        ans = np.zeros(2, np.uint64)
+        rc = self.lib.oracle_orion_combine(_vp(src), n, _vp(r0), _vp(r1), _vp(comb), root, _vp(ans))
+        assert rc == 0
+        return comb, root.raw, ans
+
+    def virgo_update(self, vma, addv, ams, r, bit):
+        """(folded tables x3, ret [6 words]) of one Virgo sumcheck round."""
+        n = vma.size // 4
+        outs = [np.zeros(2 * n, np.uint64) for _ in range(3)]
+        ret = np.zeros(6, np.uint64)
+        rc = self.lib.oracle_virgo_update(_vp(vma), _vp(addv), _vp(ams), n, _vp(r), bit,
+                                          *[_vp(o) for o in outs], _vp(ret))
+        assert rc == 0
+        return outs, ret
 
     def fft(self, coef: np.ndarray, order: int) -> np.ndarray:
         out = np.zeros(2 * order, np.uint64)

@@ -7,7 +7,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from orionlib import OrionOracle, elements, frame_bytes, frame_elements
+from orionlib import OrionOracle, digest, elements, frame_bytes, frame_elements
 
 pytestmark = pytest.mark.gpu
 
@@ -154,3 +154,44 @@ def test_commit_rejects_bad_sizes_and_values(lib):
     assert lib.tp_orion_commit(vp(bad), 256, vp(tree), None) == -1
     assert b"canonical" in lib.tp_last_error()
     assert lib.tp_orion_commit_pixels_dev(None, 1, 1, 384, 512, 384, 128, None, None, None) == -1
+
+
+def test_opening_passes_match_reference(lib, og):
+    """combine / combined tree / answer over the device codeword against the
+    reference (its primitives on its retained codeword), and the queried rows."""
+    import torch
+    dev = torch.device("cuda", 0)
+    s = torch.cuda.current_stream().cuda_stream
+    for k in og.files:
+        if not k.startswith("combinecase_"):
+            continue
+        n, seed = (int(v) for v in og[k])
+        col = n // 128
+        cw_len = lib.tp_orion_codeword_len(col)
+        leaves = lib.tp_orion_tree_leaves(n)
+        d_src = torch.from_numpy(elements(seed, n).view(np.int64)).to(dev)
+        d_rows = torch.empty(2 * 128 * cw_len, dtype=torch.int64, device=dev)
+        d_tree = torch.empty(64 * leaves, dtype=torch.uint8, device=dev)
+        assert lib.tp_orion_commit_dev(d_src.data_ptr(), n, d_rows.data_ptr(), d_tree.data_ptr(), s) == 0
+        r0 = torch.from_numpy(elements(seed + 1000, 128).view(np.int64)).to(dev)
+        r1 = torch.from_numpy(elements(seed + 2000, col).view(np.int64)).to(dev)
+        comb = torch.empty(2 * cw_len, dtype=torch.int64, device=dev)
+        ctree = torch.empty(64 * leaves, dtype=torch.uint8, device=dev)
+        ans = torch.empty(2, dtype=torch.int64, device=dev)
+        assert lib.tp_orion_combine_dev(d_rows.data_ptr(), n, r0.data_ptr(), comb.data_ptr(),
+                                        ctree.data_ptr(), s) == 0, lib.tp_last_error()
+        assert lib.tp_orion_answer_dev(comb.data_ptr(), col, r1.data_ptr(), ans.data_ptr(), s) == 0
+        q = torch.tensor([0, cw_len - 1, col, 7 % cw_len], dtype=torch.int64, device=dev)
+        qout = torch.empty(2 * 128 * 4, dtype=torch.int64, device=dev)
+        assert lib.tp_orion_query_columns_dev(d_rows.data_ptr(), n, q.data_ptr(), 4, qout.data_ptr(), s) == 0
+        torch.cuda.synchronize()
+        c = comb.cpu().numpy().view(np.uint64)
+        assert digest(c) == og["combine_%d" % n].tobytes(), n
+        t = ctree.cpu().numpy().reshape(-1, 32)
+        assert t[1].tobytes() == og["combineroot_%d" % n].tobytes(), n
+        np.testing.assert_array_equal(ans.cpu().numpy().view(np.uint64), og["combineanswer_%d" % n])
+        rows = d_rows.cpu().numpy().view(np.uint64).reshape(cw_len, 256)
+        np.testing.assert_array_equal(qout.cpu().numpy().view(np.uint64).reshape(4, 256),
+                                      rows[[0, cw_len - 1, col, 7 % cw_len]])
+        bad = torch.tensor([cw_len], dtype=torch.int64, device=dev)
+        assert lib.tp_orion_query_columns_dev(d_rows.data_ptr(), n, bad.data_ptr(), 1, qout.data_ptr(), s) == -1

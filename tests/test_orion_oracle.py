@@ -113,3 +113,28 @@ def test_commit_root_of_a_1080p_frame(orc, og):
     src = frame_elements(frame_bytes(seed, copies * cs), copies, cs, W, ci, cv, padded)
     assert src.size == 2 << 23
     assert orc.commit(src) == og["frameroot_1080"].tobytes()
+
+
+def test_opening_combine(orc, og):
+    for k in og.files:
+        if not k.startswith("combinecase_"):
+            continue
+        n, seed = (int(v) for v in og[k])
+        comb, root, ans = orc.combine(elements(seed, n), elements(seed + 1000, 128),
+                                      elements(seed + 2000, n // 128))
+        assert digest(comb) == og["combine_%d" % n].tobytes(), n
+        assert root == og["combineroot_%d" % n].tobytes(), n
+        np.testing.assert_array_equal(ans, og["combineanswer_%d" % n])
+
+
+def test_virgo_update(orc, og):
+    from orionlib import virgo_inputs
+    for k in og.files:
+        if not k.startswith("virgocase_"):
+            continue
+        phase, n, bit, seed = (int(v) for v in og[k])
+        key = k[len("virgocase_"):]
+        vma, addv, ams, r = virgo_inputs(n, seed)
+        outs, ret = orc.virgo_update(vma, addv, ams, r, bit)
+        assert b"".join(digest(o) for o in outs) == og["virgotables_" + key].tobytes(), key
+        np.testing.assert_array_equal(ret, og["virgoret_" + key])

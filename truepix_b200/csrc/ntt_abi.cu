@@ -2,6 +2,7 @@
 #include <stdint.h>
 
 #include "ntt.h"
+#include "virgo.h"
 #include "runtime.h"
 #include "../../include/orion_gpu.h"
 
@@ -140,6 +141,25 @@ int tp_rs_commit(const uint64_t* src, int log_len, uint64_t* l_eval_out, unsigne
                                       "D2H"))
         return -1;
     return tp::cuda_failed(cudaStreamSynchronize(s), "synchronize") ? -1 : 0;
+}
+
+int tp_virgo_sumcheck_update_dev(const void* d_vma, const void* d_addv, const void* d_ams, long long total_uv,
+                                 uint64_t r_real, uint64_t r_imag, int current_bit, void* d_vma_out,
+                                 void* d_addv_out, void* d_ams_out, void* d_ret, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!d_vma || !d_addv || !d_ams || !d_vma_out || !d_addv_out || !d_ams_out || !d_ret) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_virgo_sumcheck_update_dev: null buffer");
+        return -1;
+    }
+    return tp::virgo::update(static_cast<const ulonglong2*>(d_vma), static_cast<const ulonglong2*>(d_addv),
+                             static_cast<const ulonglong2*>(d_ams), total_uv, tp::mk(r_real, r_imag), current_bit,
+                             static_cast<ulonglong2*>(d_vma_out), static_cast<ulonglong2*>(d_addv_out),
+                             static_cast<ulonglong2*>(d_ams_out), static_cast<ulonglong2*>(d_ret),
+                             reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
 }
 
 }  // extern "C"

@@ -252,20 +252,28 @@ __global__ void __launch_bounds__(256) gather_bytes_kernel(const unsigned char* 
 // The Fp2 products are accumulated as their three Karatsuba parts
 // (sum xr wr, sum xi wi, sum (xr + xi)(wr + wi)), folded once per two edges,
 // and combined into re = AC - BD, im = S - AC - BD once per target.
+// CPL = columns per lane: 4 (one warp per target) for the large graphs, 1 (four
+// warps per target, a quarter of the serial edge loop each) for the small ones,
+// whose few targets would otherwise leave most SMs idle.
+template <int CPL>
 __global__ void __launch_bounds__(256) gather_kernel(ulonglong2* __restrict__ rows, long long src_row,
                                                      long long dst_row, long long n_targets,
                                                      const unsigned* __restrict__ ptr,
                                                      const unsigned* __restrict__ esrc,
                                                      const ulonglong2* __restrict__ ew)
 {
-    const long long t = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    constexpr int kWarpsPerTarget = 4 / CPL;
+    const long long gw = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const long long t = gw / kWarpsPerTarget;
+    const int sub = (int)(gw % kWarpsPerTarget);
     if (t >= n_targets) return;
     const int lane = threadIdx.x & 31;
     const unsigned e0 = ptr[t], e1 = ptr[t + 1];
-    const ulonglong2* src = rows + src_row * kColumns + lane;
-    u64 ac[4], bd[4], sm[4];   // nearly canonical (< 2^61 + 8)
+    // column of slot k: lane + 32 (sub CPL + k)
+    const ulonglong2* src = rows + src_row * kColumns + lane + 32 * sub * CPL;
+    u64 ac[CPL], bd[CPL], sm[CPL];   // nearly canonical (< 2^61 + 8)
 #pragma unroll
-    for (int k = 0; k < 4; ++k) ac[k] = bd[k] = sm[k] = 0;
+    for (int k = 0; k < CPL; ++k) ac[k] = bd[k] = sm[k] = 0;
     for (unsigned eb = e0; eb < e1; eb += 32) {
         const int cnt = (int)min(32u, e1 - eb);
         unsigned my_s = 0;
@@ -283,14 +291,14 @@ __global__ void __launch_bounds__(256) gather_kernel(ulonglong2* __restrict__ ro
             const u64 w0s = w0r + w0i, w1s = w1r + w1i;   // < 2^62
             const ulonglong2* p0 = src + (long long)s0 * kColumns;
             const ulonglong2* p1 = src + (long long)s1 * kColumns;
-            ulonglong2 v0[4], v1[4];
+            ulonglong2 v0[CPL], v1[CPL];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < CPL; ++k) {
                 v0[k] = ldg16(p0 + 32 * k);
                 v1[k] = ldg16(p1 + 32 * k);
             }
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < CPL; ++k) {
                 // three terms below 2^61 + 8 each: the sum stays below 2^63
                 ac[k] = fold61(ac[k] + lmul(v0[k].y, w0r) + lmul(v1[k].y, w1r));
                 bd[k] = fold61(bd[k] + lmul(v0[k].x, w0i) + lmul(v1[k].x, w1i));
@@ -303,7 +311,7 @@ __global__ void __launch_bounds__(256) gather_kernel(ulonglong2* __restrict__ ro
             const u64 w0s = w0r + w0i;
             const ulonglong2* p0 = src + (long long)s0 * kColumns;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < CPL; ++k) {
                 const ulonglong2 v = ldg16(p0 + 32 * k);
                 ac[k] = fold61(ac[k] + lmul(v.y, w0r));
                 bd[k] = fold61(bd[k] + lmul(v.x, w0i));
@@ -311,9 +319,9 @@ __global__ void __launch_bounds__(256) gather_kernel(ulonglong2* __restrict__ ro
             }
         }
     }
-    ulonglong2* dst = rows + (dst_row + t) * kColumns + lane;
+    ulonglong2* dst = rows + (dst_row + t) * kColumns + lane + 32 * sub * CPL;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < CPL; ++k) {
         const u64 re = fold61(ac[k] + (2 * P61 - bd[k]));
         const u64 im = fold61(sm[k] + (4 * P61 - ac[k] - bd[k]));
         dst[32 * k] = make_ulonglong2(canon61(im), canon61(re));
@@ -450,6 +458,20 @@ __global__ void __launch_bounds__(kLeafRows) sha_peak_kernel(int iters, uint32_t
         sha::hash64(w, st, sha::AddMad{one});
     }
     atomicXor(out, st[0] ^ st[1] ^ st[2] ^ st[3] ^ st[4] ^ st[5] ^ st[6] ^ st[7]);
+}
+
+// graphs with fewer targets than this get four warps per target
+constexpr long long kSmallGraph = 8192;
+
+void launch_gather(ulonglong2* rows, long long src_row, long long dst_row, long long n_targets,
+                   const unsigned* ptr, const unsigned* esrc, const ulonglong2* ew, cudaStream_t s)
+{
+    if (n_targets < kSmallGraph)
+        gather_kernel<1><<<(unsigned)((4 * n_targets + 7) / 8), 256, 0, s>>>(rows, src_row, dst_row, n_targets,
+                                                                             ptr, esrc, ew);
+    else
+        gather_kernel<4><<<(unsigned)((n_targets + 7) / 8), 256, 0, s>>>(rows, src_row, dst_row, n_targets, ptr,
+                                                                         esrc, ew);
 }
 
 bool launch_ok(const char* what)
@@ -626,9 +648,8 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
             continue;
         }
         timer_begin(s, kTagGather);
-        gather_kernel<<<(unsigned)((lv.R + 7) / 8), 256, 0, s>>>(rows, lv.off, lv.off + lv.n, lv.R,
-                                                                  enc.d_ptr + lv.c_ptr, enc.d_src + lv.c_edge,
-                                                                  enc.d_w + lv.c_edge);
+        launch_gather(rows, lv.off, lv.off + lv.n, lv.R, enc.d_ptr + lv.c_ptr, enc.d_src + lv.c_edge,
+                      enc.d_w + lv.c_edge, s);
         timer_end(s);
         if (!launch_ok("orion C gather")) return false;
     }
@@ -639,9 +660,8 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
         if (lv.RD == 0) continue;
         const long long next = lv.off + lv.n;
         timer_begin(s, kTagGather);
-        gather_kernel<<<(unsigned)((lv.RD + 7) / 8), 256, 0, s>>>(rows, next, next + lv.L, lv.RD,
-                                                                   enc.d_ptr + lv.d_ptr, enc.d_src + lv.d_edge,
-                                                                   enc.d_w + lv.d_edge);
+        launch_gather(rows, next, next + lv.L, lv.RD, enc.d_ptr + lv.d_ptr, enc.d_src + lv.d_edge,
+                      enc.d_w + lv.d_edge, s);
         timer_end(s);
         if (!launch_ok("orion D gather")) return false;
     }

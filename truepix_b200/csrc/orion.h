@@ -87,6 +87,19 @@ bool build_tree(unsigned char* tree, long long leaves, cudaStream_t s);
 // rows -> column-major codeword (the reference's encoded_codeword[c][r])
 bool rows_to_columns(const ulonglong2* rows, long long cw_len, ulonglong2* cols, cudaStream_t s);
 
+// Opening passes (orion_open.cu, src/VPD/linearPC.cpp:480-531,569-571) over the
+// rows written by commit(): combined[t] = sum_j r0[j] rows[t][j] (t < cw_len);
+// when tree != nullptr also the combined codeword's tree (leaves SHA256(x || 0^48),
+// 2 * tree_leaves(col_len) digests).
+bool combine(const ulonglong2* rows, long long col_len, long long cw_len, const ulonglong2* r0,
+             ulonglong2* combined, unsigned char* tree, cudaStream_t s);
+// out[i][.] = rows[q[i]][.] (the queried columns of the reference); synchronises
+// to report indices outside [0, cw_len)
+bool query_rows(const ulonglong2* rows, long long cw_len, const long long* q, int count, ulonglong2* out,
+                cudaStream_t s);
+// *out = sum_{i < n} r1[i] combined[i]
+bool answer(const ulonglong2* combined, const ulonglong2* r1, long long n, ulonglong2* out, cudaStream_t s);
+
 // `blocks` CTAs of 128 threads, each thread chaining `iters` SHA-256 of 64 bytes
 // in registers (2 compressions each); XORs its last digest into *out
 bool sha_peak(int blocks, int iters, uint32_t* out, cudaStream_t s);

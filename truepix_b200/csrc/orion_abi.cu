@@ -97,6 +97,56 @@ int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_
 
 int tp_orion_last_launches(void) { return tp::orion::last_launches(); }
 
+int tp_orion_combine_dev(const void* d_rows, long long N, const void* d_r0, void* d_combined, void* d_ctree,
+                         void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!check_n(N, "tp_orion_combine_dev")) return -1;
+    if (!d_rows || !d_r0 || !d_combined) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_combine_dev: null buffer");
+        return -1;
+    }
+    const long long col_len = N / tp::orion::kColumns;
+    return tp::orion::combine(static_cast<const ulonglong2*>(d_rows), col_len, tp::orion::codeword_len(col_len),
+                              static_cast<const ulonglong2*>(d_r0), static_cast<ulonglong2*>(d_combined),
+                              static_cast<unsigned char*>(d_ctree), reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_orion_query_columns_dev(const void* d_rows, long long N, const void* d_q, int count, void* d_out,
+                               void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!check_n(N, "tp_orion_query_columns_dev")) return -1;
+    if (!d_rows || !d_q || !d_out || count <= 0) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_query_columns_dev: bad arguments");
+        return -1;
+    }
+    const long long col_len = N / tp::orion::kColumns;
+    return tp::orion::query_rows(static_cast<const ulonglong2*>(d_rows), tp::orion::codeword_len(col_len),
+                                 static_cast<const long long*>(d_q), count, static_cast<ulonglong2*>(d_out),
+                                 reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_orion_answer_dev(const void* d_combined, long long msg_len, const void* d_r1, void* d_answer, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!d_combined || !d_r1 || !d_answer || msg_len <= 0) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_answer_dev: bad arguments");
+        return -1;
+    }
+    return tp::orion::answer(static_cast<const ulonglong2*>(d_combined), static_cast<const ulonglong2*>(d_r1),
+                             msg_len, static_cast<ulonglong2*>(d_answer), reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
 int tp_sha256_peak_dev(int blocks, int iters, void* d_out, void* stream)
 {
     tp::clear_error();

@@ -82,6 +82,9 @@ GKR_SIGNATURES = {
     "tp_orion_commit_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
     "tp_orion_rows_to_columns_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP]),
     "tp_orion_last_launches": (_I32, []),
+    "tp_orion_combine_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP, _VP, _VP]),
+    "tp_orion_query_columns_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _I32, _VP, _VP]),
+    "tp_orion_answer_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP, _VP]),
     "tp_sha256_peak_dev": (_I32, [_I32, _I32, _VP, _VP]),
     "tp_fft": (_I32, [_VP, _I32, _I32, _VP]),
     "tp_ifft": (_I32, [_VP, _I32, _I32, _VP]),
@@ -91,6 +94,8 @@ GKR_SIGNATURES = {
                            ctypes.c_longlong, _VP]),
     "tp_rs_commit": (_I32, [_VP, _I32, _VP, _VP]),
     "tp_rs_commit_dev": (_I32, [_VP, _I32, _VP, _VP, _VP]),
+    "tp_virgo_sumcheck_update_dev": (_I32, [_VP, _VP, _VP, ctypes.c_longlong, _U64, _U64, _I32, _VP, _VP,
+                                            _VP, _VP, _VP]),
 }
 
 _cache = {}
