@@ -730,6 +730,40 @@ def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
                     "tp_orion_commit (the whole tree back), pinned host buffers"}
 
 
+def profile_case(name):
+    """A short fixed workload for `ncu` captures (no timing, no JSON line):
+    orion = one 1080p Orion commit from bytes, one RS commit of 2^20 elements and
+    one 2^24-point forward NTT, through include/orion_gpu.h."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from orionlib import elements
+    from truepix_b200.frame import FrameLayout
+    assert name == "orion", name
+    lib = native.gkr()
+    dev = torch.device("cuda", 0)
+    s = torch.cuda.current_stream().cuda_stream
+    L = FrameLayout.for_frame(H, Wd)
+    n = L.padded_copies * L.n_wires
+    cw_len, leaves = lib.tp_orion_codeword_len(n // 128), lib.tp_orion_tree_leaves(n)
+    rng = np.random.default_rng(SEED)
+    pix = torch.from_numpy(rng.integers(0, 256, size=L.copies * L.copy_size, dtype=np.uint8)).to(dev)
+    rows = torch.empty(2 * 128 * cw_len, dtype=torch.int64, device=dev)
+    tree = torch.empty(64 * leaves, dtype=torch.uint8, device=dev)
+    native.check(lib, lib.tp_orion_commit_pixels_dev(pix.data_ptr(), L.copies, L.padded_copies, L.copy_size,
+                                                     L.n_wires, L.const_idx, L.const_val, rows.data_ptr(),
+                                                     tree.data_ptr(), s), "commit")
+    lg = 20
+    a = torch.from_numpy(elements(2, 1 << lg).view(np.int64)).to(dev)
+    cw = torch.empty(2 << (lg + 5), dtype=torch.int64, device=dev)
+    rt = torch.empty(32 << (lg - 1), dtype=torch.uint8, device=dev)
+    native.check(lib, lib.tp_rs_commit_dev(a.data_ptr(), lg, cw.data_ptr(), rt.data_ptr(), s), "rs commit")
+    m = 1 << 24
+    b = torch.from_numpy(elements(1, m).view(np.int64)).to(dev)
+    out = torch.empty_like(b)
+    native.check(lib, lib.tp_fft_dev(b.data_ptr(), m, m, out.data_ptr(), 1, 0, 0, s), "fft")
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -741,7 +775,11 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-ntt", action="store_true")
+    ap.add_argument("--profile-case", choices=["orion"], help="run a fixed short workload for ncu and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
