@@ -185,6 +185,13 @@ int tp_batch_n_copies(void* batch, int i);
 /* d_wires: frame i at d_wires + 16 * (sum of n_wires of frames < i) bytes -- with equal
  * n_wires simply [n_frames][n_wires] packed Fp2; d_beta: [n_frames] packed Fp2 */
 int tp_batch_finish(void* batch, void* d_wires, void* d_beta);
+/* Serving: frames join and leave a running batch between rounds. Finish frame i
+ * alone (its n_wires wires into d_wires, its beta into d_beta; NULL = the frame's
+ * staging buffer), then free its slot for tp_batch_set_* of a new frame while the
+ * others continue. tp_batch_release frees slot i without finishing; with
+ * free_buffers its tables go back to the pool (admission by HBM footprint). */
+int tp_batch_finish_frame(void* batch, int i, void* d_wires, void* d_beta);
+void tp_batch_release(void* batch, int i, int free_buffers);
 int tp_batch_launches(void* batch);
 /* forget every frame's configuration (tp_batch_set_* may be called again) while
  * keeping the device buffers for the next batch of the same or smaller sizes */

@@ -99,6 +99,11 @@ bool batch_fold(Batch* B, int i, fp2 r);
 // wires / beta of every frame into d_wires[i] (n_wires packed) / d_beta[i] (1 packed);
 // nullptr destinations use the frame's own staging buffer
 bool batch_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta);
+// one frame: its wires / beta (nullptr: the frame's staging buffer), then its slot
+// is free for a new frame (serving: frames join and leave between rounds)
+bool batch_finish_frame(Batch* B, int i, fp2* d_wires, fp2* d_beta);
+// free slot i without finishing; free_buffers also returns its tables to the pool
+void batch_release(Batch* B, int i, bool free_buffers);
 void batch_destroy(Batch* B);
 // forget every frame's configuration but keep its device buffers for reuse
 void batch_reset(Batch* B);

@@ -351,6 +351,48 @@ bool batch_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta)
     return launch_finish(B->d_jobs, (int)jobs.size(), max_w, B->stream, &B->launches);
 }
 
+bool batch_finish_frame(Batch* B, int i, fp2* d_wires, fp2* d_beta)
+{
+    if (i < 0 || i >= (int)B->frames.size()) {
+        set_error(TP_ERR_ARG, "frame index %d outside the batch", i);
+        return false;
+    }
+    Frame* f = B->frames[(size_t)i];
+    if (!f->configured || !f->buf[1]) {
+        set_error(TP_ERR_ARG, "frame %d is not configured", i);
+        return false;
+    }
+    if (f->pending && f->n_phys > 2 && !apply_fold(f, B->stream, &B->launches)) return false;
+    Job j = base_job(f);
+    j.kind = f->pending ? 1 : 0;
+    j.fin = d_wires ? d_wires : f->fin;
+    j.fin_beta = d_beta ? d_beta : f->fin + f->n_wires;
+    if (!ensure_workspace(B, 1, 1)) return false;
+    if (!upload_async(B->d_jobs, &j, sizeof(Job), B->stream)) return false;
+    if (!launch_finish(B->d_jobs, 1, f->n_wires, B->stream, &B->launches)) return false;
+    batch_release(B, i, false);
+    return true;
+}
+
+void batch_release(Batch* B, int i, bool free_buffers)
+{
+    if (i < 0 || i >= (int)B->frames.size()) return;
+    Frame* f = B->frames[(size_t)i];
+    f->configured = false;
+    f->n_copies = 0;
+    f->pending = false;
+    if (free_buffers) {
+        cudaStream_t s = B->stream;
+        if (!f->borrowed0) dev_free(f->buf[0], s);
+        dev_free(f->buf[1], s);
+        dev_free(f->beta[0], s);
+        dev_free(f->beta[1], s);
+        f->buf[0] = f->buf[1] = f->beta[0] = f->beta[1] = nullptr;
+        f->cap0 = f->cap1 = f->capb = 0;
+        f->borrowed0 = false;
+    }
+}
+
 void batch_reset(Batch* B)
 {
     for (Frame* f : B->frames) {

@@ -563,6 +563,21 @@ int tp_batch_finish(void* batch, void* d_wires, void* d_beta)
     return tp::batch_finish(B, w.data(), b.data()) ? 0 : -1;
 }
 
+int tp_batch_finish_frame(void* batch, int i, void* d_wires, void* d_beta)
+{
+    tp::clear_error();
+    if (!batch) return -1;
+    return tp::batch_finish_frame(static_cast<tp::Batch*>(batch), i, static_cast<fp2*>(d_wires),
+                                  static_cast<fp2*>(d_beta))
+               ? 0
+               : -1;
+}
+
+void tp_batch_release(void* batch, int i, int free_buffers)
+{
+    if (batch) tp::batch_release(static_cast<tp::Batch*>(batch), i, free_buffers != 0);
+}
+
 int tp_batch_launches(void* batch) { return batch ? static_cast<tp::Batch*>(batch)->launches : 0; }
 
 void tp_batch_destroy(void* batch) { tp::batch_destroy(static_cast<tp::Batch*>(batch)); }

@@ -66,6 +66,8 @@ GKR_SIGNATURES = {
     "tp_batch_launches": (_I32, [_VP]),
     "tp_batch_destroy": (None, [_VP]),
     "tp_batch_reset": (None, [_VP]),
+    "tp_batch_finish_frame": (_I32, [_VP, _I32, _VP, _VP]),
+    "tp_batch_release": (None, [_VP, _I32, _I32]),
     "tp_compute_beta_batch_dev": (_I32, [_VP, _I32, _I32, _VP, _VP]),
     "tp_mle_eval_pixels_batch": (_I32, [_I32, ctypes.POINTER(_VP), _PI32, _I32, _I32, _I32, _I32,
                                         _U64, _VP, _VP, _VP]),

@@ -1,0 +1,289 @@
+"""Serving loop: continuous batching of frame proofs on one GPU.
+
+Requests (an operation's circuit, a frame of some resolution, a seed for its
+transcript values) arrive over time. The server keeps up to `slots` proofs in
+flight in one tp_batch: every tick runs ONE claim launch per source kind for all
+frames in their early sumcheck rounds, whatever round each is in, reads the
+claims back (the host transcript needs them), and folds each frame by its own
+challenge. A frame whose early rounds are over is finished alone
+(tp_batch_finish_frame), its input MLE evaluated from its bytes, and its Orion
+commitment queued on a second stream, so commits overlap the rounds of the
+frames still in flight; its slot is free for the next request at once. Requests
+are admitted while a slot is free and the frame's HBM footprint fits the budget.
+
+The frame layout and the per-round work are those of truepix_b200.frame and
+truepix_b200.orion (TruePix-main/libTruePix/layerprover.py:144-290 drives the
+same early rounds one frame at a time). Challenges, z1, z2 and the MLE point
+are derived from each request's seed; a request's results do not depend on what
+else is in flight (tests/test_gpu_serving.py checks this).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import native
+from .frame import FrameLayout, pack_fp2
+
+P61 = (1 << 61) - 1
+
+
+@dataclass
+class Circuit:
+    """One layer's gate table and the frame layout it reads (copy_size inputs per
+    copy, constant wire, 512 wires per copy)."""
+    name: str
+    gate_type: np.ndarray
+    in0: np.ndarray
+    in1: np.ndarray
+    copy_size: int = 384
+    const_idx: int = 384
+    const_val: int = 128
+
+
+@dataclass
+class Request:
+    rid: int
+    circuit: Circuit
+    height: int
+    width: int
+    pixels: np.ndarray            # uint8, height * width * 3 bytes (host)
+    seed: int
+    arrival: float = 0.0          # seconds after the start of the run
+
+
+@dataclass
+class Result:
+    rid: int
+    claims: np.ndarray            # [rounds, 8] u64
+    wires: np.ndarray             # [512, 2] u64
+    beta: tuple
+    mle: tuple
+    root: bytes
+    arrival: float = 0.0
+    done: float = 0.0
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+def transcript_values(seed: int, n_gates: int, n_copy_bits: int, n_in_bits: int):
+    """z1 [2, n_gates], z2 [n_copy_bits, 2], point [n_in_bits + n_copy_bits, 2],
+    challenges [n_copy_bits, 2]: canonical, from the request's seed (they stand in
+    for the Fiat-Shamir transcript, which stays on the host)."""
+    rng = np.random.default_rng(seed)
+    f = lambda *shape: rng.integers(0, P61, size=shape, dtype=np.uint64)
+    return f(2, n_gates), f(n_copy_bits, 2), f(n_in_bits + n_copy_bits, 2), f(n_copy_bits, 2)
+
+
+def layout_for(c: Circuit, height: int, width: int) -> FrameLayout:
+    copies = math.ceil(height * width * 3 / c.copy_size)
+    return FrameLayout(copies=copies, copy_size=c.copy_size, n_wires=512, const_idx=c.const_idx,
+                       const_val=c.const_val)
+
+
+class _Job:
+    def __init__(self, srv, req: Request, slot: int):
+        torch = srv.torch
+        self.req, self.slot = req, slot
+        c = req.circuit
+        self.L = L = layout_for(c, req.height, req.width)
+        nb, ni = L.n_copy_bits, L.n_in_bits
+        self.z1, z2, point, self.chal = transcript_values(req.seed, c.gate_type.size, nb, ni)
+        dev, s = srv.dev, srv.stream
+        with torch.cuda.stream(s):
+            pix = np.zeros(L.copies * L.copy_size, np.uint8)
+            pix[:req.pixels.size] = req.pixels.reshape(-1)[:pix.size]
+            self.pix = torch.from_numpy(pix).to(dev, non_blocking=False)
+            self.z2 = torch.from_numpy(pack_fp2(z2[:, 0], z2[:, 1])).to(dev)
+            self.point = torch.from_numpy(pack_fp2(point[:, 0], point[:, 1])).to(dev)
+            self.beta = torch.empty(2 * L.padded_copies, dtype=torch.int64, device=dev)
+            self.wires = torch.zeros(2 * (L.n_wires + 1), dtype=torch.int64, device=dev)
+            self.mle = torch.zeros(2, dtype=torch.int64, device=dev)
+        n = L.padded_copies * L.n_wires
+        self.cw_len = srv.lib.tp_orion_codeword_len(n // 128)
+        self.leaves = srv.lib.tp_orion_tree_leaves(n)
+        self.rows = torch.empty(2 * 128 * self.cw_len, dtype=torch.int64, device=dev)
+        self.tree = torch.empty(64 * self.leaves, dtype=torch.uint8, device=dev)
+        self.round = 0
+        self.host_claims = []          # what the host transcript read, round by round
+        self.done_event = None
+        self.footprint = srv.footprint(L)
+
+    def rounds(self) -> int:
+        return self.L.n_copy_bits
+
+
+class ProofServer:
+    """Continuous batching of frame proofs (see the module docstring)."""
+
+    def __init__(self, slots: int = 64, hbm_budget: float = 40e9, device: int = 0):
+        import torch
+        self.torch = torch
+        self.lib = native.gkr()
+        self.dev = torch.device("cuda", device)
+        self.stream = torch.cuda.Stream(self.dev)
+        self.commit_stream = torch.cuda.Stream(self.dev)
+        self.slots = slots
+        self.budget = hbm_budget
+        self.batch = self.lib.tp_batch_create(slots, self.stream.cuda_stream)
+        if not self.batch:
+            native.check(self.lib, -1, "batch_create")
+        self.free = list(range(slots))[::-1]
+        self.active: dict = {}          # slot -> _Job
+        self.committing: list = []      # jobs whose commit is queued
+        self.used = 0.0
+        self.d_claims = torch.zeros(8 * slots, dtype=torch.int64, device=self.dev)
+        self.h_claims = torch.zeros(8 * slots, dtype=torch.int64).pin_memory()
+        self.chal = np.zeros((slots, 2), np.uint64)
+        self.ticks = 0
+        self.launches = 0
+
+    def __del__(self):
+        try:
+            if self.batch:
+                self.lib.tp_batch_destroy(self.batch)
+                self.batch = None
+        except Exception:
+            pass
+
+    @staticmethod
+    def footprint(L: FrameLayout) -> float:
+        """HBM held by one proof in flight: folded tables (rows x C/2 + rows x C/4),
+        beta, the frame's bytes, the codeword (cw_len x 2 KB) and its tree."""
+        rows = L.const_idx + 1 if L.const_idx >= 0 else L.copy_size
+        C = L.padded_copies
+        col = C * L.n_wires // 128
+        cw = col * 1.72 + 64
+        leaves = 1 << math.ceil(math.log2(2 * col))
+        return 16 * rows * (C // 2 + C // 4) + 32 * C + L.copies * L.copy_size + 2048 * cw + 64 * leaves
+
+    def _start(self, req: Request):
+        lib, s = self.lib, self.stream.cuda_stream
+        slot = self.free.pop()
+        job = _Job(self, req, slot)
+        L, c = job.L, req.circuit
+        native.check(lib, lib.tp_compute_beta_dev(job.z2.data_ptr(), L.n_copy_bits, 1, 0,
+                                                  job.beta.data_ptr(), s), "beta")
+        z1r = np.ascontiguousarray(job.z1[0])
+        z1i = np.ascontiguousarray(job.z1[1])
+        gt = np.ascontiguousarray(c.gate_type, np.int32)
+        i0 = np.ascontiguousarray(c.in0, np.int32)
+        i1 = np.ascontiguousarray(c.in1, np.int32)
+        native.check(lib, lib.tp_batch_set_pixels(
+            self.batch, slot, gt.size, gt.ctypes.data, i0.ctypes.data, i1.ctypes.data,
+            z1r.ctypes.data, z1i.ctypes.data, job.pix.data_ptr(), L.copies, L.padded_copies,
+            L.copy_size, L.n_wires, L.const_idx, L.const_val, job.beta.data_ptr()), "set_pixels")
+        self.active[slot] = job
+        self.used += job.footprint
+
+    def _finish(self, job: _Job):
+        torch, lib, s = self.torch, self.lib, self.stream.cuda_stream
+        L = job.L
+        wp = job.wires.data_ptr()
+        native.check(lib, lib.tp_batch_finish_frame(self.batch, job.slot, wp, wp + 16 * L.n_wires),
+                     "finish_frame")
+        lib.tp_batch_release(self.batch, job.slot, 1)
+        native.check(lib, lib.tp_mle_eval_pixels(job.pix.data_ptr(), L.copies, L.padded_copies,
+                                                 L.copy_size, L.n_wires, L.const_idx, L.const_val,
+                                                 job.point.data_ptr(), job.mle.data_ptr(), s), "mle")
+        ev = torch.cuda.Event()
+        ev.record(self.stream)
+        self.commit_stream.wait_event(ev)
+        native.check(lib, lib.tp_orion_commit_pixels_dev(
+            job.pix.data_ptr(), L.copies, L.padded_copies, L.copy_size, L.n_wires, L.const_idx,
+            L.const_val, job.rows.data_ptr(), job.tree.data_ptr(), self.commit_stream.cuda_stream),
+            "commit")
+        self.launches += lib.tp_orion_last_launches() + 3
+        job.done_event = torch.cuda.Event()
+        job.done_event.record(self.commit_stream)
+        del self.active[job.slot]
+        self.free.append(job.slot)
+        self.committing.append(job)
+
+    def _collect(self, t0: float, out: list, block: bool = False):
+        keep = []
+        for job in self.committing:
+            if block:
+                job.done_event.synchronize()
+            if job.done_event.query():
+                c = np.stack(job.host_claims)
+                w = job.wires.cpu().numpy().view(np.uint64).reshape(job.L.n_wires + 1, 2)
+                m = job.mle.cpu().numpy().view(np.uint64)
+                root = job.tree[32:64].cpu().numpy().tobytes()
+                out.append(Result(job.req.rid, c, w[:job.L.n_wires].copy(), (int(w[-1, 0]), int(w[-1, 1])),
+                                  (int(m[0]), int(m[1])), root, job.req.arrival, time.perf_counter() - t0))
+                self.used -= job.footprint
+            else:
+                keep.append(job)
+        self.committing = keep
+
+    def tick(self):
+        """One round for every frame in flight: claim (one launch per source kind),
+        claims to the host, fold each frame by its own challenge."""
+        lib, torch = self.lib, self.torch
+        if not self.active:
+            return
+        l0 = lib.tp_batch_launches(self.batch)
+        native.check(lib, lib.tp_batch_claim(self.batch, self.d_claims.data_ptr()), "batch_claim")
+        with torch.cuda.stream(self.stream):
+            self.h_claims.copy_(self.d_claims, non_blocking=True)
+        self.stream.synchronize()                   # the host transcript reads the claims
+        hc = self.h_claims.numpy().view(np.uint64).reshape(self.slots, 8)
+        self.chal[:] = 0
+        for slot, job in self.active.items():
+            job.host_claims.append(hc[slot].copy())  # absorbed into the frame's transcript
+            self.chal[slot] = job.chal[job.round]
+            job.round += 1
+        native.check(lib, lib.tp_batch_fold(
+            self.batch, self.chal.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))), "batch_fold")
+        for job in [j for j in self.active.values() if j.round == j.rounds()]:
+            self._finish(job)
+        self.launches += lib.tp_batch_launches(self.batch) - l0
+        self.ticks += 1
+
+    def run(self, requests, realtime: bool = True):
+        """Serve `requests` (sorted by arrival). realtime: a request enters the
+        queue when the wall clock reaches its arrival time; otherwise arrivals are
+        in ticks (arrival = tick index). Returns the results in completion order."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        queue, out = [], []
+        i = 0
+        t0 = time.perf_counter()
+        while i < len(reqs) or queue or self.active or self.committing:
+            now = time.perf_counter() - t0 if realtime else float(self.ticks)
+            while i < len(reqs) and reqs[i].arrival <= now:
+                queue.append(reqs[i])
+                i += 1
+            while queue and self.free:
+                L = layout_for(queue[0].circuit, queue[0].height, queue[0].width)
+                if self.active and self.used + self.footprint(L) > self.budget:
+                    break
+                req = queue.pop(0)
+                if not realtime:
+                    req.arrival = time.perf_counter() - t0
+                self._start(req)
+            if self.active:
+                self.tick()
+            elif not queue and i < len(reqs):
+                if realtime:
+                    time.sleep(max(0.0, min(0.001, reqs[i].arrival - now)))
+                else:
+                    self.ticks += 1
+            self._collect(t0, out, block=not self.active and not queue and i >= len(reqs))
+        return out
+
+
+def latency_stats(results):
+    lat = sorted(r.latency for r in results)
+    if not lat:
+        return {}
+    pick = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
+    span = max(r.done for r in results) - min(r.arrival for r in results)
+    return {"p50_ms": 1e3 * pick(0.5), "p99_ms": 1e3 * pick(0.99), "mean_ms": 1e3 * sum(lat) / len(lat),
+            "frames": len(lat), "frames_per_s": len(lat) / span if span > 0 else None}
