@@ -568,12 +568,18 @@ def ours_arm(args, rank, world, local_rank):
         c, w, b, m = bprover.results(B - 1)
         res_ok = bool(c.any() and w.any() and m != (0, 0) and any(committer.root(B - 1)))
 
-    ntt = e2e = e2e_ref = cpu = None
+    ntt = e2e = e2e_ref = cpu = uneven = serving = None
     if rank == 0 and not args.skip_ntt:
         ntt = ntt_bench(lib, dev, stream)
     if rank == 0 and not args.skip_e2e:
         e2e = e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream, dev)
         e2e_ref = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
+    if rank == 0 and not args.skip_serving:
+        del bprover
+        committer.rows = committer.trees = None
+        torch.cuda.empty_cache()
+        uneven = batched_uneven()
+        serving = serving_sweep()
     if rank == 0 and world == 1 and not args.skip_cpu:
         secs, kind = _cpu_worker((0, 1))
         cpu = {"value": 1.0 / secs, "unit": UNIT, "cores": 1, "kind": kind,
@@ -610,7 +616,7 @@ def ours_arm(args, rank, world, local_rank):
                                      "p99": per_batch[min(len(per_batch) - 1,
                                                           int(0.99 * len(per_batch)))]},
             "roofline": roof, "roofline_fold_kernel": roof_fold, "kernels": kernels,
-            "ntt": ntt, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
+            "ntt": ntt, "batched_uneven": uneven, "serving": serving, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
             "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
         }
         print(json.dumps(line), flush=True)
@@ -730,6 +736,74 @@ def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
                     "tp_orion_commit (the whole tree back), pinned host buffers"}
 
 
+def serving_circuits():
+    from truepix_b200.serving import Circuit
+    c = np.load(os.path.join(ROOT, "tests", "golden", "circuits.npz"))
+    g = lambda n: (c[n + "_type"], c[n + "_in0"], c[n + "_in1"])
+    return {"gray": Circuit("gray", *g("gray"), 384, 384, 128),
+            "mask": Circuit("mask", *g("mask"), 384, -1, 0),
+            "crop": Circuit("crop", *g("Crop"), 385, -1, 0)}
+
+
+def batched_uneven(seed=4):
+    """64 crop-then-gray frames of uneven size proven as one batch: sources 240p to
+    1080p (16:9), crop fractions x1 < x2, y1 < y2 uniform in [0, 1] (seeded); the
+    cropped region goes through the gray circuit (2^14 .. 2^23 input wires)."""
+    from truepix_b200.serving import ProofServer, Request, latency_stats
+    rng = np.random.default_rng(seed)
+    gray = serving_circuits()["gray"]
+    heights = [240, 360, 480, 720, 1080]
+    reqs = []
+    for i in range(64):
+        h = int(rng.choice(heights))
+        w = (h * 16 + 8) // 9
+        x = np.sort(rng.random(2))
+        y = np.sort(rng.random(2))
+        cw, ch = max(1, int(round((x[1] - x[0]) * w))), max(1, int(round((y[1] - y[0]) * h)))
+        reqs.append(Request(i, gray, ch, cw, rng.integers(0, 256, size=ch * cw * 3, dtype=np.uint8),
+                            seed=9000 + i, arrival=0.0))
+    srv = ProofServer(slots=64, hbm_budget=80e9)
+    srv.run(reqs[:8], realtime=False)              # warm-up (graphs, twiddles, pools)
+    res = srv.run(reqs, realtime=False)
+    st = latency_stats(res)
+    wires = sorted(1 << (9 + int(np.log2(max(2, 1 << int(np.ceil(np.log2(max(2, -(-r.height * r.width * 3 // 384)))))))))
+                   for r in reqs)
+    return {"workload": "64 crop-then-gray frames, sources 240p-1080p, seeded crops", "frames": len(res),
+            "frames_per_s": st.get("frames_per_s"), "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"),
+            "input_wires_min": wires[0], "input_wires_max": wires[-1], "ticks": srv.ticks,
+            "what": "GKR early rounds + MLE + Orion commit per frame, continuous batch of 64 slots"}
+
+
+def serving_sweep(rates=(100, 250, 500), n_req=96, seed=5):
+    """Poisson arrivals of gray / crop / mask proofs of 360p .. 2160p frames at rate
+    lambda (frames/s), real time, admission by HBM footprint (60 GB budget)."""
+    from truepix_b200.serving import ProofServer, Request, latency_stats
+    cs = serving_circuits()
+    sizes = [(360, 640), (480, 854), (720, 1280), (1080, 1920), (1440, 2560), (2160, 3840)]
+    rng = np.random.default_rng(seed)
+    frames = {hw: [rng.integers(0, 256, size=hw[0] * hw[1] * 3, dtype=np.uint8) for _ in range(2)]
+              for hw in sizes}
+    srv = ProofServer(slots=64, hbm_budget=60e9)
+    out = []
+    warm = [Request(k, cs["gray"], *sizes[k % len(sizes)], frames[sizes[k % len(sizes)]][0], seed=k)
+            for k in range(len(sizes))]
+    srv.run(warm, realtime=False)
+    for lam in rates:
+        t = 0.0
+        reqs = []
+        for i in range(n_req):
+            t += rng.exponential(1.0 / lam)
+            hw = sizes[int(rng.integers(len(sizes)))]
+            op = ["gray", "crop", "mask"][int(rng.integers(3))]
+            reqs.append(Request(i, cs[op], hw[0], hw[1], frames[hw][i % 2], seed=77 + i, arrival=t))
+        res = srv.run(reqs, realtime=True)
+        st = latency_stats(res)
+        st["lambda_per_s"] = lam
+        out.append(st)
+    return {"workload": "Poisson requests, ops gray/crop/mask uniform, 360p-2160p uniform, %d per rate" % n_req,
+            "slots": 64, "hbm_budget_gb": 60, "by_rate": out}
+
+
 def profile_case(name):
     """A short fixed workload for `ncu` captures (no timing, no JSON line):
     orion = one 1080p Orion commit from bytes, one RS commit of 2^20 elements and
@@ -775,6 +849,7 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-ntt", action="store_true")
+    ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--profile-case", choices=["orion"], help="run a fixed short workload for ncu and exit")
     args = ap.parse_args()
     if args.profile_case:
