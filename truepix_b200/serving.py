@@ -22,7 +22,7 @@ from __future__ import annotations
 import ctypes
 import math
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -88,31 +88,30 @@ def layout_for(c: Circuit, height: int, width: int) -> FrameLayout:
 
 
 class _Job:
+    """One request in flight: its layout, transcript values, and views into the
+    slot's persistent device buffers."""
+
     def __init__(self, srv, req: Request, slot: int):
-        torch = srv.torch
         self.req, self.slot = req, slot
         c = req.circuit
         self.L = L = layout_for(c, req.height, req.width)
+        if L.copies * L.copy_size > srv.max_bytes or L.padded_copies > srv.max_copies:
+            raise ValueError("request %d: frame larger than the server's maximum" % req.rid)
         nb, ni = L.n_copy_bits, L.n_in_bits
         self.z1, z2, point, self.chal = transcript_values(req.seed, c.gate_type.size, nb, ni)
-        dev, s = srv.dev, srv.stream
-        with torch.cuda.stream(s):
-            pix = np.zeros(L.copies * L.copy_size, np.uint8)
-            pix[:req.pixels.size] = req.pixels.reshape(-1)[:pix.size]
-            self.pix = torch.from_numpy(pix).to(dev, non_blocking=False)
-            self.z2 = torch.from_numpy(pack_fp2(z2[:, 0], z2[:, 1])).to(dev)
-            self.point = torch.from_numpy(pack_fp2(point[:, 0], point[:, 1])).to(dev)
-            self.beta = torch.empty(2 * L.padded_copies, dtype=torch.int64, device=dev)
-            self.wires = torch.zeros(2 * (L.n_wires + 1), dtype=torch.int64, device=dev)
-            self.mle = torch.zeros(2, dtype=torch.int64, device=dev)
-        n = L.padded_copies * L.n_wires
-        self.cw_len = srv.lib.tp_orion_codeword_len(n // 128)
-        self.leaves = srv.lib.tp_orion_tree_leaves(n)
-        self.rows = torch.empty(2 * 128 * self.cw_len, dtype=torch.int64, device=dev)
-        self.tree = torch.empty(64 * self.leaves, dtype=torch.uint8, device=dev)
+        b = srv.slot_bufs[slot]
+        self.pix = b["pix"][:L.copies * L.copy_size]
+        self.beta = b["beta"][:2 * L.padded_copies]
+        self.z2 = b["z2"][:2 * nb]
+        self.point = b["point"][:2 * (ni + nb)]
+        self.wires, self.mle = b["wires"], b["mle"]
+        srv.upload(self.pix, req.pixels, L.copies * L.copy_size)
+        self.z2.copy_(srv.torch.from_numpy(pack_fp2(z2[:, 0], z2[:, 1])))
+        self.point.copy_(srv.torch.from_numpy(pack_fp2(point[:, 0], point[:, 1])))
         self.round = 0
         self.host_claims = []          # what the host transcript read, round by round
         self.done_event = None
+        self.commit_buf = None
         self.footprint = srv.footprint(L)
 
     def rounds(self) -> int:
@@ -120,9 +119,18 @@ class _Job:
 
 
 class ProofServer:
-    """Continuous batching of frame proofs (see the module docstring)."""
+    """Continuous batching of frame proofs (see the module docstring).
 
-    def __init__(self, slots: int = 64, hbm_budget: float = 40e9, device: int = 0):
+    Device memory is allocated once: per slot the frame's bytes, beta and the
+    small transcript / result vectors (sized for max_height x max_width); the
+    slot's folded tables stay in the library's pool for the next frame; and
+    `commit_buffers` codeword + tree buffers that commits take in turn (a commit
+    waits for a free one). A served frame's codeword is recycled once its root
+    is read, so Result carries the root; a prover that opens the commitment
+    later keeps the codeword instead (truepix_b200.orion.FrameCommitter)."""
+
+    def __init__(self, slots: int = 64, hbm_budget: float = 40e9, device: int = 0, max_height: int = 2160,
+                 max_width: int = 3840, commit_buffers: int = 4):
         import torch
         self.torch = torch
         self.lib = native.gkr()
@@ -134,15 +142,37 @@ class ProofServer:
         self.batch = self.lib.tp_batch_create(slots, self.stream.cuda_stream)
         if not self.batch:
             native.check(self.lib, -1, "batch_create")
+        self.max_bytes = max_height * max_width * 3 + 512
+        self.max_copies = 1 << math.ceil(math.log2(max(2, -(-max_height * max_width * 3 // 384))))
+        nbmax = int(math.log2(self.max_copies))
+        i64, dev = torch.int64, self.dev
+        self.slot_bufs = [{"pix": torch.zeros(self.max_bytes, dtype=torch.uint8, device=dev),
+                           "beta": torch.empty(2 * self.max_copies, dtype=i64, device=dev),
+                           "z2": torch.empty(2 * nbmax, dtype=i64, device=dev),
+                           "point": torch.empty(2 * (9 + nbmax), dtype=i64, device=dev),
+                           "wires": torch.zeros(2 * 513, dtype=i64, device=dev),
+                           "mle": torch.zeros(2, dtype=i64, device=dev)} for _ in range(slots)]
+        col = self.max_copies * 512 // 128
+        cw_max = self.lib.tp_orion_codeword_len(col)
+        leaves_max = self.lib.tp_orion_tree_leaves(col * 128)
+        self.commit_free = [(torch.empty(2 * 128 * cw_max, dtype=i64, device=dev),
+                             torch.empty(64 * leaves_max, dtype=torch.uint8, device=dev))
+                            for _ in range(commit_buffers)]
+        # two pinned staging buffers for frame uploads (one may be in flight)
+        self.staging = [torch.empty(self.max_bytes, dtype=torch.uint8).pin_memory() for _ in range(2)]
+        self.staging_ev = [None, None]
+        self.staging_next = 0
         self.free = list(range(slots))[::-1]
         self.active: dict = {}          # slot -> _Job
-        self.committing: list = []      # jobs whose commit is queued
+        self.committing: list = []      # jobs whose commit is queued, oldest first
         self.used = 0.0
-        self.d_claims = torch.zeros(8 * slots, dtype=torch.int64, device=self.dev)
-        self.h_claims = torch.zeros(8 * slots, dtype=torch.int64).pin_memory()
+        self.d_claims = torch.zeros(8 * slots, dtype=i64, device=dev)
+        self.h_claims = torch.zeros(8 * slots, dtype=i64).pin_memory()
         self.chal = np.zeros((slots, 2), np.uint64)
         self.ticks = 0
         self.launches = 0
+        self._t0 = time.perf_counter()
+        self._out = []
 
     def __del__(self):
         try:
@@ -163,10 +193,29 @@ class ProofServer:
         leaves = 1 << math.ceil(math.log2(2 * col))
         return 16 * rows * (C // 2 + C // 4) + 32 * C + L.copies * L.copy_size + 2048 * cw + 64 * leaves
 
+    def upload(self, d_pix, pixels: np.ndarray, n: int):
+        """Frame bytes to the slot's device buffer through a pinned staging buffer
+        (zero-padded to the layout's copies x copy_size)."""
+        torch = self.torch
+        k = self.staging_next
+        self.staging_next ^= 1
+        if self.staging_ev[k] is not None:
+            self.staging_ev[k].synchronize()
+        h = self.staging[k].numpy()
+        m = min(n, pixels.size)
+        h[:m] = pixels.reshape(-1)[:m]
+        h[m:n] = 0
+        with torch.cuda.stream(self.stream):
+            d_pix.copy_(self.staging[k][:n], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+        self.staging_ev[k] = ev
+
     def _start(self, req: Request):
         lib, s = self.lib, self.stream.cuda_stream
         slot = self.free.pop()
-        job = _Job(self, req, slot)
+        with self.torch.cuda.stream(self.stream):
+            job = _Job(self, req, slot)
         L, c = job.L, req.circuit
         native.check(lib, lib.tp_compute_beta_dev(job.z2.data_ptr(), L.n_copy_bits, 1, 0,
                                                   job.beta.data_ptr(), s), "beta")
@@ -188,37 +237,43 @@ class ProofServer:
         wp = job.wires.data_ptr()
         native.check(lib, lib.tp_batch_finish_frame(self.batch, job.slot, wp, wp + 16 * L.n_wires),
                      "finish_frame")
-        lib.tp_batch_release(self.batch, job.slot, 1)
         native.check(lib, lib.tp_mle_eval_pixels(job.pix.data_ptr(), L.copies, L.padded_copies,
                                                  L.copy_size, L.n_wires, L.const_idx, L.const_val,
                                                  job.point.data_ptr(), job.mle.data_ptr(), s), "mle")
+        while not self.commit_free:                 # back-pressure: wait for the oldest commit
+            self._collect(block_first=True)
+        job.commit_buf = rows, tree = self.commit_free.pop()
         ev = torch.cuda.Event()
         ev.record(self.stream)
         self.commit_stream.wait_event(ev)
         native.check(lib, lib.tp_orion_commit_pixels_dev(
             job.pix.data_ptr(), L.copies, L.padded_copies, L.copy_size, L.n_wires, L.const_idx,
-            L.const_val, job.rows.data_ptr(), job.tree.data_ptr(), self.commit_stream.cuda_stream),
-            "commit")
+            L.const_val, rows.data_ptr(), tree.data_ptr(), self.commit_stream.cuda_stream), "commit")
         self.launches += lib.tp_orion_last_launches() + 3
         job.done_event = torch.cuda.Event()
         job.done_event.record(self.commit_stream)
         del self.active[job.slot]
-        self.free.append(job.slot)
         self.committing.append(job)
 
-    def _collect(self, t0: float, out: list, block: bool = False):
+    def _collect(self, block: bool = False, block_first: bool = False):
+        """Results of the commits that are done (all of them when block; at least
+        the oldest when block_first); their slots and commit buffers return."""
         keep = []
-        for job in self.committing:
-            if block:
+        for q, job in enumerate(self.committing):
+            if block or (block_first and q == 0):
                 job.done_event.synchronize()
             if job.done_event.query():
                 c = np.stack(job.host_claims)
-                w = job.wires.cpu().numpy().view(np.uint64).reshape(job.L.n_wires + 1, 2)
+                w = job.wires.cpu().numpy().view(np.uint64).reshape(513, 2)
                 m = job.mle.cpu().numpy().view(np.uint64)
-                root = job.tree[32:64].cpu().numpy().tobytes()
-                out.append(Result(job.req.rid, c, w[:job.L.n_wires].copy(), (int(w[-1, 0]), int(w[-1, 1])),
-                                  (int(m[0]), int(m[1])), root, job.req.arrival, time.perf_counter() - t0))
+                root = job.commit_buf[1][32:64].cpu().numpy().tobytes()
+                self._out.append(Result(job.req.rid, c, w[:job.L.n_wires].copy(),
+                                        (int(w[job.L.n_wires, 0]), int(w[job.L.n_wires, 1])),
+                                        (int(m[0]), int(m[1])), root, job.req.arrival,
+                                        time.perf_counter() - self._t0))
                 self.used -= job.footprint
+                self.commit_free.append(job.commit_buf)
+                self.free.append(job.slot)
             else:
                 keep.append(job)
         self.committing = keep
@@ -252,9 +307,10 @@ class ProofServer:
         queue when the wall clock reaches its arrival time; otherwise arrivals are
         in ticks (arrival = tick index). Returns the results in completion order."""
         reqs = sorted(requests, key=lambda r: r.arrival)
-        queue, out = [], []
+        queue = []
+        self._out = []
         i = 0
-        t0 = time.perf_counter()
+        self._t0 = t0 = time.perf_counter()
         while i < len(reqs) or queue or self.active or self.committing:
             now = time.perf_counter() - t0 if realtime else float(self.ticks)
             while i < len(reqs) and reqs[i].arrival <= now:
@@ -262,7 +318,7 @@ class ProofServer:
                 i += 1
             while queue and self.free:
                 L = layout_for(queue[0].circuit, queue[0].height, queue[0].width)
-                if self.active and self.used + self.footprint(L) > self.budget:
+                if (self.active or self.committing) and self.used + self.footprint(L) > self.budget:
                     break
                 req = queue.pop(0)
                 if not realtime:
@@ -275,8 +331,9 @@ class ProofServer:
                     time.sleep(max(0.0, min(0.001, reqs[i].arrival - now)))
                 else:
                     self.ticks += 1
-            self._collect(t0, out, block=not self.active and not queue and i >= len(reqs))
-        return out
+            self._collect(block=not self.active and not queue and i >= len(reqs),
+                          block_first=not self.active and bool(queue))
+        return self._out
 
 
 def latency_stats(results):
