@@ -374,6 +374,7 @@ def sha_peak(lib, dev, stream):
 def ntt_bench(lib, dev, stream, reps=5):
     """Config-2 microbenchmark: forward NTT, inverse NTT and the rate-2^-5 RS
     commit (IFFT + FFT per slice, FRI leaf chains, Merkle tree) at 2^16, 2^20, 2^24."""
+    import ctypes
     import torch
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from orionlib import elements
@@ -399,6 +400,11 @@ def ntt_bench(lib, dev, stream, reps=5):
             torch.cuda.synchronize()
             return e0.elapsed_time(e1) / reps
 
+        t_default = timed(lambda: native.check(lib, lib.tp_fft_dev(a.data_ptr(), n, n, f.data_ptr(), 1, 0, 0, s)))
+        digits = (ctypes.c_int * 3)()
+        tms = ctypes.c_float()
+        passes = lib.tp_ntt_autotune(lg, 1, digits, ctypes.byref(tms))
+        native.check(lib, 0 if passes > 0 else -1, "ntt autotune")
         t_f = timed(lambda: native.check(lib, lib.tp_fft_dev(a.data_ptr(), n, n, f.data_ptr(), 1, 0, 0, s)))
         t_i = timed(lambda: native.check(lib, lib.tp_ifft_dev(f.data_ptr(), n, n, back.data_ptr(), 1, 0, 0, s)))
         t_rs = timed(lambda: native.check(lib, lib.tp_rs_commit_dev(a.data_ptr(), lg, cw.data_ptr(),
@@ -406,9 +412,9 @@ def ntt_bench(lib, dev, stream, reps=5):
         ok = bool(torch.equal(back, a))
         leaves = 1 << (lg - 2)
         comp = leaves * 64 * 2 + (leaves - 1) * 2
-        passes = 1 if lg <= 10 else (2 if lg <= 20 else 3)
         out["2^%d" % lg] = {
-            "fft_ms": t_f, "ifft_ms": t_i, "round_trip_exact": ok,
+            "fft_ms": t_f, "fft_ms_default_split": t_default,
+            "autotuned_radix_bits": [int(x) for x in digits[:passes]], "ifft_ms": t_i, "round_trip_exact": ok,
             "fft_elem_per_s": n / (t_f / 1e3), "butterflies_per_s": n / 2 * lg / (t_f / 1e3),
             "fft_hbm_gbs": passes * 32 * n / (t_f / 1e3) / 1e9,
             "rs_commit_ms": t_rs, "rs_codeword_elements": n << 5,

@@ -114,6 +114,15 @@ int tp_fft_dev(const void* d_coef, long long coef_len, long long order, void* d_
 int tp_ifft_dev(const void* d_evals, long long coef_len, long long order, void* d_out, int batch,
                 long long in_stride, long long out_stride, void* stream);
 
+/* Autotuner for the transforms above (no counterpart in the reference, whose
+ * FFT is one fixed radix-2 loop): times every split of a 2^log_n-point transform
+ * into shared-memory passes (radix 2^3 .. 2^10 each) on the current device, with
+ * `batch` transforms per launch, and keeps the fastest for every later transform
+ * of that size on that device. digits_out (3 ints) receives the chosen radix
+ * bits per pass, *ms_out its time per batch. Returns the number of passes, or -1.
+ * Allocates 3 * 2^log_n * batch elements while it runs. */
+int tp_ntt_autotune(int log_n, int batch, int* digits_out, float* ms_out);
+
 /* Replaces poly_commit_prover::commit_private_array(src, log_len)
  * (include/poly_commitment/poly_commit.h:42-96) together with the
  * fri::request_init_commit(log_len, 0) it ends in (src/VPD/fri.cpp:36-123):

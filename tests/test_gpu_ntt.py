@@ -154,3 +154,19 @@ def test_transform_argument_errors(lib):
     assert lib.tp_fft(vp(bad), 8, 16, vp(out)) == -1
     assert b"canonical" in lib.tp_last_error()
     assert lib.tp_rs_commit(vp(a), 5, None, vp(out)) == -1
+
+
+def test_autotuned_splits_give_the_same_transform(lib, orc):
+    """The autotuner only changes how the passes are cut; outputs stay bit-identical."""
+    import ctypes
+    for lg, m in ((14, 1 << 14), (21, 1 << 17)):
+        digits = (ctypes.c_int * 3)()
+        ms = ctypes.c_float()
+        p = lib.tp_ntt_autotune(lg, 1, digits, ctypes.byref(ms))
+        assert p >= 1, lib.tp_last_error()
+        assert sum(digits[:p]) == lg and all(3 <= d <= 10 for d in digits[:p]) and ms.value > 0
+        coef = elements(lg, m)
+        np.testing.assert_array_equal(fft(lib, coef, 1 << lg), orc.fft(coef, 1 << lg))
+        ev = elements(lg + 1, 1 << lg)
+        np.testing.assert_array_equal(ifft(lib, ev, 1 << lg), orc.ifft(ev, 1 << lg))
+    assert lib.tp_ntt_autotune(40, 1, None, None) == -1

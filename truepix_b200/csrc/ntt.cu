@@ -53,16 +53,59 @@ __device__ __forceinline__ fp2 tw_pow(const fp2* __restrict__ lo, const fp2* __r
 
 __device__ __forceinline__ int bitrev(int j, int bits) { return bits ? (int)(__brev((unsigned)j) >> (32 - bits)) : 0; }
 
+// Shared-memory slot of row r, column c: rows of G columns, one element of
+// padding every 8 rows so that the 8-row groups of the first stage group land in
+// distinct banks.
+__device__ __forceinline__ int at(int r, int c, int log_g) { return (r << log_g) + c + (r >> 3); }
+
+// K consecutive radix-2 stages lh0 .. lh0 + K - 1 in registers: a work item is one
+// column and the 2^K rows base + m 2^lh0 (m < 2^K) that these stages combine.
+// The butterfly of stage lh on rows (u, u + 2^lh) uses w_R^(pin R / 2^(lh+1)),
+// pin = u mod 2^lh; FIRST (lh0 = 0) makes every pin a compile-time constant, so
+// the multiplications by w^0 = 1 vanish.
+template <int K, bool FIRST>
+__device__ __forceinline__ void stage_group(fp2* sm, const fp2* tws, int log_r, int log_g, int lh0)
+{
+    const int G = 1 << log_g;
+    const int items = ((1 << log_r) >> K) << log_g;
+    for (int it = threadIdx.x; it < items; it += kThreads) {
+        const int c = it & (G - 1);
+        const int q = it >> log_g;
+        const int lo = FIRST ? 0 : (q & ((1 << lh0) - 1));
+        const int sh = FIRST ? 0 : lh0;
+        const int base = ((q >> sh) << (sh + K)) + lo;
+        fp2 x[1 << K];
+#pragma unroll
+        for (int m = 0; m < (1 << K); ++m) x[m] = sm[at(base + (m << sh), c, log_g)];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const int lh = sh + j;
+#pragma unroll
+            for (int m = 0; m < (1 << K); ++m) {
+                if (m & (1 << j)) continue;
+                const int pin = ((m & ((1 << j) - 1)) << sh) + lo;
+                fp2 y = x[m + (1 << j)];
+                if (pin) y = l2mul(tws[pin << (log_r - 1 - lh)], y);
+                const fp2 a = x[m];
+                x[m] = l2add(a, y);
+                x[m + (1 << j)] = l2sub(a, y);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < (1 << K); ++m) sm[at(base + (m << sh), c, log_g)] = x[m];
+    }
+}
+
 // One pass: a CTA transforms G = 2^log_g columns of R = 2^log_r elements.
 // src and dst may be the same buffer (in-place middle pass): every CTA reads its
 // own columns completely before it writes them, and no other CTA touches them.
-__global__ void __launch_bounds__(kThreads) pass_kernel(const ulonglong2* src, ulonglong2* dst, Pass p,
+__global__ void __launch_bounds__(kThreads, 3) pass_kernel(const ulonglong2* src, ulonglong2* dst, Pass p,
                                                         const fp2* __restrict__ lo,
                                                         const fp2* __restrict__ hi, int h)
 {
     extern __shared__ fp2 sm[];
     const int R = 1 << p.log_r, G = 1 << p.log_g;
-    fp2* tws = sm + (R << p.log_g);
+    fp2* tws = sm + (R << p.log_g) + (R >> 3) + 1;
     const int tid = threadIdx.x;
     src += (long long)blockIdx.y * p.src_batch;
     dst += (long long)blockIdx.y * p.dst_batch;
@@ -107,24 +150,21 @@ __global__ void __launch_bounds__(kThreads) pass_kernel(const ulonglong2* src, u
             v = pos < p.in_len ? ld_fe(src + pos * p.in_step) : f2zero();
         else
             v = ld_fe(src + pos);
-        sm[(bitrev(j, p.log_r) << p.log_g) + c] = v;
+        sm[at(bitrev(j, p.log_r), c, p.log_g)] = v;
     }
     __syncthreads();
 
-    // radix-2 stages, natural-order output
-    for (int lh = 0; lh < p.log_r; ++lh) {
-        const int half = 1 << lh;
-        for (int bi = tid; bi < ((R / 2) << p.log_g); bi += kThreads) {
-            const int c = bi & (G - 1);
-            const int q = bi >> p.log_g;
-            const int pin = q & (half - 1);
-            const int u = ((q >> lh) << (lh + 1)) + pin;
-            const int v = u + half;
-            const fp2 w = tws[pin << (p.log_r - 1 - lh)];
-            const fp2 x = sm[(u << p.log_g) + c];
-            const fp2 y = l2mul(w, sm[(v << p.log_g) + c]);
-            sm[(u << p.log_g) + c] = l2add(x, y);
-            sm[(v << p.log_g) + c] = l2sub(x, y);
+    // radix-2 stages in register groups of three (natural-order output)
+    for (int lh0 = 0; lh0 < p.log_r; lh0 += 3) {
+        const int k = min(3, p.log_r - lh0);
+        if (lh0 == 0) {
+            if (k == 3) stage_group<3, true>(sm, tws, p.log_r, p.log_g, 0);
+            else if (k == 2) stage_group<2, true>(sm, tws, p.log_r, p.log_g, 0);
+            else stage_group<1, true>(sm, tws, p.log_r, p.log_g, 0);
+        } else {
+            if (k == 3) stage_group<3, false>(sm, tws, p.log_r, p.log_g, lh0);
+            else if (k == 2) stage_group<2, false>(sm, tws, p.log_r, p.log_g, lh0);
+            else stage_group<1, false>(sm, tws, p.log_r, p.log_g, lh0);
         }
         __syncthreads();
     }
@@ -133,7 +173,7 @@ __global__ void __launch_bounds__(kThreads) pass_kernel(const ulonglong2* src, u
     for (int idx = tid; idx < (R << p.log_g); idx += kThreads) {
         const int c = idx & (G - 1);
         const int k = idx >> p.log_g;
-        fp2 val = sm[(k << p.log_g) + c];
+        fp2 val = sm[at(k, c, p.log_g)];
         if (!p.last) {
             // w_{R S}^(k s) = w_n^((k s mod R S) n / (R S))
             const unsigned long long e =
@@ -199,12 +239,41 @@ const Tables* tables(int logn, bool inv)
 }
 
 // digit split of a 2^logn transform: at most 10 bits per pass
-std::vector<int> split(int logn)
+// digit split of a 2^logn transform: at most 10 bits per pass, as even as
+// possible -- unless the autotuner stored a measured choice for this device
+std::map<std::pair<int, int>, std::vector<int>> g_plans;   // (device, log n) -> digits
+
+std::vector<int> default_split(int logn)
 {
     const int P = logn <= kMaxLogR ? 1 : (logn + kMaxLogR - 1) / kMaxLogR;
     std::vector<int> d(P, logn / P);
     for (int i = 0; i < logn % P; ++i) d[i]++;
     return d;
+}
+
+std::vector<int> split(int logn)
+{
+    Ctx* c = ctx();
+    if (c) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = g_plans.find(std::make_pair(c->device, logn));
+        if (it != g_plans.end()) return it->second;
+    }
+    return default_split(logn);
+}
+
+// every split of logn into `parts` digits of 3..10 bits
+void splits_of(int logn, int parts, std::vector<int>& cur, std::vector<std::vector<int>>& out)
+{
+    if (parts == 0) {
+        if (logn == 0) out.push_back(cur);
+        return;
+    }
+    for (int b = 3; b <= kMaxLogR && b <= logn; ++b) {
+        cur.push_back(b);
+        splits_of(logn - b, parts - 1, cur, out);
+        cur.pop_back();
+    }
 }
 
 // n-point DFT (direction by tables) of the first-pass input `in`
@@ -216,7 +285,8 @@ bool run(const ulonglong2* in, long long in_len, long long in_step, int logn, bo
     Ctx* c = ctx();
     if (c->device >= 0 && c->device < 64 && !g_attr_set[c->device]) {
         if (cuda_failed(cudaFuncSetAttribute(pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (kTileElems + (1 << kMaxLogR) / 2) * (int)sizeof(fp2)),
+                                             (kTileElems + kTileElems / 8 + 1 + (1 << kMaxLogR) / 2) *
+                                                 (int)sizeof(fp2)),
                         "ntt smem attribute"))
             return false;
         g_attr_set[c->device] = true;
@@ -263,7 +333,8 @@ bool run(const ulonglong2* in, long long in_len, long long in_step, int logn, bo
             }
         }
         const long long ctas = n >> (p.log_r + p.log_g);
-        const size_t smem = sizeof(fp2) * (((size_t)1 << (p.log_r + p.log_g)) + ((size_t)1 << p.log_r) / 2);
+        const size_t smem = sizeof(fp2) * (((size_t)1 << (p.log_r + p.log_g)) + ((size_t)1 << p.log_r) / 8 + 1 +
+                                           ((size_t)1 << p.log_r) / 2);
         pass_kernel<<<dim3((unsigned)ctas, (unsigned)batch), kThreads, smem, s>>>(src, dst, p, tb->lo, tb->hi, tb->h);
         ++g_launches;
         ok = !cuda_failed(cudaGetLastError(), "ntt pass");
@@ -292,6 +363,57 @@ fp2 root_of_unity(int lg)
 }
 
 int passes(long long n) { return (int)split(ilog2(n)).size(); }
+
+bool autotune(int logn, int batch, std::vector<int>& best, float* best_ms)
+{
+    Ctx* c = ctx();
+    if (!c) return false;
+    if (logn < 1 || logn > kMaxLog || batch < 1 || batch > 65535) {
+        set_error(TP_ERR_ARG, "ntt autotune: log n %d or batch %d out of range", logn, batch);
+        return false;
+    }
+    std::vector<std::vector<int>> cands;
+    std::vector<int> cur;
+    const int p0 = (int)default_split(logn).size();
+    for (int parts = p0; parts <= std::min(p0 + 1, 3); ++parts) splits_of(logn, parts, cur, cands);
+    if (cands.empty()) cands.push_back(default_split(logn));
+    const size_t n = (size_t)1 << logn;
+    cudaStream_t s = c->stream;
+    ulonglong2* buf = static_cast<ulonglong2*>(dev_alloc(sizeof(ulonglong2) * n * batch * 3, s));
+    if (!buf) return false;
+    ulonglong2 *in = buf, *out = buf + n * batch, *tmp = buf + 2 * n * batch;
+    bool ok = !cuda_failed(cudaMemsetAsync(in, 0, sizeof(ulonglong2) * n * batch, s), "ntt autotune input");
+    cudaEvent_t e0, e1;
+    ok = ok && !cuda_failed(cudaEventCreate(&e0), "event") && !cuda_failed(cudaEventCreate(&e1), "event");
+    float bt = 1e30f;
+    const auto key = std::make_pair(c->device, logn);
+    for (const auto& d : cands) {
+        if (!ok) break;
+        {
+            std::lock_guard<std::mutex> lk(g_mu);
+            g_plans[key] = d;
+        }
+        for (int r = 0; r < 2 && ok; ++r)
+            ok = run(in, n, 1, logn, false, out, batch, n, n, tmp, 0, s);
+        ok = ok && !cuda_failed(cudaEventRecord(e0, s), "event");
+        for (int r = 0; r < 5 && ok; ++r) ok = run(in, n, 1, logn, false, out, batch, n, n, tmp, 0, s);
+        ok = ok && !cuda_failed(cudaEventRecord(e1, s), "event") && !cuda_failed(cudaEventSynchronize(e1), "event");
+        float ms = 0.f;
+        ok = ok && !cuda_failed(cudaEventElapsedTime(&ms, e0, e1), "event");
+        if (ok && ms / 5 < bt) {
+            bt = ms / 5;
+            best = d;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    dev_free(buf, s);
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (ok && !best.empty()) g_plans[key] = best;
+    else g_plans.erase(key);
+    if (best_ms) *best_ms = bt;
+    return ok;
+}
 
 int last_launches() { return g_launches; }
 

@@ -22,6 +22,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "fp2.cuh"
 
 namespace tp {
@@ -45,6 +47,12 @@ bool inverse(const ulonglong2* in, long long m, long long n, ulonglong2* out, in
 int passes(long long n);
 
 int last_launches();
+
+// Autotuner: times every split of a 2^logn transform into the default number of
+// passes (and one more, up to three) of 3..10 bits on this device, batch
+// transforms at a time, and keeps the fastest for later transforms of that size
+// on this device. Results are exact whatever the split.
+bool autotune(int logn, int batch, std::vector<int>& best, float* best_ms);
 
 }  // namespace ntt
 

@@ -1,6 +1,8 @@
 // C ABI of the Fp2 NTT and the Reed-Solomon commit (include/orion_gpu.h).
 #include <stdint.h>
 
+#include <vector>
+
 #include "ntt.h"
 #include "virgo.h"
 #include "runtime.h"
@@ -99,6 +101,19 @@ int tp_ifft_dev(const void* d_evals, long long coef_len, long long order, void* 
                             batch, in_stride, out_stride, nullptr, reinterpret_cast<cudaStream_t>(stream))
                ? 0
                : -1;
+}
+
+int tp_ntt_autotune(int log_n, int batch, int* digits_out, float* ms_out)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    std::vector<int> best;
+    float ms = 0.f;
+    if (!tp::ntt::autotune(log_n, batch, best, &ms)) return -1;
+    for (size_t i = 0; i < 3; ++i)
+        if (digits_out) digits_out[i] = i < best.size() ? best[i] : 0;
+    if (ms_out) *ms_out = ms;
+    return (int)best.size();
 }
 
 int tp_rs_commit_dev(const void* d_src, int log_len, void* d_l_eval, void* d_tree, void* stream)
