@@ -134,6 +134,17 @@ int tp_ntt_autotune(int log_n, int batch, int* digits_out, float* ms_out);
 int tp_rs_commit(const uint64_t* src, int log_len, uint64_t* l_eval_out, unsigned char* tree_out);
 int tp_rs_commit_dev(const void* d_src, int log_len, void* d_l_eval, void* d_tree, void* stream);
 
+/* Replaces fri::commit_phase_step(r) (src/VPD/fri.cpp:316-420) for the steps
+ * after the first oracle: d_witness holds the current witness in the
+ * interleaved layout of request_init_commit, w[(k << 7) | (j << 1) | h] = slice
+ * j's value at point k + h * M/2 (M = 2^log_m points per slice, 2 <= log_m <=
+ * 26; the reference's rs_codeword[step - 1] with its mapping applied). d_next
+ * (M/2 * 64 elements) receives the folded witness 2^-1((x + y) + w_M^-i r (x - y))
+ * in the same layout (rs_codeword[step]); d_tree (M/2 digests) its Merkle tree
+ * (merkle[step], root at 1). r canonical (real, imag). */
+int tp_fri_commit_step_dev(const void* d_witness, int log_m, uint64_t r_real, uint64_t r_imag, void* d_next,
+                           void* d_tree, void* stream);
+
 /* ---- Virgo (linear GKR) sumcheck (src/linear_gkr/prover.cpp) --------------- */
 
 /* Replaces zk_prover::sumcheck_phase1_update and sumcheck_phase2_update

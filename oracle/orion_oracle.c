@@ -543,3 +543,58 @@ int oracle_virgo_update(const u64* vma, const u64* addv, const u64* ams, long lo
     ret[4] = qc.img; ret[5] = qc.real;
     return 0;
 }
+
+/* ---- FRI commit-phase step (src/VPD/fri.cpp:316-420) ----
+ * Previous witness in the interleaved layout w[(k << 7) | (j << 1) | h] = slice
+ * j's value at k + h M/2 (M = 2^log_m per slice, k < M/2). For i < M/2:
+ * v[i][j] = 2^-1 ((x + y) + w_M^-i r (x - y)), x = w[(i<<7)|(j<<1)], y = the
+ * next one; re-interleaved: next[(i<<7)|(j<<1)|h] = v[i + h M/4][j], i < M/4;
+ * leaf i = chain over j of SHA256(next[..|0] || next[..|1] || h); tree. */
+int oracle_fri_step(const u64* w, int log_m, const u64* r, u64* next, unsigned char* root)
+{
+    if (log_m < 2 || log_m > 26) return -1;
+    const long long M = 1LL << log_m, nxt = M / 2, nl = nxt / 2;
+    const fe* W = (const fe*)w;
+    fe* N = (fe*)next;
+    const fe R = {r[0], r[1]};
+    const fe omega = root_of_unity(log_m);
+    const fe inv_omega = fe_pow(omega, (u64)(M - 1));
+    const fe inv2 = {0, 1ull << 60};
+    fe inv_mu = {0, 1};   /* w^-i, i = 0 */
+    for (long long i = 0; i < nxt; ++i) {
+        const fe t = femul(inv_mu, R);
+        for (int j = 0; j < 64; ++j) {
+            const fe x = W[(i << 7) | (j << 1)], y = W[(i << 7) | (j << 1) | 1];
+            fe d;
+            d.img = canon(x.img + (P61 - y.img));
+            d.real = canon(x.real + (P61 - y.real));
+            const fe v = femul(inv2, feadd(feadd(x, y), femul(t, d)));
+            if (i < nl)
+                N[(i << 7) | (j << 1)] = v;
+            else
+                N[((i - nl) << 7) | (j << 1) | 1] = v;
+        }
+        inv_mu = femul(inv_mu, inv_omega);
+    }
+    unsigned char* tree = (unsigned char*)calloc((size_t)(2 * nl), 32);
+    unsigned char blk[64];
+    for (long long i = 0; i < nl; ++i) {
+        unsigned char h[32];
+        memset(h, 0, 32);
+        for (int j = 0; j < 64; ++j) {
+            put_fe(blk, N[(i << 7) | (j << 1)]);
+            put_fe(blk + 16, N[(i << 7) | (j << 1) | 1]);
+            memcpy(blk + 32, h, 32);
+            oracle_sha256_64(blk, h);
+        }
+        memcpy(tree + 32 * (nl + i), h, 32);
+    }
+    for (long long k = nl - 1; k >= 1; --k) {
+        memcpy(blk, tree + 32 * (2 * k), 32);
+        memcpy(blk + 32, tree + 32 * (2 * k + 1), 32);
+        oracle_sha256_64(blk, tree + 32 * k);
+    }
+    memcpy(root, tree + 32, 32);
+    free(tree);
+    return 0;
+}

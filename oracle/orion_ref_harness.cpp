@@ -15,6 +15,7 @@
 #include "linear_gkr/prime_field.h"
 #include "linear_gkr/prover.h"
 #include "poly_commitment/poly_commit.h"
+#include "VPD/fri.h"
 #include "VPD/linearPC.h"
 #include "truepix/truepix_gkr.h"
 
@@ -162,6 +163,42 @@ void ref_virgo_update(int phase, const uint64_t* vma, const uint64_t* addv, cons
     p->C = &none;
     p->delete_self();
     delete p;
+}
+
+// One FRI commit-phase step (fri::commit_phase_step, src/VPD/fri.cpp:316-420) on
+// a previous witness given in the interleaved layout of request_init_commit /
+// earlier steps: w[(k << 7) | (j << 1) | h] = slice j's value at k + h M / 2,
+// k < M / 2 = 2^(log_m - 1). The reference's globals are set up as after an
+// earlier step (current_step_no 1, L_group = powers of the M-th root of unity).
+// Writes the next interleaved witness (M / 2 * 64 elements) and the root of its
+// tree. Call once per process.
+void ref_fri_step(const uint64_t* witness, int log_m, const uint64_t* r, uint64_t* next, unsigned char* root32)
+{
+    typedef prime_field::field_element F;
+    prime_field::init();
+    const int M = 1 << log_m;
+    poly_commit::slice_count = slice_number;
+    fri::log_current_witness_size_per_slice = log_m;
+    fri::current_step_no = 1;
+    F* prev = new F[(size_t)M * slice_number];
+    memcpy(prev, witness, 16 * (size_t)M * slice_number);
+    int* map = new int[(size_t)M * slice_number];
+    for (int i = 0; i < M / 2; ++i)
+        for (int j = 0; j < slice_number; ++j) {
+            map[(i << log_slice_number) | j] = (i << (log_slice_number + 1)) | (j << 1);
+            map[((i + M / 2) << log_slice_number) | j] = (i << (log_slice_number + 1)) | (j << 1);
+        }
+    fri::cpd.rs_codeword[0] = prev;
+    fri::cpd.rs_codeword_mapping[0] = map;
+    fri::L_group = new F[M];
+    const F w = prime_field::get_root_of_unity(log_m);
+    fri::L_group[0] = F(1ULL);
+    for (int i = 1; i < M; ++i) fri::L_group[i] = fri::L_group[i - 1] * w;
+    F fr;
+    memcpy(&fr, r, 16);
+    __hhash_digest h = fri::commit_phase_step(fr);
+    memcpy(root32, &h, 32);
+    memcpy(next, fri::cpd.rs_codeword[1], 16 * (size_t)(M / 2) * slice_number);
 }
 
 // encoded length of a column of n elements (graphs generated from the default seed)

@@ -16,6 +16,9 @@ tests/golden/orion_golden.npz:
                   (RS_polynomial.cpp:132-206)
   rs_<L>          Merkle root and codeword digest of the rate-2^-5 RS commit
                   of 2^L elements (poly_commit.h:42-96, fri.cpp:36-123)
+  fri*_<log M>    one FRI commit-phase step (fri::commit_phase_step, fri.cpp:316-420)
+                  on a seeded interleaved witness of 2^log M x 64 elements: digest of
+                  the next interleaved witness and its Merkle root
   virgo*_<p>_<n>_<bit>  one Virgo sumcheck update (zk_prover::sumcheck_phase<p>_update,
                   prover.cpp:576-644, 935-1006) of three seeded linear_poly
                   tables: digests of the folded tables and the round polynomial
@@ -60,6 +63,7 @@ FFT_CASES = [(1, 1), (1, 8), (2, 2), (8, 8), (4, 16), (16, 256), (1024, 1024), (
              (1 << 12, 1 << 17), (1 << 16, 1 << 16), (1 << 20, 1 << 20)]
 RS_CASES = [6, 7, 10, 13, 16, 18]
 COMBINE_CASES = [(1 << 14, 21), (128 * 100, 22), (1 << 18, 23)]   # (N, seed)
+FRI_CASES = [(2, 41), (3, 42), (5, 43), (10, 44), (16, 45)]   # (log2 M, seed)
 VIRGO_CASES = [(1, 2, 0, 31), (1, 2, 1, 32), (1, 16, 1, 33), (2, 16, 0, 34), (1, 1 << 10, 1, 35),
                (2, 1 << 14, 1, 36), (1, 1 << 18, 1, 37), (2, 1 << 18, 0, 38)]   # (phase, total_uv, bit, seed)
 
@@ -73,6 +77,7 @@ def _ref():
     lib.ref_encode.argtypes = [V, ctypes.c_longlong, V]
     lib.ref_combine.argtypes = [V, ctypes.c_longlong, V, V, V, V, V]
     lib.ref_virgo_update.argtypes = [ctypes.c_int, V, V, V, ctypes.c_int, V, ctypes.c_int, V, V, V, V]
+    lib.ref_fri_step.argtypes = [V, ctypes.c_int, V, V, V]
     lib.ref_encode_len.argtypes = [ctypes.c_longlong]
     lib.ref_encode_len.restype = ctypes.c_longlong
     return lib
@@ -143,6 +148,15 @@ def _virgo(args):
     return [digest(o) for o in outs], ret
 
 
+def _fri(args):
+    lm, seed = args
+    w, r = elements(seed, (1 << lm) * 64), elements(seed + 1, 1)
+    nxt = np.zeros((1 << lm) * 64, np.uint64)
+    root = ctypes.create_string_buffer(32)
+    _ref().ref_fri_step(V(w.ctypes.data), lm, V(r.ctypes.data), V(nxt.ctypes.data), root)
+    return digest(nxt), root.raw
+
+
 def _rs(lg):
     src = elements(400 + lg, 1 << lg)
     root = ctypes.create_string_buffer(32)
@@ -186,6 +200,10 @@ def main():
             out["virgocase_" + key] = np.array([phase, n, bit, seed])
             out["virgotables_" + key] = np.frombuffer(b"".join(ds), np.uint8)
             out["virgoret_" + key] = ret
+        for (lm, seed), (d, root) in zip(FRI_CASES, pool.map(_fri, FRI_CASES, chunksize=1)):
+            out["fricase_%d" % lm] = np.array([lm, seed])
+            out["frinext_%d" % lm] = np.frombuffer(d, np.uint8)
+            out["friroot_%d" % lm] = np.frombuffer(root, np.uint8)
     np.savez_compressed(os.path.join(HERE, "orion_golden.npz"), **out)
     print("wrote", len(out), "arrays")
 

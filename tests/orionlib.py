@@ -98,6 +98,7 @@ class OrionOracle:
         L.oracle_encode.argtypes = [_V, _LL, _V]
         L.oracle_encode.restype = _LL
         L.oracle_orion_combine.argtypes = [_V, _LL, _V, _V, _V, _V, _V]
+        L.oracle_fri_step.argtypes = [_V, _I, _V, _V, _V]
         L.oracle_virgo_update.argtypes = [_V, _V, _V, _LL, _V, _I, _V, _V, _V, _V]
 
     def sha256_64(self, msg: bytes) -> bytes:
@@ -138,6 +139,13 @@ class OrionOracle:
         rc = self.lib.oracle_orion_combine(_vp(src), n, _vp(r0), _vp(r1), _vp(comb), root, _vp(ans))
         assert rc == 0
         return comb, root.raw, ans
+
+    def fri_step(self, w: np.ndarray, log_m: int, r: np.ndarray):
+        """(next interleaved witness, root) of one FRI commit-phase step."""
+        nxt = np.zeros(w.size // 2, np.uint64)
+        root = ctypes.create_string_buffer(32)
+        assert self.lib.oracle_fri_step(_vp(w), log_m, _vp(r), _vp(nxt), root) == 0
+        return nxt, root.raw
 
     def virgo_update(self, vma, addv, ams, r, bit):
         """(folded tables x3, ret [6 words]) of one Virgo sumcheck round."""

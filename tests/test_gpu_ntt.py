@@ -170,3 +170,39 @@ def test_autotuned_splits_give_the_same_transform(lib, orc):
         ev = elements(lg + 1, 1 << lg)
         np.testing.assert_array_equal(ifft(lib, ev, 1 << lg), orc.ifft(ev, 1 << lg))
     assert lib.tp_ntt_autotune(40, 1, None, None) == -1
+
+
+def _fri_dev(lib, w, lm, r):
+    import torch
+    dev = torch.device("cuda", 0)
+    d_w = torch.from_numpy(w.view(np.int64)).to(dev)
+    d_next = torch.empty(w.size // 2, dtype=torch.int64, device=dev)
+    d_tree = torch.empty(32 * (1 << (lm - 1)), dtype=torch.uint8, device=dev)
+    rc = lib.tp_fri_commit_step_dev(d_w.data_ptr(), lm, int(r[1]), int(r[0]), d_next.data_ptr(),
+                                    d_tree.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, lib.tp_last_error()
+    torch.cuda.synchronize()
+    return d_next.cpu().numpy().view(np.uint64), d_tree.cpu().numpy().reshape(-1, 32)
+
+
+def test_fri_step_matches_reference(lib, og):
+    for k in og.files:
+        if not k.startswith("fricase_"):
+            continue
+        lm, seed = (int(v) for v in og[k])
+        nxt, tree = _fri_dev(lib, elements(seed, (1 << lm) * 64), lm, elements(seed + 1, 1))
+        assert digest(nxt) == og["frinext_%d" % lm].tobytes(), lm
+        assert tree[1].tobytes() == og["friroot_%d" % lm].tobytes(), lm
+
+
+def test_fri_steps_chained_match_oracle(lib, orc):
+    """Consecutive steps down to one leaf, each fed the previous step's output."""
+    w = elements(61, (1 << 12) * 64)
+    for lm in range(12, 1, -1):
+        r = elements(700 + lm, 1)
+        want, wroot = orc.fri_step(w, lm, r)
+        got, tree = _fri_dev(lib, w, lm, r)
+        np.testing.assert_array_equal(got, want)
+        assert tree[1].tobytes() == wroot
+        w = want
+    assert lib.tp_fri_commit_step_dev(None, 1, 0, 0, None, None, None) == -1

@@ -138,3 +138,13 @@ def test_virgo_update(orc, og):
         outs, ret = orc.virgo_update(vma, addv, ams, r, bit)
         assert b"".join(digest(o) for o in outs) == og["virgotables_" + key].tobytes(), key
         np.testing.assert_array_equal(ret, og["virgoret_" + key])
+
+
+def test_fri_step(orc, og):
+    for k in og.files:
+        if not k.startswith("fricase_"):
+            continue
+        lm, seed = (int(v) for v in og[k])
+        nxt, root = orc.fri_step(elements(seed, (1 << lm) * 64), lm, elements(seed + 1, 1))
+        assert digest(nxt) == og["frinext_%d" % lm].tobytes(), lm
+        assert root == og["friroot_%d" % lm].tobytes(), lm

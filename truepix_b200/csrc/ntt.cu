@@ -364,6 +364,16 @@ fp2 root_of_unity(int lg)
 
 int passes(long long n) { return (int)split(ilog2(n)).size(); }
 
+bool power_tables(int logn, bool inverse, const fp2** lo, const fp2** hi, int* h)
+{
+    const Tables* t = tables(logn, inverse);
+    if (!t) return false;
+    *lo = t->lo;
+    *hi = t->hi;
+    *h = t->h;
+    return true;
+}
+
 bool autotune(int logn, int batch, std::vector<int>& best, float* best_ms)
 {
     Ctx* c = ctx();

@@ -43,6 +43,10 @@ bool forward(const ulonglong2* in, long long m, long long n, ulonglong2* out, in
 bool inverse(const ulonglong2* in, long long m, long long n, ulonglong2* out, int batch, long long in_batch,
              long long out_batch, ulonglong2* scratch, cudaStream_t s);
 
+// The device tables of w^t for w = the 2^logn-th root of unity (or its inverse):
+// w^e = lo[e mod 2^h] * hi[e >> h], e < 2^logn. Cached per device.
+bool power_tables(int logn, bool inverse, const fp2** lo, const fp2** hi, int* h);
+
 // number of passes of an n-point transform
 int passes(long long n);
 
@@ -68,6 +72,13 @@ namespace rs {
 // tree holds 2^(log_len-1) digests. Temporary buffers come from the pool.
 constexpr int kMinLog = 6, kMaxLog = 25;
 bool commit(const ulonglong2* src, int log_len, ulonglong2* l_eval, unsigned char* tree, cudaStream_t s);
+
+// One FRI commit-phase step (src/VPD/fri.cpp:316-420) on a witness in the
+// interleaved layout w[(k << 7) | (j << 1) | h] = slice j's value at k + h M/2
+// (M = 2^log_m points per slice): next (M/2 x 64 elements, same layout) gets
+// 2^-1 ((x + y) + w_M^-i r (x - y)) re-interleaved, tree (M/2 digests) the Merkle
+// tree of its leaf chains SHA256(x || y || h) over the 64 slices, root at 1.
+bool fri_step(const ulonglong2* w, int log_m, fp2 r, ulonglong2* next, unsigned char* tree, cudaStream_t s);
 
 }  // namespace rs
 }  // namespace tp

@@ -116,6 +116,22 @@ int tp_ntt_autotune(int log_n, int batch, int* digits_out, float* ms_out)
     return (int)best.size();
 }
 
+int tp_fri_commit_step_dev(const void* d_witness, int log_m, uint64_t r_real, uint64_t r_imag, void* d_next,
+                           void* d_tree, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!d_witness || !d_next || !d_tree) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_fri_commit_step_dev: null buffer");
+        return -1;
+    }
+    return tp::rs::fri_step(static_cast<const ulonglong2*>(d_witness), log_m, tp::mk(r_real, r_imag),
+                            static_cast<ulonglong2*>(d_next), static_cast<unsigned char*>(d_tree),
+                            reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
 int tp_rs_commit_dev(const void* d_src, int log_len, void* d_l_eval, void* d_tree, void* stream)
 {
     tp::clear_error();

@@ -96,6 +96,7 @@ GKR_SIGNATURES = {
                            ctypes.c_longlong, _VP]),
     "tp_ntt_autotune": (_I32, [_I32, _I32, _PI32, ctypes.POINTER(ctypes.c_float)]),
     "tp_rs_commit": (_I32, [_VP, _I32, _VP, _VP]),
+    "tp_fri_commit_step_dev": (_I32, [_VP, _I32, _U64, _U64, _VP, _VP, _VP]),
     "tp_rs_commit_dev": (_I32, [_VP, _I32, _VP, _VP, _VP]),
     "tp_virgo_sumcheck_update_dev": (_I32, [_VP, _VP, _VP, ctypes.c_longlong, _U64, _U64, _I32, _VP, _VP,
                                             _VP, _VP, _VP]),
