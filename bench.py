@@ -424,6 +424,28 @@ def ntt_bench(lib, dev, stream, reps=5):
     return out
 
 
+def replica_seed(rank):
+    """Replicas only: every rank proves its own frames (seeded by its rank), no
+    collective on the data path."""
+    return SEED + 101 * rank
+
+
+def max_over_ranks(ms, world, device):
+    """The step time of the whole job: the slowest rank's device time."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(frames_per_rank, max_ms, world):
+    """Frames of all ranks over the slowest rank's time (frames/s)."""
+    return world * frames_per_rank / (max_ms / 1e3)
+
+
 def ours_arm(args, rank, world, local_rank):
     import ctypes
     import torch
@@ -437,7 +459,7 @@ def ours_arm(args, rank, world, local_rank):
     gt, i0, i1 = circuit()
     B = args.batch
     nb = layout.n_copy_bits
-    rng = np.random.default_rng(SEED + 101 * rank)
+    rng = np.random.default_rng(replica_seed(rank))
     frames, z1, z2, point, chal = make_inputs(rng, layout, B)
     pix = [torch.from_numpy(f).to(dev) for f in frames]
     z2_dev = torch.from_numpy(pack_fp2(z2[:, 0], z2[:, 1])).to(dev)
@@ -524,12 +546,9 @@ def ours_arm(args, rank, world, local_rank):
     ms = evs[0].elapsed_time(evs[-1])
     per_batch = sorted(evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps))
     gkr_ms = sum(evs[i].elapsed_time(mids[i]) for i in range(args.steps))
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = max_over_ranks(ms, world, dev)
     frames_done = args.steps * B
-    value = world * frames_done / (ms / 1e3)
+    value = job_throughput(frames_done, ms, world)
 
     groups = kernel_groups(list(tms[:max(0, got)]), list(ttags[:max(0, got)]), layout, B,
                            cw_len, leaves)
