@@ -294,7 +294,9 @@ def kernel_groups(ms, tags, layout, batch=1, cw_len=0, leaves=0):
     codeword-message element written; leaves = 2 KB read + 32 B written per
     codeword row, 128 compressions per row; tree = 64 B read + 32 B written and 2
     compressions per node; gathers: see ntt/commit notes (one 2 KB row read per
-    edge, L2-resident), their bytes are the rows written."""
+    edge, L2-resident); their algorithmic bytes count every source row read once
+    and every target row written once (2 KB each; the depth-0 C graph reads the
+    frame's byte matrix, 128 B per row)."""
     rows = layout.const_idx + 1 if layout.const_idx >= 0 else layout.copy_size
     pix_bytes = layout.copies * layout.copy_size
     col_len = layout.padded_copies * layout.n_wires // 128
@@ -340,7 +342,36 @@ def kernel_groups(ms, tags, layout, batch=1, cw_len=0, leaves=0):
         frames = g["launches"] / max(1, tree_launches(leaves))
         g["bytes"] = frames * 96 * (leaves - 1)
         g["compressions"] = frames * 2 * (leaves - 1)
+    levels = encoder_levels(col_len)
+    if "gather_kernel" in groups and levels:
+        # every source row read once and every target row written once (2 KB
+        # each) over the C graphs of depth >= 1 and all D graphs
+        per_frame = 2048 * (sum(n + R for n, R, L, RD in levels[1:]) + sum(L + RD for n, R, L, RD in levels))
+        g = groups["gather_kernel"]
+        g["bytes"] = per_frame * g["launches"] / (2 * len(levels) - 1)
+    if "gather_bytes_kernel" in groups and levels:
+        n0, R0 = levels[0][0], levels[0][1]
+        g = groups["gather_bytes_kernel"]
+        g["bytes"] = g["launches"] * (128 * n0 + 2048 * R0)
     return groups
+
+
+def encoder_levels(col_len):
+    """(n, R, L, RD) per depth of the expander encoder of a column of col_len
+    elements (include/linear_code/expanders.h:47-60; the same double arithmetic)."""
+    def cw(n):
+        if n <= 13:
+            return n
+        R = int(0.238 * n)
+        L = cw(R)
+        return n + L + int(n * (1.72 - 1) - L)
+    out, n = [], col_len
+    while n > 13:
+        R = int(0.238 * n)
+        L = cw(R)
+        out.append((n, R, L, int(n * (1.72 - 1) - L)))
+        n = R
+    return out
 
 
 def tree_launches(leaves):
@@ -468,7 +499,7 @@ def ours_arm(args, rank, world, local_rank):
     stream = torch.cuda.Stream(dev)
     lib = native.gkr()
     bprover = BatchFrameProver([layout] * B, gt, i0, i1, device=local_rank, stream=stream)
-    committer = FrameCommitter([layout] * B, device=local_rank, stream=stream)
+    committer = FrameCommitter([layout] * B, device=local_rank, stream=stream, side_streams=args.commit_streams)
     cw_len, leaves = committer.cw_len[0], committer.leaves[0]
     z1s = [z1] * B
     z2s = z2_dev.repeat(B)      # packed [B][nb]
@@ -553,21 +584,24 @@ def ours_arm(args, rank, world, local_rank):
     groups = kernel_groups(list(tms[:max(0, got)]), list(ttags[:max(0, got)]), layout, B,
                            cw_len, leaves)
     peak, peak_kind = peaks()
-    kernels = []
-    for name, g in sorted(groups.items(), key=lambda kv: -kv[1]["ms"]):
-        ach = g["bytes"] / (g["ms"] / 1e3) / 1e9 if g["ms"] > 0 and g["bytes"] else None
-        k = {"kernel": name, "launches": g["launches"], "total_ms": g["ms"],
-             "share_of_step": g["ms"] / ms, "achieved_gbs": ach}
-        if g["compressions"]:
-            k["g_compressions_per_s"] = g["compressions"] / (g["ms"] / 1e3) / 1e9
-        if g["by_copies"]:
-            k["avg_us_by_copies"] = {str(c): round(1e3 * v[1] / v[0], 2)
-                                     for c, v in sorted(g["by_copies"].items())}
-        kernels.append(k)
     traffic = profiled_traffic() or {}
 
-    def roof_of(k):
-        g = groups[k["kernel"]]
+    def summarize(grp, total_ms):
+        out = []
+        for name, g in sorted(grp.items(), key=lambda kv: -kv[1]["ms"]):
+            ach = g["bytes"] / (g["ms"] / 1e3) / 1e9 if g["ms"] > 0 and g["bytes"] else None
+            k = {"kernel": name, "launches": g["launches"], "total_ms": g["ms"],
+                 "share_of_step": g["ms"] / total_ms, "achieved_gbs": ach}
+            if g["compressions"]:
+                k["g_compressions_per_s"] = g["compressions"] / (g["ms"] / 1e3) / 1e9
+            if g["by_copies"]:
+                k["avg_us_by_copies"] = {str(c): round(1e3 * v[1] / v[0], 2)
+                                         for c, v in sorted(g["by_copies"].items())}
+            out.append(k)
+        return out
+
+    def roof_of(k, grp):
+        g = grp[k["kernel"]]
         r = {"kernel": k["kernel"], "bound": "hbm", "achieved": k["achieved_gbs"], "peak": peak,
              "unit": "GB/s",
              "frac": k["achieved_gbs"] / peak if k["achieved_gbs"] else None,
@@ -583,9 +617,33 @@ def ours_arm(args, rank, world, local_rank):
                                            "this GPU (tp_sha256_peak_dev, measured in this run)"}
         return r
 
-    roof = roof_of(kernels[0]) if kernels else None
+    kernels = summarize(groups, ms)
+    roof = roof_of(kernels[0], groups) if kernels else None
     hbm_kernel = next((k for k in kernels if k["kernel"] == "table_round_kernel<fold>"), None)
-    roof_fold = roof_of(hbm_kernel) if hbm_kernel else None
+    roof_fold = roof_of(hbm_kernel, groups) if hbm_kernel else None
+
+    # One more step, outside the timed region, with the commits serialised on the
+    # step's stream: per-kernel durations with no other stream's kernels sharing
+    # the SMs (the timed step spreads commits over side streams, so its
+    # per-kernel durations overlap).
+    kernels_iso = roof_iso = None
+    if rank == 0 and committer.side:
+        side, committer.side = committer.side, []
+        native.check(lib, lib.tp_timer_enable(per_step_pairs), "timer")
+        lib.tp_timer_reset()
+        with torch.cuda.stream(stream):
+            i0e, i1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            i0e.record(stream)
+            run_batch()
+            i1e.record(stream)
+        torch.cuda.synchronize()
+        got_i = lib.tp_timer_read(tms, ttags, npairs)
+        lib.tp_timer_disable()
+        committer.side = side
+        g_iso = kernel_groups(list(tms[:max(0, got_i)]), list(ttags[:max(0, got_i)]), layout, B, cw_len, leaves)
+        kernels_iso = summarize(g_iso, i0e.elapsed_time(i1e))
+        roof_iso = roof_of(kernels_iso[0], g_iso) if kernels_iso else None
+
     folded = sum(g["folded"] for g in groups.values())
 
     res_ok = None
@@ -640,7 +698,15 @@ def ours_arm(args, rank, world, local_rank):
             "latency_ms_per_batch": {"p50": per_batch[len(per_batch) // 2],
                                      "p99": per_batch[min(len(per_batch) - 1,
                                                           int(0.99 * len(per_batch)))]},
-            "roofline": roof, "roofline_fold_kernel": roof_fold, "kernels": kernels,
+            "roofline": roof_iso or roof, "roofline_fold_kernel": roof_fold,
+            "kernels": kernels_iso or kernels,
+            "roofline_timed_region": roof, "kernels_timed_region": kernels,
+            "kernels_note": "the timed steps spread the commits over %d side streams, so their "
+                            "per-kernel durations overlap (kernels_timed_region, "
+                            "roofline_timed_region); roofline and kernels come from one more step "
+                            "with the commits serialised on the step's stream (CUDA events around "
+                            "every launch), whose shares match the serialised ncu launch list"
+                            % len(committer.side),
             "ntt": ntt, "batched_uneven": uneven, "serving": serving, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
             "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
         }
@@ -875,6 +941,8 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-ntt", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--commit-streams", type=int, default=8,
+                    help="streams the step's commits are spread over (0: the step's stream)")
     ap.add_argument("--profile-case", choices=["orion"], help="run a fixed short workload for ncu and exit")
     args = ap.parse_args()
     if args.profile_case:

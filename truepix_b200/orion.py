@@ -20,7 +20,11 @@ class FrameCommitter:
     their device bytes. One codeword (cw_len x 128 elements, row-major) and one
     tree (2 * leaves digests) per frame, allocated once and reused."""
 
-    def __init__(self, layouts, device: int = 0, stream=None):
+    def __init__(self, layouts, device: int = 0, stream=None, side_streams: int = 0):
+        """side_streams > 0: frames are committed round-robin on that many extra
+        streams (joined back into `stream` at the end of commit()), so that one
+        frame's latency-bound phases (the tree levels, the small expander graphs)
+        overlap another frame's SHA-256 leaves."""
         import torch
         self.torch = torch
         self.lib = native.gkr()
@@ -36,6 +40,7 @@ class FrameCommitter:
             self.leaves.append(lv)
             self.rows.append(torch.empty(2 * 128 * cw, dtype=torch.int64, device=self.dev))
             self.trees.append(torch.empty(64 * lv, dtype=torch.uint8, device=self.dev))
+        self.side = [torch.cuda.Stream(self.dev) for _ in range(side_streams)]
         self.launches_last = 0
 
     def _s(self):
@@ -44,14 +49,25 @@ class FrameCommitter:
 
     def commit(self, pixels) -> None:
         """Queue the commits of all frames (pixels: one uint8 device tensor each)."""
-        lib, s = self.lib, self._s()
+        torch, lib, s = self.torch, self.lib, self._s()
         launches = 0
+        main = self.stream if self.stream is not None else torch.cuda.current_stream(self.dev)
+        if self.side:
+            ready = torch.cuda.Event()
+            ready.record(main)
+            for q in self.side:
+                q.wait_event(ready)
         for f, L in enumerate(self.layouts):
+            fs = self.side[f % len(self.side)].cuda_stream if self.side else s
             native.check(lib, lib.tp_orion_commit_pixels_dev(
                 pixels[f].data_ptr(), L.copies, L.padded_copies, L.copy_size, L.n_wires,
-                L.const_idx, L.const_val, self.rows[f].data_ptr(), self.trees[f].data_ptr(), s),
+                L.const_idx, L.const_val, self.rows[f].data_ptr(), self.trees[f].data_ptr(), fs),
                 "orion commit")
             launches += lib.tp_orion_last_launches()
+        for q in self.side:
+            done = torch.cuda.Event()
+            done.record(q)
+            main.wait_event(done)
         self.launches_last = launches
 
     def root(self, f: int) -> bytes:
