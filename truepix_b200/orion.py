@@ -47,8 +47,10 @@ class FrameCommitter:
         return self.stream.cuda_stream if self.stream is not None else \
             self.torch.cuda.current_stream(self.dev).cuda_stream
 
-    def commit(self, pixels) -> None:
-        """Queue the commits of all frames (pixels: one uint8 device tensor each)."""
+    def commit(self, pixels, join: bool = True) -> None:
+        """Queue the commits of all frames (pixels: one uint8 device tensor each).
+        With side streams and join=False the step's stream does not wait for them
+        here (work queued on it next overlaps the commits); call join() later."""
         torch, lib, s = self.torch, self.lib, self._s()
         launches = 0
         main = self.stream if self.stream is not None else torch.cuda.current_stream(self.dev)
@@ -64,11 +66,21 @@ class FrameCommitter:
                 L.const_idx, L.const_val, self.rows[f].data_ptr(), self.trees[f].data_ptr(), fs),
                 "orion commit")
             launches += lib.tp_orion_last_launches()
+        self._pending = []
         for q in self.side:
             done = torch.cuda.Event()
             done.record(q)
-            main.wait_event(done)
+            self._pending.append(done)
+        if join:
+            self.join()
         self.launches_last = launches
+
+    def join(self) -> None:
+        """Make the step's stream wait for the commits queued by commit(join=False)."""
+        main = self.stream if self.stream is not None else self.torch.cuda.current_stream(self.dev)
+        for done in getattr(self, "_pending", []):
+            main.wait_event(done)
+        self._pending = []
 
     def root(self, f: int) -> bytes:
         return self.trees[f][32:64].cpu().numpy().tobytes()

@@ -7,8 +7,8 @@ frames in their early sumcheck rounds, whatever round each is in, reads the
 claims back (the host transcript needs them), and folds each frame by its own
 challenge. A frame whose early rounds are over is finished alone
 (tp_batch_finish_frame), its input MLE evaluated from its bytes, and its Orion
-commitment queued on a second stream, so commits overlap the rounds of the
-frames still in flight; its slot is free for the next request at once. Requests
+commitment queued on one of several commit streams, so commits overlap each
+other and the rounds of the frames still in flight; its slot is free for the next request at once. Requests
 are admitted while a slot is free and the frame's HBM footprint fits the budget.
 
 The frame layout and the per-round work are those of truepix_b200.frame and
@@ -130,13 +130,16 @@ class ProofServer:
     later keeps the codeword instead (truepix_b200.orion.FrameCommitter)."""
 
     def __init__(self, slots: int = 64, hbm_budget: float = 40e9, device: int = 0, max_height: int = 2160,
-                 max_width: int = 3840, commit_buffers: int = 4):
+                 max_width: int = 3840, commit_buffers: int = 8):
         import torch
         self.torch = torch
         self.lib = native.gkr()
         self.dev = torch.device("cuda", device)
         self.stream = torch.cuda.Stream(self.dev)
-        self.commit_stream = torch.cuda.Stream(self.dev)
+        # commits go round-robin over a few streams so that one frame's
+        # latency-bound commit phases overlap another's SHA-256 leaves
+        self.commit_streams = [torch.cuda.Stream(self.dev) for _ in range(max(1, commit_buffers))]
+        self.commit_next = 0
         self.slots = slots
         self.budget = hbm_budget
         self.batch = self.lib.tp_batch_create(slots, self.stream.cuda_stream)
@@ -243,15 +246,17 @@ class ProofServer:
         while not self.commit_free:                 # back-pressure: wait for the oldest commit
             self._collect(block_first=True)
         job.commit_buf = rows, tree = self.commit_free.pop()
+        cs = self.commit_streams[self.commit_next]
+        self.commit_next = (self.commit_next + 1) % len(self.commit_streams)
         ev = torch.cuda.Event()
         ev.record(self.stream)
-        self.commit_stream.wait_event(ev)
+        cs.wait_event(ev)
         native.check(lib, lib.tp_orion_commit_pixels_dev(
             job.pix.data_ptr(), L.copies, L.padded_copies, L.copy_size, L.n_wires, L.const_idx,
-            L.const_val, rows.data_ptr(), tree.data_ptr(), self.commit_stream.cuda_stream), "commit")
+            L.const_val, rows.data_ptr(), tree.data_ptr(), cs.cuda_stream), "commit")
         self.launches += lib.tp_orion_last_launches() + 3
         job.done_event = torch.cuda.Event()
-        job.done_event.record(self.commit_stream)
+        job.done_event.record(cs)
         del self.active[job.slot]
         self.committing.append(job)
 
