@@ -161,6 +161,33 @@ def _cpu_worker(args):
     return time.perf_counter() - t0, kind if kind == ckind else kind + "+" + ckind
 
 
+def _cpu_zk_commit(_):
+    """The zero-knowledge commit phase (Orion_zk commit_pair of the masked
+    polynomial and the mask) of one 1080p frame on one core: (seconds, kind). The
+    reference's own sources (oracle/_ref/liborion_zk_ref.so) when built, else the
+    oracle's restatement."""
+    import ctypes
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from orionlib import ORION_ZK_REF_LIB, OrionOracle, frame_bytes
+    from truepix_b200.frame import FrameLayout
+    L = FrameLayout.for_frame(H, Wd)
+    pix = frame_bytes(SEED, L.copies * L.copy_size)
+    if not os.path.exists(ORION_ZK_REF_LIB):
+        orc = OrionOracle()
+        t0 = time.perf_counter()
+        orc.zk_commit(pix, L.copies, L.copy_size, L.n_wires, L.const_idx, L.const_val, L.padded_copies, 12345)
+        return time.perf_counter() - t0, "port"
+    lib = ctypes.CDLL(ORION_ZK_REF_LIB)
+    V = ctypes.c_void_p
+    lib.ref_zk_commit.argtypes = [V, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
+                                  V, V, V, V, V]
+    coefs = frame_elements(pix, L)
+    bufs = [ctypes.create_string_buffer(80) for _ in range(4)]
+    t0 = time.perf_counter()
+    lib.ref_zk_commit(V(coefs.ctypes.data), L.copies, L.copy_size, L.const_idx, L.const_val, 12345, *bufs, None)
+    return time.perf_counter() - t0, "reference"
+
+
 def reference_arm(args, rank, world):
     """The reference CPU implementation on all host cores (rank 0 only). One step
     = one frame per worker process; at most 6 timed frames per worker (a frame
@@ -661,9 +688,11 @@ def ours_arm(args, rank, world, local_rank):
         c, w, b, m = bprover.results(B - 1)
         res_ok = bool(c.any() and w.any() and m != (0, 0) and any(committer.root(B - 1)))
 
-    ntt = e2e = e2e_ref = cpu = uneven = serving = None
+    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = None
     if rank == 0 and not args.skip_ntt:
         ntt = ntt_bench(lib, dev, stream)
+    if rank == 0 and not args.skip_zk:
+        zk = zk_step(args, bprover, pix, z1s, z2s, pts, chal_b, layout, stream, local_rank)
     if rank == 0 and not args.skip_e2e:
         e2e = e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream, dev)
         e2e_ref = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
@@ -718,10 +747,58 @@ def ours_arm(args, rank, world, local_rank):
                             "with the commits serialised on the step's stream (CUDA events around "
                             "every launch), whose shares match the serialised ncu launch list"
                             % len(committer.side),
-            "ntt": ntt, "batched_uneven": uneven, "serving": serving, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
+            "ntt": ntt, "zk": zk, "batched_uneven": uneven, "serving": serving, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
             "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
         }
         print(json.dumps(line), flush=True)
+
+
+def zk_step(args, bprover, pix, z1s, z2s, pts, chal_b, layout, stream, local_rank):
+    """The step with TruePix's default zero-knowledge commit: the batched GKR
+    input layer plus, per frame, the commit pair of the masked polynomial and the
+    mask (Orion_zk commit_pair, two encodes and two trees), the pairs on side
+    streams under the rounds as in the timed steps. Device time, CUDA events."""
+    import torch
+    from truepix_b200.orion import FrameCommitter
+    B = bprover.B
+    zc = FrameCommitter([layout] * B, device=local_rank, stream=stream, side_streams=args.commit_streams, zk=True)
+    seeds = [0x5EED0000 + f for f in range(B)]
+
+    def one():
+        zc.commit(pix, join=False, mask_seeds=seeds)
+        bprover.prove(pix, z1s, z2s, pts, chal_b)
+        zc.join()
+
+    steps = max(2, min(args.steps, 5))
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            one()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            one()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    ok = any(zc.root(B - 1)) and any(zc.mask_root(B - 1)) and zc.root(B - 1) != zc.mask_root(B - 1)
+    out = {"frames_per_s": B / (ms / 1e3), "ms_per_step": ms, "steps": steps, "frames_per_step": B,
+           "commit_pairs_per_step": B, "roots_nonzero": bool(ok),
+           "what": "batched GKR input layer + ZK commit pair per frame (masked polynomial and mask, "
+                   "tp_orion_commit_zk_pixels_dev) from resident bytes, pairs on %d side streams"
+                   % len(zc.side)}
+    del zc
+    torch.cuda.empty_cache()
+    if not args.skip_cpu:
+        try:
+            import multiprocessing as mp
+            with mp.get_context("spawn").Pool(1, maxtasksperchild=1) as pool:
+                secs, kind = pool.apply(_cpu_zk_commit, (0,))
+            out["cpu_zk_commit"] = {"seconds_per_frame": secs, "cores": 1, "kind": kind,
+                                    "sample": "one 1080p frame: Orion_zk commit_pair (masked polynomial "
+                                              "and mask from a seed), one process"}
+        except OSError as e:
+            out["cpu_zk_commit"] = {"unavailable": str(e)}
+    return out
 
 
 def e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream, dev):
@@ -953,6 +1030,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-ntt", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--skip-zk", action="store_true")
     ap.add_argument("--commit-streams", type=int, default=8,
                     help="streams the step's commits are spread over (0: the step's stream)")
     ap.add_argument("--profile-case", choices=["orion"], help="run a fixed short workload for ncu and exit")

@@ -58,6 +58,36 @@ int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_
                                int n_wires, int const_idx, uint64_t const_val, void* d_rows,
                                void* d_tree, void* stream);
 
+/* Zero-knowledge commits (TruePix-main/Orion/Orion_zk). Replaces
+ * commit_pair(masked, mask, N) of src/VPD/linearPC.cpp:253-460: two Orion
+ * commits, each byte-identical to commit() of its polynomial, trees returned
+ * (tree_masked, tree_mask: 2 * tp_orion_tree_leaves(N) digests each; roots at
+ * digest 1). Host buffers, N elements {img, real} each, canonical. */
+int tp_orion_commit_pair(const uint64_t* masked, const uint64_t* mask, long long N, unsigned char* tree_masked,
+                         unsigned char* tree_mask);
+
+/* The ZK commit of a frame from its bytes and the mask seed: the masked
+ * polynomial (frame + mask) and the mask, as alloc_masked_from_seed /
+ * alloc_mask_from_seed build them (include/truepix/truepix_gkr.h:286-384: the
+ * mask is zero except at the private wires, wire < copy_size and copy <
+ * n_copies, where the k-th one in flat order holds the (k+1)-th splitmix64
+ * output of the seed mod 2^61 - 1), committed into two row-major codewords
+ * and two trees as by tp_orion_commit_pixels_dev. Neither polynomial is
+ * materialised. Replaces the commit phase of
+ * examples/multivariate_PC_test_commit.cpp:280-340 (linearPC_multi_commit_zk). */
+int tp_orion_commit_zk_pixels_dev(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size,
+                                  int n_wires, int const_idx, uint64_t const_val, uint64_t mask_seed,
+                                  void* d_rows_masked, void* d_tree_masked, void* d_rows_mask, void* d_tree_mask,
+                                  void* stream);
+
+/* The polynomial a frame stands for, as N = n_copies_padded * n_wires base-field
+ * values (u64, imaginary parts are zero): mask_mode 0 the frame
+ * (truepix::load_coefs), 1 the masked polynomial, 2 the mask (as above). For
+ * the MLE evaluations of the ZK opening (tp_mle_eval_base_dev on d_out). */
+int tp_orion_pixel_vector_dev(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size, int n_wires,
+                              int const_idx, uint64_t const_val, uint64_t mask_seed, int mask_mode, void* d_out,
+                              void* stream);
+
 /* Prover-side passes of tensor_product_protocol (src/VPD/linearPC.cpp:480-531,
  * 569-571) over the ROW-major codeword d_rows that a commit above left on the
  * device. d_r0: 128 elements (the column weights r0). d_combined: cw_len

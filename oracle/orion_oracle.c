@@ -598,3 +598,44 @@ int oracle_fri_step(const u64* w, int log_m, const u64* r, u64* next, unsigned c
     free(tree);
     return 0;
 }
+
+/*
+ * The polynomial of a frame in TruePix's layout, optionally masked
+ * (TruePix-main/Orion/Orion_zk/include/truepix/truepix_gkr.h: load_coefs
+ * :157-206, mask_hides_index / fill_mask :333-362, alloc_masked_from_seed
+ * :374-384). out[f], f < padded * W, real parts only (the imaginary parts are 0):
+ *   mode 0: pixel[copy * cs + wire] for wire < cs, const_val at const_idx
+ *           (copy < copies), 0 elsewhere;
+ *   mode 1: mode 0 + mask; mode 2: the mask.
+ * The mask walks the indices in order with one splitmix64 state (seeded with
+ * `seed`) and draws the next output, reduced mod p, at each private wire
+ * (wire < cs, copy < copies); it is 0 elsewhere.
+ */
+static u64 splitmix64_next(u64* state)
+{
+    *state += 0x9E3779B97F4A7C15ULL;
+    u64 z = *state;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+int oracle_frame_vector(const unsigned char* pix, int copies, int padded, int cs, int W, int const_idx,
+                        u64 const_val, u64 seed, int mode, u64* out)
+{
+    if (mode < 0 || mode > 2 || copies > padded || cs > W) return -1;
+    u64 state = seed;
+    const long long n = (long long)padded * W;
+    for (long long f = 0; f < n; ++f) {
+        const long long copy = f / W;
+        const int wire = (int)(f % W);
+        u64 v = 0;
+        if (copy < copies && mode != 2) {
+            if (wire < cs) v = pix[copy * cs + wire];
+            else if (wire == const_idx) v = const_val;
+        }
+        if (mode != 0 && copy < copies && wire < cs) v = fadd(v, splitmix64_next(&state) % P61);
+        out[f] = v;
+    }
+    return 0;
+}

@@ -26,11 +26,21 @@ tests/golden/orion_golden.npz:
                   569-571) run with the reference's primitives on its retained
                   codeword: combined codeword digest, its Merkle root, answer
 
+and, from the zero-knowledge tree (TruePix-main/Orion/Orion_zk, built into
+oracle/_ref/liborion_zk_ref.so with oracle/orion_zk_ref_harness.cpp), in
+tests/golden/orion_zk_golden.npz:
+
+  zk*_<case>      the commit phase of linearPC_multi_commit_zk on a seeded frame
+                  (examples/multivariate_PC_test_commit.cpp:280-340): masked and
+                  mask Merkle roots of commit_pair (linearPC.cpp:253-460) and the
+                  digest of the mask polynomial (truepix_gkr.h:286-384)
+
 Every reference call runs in a fresh spawned process: the reference keeps
 global scratch state sized by its first call.
 
 Run here (needs the reference checkout and `make -C oracle ref`):
-    python tests/golden/gen_orion_golden.py
+    python tests/golden/gen_orion_golden.py          # both files
+    python tests/golden/gen_orion_golden.py zk       # the ZK file only
 """
 from __future__ import annotations
 
@@ -43,7 +53,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
-from orionlib import (ORION_REF_LIB, digest, elements, frame_bytes, frame_elements,  # noqa: E402
+from orionlib import (ORION_REF_LIB, ORION_ZK_REF_LIB, digest, elements, frame_bytes, frame_elements,  # noqa: E402
                       virgo_inputs)
 
 V = ctypes.c_void_p
@@ -66,6 +76,14 @@ COMBINE_CASES = [(1 << 14, 21), (128 * 100, 22), (1 << 18, 23)]   # (N, seed)
 FRI_CASES = [(2, 41), (3, 42), (5, 43), (10, 44), (16, 45)]   # (log2 M, seed)
 VIRGO_CASES = [(1, 2, 0, 31), (1, 2, 1, 32), (1, 16, 1, 33), (2, 16, 0, 34), (1, 1 << 10, 1, 35),
                (2, 1 << 14, 1, 36), (1, 1 << 18, 1, 37), (2, 1 << 18, 0, 38)]   # (phase, total_uv, bit, seed)
+
+# (name, copies, copy_size, const_idx, const_val, padded copies, pixel seed, mask seed)
+ZK_CASES = [
+    ("gray40", 40, 384, 384, 128, 64, 3, 0x0123456789ABCDEF), ("crop33", 33, 385, -1, 0, 64, 4, 99),
+    ("inv7", 7, 384, 384, 255, 8, 5, 1), ("one", 1, 384, 384, 128, 1, 6, 0),
+    ("all512", 16, 512, -1, 0, 16, 7, 0xFFFFFFFFFFFFFFFF), ("gray1000", 1000, 384, 384, 128, 1024, 8, 42),
+    ("zk1080", 16200, 384, 384, 128, 16384, 12, 0x5EED5EED5EED5EED),
+]
 
 
 def _ref():
@@ -165,6 +183,35 @@ def _rs(lg):
     return root.raw, digest(cw)
 
 
+def _zk(case):
+    _, copies, cs, ci, cv, padded, pseed, mseed = case
+    lib = ctypes.CDLL(ORION_ZK_REF_LIB)
+    lib.ref_zk_commit.argtypes = [V, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
+                                  V, V, V, V, V]
+    coefs = frame_elements(frame_bytes(pseed, copies * cs), copies, cs, 512, ci, cv, padded)
+    ra, rb = ctypes.create_string_buffer(32), ctypes.create_string_buffer(32)
+    ha, hb = ctypes.create_string_buffer(80), ctypes.create_string_buffer(80)
+    mask = np.zeros(2 * padded * 512, np.uint64)
+    lib.ref_zk_commit(V(coefs.ctypes.data), copies, cs, ci, cv, mseed, ra, rb, ha, hb, V(mask.ctypes.data))
+    return ra.raw, rb.raw, ha.value, digest(mask)
+
+
+def main_zk():
+    ctx = mp.get_context("spawn")
+    out = {}
+    with ctx.Pool(8, maxtasksperchild=1) as pool:
+        for case, (ra, rb, hx, md) in zip(ZK_CASES, pool.map(_zk, ZK_CASES, chunksize=1)):
+            name = case[0]
+            out["zkcase_" + name] = np.array(case[1:7], np.int64)
+            out["zkseed_" + name] = np.array([case[7]], np.uint64)
+            out["zkmasked_" + name] = np.frombuffer(ra, np.uint8)
+            out["zkmask_" + name] = np.frombuffer(rb, np.uint8)
+            out["zkmaskedhex_" + name] = np.frombuffer(hx, np.uint8)
+            out["zkmaskdigest_" + name] = np.frombuffer(md, np.uint8)
+    np.savez_compressed(os.path.join(HERE, "orion_zk_golden.npz"), **out)
+    print("wrote", len(out), "arrays")
+
+
 def main():
     ctx = mp.get_context("spawn")
     out = {}
@@ -209,4 +256,6 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] != ["zk"]:
+        main()
+    main_zk()

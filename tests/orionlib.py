@@ -20,6 +20,7 @@ P61 = (1 << 61) - 1
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORION_ORACLE_LIB = os.path.join(ROOT, "oracle", "liborion_oracle.so")
 ORION_REF_LIB = os.path.join(ROOT, "oracle", "_ref", "liborion_ref.so")
+ORION_ZK_REF_LIB = os.path.join(ROOT, "oracle", "_ref", "liborion_zk_ref.so")
 
 _V = ctypes.c_void_p
 _LL = ctypes.c_longlong
@@ -100,6 +101,7 @@ class OrionOracle:
         L.oracle_orion_combine.argtypes = [_V, _LL, _V, _V, _V, _V, _V]
         L.oracle_fri_step.argtypes = [_V, _I, _V, _V, _V]
         L.oracle_virgo_update.argtypes = [_V, _V, _V, _LL, _V, _I, _V, _V, _V, _V]
+        L.oracle_frame_vector.argtypes = [_V, _I, _I, _I, _I, _I, ctypes.c_uint64, ctypes.c_uint64, _I, _V]
 
     def sha256_64(self, msg: bytes) -> bytes:
         assert len(msg) == 64
@@ -129,6 +131,28 @@ class OrionOracle:
         if rc != 0:
             raise ValueError("oracle_orion_commit: %d" % rc)
         return (root.raw, lv.reshape(-1, 32)) if leaves else root.raw
+
+    def frame_vector(self, pix: np.ndarray, copies: int, cs: int, W: int, const_idx: int, const_val: int,
+                     padded: int, seed: int = 0, mode: int = 0) -> np.ndarray:
+        """The frame's polynomial as base-field values (mode 0 plain, 1 masked, 2 mask)."""
+        out = np.zeros(padded * W, np.uint64)
+        pix = np.ascontiguousarray(pix, np.uint8)
+        rc = self.lib.oracle_frame_vector(_vp(pix), copies, padded, cs, W, const_idx, const_val, seed, mode,
+                                          _vp(out))
+        if rc != 0:
+            raise ValueError("oracle_frame_vector: %d" % rc)
+        return out
+
+    def zk_commit(self, pix: np.ndarray, copies: int, cs: int, W: int, const_idx: int, const_val: int,
+                  padded: int, seed: int):
+        """(masked root, mask root) of the ZK commit pair of a frame."""
+        roots = []
+        for mode in (1, 2):
+            v = self.frame_vector(pix, copies, cs, W, const_idx, const_val, padded, seed, mode)
+            src = np.zeros(2 * v.size, np.uint64)
+            src[1::2] = v
+            roots.append(self.commit(src))
+        return tuple(roots)
 
     def combine(self, src: np.ndarray, r0: np.ndarray, r1: np.ndarray):
         """(combined codeword, root of its tree, answer) of the opening passes."""

@@ -148,3 +148,44 @@ def test_fri_step(orc, og):
         nxt, root = orc.fri_step(elements(seed, (1 << lm) * 64), lm, elements(seed + 1, 1))
         assert digest(nxt) == og["frinext_%d" % lm].tobytes(), lm
         assert root == og["friroot_%d" % lm].tobytes(), lm
+
+
+@pytest.fixture(scope="module")
+def zg():
+    return np.load(os.path.join(ROOT, "tests", "golden", "orion_zk_golden.npz"))
+
+
+def zk_cases(zg, largest=True):
+    for k in sorted(zg.files):
+        if k.startswith("zkcase_"):
+            name = k[len("zkcase_"):]
+            copies, cs, ci, cv, padded, pseed = (int(x) for x in zg[k])
+            if not largest and copies > 4096:
+                continue
+            yield name, (copies, cs, ci, cv, padded, pseed, int(zg["zkseed_" + name][0]))
+
+
+def test_zk_commit_pair_and_mask(orc, zg):
+    """The ZK commit phase (Orion_zk commit_pair of the masked polynomial and the
+    mask drawn from the seed) against the reference's roots and mask."""
+    from orionlib import frame_bytes
+    for name, (copies, cs, ci, cv, padded, pseed, mseed) in zk_cases(zg):
+        pix = frame_bytes(pseed, copies * cs)
+        mask = orc.frame_vector(pix, copies, cs, 512, ci, cv, padded, mseed, 2)
+        words = np.zeros(2 * mask.size, np.uint64)
+        words[1::2] = mask
+        assert digest(words) == zg["zkmaskdigest_" + name].tobytes(), name
+        plain = orc.frame_vector(pix, copies, cs, 512, ci, cv, padded, mseed, 0)
+        masked = orc.frame_vector(pix, copies, cs, 512, ci, cv, padded, mseed, 1)
+        assert np.array_equal(masked, (plain + mask) % np.uint64(P61)), name
+        ra, rb = orc.zk_commit(pix, copies, cs, 512, ci, cv, padded, mseed)
+        assert ra == zg["zkmasked_" + name].tobytes(), name
+        assert rb == zg["zkmask_" + name].tobytes(), name
+
+
+def test_zk_mask_only_hides_private_wires(orc):
+    from orionlib import frame_bytes
+    pix = frame_bytes(1, 5 * 384)
+    m = orc.frame_vector(pix, 5, 384, 512, 384, 128, 8, 77, 2).reshape(8, 512)
+    assert not m[:, 384:].any() and not m[5:].any()
+    assert m[:5, :384].all()       # a zero draw has probability ~2^-50 here

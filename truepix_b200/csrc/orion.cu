@@ -162,9 +162,42 @@ __global__ void __launch_bounds__(256) transpose_kernel(const ulonglong2* __rest
     }
 }
 
+// splitmix64 (the reference's truepix::splitmix64) output number k + 1 from the
+// state `seed`: the state after k + 1 increments is seed + (k + 1) * golden, so
+// every private wire's mask is computed independently of the others.
+__device__ __forceinline__ uint64_t zk_mask(uint64_t seed, long long k)
+{
+    uint64_t z = seed + (uint64_t)(k + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return canon61(z);   // z mod 2^61 - 1
+}
+
+// element f = copy * W + wire of the polynomial a PixelInput stands for
+__device__ __forceinline__ uint64_t pixel_value(const PixelInput& px, long long f, int w_shift)
+{
+    const long long copy = f >> w_shift;
+    const int wire = (int)(f & ((1LL << w_shift) - 1));
+    if (copy >= px.copies) return 0;
+    const bool priv = wire < px.cs;
+    uint64_t v = 0;
+    if (px.mask_mode != kMaskOnly) {
+        if (priv)
+            v = px.pix[copy * px.cs + wire];
+        else if (wire == px.const_idx)
+            v = px.const_val;
+    }
+    if (px.mask_mode != kMaskNone && priv) {
+        const uint64_t m = zk_mask(px.mask_seed, copy * px.cs + wire);
+        v = canon61(v + m);
+    }
+    return v;
+}
+
 // rows[r][c] = input element c * col_len + r of a frame (PixelInput layout)
 // (and, when `bytes` is set, the same values as a row-major byte matrix
-// bytes[r][c]: every value of a frame is < 256 when its constant is)
+// bytes[r][c]: every value of an unmasked frame is < 256 when its constant is)
 __global__ void __launch_bounds__(256) pixel_rows_kernel(PixelInput px, long long col_len, int w_shift,
                                                          ulonglong2* __restrict__ rows,
                                                          unsigned char* __restrict__ bytes)
@@ -172,18 +205,16 @@ __global__ void __launch_bounds__(256) pixel_rows_kernel(PixelInput px, long lon
     const long long i = (long long)blockIdx.x * 256 + threadIdx.x;
     if (i >= col_len * kColumns) return;
     const long long r = i >> 7, c = i & 127;
-    const long long f = c * col_len + r;
-    const long long copy = f >> w_shift;
-    const int wire = (int)(f & ((1LL << w_shift) - 1));
-    uint64_t v = 0;
-    if (copy < px.copies) {
-        if (wire < px.cs)
-            v = px.pix[copy * px.cs + wire];
-        else if (wire == px.const_idx)
-            v = px.const_val;
-    }
+    const uint64_t v = pixel_value(px, c * col_len + r, w_shift);
     rows[i] = make_ulonglong2(0, v);
     if (bytes) bytes[i] = (unsigned char)v;
+}
+
+__global__ void __launch_bounds__(256) pixel_vector_kernel(PixelInput px, long long n, int w_shift,
+                                                           uint64_t* __restrict__ out)
+{
+    const long long f = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (f < n) out[f] = pixel_value(px, f, w_shift);
 }
 
 // The depth-0 C multiplication of a frame, from its byte matrix: every source
@@ -587,6 +618,7 @@ const Encoder* encoder(long long col_len)
 }
 
 int last_launches() { return g_launches; }
+void add_launches(int n) { g_launches += n; }
 
 bool sha_peak(int blocks, int iters, uint32_t* out, cudaStream_t s)
 {
@@ -600,6 +632,14 @@ bool rows_to_columns(const ulonglong2* rows, long long cw_len, ulonglong2* cols,
 {
     transpose_kernel<<<transpose_grid(cw_len, kColumns), 256, 0, s>>>(rows, cols, cw_len, kColumns);
     return launch_ok("orion rows_to_columns");
+}
+
+bool pixel_vector(const PixelInput& px, long long n, uint64_t* out, cudaStream_t s)
+{
+    int w_shift = 0;
+    while ((1 << w_shift) < px.W) ++w_shift;
+    pixel_vector_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(px, n, w_shift, out);
+    return launch_ok("orion pixel vector");
 }
 
 bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulonglong2* rows,
@@ -622,7 +662,8 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
         while ((1 << w_shift) < px->W) ++w_shift;
         const long long n = col_len * kColumns;
         // byte path of the depth-0 C multiplication: values < 2^8, in-degree < 2^16
-        if (px->const_val < 256 && !enc.levels.empty() && enc.max_c0_in_degree < (1u << 16)) {
+        if (px->mask_mode == kMaskNone && px->const_val < 256 && !enc.levels.empty() &&
+            enc.max_c0_in_degree < (1u << 16)) {
             bytes = static_cast<unsigned char*>(dev_alloc((size_t)n, s));
             if (!bytes) return false;
         }

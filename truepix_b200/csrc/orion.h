@@ -66,11 +66,25 @@ void zero_block_hash(unsigned char out[32]);
 // Frame bytes as the commit's input vector (TruePix layout, truepix_gkr.h:107-206):
 // element f = copy * W + wire is pixel[copy * cs + wire] for wire < cs and copy < copies,
 // const_val at wire == const_idx (copy < copies), zero elsewhere (real part; img 0).
+//
+// ZK commits (TruePix-main/Orion/Orion_zk/include/truepix/truepix_gkr.h:286-384)
+// replace that vector by the masked polynomial (mask_mode kMaskMasked: element +
+// mask) or the mask alone (kMaskOnly). The mask is zero except at the private
+// wires (wire < cs, copy < copies), where the k-th private wire in flat order,
+// k = copy * cs + wire, holds splitmix64 output number k + 1 of the state
+// mask_seed, reduced mod 2^61 - 1 (real part; img 0).
+enum MaskMode { kMaskNone = 0, kMaskMasked = 1, kMaskOnly = 2 };
+
 struct PixelInput {
     const unsigned char* pix;
     int copies, cs, W, const_idx;
     uint64_t const_val;
+    uint64_t mask_seed = 0;
+    int mask_mode = kMaskNone;
 };
+
+// the polynomial a PixelInput stands for, as base-field values out[f], f < copies_padded * W
+bool pixel_vector(const PixelInput& px, long long n, uint64_t* out, cudaStream_t s);
 
 // Full commit into caller buffers: rows (cw_len x 128 elements) and tree
 // (2 * tree_leaves digests of 32 bytes, heap order, root at index 1).
@@ -106,6 +120,8 @@ bool sha_peak(int blocks, int iters, uint32_t* out, cudaStream_t s);
 
 // launches issued by commit() / build_tree() on this thread since the last commit()
 int last_launches();
+// adds n to that count (entry points that run several commits)
+void add_launches(int n);
 
 }  // namespace orion
 }  // namespace tp

@@ -31,6 +31,74 @@ struct DevBuf {
     }
 };
 
+// checks a frame layout (the TruePix layout of truepix_gkr.h:107-206) and fills px and N
+bool pixel_layout(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size, int n_wires,
+                  int const_idx, uint64_t const_val, const char* who, tp::orion::PixelInput& px, long long& N)
+{
+    if (!d_pixels || n_copies < 0 || n_copies > n_copies_padded || copy_size <= 0 || copy_size > n_wires ||
+        n_wires <= 0 || (n_wires & (n_wires - 1)) || n_copies_padded <= 0 || const_idx >= n_wires ||
+        (const_idx >= 0 && const_idx < copy_size) || const_val >= tp::P61) {
+        tp::set_error(tp::TP_ERR_ARG, "%s: layout copies %d/%d, copy_size %d, wires %d, const %d", who, n_copies,
+                      n_copies_padded, copy_size, n_wires, const_idx);
+        return false;
+    }
+    N = (long long)n_copies_padded * n_wires;
+    if (!check_n(N, who)) return false;
+    px.pix = static_cast<const unsigned char*>(d_pixels);
+    px.copies = n_copies;
+    px.cs = copy_size;
+    px.W = n_wires;
+    px.const_idx = const_idx;
+    px.const_val = const_val;
+    return true;
+}
+
+// a host-buffer commit of N elements {img, real}: the tree to tree_out, the
+// column-major codeword to codeword_out when it is set
+int commit_host(const uint64_t* src, long long N, unsigned char* tree_out, uint64_t* codeword_out, const char* who)
+{
+    tp::Ctx* c = tp::ctx();
+    if (!c) return -1;
+    if (!check_n(N, who)) return -1;
+    if (!src || !tree_out) {
+        tp::set_error(tp::TP_ERR_ARG, "%s: null buffer", who);
+        return -1;
+    }
+    for (long long i = 0; i < 2 * N; ++i)
+        if (src[i] >= tp::P61) {
+            tp::set_error(tp::TP_ERR_ARG, "%s: element %lld is not canonical", who, i / 2);
+            return -1;
+        }
+    const long long col_len = N / tp::orion::kColumns;
+    const tp::orion::Encoder* e = tp::orion::encoder(col_len);
+    if (!e) return -1;
+    const long long cw_len = e->cw_len, leaves = tp::orion::tree_leaves(col_len);
+    cudaStream_t s = c->stream;
+    DevBuf d_src(16 * (size_t)N, s), d_rows(16 * (size_t)cw_len * tp::orion::kColumns, s),
+        d_tree(64 * (size_t)leaves, s);
+    if (!d_src.p || !d_rows.p || !d_tree.p) return -1;
+    if (tp::cuda_failed(cudaMemcpyAsync(d_src.p, src, 16 * (size_t)N, cudaMemcpyHostToDevice, s), "H2D"))
+        return -1;
+    if (!tp::orion::commit(*e, static_cast<const ulonglong2*>(d_src.p), nullptr, static_cast<ulonglong2*>(d_rows.p),
+                           static_cast<unsigned char*>(d_tree.p), s))
+        return -1;
+    if (tp::cuda_failed(cudaMemcpyAsync(tree_out, d_tree.p, 64 * (size_t)leaves, cudaMemcpyDeviceToHost, s), "D2H"))
+        return -1;
+    if (codeword_out) {
+        DevBuf d_cols(16 * (size_t)cw_len * tp::orion::kColumns, s);
+        if (!d_cols.p) return -1;
+        if (!tp::orion::rows_to_columns(static_cast<const ulonglong2*>(d_rows.p), cw_len,
+                                        static_cast<ulonglong2*>(d_cols.p), s))
+            return -1;
+        if (tp::cuda_failed(cudaMemcpyAsync(codeword_out, d_cols.p, 16 * (size_t)cw_len * tp::orion::kColumns,
+                                            cudaMemcpyDeviceToHost, s),
+                            "D2H"))
+            return -1;
+        if (tp::cuda_failed(cudaStreamSynchronize(s), "synchronize")) return -1;
+    }
+    return tp::cuda_failed(cudaStreamSynchronize(s), "synchronize") ? -1 : 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -70,27 +138,74 @@ int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_
 {
     tp::clear_error();
     if (!tp::ctx()) return -1;
-    if (!d_pixels || !d_rows || !d_tree || n_copies < 0 || n_copies > n_copies_padded || copy_size <= 0 ||
-        copy_size > n_wires || n_wires <= 0 || (n_wires & (n_wires - 1)) || n_copies_padded <= 0 ||
-        const_idx >= n_wires || (const_idx >= 0 && const_idx < copy_size) || const_val >= tp::P61) {
-        tp::set_error(tp::TP_ERR_ARG,
-                      "tp_orion_commit_pixels_dev: layout copies %d/%d, copy_size %d, wires %d, const %d",
-                      n_copies, n_copies_padded, copy_size, n_wires, const_idx);
+    tp::orion::PixelInput px;
+    long long N = 0;
+    if (!pixel_layout(d_pixels, n_copies, n_copies_padded, copy_size, n_wires, const_idx, const_val,
+                      "tp_orion_commit_pixels_dev", px, N))
+        return -1;
+    if (!d_rows || !d_tree) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_commit_pixels_dev: null buffer");
         return -1;
     }
-    const long long N = (long long)n_copies_padded * n_wires;
-    if (!check_n(N, "tp_orion_commit_pixels_dev")) return -1;
     const tp::orion::Encoder* e = tp::orion::encoder(N / tp::orion::kColumns);
     if (!e) return -1;
-    tp::orion::PixelInput px;
-    px.pix = static_cast<const unsigned char*>(d_pixels);
-    px.copies = n_copies;
-    px.cs = copy_size;
-    px.W = n_wires;
-    px.const_idx = const_idx;
-    px.const_val = const_val;
     return tp::orion::commit(*e, nullptr, &px, static_cast<ulonglong2*>(d_rows),
                              static_cast<unsigned char*>(d_tree), reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_orion_commit_zk_pixels_dev(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size,
+                                  int n_wires, int const_idx, uint64_t const_val, uint64_t mask_seed,
+                                  void* d_rows_masked, void* d_tree_masked, void* d_rows_mask, void* d_tree_mask,
+                                  void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    tp::orion::PixelInput px;
+    long long N = 0;
+    if (!pixel_layout(d_pixels, n_copies, n_copies_padded, copy_size, n_wires, const_idx, const_val,
+                      "tp_orion_commit_zk_pixels_dev", px, N))
+        return -1;
+    if (!d_rows_masked || !d_tree_masked || !d_rows_mask || !d_tree_mask) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_commit_zk_pixels_dev: null buffer");
+        return -1;
+    }
+    const tp::orion::Encoder* e = tp::orion::encoder(N / tp::orion::kColumns);
+    if (!e) return -1;
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    px.mask_seed = mask_seed;
+    px.mask_mode = tp::orion::kMaskMasked;
+    if (!tp::orion::commit(*e, nullptr, &px, static_cast<ulonglong2*>(d_rows_masked),
+                           static_cast<unsigned char*>(d_tree_masked), s))
+        return -1;
+    const int first = tp::orion::last_launches();
+    px.mask_mode = tp::orion::kMaskOnly;
+    if (!tp::orion::commit(*e, nullptr, &px, static_cast<ulonglong2*>(d_rows_mask),
+                           static_cast<unsigned char*>(d_tree_mask), s))
+        return -1;
+    tp::orion::add_launches(first);
+    return 0;
+}
+
+int tp_orion_pixel_vector_dev(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size, int n_wires,
+                              int const_idx, uint64_t const_val, uint64_t mask_seed, int mask_mode, void* d_out,
+                              void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    tp::orion::PixelInput px;
+    long long N = 0;
+    if (!pixel_layout(d_pixels, n_copies, n_copies_padded, copy_size, n_wires, const_idx, const_val,
+                      "tp_orion_pixel_vector_dev", px, N))
+        return -1;
+    if (!d_out || mask_mode < tp::orion::kMaskNone || mask_mode > tp::orion::kMaskOnly) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_pixel_vector_dev: null output or mask mode %d", mask_mode);
+        return -1;
+    }
+    px.mask_seed = mask_seed;
+    px.mask_mode = mask_mode;
+    return tp::orion::pixel_vector(px, N, static_cast<uint64_t*>(d_out), reinterpret_cast<cudaStream_t>(stream))
                ? 0
                : -1;
 }
@@ -177,46 +292,15 @@ int tp_orion_rows_to_columns_dev(const void* d_rows, long long cw_len, void* d_c
 int tp_orion_commit(const uint64_t* src, long long N, unsigned char* tree_out, uint64_t* codeword_out)
 {
     tp::clear_error();
-    tp::Ctx* c = tp::ctx();
-    if (!c) return -1;
-    if (!check_n(N, "tp_orion_commit")) return -1;
-    if (!src || !tree_out) {
-        tp::set_error(tp::TP_ERR_ARG, "tp_orion_commit: null buffer");
-        return -1;
-    }
-    for (long long i = 0; i < 2 * N; ++i)
-        if (src[i] >= tp::P61) {
-            tp::set_error(tp::TP_ERR_ARG, "tp_orion_commit: element %lld is not canonical", i / 2);
-            return -1;
-        }
-    const long long col_len = N / tp::orion::kColumns;
-    const tp::orion::Encoder* e = tp::orion::encoder(col_len);
-    if (!e) return -1;
-    const long long cw_len = e->cw_len, leaves = tp::orion::tree_leaves(col_len);
-    cudaStream_t s = c->stream;
-    DevBuf d_src(16 * (size_t)N, s), d_rows(16 * (size_t)cw_len * tp::orion::kColumns, s),
-        d_tree(64 * (size_t)leaves, s);
-    if (!d_src.p || !d_rows.p || !d_tree.p) return -1;
-    if (tp::cuda_failed(cudaMemcpyAsync(d_src.p, src, 16 * (size_t)N, cudaMemcpyHostToDevice, s), "H2D"))
-        return -1;
-    if (!tp::orion::commit(*e, static_cast<const ulonglong2*>(d_src.p), nullptr, static_cast<ulonglong2*>(d_rows.p),
-                           static_cast<unsigned char*>(d_tree.p), s))
-        return -1;
-    if (tp::cuda_failed(cudaMemcpyAsync(tree_out, d_tree.p, 64 * (size_t)leaves, cudaMemcpyDeviceToHost, s), "D2H"))
-        return -1;
-    if (codeword_out) {
-        DevBuf d_cols(16 * (size_t)cw_len * tp::orion::kColumns, s);
-        if (!d_cols.p) return -1;
-        if (!tp::orion::rows_to_columns(static_cast<const ulonglong2*>(d_rows.p), cw_len,
-                                        static_cast<ulonglong2*>(d_cols.p), s))
-            return -1;
-        if (tp::cuda_failed(cudaMemcpyAsync(codeword_out, d_cols.p, 16 * (size_t)cw_len * tp::orion::kColumns,
-                                            cudaMemcpyDeviceToHost, s),
-                            "D2H"))
-            return -1;
-        if (tp::cuda_failed(cudaStreamSynchronize(s), "synchronize")) return -1;
-    }
-    return tp::cuda_failed(cudaStreamSynchronize(s), "synchronize") ? -1 : 0;
+    return commit_host(src, N, tree_out, codeword_out, "tp_orion_commit");
+}
+
+int tp_orion_commit_pair(const uint64_t* masked, const uint64_t* mask, long long N, unsigned char* tree_masked,
+                         unsigned char* tree_mask)
+{
+    tp::clear_error();
+    if (commit_host(masked, N, tree_masked, nullptr, "tp_orion_commit_pair (masked)")) return -1;
+    return commit_host(mask, N, tree_mask, nullptr, "tp_orion_commit_pair (mask)");
 }
 
 }  // extern "C"

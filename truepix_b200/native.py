@@ -82,6 +82,10 @@ GKR_SIGNATURES = {
     "tp_orion_commit": (_I32, [_VP, ctypes.c_longlong, _VP, _VP]),
     "tp_orion_commit_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP, _VP]),
     "tp_orion_commit_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
+    "tp_orion_commit_pair": (_I32, [_VP, _VP, ctypes.c_longlong, _VP, _VP]),
+    "tp_orion_commit_zk_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _U64, _VP, _VP, _VP, _VP,
+                                             _VP]),
+    "tp_orion_pixel_vector_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _U64, _I32, _VP, _VP]),
     "tp_orion_rows_to_columns_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP]),
     "tp_orion_last_launches": (_I32, []),
     "tp_orion_combine_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP, _VP, _VP]),
