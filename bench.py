@@ -688,9 +688,11 @@ def ours_arm(args, rank, world, local_rank):
         c, w, b, m = bprover.results(B - 1)
         res_ok = bool(c.any() and w.any() and m != (0, 0) and any(committer.root(B - 1)))
 
-    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = None
+    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = None
     if rank == 0 and not args.skip_ntt:
         ntt = ntt_bench(lib, dev, stream)
+    if rank == 0 and not args.skip_opening:
+        opening = opening_bench(args, lib, committer, layout, dev, stream, sha_gcs)
     if rank == 0 and not args.skip_zk:
         zk = zk_step(args, bprover, pix, z1s, z2s, pts, chal_b, layout, stream, local_rank)
     if rank == 0 and not args.skip_e2e:
@@ -747,7 +749,7 @@ def ours_arm(args, rank, world, local_rank):
                             "with the commits serialised on the step's stream (CUDA events around "
                             "every launch), whose shares match the serialised ncu launch list"
                             % len(committer.side),
-            "ntt": ntt, "zk": zk, "batched_uneven": uneven, "serving": serving, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
+            "ntt": ntt, "opening": opening, "zk": zk, "batched_uneven": uneven, "serving": serving, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
             "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
         }
         print(json.dumps(line), flush=True)
@@ -798,6 +800,143 @@ def zk_step(args, bprover, pix, z1s, z2s, pts, chal_b, layout, stream, local_ran
                                               "and mask from a seed), one process"}
         except OSError as e:
             out["cpu_zk_commit"] = {"unavailable": str(e)}
+    return out
+
+
+def _cpu_opening(job):
+    """The reference's own code for one opening-side row on one core (oracle/_ref,
+    one fresh process per call): seconds of its work (ref_last_seconds), or None
+    when the reference build is absent."""
+    import ctypes
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from orionlib import ORION_REF_LIB, elements, virgo_inputs
+    if not os.path.exists(ORION_REF_LIB):
+        return None
+    lib = ctypes.CDLL(ORION_REF_LIB)
+    V = ctypes.c_void_p
+    lib.ref_last_seconds.restype = ctypes.c_double
+    kind, size = job
+    if kind == "combine":
+        lib.ref_combine.argtypes = [V, ctypes.c_longlong, V, V, V, V, V]
+        lib.ref_encode_len.argtypes = [ctypes.c_longlong]
+        lib.ref_encode_len.restype = ctypes.c_longlong
+        src = elements(1, size)
+        r0, r1 = elements(2, 128), elements(3, size // 128)
+        comb = np.zeros(2 * lib.ref_encode_len(size // 128), np.uint64)
+        ans = np.zeros(2, np.uint64)
+        lib.ref_combine(V(src.ctypes.data), size, V(r0.ctypes.data), V(r1.ctypes.data), V(comb.ctypes.data),
+                        ctypes.create_string_buffer(32), V(ans.ctypes.data))
+    elif kind == "virgo":
+        lib.ref_virgo_update.argtypes = [ctypes.c_int, V, V, V, ctypes.c_int, V, ctypes.c_int, V, V, V, V]
+        vma, addv, ams, r = virgo_inputs(size, 4)
+        outs = [np.zeros(4 * size, np.uint64) for _ in range(3)]
+        ret = np.zeros(6, np.uint64)
+        lib.ref_virgo_update(1, V(vma.ctypes.data), V(addv.ctypes.data), V(ams.ctypes.data), size,
+                             V(r.ctypes.data), 1, *[V(o.ctypes.data) for o in outs], V(ret.ctypes.data))
+    else:
+        lib.ref_fri_step.argtypes = [V, ctypes.c_int, V, V, V]
+        w = elements(5, (1 << size) * 64)
+        nxt = np.zeros(w.size // 2, np.uint64)
+        lib.ref_fri_step(V(w.ctypes.data), size, V(elements(6, 1).ctypes.data), V(nxt.ctypes.data),
+                         ctypes.create_string_buffer(32))
+    return lib.ref_last_seconds()
+
+
+def opening_bench(args, lib, committer, layout, dev, stream, sha_gcs, reps=5):
+    """The opening-side rows on the device, each against its roofline, with the
+    reference's CPU code for the same work timed beside it: the tensor-product
+    passes over a resident 1080p codeword (combine, its Merkle tree, answer,
+    queried columns), one Virgo sumcheck update and one FRI commit-phase step."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from orionlib import elements, virgo_inputs
+    peak, peak_kind = peaks()
+    s = stream.cuda_stream
+    N = layout.padded_copies * layout.n_wires
+    cw, leaves = committer.cw_len[0], committer.leaves[0]
+    rows = committer.rows[0]
+    dt = lambda a: torch.from_numpy(a.view(np.int64)).to(dev)
+    r0, r1 = dt(elements(2, 128)), dt(elements(3, N // 128))
+    comb = torch.empty(2 * cw, dtype=torch.int64, device=dev)
+    ctree = torch.empty(64 * leaves, dtype=torch.uint8, device=dev)
+    ans = torch.empty(2, dtype=torch.int64, device=dev)
+    q = torch.from_numpy(np.random.default_rng(7).integers(0, cw, size=1222, dtype=np.int64)).to(dev)
+    qout = torch.empty(2 * 128 * 1222, dtype=torch.int64, device=dev)
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def roof(bytes_, ms):
+        gbs = bytes_ / (ms / 1e3) / 1e9
+        return {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                "peak_source": peak_kind + " hbm_gbs" if peak_kind == "measured" else "fallback"}
+
+    out = {}
+    ms = timed(lambda: native.check(lib, lib.tp_orion_combine_dev(rows.data_ptr(), N, r0.data_ptr(),
+                                                                  comb.data_ptr(), None, s), "combine"))
+    out["combine"] = {"ms": ms, "rows": cw, "roofline": roof(cw * (2048 + 16), ms)}
+    ms_t = timed(lambda: native.check(lib, lib.tp_orion_combine_dev(rows.data_ptr(), N, r0.data_ptr(),
+                                                                    comb.data_ptr(), ctree.data_ptr(), s), "combine"))
+    comp = 2 * leaves + 2 * (leaves - 1)
+    out["combine_with_tree"] = {"ms": ms_t, "tree_ms": ms_t - ms, "leaves": leaves,
+                                "g_compressions_per_s": comp / ((ms_t - ms) / 1e3) / 1e9,
+                                "sha_peak_g_compressions_per_s": sha_gcs}
+    ms = timed(lambda: native.check(lib, lib.tp_orion_answer_dev(comb.data_ptr(), N // 128, r1.data_ptr(),
+                                                                 ans.data_ptr(), s), "answer"))
+    out["answer"] = {"ms": ms, "roofline": roof(32 * (N // 128), ms)}
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        native.check(lib, lib.tp_orion_query_columns_dev(rows.data_ptr(), N, q.data_ptr(), 1222, qout.data_ptr(),
+                                                         s), "query")
+    out["query_1222_columns"] = {"ms": 1e3 * (time.perf_counter() - t0) / reps,
+                                 "timer": "host wall clock (the call synchronises to check indices)"}
+    del comb, ctree, qout
+
+    n_v = 1 << 22
+    vma, addv, ams, r = (dt(a) for a in virgo_inputs(n_v, 4))
+    vouts = [torch.empty(4 * n_v // 2, dtype=torch.int64, device=dev) for _ in range(3)]
+    ret = torch.empty(6, dtype=torch.int64, device=dev)
+    rr = [int(x) for x in r.cpu().numpy().view(np.uint64)]
+    ms = timed(lambda: native.check(lib, lib.tp_virgo_sumcheck_update_dev(
+        vma.data_ptr(), addv.data_ptr(), ams.data_ptr(), n_v, rr[1], rr[0], 1, vouts[0].data_ptr(),
+        vouts[1].data_ptr(), vouts[2].data_ptr(), ret.data_ptr(), s), "virgo"))
+    out["virgo_update"] = {"ms": ms, "total_uv": n_v, "roofline": roof((192 + 96) * (n_v // 2), ms)}
+    del vma, addv, ams, vouts
+
+    lm = 18
+    w = dt(elements(5, (1 << lm) * 64))
+    nxt = torch.empty(w.numel() // 2, dtype=torch.int64, device=dev)
+    ftree = torch.empty(64 * (1 << (lm - 2)), dtype=torch.uint8, device=dev)
+    fr = [int(x) for x in elements(6, 1)]
+    ms = timed(lambda: native.check(lib, lib.tp_fri_commit_step_dev(w.data_ptr(), lm, fr[1], fr[0], nxt.data_ptr(),
+                                                                    ftree.data_ptr(), s), "fri step"))
+    n_leaves = 1 << (lm - 2)
+    comp = n_leaves * 128 + 2 * (n_leaves - 1)
+    out["fri_step"] = {"ms": ms, "log_m": lm, "witness_elements": (1 << lm) * 64,
+                       "g_compressions_per_s": comp / (ms / 1e3) / 1e9, "sha_peak_g_compressions_per_s": sha_gcs}
+    del w, nxt, ftree
+    torch.cuda.empty_cache()
+
+    if not args.skip_cpu:
+        import multiprocessing as mp
+        jobs = [("combine", N), ("virgo", n_v), ("fri", lm)]
+        with mp.get_context("spawn").Pool(1, maxtasksperchild=1) as pool:
+            secs = pool.map(_cpu_opening, jobs, chunksize=1)
+        for (kind, _), sec, key in zip(jobs, secs, ("combine_with_tree", "virgo_update", "fri_step")):
+            if sec is not None:
+                out[key]["cpu_reference_ms"] = 1e3 * sec
+                out[key]["speedup_vs_cpu_reference"] = 1e3 * sec / out[key]["ms"]
+        out["cpu_note"] = ("reference sources (oracle/_ref/liborion_ref.so) on one core, same sizes: "
+                           "combine + leaves + tree of a 2^23-element commit, phase-1 update of 2^22 "
+                           "entries, FRI step of 2^18 x 64 elements")
     return out
 
 
@@ -1031,6 +1170,7 @@ def main():
     ap.add_argument("--skip-ntt", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--skip-zk", action="store_true")
+    ap.add_argument("--skip-opening", action="store_true")
     ap.add_argument("--commit-streams", type=int, default=8,
                     help="streams the step's commits are spread over (0: the step's stream)")
     ap.add_argument("--profile-case", choices=["orion"], help="run a fixed short workload for ncu and exit")

@@ -4,6 +4,7 @@
 // under TruePix-main/Orion/Orion_nonzk (their own sources, compiled in place)
 // into oracle/_ref/liborion_ref.so. The golden generator and the CPU baseline
 // call these; the shipped library never links them.
+#include <chrono>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -22,7 +23,16 @@
 // the codeword commit() retains (defined in src/VPD/linearPC.cpp)
 extern prime_field::field_element** encoded_codeword;
 
+namespace {
+double g_seconds = 0;   // duration of the reference work of the last ref_combine / ref_virgo_update / ref_fri_step
+double now() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+}  // namespace
+
 extern "C" {
+
+// seconds the reference's own work took in the last ref_combine (the passes
+// after commit()), ref_virgo_update (the update call) or ref_fri_step (the step)
+double ref_last_seconds(void) { return g_seconds; }
 
 // SHA-256 of one 64-byte block exactly as Orion hashes it (my_hhash)
 void ref_hhash64(const unsigned char* in, unsigned char* out32)
@@ -112,6 +122,7 @@ void ref_combine(const uint64_t* src, long long N, const uint64_t* r0, const uin
     const long long msg_len = N / column_size, cw_len = encode_output_len(msg_len);
     const F* R0 = reinterpret_cast<const F*>(r0);
     const F* R1 = reinterpret_cast<const F*>(r1);
+    const double t0 = now();
     F* comb = new F[cw_len];
     for (long long t = 0; t < cw_len; ++t) comb[t] = F(0ULL);
     for (int j = 0; j < column_size; ++j)
@@ -127,6 +138,7 @@ void ref_combine(const uint64_t* src, long long N, const uint64_t* r0, const uin
         leaves[i] = merkle_tree::hash_single_field_element(i < cw_len ? comb[i] : zero);
     __hhash_digest* mt = nullptr;
     merkle_tree::merkle_tree_prover::create_tree(leaves, msg_len * 2, mt, sizeof(__hhash_digest), true);
+    g_seconds = now() - t0;
     memcpy(root32, &mt[1], 32);
     free(mt);
     delete[] leaves;
@@ -152,8 +164,10 @@ void ref_virgo_update(int phase, const uint64_t* vma, const uint64_t* addv, cons
     p->total_uv = n;
     prime_field::field_element pr;
     memcpy(&pr, r, 16);
+    const double t0 = now();
     quadratic_poly q = phase == 1 ? p->sumcheck_phase1_update(pr, current_bit)
                                   : p->sumcheck_phase2_update(pr, current_bit);
+    g_seconds = now() - t0;
     memcpy(vma_out, p->V_mult_add, 16 * (size_t)n);
     memcpy(addv_out, p->addV_array, 16 * (size_t)n);
     memcpy(ams_out, p->add_mult_sum, 16 * (size_t)n);
@@ -196,7 +210,9 @@ void ref_fri_step(const uint64_t* witness, int log_m, const uint64_t* r, uint64_
     for (int i = 1; i < M; ++i) fri::L_group[i] = fri::L_group[i - 1] * w;
     F fr;
     memcpy(&fr, r, 16);
+    const double t0 = now();
     __hhash_digest h = fri::commit_phase_step(fr);
+    g_seconds = now() - t0;
     memcpy(root32, &h, 32);
     memcpy(next, fri::cpd.rs_codeword[1], 16 * (size_t)(M / 2) * slice_number);
 }
