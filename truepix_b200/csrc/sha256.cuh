@@ -147,13 +147,64 @@ __host__ __device__ __forceinline__ void compress_pad64(uint32_t st[8], Add add)
     st[4] = add(st[4], e); st[5] = add(st[5], f); st[6] = add(st[6], g); st[7] = add(st[7], h);
 }
 
+#ifdef __CUDACC__
+// round constants (and the padding block's k + w) for the device's compact form
+static __constant__ Tables kShaTables = make_tables();
+
+// One compression in compact form: four passes over a 16-round body (the
+// schedule's rolling index and the round variables' rotation repeat every 16
+// rounds, so the body indexes registers statically) with the round constants
+// read from constant memory. A quarter of the fully unrolled code: the leaf and
+// tree kernels, which keep one hash in flight per thread, then run from the
+// instruction cache instead of streaming ~40 KB of straight-line code per hash.
+// kSched: message block w (consumed as the rolling schedule); otherwise the
+// constant padding block, K holding its k + w.
+template <bool kSched, class Add>
+__device__ __forceinline__ void compress_compact(uint32_t st[8], uint32_t w[16], const uint32_t* K, Add add)
+{
+    uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
+#pragma unroll 1
+    for (int i = 0; i < 64; i += 16) {
+#pragma unroll
+        for (int j = 0; j < 16; j += 8) {
+            if (kSched && i > 0) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int t = j + q;    // w[t] holds word i + t - 16 here
+                    const uint32_t x = w[(t + 1) & 15], y = w[(t + 14) & 15];
+                    w[t] = add(add(w[t], rotr(x, 7) ^ rotr(x, 18) ^ (x >> 3)),
+                               add(w[(t + 9) & 15], rotr(y, 17) ^ rotr(y, 19) ^ (y >> 10)));
+                }
+            }
+#define TP_SHA_KW(q) (kSched ? add(w[j + q], K[i + j + q]) : K[i + j + q])
+            TP_SHA_ROUND(a, b, c, d, e, f, g, h, TP_SHA_KW(0));
+            TP_SHA_ROUND(h, a, b, c, d, e, f, g, TP_SHA_KW(1));
+            TP_SHA_ROUND(g, h, a, b, c, d, e, f, TP_SHA_KW(2));
+            TP_SHA_ROUND(f, g, h, a, b, c, d, e, TP_SHA_KW(3));
+            TP_SHA_ROUND(e, f, g, h, a, b, c, d, TP_SHA_KW(4));
+            TP_SHA_ROUND(d, e, f, g, h, a, b, c, TP_SHA_KW(5));
+            TP_SHA_ROUND(c, d, e, f, g, h, a, b, TP_SHA_KW(6));
+            TP_SHA_ROUND(b, c, d, e, f, g, h, a, TP_SHA_KW(7));
+#undef TP_SHA_KW
+        }
+    }
+    st[0] = add(st[0], a); st[1] = add(st[1], b); st[2] = add(st[2], c); st[3] = add(st[3], d);
+    st[4] = add(st[4], e); st[5] = add(st[5], f); st[6] = add(st[6], g); st[7] = add(st[7], h);
+}
+#endif
+
 // SHA-256 of the 64-byte message given as 16 big-endian words; out = state words
 template <class Add = AddAlu>
 __host__ __device__ __forceinline__ void hash64(uint32_t w[16], uint32_t out[8], Add add = Add())
 {
     init(out);
+#ifdef __CUDA_ARCH__
+    compress_compact<true>(out, w, kShaTables.k, add);
+    compress_compact<false>(out, w, kShaTables.pad_kw, add);
+#else
     compress(out, w, add);
     compress_pad64(out, add);
+#endif
 }
 
 // The message words of a field element (16 bytes: u64 img then u64 real, both
