@@ -959,11 +959,20 @@ def e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream,
         claims_h.copy_(bprover.claims[k * B * 8:(k + 1) * B * 8], non_blocking=True)
         stream.synchronize()
 
+    copy = torch.cuda.Stream(dev)
+    landed = [torch.cuda.Event() for _ in range(B)]
+
     def one():
-        with torch.cuda.stream(stream):
-            for d, h in zip(dpix, host):
+        # frames go up on a copy stream one by one; each frame's commit starts when
+        # its own bytes have landed, the batched rounds when all have
+        copy.wait_stream(stream)
+        with torch.cuda.stream(copy):
+            for d, h, ev in zip(dpix, host, landed):
                 d.copy_(h, non_blocking=True)
-            committer.commit(dpix, join=False)      # commits run under the rounds
+                ev.record(copy)
+        with torch.cuda.stream(stream):
+            committer.commit(dpix, join=False, ready=landed)      # commits run under the rounds
+            stream.wait_event(landed[-1])
             bprover.prove(dpix, z1s, z2s, pts, chal_b, round_hook=hook)
             committer.join()
             for f in range(B):
@@ -984,7 +993,8 @@ def e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream,
     return {"value": steps * B / wall, "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": steps, "frames_per_step": B,
             "timer": "host wall clock", "path": "tp_batch_* + tp_orion_commit_pixels_dev from "
-            "pinned host frames, claims read back every round, roots at the end"}
+            "pinned host frames (copied frame by frame on a copy stream; each commit starts when its "
+            "frame has landed), claims read back every round, roots at the end"}
 
 
 def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):

@@ -195,3 +195,29 @@ def test_opening_passes_match_reference(lib, og):
                                       rows[[0, cw_len - 1, col, 7 % cw_len]])
         bad = torch.tensor([cw_len], dtype=torch.int64, device=dev)
         assert lib.tp_orion_query_columns_dev(d_rows.data_ptr(), n, bad.data_ptr(), 1, qout.data_ptr(), s) == -1
+
+
+def test_committer_waits_for_each_frames_upload(lib, orc):
+    """Frames uploaded one by one on a copy stream, each commit gated on its own
+    frame's event (FrameCommitter.commit(ready=...)): same roots as the oracle."""
+    import torch
+    from truepix_b200.frame import FrameLayout
+    from truepix_b200.orion import FrameCommitter
+    layouts = [FrameLayout(copies=c) for c in (100, 64, 30, 200)]
+    host = [torch.from_numpy(frame_bytes(40 + f, L.copies * 384)).pin_memory() for f, L in enumerate(layouts)]
+    dev = torch.device("cuda", 0)
+    dpix = [torch.empty_like(h, device=dev) for h in host]
+    copy = torch.cuda.Stream(dev)
+    ev = [torch.cuda.Event() for _ in layouts]
+    fc = FrameCommitter(layouts, side_streams=2)
+    for _ in range(2):
+        copy.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(copy):
+            for d, h, e in zip(dpix, host, ev):
+                d.copy_(h, non_blocking=True)
+                e.record(copy)
+        fc.commit(dpix, ready=ev)
+        torch.cuda.synchronize()
+        for f, L in enumerate(layouts):
+            src = frame_elements(host[f].numpy(), L.copies, 384, 512, 384, 128, L.padded_copies)
+            assert fc.root(f) == orc.commit(src), f

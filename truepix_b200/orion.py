@@ -59,23 +59,28 @@ class FrameCommitter:
         return self.stream.cuda_stream if self.stream is not None else \
             self.torch.cuda.current_stream(self.dev).cuda_stream
 
-    def commit(self, pixels, join: bool = True, mask_seeds=None) -> None:
+    def commit(self, pixels, join: bool = True, mask_seeds=None, ready=None) -> None:
         """Queue the commits of all frames (pixels: one uint8 device tensor each).
         With side streams and join=False the step's stream does not wait for them
         here (work queued on it next overlaps the commits); call join() later.
-        mask_seeds: one 64-bit seed per frame, required (only) for zk."""
+        mask_seeds: one 64-bit seed per frame, required (only) for zk.
+        ready: optional CUDA events, one per frame, recorded when that frame's
+        bytes are in place (e.g. after its host-to-device copy on a copy stream):
+        each frame's commit waits for its own event only."""
         if self.zk != (mask_seeds is not None):
             raise ValueError("mask_seeds are given exactly for a zk committer")
         torch, lib, s = self.torch, self.lib, self._s()
         launches = 0
         main = self.stream if self.stream is not None else torch.cuda.current_stream(self.dev)
         if self.side:
-            ready = torch.cuda.Event()
-            ready.record(main)
+            start = torch.cuda.Event()
+            start.record(main)
             for q in self.side:
-                q.wait_event(ready)
+                q.wait_event(start)
         for f, L in enumerate(self.layouts):
             fs = self.side[f % len(self.side)].cuda_stream if self.side else s
+            if ready is not None:
+                (self.side[f % len(self.side)] if self.side else main).wait_event(ready[f])
             if self.zk:
                 native.check(lib, lib.tp_orion_commit_zk_pixels_dev(
                     pixels[f].data_ptr(), L.copies, L.padded_copies, L.copy_size, L.n_wires,
