@@ -100,3 +100,25 @@ def test_admission_respects_the_hbm_budget():
     out = srv.run(reqs, realtime=False)
     assert len(out) == len(reqs)
     assert peak[0] <= budget
+
+
+def test_pinned_tensor_frames_equal_numpy_frames():
+    """Frames handed over in pinned host memory (copied straight to the device)
+    and as numpy arrays (through the staging buffers), in one realtime run with
+    small commit and slot pools: identical results."""
+    import torch
+    from truepix_b200.serving import ProofServer
+    base = by_rid(ProofServer(slots=4).run(requests(), realtime=False))
+    reqs = requests()
+    for k, r in enumerate(reqs):
+        if k % 2 == 0:
+            r.pixels = torch.from_numpy(r.pixels).pin_memory()
+        r.arrival = 0.002 * k
+    srv = ProofServer(slots=3, commit_buffers=2)
+    got = by_rid(srv.run(reqs, realtime=True))
+    assert sorted(got) == sorted(base)
+    for rid in base:
+        assert same(got[rid], base[rid]), rid
+    with pytest.raises(ValueError):
+        srv.run([type(reqs[0])(99, reqs[0].circuit, 120, 160, torch.zeros(120 * 160 * 3, dtype=torch.uint8),
+                               seed=1)], realtime=False)

@@ -51,7 +51,10 @@ class Request:
     circuit: Circuit
     height: int
     width: int
-    pixels: np.ndarray            # uint8, height * width * 3 bytes (host)
+    # uint8, height * width * 3 bytes on the host: a numpy array (copied through
+    # a pinned staging buffer) or a pinned torch tensor (copied straight to the
+    # device; keep it unchanged until the request's Result is returned)
+    pixels: object
     seed: int
     arrival: float = 0.0          # seconds after the start of the run
 
@@ -105,9 +108,15 @@ class _Job:
         self.z2 = b["z2"][:2 * nb]
         self.point = b["point"][:2 * (ni + nb)]
         self.wires, self.mle = b["wires"], b["mle"]
-        srv.upload(self.pix, req.pixels, L.copies * L.copy_size)
-        self.z2.copy_(srv.torch.from_numpy(pack_fp2(z2[:, 0], z2[:, 1])))
-        self.point.copy_(srv.torch.from_numpy(pack_fp2(point[:, 0], point[:, 1])))
+        self.out_h = b["out_h"]      # pinned: wires, beta, MLE, root after the commit
+        # transcript values through the slot's pinned buffer (a pageable source
+        # would synchronise the stream); the slot's previous job is long done
+        zh = b["z_h"].numpy()
+        zh[:2 * nb] = pack_fp2(z2[:, 0], z2[:, 1])
+        zh[2 * nb:2 * nb + 2 * (ni + nb)] = pack_fp2(point[:, 0], point[:, 1])
+        srv.upload(self.pix, req.pixels, L.copies * L.copy_size, after=lambda: (
+            self.z2.copy_(b["z_h"][:2 * nb], non_blocking=True),
+            self.point.copy_(b["z_h"][2 * nb:2 * nb + 2 * (ni + nb)], non_blocking=True)))
         self.round = 0
         self.host_claims = []          # what the host transcript read, round by round
         self.done_event = None
@@ -130,12 +139,15 @@ class ProofServer:
     later keeps the codeword instead (truepix_b200.orion.FrameCommitter)."""
 
     def __init__(self, slots: int = 64, hbm_budget: float = 40e9, device: int = 0, max_height: int = 2160,
-                 max_width: int = 3840, commit_buffers: int = 8):
+                 max_width: int = 3840, commit_buffers: int = 16):
         import torch
         self.torch = torch
         self.lib = native.gkr()
         self.dev = torch.device("cuda", device)
-        self.stream = torch.cuda.Stream(self.dev)
+        # the rounds' stream has the higher priority: its small claim and fold
+        # kernels (on which the host waits every tick) go ahead of queued commits
+        self.stream = torch.cuda.Stream(self.dev, priority=-1)
+        self.upload_stream = torch.cuda.Stream(self.dev)
         # commits go round-robin over a few streams so that one frame's
         # latency-bound commit phases overlap another's SHA-256 leaves
         self.commit_streams = [torch.cuda.Stream(self.dev) for _ in range(max(1, commit_buffers))]
@@ -154,16 +166,19 @@ class ProofServer:
                            "z2": torch.empty(2 * nbmax, dtype=i64, device=dev),
                            "point": torch.empty(2 * (9 + nbmax), dtype=i64, device=dev),
                            "wires": torch.zeros(2 * 513, dtype=i64, device=dev),
-                           "mle": torch.zeros(2, dtype=i64, device=dev)} for _ in range(slots)]
+                           "mle": torch.zeros(2, dtype=i64, device=dev),
+                           "z_h": torch.zeros(2 * (9 + 2 * nbmax), dtype=i64).pin_memory(),
+                           "out_h": torch.zeros(2 * 513 + 2 + 4, dtype=i64).pin_memory()}
+                          for _ in range(slots)]
         col = self.max_copies * 512 // 128
         cw_max = self.lib.tp_orion_codeword_len(col)
         leaves_max = self.lib.tp_orion_tree_leaves(col * 128)
         self.commit_free = [(torch.empty(2 * 128 * cw_max, dtype=i64, device=dev),
                              torch.empty(64 * leaves_max, dtype=torch.uint8, device=dev))
                             for _ in range(commit_buffers)]
-        # two pinned staging buffers for frame uploads (one may be in flight)
-        self.staging = [torch.empty(self.max_bytes, dtype=torch.uint8).pin_memory() for _ in range(2)]
-        self.staging_ev = [None, None]
+        # pinned staging buffers for numpy frames (a few uploads may be in flight)
+        self.staging = [torch.empty(self.max_bytes, dtype=torch.uint8).pin_memory() for _ in range(3)]
+        self.staging_ev = [None] * len(self.staging)
         self.staging_next = 0
         self.free = list(range(slots))[::-1]
         self.active: dict = {}          # slot -> _Job
@@ -196,23 +211,39 @@ class ProofServer:
         leaves = 1 << math.ceil(math.log2(2 * col))
         return 16 * rows * (C // 2 + C // 4) + 32 * C + L.copies * L.copy_size + 2048 * cw + 64 * leaves
 
-    def upload(self, d_pix, pixels: np.ndarray, n: int):
-        """Frame bytes to the slot's device buffer through a pinned staging buffer
-        (zero-padded to the layout's copies x copy_size)."""
+    def upload(self, d_pix, pixels, n: int, after=None):
+        """Frame bytes to the slot's device buffer (zero-padded to the layout's
+        copies x copy_size) on the upload stream: a pinned torch tensor directly,
+        a numpy array through a pinned staging buffer. `after()` queues more
+        copies behind it. The rounds' stream waits for the upload, the host only
+        for a staging buffer's previous copy (DMA, never kernels)."""
         torch = self.torch
-        k = self.staging_next
-        self.staging_next ^= 1
-        if self.staging_ev[k] is not None:
-            self.staging_ev[k].synchronize()
-        h = self.staging[k].numpy()
-        m = min(n, pixels.size)
-        h[:m] = pixels.reshape(-1)[:m]
-        h[m:n] = 0
-        with torch.cuda.stream(self.stream):
-            d_pix.copy_(self.staging[k][:n], non_blocking=True)
+        with torch.cuda.stream(self.upload_stream):
+            if isinstance(pixels, torch.Tensor):
+                if not pixels.is_pinned():
+                    raise ValueError("tensor frames must be in pinned host memory")
+                src = pixels.reshape(-1)
+                m = min(n, src.numel())
+                d_pix[:m].copy_(src[:m], non_blocking=True)
+                if m < n:
+                    d_pix[m:n].zero_()
+            else:
+                k = self.staging_next
+                self.staging_next = (k + 1) % len(self.staging)
+                if self.staging_ev[k] is not None:
+                    self.staging_ev[k].synchronize()
+                h = self.staging[k].numpy()
+                m = min(n, pixels.size)
+                h[:m] = pixels.reshape(-1)[:m]
+                h[m:n] = 0
+                d_pix.copy_(self.staging[k][:n], non_blocking=True)
+                self.staging_ev[k] = torch.cuda.Event()
+                self.staging_ev[k].record(self.upload_stream)
+            if after is not None:
+                after()
             ev = torch.cuda.Event()
-            ev.record(self.stream)
-        self.staging_ev[k] = ev
+            ev.record(self.upload_stream)
+        self.stream.wait_event(ev)
 
     def _start(self, req: Request):
         lib, s = self.lib, self.stream.cuda_stream
@@ -255,6 +286,11 @@ class ProofServer:
             job.pix.data_ptr(), L.copies, L.padded_copies, L.copy_size, L.n_wires, L.const_idx,
             L.const_val, rows.data_ptr(), tree.data_ptr(), cs.cuda_stream), "commit")
         self.launches += lib.tp_orion_last_launches() + 3
+        # results to the slot's pinned buffer behind the commit (read by _collect)
+        with torch.cuda.stream(cs):
+            job.out_h[:2 * 513].copy_(job.wires, non_blocking=True)
+            job.out_h[2 * 513:2 * 513 + 2].copy_(job.mle, non_blocking=True)
+            job.out_h[2 * 513 + 2:].copy_(tree[32:64].view(torch.int64), non_blocking=True)
         job.done_event = torch.cuda.Event()
         job.done_event.record(cs)
         del self.active[job.slot]
@@ -269,9 +305,10 @@ class ProofServer:
                 job.done_event.synchronize()
             if job.done_event.query():
                 c = np.stack(job.host_claims)
-                w = job.wires.cpu().numpy().view(np.uint64).reshape(513, 2)
-                m = job.mle.cpu().numpy().view(np.uint64)
-                root = job.commit_buf[1][32:64].cpu().numpy().tobytes()
+                out = job.out_h.numpy().view(np.uint64)
+                w = out[:2 * 513].reshape(513, 2)
+                m = out[2 * 513:2 * 513 + 2]
+                root = out[2 * 513 + 2:].tobytes()
                 self._out.append(Result(job.req.rid, c, w[:job.L.n_wires].copy(),
                                         (int(w[job.L.n_wires, 0]), int(w[job.L.n_wires, 1])),
                                         (int(m[0]), int(m[1])), root, job.req.arrival,
