@@ -58,6 +58,13 @@ int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_
                                int n_wires, int const_idx, uint64_t const_val, void* d_rows,
                                void* d_tree, void* stream);
 
+/* No counterpart in the reference. The SHA-256 row-leaf chains of later commits
+ * (of every kind) run as n launches of 64 / n column pairs each, n in {1, 2, 4,
+ * 8, 16}, default 1 (process-wide). Shorter launches release SMs sooner to
+ * kernels of other streams, e.g. the rounds a serving loop waits on; the
+ * digests do not depend on n. 0, or -1 for another n. */
+int tp_orion_set_leaf_chunks(int n);
+
 /* Zero-knowledge commits (TruePix-main/Orion/Orion_zk). Replaces
  * commit_pair(masked, mask, N) of src/VPD/linearPC.cpp:253-460: two Orion
  * commits, each byte-identical to commit() of its polynomial, trees returned

@@ -221,3 +221,24 @@ def test_committer_waits_for_each_frames_upload(lib, orc):
         for f, L in enumerate(layouts):
             src = frame_elements(host[f].numpy(), L.copies, 384, 512, 384, 128, L.padded_copies)
             assert fc.root(f) == orc.commit(src), f
+
+
+def test_leaf_chains_split_over_launches_give_the_same_tree(lib, orc):
+    """tp_orion_set_leaf_chunks: the row-leaf chains run as 1, 2, 4, 8 or 16
+    launches carrying the running state in the leaf slots; the trees agree
+    bit for bit (and with the oracle), other values are rejected."""
+    pix = frame_bytes(77, 100 * 384)
+    want = None
+    try:
+        for n in (1, 2, 4, 8, 16):
+            assert lib.tp_orion_set_leaf_chunks(n) == 0
+            tree = _pixel_commit(lib, pix, 100, 384, 512, 384, 128, 128)
+            if want is None:
+                want = tree
+                src = frame_elements(pix, 100, 384, 512, 384, 128, 128)
+                assert tree[1].tobytes() == orc.commit(src)
+            np.testing.assert_array_equal(tree, want)
+        for bad in (0, 3, 32, -1):
+            assert lib.tp_orion_set_leaf_chunks(bad) == -1
+    finally:
+        lib.tp_orion_set_leaf_chunks(1)

@@ -1,6 +1,7 @@
 // Orion commit on the device: expander encode (gathers over target-sorted
 // graphs) and the SHA-256 Merkle tree. See orion.h for the layout.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -17,6 +18,7 @@ namespace orion {
 namespace {
 
 thread_local int g_launches = 0;
+std::atomic<int> g_leaf_chunks{1};   // launches the row-leaf chains are split into
 
 // kernel-timer tags (runtime.h timer_*): commit kernels are 9100 + kind
 constexpr int kTagLoad = 9100, kTagGatherBytes = 9101, kTagGather = 9102, kTagLeaf = 9103, kTagTree = 9104;
@@ -384,17 +386,23 @@ __device__ __forceinline__ void load_digest(const unsigned char* tree, long long
 // h <- SHA256(h || rows[r][2j] || rows[r][2j+1]) for j = 0..63 from h = 0.
 // One thread per row; the CTA stages 128 rows x 8 columns (padded to 9, so
 // that 16-byte reads of consecutive rows fall in distinct banks) at a time.
+// A launch covers the column pairs [pair0, pair1) (multiples of kLeafPairs): a
+// chain split over several launches keeps its running state in the row's leaf
+// slot (raw state words) between them, the last launch stores the digest bytes.
+// Shorter launches free SMs sooner for other streams' kernels.
 __global__ void __launch_bounds__(kLeafRows) leaf_kernel(const ulonglong2* __restrict__ rows, long long cw_len,
                                                          unsigned char* __restrict__ tree, long long leaf0,
-                                                         uint32_t one)
+                                                         uint32_t one, int pair0, int pair1)
 {
     __shared__ ulonglong2 tile[kLeafRows][2 * kLeafPairs + 1];
     const long long r0 = (long long)blockIdx.x * kLeafRows;
     const int tid = threadIdx.x;
+    const bool live = r0 + tid < cw_len;
+    uint32_t* slot = reinterpret_cast<uint32_t*>(tree + (leaf0 + r0 + tid) * 32);
     uint32_t st[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) st[i] = 0;
-    for (int pair = 0; pair < kColumns / 2; pair += kLeafPairs) {
+    for (int i = 0; i < 8; ++i) st[i] = (pair0 > 0 && live) ? slot[i] : 0;
+    for (int pair = pair0; pair < pair1; pair += kLeafPairs) {
 #pragma unroll
         for (int k = 0; k < 2 * kLeafPairs; ++k) {
             const int i = tid + k * kLeafRows;
@@ -415,7 +423,13 @@ __global__ void __launch_bounds__(kLeafRows) leaf_kernel(const ulonglong2* __res
         }
         __syncthreads();
     }
-    if (r0 + tid < cw_len) store_digest(tree, leaf0 + r0 + tid, st);
+    if (!live) return;
+    if (pair1 == kColumns / 2) {
+        store_digest(tree, leaf0 + r0 + tid, st);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) slot[i] = st[i];
+    }
 }
 
 // tree[leaf0 + i] for i in [from, to): `a` below `split`, `b` from there on
@@ -618,6 +632,16 @@ const Encoder* encoder(long long col_len)
 }
 
 int last_launches() { return g_launches; }
+
+bool set_leaf_chunks(int n)
+{
+    if (n != 1 && n != 2 && n != 4 && n != 8 && n != 16) {
+        set_error(TP_ERR_ARG, "leaf chunks %d: must be 1, 2, 4, 8 or 16", n);
+        return false;
+    }
+    g_leaf_chunks.store(n);
+    return true;
+}
 void add_launches(int n) { g_launches += n; }
 
 bool sha_peak(int blocks, int iters, uint32_t* out, cudaStream_t s)
@@ -707,10 +731,14 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
         if (!launch_ok("orion D gather")) return false;
     }
     // 4. row leaves, constant leaves for the zero rows and the tree padding
-    timer_begin(s, kTagLeaf);
-    leaf_kernel<<<(unsigned)((cw_len + kLeafRows - 1) / kLeafRows), kLeafRows, 0, s>>>(rows, cw_len, tree, size, 1u);
-    timer_end(s);
-    if (!launch_ok("orion leaves")) return false;
+    const int chunks = g_leaf_chunks.load();
+    for (int k = 0; k < chunks; ++k) {
+        timer_begin(s, kTagLeaf);
+        leaf_kernel<<<(unsigned)((cw_len + kLeafRows - 1) / kLeafRows), kLeafRows, 0, s>>>(
+            rows, cw_len, tree, size, 1u, k * (kColumns / 2) / chunks, (k + 1) * (kColumns / 2) / chunks);
+        timer_end(s);
+        if (!launch_ok("orion leaves")) return false;
+    }
     if (size > cw_len) {
         unsigned char zr[32], zb[32];
         zero_row_leaf(zr);

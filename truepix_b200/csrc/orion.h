@@ -118,6 +118,12 @@ bool answer(const ulonglong2* combined, const ulonglong2* r1, long long n, ulong
 // in registers (2 compressions each); XORs its last digest into *out
 bool sha_peak(int blocks, int iters, uint32_t* out, cudaStream_t s);
 
+// The row-leaf chains of later commits run as n launches of 64 / n column pairs
+// each (n in 1, 2, 4, 8, 16; default 1): shorter launches release SMs sooner to
+// kernels of other streams (latency of a serving loop's rounds), at the cost of
+// n - 1 launches and 64 bytes per row of extra traffic. Same digests for any n.
+bool set_leaf_chunks(int n);
+
 // launches issued by commit() / build_tree() on this thread since the last commit()
 int last_launches();
 // adds n to that count (entry points that run several commits)

@@ -212,6 +212,12 @@ int tp_orion_pixel_vector_dev(const void* d_pixels, int n_copies, int n_copies_p
 
 int tp_orion_last_launches(void) { return tp::orion::last_launches(); }
 
+int tp_orion_set_leaf_chunks(int n)
+{
+    tp::clear_error();
+    return tp::orion::set_leaf_chunks(n) ? 0 : -1;
+}
+
 int tp_orion_combine_dev(const void* d_rows, long long N, const void* d_r0, void* d_combined, void* d_ctree,
                          void* stream)
 {

@@ -139,10 +139,14 @@ class ProofServer:
     later keeps the codeword instead (truepix_b200.orion.FrameCommitter)."""
 
     def __init__(self, slots: int = 64, hbm_budget: float = 40e9, device: int = 0, max_height: int = 2160,
-                 max_width: int = 3840, commit_buffers: int = 16):
+                 max_width: int = 3840, commit_buffers: int = 16, leaf_chunks: int = 4):
+        """leaf_chunks: the commits' SHA-256 leaf chains run as that many shorter
+        launches (tp_orion_set_leaf_chunks, process-wide), so SMs free up sooner
+        for the rounds the loop waits on every tick."""
         import torch
         self.torch = torch
         self.lib = native.gkr()
+        native.check(self.lib, self.lib.tp_orion_set_leaf_chunks(leaf_chunks), "leaf chunks")
         self.dev = torch.device("cuda", device)
         # the rounds' stream has the higher priority: its small claim and fold
         # kernels (on which the host waits every tick) go ahead of queued commits
