@@ -525,6 +525,7 @@ def ours_arm(args, rank, world, local_rank):
     chal_b = np.ascontiguousarray(np.broadcast_to(chal[:, None, :], (nb, B, 2)))
     stream = torch.cuda.Stream(dev)
     lib = native.gkr()
+    native.check(lib, lib.tp_orion_set_leaf_chunks(args.leaf_chunks), "leaf chunks")
     bprover = BatchFrameProver([layout] * B, gt, i0, i1, device=local_rank, stream=stream)
     committer = FrameCommitter([layout] * B, device=local_rank, stream=stream, side_streams=args.commit_streams)
     cw_len, leaves = committer.cw_len[0], committer.leaves[0]
@@ -1190,6 +1191,8 @@ def main():
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--skip-zk", action="store_true")
     ap.add_argument("--skip-opening", action="store_true")
+    ap.add_argument("--leaf-chunks", type=int, default=1,
+                    help="launches the commits' SHA-256 leaf chains are split into (tp_orion_set_leaf_chunks)")
     ap.add_argument("--commit-streams", type=int, default=8,
                     help="streams the step's commits are spread over (0: the step's stream)")
     ap.add_argument("--profile-case", choices=["orion"], help="run a fixed short workload for ncu and exit")
