@@ -689,7 +689,7 @@ def ours_arm(args, rank, world, local_rank):
         c, w, b, m = bprover.results(B - 1)
         res_ok = bool(c.any() and w.any() and m != (0, 0) and any(committer.root(B - 1)))
 
-    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = None
+    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = ref_gpu = None
     if rank == 0 and not args.skip_ntt:
         ntt = ntt_bench(lib, dev, stream)
     if rank == 0 and not args.skip_opening:
@@ -699,6 +699,7 @@ def ours_arm(args, rank, world, local_rank):
     if rank == 0 and not args.skip_e2e:
         e2e = e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream, dev)
         e2e_ref = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
+        ref_gpu = reference_gpu_lib(frames[0], layout, gt, i0, i1, z1, z2, point, chal)
     if rank == 0 and not args.skip_serving:
         del bprover
         committer.rows = committer.trees = None
@@ -751,6 +752,7 @@ def ours_arm(args, rank, world, local_rank):
                             "every launch), whose shares match the serialised ncu launch list"
                             % len(committer.side),
             "ntt": ntt, "opening": opening, "zk": zk, "batched_uneven": uneven, "serving": serving, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
+            "reference_gpu_library": ref_gpu,
             "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
         }
         print(json.dumps(line), flush=True)
@@ -1064,6 +1066,49 @@ def e2e_c_abi(args, lib, pix, layout, gt, i0, i1, z1, z2, point, chal):
             "d2h_bytes_per_step": d2h, "steps": steps, "timer": "host wall clock (synchronous API)",
             "path": "native_fp2_compute_beta/early_create/claim/fold/finish/mle_eval_base + "
                     "tp_orion_commit (the whole tree back), pinned host buffers"}
+
+
+def reference_gpu_lib(frame, layout, gt, i0, i1, z1, z2, point, chal, reps=3):
+    """The GKR part of one 1080p frame (compute_beta, early_create, 14 x claim +
+    fold, finish, mle_eval_base) through the 14-symbol C ABI with host buffers,
+    for the reference's own CUDA library (native_fp2.cu built for sm_100a,
+    oracle/_ref/libnative_fp2_ref_gpu.so) and for ours, same inputs, same calls;
+    outputs compared bit for bit. Host wall clock, synchronous API."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from fp2lib import GPU_LIB, REF_GPU_LIB, Fp2Lib, run_session
+    if not os.path.exists(REF_GPU_LIB):
+        return {"unavailable": "oracle/_ref/libnative_fp2_ref_gpu.so not built"}
+    C, W, nb = layout.padded_copies, layout.n_wires, layout.n_copy_bits
+    table, inputs = host_tables(frame, layout)
+    zero = np.zeros_like(table)
+    gti, i0i, i1i = (np.ascontiguousarray(x, np.int32) for x in (gt, i0, i1))
+    z1r, z1i = np.ascontiguousarray(z1[0]), np.ascontiguousarray(z1[1])
+    z2r, z2i = np.ascontiguousarray(z2[:, 0]), np.ascontiguousarray(z2[:, 1])
+    pr, pim = np.ascontiguousarray(point[:, 0]), np.ascontiguousarray(point[:, 1])
+    out, res = {}, {}
+    for name, path in (("reference", REF_GPU_LIB), ("ours", GPU_LIB)):
+        lib = Fp2Lib(path)
+        lib.init()
+        if lib.cuda_available() != 1:
+            return {"unavailable": name + " library sees no CUDA device"}
+
+        def one():
+            bre, bim = lib.compute_beta(z2r, z2i, (1, 0))
+            sess = run_session(lib, gti, i0i, i1i, z1r, z1i, C, W, table, zero, bre, bim, chal)
+            return sess[:4], lib.mle_eval_base(inputs, pr, pim)
+
+        res[name] = one()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            one()
+        out[name + "_frames_per_s"] = reps / (time.perf_counter() - t0)
+    a, b = res["reference"], res["ours"]
+    out["identical_outputs"] = bool(np.array_equal(a[0][0], b[0][0]) and np.array_equal(a[0][1], b[0][1])
+                                    and np.array_equal(a[0][2], b[0][2]) and a[0][3] == b[0][3] and a[1] == b[1])
+    out["ours_over_reference"] = out["ours_frames_per_s"] / out["reference_frames_per_s"]
+    out["what"] = ("GKR input layer of one 1080p frame through the native_fp2 C ABI (host buffers, %d rounds): "
+                   "the reference's native_fp2.cu (its build.sh recipe, -arch=sm_100a) vs ours" % nb)
+    return out
 
 
 def pinned_frame(a):

@@ -17,6 +17,8 @@ P61 = (1 << 61) - 1
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_LIB = os.path.join(ROOT, "oracle", "liboracle_fp2.so")
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libnative_fp2_ref.so")
+# the reference's GPU library (TruePix-main/native_fp2/native_fp2.cu for sm_100a)
+REF_GPU_LIB = os.path.join(ROOT, "oracle", "_ref", "libnative_fp2_ref_gpu.so")
 GPU_LIB = os.path.join(ROOT, "truepix_b200", "lib", "libnative_fp2_gpu.so")
 
 _U64P = ctypes.POINTER(ctypes.c_uint64)
