@@ -187,8 +187,7 @@ bool batch_load_host(Batch* B, int i, const u64* v_re, const u64* v_im, const u6
     u64* stage_im = (u64*)dev_alloc(sizeof(u64) * vn, s);
     if (!stage_im) return false;
     int launches = 0;
-    bool ok = !cuda_failed(cudaMemcpyAsync(stage_re, v_re, 8 * vn, cudaMemcpyHostToDevice, s), "H2D values") &&
-              !cuda_failed(cudaMemcpyAsync(stage_im, v_im, 8 * vn, cudaMemcpyHostToDevice, s), "H2D values") &&
+    bool ok = host_to_device(stage_re, v_re, 8 * vn, s) && host_to_device(stage_im, v_im, 8 * vn, s) &&
               launch_pack(stage_re, stage_im, vn, f->buf[0], s, &launches);
     const size_t n = (size_t)f->n_copies0;
     u64* bst = reinterpret_cast<u64*>(f->beta[1]);  // 16 B x n: room for both limb arrays

@@ -43,16 +43,8 @@ struct Scratch {
     }
 };
 
-bool h2d(void* d, const void* h, size_t bytes, cudaStream_t s)
-{
-    if (!bytes) return true;
-    return !tp::cuda_failed(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s), "H2D");
-}
-bool d2h(void* h, const void* d, size_t bytes, cudaStream_t s)
-{
-    if (!bytes) return true;
-    return !tp::cuda_failed(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s), "D2H");
-}
+bool h2d(void* d, const void* h, size_t bytes, cudaStream_t s) { return tp::host_to_device(d, h, bytes, s); }
+bool d2h(void* h, const void* d, size_t bytes, cudaStream_t s) { return tp::device_to_host(h, d, bytes, s); }
 bool sync(cudaStream_t s) { return !tp::cuda_failed(cudaStreamSynchronize(s), "synchronize"); }
 
 // NULL is the CUDA default stream, as everywhere in CUDA; callers that mix these

@@ -48,15 +48,13 @@ int host_transform(const uint64_t* in, int coef_len, int order, uint64_t* out, b
     cudaStream_t s = c->stream;
     DevBuf d_in(16 * (size_t)n_in, s), d_out(16 * (size_t)n_out, s);
     if (!d_in.p || !d_out.p) return -1;
-    if (tp::cuda_failed(cudaMemcpyAsync(d_in.p, in, 16 * (size_t)n_in, cudaMemcpyHostToDevice, s), "H2D")) return -1;
+    if (!tp::host_to_device(d_in.p, in, 16 * (size_t)n_in, s)) return -1;
     const ulonglong2* di = static_cast<const ulonglong2*>(d_in.p);
     ulonglong2* dout = static_cast<ulonglong2*>(d_out.p);
     const bool ok = inv ? tp::ntt::inverse(di, coef_len, order, dout, 1, 0, 0, nullptr, s)
                         : tp::ntt::forward(di, coef_len, order, dout, 1, 0, 0, nullptr, s);
     if (!ok) return -1;
-    if (tp::cuda_failed(cudaMemcpyAsync(out, d_out.p, 16 * (size_t)n_out, cudaMemcpyDeviceToHost, s), "D2H"))
-        return -1;
-    return tp::cuda_failed(cudaStreamSynchronize(s), "synchronize") ? -1 : 0;
+    return tp::device_to_host(out, d_out.p, 16 * (size_t)n_out, s) ? 0 : -1;
 }
 
 }  // namespace
@@ -161,17 +159,13 @@ int tp_rs_commit(const uint64_t* src, int log_len, uint64_t* l_eval_out, unsigne
     cudaStream_t s = c->stream;
     DevBuf d_src(16 * (size_t)n, s), d_eval(16 * (size_t)n_eval, s), d_tree(32 * (size_t)n_tree, s);
     if (!d_src.p || !d_eval.p || !d_tree.p) return -1;
-    if (tp::cuda_failed(cudaMemcpyAsync(d_src.p, src, 16 * (size_t)n, cudaMemcpyHostToDevice, s), "H2D")) return -1;
+    if (!tp::host_to_device(d_src.p, src, 16 * (size_t)n, s)) return -1;
     if (!tp::rs::commit(static_cast<const ulonglong2*>(d_src.p), log_len, static_cast<ulonglong2*>(d_eval.p),
                         static_cast<unsigned char*>(d_tree.p), s))
         return -1;
-    if (tp::cuda_failed(cudaMemcpyAsync(tree_out, d_tree.p, 32 * (size_t)n_tree, cudaMemcpyDeviceToHost, s), "D2H"))
-        return -1;
-    if (l_eval_out && tp::cuda_failed(cudaMemcpyAsync(l_eval_out, d_eval.p, 16 * (size_t)n_eval,
-                                                      cudaMemcpyDeviceToHost, s),
-                                      "D2H"))
-        return -1;
-    return tp::cuda_failed(cudaStreamSynchronize(s), "synchronize") ? -1 : 0;
+    if (!tp::device_to_host(tree_out, d_tree.p, 32 * (size_t)n_tree, s)) return -1;
+    if (l_eval_out && !tp::device_to_host(l_eval_out, d_eval.p, 16 * (size_t)n_eval, s)) return -1;
+    return 0;
 }
 
 int tp_virgo_sumcheck_update_dev(const void* d_vma, const void* d_addv, const void* d_ams, long long total_uv,

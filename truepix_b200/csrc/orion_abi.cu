@@ -2,6 +2,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
+
 #include "fp2.cuh"
 #include "orion.h"
 #include "runtime.h"
@@ -53,6 +55,34 @@ bool pixel_layout(const void* d_pixels, int n_copies, int n_copies_padded, int c
     return true;
 }
 
+// *first = min(*first, i) over words w[i] >= p (non-canonical limbs)
+__global__ void __launch_bounds__(256) noncanonical_kernel(const uint64_t* __restrict__ w, long long n,
+                                                           unsigned long long* __restrict__ first)
+{
+    for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
+        if (w[i] >= tp::P61) atomicMin(first, (unsigned long long)i);
+}
+
+// the index of the first non-canonical limb of d_words (n words) or -1; false
+// on a CUDA error. Synchronises s.
+bool first_noncanonical(const void* d_words, long long n, cudaStream_t s, long long* first)
+{
+    DevBuf flag(8, s);
+    if (!flag.p) return false;
+    unsigned long long h = ~0ull;
+    if (tp::cuda_failed(cudaMemsetAsync(flag.p, 0xFF, 8, s), "canonical check")) return false;
+    const tp::Ctx* c = tp::ctx();
+    const long long blocks = std::min<long long>((n + 255) / 256, (long long)c->n_sm * 16);
+    noncanonical_kernel<<<(unsigned)std::max<long long>(1, blocks), 256, 0, s>>>(
+        static_cast<const uint64_t*>(d_words), n, static_cast<unsigned long long*>(flag.p));
+    if (tp::cuda_failed(cudaGetLastError(), "canonical check") ||
+        tp::cuda_failed(cudaMemcpyAsync(&h, flag.p, 8, cudaMemcpyDeviceToHost, s), "D2H") ||
+        tp::cuda_failed(cudaStreamSynchronize(s), "synchronize"))
+        return false;
+    *first = h == ~0ull ? -1 : (long long)h;
+    return true;
+}
+
 // a host-buffer commit of N elements {img, real}: the tree to tree_out, the
 // column-major codeword to codeword_out when it is set
 int commit_host(const uint64_t* src, long long N, unsigned char* tree_out, uint64_t* codeword_out, const char* who)
@@ -64,11 +94,6 @@ int commit_host(const uint64_t* src, long long N, unsigned char* tree_out, uint6
         tp::set_error(tp::TP_ERR_ARG, "%s: null buffer", who);
         return -1;
     }
-    for (long long i = 0; i < 2 * N; ++i)
-        if (src[i] >= tp::P61) {
-            tp::set_error(tp::TP_ERR_ARG, "%s: element %lld is not canonical", who, i / 2);
-            return -1;
-        }
     const long long col_len = N / tp::orion::kColumns;
     const tp::orion::Encoder* e = tp::orion::encoder(col_len);
     if (!e) return -1;
@@ -77,24 +102,24 @@ int commit_host(const uint64_t* src, long long N, unsigned char* tree_out, uint6
     DevBuf d_src(16 * (size_t)N, s), d_rows(16 * (size_t)cw_len * tp::orion::kColumns, s),
         d_tree(64 * (size_t)leaves, s);
     if (!d_src.p || !d_rows.p || !d_tree.p) return -1;
-    if (tp::cuda_failed(cudaMemcpyAsync(d_src.p, src, 16 * (size_t)N, cudaMemcpyHostToDevice, s), "H2D"))
+    if (!tp::host_to_device(d_src.p, src, 16 * (size_t)N, s)) return -1;
+    long long bad = -1;
+    if (!first_noncanonical(d_src.p, 2 * N, s, &bad)) return -1;
+    if (bad >= 0) {
+        tp::set_error(tp::TP_ERR_ARG, "%s: element %lld is not canonical", who, bad / 2);
         return -1;
+    }
     if (!tp::orion::commit(*e, static_cast<const ulonglong2*>(d_src.p), nullptr, static_cast<ulonglong2*>(d_rows.p),
                            static_cast<unsigned char*>(d_tree.p), s))
         return -1;
-    if (tp::cuda_failed(cudaMemcpyAsync(tree_out, d_tree.p, 64 * (size_t)leaves, cudaMemcpyDeviceToHost, s), "D2H"))
-        return -1;
+    if (!tp::device_to_host(tree_out, d_tree.p, 64 * (size_t)leaves, s)) return -1;
     if (codeword_out) {
         DevBuf d_cols(16 * (size_t)cw_len * tp::orion::kColumns, s);
         if (!d_cols.p) return -1;
         if (!tp::orion::rows_to_columns(static_cast<const ulonglong2*>(d_rows.p), cw_len,
                                         static_cast<ulonglong2*>(d_cols.p), s))
             return -1;
-        if (tp::cuda_failed(cudaMemcpyAsync(codeword_out, d_cols.p, 16 * (size_t)cw_len * tp::orion::kColumns,
-                                            cudaMemcpyDeviceToHost, s),
-                            "D2H"))
-            return -1;
-        if (tp::cuda_failed(cudaStreamSynchronize(s), "synchronize")) return -1;
+        if (!tp::device_to_host(codeword_out, d_cols.p, 16 * (size_t)cw_len * tp::orion::kColumns, s)) return -1;
     }
     return tp::cuda_failed(cudaStreamSynchronize(s), "synchronize") ? -1 : 0;
 }

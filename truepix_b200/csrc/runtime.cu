@@ -6,7 +6,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 namespace tp {
@@ -143,6 +145,170 @@ bool upload_async(void* d_dst, const void* h_src, size_t bytes, cudaStream_t s)
         return false;
     g_ring_used[slot] = true;
     return !cuda_failed(cudaEventRecord(g_ring_ev[slot], s), "staging record");
+}
+
+namespace {
+
+// Host threads that copy one buffer in parts (the caller takes parts too).
+// Jobs are serialised by the caller (g_big_mu); the pool lives until exit.
+class CopyPool {
+public:
+    explicit CopyPool(int workers) : n_(workers + 1)
+    {
+        for (int i = 0; i < workers; ++i) th_.emplace_back([this] { loop(); });
+    }
+    void copy(void* dst, const void* src, size_t len)
+    {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            dst_ = static_cast<unsigned char*>(dst);
+            src_ = static_cast<const unsigned char*>(src);
+            len_ = len;
+            parts_ = n_;
+            taken_ = done_ = 0;
+        }
+        work_.notify_all();
+        for (;;) {
+            int part;
+            {
+                std::lock_guard<std::mutex> lk(m_);
+                if (taken_ >= parts_) break;
+                part = taken_++;
+            }
+            run(part);
+        }
+        std::unique_lock<std::mutex> lk(m_);
+        idle_.wait(lk, [this] { return done_ == parts_; });
+        parts_ = taken_ = done_ = 0;
+    }
+
+private:
+    void run(int part)
+    {
+        const size_t step = (len_ + parts_ - 1) / parts_;
+        const size_t lo = std::min(len_, step * part), hi = std::min(len_, lo + step);
+        if (hi > lo) memcpy(dst_ + lo, src_ + lo, hi - lo);
+        std::lock_guard<std::mutex> lk(m_);
+        if (++done_ == parts_) idle_.notify_all();
+    }
+    void loop()
+    {
+        for (;;) {
+            int part;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                work_.wait(lk, [this] { return taken_ < parts_; });
+                part = taken_++;
+            }
+            run(part);
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex m_;
+    std::condition_variable work_, idle_;
+    unsigned char* dst_ = nullptr;
+    const unsigned char* src_ = nullptr;
+    size_t len_ = 0;
+    const int n_;
+    int parts_ = 0, taken_ = 0, done_ = 0;
+};
+
+constexpr size_t kBigChunk = 16u << 20;   // bytes per staging buffer
+constexpr size_t kBigMin = 4u << 20;      // smaller copies go straight to cudaMemcpyAsync
+std::mutex g_big_mu;
+CopyPool* g_copy_pool = nullptr;
+unsigned char* g_big_stage[2] = {nullptr, nullptr};
+cudaEvent_t g_big_ev[2];
+bool g_big_used[2] = {false, false};
+
+bool host_pinned(const void* h)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// under g_big_mu
+bool big_init()
+{
+    if (g_copy_pool) return true;
+    for (int b = 0; b < 2; ++b) {
+        if (cuda_failed(cudaHostAlloc((void**)&g_big_stage[b], kBigChunk, cudaHostAllocDefault), "pinned staging"))
+            return false;
+        if (cuda_failed(cudaEventCreateWithFlags(&g_big_ev[b], cudaEventDisableTiming), "staging event"))
+            return false;
+    }
+    const unsigned hc = std::thread::hardware_concurrency();
+    g_copy_pool = new CopyPool((int)std::min(7u, std::max(1u, hc / 2)));
+    return true;
+}
+
+bool big_wait(int b)
+{
+    if (!g_big_used[b]) return true;
+    g_big_used[b] = false;
+    return !cuda_failed(cudaEventSynchronize(g_big_ev[b]), "staging wait");
+}
+
+}  // namespace
+
+bool host_to_device(void* d_dst, const void* h_src, size_t bytes, cudaStream_t s)
+{
+    if (bytes == 0) return true;
+    if (bytes < kBigMin || host_pinned(h_src))
+        return !cuda_failed(cudaMemcpyAsync(d_dst, h_src, bytes, cudaMemcpyHostToDevice, s), "H2D");
+    std::lock_guard<std::mutex> lock(g_big_mu);
+    if (!big_init()) return false;
+    const unsigned char* h = static_cast<const unsigned char*>(h_src);
+    unsigned char* d = static_cast<unsigned char*>(d_dst);
+    for (size_t off = 0, k = 0; off < bytes; off += kBigChunk, ++k) {
+        const int b = (int)(k & 1);
+        const size_t len = std::min(kBigChunk, bytes - off);
+        if (!big_wait(b)) return false;
+        g_copy_pool->copy(g_big_stage[b], h + off, len);
+        if (cuda_failed(cudaMemcpyAsync(d + off, g_big_stage[b], len, cudaMemcpyHostToDevice, s), "H2D") ||
+            cuda_failed(cudaEventRecord(g_big_ev[b], s), "staging record"))
+            return false;
+        g_big_used[b] = true;
+    }
+    return true;
+}
+
+bool device_to_host(void* h_dst, const void* d_src, size_t bytes, cudaStream_t s)
+{
+    if (bytes == 0) return true;
+    if (bytes < kBigMin || host_pinned(h_dst)) {
+        return !cuda_failed(cudaMemcpyAsync(h_dst, d_src, bytes, cudaMemcpyDeviceToHost, s), "D2H") &&
+               !cuda_failed(cudaStreamSynchronize(s), "synchronize");
+    }
+    std::lock_guard<std::mutex> lock(g_big_mu);
+    if (!big_init()) return false;
+    unsigned char* h = static_cast<unsigned char*>(h_dst);
+    const unsigned char* d = static_cast<const unsigned char*>(d_src);
+    const size_t n_chunks = (bytes + kBigChunk - 1) / kBigChunk;
+    // chunk k goes to staging k & 1; chunk k + 1 is in flight while chunk k is copied out
+    auto issue = [&](size_t k) {
+        const int b = (int)(k & 1);
+        const size_t off = k * kBigChunk, len = std::min(kBigChunk, bytes - off);
+        if (!big_wait(b)) return false;
+        if (cuda_failed(cudaMemcpyAsync(g_big_stage[b], d + off, len, cudaMemcpyDeviceToHost, s), "D2H") ||
+            cuda_failed(cudaEventRecord(g_big_ev[b], s), "staging record"))
+            return false;
+        g_big_used[b] = true;
+        return true;
+    };
+    if (!issue(0)) return false;
+    for (size_t k = 0; k < n_chunks; ++k) {
+        if (k + 1 < n_chunks && !issue(k + 1)) return false;
+        const int b = (int)(k & 1);
+        if (!big_wait(b)) return false;
+        const size_t off = k * kBigChunk, len = std::min(kBigChunk, bytes - off);
+        g_copy_pool->copy(h + off, g_big_stage[b], len);
+    }
+    return true;
 }
 
 namespace {

@@ -38,6 +38,15 @@ void dev_free(void* p, cudaStream_t s);
 // uploads are copied synchronously.
 bool upload_async(void* d_dst, const void* h_src, size_t bytes, cudaStream_t s);
 
+// Large copies between caller-owned host buffers and the device. A pinned host
+// buffer is copied directly; a pageable one of 4 MB or more goes through two
+// 16 MB pinned staging buffers filled (or drained) by several host threads while
+// the other buffer's DMA runs. host_to_device returns once the host buffer has
+// been read (the device copy completes in stream order on s); device_to_host
+// returns once the host buffer holds the data (it synchronises s).
+bool host_to_device(void* d_dst, const void* h_src, size_t bytes, cudaStream_t s);
+bool device_to_host(void* h_dst, const void* d_src, size_t bytes, cudaStream_t s);
+
 // Kernel timer: when enabled, kernels that support it record a CUDA event pair
 // around their launch with an integer tag; read back after synchronising.
 bool timer_enable(int max_pairs);
