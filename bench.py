@@ -1111,6 +1111,16 @@ def reference_gpu_lib(frame, layout, gt, i0, i1, z1, z2, point, chal, reps=3):
     return out
 
 
+def release(srv):
+    """Free a server's device memory before the next measurement (outside it)."""
+    import gc
+    import torch
+    srv.close()
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+
 def pinned_frame(a):
     """A frame as the serving loop takes it from a decoder: pinned host memory
     (copied straight to the device, no staging copy on the host)."""
@@ -1145,14 +1155,16 @@ def batched_uneven(seed=4):
         reqs.append(Request(i, gray, ch, cw, pinned_frame(rng.integers(0, 256, size=ch * cw * 3, dtype=np.uint8)),
                             seed=9000 + i, arrival=0.0))
     srv = ProofServer(slots=64, hbm_budget=80e9)
-    srv.run(reqs[:8], realtime=False)              # warm-up (graphs, twiddles, pools)
+    srv.run(reqs, realtime=False)                  # warm-up: every size's expander graphs, pools
     res = srv.run(reqs, realtime=False)
     st = latency_stats(res)
+    ticks = srv.ticks
+    release(srv)
     wires = sorted(1 << (9 + int(np.log2(max(2, 1 << int(np.ceil(np.log2(max(2, -(-r.height * r.width * 3 // 384)))))))))
                    for r in reqs)
     return {"workload": "64 crop-then-gray frames, sources 240p-1080p, seeded crops", "frames": len(res),
             "frames_per_s": st.get("frames_per_s"), "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"),
-            "input_wires_min": wires[0], "input_wires_max": wires[-1], "ticks": srv.ticks,
+            "input_wires_min": wires[0], "input_wires_max": wires[-1], "ticks": ticks,
             "what": "GKR early rounds + MLE + Orion commit per frame, continuous batch of 64 slots"}
 
 
@@ -1168,9 +1180,7 @@ def serving_sweep(rates=(100, 250, 500, 1000), n_req=192, seed=5):
               for hw in sizes}
     srv = ProofServer(slots=64, hbm_budget=60e9)
     out = []
-    warm = [Request(k, cs["gray"], *sizes[k % len(sizes)], frames[sizes[k % len(sizes)]][0], seed=k)
-            for k in range(len(sizes))]
-    srv.run(warm, realtime=False)
+    runs = []
     for lam in rates:
         t = 0.0
         reqs = []
@@ -1179,10 +1189,16 @@ def serving_sweep(rates=(100, 250, 500, 1000), n_req=192, seed=5):
             hw = sizes[int(rng.integers(len(sizes)))]
             op = ["gray", "crop", "mask"][int(rng.integers(3))]
             reqs.append(Request(i, cs[op], hw[0], hw[1], frames[hw][i % 2], seed=77 + i, arrival=t))
+        runs.append((lam, reqs))
+    # warm-up: one rate's requests all at once (every size's graphs, the pools
+    # grown to a full batch's footprint)
+    srv.run(runs[-1][1], realtime=False)
+    for lam, reqs in runs:
         res = srv.run(reqs, realtime=True)
         st = latency_stats(res)
         st["lambda_per_s"] = lam
         out.append(st)
+    release(srv)
     return {"workload": "Poisson requests, ops gray/crop/mask uniform, 360p-2160p uniform, %d per rate, "
                         "frames in pinned host memory" % n_req,
             "slots": 64, "hbm_budget_gb": 60, "by_rate": out}

@@ -196,11 +196,20 @@ class ProofServer:
         self._t0 = time.perf_counter()
         self._out = []
 
+    def close(self):
+        """Release the batch and the server's device buffers now (freeing device
+        memory synchronises the device, so a server that is dropped inside
+        another one's run would stall it)."""
+        if getattr(self, "batch", None):
+            self.torch.cuda.synchronize(self.dev)
+            self.lib.tp_batch_destroy(self.batch)
+            self.batch = None
+        self.slot_bufs = self.commit_free = self.staging = []
+        self.active, self.committing = {}, []
+
     def __del__(self):
         try:
-            if self.batch:
-                self.lib.tp_batch_destroy(self.batch)
-                self.batch = None
+            self.close()
         except Exception:
             pass
 
