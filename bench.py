@@ -1192,7 +1192,8 @@ def serving_sweep(rates=(100, 250, 500, 1000), n_req=192, seed=5):
         runs.append((lam, reqs))
     # warm-up: one rate's requests all at once (every size's graphs, the pools
     # grown to a full batch's footprint)
-    srv.run(runs[-1][1], realtime=False)
+    import dataclasses
+    srv.run([dataclasses.replace(r) for r in runs[-1][1]], realtime=False)
     for lam, reqs in runs:
         res = srv.run(reqs, realtime=True)
         st = latency_stats(res)
