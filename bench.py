@@ -836,6 +836,16 @@ def _cpu_opening(job):
         ret = np.zeros(6, np.uint64)
         lib.ref_virgo_update(1, V(vma.ctypes.data), V(addv.ctypes.data), V(ams.ctypes.data), size,
                              V(r.ctypes.data), 1, *[V(o.ctypes.data) for o in outs], V(ret.ctypes.data))
+    elif kind == "vinit":
+        from orionlib import virgo_layer
+        phase, lg, lu = size
+        L = virgo_layer(71, lg, lu)
+        lib.ref_virgo_init.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [V] * 17
+        outs = [np.zeros(4 << lu, np.uint64) for _ in range(3)]
+        vp = lambda a: V(a.ctypes.data)
+        lib.ref_virgo_init(phase, lg, lu, vp(L["ty"]), vp(L["u"]), vp(L["v"]), vp(L["comb_ptr"]), vp(L["comb_src"]),
+                           vp(L["comb_w"]), vp(L["values"]), vp(L["r0"]), vp(L["r1"]), vp(L["alpha"]),
+                           vp(L["beta"]), vp(L["vma0"]), vp(L["prev_r"]), vp(L["r_u"]), *[vp(o) for o in outs])
     else:
         lib.ref_fri_step.argtypes = [V, ctypes.c_int, V, V, V]
         w = elements(5, (1 << size) * 64)
@@ -914,6 +924,31 @@ def opening_bench(args, lib, committer, layout, dev, stream, sha_gcs, reps=5):
     out["virgo_update"] = {"ms": ms, "total_uv": n_v, "roofline": roof((192 + 96) * (n_v // 2), ms)}
     del vma, addv, ams, vouts
 
+    # Virgo layer inits: 2^20 gates of every kind over 2^20 values
+    from orionlib import virgo_layer
+    import ctypes
+    lgv = 20
+    L = virgo_layer(71, lgv, lgv)
+    vp = lambda a: ctypes.c_void_p(a.ctypes.data)
+    h = lib.tp_virgo_layer_create(lgv, lgv, vp(L["ty"]), vp(L["u"]), vp(L["v"]), vp(L["comb_ptr"]),
+                                  vp(L["comb_src"]), vp(L["comb_w"]))
+    if not h:
+        native.check(lib, -1, "virgo layer")
+    vals = dt(L["values"])
+    vouts = [torch.empty(4 << lgv, dtype=torch.int64, device=dev) for _ in range(3)]
+    vma0 = dt(L["vma0"])
+    ms1 = timed(lambda: native.check(lib, lib.tp_virgo_phase1_init_dev(
+        h, vals.data_ptr(), vp(L["r0"]), vp(L["r1"]), vp(L["alpha"]), vp(L["beta"]),
+        *[o.data_ptr() for o in vouts], s), "virgo phase1 init"))
+    ms2 = timed(lambda: native.check(lib, lib.tp_virgo_phase2_init_dev(
+        h, vals.data_ptr(), vp(L["r0"]), vp(L["r1"]), vp(L["alpha"]), vp(L["beta"]), vma0.data_ptr(),
+        vp(L["prev_r"]), vp(L["r_u"]), *[o.data_ptr() for o in vouts], s), "virgo phase2 init"))
+    lib.tp_virgo_layer_destroy(h)
+    out["virgo_inits"] = {"phase1_ms": ms1, "phase2_ms": ms2, "gates": 1 << lgv, "values": 1 << lgv,
+                          "what": "sumcheck_phase1_init / phase2_init of a seeded layer with every gate kind "
+                                  "(tests/orionlib.py virgo_layer), tables written to HBM"}
+    del vals, vouts, vma0
+
     lm = 18
     w = dt(elements(5, (1 << lm) * 64))
     nxt = torch.empty(w.numel() // 2, dtype=torch.int64, device=dev)
@@ -930,16 +965,21 @@ def opening_bench(args, lib, committer, layout, dev, stream, sha_gcs, reps=5):
 
     if not args.skip_cpu:
         import multiprocessing as mp
-        jobs = [("combine", N), ("virgo", n_v), ("fri", lm)]
+        jobs = [("combine", N), ("virgo", n_v), ("fri", lm), ("vinit", (1, lgv, lgv)), ("vinit", (2, lgv, lgv))]
         with mp.get_context("spawn").Pool(1, maxtasksperchild=1) as pool:
             secs = pool.map(_cpu_opening, jobs, chunksize=1)
-        for (kind, _), sec, key in zip(jobs, secs, ("combine_with_tree", "virgo_update", "fri_step")):
+        for (kind, _), sec, key in zip(jobs[:3], secs[:3], ("combine_with_tree", "virgo_update", "fri_step")):
             if sec is not None:
                 out[key]["cpu_reference_ms"] = 1e3 * sec
                 out[key]["speedup_vs_cpu_reference"] = 1e3 * sec / out[key]["ms"]
+        if secs[3] is not None and secs[4] is not None:
+            vi = out["virgo_inits"]
+            vi["cpu_reference_phase1_ms"], vi["cpu_reference_phase2_ms"] = 1e3 * secs[3], 1e3 * secs[4]
+            vi["speedup_vs_cpu_reference"] = (secs[3] + secs[4]) * 1e3 / (vi["phase1_ms"] + vi["phase2_ms"])
         out["cpu_note"] = ("reference sources (oracle/_ref/liborion_ref.so) on one core, same sizes: "
                            "combine + leaves + tree of a 2^23-element commit, phase-1 update of 2^22 "
-                           "entries, FRI step of 2^18 x 64 elements")
+                           "entries, FRI step of 2^18 x 64 elements, phase-1 / phase-2 inits of the 2^20-gate "
+                           "layer")
     return out
 
 

@@ -195,6 +195,34 @@ int tp_virgo_sumcheck_update_dev(const void* d_vma, const void* d_addv, const vo
                                  uint64_t r_real, uint64_t r_imag, int current_bit, void* d_vma_out,
                                  void* d_addv_out, void* d_ams_out, void* d_ret, void* stream);
 
+/* Layer inits of the Virgo sumcheck: zk_prover::sumcheck_phase1_init and
+ * sumcheck_phase2_init (prover.cpp:246-570, 645-930) for layer
+ * sumcheck_layer_id of a layered circuit. The layer is given once: 2^length_g
+ * gates (ty[g], u[g], v[g] as in circuit_fast_track.h's gate; type-14 gates take
+ * the (src, weight) pairs comb_src / comb_w[comb_ptr[g] .. comb_ptr[g + 1]),
+ * weights {img, real}; comb_* may be NULL without type-14 gates) over a previous
+ * layer of 2^length_u values. Indices outside the layer are rejected (NULL);
+ * unknown gate types contribute nothing, as in the reference. */
+void* tp_virgo_layer_create(int length_g, int length_u, const int* ty, const long long* u, const long long* v,
+                            const int* comb_ptr, const int* comb_src, const uint64_t* comb_w);
+void tp_virgo_layer_destroy(void* layer);
+
+/* Phase 1: d_values = circuit_value[layer - 1] (2^length_u elements, device);
+ * r0, r1: length_g host elements, alpha, beta: one each (sumcheck_init's
+ * arguments). Writes the linear_poly tables V_mult_add, addV_array,
+ * add_mult_sum (2^length_u entries of 32 bytes each, device) that
+ * tp_virgo_sumcheck_update_dev folds. */
+int tp_virgo_phase1_init_dev(void* layer, const void* d_values, const uint64_t* r0, const uint64_t* r1,
+                             const uint64_t* alpha, const uint64_t* beta, void* d_vma, void* d_addv, void* d_ams,
+                             void* stream);
+
+/* Phase 2: as phase 1 plus d_vma0 (device: the one-entry V_mult_add that phase
+ * 1's rounds leave, whose value at prev_r is v_u), prev_r (one host element)
+ * and r_u (length_u host elements). */
+int tp_virgo_phase2_init_dev(void* layer, const void* d_values, const uint64_t* r0, const uint64_t* r1,
+                             const uint64_t* alpha, const uint64_t* beta, const void* d_vma0, const uint64_t* prev_r,
+                             const uint64_t* r_u, void* d_vma, void* d_addv, void* d_ams, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -639,3 +639,154 @@ int oracle_frame_vector(const unsigned char* pix, int copies, int padded, int cs
     }
     return 0;
 }
+
+/* ---- Virgo layer inits (zk_prover::sumcheck_phase1_init, prover.cpp:246-570;
+ * sumcheck_phase2_init, prover.cpp:645-930) ----
+ * A layer of n_gates = 2^length_g gates (type ty, inputs u, v; type 14 gates
+ * carry (src, weight) lists comb_src/comb_w[comb_ptr[g] .. comb_ptr[g+1])) over a
+ * previous layer of total_uv = 2^length_u values. Tables are linear_poly arrays
+ * {a, b} of total_uv entries. tmp_g(i) = alpha eq(r0, i) + beta eq(r1, i), eq with
+ * bit k of i <-> r[k]. Unknown gate types contribute nothing (the reference
+ * prints a warning and skips them). Returns -1 on an index outside its range. */
+static fe fe_of(const u64* p) { fe x = {p[0], p[1]}; return x; }
+static void put_lp(u64* t, long long i, fe a, fe b) { t[4 * i] = a.img; t[4 * i + 1] = a.real; t[4 * i + 2] = b.img; t[4 * i + 3] = b.real; }
+static fe fesub(fe a, fe b) { fe r = {fadd(a.img, canon(P61 - b.img)), fadd(a.real, canon(P61 - b.real))}; return r; }
+
+static fe eq_at(const u64* r, int len, long long i, fe s)
+{
+    const fe one = {0, 1};
+    for (int k = 0; k < len; ++k) s = femul(s, ((i >> k) & 1) ? fe_of(r + 2 * k) : fesub(one, fe_of(r + 2 * k)));
+    return s;
+}
+
+static int virgo_layer_ok(long long n_gates, const int* ty, const long long* u, const long long* v, const int* comb_ptr,
+                          const int* comb_src, int length_g, int length_u)
+{
+    const long long G = 1LL << length_g, U = 1LL << length_u;
+    if (n_gates != G) return 0;
+    for (long long g = 0; g < G; ++g) {
+        switch (ty[g]) {
+        case 0: case 1: case 6: case 7: case 8: case 9: case 10: case 13:
+            if (u[g] < 0 || u[g] >= U || v[g] < 0 || v[g] >= U) return 0;
+            break;
+        case 4:   /* u indexes both the gate randoms and the table */
+            if (u[g] < 0 || u[g] >= G || u[g] >= U || v[g] < 0 || v[g] >= U) return 0;
+            break;
+        case 5:
+            if (u[g] < 0 || v[g] > U || u[g] > v[g]) return 0;
+            break;
+        case 12:
+            if (u[g] < 0 || v[g] >= U || u[g] > v[g] + 1) return 0;
+            break;
+        case 14:
+            if (!comb_ptr) return 0;
+            for (int k = comb_ptr[g]; k < comb_ptr[g + 1]; ++k)
+                if (comb_src[k] < 0 || comb_src[k] >= U) return 0;
+            break;
+        default:
+            break;
+        }
+    }
+    return 1;
+}
+
+int oracle_virgo_phase1_init(long long n_gates, const int* ty, const long long* u, const long long* v, const int* comb_ptr,
+                             const int* comb_src, const u64* comb_w, int length_g, int length_u, const u64* values,
+                             const u64* r0, const u64* r1, const u64* alpha, const u64* beta, u64* vma, u64* addv,
+                             u64* ams)
+{
+    if (!virgo_layer_ok(n_gates, ty, u, v, comb_ptr, comb_src, length_g, length_u)) return -1;
+    const long long U = 1LL << length_u;
+    const fe zero = {0, 0};
+    fe* A = (fe*)calloc((size_t)U, sizeof(fe));   /* addV_array[.].b */
+    fe* M = (fe*)calloc((size_t)U, sizeof(fe));   /* add_mult_sum[.].b */
+    if (!A || !M) { free(A); free(M); return -1; }
+    const fe al = fe_of(alpha), be = fe_of(beta);
+    for (long long g = 0; g < n_gates; ++g) {
+        const int t = ty[g];
+        if (t == 2) continue;
+        const long long at = t == 4 ? u[g] : g;
+        const fe tmp = feadd(eq_at(r0, length_g, at, al), eq_at(r1, length_g, at, be));
+        const long long uu = u[g];
+        switch (t) {
+        case 0: { const fe tv = femul(fe_of(values + 2 * v[g]), tmp); A[uu] = feadd(A[uu], tv); M[uu] = feadd(M[uu], tmp); break; }
+        case 1: { M[uu] = feadd(M[uu], femul(fe_of(values + 2 * v[g]), tmp)); break; }
+        case 4: { M[uu] = feadd(M[uu], tmp); break; }
+        case 5: for (long long j = uu; j < v[g]; ++j) M[j] = feadd(M[j], tmp); break;
+        case 12: { fe x = tmp; for (long long j = uu; j <= v[g]; ++j) { M[j] = feadd(M[j], x); x = feadd(x, x); } break; }
+        case 14:
+            for (int k = comb_ptr[g]; k < comb_ptr[g + 1]; ++k)
+                M[comb_src[k]] = feadd(M[comb_src[k]], femul(fe_of(comb_w + 2 * k), tmp));
+            break;
+        case 6: { M[uu] = fesub(M[uu], tmp); A[uu] = feadd(A[uu], tmp); break; }
+        case 7: { const fe tv = femul(fe_of(values + 2 * v[g]), tmp); A[uu] = fesub(A[uu], tv); M[uu] = feadd(M[uu], tmp); break; }
+        case 8: { const fe tv = femul(tmp, fe_of(values + 2 * v[g])); A[uu] = feadd(A[uu], tv); M[uu] = fesub(fesub(feadd(M[uu], tmp), tv), tv); break; }
+        case 13: { const fe tv = femul(tmp, fe_of(values + 2 * v[g])); M[uu] = feadd(fesub(M[uu], tv), tmp); break; }
+        case 9: { const fe tv = femul(tmp, fe_of(values + 2 * v[g])); A[uu] = feadd(A[uu], tv); M[uu] = fesub(M[uu], tv); break; }
+        case 10: { M[uu] = feadd(M[uu], tmp); break; }
+        default: break;
+        }
+    }
+    for (long long i = 0; i < U; ++i) {
+        put_lp(vma, i, zero, fe_of(values + 2 * i));
+        put_lp(addv, i, zero, A[i]);
+        put_lp(ams, i, zero, M[i]);
+    }
+    free(A);
+    free(M);
+    return 0;
+}
+
+int oracle_virgo_phase2_init(long long n_gates, const int* ty, const long long* u, const long long* v, const int* comb_ptr,
+                             const int* comb_src, const u64* comb_w, int length_g, int length_u, const u64* values,
+                             const u64* r0, const u64* r1, const u64* alpha, const u64* beta, const u64* vma0,
+                             const u64* prev_r, const u64* r_u, u64* vma, u64* addv, u64* ams)
+{
+    if (!virgo_layer_ok(n_gates, ty, u, v, comb_ptr, comb_src, length_g, length_u)) return -1;
+    const long long U = 1LL << length_u;
+    const fe zero = {0, 0}, one = {0, 1};
+    fe* A = (fe*)calloc((size_t)U, sizeof(fe));
+    fe* M = (fe*)calloc((size_t)U, sizeof(fe));
+    if (!A || !M) { free(A); free(M); return -1; }
+    const fe al = fe_of(alpha), be = fe_of(beta);
+    const fe v_u = feadd(femul(fe_of(vma0), fe_of(prev_r)), fe_of(vma0 + 2));
+    for (long long g = 0; g < n_gates; ++g) {
+        const int t = ty[g];
+        if (t == 2 || t == 4) continue;
+        const fe tg = feadd(eq_at(r0, length_g, g, al), eq_at(r1, length_g, g, be));
+        const long long vv = v[g];
+        if (t == 5 || t == 12 || t == 14) {
+            fe x = femul(tg, v_u);
+            if (t == 5) {
+                for (long long j = u[g]; j < vv; ++j) A[0] = feadd(A[0], femul(x, eq_at(r_u, length_u, j, one)));
+            } else if (t == 12) {
+                for (long long j = u[g]; j <= vv; ++j) { A[0] = feadd(A[0], femul(x, eq_at(r_u, length_u, j, one))); x = feadd(x, x); }
+            } else {
+                for (int k = comb_ptr[g]; k < comb_ptr[g + 1]; ++k)
+                    A[0] = feadd(A[0], femul(femul(x, eq_at(r_u, length_u, comb_src[k], one)), fe_of(comb_w + 2 * k)));
+            }
+            continue;
+        }
+        const fe tgu = femul(tg, eq_at(r_u, length_u, u[g], one));
+        const fe tv = femul(tgu, v_u);
+        switch (t) {
+        case 1: M[vv] = feadd(M[vv], tv); break;
+        case 0: M[vv] = feadd(M[vv], tgu); A[vv] = feadd(A[vv], tv); break;
+        case 6: A[vv] = feadd(A[vv], fesub(tgu, tv)); break;
+        case 7: M[vv] = fesub(M[vv], tgu); A[vv] = feadd(A[vv], tv); break;
+        case 8: M[vv] = feadd(M[vv], fesub(fesub(tgu, tv), tv)); A[vv] = feadd(A[vv], tv); break;
+        case 13: M[vv] = fesub(M[vv], tv); A[vv] = feadd(A[vv], tv); break;
+        case 9: M[vv] = feadd(M[vv], fesub(tgu, tv)); break;
+        case 10: A[vv] = feadd(A[vv], tv); break;
+        default: break;
+        }
+    }
+    for (long long i = 0; i < U; ++i) {
+        put_lp(vma, i, zero, fe_of(values + 2 * i));
+        put_lp(addv, i, zero, A[i]);
+        put_lp(ams, i, zero, M[i]);
+    }
+    free(A);
+    free(M);
+    return 0;
+}

@@ -24,14 +24,15 @@
 extern prime_field::field_element** encoded_codeword;
 
 namespace {
-double g_seconds = 0;   // duration of the reference work of the last ref_combine / ref_virgo_update / ref_fri_step
+double g_seconds = 0;   // duration of the reference work of the last timed call
 double now() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
 }  // namespace
 
 extern "C" {
 
 // seconds the reference's own work took in the last ref_combine (the passes
-// after commit()), ref_virgo_update (the update call) or ref_fri_step (the step)
+// after commit()), ref_virgo_update (the update call), ref_fri_step (the step)
+// or ref_virgo_init (the init call of the requested phase)
 double ref_last_seconds(void) { return g_seconds; }
 
 // SHA-256 of one 64-byte block exactly as Orion hashes it (my_hhash)
@@ -215,6 +216,91 @@ void ref_fri_step(const uint64_t* witness, int log_m, const uint64_t* r, uint64_
     g_seconds = now() - t0;
     memcpy(root32, &h, 32);
     memcpy(next, fri::cpd.rs_codeword[1], 16 * (size_t)(M / 2) * slice_number);
+}
+
+// zk_prover::sumcheck_phase1_init (phase 1) or sumcheck_phase2_init (phase 2;
+// src/linear_gkr/prover.cpp:246-570, 645-930) of layer 1 of a two-layer circuit:
+// layer 1 has 2^length_g gates (ty, u, v; type-14 gates take (src, weight)
+// lists comb_src / comb_w[comb_ptr[g] .. comb_ptr[g + 1])), layer 0 holds the
+// 2^length_u values. r0, r1: length_g elements; alpha, beta: one each. Phase 2
+// runs phase 1's init first (its beta tables), sets V_mult_add[0] to the
+// linear_poly vma0 = {a, b} (the table phase 1's rounds leave) and calls
+// sumcheck_phase2_init(prev_r, r_u, 1 - r_u), r_u of length_u elements. Writes
+// the three linear_poly tables (2^length_u entries {a, b}). Call once per process.
+void ref_virgo_init(int phase, int length_g, int length_u, const int* ty, const long long* u, const long long* v,
+                    const int* comb_ptr, const int* comb_src, const uint64_t* comb_w, const uint64_t* values,
+                    const uint64_t* r0, const uint64_t* r1, const uint64_t* alpha, const uint64_t* beta,
+                    const uint64_t* vma0, const uint64_t* prev_r, const uint64_t* r_u, uint64_t* vma_out,
+                    uint64_t* addv_out, uint64_t* ams_out)
+{
+    typedef prime_field::field_element F;
+    prime_field::init();
+    const long long G = 1LL << length_g, U = 1LL << length_u;
+    layered_circuit* C = new layered_circuit();
+    C->total_depth = 2;
+    C->circuit = new layer[2];
+    C->circuit[0].bit_length = length_u;
+    C->circuit[1].bit_length = length_g;
+    C->circuit[1].gates = new gate[G];
+    for (long long g = 0; g < G; ++g) {
+        gate& q = C->circuit[1].gates[g];
+        q.ty = ty[g];
+        q.u = u[g];
+        q.v = v[g];
+        if (ty[g] == 14 && comb_ptr) {
+            const int n = comb_ptr[g + 1] - comb_ptr[g];
+            q.parameter_length = n;
+            q.src = new int[n > 0 ? n : 1];
+            q.weight = new F[n > 0 ? n : 1];
+            for (int k = 0; k < n; ++k) {
+                q.src[k] = comb_src[comb_ptr[g] + k];
+                memcpy(&q.weight[k], comb_w + 2 * (comb_ptr[g] + k), 16);
+            }
+        }
+    }
+    zk_prover* p = new zk_prover();
+    p->init_array(length_g > length_u ? length_g : length_u);
+    p->C = C;
+    p->circuit_value[0] = new F[U];
+    memcpy(p->circuit_value[0], values, 16 * (size_t)U);
+    F* R0 = new F[length_g + 1];
+    F* R1 = new F[length_g + 1];
+    F* O0 = new F[length_g + 1];
+    F* O1 = new F[length_g + 1];
+    const F one(1ULL);
+    for (int k = 0; k < length_g; ++k) {
+        memcpy(&R0[k], r0 + 2 * k, 16);
+        memcpy(&R1[k], r1 + 2 * k, 16);
+        O0[k] = one - R0[k];
+        O1[k] = one - R1[k];
+    }
+    F al, be;
+    memcpy(&al, alpha, 16);
+    memcpy(&be, beta, 16);
+    p->sumcheck_init(1, length_g, length_u, length_u, al, be, R0, R1, O0, O1);
+    const double t0 = now();
+    p->sumcheck_phase1_init();
+    if (phase == 2) {
+        F a, b, pr;
+        memcpy(&a, vma0, 16);
+        memcpy(&b, vma0 + 2, 16);
+        memcpy(&pr, prev_r, 16);
+        p->V_mult_add[0] = linear_poly(a, b);
+        F* RU = new F[length_u + 1];
+        F* OU = new F[length_u + 1];
+        for (int k = 0; k < length_u; ++k) {
+            memcpy(&RU[k], r_u + 2 * k, 16);
+            OU[k] = one - RU[k];
+        }
+        const double t1 = now();
+        p->sumcheck_phase2_init(pr, RU, OU);
+        g_seconds = now() - t1;
+    } else {
+        g_seconds = now() - t0;
+    }
+    memcpy(vma_out, p->V_mult_add, 32 * (size_t)U);
+    memcpy(addv_out, p->addV_array, 32 * (size_t)U);
+    memcpy(ams_out, p->add_mult_sum, 32 * (size_t)U);
 }
 
 // encoded length of a column of n elements (graphs generated from the default seed)

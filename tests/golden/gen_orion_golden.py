@@ -30,6 +30,13 @@ and, from the zero-knowledge tree (TruePix-main/Orion/Orion_zk, built into
 oracle/_ref/liborion_zk_ref.so with oracle/orion_zk_ref_harness.cpp), in
 tests/golden/orion_zk_golden.npz:
 
+and, in tests/golden/virgo_init_golden.npz (from oracle/_ref/liborion_ref.so):
+
+  vinit*_<p>_<seed>  zk_prover::sumcheck_phase<p>_init (prover.cpp:246-570,
+                  645-930) of a seeded layer (tests/orionlib.py virgo_layer: every
+                  gate type, 2^length_g gates over 2^length_u values): digests
+                  of V_mult_add, addV_array, add_mult_sum
+
   zk*_<case>      the commit phase of linearPC_multi_commit_zk on a seeded frame
                   (examples/multivariate_PC_test_commit.cpp:280-340): masked and
                   mask Merkle roots of commit_pair (linearPC.cpp:253-460) and the
@@ -41,6 +48,7 @@ global scratch state sized by its first call.
 Run here (needs the reference checkout and `make -C oracle ref`):
     python tests/golden/gen_orion_golden.py          # both files
     python tests/golden/gen_orion_golden.py zk       # the ZK file only
+    python tests/golden/gen_orion_golden.py vinit    # the Virgo init file only
 """
 from __future__ import annotations
 
@@ -53,7 +61,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
-from orionlib import (ORION_REF_LIB, ORION_ZK_REF_LIB, digest, elements, frame_bytes, frame_elements,  # noqa: E402
+from orionlib import (ORION_REF_LIB, ORION_ZK_REF_LIB, digest, virgo_layer, elements, frame_bytes, frame_elements,  # noqa: E402
                       virgo_inputs)
 
 V = ctypes.c_void_p
@@ -196,6 +204,36 @@ def _zk(case):
     return ra.raw, rb.raw, ha.value, digest(mask)
 
 
+# (phase, seed, length_g, length_u)
+VINIT_CASES = [(1, 1, 1, 1), (2, 1, 1, 1), (1, 2, 4, 4), (2, 3, 4, 4), (1, 4, 8, 6), (2, 5, 8, 6), (1, 6, 6, 10),
+               (2, 7, 6, 10), (1, 8, 12, 12), (2, 9, 12, 12), (1, 10, 16, 14), (2, 11, 16, 14)]
+
+
+def _vinit(case):
+    phase, seed, lg, lu = case
+    L = virgo_layer(seed, lg, lu)
+    lib = ctypes.CDLL(ORION_REF_LIB)
+    lib.ref_virgo_init.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [V] * 17
+    outs = [np.zeros(4 << lu, np.uint64) for _ in range(3)]
+    vp = lambda a: V(a.ctypes.data)
+    lib.ref_virgo_init(phase, lg, lu, vp(L["ty"]), vp(L["u"]), vp(L["v"]), vp(L["comb_ptr"]), vp(L["comb_src"]),
+                       vp(L["comb_w"]), vp(L["values"]), vp(L["r0"]), vp(L["r1"]), vp(L["alpha"]), vp(L["beta"]),
+                       vp(L["vma0"]), vp(L["prev_r"]), vp(L["r_u"]), *[vp(o) for o in outs])
+    return b"".join(digest(o) for o in outs)
+
+
+def main_vinit():
+    ctx = mp.get_context("spawn")
+    out = {}
+    with ctx.Pool(8, maxtasksperchild=1) as pool:
+        for case, d in zip(VINIT_CASES, pool.map(_vinit, VINIT_CASES, chunksize=1)):
+            key = "%d_%d" % (case[0], case[1])
+            out["vinitcase_" + key] = np.array(case, np.int64)
+            out["vinit_" + key] = np.frombuffer(d, np.uint8)
+    np.savez_compressed(os.path.join(HERE, "virgo_init_golden.npz"), **out)
+    print("wrote", len(out), "arrays")
+
+
 def main_zk():
     ctx = mp.get_context("spawn")
     out = {}
@@ -256,6 +294,10 @@ def main():
 
 
 if __name__ == "__main__":
-    if sys.argv[1:] != ["zk"]:
+    only = sys.argv[1:]
+    if not only:
         main()
-    main_zk()
+    if not only or only == ["zk"]:
+        main_zk()
+    if not only or only == ["vinit"]:
+        main_vinit()

@@ -74,6 +74,37 @@ def virgo_inputs(n: int, seed: int):
             elements(seed + 3, 1))
 
 
+VIRGO_TYPES = (0, 1, 2, 4, 5, 6, 7, 8, 9, 10, 12, 13, 14)
+
+
+def virgo_layer(seed: int, length_g: int, length_u: int, types=VIRGO_TYPES) -> dict:
+    """A seeded two-layer circuit slice for the Virgo inits: 2^length_g gates of the
+    given types over 2^length_u values (ranges of sum / exp-sum gates at most 8
+    long, 1-4 (src, weight) terms per custom-comb gate), the randoms r0, r1
+    (length_g), alpha, beta, and for phase 2 vma0 ({a, b}), prev_r and r_u
+    (length_u). Element arrays as everywhere here: u64 words [img, real, ...]."""
+    rng = np.random.default_rng(seed)
+    G, U = 1 << length_g, 1 << length_u
+    ty = rng.choice(np.array(types, np.int32), size=G).astype(np.int32)
+    u = rng.integers(0, U, size=G, dtype=np.int64)
+    v = rng.integers(0, U, size=G, dtype=np.int64)
+    span = rng.integers(0, 8, size=G, dtype=np.int64)
+    u[ty == 4] = rng.integers(0, min(G, U), size=int((ty == 4).sum()), dtype=np.int64)   # a gate and a value index
+    lo = rng.integers(0, max(1, U - 8), size=G, dtype=np.int64)
+    r5, r12 = ty == 5, ty == 12
+    u[r5], v[r5] = lo[r5], np.minimum(lo[r5] + span[r5], U)
+    u[r12], v[r12] = lo[r12], np.minimum(lo[r12] + span[r12], U - 1)
+    n_terms = np.where(ty == 14, rng.integers(1, 5, size=G), 0)
+    comb_ptr = np.zeros(G + 1, np.int32)
+    comb_ptr[1:] = np.cumsum(n_terms)
+    comb_src = rng.integers(0, U, size=max(1, int(comb_ptr[-1])), dtype=np.int64).astype(np.int32)
+    comb_w = elements(seed + 7, max(1, int(comb_ptr[-1])))
+    return dict(length_g=length_g, length_u=length_u, ty=ty, u=u, v=v, comb_ptr=comb_ptr, comb_src=comb_src,
+                comb_w=comb_w, values=elements(seed + 1, U), r0=elements(seed + 2, length_g),
+                r1=elements(seed + 3, length_g), alpha=elements(seed + 4, 1), beta=elements(seed + 5, 1),
+                vma0=elements(seed + 6, 2), prev_r=elements(seed + 8, 1), r_u=elements(seed + 9, max(1, length_u)))
+
+
 def digest(a: np.ndarray) -> bytes:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest()
 
@@ -101,6 +132,9 @@ class OrionOracle:
         L.oracle_orion_combine.argtypes = [_V, _LL, _V, _V, _V, _V, _V]
         L.oracle_fri_step.argtypes = [_V, _I, _V, _V, _V]
         L.oracle_virgo_update.argtypes = [_V, _V, _V, _LL, _V, _I, _V, _V, _V, _V]
+        L.oracle_virgo_phase1_init.argtypes = [_LL, _V, _V, _V, _V, _V, _V, _I, _I, _V, _V, _V, _V, _V, _V, _V, _V]
+        L.oracle_virgo_phase2_init.argtypes = [_LL, _V, _V, _V, _V, _V, _V, _I, _I, _V, _V, _V, _V, _V, _V, _V, _V,
+                                               _V, _V, _V]
         L.oracle_frame_vector.argtypes = [_V, _I, _I, _I, _I, _I, ctypes.c_uint64, ctypes.c_uint64, _I, _V]
 
     def sha256_64(self, msg: bytes) -> bytes:
@@ -153,6 +187,22 @@ class OrionOracle:
             src[1::2] = v
             roots.append(self.commit(src))
         return tuple(roots)
+
+    def virgo_init(self, phase: int, L: dict):
+        """(V_mult_add, addV_array, add_mult_sum) after sumcheck_phase{1,2}_init."""
+        U = 1 << L["length_u"]
+        outs = [np.zeros(4 * U, np.uint64) for _ in range(3)]
+        common = [1 << L["length_g"], _vp(L["ty"]), _vp(L["u"]), _vp(L["v"]), _vp(L["comb_ptr"]), _vp(L["comb_src"]),
+                  _vp(L["comb_w"]), L["length_g"], L["length_u"], _vp(L["values"]), _vp(L["r0"]), _vp(L["r1"]),
+                  _vp(L["alpha"]), _vp(L["beta"])]
+        if phase == 1:
+            rc = self.lib.oracle_virgo_phase1_init(*common, *[_vp(o) for o in outs])
+        else:
+            rc = self.lib.oracle_virgo_phase2_init(*common, _vp(L["vma0"]), _vp(L["prev_r"]), _vp(L["r_u"]),
+                                                   *[_vp(o) for o in outs])
+        if rc != 0:
+            raise ValueError("oracle_virgo_phase%d_init: %d" % (phase, rc))
+        return tuple(outs)
 
     def combine(self, src: np.ndarray, r0: np.ndarray, r1: np.ndarray):
         """(combined codeword, root of its tree, answer) of the opening passes."""

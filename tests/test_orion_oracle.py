@@ -189,3 +189,27 @@ def test_zk_mask_only_hides_private_wires(orc):
     m = orc.frame_vector(pix, 5, 384, 512, 384, 128, 8, 77, 2).reshape(8, 512)
     assert not m[:, 384:].any() and not m[5:].any()
     assert m[:5, :384].all()       # a zero draw has probability ~2^-50 here
+
+
+def test_virgo_layer_inits(orc):
+    """sumcheck_phase1_init / phase2_init restated (every gate type) against the
+    reference's tables (digests in tests/golden/virgo_init_golden.npz)."""
+    from orionlib import virgo_layer
+    g = np.load(os.path.join(ROOT, "tests", "golden", "virgo_init_golden.npz"))
+    n = 0
+    for k in g.files:
+        if not k.startswith("vinitcase_"):
+            continue
+        phase, seed, lg, lu = (int(x) for x in g[k])
+        outs = orc.virgo_init(phase, virgo_layer(seed, lg, lu))
+        assert b"".join(digest(o) for o in outs) == g["vinit_" + k[len("vinitcase_"):]].tobytes(), k
+        n += 1
+    assert n >= 12
+
+
+def test_virgo_init_rejects_out_of_range_gates(orc):
+    from orionlib import virgo_layer
+    L = virgo_layer(3, 4, 4, types=(0,))
+    L["u"][5] = 1 << 4
+    with pytest.raises(ValueError):
+        orc.virgo_init(1, L)

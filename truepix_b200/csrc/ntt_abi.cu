@@ -187,4 +187,49 @@ int tp_virgo_sumcheck_update_dev(const void* d_vma, const void* d_addv, const vo
                : -1;
 }
 
+void* tp_virgo_layer_create(int length_g, int length_u, const int* ty, const long long* u, const long long* v,
+                            const int* comb_ptr, const int* comb_src, const uint64_t* comb_w)
+{
+    tp::clear_error();
+    return tp::virgo::layer_create(length_g, length_u, ty, u, v, comb_ptr, comb_src, comb_w);
+}
+
+void tp_virgo_layer_destroy(void* layer) { tp::virgo::layer_destroy(static_cast<tp::virgo::Layer*>(layer)); }
+
+int tp_virgo_phase1_init_dev(void* layer, const void* d_values, const uint64_t* r0, const uint64_t* r1,
+                             const uint64_t* alpha, const uint64_t* beta, void* d_vma, void* d_addv, void* d_ams,
+                             void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!layer || !d_values || !d_vma || !d_addv || !d_ams) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_virgo_phase1_init_dev: null layer or buffer");
+        return -1;
+    }
+    return tp::virgo::phase1_init(*static_cast<tp::virgo::Layer*>(layer), static_cast<const ulonglong2*>(d_values),
+                                  r0, r1, alpha, beta, static_cast<ulonglong2*>(d_vma),
+                                  static_cast<ulonglong2*>(d_addv), static_cast<ulonglong2*>(d_ams),
+                                  reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_virgo_phase2_init_dev(void* layer, const void* d_values, const uint64_t* r0, const uint64_t* r1,
+                             const uint64_t* alpha, const uint64_t* beta, const void* d_vma0, const uint64_t* prev_r,
+                             const uint64_t* r_u, void* d_vma, void* d_addv, void* d_ams, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!layer || !d_values || !d_vma || !d_addv || !d_ams) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_virgo_phase2_init_dev: null layer or buffer");
+        return -1;
+    }
+    return tp::virgo::phase2_init(*static_cast<tp::virgo::Layer*>(layer), static_cast<const ulonglong2*>(d_values),
+                                  r0, r1, alpha, beta, static_cast<const ulonglong2*>(d_vma0), prev_r, r_u,
+                                  static_cast<ulonglong2*>(d_vma), static_cast<ulonglong2*>(d_addv),
+                                  static_cast<ulonglong2*>(d_ams), reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
 }  // extern "C"

@@ -84,6 +84,10 @@ GKR_SIGNATURES = {
     "tp_orion_commit_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
     "tp_orion_commit_pair": (_I32, [_VP, _VP, ctypes.c_longlong, _VP, _VP]),
     "tp_orion_set_leaf_chunks": (_I32, [_I32]),
+    "tp_virgo_layer_create": (_VP, [_I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "tp_virgo_layer_destroy": (None, [_VP]),
+    "tp_virgo_phase1_init_dev": (_I32, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "tp_virgo_phase2_init_dev": (_I32, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "tp_orion_commit_zk_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _U64, _VP, _VP, _VP, _VP,
                                              _VP]),
     "tp_orion_pixel_vector_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _U64, _I32, _VP, _VP]),
