@@ -690,17 +690,22 @@ def ours_arm(args, rank, world, local_rank):
         res_ok = bool(c.any() and w.any() and m != (0, 0) and any(committer.root(B - 1)))
 
     ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = ref_gpu = None
-    if rank == 0 and not args.skip_ntt:
+    # The side measurements run once, at N = 1 (a scaling run holds every GPU
+    # while rank 0 works; it only needs the step's value).
+    extras = rank == 0 and world == 1
+    if extras and not args.skip_ntt:
         ntt = ntt_bench(lib, dev, stream)
-    if rank == 0 and not args.skip_opening:
+    if extras and not args.skip_opening:
         opening = opening_bench(args, lib, committer, layout, dev, stream, sha_gcs)
-    if rank == 0 and not args.skip_zk:
+    if extras and not args.skip_zk:
         zk = zk_step(args, bprover, pix, z1s, z2s, pts, chal_b, layout, stream, local_rank)
-    if rank == 0 and not args.skip_e2e:
-        e2e = e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream, dev)
+    if not args.skip_e2e:
+        # every rank: the job's e2e is all ranks' frames over the slowest rank's time
+        e2e = e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream, dev, world)
+    if extras and not args.skip_e2e:
         e2e_ref = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
         ref_gpu = reference_gpu_lib(frames[0], layout, gt, i0, i1, z1, z2, point, chal)
-    if rank == 0 and not args.skip_serving:
+    if extras and not args.skip_serving:
         del bprover
         committer.rows = committer.trees = None
         torch.cuda.empty_cache()
@@ -983,7 +988,7 @@ def opening_bench(args, lib, committer, layout, dev, stream, sha_gcs, reps=5):
     return out
 
 
-def e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream, dev):
+def e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream, dev, world=1):
     """The batched path from pinned host frames: H2D of every frame's bytes, a D2H
     of all claims after every round with a synchronise, the commits, D2H of wires,
     MLEs and commitment roots."""
@@ -1027,13 +1032,18 @@ def e2e_batched(args, bprover, committer, frames, z1s, z2s, pts, chal_b, stream,
 
     one()
     steps = max(2, min(args.steps, 5))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(steps):
         one()
     wall = time.perf_counter() - t0
+    if world > 1:
+        wall = max_over_ranks(1e3 * wall, world, dev) / 1e3
     h2d = sum(f.nbytes for f in frames)
     d2h = R * B * 64 + bprover.wires.numel() * 8 + bprover.mle.numel() * 8 + 32 * B
-    return {"value": steps * B / wall, "unit": UNIT, "h2d_bytes_per_step": h2d,
+    return {"value": world * steps * B / wall, "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": steps, "frames_per_step": B,
             "timer": "host wall clock", "path": "tp_batch_* + tp_orion_commit_pixels_dev from "
             "pinned host frames (copied frame by frame on a copy stream; each commit starts when its "
