@@ -709,8 +709,7 @@ def ours_arm(args, rank, world, local_rank):
         del bprover
         committer.rows = committer.trees = None
         torch.cuda.empty_cache()
-        uneven = batched_uneven()
-        serving = serving_sweep()
+        uneven, serving = serving_in_own_process(local_rank)
     if rank == 0 and world == 1 and not args.skip_cpu:
         secs, kind = _cpu_worker((0, 1))
         cpu = {"value": 1.0 / secs, "unit": UNIT, "cores": 1, "kind": kind,
@@ -1159,6 +1158,21 @@ def reference_gpu_lib(frame, layout, gt, i0, i1, z1, z2, point, chal, reps=3):
     out["what"] = ("GKR input layer of one 1080p frame through the native_fp2 C ABI (host buffers, %d rounds): "
                    "the reference's native_fp2.cu (its build.sh recipe, -arch=sm_100a) vs ours" % nb)
     return out
+
+
+def _serving_job(device):
+    import torch
+    torch.cuda.set_device(device)
+    return batched_uneven(), serving_sweep()
+
+
+def serving_in_own_process(device):
+    """Configs 4 and 5 in a fresh process on the same GPU: their latencies then do
+    not depend on what this process left in the device's pools and caches (the
+    step's batch, the committers, other libraries loaded for the comparisons)."""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(1, maxtasksperchild=1) as pool:
+        return pool.apply(_serving_job, (device,))
 
 
 def release(srv):
