@@ -282,7 +282,8 @@ def test_device_buffer_api(gpu_lib, oracle_lib, circuits):
     ("gray", (1080, 1920), "pixels"), ("gray", (1080, 1920), "table"),
     ("Crop", (240, 426), "pixels"), ("Crop", (240, 426), "table"),
     ("inv", (360, 640), "pixels"), ("mask", (8, 8), "pixels"), ("gray", (4, 8), "pixels"),
-    ("Crop", (2, 64), "pixels"), ("gray", (720, 1280), "pixels")])
+    ("Crop", (2, 64), "pixels"), ("gray", (720, 1280), "pixels"),
+    ("gray", (2160, 3840), "pixels")])    # 4K: 64,800 copies -> 2^25 input wires, the largest serving frame
 def test_frame_prover_vs_oracle(oracle_lib, circuits, name, hw, mode):
     """The device-resident frame path (bytes -> beta -> rounds -> MLE) in both modes:
     straight from the bytes, and through the materialised table."""

@@ -97,6 +97,38 @@ def test_size_2_24_round_trip_and_linearity(lib):
     assert int(got.max()) < P61
 
 
+def test_size_2_28_round_trip_and_linearity_on_device(lib):
+    """The largest supported transform (2^28 points; the reference asserts beyond
+    2^27): ifft(fft(a)) == a and fft(a + b) == fft(a) + fft(b), inputs drawn and
+    results compared on the device."""
+    import torch
+    n = 1 << 28
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(28)
+    p = (1 << 61) - 1
+    a = torch.randint(0, p, (2 * n,), dtype=torch.int64, device=dev, generator=g)
+    b = torch.randint(0, p, (2 * n,), dtype=torch.int64, device=dev, generator=g)
+    s = torch.cuda.current_stream().cuda_stream
+    fa, fb = torch.empty_like(a), torch.empty_like(a)
+    assert lib.tp_fft_dev(a.data_ptr(), n, n, fa.data_ptr(), 1, 0, 0, s) == 0, lib.tp_last_error()
+    assert lib.tp_fft_dev(b.data_ptr(), n, n, fb.data_ptr(), 1, 0, 0, s) == 0, lib.tp_last_error()
+    back = torch.empty_like(a)
+    assert lib.tp_ifft_dev(fa.data_ptr(), n, n, back.data_ptr(), 1, 0, 0, s) == 0, lib.tp_last_error()
+    torch.cuda.synchronize()
+    assert torch.equal(back, a)
+    del back
+    ab = a + b
+    ab = torch.where(ab >= p, ab - p, ab)
+    fab = torch.empty_like(a)
+    assert lib.tp_fft_dev(ab.data_ptr(), n, n, fab.data_ptr(), 1, 0, 0, s) == 0, lib.tp_last_error()
+    want = fa + fb
+    want = torch.where(want >= p, want - p, want)
+    torch.cuda.synchronize()
+    assert torch.equal(fab, want)
+    assert int(fab.max()) < p and int(fab.min()) >= 0
+
+
 def test_batched_device_transforms(lib, orc):
     import torch
     m, o, batch = 1 << 8, 1 << 13, 64

@@ -242,3 +242,15 @@ def test_leaf_chains_split_over_launches_give_the_same_tree(lib, orc):
             assert lib.tp_orion_set_leaf_chunks(bad) == -1
     finally:
         lib.tp_orion_set_leaf_chunks(1)
+
+
+def test_commit_of_a_4k_frame_matches_oracle(lib, orc):
+    """The largest serving frame: 2160 x 3840 x 3 bytes = 64,800 copies -> 65,536
+    x 512 = 2^25 elements, 128 columns of 2^18, codeword 450,887 rows."""
+    copies = 2160 * 3840 * 3 // 384
+    pix = frame_bytes(4096, copies * 384)
+    tree = _pixel_commit(lib, pix, copies, 384, 512, 384, 128, 65536)
+    src = frame_elements(pix, copies, 384, 512, 384, 128, 65536)
+    assert src.size == 2 << 25
+    assert lib.tp_orion_codeword_len(1 << 18) == 450887
+    assert tree[1].tobytes() == orc.commit(src)
