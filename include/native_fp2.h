@@ -228,6 +228,35 @@ int tp_timer_read(float* ms, int* tags, int max_pairs);
 int tp_mle_eval_base_noalloc(const void* d_inputs, const void* d_z, int n_z, void* d_out,
                              void* stream);
 
+/* ---- Fiat-Shamir transcript (TruePix-main/libTruePix/fiatshamir.py) ----------
+ * The reference prover's transcript in its binary format: one running SHA-256
+ * over everything put, challenges drawn from digests of the running state. A
+ * state is tp_fs_state_bytes() (= 120) bytes of caller memory, host or device; it
+ * moves between the two by a plain copy (cudaMemcpy), so a transcript begun on
+ * the host (the circuit's IO, the commitment roots) continues on the device.
+ * Host calls take one state in host memory; *_dev calls take n states in device
+ * memory, one per frame, and are asynchronous on `stream`. */
+int tp_fs_state_bytes(void);
+/* FiatShamir(q, protocol).__init__ (fiatshamir.py:27-74) for q = 2^61 - 1 */
+int tp_fs_init(void* state, const char* protocol);
+/* put(list of ints < 2^64): the array('Q') path (fiatshamir.py:112-120) */
+int tp_fs_put_u64s(void* state, const uint64_t* values, size_t n);
+/* put(Fp2) for each (re[i], im[i]) in turn (fiatshamir.py:129-131) */
+int tp_fs_put_fp2s(void* state, const uint64_t* re, const uint64_t* im, size_t n);
+/* put(str) (fiatshamir.py:132-136) */
+int tp_fs_put_str(void* state, const char* str);
+/* rand_scalar() (fiatshamir.py:141-148) */
+int tp_fs_rand_scalar(void* state, uint64_t* out);
+/* rand_ext(label) (fiatshamir.py:150-162); labels up to 64 bytes */
+int tp_fs_rand_ext(void* state, const char* label, uint64_t* re, uint64_t* im);
+/* hash.digest() of the running state (32 bytes; the state is unchanged) */
+int tp_fs_digest(const void* state, unsigned char* out32);
+/* state i puts the k Fp2 d_values[i * k .. i * k + k) (packed {re, im} u64 pairs,
+ * e.g. a frame's four round claims) */
+int tp_fs_put_fp2s_dev(void* d_states, int n, const void* d_values, int k, void* stream);
+/* state i draws rand_ext(label) into d_out[i] (packed {re, im}) */
+int tp_fs_rand_ext_dev(void* d_states, int n, const char* label, void* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

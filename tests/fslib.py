@@ -1,0 +1,109 @@
+"""Replay of the Fiat-Shamir golden scripts (tests/golden/fs_golden.npz).
+
+`replay_python` restates the reference transcript's binary format with Python's
+hashlib (test infrastructure: it checks the golden vectors on CPU);
+`replay_lib` drives the library's tp_fs_* host entry points through ctypes."""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import json
+import os
+import struct
+
+import numpy as np
+
+P61 = (1 << 61) - 1
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def golden():
+    return np.load(os.path.join(ROOT, "tests", "golden", "fs_golden.npz"))
+
+
+def scripts(g):
+    for k in sorted(g.files):
+        if k.startswith("fsscript_"):
+            name = k[len("fsscript_"):]
+            protocol, ops = json.loads(g[k].tobytes().decode())
+            yield name, protocol, ops
+
+
+class PyTranscript:
+    def __init__(self, protocol):
+        self.h = hashlib.sha256(b"TruePix," + protocol.encode() + b"," + b"binhash1,")
+        self.rnum = 0
+
+    def u64s(self, v):
+        self.h.update(b"\x01" + struct.pack("<I", len(v)) + b"".join(struct.pack("<Q", x) for x in v))
+
+    def fp2(self, re, im):
+        self.h.update(b"\x03" + struct.pack("<QQ", re, im))
+
+    def str(self, s):
+        b = s.encode()
+        self.h.update(b"\x04" + struct.pack("<I", len(b)) + b)
+
+    def scalar(self):
+        while True:
+            self.u64s([self.rnum])
+            self.rnum += 1
+            v = int.from_bytes(self.h.digest(), "big") & P61
+            if v < P61:
+                return v
+
+    def ext(self, label):
+        self.str("ext"), self.str(label), self.str("real")
+        re = self.scalar()
+        self.str("ext"), self.str(label), self.str("imag")
+        return re, self.scalar()
+
+
+def replay_python(protocol, ops):
+    t = PyTranscript(protocol)
+    outs, digs = [], b""
+    for op in ops:
+        if op[0] == "u64s":
+            t.u64s(op[1])
+        elif op[0] == "fp2s":
+            for re, im in op[1]:
+                t.fp2(re, im)
+        elif op[0] == "str":
+            t.str(op[1])
+        elif op[0] == "ext":
+            outs += list(t.ext(op[1]))
+        elif op[0] == "scalar":
+            outs.append(t.scalar())
+        elif op[0] == "digest":
+            digs += t.h.digest()
+    return np.array(outs, np.uint64), digs
+
+
+def replay_lib(lib, protocol, ops, state=None):
+    """(outputs, digests, state buffer) through tp_fs_*; `state` continues a given one"""
+    st = state if state is not None else ctypes.create_string_buffer(lib.tp_fs_state_bytes())
+    if state is None:
+        assert lib.tp_fs_init(st, protocol.encode()) == 0
+    outs, digs = [], b""
+    re, im = ctypes.c_uint64(), ctypes.c_uint64()
+    d = ctypes.create_string_buffer(32)
+    for op in ops:
+        if op[0] == "u64s":
+            a = np.array(op[1], np.uint64)
+            assert lib.tp_fs_put_u64s(st, a.ctypes.data, a.size) == 0
+        elif op[0] == "fp2s":
+            a = np.array(op[1], np.uint64).reshape(-1, 2)
+            r, i = np.ascontiguousarray(a[:, 0]), np.ascontiguousarray(a[:, 1])
+            assert lib.tp_fs_put_fp2s(st, r.ctypes.data, i.ctypes.data, r.size) == 0
+        elif op[0] == "str":
+            assert lib.tp_fs_put_str(st, op[1].encode()) == 0
+        elif op[0] == "ext":
+            assert lib.tp_fs_rand_ext(st, op[1].encode(), ctypes.byref(re), ctypes.byref(im)) == 0
+            outs += [re.value, im.value]
+        elif op[0] == "scalar":
+            assert lib.tp_fs_rand_scalar(st, ctypes.byref(re)) == 0
+            outs.append(re.value)
+        elif op[0] == "digest":
+            assert lib.tp_fs_digest(st, d) == 0
+            digs += d.raw
+    return np.array(outs, np.uint64), digs, st

@@ -1,0 +1,86 @@
+"""The Fiat-Shamir transcript (tp_fs_*): the host entry points against the
+reference's own FiatShamir class (tests/golden/fs_golden.npz), and the batched
+device entry points (one state per frame in device memory) against the host
+ones: a batch of transcripts moved to the device absorbs each frame's four
+claims and draws its challenge round after round, bit-identical to doing the
+same on the host, and continues on the host after the copy back."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from fslib import P61, golden, replay_lib, scripts
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from truepix_b200 import native
+    return native.gkr()
+
+
+def test_host_transcript_matches_reference_vectors(lib):
+    g = golden()
+    for name, protocol, ops in scripts(g):
+        outs, digs, _ = replay_lib(lib, protocol, ops)
+        np.testing.assert_array_equal(outs, g["fsout_" + name])
+        assert digs == g["fsdigest_" + name].tobytes(), name
+
+
+def test_device_batch_rounds_match_host(lib):
+    import torch
+    nb = lib.tp_fs_state_bytes()
+    assert nb == 120
+    n, rounds = 96, 14
+    rng = np.random.default_rng(7)
+    host = []
+    for f in range(n):   # distinct histories of different lengths (partial blocks differ)
+        _, _, st = replay_lib(lib, "truepix", [["u64s", [f] * (1 + f % 9)], ["str", "frame-%d" % f],
+                                               ["ext", "z2-0"]])
+        host.append(st)
+    dev = torch.device("cuda", 0)
+    d_states = torch.from_numpy(np.frombuffer(b"".join(s.raw for s in host), np.uint8).copy()).to(dev)
+    d_claims = torch.empty(n * 8, dtype=torch.int64, device=dev)
+    d_chal = torch.empty(n * 2, dtype=torch.int64, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    re, im = ctypes.c_uint64(), ctypes.c_uint64()
+    for rd in range(rounds):
+        claims = rng.integers(0, P61, size=n * 8, dtype=np.uint64)
+        claims[:8] = P61 - 1 if rd % 2 else 0
+        d_claims.copy_(torch.from_numpy(claims.view(np.int64)))
+        label = ("sc-0-%d" % rd).encode()
+        assert lib.tp_fs_put_fp2s_dev(d_states.data_ptr(), n, d_claims.data_ptr(), 4, s) == 0, lib.tp_last_error()
+        assert lib.tp_fs_rand_ext_dev(d_states.data_ptr(), n, label, d_chal.data_ptr(), s) == 0, lib.tp_last_error()
+        got = d_chal.cpu().numpy().view(np.uint64).reshape(n, 2)
+        c = claims.reshape(n, 4, 2)
+        for f in range(n):
+            r = np.ascontiguousarray(c[f, :, 0])
+            i = np.ascontiguousarray(c[f, :, 1])
+            assert lib.tp_fs_put_fp2s(host[f], r.ctypes.data, i.ctypes.data, 4) == 0
+            assert lib.tp_fs_rand_ext(host[f], label, ctypes.byref(re), ctypes.byref(im)) == 0
+            assert (int(got[f, 0]), int(got[f, 1])) == (re.value, im.value), (rd, f)
+            assert re.value < P61 and im.value < P61
+    back = d_states.cpu().numpy().tobytes()
+    d1, d2 = ctypes.create_string_buffer(32), ctypes.create_string_buffer(32)
+    for f in range(n):
+        st = ctypes.create_string_buffer(back[f * nb:(f + 1) * nb], nb)
+        assert lib.tp_fs_digest(st, d1) == 0 and lib.tp_fs_digest(host[f], d2) == 0
+        assert d1.raw == d2.raw
+        # the device state continues on the host like the host one
+        a = ctypes.c_uint64(), ctypes.c_uint64()
+        assert lib.tp_fs_rand_ext(st, b"tau-0", ctypes.byref(a[0]), ctypes.byref(a[1])) == 0
+        assert lib.tp_fs_rand_ext(host[f], b"tau-0", ctypes.byref(re), ctypes.byref(im)) == 0
+        assert (a[0].value, a[1].value) == (re.value, im.value)
+
+
+def test_transcript_rejects_bad_arguments(lib):
+    import torch
+    st = ctypes.create_string_buffer(lib.tp_fs_state_bytes())
+    assert lib.tp_fs_init(st, b"truepix") == 0
+    re, im = ctypes.c_uint64(), ctypes.c_uint64()
+    assert lib.tp_fs_rand_ext(st, b"x" * 65, ctypes.byref(re), ctypes.byref(im)) == -1
+    assert b"64 bytes" in lib.tp_last_error()
+    assert lib.tp_fs_put_u64s(st, None, 0) == -1
+    buf = torch.zeros(120, dtype=torch.uint8, device="cuda")
+    assert lib.tp_fs_rand_ext_dev(buf.data_ptr(), 0, b"a", buf.data_ptr(), None) == -1
