@@ -181,6 +181,13 @@ int tp_batch_set_table(void* batch, int i, int n_gates, const int* gate_type, co
 int tp_batch_claim(void* batch, void* d_claims);
 /* fold every frame that has >= 2 copies by (challenges[2i], challenges[2i+1]) (host array) */
 int tp_batch_fold(void* batch, const uint64_t* challenges);
+/* tp_batch_fold with the challenges in device memory (n_frames packed {re, im}
+ * Fp2, canonical, e.g. drawn by tp_fs_rand_ext_dev): they are read in stream
+ * order when the next tp_batch_claim / tp_batch_finish is queued on the batch's
+ * stream, so they must be written before that point in stream order and stay
+ * unchanged until it. Every frame needs a claim or a finish before its next
+ * fold. No host round trip between rounds. */
+int tp_batch_fold_dev(void* batch, const void* d_challenges);
 int tp_batch_n_copies(void* batch, int i);
 /* d_wires: frame i at d_wires + 16 * (sum of n_wires of frames < i) bytes -- with equal
  * n_wires simply [n_frames][n_wires] packed Fp2; d_beta: [n_frames] packed Fp2 */

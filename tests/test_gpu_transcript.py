@@ -84,3 +84,65 @@ def test_transcript_rejects_bad_arguments(lib):
     assert lib.tp_fs_put_u64s(st, None, 0) == -1
     buf = torch.zeros(120, dtype=torch.uint8, device="cuda")
     assert lib.tp_fs_rand_ext_dev(buf.data_ptr(), 0, b"a", buf.data_ptr(), None) == -1
+
+
+def test_batched_rounds_with_device_transcripts_match_host_transcripts(lib):
+    """BatchFrameProver driven by device transcripts (claims put and challenges
+    drawn on the device, tp_batch_fold_dev) against the same batch driven by host
+    transcripts fed with the claims read back every round: identical claims,
+    challenges, wires, beta, MLE and final transcript states."""
+    import torch
+    from truepix_b200.frame import BatchFrameProver, FrameLayout, pack_fp2
+    import os
+    from fslib import ROOT
+    c = np.load(os.path.join(ROOT, "tests", "golden", "circuits.npz"))
+    gt, i0, i1 = c["gray_type"], c["gray_in0"], c["gray_in1"]
+    B = 6
+    layout = FrameLayout.for_frame(240, 426)
+    nb = layout.n_copy_bits
+    rng = np.random.default_rng(99)
+    dev = torch.device("cuda", 0)
+    pix = [torch.from_numpy(rng.integers(0, 256, size=layout.copies * 384, dtype=np.uint8)).to(dev)
+           for _ in range(B)]
+    z1 = np.stack([rng.integers(0, P61, size=384, dtype=np.uint64) for _ in range(2)])
+    z2 = rng.integers(0, P61, size=(nb, 2), dtype=np.uint64)
+    pt = rng.integers(0, P61, size=(nb + 9, 2), dtype=np.uint64)
+    z2d = torch.from_numpy(pack_fp2(z2[:, 0], z2[:, 1])).to(dev).repeat(B)
+    ptd = torch.from_numpy(pack_fp2(pt[:, 0], pt[:, 1])).to(dev).repeat(B)
+    states = [replay_lib(lib, "truepix", [["u64s", [f, 7]], ["ext", "z2-0"]])[2] for f in range(B)]
+
+    # host transcripts: read each round's claims back, draw the challenges on the host
+    host_prover = BatchFrameProver([layout] * B, gt, i0, i1)
+    chal = np.zeros((nb, B, 2), np.uint64)
+    hstates = [ctypes.create_string_buffer(s.raw, len(s.raw)) for s in states]
+    re, im = ctypes.c_uint64(), ctypes.c_uint64()
+
+    def hook(k):
+        torch.cuda.synchronize()
+        cl = host_prover.claims.cpu().numpy().view(np.uint64).reshape(nb, B, 4, 2)[k]
+        for f in range(B):
+            r, i = np.ascontiguousarray(cl[f, :, 0]), np.ascontiguousarray(cl[f, :, 1])
+            assert lib.tp_fs_put_fp2s(hstates[f], r.ctypes.data, i.ctypes.data, 4) == 0
+            assert lib.tp_fs_rand_ext(hstates[f], ("sc-0-%d" % k).encode(), ctypes.byref(re), ctypes.byref(im)) == 0
+            chal[k, f] = (re.value, im.value)
+
+    host_prover.prove(pix, [z1] * B, z2d, ptd, chal, round_hook=hook)
+    torch.cuda.synchronize()
+
+    dev_prover = BatchFrameProver([layout] * B, gt, i0, i1)
+    d_states = torch.from_numpy(np.frombuffer(b"".join(s.raw for s in states), np.uint8).copy()).to(dev)
+    dev_prover.prove(pix, [z1] * B, z2d, ptd, None, transcripts=d_states)
+    torch.cuda.synchronize()
+
+    got_ch = dev_prover.device_challenges.cpu().numpy().view(np.uint64).reshape(nb, B, 2)
+    np.testing.assert_array_equal(got_ch, chal)
+    for f in range(B):
+        a, b = host_prover.results(f), dev_prover.results(f)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2] and a[3] == b[3], f
+    back = d_states.cpu().numpy().tobytes()
+    d1, d2 = ctypes.create_string_buffer(32), ctypes.create_string_buffer(32)
+    n = lib.tp_fs_state_bytes()
+    for f in range(B):
+        st = ctypes.create_string_buffer(back[f * n:(f + 1) * n], n)
+        assert lib.tp_fs_digest(st, d1) == 0 and lib.tp_fs_digest(hstates[f], d2) == 0
+        assert d1.raw == d2.raw

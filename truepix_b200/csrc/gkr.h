@@ -59,6 +59,7 @@ struct Frame {
     PixSrc px;
     bool pending = false;  // fold recorded, applied by the next claim / fold / finish
     fp2 r;
+    const fp2* r_dev = nullptr;  // the pending fold's challenge in device memory (batch_fold_dev)
     DevGateForm form;
     std::vector<fp2> L_host;
     fp2 Lc;                // L[const_idx] * const_val (byte source)
@@ -82,6 +83,8 @@ struct Batch {
     size_t cap_partials = 0;  // in CTAs (4 fp2 each)
     unsigned* tickets = nullptr;
     size_t cap_tickets = 0;
+    void* d_patch = nullptr;   // (job, device challenge) pairs patched into the job array
+    size_t cap_patch = 0;
     int launches = 0;
 };
 
@@ -96,6 +99,9 @@ bool batch_load_pixels(Batch* B, int i, const PixSrc& px, const fp2* d_beta);
 // claims of all unfinished frames; d_claims[i] (8 u64, device) or the frame's slot
 bool batch_claim(Batch* B, u64* const* d_claims);
 bool batch_fold(Batch* B, int i, fp2 r);
+// the same with the challenge in device memory (read in stream order when the
+// next claim or finish is queued); needs a claim or finish before the next fold
+bool batch_fold_dev(Batch* B, int i, const fp2* d_r);
 // wires / beta of every frame into d_wires[i] (n_wires packed) / d_beta[i] (1 packed);
 // nullptr destinations use the frame's own staging buffer
 bool batch_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta);

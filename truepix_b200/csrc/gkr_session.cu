@@ -46,6 +46,7 @@ bool frame_alloc(Frame* f, size_t rows0, size_t rows1, cudaStream_t s)
     }
     f->cur = 0;
     f->pending = false;
+    f->r_dev = nullptr;
     f->pix_cur = false;
     return (!rows0 || f->buf[0]) && f->buf[1] && f->beta[0] && f->beta[1];
 }
@@ -95,6 +96,51 @@ bool ensure_workspace(Batch* B, size_t jobs, size_t ctas)
         if (!B->partials) return false;
     }
     return true;
+}
+
+// A job whose frame's pending fold takes its challenge from device memory gets
+// it written into the uploaded job array, in stream order, before the launch.
+struct RPatch {
+    const fp2* r;
+    long long job;
+};
+
+__global__ void patch_r_kernel(Job* __restrict__ jobs, const RPatch* __restrict__ p, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) jobs[p[i].job].r = *p[i].r;
+}
+
+bool upload_jobs(Batch* B, const Job* jobs, size_t n, const std::vector<const fp2*>& rdev)
+{
+    if (!upload_async(B->d_jobs, jobs, sizeof(Job) * n, B->stream)) return false;
+    std::vector<RPatch> p;
+    for (size_t q = 0; q < n && q < rdev.size(); ++q)
+        if (rdev[q]) p.push_back(RPatch{rdev[q], (long long)q});
+    if (p.empty()) return true;
+    if (p.size() > B->cap_patch) {
+        dev_free(B->d_patch, B->stream);
+        B->cap_patch = std::max<size_t>(p.size(), 64);
+        B->d_patch = dev_alloc(sizeof(RPatch) * B->cap_patch, B->stream);
+        if (!B->d_patch) {
+            B->cap_patch = 0;
+            return false;
+        }
+    }
+    if (!upload_async(B->d_patch, p.data(), sizeof(RPatch) * p.size(), B->stream)) return false;
+    patch_r_kernel<<<(unsigned)((p.size() + 127) / 128), 128, 0, B->stream>>>(
+        B->d_jobs, static_cast<const RPatch*>(B->d_patch), (int)p.size());
+    ++B->launches;
+    return !cuda_failed(cudaGetLastError(), "challenge patch");
+}
+
+bool device_fold_blocked(const Frame* f)
+{
+    if (f->pending && f->r_dev) {
+        set_error(TP_ERR_ARG, "a fold with a device challenge needs a claim or finish before the next fold");
+        return true;
+    }
+    return false;
 }
 
 Job base_job(const Frame* f)
@@ -285,7 +331,10 @@ bool batch_claim(Batch* B, u64* const* d_claims)
             jobs[q].partials = B->partials + 4 * (size_t)jobs[q].cta0;
             jobs[q].ticket = B->tickets + q;
         }
-        if (!upload_async(B->d_jobs, jobs.data(), sizeof(Job) * jobs.size(), B->stream)) return false;
+        std::vector<const fp2*> rdev(jobs.size(), nullptr);
+        for (size_t q = 0; q < jobs.size(); ++q)
+            if (fr[k][q]->pending) rdev[q] = fr[k][q]->r_dev;
+        if (!upload_jobs(B, jobs.data(), jobs.size(), rdev)) return false;
         int lg = 0;
         while ((1 << lg) < 2 * jobs[0].n_pairs) ++lg;
         timer_begin(B->stream, 1000 * (k >> 1) + 100 * (k & 1) + lg);
@@ -298,6 +347,7 @@ bool batch_claim(Batch* B, u64* const* d_claims)
                 f->pix_cur = false;
                 f->n_phys >>= 1;
                 f->pending = false;
+                f->r_dev = nullptr;
             }
         }
     }
@@ -319,9 +369,37 @@ bool batch_fold(Batch* B, int i, fp2 r)
         set_error(TP_ERR_ARG, "fold challenge is not a canonical field element");
         return false;
     }
+    if (device_fold_blocked(f)) return false;
     if (f->pending && !apply_fold(f, B->stream, &B->launches)) return false;
     f->pending = true;
     f->r = r;
+    f->r_dev = nullptr;
+    f->n_copies >>= 1;
+    return true;
+}
+
+bool batch_fold_dev(Batch* B, int i, const fp2* d_r)
+{
+    if (i < 0 || i >= (int)B->frames.size()) {
+        set_error(TP_ERR_ARG, "frame index %d outside the batch", i);
+        return false;
+    }
+    Frame* f = B->frames[(size_t)i];
+    if (f->n_copies < 2) {
+        set_error(TP_ERR_ARG, "fold needs at least 2 copies (have %d)", f->n_copies);
+        return false;
+    }
+    if (!d_r) {
+        set_error(TP_ERR_ARG, "null device challenge");
+        return false;
+    }
+    if (f->pending) {
+        set_error(TP_ERR_ARG, "a fold with a device challenge needs a claim or finish after the previous fold");
+        return false;
+    }
+    f->pending = true;
+    f->r = f2zero();
+    f->r_dev = d_r;
     f->n_copies >>= 1;
     return true;
 }
@@ -329,6 +407,7 @@ bool batch_fold(Batch* B, int i, fp2 r)
 bool batch_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta)
 {
     std::vector<Job> jobs;
+    std::vector<const fp2*> rdev;
     int max_w = 0;
     for (size_t i = 0; i < B->frames.size(); ++i) {
         Frame* f = B->frames[i];
@@ -337,16 +416,18 @@ bool batch_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta)
             set_error(TP_ERR_ARG, "frame %zu has no table", i);
             return false;
         }
-        if (f->pending && f->n_phys > 2 && !apply_fold(f, B->stream, &B->launches)) return false;
+        if (f->pending && f->n_phys > 2 && (device_fold_blocked(f) || !apply_fold(f, B->stream, &B->launches)))
+            return false;
         Job j = base_job(f);
         j.kind = f->pending ? 1 : 0;  // a pending fold of the last two copies
         j.fin = (d_wires && d_wires[i]) ? d_wires[i] : f->fin;
         j.fin_beta = (d_beta && d_beta[i]) ? d_beta[i] : f->fin + f->n_wires;
         max_w = std::max(max_w, f->n_wires);
         jobs.push_back(j);
+        rdev.push_back(f->pending ? f->r_dev : nullptr);
     }
     if (!ensure_workspace(B, jobs.size(), 1)) return false;
-    if (!upload_async(B->d_jobs, jobs.data(), sizeof(Job) * jobs.size(), B->stream)) return false;
+    if (!upload_jobs(B, jobs.data(), jobs.size(), rdev)) return false;
     return launch_finish(B->d_jobs, (int)jobs.size(), max_w, B->stream, &B->launches);
 }
 
@@ -361,13 +442,14 @@ bool batch_finish_frame(Batch* B, int i, fp2* d_wires, fp2* d_beta)
         set_error(TP_ERR_ARG, "frame %d is not configured", i);
         return false;
     }
-    if (f->pending && f->n_phys > 2 && !apply_fold(f, B->stream, &B->launches)) return false;
+    if (f->pending && f->n_phys > 2 && (device_fold_blocked(f) || !apply_fold(f, B->stream, &B->launches)))
+        return false;
     Job j = base_job(f);
     j.kind = f->pending ? 1 : 0;
     j.fin = d_wires ? d_wires : f->fin;
     j.fin_beta = d_beta ? d_beta : f->fin + f->n_wires;
     if (!ensure_workspace(B, 1, 1)) return false;
-    if (!upload_async(B->d_jobs, &j, sizeof(Job), B->stream)) return false;
+    if (!upload_jobs(B, &j, 1, std::vector<const fp2*>{f->pending ? f->r_dev : nullptr})) return false;
     if (!launch_finish(B->d_jobs, 1, f->n_wires, B->stream, &B->launches)) return false;
     batch_release(B, i, false);
     return true;
@@ -380,6 +462,7 @@ void batch_release(Batch* B, int i, bool free_buffers)
     f->configured = false;
     f->n_copies = 0;
     f->pending = false;
+    f->r_dev = nullptr;
     if (free_buffers) {
         cudaStream_t s = B->stream;
         if (!f->borrowed0) dev_free(f->buf[0], s);
@@ -417,6 +500,7 @@ void batch_destroy(Batch* B)
     dev_free(B->d_jobs, s);
     dev_free(B->partials, s);
     dev_free(B->tickets, s);
+    dev_free(B->d_patch, s);
     delete B;
 }
 

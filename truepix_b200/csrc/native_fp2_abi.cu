@@ -533,6 +533,22 @@ int tp_batch_fold(void* batch, const uint64_t* challenges)
     return 0;
 }
 
+int tp_batch_fold_dev(void* batch, const void* d_challenges)
+{
+    tp::clear_error();
+    if (!batch || !d_challenges) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_batch_fold_dev: null batch or challenges");
+        return -1;
+    }
+    tp::Batch* B = static_cast<tp::Batch*>(batch);
+    const tp::fp2* d = static_cast<const tp::fp2*>(d_challenges);
+    for (size_t i = 0; i < B->frames.size(); ++i) {
+        if (B->frames[i]->n_copies < 2) continue;
+        if (!tp::batch_fold_dev(B, (int)i, d + i)) return -1;
+    }
+    return 0;
+}
+
 int tp_batch_n_copies(void* batch, int i)
 {
     if (!batch) return 0;

@@ -221,13 +221,19 @@ class BatchFrameProver:
             self.torch.cuda.current_stream(self.dev).cuda_stream
 
     def prove(self, pixels, z1s, z2s_dev, points_dev, challenges: np.ndarray,
-              round_hook=None) -> None:
+              round_hook=None, transcripts=None, layer: int = 0) -> None:
         """pixels: one uint8 device tensor per frame; z1s: uint64 [2, n_gates] per
         frame; z2s_dev / points_dev: per padded size C, a packed Fp2 device tensor
         [frames of size C][log2 C] / [..][log2 W + log2 C], frames in batch order
         (dicts keyed by C; a single tensor is accepted when all frames share C);
         challenges: uint64 [max_rounds, B, 2]. round_hook(k) runs after round k's
-        claims are queued (where a prover reads them back for its transcript)."""
+        claims are queued (where a prover reads them back for its transcript).
+        transcripts: instead of `challenges`, one Fiat-Shamir state per frame in
+        device memory (uint8 tensor [B * tp_fs_state_bytes()]): every round, each
+        frame's transcript puts its four claims and draws the fold challenge
+        rand_ext("sc-<layer>-<round>") on the device (tp_fs_*_dev, tp_batch_fold_dev),
+        with no host round trip; all frames must then have the same number of
+        rounds. The drawn challenges are left in self.device_challenges."""
         lib, s, b = self.lib, self._s(), self.handle
         if not isinstance(z2s_dev, dict):
             assert len(self.groups) == 1
@@ -252,13 +258,31 @@ class BatchFrameProver:
                 b, f, self.gt.size, self.gt.ctypes.data, self.i0.ctypes.data, self.i1.ctypes.data,
                 z1r.ctypes.data, z1i.ctypes.data, pixels[f].data_ptr(), L.copies, L.padded_copies,
                 L.copy_size, L.n_wires, L.const_idx, L.const_val, beta_of[f]), "batch_set_pixels")
-        ch = np.ascontiguousarray(challenges, np.uint64)
         base = self.claims.data_ptr()
+        if transcripts is not None:
+            if any(L.n_copy_bits != self.max_rounds for L in self.layouts):
+                raise ValueError("device transcripts need frames with the same number of rounds")
+            if transcripts.numel() != self.B * lib.tp_fs_state_bytes():
+                raise ValueError("one transcript state per frame")
+            if getattr(self, "device_challenges", None) is None:
+                self.device_challenges = self.torch.zeros(self.max_rounds * self.B * 2, dtype=self.torch.int64,
+                                                          device=self.dev)
+        else:
+            ch = np.ascontiguousarray(challenges, np.uint64)
         l0 = lib.tp_batch_launches(b)
         for k in range(self.max_rounds):
             native.check(lib, lib.tp_batch_claim(b, base + 64 * self.B * k), "batch_claim")
             if round_hook is not None:
                 round_hook(k)
+            if transcripts is not None:
+                d_ch = self.device_challenges.data_ptr() + 16 * self.B * k
+                native.check(lib, lib.tp_fs_put_fp2s_dev(transcripts.data_ptr(), self.B, base + 64 * self.B * k, 4,
+                                                         s), "transcript put")
+                native.check(lib, lib.tp_fs_rand_ext_dev(transcripts.data_ptr(), self.B,
+                                                         ("sc-%d-%d" % (layer, k)).encode(), d_ch, s), "rand_ext")
+                native.check(lib, lib.tp_batch_fold_dev(b, d_ch), "batch_fold_dev")
+                launches += 2
+                continue
             native.check(lib, lib.tp_batch_fold(
                 b, ch[k].reshape(-1).ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))), "batch_fold")
         native.check(lib, lib.tp_batch_finish(b, self.wires.data_ptr(), self.fin_beta.data_ptr()),

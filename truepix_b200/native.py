@@ -84,6 +84,7 @@ GKR_SIGNATURES = {
     "tp_orion_commit_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
     "tp_orion_commit_pair": (_I32, [_VP, _VP, ctypes.c_longlong, _VP, _VP]),
     "tp_orion_set_leaf_chunks": (_I32, [_I32]),
+    "tp_batch_fold_dev": (_I32, [_VP, _VP]),
     "tp_fs_state_bytes": (_I32, []),
     "tp_fs_init": (_I32, [_VP, ctypes.c_char_p]),
     "tp_fs_put_u64s": (_I32, [_VP, _VP, ctypes.c_size_t]),
