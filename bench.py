@@ -689,7 +689,7 @@ def ours_arm(args, rank, world, local_rank):
         c, w, b, m = bprover.results(B - 1)
         res_ok = bool(c.any() and w.any() and m != (0, 0) and any(committer.root(B - 1)))
 
-    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = ref_gpu = None
+    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = ref_gpu = fs_rounds = None
     # The side measurements run once, at N = 1 (a scaling run holds every GPU
     # while rank 0 works; it only needs the step's value).
     extras = rank == 0 and world == 1
@@ -705,6 +705,7 @@ def ours_arm(args, rank, world, local_rank):
     if extras and not args.skip_e2e:
         e2e_ref = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
         ref_gpu = reference_gpu_lib(frames[0], layout, gt, i0, i1, z1, z2, point, chal)
+        fs_rounds = transcript_rounds(bprover, pix, z1s, z2s, pts, stream)
     if extras and not args.skip_serving:
         del bprover
         committer.rows = committer.trees = None
@@ -756,7 +757,7 @@ def ours_arm(args, rank, world, local_rank):
                             "every launch), whose shares match the serialised ncu launch list"
                             % len(committer.side),
             "ntt": ntt, "opening": opening, "zk": zk, "batched_uneven": uneven, "serving": serving, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
-            "reference_gpu_library": ref_gpu,
+            "reference_gpu_library": ref_gpu, "transcript_rounds": fs_rounds,
             "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
         }
         print(json.dumps(line), flush=True)
@@ -1183,6 +1184,72 @@ def release(srv):
     gc.collect()
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
+
+
+def transcript_rounds(bprover, pix, z1s, z2s, pts, stream, reps=3):
+    """The batched GKR input layer of the step's 64 frames with a Fiat-Shamir
+    transcript per frame (the reference's binary format, tp_fs_*): (host) every
+    round the claims come back to the host, each frame's host transcript puts
+    them and draws the fold challenge; (device) the transcripts live on the
+    device and the same happens there (tp_fs_*_dev, tp_batch_fold_dev). Host
+    wall clock per batch; both give the same challenges."""
+    import ctypes
+    import torch
+    lib = bprover.lib
+    B, R = bprover.B, bprover.max_rounds
+    nbytes = lib.tp_fs_state_bytes()
+    states = []
+    for f in range(B):
+        st = ctypes.create_string_buffer(nbytes)
+        lib.tp_fs_init(st, b"truepix")
+        v = np.array([f], np.uint64)
+        lib.tp_fs_put_u64s(st, v.ctypes.data, 1)
+        states.append(st)
+    init = b"".join(st.raw for st in states)
+    chal = np.zeros((R, B, 2), np.uint64)
+    claims_h = torch.zeros(B * 8, dtype=torch.int64).pin_memory()
+    re, im = ctypes.c_uint64(), ctypes.c_uint64()
+    hs = []
+
+    def hook(k):
+        claims_h.copy_(bprover.claims[k * B * 8:(k + 1) * B * 8], non_blocking=True)
+        stream.synchronize()
+        cl = claims_h.numpy().view(np.uint64).reshape(B, 4, 2)
+        label = ("sc-0-%d" % k).encode()
+        for f in range(B):
+            r, i = np.ascontiguousarray(cl[f, :, 0]), np.ascontiguousarray(cl[f, :, 1])
+            lib.tp_fs_put_fp2s(hs[f], r.ctypes.data, i.ctypes.data, 4)
+            lib.tp_fs_rand_ext(hs[f], label, ctypes.byref(re), ctypes.byref(im))
+            chal[k, f] = (re.value, im.value)
+
+    d_states = torch.empty(B * nbytes, dtype=torch.uint8, device=bprover.dev)
+    init_t = torch.from_numpy(np.frombuffer(init, np.uint8).copy())
+
+    def host_run():
+        hs[:] = [ctypes.create_string_buffer(init[f * nbytes:(f + 1) * nbytes], nbytes) for f in range(B)]
+        with torch.cuda.stream(stream):
+            bprover.prove(pix, z1s, z2s, pts, chal, round_hook=hook)
+        stream.synchronize()
+
+    def dev_run():
+        with torch.cuda.stream(stream):
+            d_states.copy_(init_t, non_blocking=True)
+            bprover.prove(pix, z1s, z2s, pts, None, transcripts=d_states)
+        stream.synchronize()
+
+    out = {}
+    for name, fn in (("host_transcripts", host_run), ("device_transcripts", dev_run)):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        out[name + "_frames_per_s"] = reps * B / (time.perf_counter() - t0)
+    got = bprover.device_challenges.cpu().numpy().view(np.uint64).reshape(R, B, 2)
+    out["same_challenges"] = bool(np.array_equal(got, chal))
+    out["what"] = ("batched GKR input layer of %d 1080p frames (%d rounds, beta, MLE) with one Fiat-Shamir "
+                   "transcript per frame: claims read back and challenges drawn on the host every round, vs "
+                   "put and drawn on the device; host wall clock" % (B, R))
+    return out
 
 
 def pinned_frame(a):
