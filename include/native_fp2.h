@@ -264,6 +264,28 @@ int tp_fs_put_fp2s_dev(void* d_states, int n, const void* d_values, int k, void*
 /* state i draws rand_ext(label) into d_out[i] (packed {re, im}) */
 int tp_fs_rand_ext_dev(void* d_states, int n, const char* label, void* d_out, void* stream);
 
+/* One VOLE-committed sumcheck round per frame, as the reference prover's round
+ * loop does it (circuitnizkvec_vole.py:396-418 with create_pok_temp :113-128 and
+ * create_eq_proof :220-234): the round polynomial's coefficients from the four
+ * claims at (0, 1, -1, 2) (util.interpolate_cubic), each committed with the next
+ * VOLE correlation (ExtVOLECommit.commit: d = c - u put into the transcript, tag
+ * v kept), the equality proof of the tags at 0 + 1 against the previous round's
+ * value (rand_ext("eq"), est_eq / est_val put), the fold challenge
+ * rand_ext(label) into d_chal[i], and the next previous value (the tags'
+ * polynomial at the challenge). Frame i's correlations: d_u / d_v[i * count ..
+ * (i + 1) * count) (packed {re, im}, the prover's u and v, one repetition). A
+ * VOLE state (tp_vole_state_bytes() = 160 bytes, device) per frame holds the
+ * next correlation index, the previous value and the running sums of tags and
+ * coefficients; a frame whose correlations run out is marked (its `bad` word)
+ * and left unchanged. d_proof (optional): per frame the four d and the equality
+ * value (5 packed Fp2), the round's proof elements. */
+int tp_vole_state_bytes(void);
+/* host: a fresh VOLE state (prev NULL: no previous value, the first round of a proof) */
+int tp_vole_state_init(void* state, uint64_t first_correlation, const uint64_t* prev);
+int tp_vole_round_dev(void* d_fs_states, void* d_vole_states, int n, const void* d_claims, const void* d_u,
+                      const void* d_v, long long count, const char* label, void* d_chal, void* d_proof,
+                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif

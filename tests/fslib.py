@@ -107,3 +107,52 @@ def replay_lib(lib, protocol, ops, state=None):
             assert lib.tp_fs_digest(st, d) == 0
             digs += d.raw
     return np.array(outs, np.uint64), digs, st
+
+
+# ---- VOLE-committed sumcheck round (circuitnizkvec_vole.py:396-418) ----------
+HALF, THIRD = 1152921504606846976, 1537228672809129301   # 2^-1, 3^-1 mod p
+
+
+def f2add(a, b): return ((a[0] + b[0]) % P61, (a[1] + b[1]) % P61)
+def f2sub(a, b): return ((a[0] - b[0]) % P61, (a[1] - b[1]) % P61)
+def f2mul(a, b): return ((a[0] * b[0] - a[1] * b[1]) % P61, (a[0] * b[1] + a[1] * b[0]) % P61)
+def f2scale(a, k): return (a[0] * k % P61, a[1] * k % P61)
+
+
+def interpolate_cubic(f0, f1, fm1, f2):
+    """util.interpolate_cubic: coefficients from the values at 0, 1, -1, 2"""
+    a = f2sub((0, 0), fm1)
+    b = f2scale(f2add(f1, fm1), HALF)
+    c = f2scale(f2add(f1, a), HALF)
+    d = f2scale(f2add(f2, a), THIRD)
+    c2 = f2sub(b, f0)
+    c3 = f2scale(f2sub(f2sub(d, c), c2), HALF)
+    return [f0, f2sub(c, c3), c2, c3]
+
+
+def vole_rounds_python(g, name):
+    """Replay of a golden case (tests/golden/vole_round_golden.npz)"""
+    T = PyTranscript("truepix")
+    T.u64s([int(x) for x in g[name + "_prefix"]])
+    u, v = g[name + "_u"], g[name + "_v"]
+    idx = int(g[name + "_start"][0])
+    prev = tuple(int(x) for x in g[name + "_prev0"]) if int(g[name + "_has_prev"][0]) else None
+    chals, vzs = [], []
+    for cl in g[name + "_claims"]:
+        f = [(int(a), int(b)) for a, b in cl]
+        outs = interpolate_cubic(*f)
+        tags = []
+        for c in outs:
+            tags.append((int(v[idx, 0]), int(v[idx, 1])))
+            d = f2sub(c, (int(u[idx, 0]), int(u[idx, 1])))
+            idx += 1
+            T.fp2(*d)
+        zp1 = f2add(f2add(f2add(f2add(tags[0], tags[1]), tags[2]), tags[3]), tags[0])
+        ch = T.ext("eq")
+        vz = f2mul(zp1, ch) if prev is None else f2mul(f2sub(prev, zp1), ch)
+        T.fp2(*vz)
+        vzs.append(vz)
+        r = T.ext("sc-0-%d" % len(chals))
+        chals.append(r)
+        prev = f2add(f2mul(f2add(f2mul(f2add(f2mul(tags[3], r), tags[2]), r), tags[1]), r), tags[0])
+    return np.array(chals, np.uint64), np.array(vzs, np.uint64), prev, T.h.digest(), idx

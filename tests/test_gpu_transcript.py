@@ -146,3 +146,102 @@ def test_batched_rounds_with_device_transcripts_match_host_transcripts(lib):
         st = ctypes.create_string_buffer(back[f * n:(f + 1) * n], n)
         assert lib.tp_fs_digest(st, d1) == 0 and lib.tp_fs_digest(hstates[f], d2) == 0
         assert d1.raw == d2.raw
+
+
+def _vole_case(g, name):
+    return {k[len(name) + 1:]: g[k] for k in g.files if k.startswith(name + "_")}
+
+
+def test_vole_round_kernel_matches_reference_vectors(lib):
+    """tp_vole_round_dev round after round on the golden cases (made from the
+    reference's util / ExtVOLECommit / FiatShamir): every challenge, equality
+    value, the final previous value, correlations used, running sums, digest."""
+    import os
+    import torch
+    from fslib import ROOT
+    g = np.load(os.path.join(ROOT, "tests", "golden", "vole_round_golden.npz"))
+    dev = torch.device("cuda", 0)
+    for name in ("r3", "r14", "r11_prev"):
+        c = _vole_case(g, name)
+        _, _, st = replay_lib(lib, "truepix", [["u64s", [int(x) for x in c["prefix"]]]])
+        vs = ctypes.create_string_buffer(lib.tp_vole_state_bytes())
+        prev = np.ascontiguousarray(c["prev0"], np.uint64)
+        assert lib.tp_vole_state_init(vs, int(c["start"][0]), prev.ctypes.data if c["has_prev"][0] else None) == 0
+        d_fs = torch.from_numpy(np.frombuffer(st.raw, np.uint8).copy()).to(dev)
+        d_vs = torch.from_numpy(np.frombuffer(vs.raw, np.uint8).copy()).to(dev)
+        d_u = torch.from_numpy(np.ascontiguousarray(c["u"]).view(np.int64).reshape(-1)).to(dev)
+        d_v = torch.from_numpy(np.ascontiguousarray(c["v"]).view(np.int64).reshape(-1)).to(dev)
+        count = c["u"].shape[0]
+        d_cl = torch.empty(8, dtype=torch.int64, device=dev)
+        d_ch = torch.empty(2, dtype=torch.int64, device=dev)
+        d_pf = torch.empty(10, dtype=torch.int64, device=dev)
+        s = torch.cuda.current_stream().cuda_stream
+        for rd, cl in enumerate(c["claims"]):
+            d_cl.copy_(torch.from_numpy(np.ascontiguousarray(cl).view(np.int64).reshape(-1)))
+            assert lib.tp_vole_round_dev(d_fs.data_ptr(), d_vs.data_ptr(), 1, d_cl.data_ptr(), d_u.data_ptr(),
+                                         d_v.data_ptr(), count, ("sc-0-%d" % rd).encode(), d_ch.data_ptr(),
+                                         d_pf.data_ptr(), s) == 0, lib.tp_last_error()
+            np.testing.assert_array_equal(d_ch.cpu().numpy().view(np.uint64), c["chals"][rd])
+            np.testing.assert_array_equal(d_pf.cpu().numpy().view(np.uint64)[8:], c["vzs"][rd])
+        w = d_vs.cpu().numpy()
+        idx = int(w[:8].view(np.uint64)[0])
+        has_prev, bad = w[8:16].view(np.uint32)
+        words = w[16:].view(np.uint64).reshape(9, 2)
+        assert idx == int(c["used"][0]) and bad == 0 and has_prev == 1
+        np.testing.assert_array_equal(words[0], c["prev"][0])
+        np.testing.assert_array_equal(words[1:5], c["v_elem"])
+        np.testing.assert_array_equal(words[5:9], c["out_elem"])
+        dg = ctypes.create_string_buffer(32)
+        st2 = ctypes.create_string_buffer(d_fs.cpu().numpy().tobytes(), len(st.raw))
+        assert lib.tp_fs_digest(st2, dg) == 0 and dg.raw == c["digest"].tobytes()
+
+
+def test_batched_vole_rounds_match_restatement_and_stop_when_correlations_run_out(lib):
+    """BatchFrameProver with per-frame transcripts and VOLE states: each frame's
+    challenges equal the restated round loop replayed on that frame's claims;
+    a frame given too few correlations is marked and draws nothing."""
+    import os
+    import torch
+    from truepix_b200.frame import BatchFrameProver, FrameLayout, pack_fp2
+    from fslib import ROOT, vole_rounds_python
+    c = np.load(os.path.join(ROOT, "tests", "golden", "circuits.npz"))
+    gt, i0, i1 = c["gray_type"], c["gray_in0"], c["gray_in1"]
+    B = 5
+    layout = FrameLayout.for_frame(180, 320)
+    nb = layout.n_copy_bits
+    rng = np.random.default_rng(5)
+    dev = torch.device("cuda", 0)
+    pix = [torch.from_numpy(rng.integers(0, 256, size=layout.copies * 384, dtype=np.uint8)).to(dev)
+           for _ in range(B)]
+    z1 = np.stack([rng.integers(0, P61, size=384, dtype=np.uint64) for _ in range(2)])
+    z2 = rng.integers(0, P61, size=(nb, 2), dtype=np.uint64)
+    pt = rng.integers(0, P61, size=(nb + 9, 2), dtype=np.uint64)
+    count = 4 * nb + 3
+    u = rng.integers(0, P61, size=(B, count, 2), dtype=np.uint64)
+    v = rng.integers(0, P61, size=(B, count, 2), dtype=np.uint64)
+    prefixes = [[f, 11] for f in range(B)]
+    fs = b"".join(replay_lib(lib, "truepix", [["u64s", p]])[2].raw for p in prefixes)
+    vsb = []
+    for f in range(B):
+        vs = ctypes.create_string_buffer(lib.tp_vole_state_bytes())
+        assert lib.tp_vole_state_init(vs, 3 if f != B - 1 else count - 4, None) == 0
+        vsb.append(vs.raw)
+    d_fs = torch.from_numpy(np.frombuffer(fs, np.uint8).copy()).to(dev)
+    vole = dict(states=torch.from_numpy(np.frombuffer(b"".join(vsb), np.uint8).copy()).to(dev),
+                u=torch.from_numpy(u.view(np.int64).reshape(-1)).to(dev),
+                v=torch.from_numpy(v.view(np.int64).reshape(-1)).to(dev), count=count)
+    prover = BatchFrameProver([layout] * B, gt, i0, i1)
+    prover.prove(pix, [z1] * B, torch.from_numpy(pack_fp2(z2[:, 0], z2[:, 1])).to(dev).repeat(B),
+                 torch.from_numpy(pack_fp2(pt[:, 0], pt[:, 1])).to(dev).repeat(B), None, transcripts=d_fs, vole=vole)
+    torch.cuda.synchronize()
+    ch = prover.device_challenges.cpu().numpy().view(np.uint64).reshape(nb, B, 2)
+    claims = prover.claims.cpu().numpy().view(np.uint64).reshape(nb, B, 4, 2)
+    for f in range(B - 1):
+        g = {"x_prefix": np.array(prefixes[f], np.uint64), "x_u": u[f], "x_v": v[f], "x_start": np.array([3]),
+             "x_prev0": np.zeros(2, np.uint64), "x_has_prev": np.array([0]), "x_claims": claims[:, f]}
+        want, _, _, _, used = vole_rounds_python(g, "x")
+        np.testing.assert_array_equal(ch[:, f], want)
+        assert used == 3 + 4 * nb
+    st = vole["states"].cpu().numpy()[(B - 1) * 160:B * 160]
+    assert st[12:16].view(np.uint32)[0] == 1       # the last frame ran out after one round
+    assert not ch[1:, B - 1].any()

@@ -221,7 +221,7 @@ class BatchFrameProver:
             self.torch.cuda.current_stream(self.dev).cuda_stream
 
     def prove(self, pixels, z1s, z2s_dev, points_dev, challenges: np.ndarray,
-              round_hook=None, transcripts=None, layer: int = 0) -> None:
+              round_hook=None, transcripts=None, layer: int = 0, vole=None) -> None:
         """pixels: one uint8 device tensor per frame; z1s: uint64 [2, n_gates] per
         frame; z2s_dev / points_dev: per padded size C, a packed Fp2 device tensor
         [frames of size C][log2 C] / [..][log2 W + log2 C], frames in batch order
@@ -233,7 +233,12 @@ class BatchFrameProver:
         frame's transcript puts its four claims and draws the fold challenge
         rand_ext("sc-<layer>-<round>") on the device (tp_fs_*_dev, tp_batch_fold_dev),
         with no host round trip; all frames must then have the same number of
-        rounds. The drawn challenges are left in self.device_challenges."""
+        rounds. The drawn challenges are left in self.device_challenges.
+        vole: with transcripts, run each round as the reference's VOLE-committed
+        round (tp_vole_round_dev): a dict of `states` (uint8 [B * 160], device),
+        `u`, `v` (int64 [B * count * 2], device: each frame's correlations) and
+        `count`; the round's proof elements (four commitments and the equality
+        value per frame) are left in self.device_proof [rounds][B][5] Fp2."""
         lib, s, b = self.lib, self._s(), self.handle
         if not isinstance(z2s_dev, dict):
             assert len(self.groups) == 1
@@ -267,6 +272,9 @@ class BatchFrameProver:
             if getattr(self, "device_challenges", None) is None:
                 self.device_challenges = self.torch.zeros(self.max_rounds * self.B * 2, dtype=self.torch.int64,
                                                           device=self.dev)
+            if vole is not None and getattr(self, "device_proof", None) is None:
+                self.device_proof = self.torch.zeros(self.max_rounds * self.B * 10, dtype=self.torch.int64,
+                                                     device=self.dev)
         else:
             ch = np.ascontiguousarray(challenges, np.uint64)
         l0 = lib.tp_batch_launches(b)
@@ -276,10 +284,17 @@ class BatchFrameProver:
                 round_hook(k)
             if transcripts is not None:
                 d_ch = self.device_challenges.data_ptr() + 16 * self.B * k
-                native.check(lib, lib.tp_fs_put_fp2s_dev(transcripts.data_ptr(), self.B, base + 64 * self.B * k, 4,
-                                                         s), "transcript put")
-                native.check(lib, lib.tp_fs_rand_ext_dev(transcripts.data_ptr(), self.B,
-                                                         ("sc-%d-%d" % (layer, k)).encode(), d_ch, s), "rand_ext")
+                label = ("sc-%d-%d" % (layer, k)).encode()
+                if vole is not None:
+                    native.check(lib, lib.tp_vole_round_dev(
+                        transcripts.data_ptr(), vole["states"].data_ptr(), self.B, base + 64 * self.B * k,
+                        vole["u"].data_ptr(), vole["v"].data_ptr(), vole["count"], label, d_ch,
+                        self.device_proof.data_ptr() + 80 * self.B * k, s), "vole round")
+                else:
+                    native.check(lib, lib.tp_fs_put_fp2s_dev(transcripts.data_ptr(), self.B,
+                                                             base + 64 * self.B * k, 4, s), "transcript put")
+                    native.check(lib, lib.tp_fs_rand_ext_dev(transcripts.data_ptr(), self.B, label, d_ch, s),
+                                 "rand_ext")
                 native.check(lib, lib.tp_batch_fold_dev(b, d_ch), "batch_fold_dev")
                 launches += 2
                 continue

@@ -86,6 +86,10 @@ GKR_SIGNATURES = {
     "tp_orion_set_leaf_chunks": (_I32, [_I32]),
     "tp_batch_fold_dev": (_I32, [_VP, _VP]),
     "tp_fs_state_bytes": (_I32, []),
+    "tp_vole_state_bytes": (_I32, []),
+    "tp_vole_state_init": (_I32, [_VP, _U64, _VP]),
+    "tp_vole_round_dev": (_I32, [_VP, _VP, _I32, _VP, _VP, _VP, ctypes.c_longlong, ctypes.c_char_p, _VP, _VP,
+                                 _VP]),
     "tp_fs_init": (_I32, [_VP, ctypes.c_char_p]),
     "tp_fs_put_u64s": (_I32, [_VP, _VP, ctypes.c_size_t]),
     "tp_fs_put_fp2s": (_I32, [_VP, _VP, _VP, ctypes.c_size_t]),
