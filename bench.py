@@ -1237,18 +1237,36 @@ def transcript_rounds(bprover, pix, z1s, z2s, pts, stream, reps=3):
             bprover.prove(pix, z1s, z2s, pts, None, transcripts=d_states)
         stream.synchronize()
 
+    count = 4 * R
+    vole = dict(states=torch.empty(B * lib.tp_vole_state_bytes(), dtype=torch.uint8, device=bprover.dev),
+                u=torch.randint(0, P61, (B * count * 2,), dtype=torch.int64, device=bprover.dev),
+                v=torch.randint(0, P61, (B * count * 2,), dtype=torch.int64, device=bprover.dev), count=count)
+    vs = ctypes.create_string_buffer(lib.tp_vole_state_bytes())
+    lib.tp_vole_state_init(vs, 0, None)
+    vole_init = torch.from_numpy(np.frombuffer(vs.raw * B, np.uint8).copy())
+
+    def vole_run():
+        with torch.cuda.stream(stream):
+            d_states.copy_(init_t, non_blocking=True)
+            vole["states"].copy_(vole_init, non_blocking=True)
+            bprover.prove(pix, z1s, z2s, pts, None, transcripts=d_states, vole=vole)
+        stream.synchronize()
+
     out = {}
-    for name, fn in (("host_transcripts", host_run), ("device_transcripts", dev_run)):
+    for name, fn in (("host_transcripts", host_run), ("device_transcripts", dev_run),
+                     ("device_vole_rounds", vole_run)):
         fn()
         t0 = time.perf_counter()
         for _ in range(reps):
             fn()
         out[name + "_frames_per_s"] = reps * B / (time.perf_counter() - t0)
+    dev_run()
     got = bprover.device_challenges.cpu().numpy().view(np.uint64).reshape(R, B, 2)
     out["same_challenges"] = bool(np.array_equal(got, chal))
     out["what"] = ("batched GKR input layer of %d 1080p frames (%d rounds, beta, MLE) with one Fiat-Shamir "
                    "transcript per frame: claims read back and challenges drawn on the host every round, vs "
-                   "put and drawn on the device; host wall clock" % (B, R))
+                   "put and drawn on the device; and the reference prover's VOLE-committed round on the device "
+                   "(interpolation, commitments, equality proof, challenge); host wall clock" % (B, R))
     return out
 
 
