@@ -246,6 +246,9 @@ int tp_mle_eval_base_noalloc(const void* d_inputs, const void* d_z, int n_z, voi
 int tp_fs_state_bytes(void);
 /* FiatShamir(q, protocol).__init__ (fiatshamir.py:27-74) for q = 2^61 - 1 */
 int tp_fs_init(void* state, const char* protocol);
+/* absorb raw bytes already in the transcript's encoding (fiatshamir.py:101-138:
+ * e.g. 0x02 || LE64 for an int inside a mixed list, 0x05 for None) */
+int tp_fs_absorb(void* state, const void* bytes, size_t n);
 /* put(list of ints < 2^64): the array('Q') path (fiatshamir.py:112-120) */
 int tp_fs_put_u64s(void* state, const uint64_t* values, size_t n);
 /* put(Fp2) for each (re[i], im[i]) in turn (fiatshamir.py:129-131) */

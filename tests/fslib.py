@@ -29,6 +29,52 @@ def scripts(g):
             yield name, protocol, ops
 
 
+def py_value(x, fp2=lambda re, im: ("fp2", re, im)):
+    """the JSON form of a put() argument in the golden scripts -> Python values:
+    {"fp2": [re, im]} is an Fp2 (built by `fp2`), {"tuple": [...]} a tuple,
+    {"dict": [[k, v], ...]} a dict"""
+    if isinstance(x, dict):
+        if "fp2" in x:
+            return fp2(int(x["fp2"][0]), int(x["fp2"][1]))
+        if "tuple" in x:
+            return tuple(py_value(v, fp2) for v in x["tuple"])
+        return {k: py_value(v, fp2) for k, v in x["dict"]}
+    if isinstance(x, list):
+        return [py_value(v, fp2) for v in x]
+    return x
+
+
+def _flat(vals):
+    for v in vals:
+        if isinstance(v, (list, tuple)) and not (isinstance(v, tuple) and v[:1] == ("fp2",)):
+            yield from _flat(v)
+        else:
+            yield v
+
+
+def encode_put(x):
+    """bytes a reference transcript absorbs for put(x) (fiatshamir.py:101-138, 168-186)"""
+    vals = py_value(x)
+    if isinstance(vals, dict):
+        vals = list(vals.items())
+    elif not isinstance(vals, list):
+        vals = [vals]
+    if vals and type(vals[0]) is int and all(type(v) is int and 0 <= v < 1 << 64 for v in vals):
+        return b"\x01" + struct.pack("<I", len(vals)) + b"".join(struct.pack("<Q", v) for v in vals)
+    out = b""
+    for e in _flat(vals):
+        if type(e) is int:
+            out += b"\x02" + struct.pack("<Q", e & ((1 << 64) - 1))
+        elif isinstance(e, tuple):
+            out += b"\x03" + struct.pack("<QQ", e[1], e[2])
+        elif isinstance(e, str):
+            out += b"\x04" + struct.pack("<I", len(e.encode())) + e.encode()
+        else:
+            assert e is None
+            out += b"\x05"
+    return out
+
+
 class PyTranscript:
     def __init__(self, protocol):
         self.h = hashlib.sha256(b"TruePix," + protocol.encode() + b"," + b"binhash1,")
@@ -70,6 +116,8 @@ def replay_python(protocol, ops):
                 t.fp2(re, im)
         elif op[0] == "str":
             t.str(op[1])
+        elif op[0] == "put_py":
+            t.h.update(encode_put(op[1]))
         elif op[0] == "ext":
             outs += list(t.ext(op[1]))
         elif op[0] == "scalar":
@@ -97,6 +145,9 @@ def replay_lib(lib, protocol, ops, state=None):
             assert lib.tp_fs_put_fp2s(st, r.ctypes.data, i.ctypes.data, r.size) == 0
         elif op[0] == "str":
             assert lib.tp_fs_put_str(st, op[1].encode()) == 0
+        elif op[0] == "put_py":
+            b = encode_put(op[1])
+            assert lib.tp_fs_absorb(st, b, len(b)) == 0
         elif op[0] == "ext":
             assert lib.tp_fs_rand_ext(st, op[1].encode(), ctypes.byref(re), ctypes.byref(im)) == 0
             outs += [re.value, im.value]

@@ -40,10 +40,32 @@ def scripts():
         ops.append(["scalar"])
         ops.append(["digest"])
     out.append(("boundaries", "truepix", ops))
+    # put() of mixed Python values through the general encoder (fiatshamir.py:122-138):
+    # {"fp2": [re, im]} stands for an Fp2, {"tuple": [...]} for a tuple, {"dict": [[k, v]...]} for a dict
+    fp = lambda: {"fp2": r(2)}
+    ops = [["put_py", ["private_input_omitted", 384]], ["put_py", None], ["put_py", {"tuple": [fp(), fp()]}],
+           ["put_py", [fp(), [fp(), 7, "s"], {"tuple": [None, 5]}]], ["put_py", {"dict": [["a", 1], ["b", fp()]]}],
+           ["put_py", 12345], ["put_py", [1, 2, (1 << 64) - 1]], ["put_py", [3, "mixed", 4]],
+           ["put_py", {"fp2": [0, P61 - 1]}], ["ext", "gkr_input_point"], ["put_py", [-1, 5]], ["scalar"],
+           ["digest"]]
+    out.append(("mixed_puts", "truepix", ops))
     # another protocol name and many draws in a row
     ops = [["ext", "pok-%d" % k] for k in range(40)] + [["digest"]]
     out.append(("draws", "orion-opening", ops))
     return out
+
+
+def py_value(x, Fp2):
+    """the JSON form of a put() argument -> Python values with the given Fp2 type"""
+    if isinstance(x, dict):
+        if "fp2" in x:
+            return Fp2(int(x["fp2"][0]), int(x["fp2"][1]), P61)
+        if "tuple" in x:
+            return tuple(py_value(v, Fp2) for v in x["tuple"])
+        return {k: py_value(v, Fp2) for k, v in x["dict"]}
+    if isinstance(x, list):
+        return [py_value(v, Fp2) for v in x]
+    return x
 
 
 def run(protocol, ops):
@@ -60,6 +82,8 @@ def run(protocol, ops):
                 fs.put(Fp2(re, im, P61))
         elif op[0] == "str":
             fs.put(op[1])
+        elif op[0] == "put_py":
+            fs.put(py_value(op[1], Fp2))
         elif op[0] == "ext":
             c = fs.rand_ext(op[1])
             outs += [int(c.real), int(c.imag)]

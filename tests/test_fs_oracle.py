@@ -13,7 +13,7 @@ def test_transcript_restatement_matches_reference_vectors():
         np.testing.assert_array_equal(outs, g["fsout_" + name])
         assert digs == g["fsdigest_" + name].tobytes(), name
         n += 1
-    assert n == 3
+    assert n == 4
 
 
 def test_vole_round_restatement_matches_reference_vectors():

@@ -160,6 +160,18 @@ int tp_fs_init(void* state, const char* protocol)
     return 0;
 }
 
+int tp_fs_absorb(void* state, const void* bytes, size_t n)
+{
+    tp::clear_error();
+    if (!state_ok(state, "tp_fs_absorb")) return -1;
+    if (n && !bytes) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_fs_absorb: null bytes");
+        return -1;
+    }
+    tp::fs::absorb(*static_cast<State*>(state), static_cast<const uint8_t*>(bytes), n);
+    return 0;
+}
+
 int tp_fs_put_u64s(void* state, const uint64_t* v, size_t n)
 {
     tp::clear_error();

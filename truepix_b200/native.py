@@ -91,6 +91,7 @@ GKR_SIGNATURES = {
     "tp_vole_round_dev": (_I32, [_VP, _VP, _I32, _VP, _VP, _VP, ctypes.c_longlong, ctypes.c_char_p, _VP, _VP,
                                  _VP]),
     "tp_fs_init": (_I32, [_VP, ctypes.c_char_p]),
+    "tp_fs_absorb": (_I32, [_VP, _VP, ctypes.c_size_t]),
     "tp_fs_put_u64s": (_I32, [_VP, _VP, ctypes.c_size_t]),
     "tp_fs_put_fp2s": (_I32, [_VP, _VP, _VP, ctypes.c_size_t]),
     "tp_fs_put_str": (_I32, [_VP, ctypes.c_char_p]),
