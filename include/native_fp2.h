@@ -223,6 +223,27 @@ void tp_timer_disable(void);
 void tp_timer_reset(void);
 int tp_timer_read(float* ms, int* tags, int max_pairs);
 
+/* ---- circuit evaluation: the prover's output vector ----
+ * Replaces ArithCircuitIncrementalBuilder.run (libTruePix/arithcircuitbuilder.py:71-108,
+ * arithcircuit.py:121-131, 172-181) as called by CircuitProver.set_inputs
+ * (circuitprover.py:82-98) for the one-layer TruePix circuits, and the output
+ * vector circuitnizkvec_vole.py:351-355 puts into the transcript: for each real
+ * copy c the values of gates 0..n_gates-1 on the copy's inputs, at
+ * d_out[c << out_bits + g] with out_bits = tp_circuit_out_bits(n_gates) =
+ * ceil(log2 n_gates); every other element (a copy's padding outputs, the copies
+ * n_copies..n_copies_padded-1) is zero. u64, canonical mod 2^61 - 1; the bytes
+ * of the array are the LE64 encoding the transcript absorbs (tp_fs_put_u64s).
+ * Inputs in the layout of tp_table_from_pixels (d_pixels: n_copies * copy_size
+ * bytes, constant wire const_idx, -1 for none). Gate values as in
+ * native_fp2_core.hpp:32-51 (types 0..12). n_gates <= 960, n_wires <= 16384;
+ * gate tables in host memory (copied into the launch). d_out: n_copies_padded
+ * << out_bits u64. Asynchronous on `stream`. */
+int tp_circuit_out_bits(int n_gates);
+int tp_circuit_outputs_pixels_dev(const void* d_pixels, int n_copies, int n_copies_padded, int copy_size,
+                                  int n_wires, int const_idx, uint64_t const_val, int n_gates,
+                                  const int* gate_type, const int* in0, const int* in1, void* d_out,
+                                  void* stream);
+
 /* No counterpart in the reference. tp_mle_eval_base_dev for callers that cannot
  * allocate device memory (their GPU memory belongs to another allocator, or a
  * time-critical loop cannot afford cudaMalloc/cudaFree): it calls no allocator

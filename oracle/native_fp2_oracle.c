@@ -312,3 +312,66 @@ void oracle_fp2_early_destroy(void* h)
     free(s->b_re); free(s->b_im);
     free(s);
 }
+
+/* ---- circuit evaluation (the prover's output vector) ----------------------
+ * arithcircuit.py:20-110: the C gates on base-field values, each result reduced
+ * like Python's % (non-negative); types by the native index (native_fp2_bridge.py
+ * :450-472), with 3 / 4 the left / right multiplexer input as in
+ * native_fp2_core.hpp:38-39. */
+static u64 modp(__int128 v)
+{
+    __int128 r = v % (__int128)P61;
+    return (u64)(r < 0 ? r + (__int128)P61 : r);
+}
+
+static u64 cgate(int tp, u64 a, u64 b)
+{
+    const __int128 x = (__int128)a, y = (__int128)b;
+    switch (tp) {
+    case 0: return modp(x * y);
+    case 1: return modp(x + y);
+    case 2: return modp(x - y);
+    case 3: return a;
+    case 4: return b;
+    case 5: return modp(x + y - x * y);
+    case 6: return modp(x + y - 2 * x * y);
+    case 7: return modp(1 - x);
+    case 8: return modp(1 - x * y);
+    case 9: return modp(1 + x * y - x - y);
+    case 10: return modp(1 + 2 * x * y - x - y);
+    case 11: return modp((1 - x) * y);
+    default: return a;
+    }
+}
+
+/* ArithCircuitBuilder.run over the copies of a frame (arithcircuitbuilder.py:36-46,
+ * arithcircuit.py:121-131, 160-181) and the output vector of circuitnizkvec_vole.py
+ * :351-355: copy c's input layer is its copy_size bytes, const_val at const_idx
+ * (-1: none), zeros up to n_wires; its outputs are the gate values padded with
+ * zeros to 2^ceil(log2 n_gates); the copies are concatenated and padded with zeros
+ * to n_copies_padded copies. out: n_copies_padded << ceil(log2 n_gates) values. */
+int oracle_circuit_outputs(const unsigned char* pix, int n_copies, int n_copies_padded, int copy_size,
+                           int n_wires, int const_idx, u64 const_val, int n_gates, const int* type,
+                           const int* in0, const int* in1, u64* out)
+{
+    int bits = 0;
+    if (n_copies < 1 || n_copies_padded < n_copies || copy_size > n_wires || n_gates < 1) return -1;
+    while ((1 << bits) < n_gates) ++bits;
+    const size_t opc = (size_t)1 << bits;
+    u64* in = (u64*)calloc((size_t)n_wires, sizeof(u64));
+    if (!in) return -1;
+    memset(out, 0, (size_t)n_copies_padded * opc * sizeof(u64));
+    for (int c = 0; c < n_copies; ++c) {
+        for (int w = 0; w < n_wires; ++w)
+            in[w] = w < copy_size ? (u64)pix[(size_t)c * copy_size + w] : (w == const_idx ? const_val : 0);
+        for (int g = 0; g < n_gates; ++g) {
+            if (in0[g] < 0 || in0[g] >= n_wires || in1[g] < 0 || in1[g] >= n_wires) {
+                free(in);
+                return -1;
+            }
+            out[(size_t)c * opc + g] = cgate(type[g], in[in0[g]], in[in1[g]]);
+        }
+    }
+    free(in);
+    return 0;
+}

@@ -245,3 +245,68 @@ def test_batched_vole_rounds_match_restatement_and_stop_when_correlations_run_ou
     st = vole["states"].cpu().numpy()[(B - 1) * 160:B * 160]
     assert st[12:16].view(np.uint32)[0] == 1       # the last frame ran out after one round
     assert not ch[1:, B - 1].any()
+
+
+def _random_absorbs(lib, rng, trials):
+    """random mixes of raw absorbs, int-list puts and Fp2 puts of many lengths
+    (block-boundary cases) through the host entry points, against hashlib"""
+    import hashlib
+    import struct
+    d = ctypes.create_string_buffer(32)
+    for trial in range(trials):
+        st = ctypes.create_string_buffer(lib.tp_fs_state_bytes())
+        assert lib.tp_fs_init(st, b"truepix") == 0
+        h = hashlib.sha256(b"TruePix,truepix,binhash1,")
+        for _ in range(int(rng.integers(1, 6))):
+            n = int(rng.choice([0, 1, 5, 55, 63, 64, 65, 127, 128, 129, 1000, 4096, 9999]))
+            kind = int(rng.integers(0, 3))
+            if kind == 0:
+                b = rng.integers(0, 256, size=n, dtype=np.uint8).tobytes()
+                assert lib.tp_fs_absorb(st, b, len(b)) == 0
+                h.update(b)
+            elif kind == 1 and n:
+                v = rng.integers(0, 2 ** 63, size=n, dtype=np.uint64) * np.uint64(2) + np.uint64(1)
+                assert lib.tp_fs_put_u64s(st, v.ctypes.data, n) == 0
+                h.update(b"\x01" + struct.pack("<I", n) + v.tobytes())
+            else:
+                re = rng.integers(0, P61, size=n, dtype=np.uint64)
+                im = rng.integers(0, P61, size=n, dtype=np.uint64)
+                assert lib.tp_fs_put_fp2s(st, re.ctypes.data, im.ctypes.data, n) == 0
+                h.update(b"".join(b"\x03" + struct.pack("<QQ", int(a), int(c)) for a, c in zip(re, im)))
+        assert lib.tp_fs_digest(st, d) == 0
+        assert d.raw == h.digest(), trial
+
+
+def test_host_bulk_absorb_matches_hashlib(lib):
+    """Long absorbs are compressed block by block straight from the caller's
+    bytes (with the x86 SHA extensions where the CPU has them): same digests as
+    hashlib for every split, and an 8 MiB int list (a frame's circuit outputs are
+    64 MiB) in one put."""
+    import hashlib
+    import struct
+    rng = np.random.default_rng(5)
+    _random_absorbs(lib, rng, 120)
+    a = rng.integers(0, 256, size=1 << 20, dtype=np.uint64)
+    st = ctypes.create_string_buffer(lib.tp_fs_state_bytes())
+    assert lib.tp_fs_init(st, b"truepix") == 0
+    assert lib.tp_fs_put_u64s(st, a.ctypes.data, a.size) == 0
+    d = ctypes.create_string_buffer(32)
+    assert lib.tp_fs_digest(st, d) == 0
+    assert d.raw == hashlib.sha256(b"TruePix,truepix,binhash1,\x01" + struct.pack("<I", a.size) + a.tobytes()).digest()
+
+
+def test_host_portable_compression_matches_hashlib():
+    """the same with the portable compression (TRUEPIX_HOST_SHA_PORTABLE=1), in a
+    child process so that the choice is made afresh"""
+    import os
+    import subprocess
+    import sys
+    from fslib import ROOT
+    code = ("import numpy as np, sys; sys.path[:0] = [%r, %r]\n"
+            "from truepix_b200 import native\n"
+            "import test_gpu_transcript as t\n"
+            "t._random_absorbs(native.gkr(require_device=False), np.random.default_rng(6), 60)\n"
+            % (ROOT, os.path.join(ROOT, "tests")))
+    env = dict(os.environ, TRUEPIX_HOST_SHA_PORTABLE="1")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]

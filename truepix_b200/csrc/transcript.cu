@@ -4,15 +4,20 @@
 // transcripts of a batch can absorb their claims and draw their next challenges
 // without a round trip to the host.
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "runtime.h"
 #include "transcript.cuh"
 #include "../../include/native_fp2.h"
 
+extern "C" int tp_host_sha_ext_available(void);
+extern "C" void tp_host_sha_ext_blocks(uint32_t h[8], const uint8_t* p, size_t nblocks, const uint32_t K[64]);
+
 namespace {
 
 using tp::fs::State;
+static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "the LE64 encoding is the host's own u64 bytes");
 
 constexpr int kMaxLabel = 64;
 
@@ -127,6 +132,62 @@ __global__ void vole_round_kernel(State* __restrict__ st, VoleState* __restrict_
     chal[i] = r;
 }
 
+// ---- host absorbs: whole blocks compressed straight from the caller's bytes,
+// with the x86 SHA extensions where the CPU has them (sha256_host.cpp) ----------
+constexpr tp::sha::Tables kHostTables = tp::sha::make_tables();
+
+// TRUEPIX_HOST_SHA_PORTABLE=1 selects the portable compression on any CPU
+bool host_sha_ext()
+{
+    static const bool ok = tp_host_sha_ext_available() != 0 && !getenv("TRUEPIX_HOST_SHA_PORTABLE");
+    return ok;
+}
+
+void host_blocks(uint32_t h[8], const uint8_t* p, size_t nblocks)
+{
+    if (host_sha_ext()) {
+        tp_host_sha_ext_blocks(h, p, nblocks, kHostTables.k);
+        return;
+    }
+    for (size_t b = 0; b < nblocks; ++b, p += 64) {
+        uint32_t w[16];
+        for (int i = 0; i < 16; ++i)
+            w[i] = ((uint32_t)p[4 * i] << 24) | ((uint32_t)p[4 * i + 1] << 16) | ((uint32_t)p[4 * i + 2] << 8) |
+                   (uint32_t)p[4 * i + 3];
+        tp::sha::compress(h, w, tp::sha::AddAlu{});
+    }
+}
+
+// the same bytes and state as tp::fs::absorb
+void host_absorb(State& s, const uint8_t* p, uint64_t n)
+{
+    s.total += n;
+    if (s.nbuf) {
+        const uint64_t take = n < 64u - s.nbuf ? n : 64u - s.nbuf;
+        memcpy(s.buf + s.nbuf, p, take);
+        s.nbuf += (uint32_t)take;
+        p += take;
+        n -= take;
+        if (s.nbuf < 64) return;
+        host_blocks(s.h, s.buf, 1);
+        s.nbuf = 0;
+    }
+    const uint64_t nb = n / 64;
+    if (nb) {
+        host_blocks(s.h, p, nb);
+        p += 64 * nb;
+        n -= 64 * nb;
+    }
+    memcpy(s.buf, p, n);
+    s.nbuf = (uint32_t)n;
+}
+
+void host_absorb_header(State& s, uint8_t tag, uint32_t n)
+{
+    const uint8_t b[5] = {tag, (uint8_t)n, (uint8_t)(n >> 8), (uint8_t)(n >> 16), (uint8_t)(n >> 24)};
+    host_absorb(s, b, 5);
+}
+
 bool state_ok(const void* state, const char* who)
 {
     if (!state) {
@@ -168,7 +229,7 @@ int tp_fs_absorb(void* state, const void* bytes, size_t n)
         tp::set_error(tp::TP_ERR_ARG, "tp_fs_absorb: null bytes");
         return -1;
     }
-    tp::fs::absorb(*static_cast<State*>(state), static_cast<const uint8_t*>(bytes), n);
+    host_absorb(*static_cast<State*>(state), static_cast<const uint8_t*>(bytes), n);
     return 0;
 }
 
@@ -180,7 +241,9 @@ int tp_fs_put_u64s(void* state, const uint64_t* v, size_t n)
         tp::set_error(tp::TP_ERR_ARG, "tp_fs_put_u64s: need 1 <= n < 2^32 values");
         return -1;
     }
-    tp::fs::put_u64s(*static_cast<State*>(state), v, n);
+    State& s = *static_cast<State*>(state);
+    host_absorb_header(s, 0x01, (uint32_t)n);
+    host_absorb(s, reinterpret_cast<const uint8_t*>(v), 8 * (uint64_t)n);
     return 0;
 }
 
@@ -193,7 +256,18 @@ int tp_fs_put_fp2s(void* state, const uint64_t* re, const uint64_t* im, size_t n
         return -1;
     }
     State& s = *static_cast<State*>(state);
-    for (size_t i = 0; i < n; ++i) tp::fs::put_fp2(s, re[i], im[i]);
+    uint8_t buf[17 * 240];
+    size_t nb = 0;
+    for (size_t i = 0; i < n; ++i) {
+        buf[nb] = 0x03;
+        memcpy(buf + nb + 1, re + i, 8);
+        memcpy(buf + nb + 9, im + i, 8);
+        nb += 17;
+        if (nb == sizeof(buf) || i + 1 == n) {
+            host_absorb(s, buf, nb);
+            nb = 0;
+        }
+    }
     return 0;
 }
 
@@ -205,7 +279,10 @@ int tp_fs_put_str(void* state, const char* str)
         tp::set_error(tp::TP_ERR_ARG, "tp_fs_put_str: null string");
         return -1;
     }
-    tp::fs::put_str(*static_cast<State*>(state), reinterpret_cast<const uint8_t*>(str), (uint32_t)strlen(str));
+    State& s = *static_cast<State*>(state);
+    const size_t len = strlen(str);
+    host_absorb_header(s, 0x04, (uint32_t)len);
+    host_absorb(s, reinterpret_cast<const uint8_t*>(str), len);
     return 0;
 }
 

@@ -5,7 +5,9 @@ library's transcript (tp_fs_*, include/native_fp2.h).
 Same constructor and methods (put / take with the io and trans queues,
 hash_update, hash_append, rand_scalar, rand_ext, to_string / from_string,
 proof_size, unpack_proof), same bytes absorbed and the same challenges for
-q = 2^61 - 1 with the binary encoding (fiatshamir.py:101-138). In addition the
+q = 2^61 - 1 with the binary encoding (fiatshamir.py:101-138). put() also takes
+a 1-D numpy integer array, absorbed as the list of its values (the circuit
+outputs of truepix_b200.frame.circuit_outputs, copied to the host). In addition the
 running state is a 120-byte buffer (`state()` / `set_state()`): a transcript
 begun here can continue on the device, one state per frame, where the batched
 rounds put their claims and draw their challenges (tp_fs_*_dev,
@@ -19,6 +21,8 @@ import ctypes
 import pickle
 import struct
 from collections import deque
+
+import numpy as np
 
 from . import native
 
@@ -91,6 +95,9 @@ class FiatShamir:
             native.check(self.lib, self.lib.tp_fs_absorb(self._st, b, len(b)), "tp_fs_absorb")
 
     def hash_update(self, vals):
+        if isinstance(vals, np.ndarray):
+            self._hash_array(vals)
+            return
         if isinstance(vals, list) and vals and type(vals[0]) is int:
             try:
                 a = array.array("Q", vals)
@@ -114,6 +121,19 @@ class FiatShamir:
                 raise TypeError("unsupported FS element: %r" % (type(elm),))
         self._absorb(bytes(buf))
 
+    def _hash_array(self, a: np.ndarray) -> None:
+        """A 1-D integer array absorbs as the list of its values would
+        (a frame's circuit outputs, 2^23 values at 1080p, without a Python list)."""
+        if a.ndim != 1 or a.dtype.kind not in "iu":
+            raise TypeError("unsupported FS array: %r %r" % (a.dtype, a.shape))
+        if a.size == 0:
+            return
+        if a.dtype.kind == "i" and (a < 0).any():
+            self.hash_update(a.tolist())
+            return
+        a = np.ascontiguousarray(a.astype(np.uint64, copy=False))
+        native.check(self.lib, self.lib.tp_fs_put_u64s(self._st, a.ctypes.data, a.size), "tp_fs_put_u64s")
+
     def hash_append(self, elm):
         self.hash_update([elm])
 
@@ -121,7 +141,7 @@ class FiatShamir:
         if not self.can_put:
             raise AssertionError("Cannot put values into an input FS transcript")
         call_items = isinstance(vals, dict)
-        if not call_items and not isinstance(vals, list):
+        if not call_items and not isinstance(vals, (list, np.ndarray)):
             vals = [vals]
         (self.io if is_io else self.trans).append(vals)
         self.hash_update(list(vals.items()) if call_items else vals)

@@ -67,6 +67,33 @@ def pack_fp2(re: np.ndarray, im: np.ndarray) -> np.ndarray:
     return np.stack([re.astype(np.uint64), im.astype(np.uint64)], axis=1).reshape(-1).view(np.int64)
 
 
+def circuit_outputs(pixels, layout: FrameLayout, gate_type, in0, in1, out=None, stream=None):
+    """The prover's output vector of a frame, on the device (int64 tensor holding
+    u64 values): for each real copy the circuit's gate values on the copy's
+    inputs, padded per copy to 2^ceil(log2 gates), the copies padded with zeros
+    to layout.padded_copies -- what circuitnizkvec_vole.py:351-355 puts into the
+    transcript (FiatShamir.put(values, True)). pixels: uint8 device tensor of
+    layout.copies * layout.copy_size bytes. Asynchronous on `stream`."""
+    import torch
+    lib = native.gkr()
+    gt, i0, i1 = (np.ascontiguousarray(a, np.int32) for a in (gate_type, in0, in1))
+    bits = lib.tp_circuit_out_bits(len(gt))
+    n = layout.padded_copies << bits
+    if pixels.dtype != torch.uint8 or not pixels.is_cuda or pixels.numel() < layout.copies * layout.copy_size:
+        raise ValueError("pixels: uint8 device tensor of copies * copy_size bytes expected")
+    if out is None:
+        out = torch.empty(n, dtype=torch.int64, device=pixels.device)
+    elif out.dtype != torch.int64 or out.numel() < n or not out.is_contiguous():
+        raise ValueError("out: contiguous int64 tensor of %d elements expected" % n)
+    s = stream.cuda_stream if stream is not None else torch.cuda.current_stream(pixels.device).cuda_stream
+    I32P = ctypes.POINTER(ctypes.c_int)
+    native.check(lib, lib.tp_circuit_outputs_pixels_dev(
+        pixels.data_ptr(), layout.copies, layout.padded_copies, layout.copy_size, layout.n_wires,
+        layout.const_idx, layout.const_val, len(gt), gt.ctypes.data_as(I32P), i0.ctypes.data_as(I32P),
+        i1.ctypes.data_as(I32P), out.data_ptr(), s), "tp_circuit_outputs_pixels_dev")
+    return out
+
+
 class GkrInputLayerProver:
     """Holds device buffers for one frame size and proves frames into them."""
 
