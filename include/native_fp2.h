@@ -223,6 +223,37 @@ void tp_timer_disable(void);
 void tp_timer_reset(void);
 int tp_timer_read(float* ms, int* tags, int max_pairs);
 
+/* ---- late rounds and line projection of the input layer ----
+ * Replaces the reference's Python late rounds, LayerProver.compute_outputs /
+ * next_round for rounds nCopyBits..nCopyBits + 2n - 1 (libTruePix/layerprover.py
+ * :231-290, gateprover.py:105-185, layercompute.py:16-150) and the final
+ * LayerComputeH output (layercompute.py:152-247), for n_frames frames in one
+ * launch (one CTA each). Per frame, from the early phase's results: d_wires
+ * [n_frames][2^n_in_bits] packed Fp2 (tp_batch_finish's wires), d_beta
+ * [n_frames] (its beta); d_gate_weights: the gates' z1 eq values, [n_frames]
+ * [n_gates] packed Fp2 with weights_per_frame = 1, or one [n_gates] vector for
+ * all frames with 0. Gate tables in host memory (n_gates <= 768, n_in_bits <= 9).
+ * Challenges, one of:
+ *   d_challenges [n_frames][2 n_in_bits] given (the other transcript arguments NULL);
+ *   d_challenges NULL: each round is the reference's VOLE-committed round
+ *     (circuitnizkvec_vole.py:396-418) on the round's three coefficients, with
+ *     the frame's transcript d_fs_states[i] (tp_fs_state_bytes() each), VOLE
+ *     state d_vole_states[i] (tp_vole_state_bytes() each, continuing from the
+ *     early rounds) and correlations d_u / d_v [n_frames][count] packed Fp2, the
+ *     challenge rand_ext("sc-<layer>-<round0 + round>"); the states are updated
+ *     in place. A frame whose correlations run out stops (VOLE state bad = 1).
+ * Outputs: d_coefs [n_frames][2 n_in_bits][3] (util.interpolate_quadratic of
+ * the values at 0, 1, -1), d_line [n_frames][n_in_bits + 1] (coefficients,
+ * constant first, of the input values on the line w1 + t (w2 - w1): the
+ * project_line output the layer's final proof commits), d_challenges_out
+ * [n_frames][2 n_in_bits], d_proof (VOLE mode, optional) [n_frames][2 n_in_bits]
+ * [4] (three commitments d, the equality value). Asynchronous on `stream`. */
+int tp_late_rounds_dev(int n_frames, int n_in_bits, int n_gates, const int* gate_type, const int* in0,
+                       const int* in1, const void* d_wires, const void* d_beta, const void* d_gate_weights,
+                       int weights_per_frame, const void* d_challenges, void* d_fs_states, void* d_vole_states,
+                       const void* d_u, const void* d_v, long long count, int layer, int round0, void* d_coefs,
+                       void* d_line, void* d_challenges_out, void* d_proof, void* stream);
+
 /* ---- circuit evaluation: the prover's output vector ----
  * Replaces ArithCircuitIncrementalBuilder.run (libTruePix/arithcircuitbuilder.py:71-108,
  * arithcircuit.py:121-131, 172-181) as called by CircuitProver.set_inputs

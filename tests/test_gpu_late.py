@@ -1,0 +1,250 @@
+"""Late rounds and line projection on the device (tp_late_rounds_dev,
+BatchFrameProver.prove_late) against the reference: given challenges, bit-exact
+with vectors made by the reference's own LayerProver (tests/golden/
+late_golden.npz); the VOLE-committed rounds, bit-exact with the reference's
+LayerProver + ExtVOLECommit + FiatShamir chain (tests/golden/
+layer_vole_golden.npz: coefficients, commitments, equality values, challenges,
+line, VOLE state, transcript digest); batches against the oracle; whole 1080p
+frames after the device early rounds, against the oracle and against the
+multilinear extension of the frame's bytes at the two late points."""
+import ctypes
+import struct
+
+import numpy as np
+import pytest
+
+from latelib import golden_cases, oracle, pairs
+
+pytestmark = pytest.mark.gpu
+
+I32P = ctypes.POINTER(ctypes.c_int)
+P61 = (1 << 61) - 1
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from truepix_b200 import native
+    return native.gkr()
+
+
+def dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, np.uint64).reshape(-1).view(np.int64).copy()).cuda()
+
+
+def host(t, shape):
+    return t.cpu().numpy().view(np.uint64).reshape(shape)
+
+
+def run_given(lib, n, gates, wires, beta, zg, chal, n_frames=1, per_frame=1):
+    import torch
+    gt, i0, i1 = (np.ascontiguousarray(r, np.int32) for r in gates)
+    d_w, d_b, d_z, d_c = dev(wires), dev(beta), dev(zg), dev(chal)
+    coefs = torch.zeros(n_frames * 12 * n, dtype=torch.int64, device="cuda")
+    line = torch.zeros(n_frames * 2 * (n + 1), dtype=torch.int64, device="cuda")
+    cho = torch.zeros(n_frames * 4 * n, dtype=torch.int64, device="cuda")
+    rc = lib.tp_late_rounds_dev(n_frames, n, gt.size, gt.ctypes.data_as(I32P), i0.ctypes.data_as(I32P),
+                                i1.ctypes.data_as(I32P), d_w.data_ptr(), d_b.data_ptr(), d_z.data_ptr(), per_frame,
+                                d_c.data_ptr(), None, None, None, None, 0, 0, 0, coefs.data_ptr(), line.data_ptr(),
+                                cho.data_ptr(), None, None)
+    assert rc == 0, lib.tp_last_error()
+    torch.cuda.synchronize()
+    return (host(coefs, (n_frames, 6 * n, 2)), host(line, (n_frames, n + 1, 2)), host(cho, (n_frames, 2 * n, 2)))
+
+
+def test_given_challenges_match_reference_layer_prover(lib):
+    n_cases = 0
+    for c in golden_cases():
+        n, nb = c["n_in_bits"], c["n_copy_bits"]
+        coefs, line, cho = run_given(lib, n, c["gates"], c["wires"], c["beta"], c["zg"], c["chal"][nb:])
+        np.testing.assert_array_equal(coefs[0], c["late"], err_msg=c["name"])
+        np.testing.assert_array_equal(line[0], c["final"], err_msg=c["name"])
+        np.testing.assert_array_equal(cho[0], c["chal"][nb:])
+        n_cases += 1
+    assert n_cases == 6
+
+
+def test_vole_rounds_match_reference_chain(lib):
+    import torch
+    from layervole import cases, early_transcript, vole_state_fields, vole_state_mid
+    n_cases = 0
+    for c in cases():
+        n, nb = c["n_in_bits"], c["nb"]
+        st, ch = early_transcript(lib, c)
+        assert [list(x) for x in ch] == [[int(a), int(b)] for a, b in c["chal"][:nb]]
+        d_st = torch.frombuffer(bytearray(st.raw), dtype=torch.uint8).cuda()
+        d_vs = torch.frombuffer(bytearray(vole_state_mid(c)), dtype=torch.uint8).cuda()
+        gt, i0, i1 = (np.ascontiguousarray(r, np.int32) for r in c["gates"])
+        d_w, d_b, d_z, d_u, d_v = dev(c["wires"]), dev(c["beta"]), dev(c["zg"]), dev(c["u"]), dev(c["v"])
+        coefs = torch.zeros(12 * n, dtype=torch.int64, device="cuda")
+        line = torch.zeros(2 * (n + 1), dtype=torch.int64, device="cuda")
+        cho = torch.zeros(4 * n, dtype=torch.int64, device="cuda")
+        proof = torch.zeros(16 * n, dtype=torch.int64, device="cuda")
+        rc = lib.tp_late_rounds_dev(1, n, gt.size, gt.ctypes.data_as(I32P), i0.ctypes.data_as(I32P),
+                                    i1.ctypes.data_as(I32P), d_w.data_ptr(), d_b.data_ptr(), d_z.data_ptr(), 1, None,
+                                    d_st.data_ptr(), d_vs.data_ptr(), d_u.data_ptr(), d_v.data_ptr(), len(c["u"]), 0,
+                                    nb, coefs.data_ptr(), line.data_ptr(), cho.data_ptr(), proof.data_ptr(), None)
+        assert rc == 0, lib.tp_last_error()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(host(coefs, (6 * n, 2)), c["coefs"][4 * nb:])
+        np.testing.assert_array_equal(host(cho, (2 * n, 2)), c["chal"][nb:])
+        pr = host(proof, (2 * n, 4, 2))
+        np.testing.assert_array_equal(pr[:, :3].reshape(-1, 2), c["d"][4 * nb:])
+        np.testing.assert_array_equal(pr[:, 3], c["vz"][nb:])
+        np.testing.assert_array_equal(host(line, (n + 1, 2)), c["final"])
+        f = vole_state_fields(d_vs.cpu().numpy().tobytes())
+        assert f["idx"] == int(c["used"][0]) and f["bad"] == 0 and f["has_prev"] == 1
+        assert f["prev"] == tuple(int(x) for x in c["prev"][0])
+        assert f["v_elem"] == [tuple(int(x) for x in r) for r in c["v_elem"]]
+        assert f["out_elem"] == [tuple(int(x) for x in r) for r in c["out_elem"]]
+        d = ctypes.create_string_buffer(32)
+        assert lib.tp_fs_digest(d_st.cpu().numpy().tobytes(), d) == 0
+        assert d.raw == c["digest"].tobytes()
+        n_cases += 1
+    assert n_cases == 2
+
+
+def test_running_out_of_correlations_stops_the_frame(lib):
+    """a frame whose correlations end inside the late rounds is marked bad and
+    stops at that round; the other frame of the launch finishes"""
+    import torch
+    from layervole import cases, early_transcript, vole_state_fields, vole_state_mid
+    c = [x for x in cases() if x["name"] == "random"][0]
+    n, nb = c["n_in_bits"], c["nb"]
+    st, _ = early_transcript(lib, c)
+    used = int(c["used_mid"][0])
+    count = len(c["u"])
+    short = used + 3 * 4 + 1           # frame 1: enough correlations for four late rounds, not a fifth
+    shift = count - short
+    u = np.zeros((2, count, 2), np.uint64)
+    v = np.zeros((2, count, 2), np.uint64)
+    u[0], v[0] = c["u"], c["v"]
+    u[1, used + shift:], v[1, used + shift:] = c["u"][used:short], c["v"][used:short]
+    vs0 = bytearray(vole_state_mid(c))
+    vs1 = bytearray(vs0)
+    struct.pack_into("<Q", vs1, 0, used + shift)   # frame 1's next correlation: its list ends at `count`
+    d_st = torch.frombuffer(bytearray(st.raw * 2), dtype=torch.uint8).cuda()
+    d_vs = torch.frombuffer(vs0 + vs1, dtype=torch.uint8).cuda()
+    gt, i0, i1 = (np.ascontiguousarray(r, np.int32) for r in c["gates"])
+    d_w = dev(np.concatenate([c["wires"], c["wires"]]))
+    d_b = dev(np.concatenate([c["beta"], c["beta"]]))
+    d_z, d_u, d_v = dev(c["zg"]), dev(u), dev(v)
+    coefs = torch.zeros(2 * 12 * n, dtype=torch.int64, device="cuda")
+    line = torch.zeros(2 * 2 * (n + 1), dtype=torch.int64, device="cuda")
+    cho = torch.zeros(2 * 4 * n, dtype=torch.int64, device="cuda")
+    rc = lib.tp_late_rounds_dev(2, n, gt.size, gt.ctypes.data_as(I32P), i0.ctypes.data_as(I32P),
+                                i1.ctypes.data_as(I32P), d_w.data_ptr(), d_b.data_ptr(), d_z.data_ptr(), 0, None,
+                                d_st.data_ptr(), d_vs.data_ptr(), d_u.data_ptr(), d_v.data_ptr(), count, 0, nb,
+                                coefs.data_ptr(), line.data_ptr(), cho.data_ptr(), None, None)
+    assert rc == 0, lib.tp_last_error()
+    torch.cuda.synchronize()
+    raw = d_vs.cpu().numpy().tobytes()
+    f0, f1 = vole_state_fields(raw[:160]), vole_state_fields(raw[160:])
+    assert f0["bad"] == 0 and f0["idx"] == int(c["used"][0])
+    assert f1["bad"] == 1 and f1["idx"] == used + shift + 12
+    ch = host(cho, (2, 2 * n, 2))
+    np.testing.assert_array_equal(ch[0], c["chal"][nb:])
+    np.testing.assert_array_equal(ch[1][:4], c["chal"][nb:nb + 4])    # the same first four rounds
+    assert (ch[1][4] == 0).all()
+
+
+def test_batch_matches_oracle(lib):
+    """8 frames of the gray circuit with field-size wires, one weight vector per frame"""
+    import os
+    from latelib import ROOT
+    circ = np.load(os.path.join(ROOT, "tests", "golden", "circuits.npz"))
+    gates = (circ["gray_type"], circ["gray_in0"], circ["gray_in1"])
+    rng = np.random.default_rng(404)
+    B, n = 8, 9
+    wires = rng.integers(0, P61, size=(B, 512, 2), dtype=np.uint64)
+    beta = rng.integers(0, P61, size=(B, 2), dtype=np.uint64)
+    zg = rng.integers(0, P61, size=(B, 384, 2), dtype=np.uint64)
+    chal = rng.integers(0, P61, size=(B, 18, 2), dtype=np.uint64)
+    coefs, line, cho = run_given(lib, n, gates, wires, beta, zg, chal, n_frames=B)
+    g3 = tuple([int(x) for x in a] for a in gates)
+    for f in range(B):
+        cf, h, _, _ = oracle.late_rounds(pairs(wires[f]), pairs(beta[f])[0], pairs(zg[f]), g3, n, pairs(chal[f]))
+        assert [x for r in cf for x in r] == pairs(coefs[f]), f
+        assert h == pairs(line[f]), f
+    # one weight vector for every frame gives frame 0's answer for frame 0
+    coefs1, line1, _ = run_given(lib, n, gates, wires, beta, zg[0], chal, n_frames=B, per_frame=0)
+    np.testing.assert_array_equal(coefs1[0], coefs[0])
+    np.testing.assert_array_equal(line1[0], line[0])
+
+
+def test_whole_frames_after_device_early_rounds(lib):
+    """Two 1080p gray frames: early rounds (BatchFrameProver.prove), then
+    prove_late; the late outputs equal the oracle on the batch's own wires and
+    beta, and the line's values at 0 and 1 equal the multilinear extension of
+    each frame's input vector at (w1, w3) and (w2, w3) (layer.py's identity)."""
+    import os
+    import torch
+    from latelib import ROOT
+    from truepix_b200.frame import BatchFrameProver, FrameLayout, pack_fp2
+    circ = np.load(os.path.join(ROOT, "tests", "golden", "circuits.npz"))
+    gt, i0, i1 = circ["gray_type"], circ["gray_in0"], circ["gray_in1"]
+    B = 2
+    layout = FrameLayout.for_frame(1080, 1920)
+    nb, n = layout.n_copy_bits, 9
+    rng = np.random.default_rng(1080)
+    pix = [torch.from_numpy(rng.integers(0, 256, size=layout.copies * 384, dtype=np.uint8)).cuda() for _ in range(B)]
+    z1s = [rng.integers(0, P61, size=(2, 384), dtype=np.uint64) for _ in range(B)]
+    z2 = rng.integers(0, P61, size=(B, nb, 2), dtype=np.uint64)
+    pt = rng.integers(0, P61, size=(B, nb + 9, 2), dtype=np.uint64)
+    z2d = torch.from_numpy(pack_fp2(z2[..., 0].reshape(-1), z2[..., 1].reshape(-1))).cuda()
+    ptd = torch.from_numpy(pack_fp2(pt[..., 0].reshape(-1), pt[..., 1].reshape(-1))).cuda()
+    early = rng.integers(0, P61, size=(nb, B, 2), dtype=np.uint64)
+    late = rng.integers(0, P61, size=(B, 2 * n, 2), dtype=np.uint64)
+    bp = BatchFrameProver([layout] * B, gt, i0, i1)
+    bp.prove(pix, z1s, z2d, ptd, early)
+    bp.prove_late(z1s, challenges=late)
+    torch.cuda.synchronize()
+    coefs = host(bp.late_coefs, (B, 6 * n, 2))
+    line = host(bp.line, (B, n + 1, 2))
+    g3 = ([int(x) for x in gt], [int(x) for x in i0], [int(x) for x in i1])
+    for f in range(B):
+        _, wires, beta, _ = bp.results(f)
+        zg = list(zip([int(x) for x in z1s[f][0]], [int(x) for x in z1s[f][1]]))
+        cf, h, v1, v2 = oracle.late_rounds(pairs(wires), beta, zg, g3, n, pairs(late[f]))
+        assert [x for r in cf for x in r] == pairs(coefs[f])
+        assert h == pairs(line[f])
+        for t, w in ((0, late[f][:n]), (1, late[f][n:])):
+            point = np.concatenate([w, early[:, f]])          # wire bits first, then copy bits
+            d_pt = torch.from_numpy(pack_fp2(point[:, 0], point[:, 1])).cuda()
+            out = torch.zeros(2, dtype=torch.int64, device="cuda")
+            assert lib.tp_mle_eval_pixels(pix[f].data_ptr(), layout.copies, layout.padded_copies, 384, 512, 384, 128,
+                                          d_pt.data_ptr(), out.data_ptr(), None) == 0
+            torch.cuda.synchronize()
+            m = tuple(int(x) for x in host(out, (2,)))
+            if t == 0:
+                assert m == h[0] == v1                      # the line at 0
+            else:
+                s = (0, 0)
+                for x in h:
+                    s = oracle.add(s, x)
+                assert m == s == v2                         # the line at 1: the sum of its coefficients
+
+
+def test_bad_arguments_are_rejected(lib):
+    import torch
+    g = np.zeros(4, np.int32)
+    bufs = [torch.zeros(256, dtype=torch.int64, device="cuda") for _ in range(7)]
+    wires, beta, zg, chal, coefs, line, cho = (b.data_ptr() for b in bufs)
+
+    def call(n=3, gt=g, i0=g, i1=g, ch=chal, proof=None):
+        return lib.tp_late_rounds_dev(1, n, len(gt), np.ascontiguousarray(gt, np.int32).ctypes.data_as(I32P),
+                                      np.ascontiguousarray(i0, np.int32).ctypes.data_as(I32P),
+                                      np.ascontiguousarray(i1, np.int32).ctypes.data_as(I32P), wires, beta, zg, 1,
+                                      ch, None, None, None, None, 0, 0, 0, coefs, line, cho, proof, None)
+
+    assert call() == 0
+    assert call(n=10) == -1
+    assert call(n=0) == -1
+    assert call(gt=np.array([13, 0, 0, 0])) == -1
+    assert call(i0=np.array([0, 8, 0, 0])) == -1            # 8 wires at n = 3
+    assert b"gate 1" in lib.tp_last_error()
+    assert call(ch=None) == -1                              # neither challenges nor transcripts
+    assert call(proof=coefs) == -1                          # proof only with VOLE rounds
+    big = np.zeros(769, np.int32)
+    assert call(gt=big, i0=big, i1=big) == -1
+    torch.cuda.synchronize()

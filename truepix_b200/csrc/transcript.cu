@@ -9,6 +9,7 @@
 
 #include "runtime.h"
 #include "transcript.cuh"
+#include "vole.cuh"
 #include "../../include/native_fp2.h"
 
 extern "C" int tp_host_sha_ext_available(void);
@@ -65,20 +66,8 @@ __global__ void rand_ext_kernel(State* __restrict__ st, int n, Label L, ulonglon
     out[i] = make_ulonglong2(re, im);
 }
 
-// ---- VOLE-committed sumcheck round (circuitnizkvec_vole.py:396-418) ----------
-// Per frame: the round polynomial's coefficients from the claims at (0, 1, -1, 2)
-// (util.interpolate_cubic), each committed with the next correlation (d = c - u
-// put, tag v kept), the equality proof of the tags' value at 0 + 1 against the
-// previous round's (challenge rand_ext("eq"), (prev - now) * challenge put; the
-// value alone, now * challenge, when there is none), the fold challenge
-// rand_ext(label) and the next previous value, the tags' polynomial at it.
-struct VoleState {
-    unsigned long long idx;   // next correlation
-    unsigned has_prev, bad;   // bad: the correlations ran out (nothing done)
-    tp::fp2 prev;
-    tp::fp2 v_elem[4], out_elem[4];   // running sums of tags / coefficients (the final proof of knowledge)
-};
-static_assert(sizeof(VoleState) == 160, "vole state layout");
+// ---- VOLE-committed early round (vole.cuh), one thread per frame ----------------
+using VoleState = tp::vole::State;
 
 __global__ void vole_round_kernel(State* __restrict__ st, VoleState* __restrict__ vs, int n,
                                   const tp::fp2* __restrict__ claims, const tp::fp2* __restrict__ u,
@@ -89,44 +78,12 @@ __global__ void vole_round_kernel(State* __restrict__ st, VoleState* __restrict_
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     VoleState w = vs[i];
-    if (w.bad || w.idx + 4 > (unsigned long long)count) {
-        w.bad = 1;
-        vs[i] = w;
-        chal[i] = f2zero();
-        return;
-    }
     State s = st[i];
-    const fp2 f0 = claims[4 * i], f1 = claims[4 * i + 1], fm1 = claims[4 * i + 2], f2 = claims[4 * i + 3];
-    const u64 half = 1ull << 60, third = 1537228672809129301ull;
-    const fp2 a = f2sub(f2zero(), fm1);
-    const fp2 b = f2scale(f2add(f1, fm1), half);
-    const fp2 c = f2scale(f2add(f1, a), half);
-    const fp2 d = f2scale(f2add(f2, a), third);
-    const fp2 c2 = f2sub(b, f0);
-    const fp2 c3 = f2scale(f2sub(f2sub(d, c), c2), half);
-    const fp2 coef[4] = {f0, f2sub(c, c3), c2, c3};
+    fp2 coef[4];
+    vole::interpolate_cubic(claims[4 * i], claims[4 * i + 1], claims[4 * i + 2], claims[4 * i + 3], coef);
     const long long base = (long long)i * count;
-    fp2 tag[4];
-    for (int k = 0; k < 4; ++k) {
-        tag[k] = v[base + w.idx];
-        const fp2 dm = f2sub(coef[k], u[base + w.idx]);
-        ++w.idx;
-        fs::put_fp2(s, dm.re, dm.im);
-        if (proof) proof[5 * i + k] = dm;
-        w.v_elem[k] = f2add(w.v_elem[k], tag[k]);
-        w.out_elem[k] = f2add(w.out_elem[k], coef[k]);
-    }
-    const fp2 now = f2add(f2add(f2add(f2add(tag[0], tag[1]), tag[2]), tag[3]), tag[0]);
-    const uint8_t eq[2] = {'e', 'q'};
-    fp2 e;
-    fs::rand_ext(s, eq, 2, reinterpret_cast<uint64_t*>(&e.re), reinterpret_cast<uint64_t*>(&e.im));
-    const fp2 vz = w.has_prev ? f2mul(f2sub(w.prev, now), e) : f2mul(now, e);
-    fs::put_fp2(s, vz.re, vz.im);
-    if (proof) proof[5 * i + 4] = vz;
     fp2 r;
-    fs::rand_ext(s, L.b, L.len, reinterpret_cast<uint64_t*>(&r.re), reinterpret_cast<uint64_t*>(&r.im));
-    w.prev = f2add(f2mul(f2add(f2mul(f2add(f2mul(tag[3], r), tag[2]), r), tag[1]), r), tag[0]);
-    w.has_prev = 1;
+    vole::round(s, w, coef, 4, u + base, v + base, count, L.b, L.len, proof ? proof + 5 * i : nullptr, &r);
     st[i] = s;
     vs[i] = w;
     chal[i] = r;

@@ -23,6 +23,7 @@ Challenges come from the host transcript in TruePix; here they are arguments.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import math
 from dataclasses import dataclass
@@ -345,6 +346,61 @@ class BatchFrameProver:
                 for q, f in enumerate(fs):
                     self.mle[2 * f:2 * f + 2].copy_(out[2 * q:2 * q + 2])
         self.launches_last = launches
+
+    def prove_late(self, z1s, challenges=None, transcripts=None, vole=None, layer: int = 0) -> None:
+        """The late rounds and the line projection of every frame, after prove():
+        one launch (tp_late_rounds_dev) from the batch's wires and beta. z1s: the
+        per-gate weights given to prove() (uint64 [2, n_gates] per frame).
+        challenges: uint64 [B, 2 log2 W, 2]; or, instead, transcripts and vole as
+        in prove() (the states continue from the early rounds; round labels
+        continue at the frame's copy-bit count). Results in self.late_coefs
+        [B][2 log2 W][3], self.line [B][log2 W + 1], self.late_challenges
+        [B][2 log2 W] and, with vole, self.late_proof [B][2 log2 W][4] (packed
+        Fp2, int64 device tensors)."""
+        torch, lib, s = self.torch, self.lib, self._s()
+        n = int(math.log2(self.W))
+        G = self.gt.size
+        zg = np.stack([np.stack([np.asarray(z[0], np.uint64), np.asarray(z[1], np.uint64)], axis=1)
+                       for z in z1s]).reshape(-1)
+        # uploads on the launch stream, so that the kernel is ordered after them
+        def on_stream():
+            return torch.cuda.stream(self.stream) if self.stream is not None else contextlib.nullcontext()
+        with on_stream():
+            d_zg = torch.from_numpy(zg.view(np.int64).copy()).to(self.dev)
+        i64 = torch.int64
+        with on_stream():
+            self.late_coefs = torch.zeros(self.B * 2 * n * 3 * 2, dtype=i64, device=self.dev)
+            self.line = torch.zeros(self.B * (n + 1) * 2, dtype=i64, device=self.dev)
+            self.late_challenges = torch.zeros(self.B * 2 * n * 2, dtype=i64, device=self.dev)
+        I32P = ctypes.POINTER(ctypes.c_int)
+        gt, i0, i1 = (a.ctypes.data_as(I32P) for a in (self.gt, self.i0, self.i1))
+        keep = [d_zg]
+        if transcripts is None:
+            ch = np.ascontiguousarray(challenges, np.uint64).reshape(-1)
+            if ch.size != self.B * 2 * n * 2:
+                raise ValueError("challenges: [B, 2 log2 W, 2] expected")
+            with on_stream():
+                d_ch = torch.from_numpy(ch.view(np.int64).copy()).to(self.dev)
+            keep.append(d_ch)
+            self.late_proof = None
+            rc = lib.tp_late_rounds_dev(self.B, n, G, gt, i0, i1, self.wires.data_ptr(), self.fin_beta.data_ptr(),
+                                        d_zg.data_ptr(), 1, d_ch.data_ptr(), None, None, None, None, 0, layer, 0,
+                                        self.late_coefs.data_ptr(), self.line.data_ptr(),
+                                        self.late_challenges.data_ptr(), None, s)
+        else:
+            if vole is None:
+                raise ValueError("the late rounds on device transcripts are the VOLE-committed rounds: pass vole")
+            if any(L.n_copy_bits != self.max_rounds for L in self.layouts):
+                raise ValueError("device transcripts need frames with the same number of rounds")
+            with on_stream():
+                self.late_proof = torch.zeros(self.B * 2 * n * 4 * 2, dtype=i64, device=self.dev)
+            rc = lib.tp_late_rounds_dev(self.B, n, G, gt, i0, i1, self.wires.data_ptr(), self.fin_beta.data_ptr(),
+                                        d_zg.data_ptr(), 1, None, transcripts.data_ptr(), vole["states"].data_ptr(),
+                                        vole["u"].data_ptr(), vole["v"].data_ptr(), vole["count"], layer,
+                                        self.max_rounds, self.late_coefs.data_ptr(), self.line.data_ptr(),
+                                        self.late_challenges.data_ptr(), self.late_proof.data_ptr(), s)
+        native.check(lib, rc, "tp_late_rounds_dev")
+        self._late_keep = keep     # inputs stay alive until the stream has used them
 
     def results(self, f: int):
         """Frame f: (claims [n_copy_bits, 8], wires [W, 2], beta, mle)."""
