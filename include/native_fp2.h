@@ -247,12 +247,29 @@ int tp_timer_read(float* ms, int* tags, int max_pairs);
  * constant first, of the input values on the line w1 + t (w2 - w1): the
  * project_line output the layer's final proof commits), d_challenges_out
  * [n_frames][2 n_in_bits], d_proof (VOLE mode, optional) [n_frames][2 n_in_bits]
- * [4] (three commitments d, the equality value). Asynchronous on `stream`. */
+ * [4] (three commitments d, the equality value).
+ * The layer's closing proofs (VOLE mode, d_closing not NULL), circuitnizkvec_vole.py
+ * :433-500 for a one-layer circuit: create_final_prod_pok on the line's
+ * coefficients, the wiring predicates' multilinear extensions times the committed
+ * gate values (CircuitVerifier.eval_mlext with GateFunctionsPC) and beta's factor
+ * from d_z2 [n_frames][round0] (the copy part of the layer's point) and the early
+ * challenges d_w3 (frame i, round k at d_w3[i * w3_frame_stride + k *
+ * w3_round_stride], packed Fp2 elements), the equality proof, tau =
+ * rand_ext("tau-<layer>"), create_pok_final, put(["gkr_input_point", point]),
+ * create_input_value_proof. Outputs: d_closing [n_frames][n_in_bits + 10] (the
+ * Fp2 values in the order they are put: d of the first coefficient and of the
+ * product, d of the other coefficients, the two proof-of-knowledge values, the
+ * two product-proof values, the equality value, the two final proof-of-knowledge
+ * values, the input value proof), d_point [n_frames][n_in_bits + round0] (the
+ * input point: the line at tau, then the early challenges), d_tag [n_frames] (its
+ * tag). round0 is the number of early rounds (<= 64). Asynchronous on `stream`. */
 int tp_late_rounds_dev(int n_frames, int n_in_bits, int n_gates, const int* gate_type, const int* in0,
                        const int* in1, const void* d_wires, const void* d_beta, const void* d_gate_weights,
                        int weights_per_frame, const void* d_challenges, void* d_fs_states, void* d_vole_states,
                        const void* d_u, const void* d_v, long long count, int layer, int round0, void* d_coefs,
-                       void* d_line, void* d_challenges_out, void* d_proof, void* stream);
+                       void* d_line, void* d_challenges_out, void* d_proof, const void* d_z2, const void* d_w3,
+                       long long w3_frame_stride, long long w3_round_stride, void* d_closing, void* d_point,
+                       void* d_tag, void* stream);
 
 /* ---- circuit evaluation: the prover's output vector ----
  * Replaces ArithCircuitIncrementalBuilder.run (libTruePix/arithcircuitbuilder.py:71-108,

@@ -1,16 +1,21 @@
-"""Golden vectors of the input layer's whole VOLE-committed sumcheck, early and
-late rounds, made by the reference's own pieces in the order of its prover loop
-(TruePix-main/libTruePix/circuitnizkvec_vole.py:386-418): LayerProver
-(layerprover.py) for the round polynomials, ExtVOLECommit.commit / est_val /
-est_eq for the commitments and equality proofs, FiatShamir put / rand_ext for
-the transcript, util.horner_eval for the next round's value.
+"""Golden vectors of the input layer's whole VOLE-committed proof -- early and
+late rounds and the layer's closing proofs -- made by the reference prover's
+own code in the order of its loop (TruePix-main/libTruePix/circuitnizkvec_vole.py
+:386-500): LayerProver (layerprover.py) for the round polynomials and the line;
+CircuitProverNIZK's create_pok_temp, create_eq_proof, create_final_prod_pok,
+create_pok_final, create_input_value_proof and _challenge, and
+CircuitVerifier.eval_mlext, called on a prover object that carries only the
+state they read (commitment, transcript, gate tables); GateFunctionsPC for the
+committed gate values; ExtVOLECommit for the commitments; FiatShamir for the
+transcript.
 
 Per case: gates, inputs, z1, z2, the per-gate weights, correlations u, v and the
 first one used, the transcript prefix; per round the coefficients, the values d
 put, the equality value, the challenge; between the phases the wires, beta, the
-previous value and the running tag / coefficient sums; at the end the line
-coefficients, the last previous value, the sums, the correlations used and the
-transcript digest.
+previous value and the running tag / coefficient sums; after the late rounds
+the line coefficients, the previous value, the sums, the correlations used and
+the transcript digest; then the closing proof's Fp2 values in the order they are
+put, the input point, its tag, the correlations used and the final digest.
 
 Run here (needs the reference checkout):  python tests/golden/gen_layer_vole_golden.py
 """
@@ -55,7 +60,7 @@ def run_case(rng, n_in_bits, n_copies, gt, i0, i1, inputs, start):
     L.set_z(z1, z2, None, None, True)
     zg = [g.accum_z1 for g in L.gates]
 
-    n_vole = start + 4 * nb + 3 * 2 * n_in_bits + 2
+    n_vole = start + 4 * nb + 3 * 2 * n_in_bits + (n_in_bits + 2) + 1
     u = rng.integers(0, P61, size=(n_vole, 2), dtype=np.uint64)
     v = rng.integers(0, P61, size=(n_vole, 2), dtype=np.uint64)
     com = ExtVOLECommit(P61)
@@ -67,51 +72,80 @@ def run_case(rng, n_in_bits, n_copies, gt, i0, i1, inputs, start):
     fs = FiatShamir(P61, protocol="truepix")
     fs.put(prefix)
 
+    from libTruePix.circuitnizkvec_vole import CircuitProverNIZK
+    from libTruePix.gateprover_vole import GateFunctionsPC
+    from libTruePix.extfield import serialize_point
+    prv = CircuitProverNIZK.__new__(CircuitProverNIZK)      # the state its proof methods read
+    prv.com, prv.fs, prv.v_elem, prv.out_elem, prv.com_q_a, prv.tV_a = com, fs, [], [], None, None
+    prv.layInBits, prv.layOutBits, prv.nCopyBits = [n_in_bits], [n_out_bits], nb
+    prv.in0vv, prv.in1vv, prv.muxvv = [[int(x) for x in i0]], [[int(x) for x in i1]], None
+    prv.typvv = [[by_idx[int(t)] for t in gt]]
+
+    lay = 0
     prev = None
-    v_elem, out_elem = [], []
     rec = dict(coefs=[], d=[], vz=[], chal=[])
     mid = {}
+    w1, w2, w3 = [], [], []
     for rd in range(n_rounds):
         L.compute_outputs()
         outs = list(L.output)
-        rvals = []
-        for num, val in enumerate(outs):          # create_pok_temp
-            v_m, d_m = com.commit(val)
-            rvals.append(v_m)
-            fs.put(d_m)
-            rec["d"].append(d_m)
-            if len(v_elem) < len(outs):
-                v_elem.append(0)
-                out_elem.append(0)
-        for num in range(len(rvals)):
-            v_elem[num] += rvals[num]
-            out_elem[num] += outs[num]
+        mark = len(fs.trans)
+        rvals = prv.create_pok_temp(outs)
+        rec["d"].extend(x[0] for x in list(fs.trans)[mark:])
         zp1 = (sum(rvals) + rvals[0]) % P61
-        chal = fs.rand_ext("eq")                  # create_eq_proof
-        v_z = com.est_val(zp1, chal) if prev is None else com.est_eq(prev, zp1, chal)
-        fs.put(v_z)
-        rec["vz"].append(v_z)
-        nrand = fs.rand_ext("sc-0-%d" % rd)
+        prv.create_eq_proof(prev, zp1)
+        rec["vz"].append(fs.trans[-1][0])
+        nrand = prv._challenge("sc-%d-%d" % (lay, rd))
         L.next_round(nrand)
         prev = util.horner_eval(rvals, nrand)
         rec["coefs"].extend(outs)
         rec["chal"].append(nrand)
+        (w3 if rd < nb else w1 if rd < nb + n_in_bits else w2).append(nrand)
         if rd == nb - 1:
             mid = dict(wires=list(L.compute_v_final.inputs), beta=[L.compute_beta.prevPassValue], prev_mid=[prev],
-                       v_elem_mid=list(v_elem) + [0] * (4 - len(v_elem)),
-                       out_elem_mid=list(out_elem) + [0] * (4 - len(out_elem)), used_mid=[com.numVOLE])
+                       v_elem_mid=list(prv.v_elem) + [0] * (4 - len(prv.v_elem)),
+                       out_elem_mid=list(prv.out_elem) + [0] * (4 - len(prv.out_elem)), used_mid=[com.numVOLE])
     L.compute_outputs()
     final = list(L.output)
+    v_elem, out_elem = list(prv.v_elem), list(prv.out_elem)
+    late_end = dict(prev=[prev], used=np.array([com.numVOLE], np.int64),
+                    digest=np.frombuffer(fs.hash.digest(), np.uint8))
+
+    # the layer's closing proofs, circuitnizkvec_vole.py:433-500 (one layer: project_line)
+    mark = len(fs.trans)
+    (outs_rvals, pr_rvals) = prv.create_final_prod_pok(final)
+    (mlext_evals, mlx_z2) = prv.eval_mlext(lay, z1, z2, w1, w2, w3, None, None)
+    tV = 0
+    for (idx, elm) in enumerate(mlext_evals):
+        tV += elm * GateFunctionsPC[idx](pr_rvals[0], pr_rvals[1], pr_rvals[2], None)
+        tV %= P61
+    tV = tV * mlx_z2 % P61
+    prv.create_eq_proof(prev, tV)
+    tau = prv._challenge("tau-%d" % lay)
+    tag = util.horner_eval(outs_rvals, tau)
+    zz1 = [(e1 + (e2 - e1) * tau) % P61 for (e1, e2) in zip(w1, w2)]
+    prv.create_pok_final()
+    point = list(zz1) + list(w3)
+    fs.put(["gkr_input_point", serialize_point(point)])
+    prv.create_input_value_proof(tag, None)
+    closing = []
+    for item in list(fs.trans)[mark:]:
+        for x in util.flatten(item):
+            if isinstance(x, Fp2):
+                closing.append(x)
 
     def f2(xs):
         return np.array([[int(x.real), int(x.imag)] if hasattr(x, "real") and not isinstance(x, int) else [int(x), 0]
                          for x in xs], np.uint64).reshape(-1, 2)
     out = {k: f2(vv) for k, vv in rec.items()}
     out.update({k: (f2(vv) if k != "used_mid" else np.array(vv, np.int64)) for k, vv in mid.items()})
-    out.update(z1=f2(z1), z2=f2(z2), zg=f2(zg), final=f2(final), prev=f2([prev]),
+    out.update(z1=f2(z1), z2=f2(z2), zg=f2(zg), final=f2(final), prev=f2(late_end["prev"]),
                v_elem=f2(v_elem + [0] * (4 - len(v_elem))), out_elem=f2(out_elem + [0] * (4 - len(out_elem))),
                u=u, v=v, start=np.array([start], np.int64), prefix=np.array(prefix, np.uint64),
-               used=np.array([com.numVOLE], np.int64), digest=np.frombuffer(fs.hash.digest(), np.uint8))
+               used=late_end["used"], digest=late_end["digest"],
+               closing=f2(closing), point=f2(point), tau=f2([tau]), tag=f2([tag]),
+               used_closed=np.array([com.numVOLE], np.int64),
+               digest_closed=np.frombuffer(fs.hash.digest(), np.uint8))
     return out
 
 

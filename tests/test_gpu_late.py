@@ -4,7 +4,9 @@ with vectors made by the reference's own LayerProver (tests/golden/
 late_golden.npz); the VOLE-committed rounds, bit-exact with the reference's
 LayerProver + ExtVOLECommit + FiatShamir chain (tests/golden/
 layer_vole_golden.npz: coefficients, commitments, equality values, challenges,
-line, VOLE state, transcript digest); batches against the oracle; whole 1080p
+line, VOLE state, transcript digest, and the layer's closing proofs: product
+proof, proofs of knowledge, equality proof, input point, its tag and value
+proof); batches against the oracle; whole 1080p
 frames after the device early rounds, against the oracle and against the
 multilinear extension of the frame's bytes at the two late points."""
 import ctypes
@@ -46,7 +48,7 @@ def run_given(lib, n, gates, wires, beta, zg, chal, n_frames=1, per_frame=1):
     rc = lib.tp_late_rounds_dev(n_frames, n, gt.size, gt.ctypes.data_as(I32P), i0.ctypes.data_as(I32P),
                                 i1.ctypes.data_as(I32P), d_w.data_ptr(), d_b.data_ptr(), d_z.data_ptr(), per_frame,
                                 d_c.data_ptr(), None, None, None, None, 0, 0, 0, coefs.data_ptr(), line.data_ptr(),
-                                cho.data_ptr(), None, None)
+                                cho.data_ptr(), None, None, None, 0, 0, None, None, None, None)
     assert rc == 0, lib.tp_last_error()
     torch.cuda.synchronize()
     return (host(coefs, (n_frames, 6 * n, 2)), host(line, (n_frames, n + 1, 2)), host(cho, (n_frames, 2 * n, 2)))
@@ -80,25 +82,45 @@ def test_vole_rounds_match_reference_chain(lib):
         line = torch.zeros(2 * (n + 1), dtype=torch.int64, device="cuda")
         cho = torch.zeros(4 * n, dtype=torch.int64, device="cuda")
         proof = torch.zeros(16 * n, dtype=torch.int64, device="cuda")
-        rc = lib.tp_late_rounds_dev(1, n, gt.size, gt.ctypes.data_as(I32P), i0.ctypes.data_as(I32P),
-                                    i1.ctypes.data_as(I32P), d_w.data_ptr(), d_b.data_ptr(), d_z.data_ptr(), 1, None,
-                                    d_st.data_ptr(), d_vs.data_ptr(), d_u.data_ptr(), d_v.data_ptr(), len(c["u"]), 0,
-                                    nb, coefs.data_ptr(), line.data_ptr(), cho.data_ptr(), proof.data_ptr(), None)
-        assert rc == 0, lib.tp_last_error()
-        torch.cuda.synchronize()
+        d_z2, d_w3 = dev(c["z2"]), dev(c["chal"][:nb])
+        closing = torch.zeros(2 * (n + 10), dtype=torch.int64, device="cuda")
+        point = torch.zeros(2 * (n + nb), dtype=torch.int64, device="cuda")
+        tag = torch.zeros(2, dtype=torch.int64, device="cuda")
+        st_late = None
+        for close in (False, True):
+            if close:   # again from the same start, now with the layer's closing proofs
+                d_st.copy_(torch.frombuffer(bytearray(st.raw), dtype=torch.uint8).cuda())
+                d_vs.copy_(torch.frombuffer(bytearray(vole_state_mid(c)), dtype=torch.uint8).cuda())
+            rc = lib.tp_late_rounds_dev(1, n, gt.size, gt.ctypes.data_as(I32P), i0.ctypes.data_as(I32P),
+                                        i1.ctypes.data_as(I32P), d_w.data_ptr(), d_b.data_ptr(), d_z.data_ptr(), 1,
+                                        None, d_st.data_ptr(), d_vs.data_ptr(), d_u.data_ptr(), d_v.data_ptr(),
+                                        len(c["u"]), 0, nb, coefs.data_ptr(), line.data_ptr(), cho.data_ptr(),
+                                        proof.data_ptr(), d_z2.data_ptr(), d_w3.data_ptr(), 0, 1,
+                                        closing.data_ptr() if close else None, point.data_ptr(), tag.data_ptr(),
+                                        None)
+            assert rc == 0, lib.tp_last_error()
+            torch.cuda.synchronize()
+            if not close:
+                st_late, vs_late = d_st.cpu().numpy().tobytes(), d_vs.cpu().numpy().tobytes()
+        np.testing.assert_array_equal(host(closing, (n + 10, 2)), c["closing"])
+        np.testing.assert_array_equal(host(point, (n + nb, 2)), c["point"])
+        np.testing.assert_array_equal(host(tag, (1, 2)), c["tag"])
+        assert vole_state_fields(d_vs.cpu().numpy().tobytes())["idx"] == int(c["used_closed"][0])
+        d = ctypes.create_string_buffer(32)
+        assert lib.tp_fs_digest(d_st.cpu().numpy().tobytes(), d) == 0
+        assert d.raw == c["digest_closed"].tobytes()
         np.testing.assert_array_equal(host(coefs, (6 * n, 2)), c["coefs"][4 * nb:])
         np.testing.assert_array_equal(host(cho, (2 * n, 2)), c["chal"][nb:])
         pr = host(proof, (2 * n, 4, 2))
         np.testing.assert_array_equal(pr[:, :3].reshape(-1, 2), c["d"][4 * nb:])
         np.testing.assert_array_equal(pr[:, 3], c["vz"][nb:])
         np.testing.assert_array_equal(host(line, (n + 1, 2)), c["final"])
-        f = vole_state_fields(d_vs.cpu().numpy().tobytes())
+        f = vole_state_fields(vs_late)
         assert f["idx"] == int(c["used"][0]) and f["bad"] == 0 and f["has_prev"] == 1
         assert f["prev"] == tuple(int(x) for x in c["prev"][0])
         assert f["v_elem"] == [tuple(int(x) for x in r) for r in c["v_elem"]]
         assert f["out_elem"] == [tuple(int(x) for x in r) for r in c["out_elem"]]
-        d = ctypes.create_string_buffer(32)
-        assert lib.tp_fs_digest(d_st.cpu().numpy().tobytes(), d) == 0
+        assert lib.tp_fs_digest(st_late, d) == 0
         assert d.raw == c["digest"].tobytes()
         n_cases += 1
     assert n_cases == 2
@@ -135,7 +157,8 @@ def test_running_out_of_correlations_stops_the_frame(lib):
     rc = lib.tp_late_rounds_dev(2, n, gt.size, gt.ctypes.data_as(I32P), i0.ctypes.data_as(I32P),
                                 i1.ctypes.data_as(I32P), d_w.data_ptr(), d_b.data_ptr(), d_z.data_ptr(), 0, None,
                                 d_st.data_ptr(), d_vs.data_ptr(), d_u.data_ptr(), d_v.data_ptr(), count, 0, nb,
-                                coefs.data_ptr(), line.data_ptr(), cho.data_ptr(), None, None)
+                                coefs.data_ptr(), line.data_ptr(), cho.data_ptr(), None, None, None, 0, 0, None, None,
+                                None, None)
     assert rc == 0, lib.tp_last_error()
     torch.cuda.synchronize()
     raw = d_vs.cpu().numpy().tobytes()
@@ -231,11 +254,12 @@ def test_bad_arguments_are_rejected(lib):
     bufs = [torch.zeros(256, dtype=torch.int64, device="cuda") for _ in range(7)]
     wires, beta, zg, chal, coefs, line, cho = (b.data_ptr() for b in bufs)
 
-    def call(n=3, gt=g, i0=g, i1=g, ch=chal, proof=None):
+    def call(n=3, gt=g, i0=g, i1=g, ch=chal, proof=None, closing=None):
         return lib.tp_late_rounds_dev(1, n, len(gt), np.ascontiguousarray(gt, np.int32).ctypes.data_as(I32P),
                                       np.ascontiguousarray(i0, np.int32).ctypes.data_as(I32P),
                                       np.ascontiguousarray(i1, np.int32).ctypes.data_as(I32P), wires, beta, zg, 1,
-                                      ch, None, None, None, None, 0, 0, 0, coefs, line, cho, proof, None)
+                                      ch, None, None, None, None, 0, 0, 0, coefs, line, cho, proof, None, None, 0, 0,
+                                      closing, line, cho, None)
 
     assert call() == 0
     assert call(n=10) == -1
@@ -245,6 +269,117 @@ def test_bad_arguments_are_rejected(lib):
     assert b"gate 1" in lib.tp_last_error()
     assert call(ch=None) == -1                              # neither challenges nor transcripts
     assert call(proof=coefs) == -1                          # proof only with VOLE rounds
+    assert call(closing=coefs) == -1                        # closing proofs only with VOLE rounds
     big = np.zeros(769, np.int32)
     assert call(gt=big, i0=big, i1=big) == -1
     torch.cuda.synchronize()
+
+
+def test_whole_layer_proof_on_device_matches_restatement(lib):
+    """Three 360p gray frames, the whole input layer's proof on the device: the
+    VOLE-committed early rounds (BatchFrameProver.prove with transcripts and
+    VOLE states), then prove_late: late rounds, line and closing proofs, with no
+    host round trip. Per frame, the restated loop (hashlib transcript, the
+    oracle's late rounds, the restated closing proofs) fed with the device's
+    early claims draws the same challenges and puts the same values, and ends
+    in the same transcript digest."""
+    import os
+    import torch
+    from fslib import PyTranscript, f2add, f2mul, f2sub, interpolate_cubic, replay_lib
+    from latelib import ROOT
+    from layervole import closing_python
+    from truepix_b200.frame import BatchFrameProver, FrameLayout, pack_fp2
+    circ = np.load(os.path.join(ROOT, "tests", "golden", "circuits.npz"))
+    gt, i0, i1 = circ["gray_type"], circ["gray_in0"], circ["gray_in1"]
+    B, n = 3, 9
+    layout = FrameLayout.for_frame(360, 640)
+    nb = layout.n_copy_bits
+    rng = np.random.default_rng(360)
+    pix = [torch.from_numpy(rng.integers(0, 256, size=layout.copies * 384, dtype=np.uint8)).cuda() for _ in range(B)]
+    z1s = [rng.integers(0, P61, size=(2, 384), dtype=np.uint64) for _ in range(B)]
+    z2 = rng.integers(0, P61, size=(B, nb, 2), dtype=np.uint64)
+    pt = rng.integers(0, P61, size=(B, nb + 9, 2), dtype=np.uint64)
+    count = 4 * nb + 6 * n + (n + 2) + 5
+    u = rng.integers(0, P61, size=(B, count, 2), dtype=np.uint64)
+    v = rng.integers(0, P61, size=(B, count, 2), dtype=np.uint64)
+    prefixes = [[f, 11, 7] for f in range(B)]
+    states = b"".join(replay_lib(lib, "truepix", [["u64s", p]])[2].raw for p in prefixes)
+    vsb = b""
+    for f in range(B):
+        vs = ctypes.create_string_buffer(lib.tp_vole_state_bytes())
+        assert lib.tp_vole_state_init(vs, 2, None) == 0
+        vsb += vs.raw
+    d_fs = torch.from_numpy(np.frombuffer(states, np.uint8).copy()).cuda()
+    vole = dict(states=torch.from_numpy(np.frombuffer(vsb, np.uint8).copy()).cuda(),
+                u=torch.from_numpy(u.view(np.int64).reshape(-1)).cuda(),
+                v=torch.from_numpy(v.view(np.int64).reshape(-1)).cuda(), count=count)
+    bp = BatchFrameProver([layout] * B, gt, i0, i1)
+    bp.prove(pix, z1s, torch.from_numpy(pack_fp2(z2[..., 0].reshape(-1), z2[..., 1].reshape(-1))).cuda(),
+             torch.from_numpy(pack_fp2(pt[..., 0].reshape(-1), pt[..., 1].reshape(-1))).cuda(), None,
+             transcripts=d_fs, vole=vole)
+    bp.prove_late(z1s, transcripts=d_fs, vole=vole)
+    torch.cuda.synchronize()
+    claims = host(bp.claims, (nb, B, 4, 2))
+    early_ch = host(bp.device_challenges, (nb, B, 2))
+    late_ch = host(bp.late_challenges, (B, 2 * n, 2))
+    late_pr = host(bp.late_proof, (B, 2 * n, 4, 2))
+    closing = host(bp.closing, (B, n + 10, 2))
+    point = host(bp.input_point, (B, n + nb, 2))
+    tag = host(bp.input_tag, (B, 2))
+    raw = d_fs.cpu().numpy().tobytes()
+    nst = lib.tp_fs_state_bytes()
+    g3 = ([int(x) for x in gt], [int(x) for x in i0], [int(x) for x in i1])
+    for f in range(B):
+        T = PyTranscript("truepix")
+        T.u64s(prefixes[f])
+        uu, vv = pairs(u[f]), pairs(v[f])
+        idx, prev = 2, None
+        v_elem, out_elem = [(0, 0)] * 4, [(0, 0)] * 4
+        _, wires, beta, _ = bp.results(f)
+        zg = list(zip([int(x) for x in z1s[f][0]], [int(x) for x in z1s[f][1]]))
+        late = oracle.LateRounds(pairs(wires), beta, zg, g3, n)
+        chals, late_vals = [], []
+        for rd in range(nb + 2 * n):
+            if rd < nb:
+                cf = interpolate_cubic(*pairs(claims[rd, f]))
+            else:
+                cf = late.coefs()
+            tags = []
+            for k, x in enumerate(cf):
+                tags.append(vv[idx])
+                d = f2sub(x, uu[idx])
+                idx += 1
+                T.fp2(*d)
+                if rd >= nb:
+                    late_vals.append(d)
+                v_elem[k] = f2add(v_elem[k], tags[-1])
+                out_elem[k] = f2add(out_elem[k], x)
+            now = tags[0]
+            for t in tags:
+                now = f2add(now, t)
+            e = T.ext("eq")
+            vz = f2mul(now, e) if prev is None else f2mul(f2sub(prev, now), e)
+            T.fp2(*vz)
+            if rd >= nb:
+                late_vals.append(vz)
+            r = T.ext("sc-0-%d" % rd)
+            chals.append(r)
+            p = tags[-1]
+            for t in reversed(tags[:-1]):
+                p = f2add(f2mul(p, r), t)
+            prev = p
+            if rd >= nb:
+                late.next_round(r)
+        assert chals[:nb] == pairs(early_ch[:, f]), f
+        assert chals[nb:] == pairs(late_ch[f]), f
+        assert late_vals == pairs(late_pr[f]), f
+        w3, w1, w2 = chals[:nb], chals[nb:nb + n], chals[nb + n:]
+        cl, pnt, tg, used = closing_python(T, late.line(), prev, idx, v_elem, out_elem, uu, vv, w1, w2, w3,
+                                           pairs(z2[f]), zg, g3)
+        assert cl == pairs(closing[f]), f
+        assert pnt == pairs(point[f]) and tg == tuple(int(x) for x in tag[f])
+        d = ctypes.create_string_buffer(32)
+        assert lib.tp_fs_digest(raw[f * nst:(f + 1) * nst], d) == 0
+        assert d.raw == T.h.digest(), f
+        st = vole["states"].cpu().numpy().tobytes()[f * 160:(f + 1) * 160]
+        assert struct.unpack_from("<Q", st, 0)[0] == used

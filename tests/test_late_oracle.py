@@ -21,14 +21,14 @@ def test_oracle_matches_reference_layer_prover():
 
 
 def test_vole_chain_restatement_matches_reference():
-    """The whole layer's VOLE-committed rounds restated (hashlib transcript, the
+    """The whole layer's VOLE-committed rounds and closing proofs restated (hashlib transcript, the
     commit / equality / challenge / Horner steps, the oracle's late rounds fed
     round by round with the drawn challenges) against the reference's
     LayerProver + ExtVOLECommit + FiatShamir chain (tests/golden/
     layer_vole_golden.npz). The early rounds' coefficients are the golden ones
     (their computation is pinned by the native_fp2 vectors)."""
     from fslib import PyTranscript, f2add, f2mul, f2sub
-    from layervole import cases
+    from layervole import cases, closing_python
     n_cases = 0
     for c in cases():
         n, nb = c["n_in_bits"], c["nb"]
@@ -74,5 +74,14 @@ def test_vole_chain_restatement_matches_reference():
         assert prev == pairs(c["prev"])[0] and idx == int(c["used"][0])
         assert v_elem == pairs(c["v_elem"]) and out_elem == pairs(c["out_elem"])
         assert T.h.digest() == c["digest"].tobytes()
+        # the layer's closing proofs
+        chal = pairs(c["chal"])
+        w3, w1, w2 = chal[:nb], chal[nb:nb + n], chal[nb + n:]
+        closing, point, tag, used = closing_python(T, late.line(), prev, idx, v_elem, out_elem, u, v, w1, w2, w3,
+                                                   pairs(c["z2"]), pairs(c["zg"]), gates)
+        assert closing == pairs(c["closing"]), c["name"]
+        assert point == pairs(c["point"]) and tag == pairs(c["tag"])[0]
+        assert used == int(c["used_closed"][0])
+        assert T.h.digest() == c["digest_closed"].tobytes()
         n_cases += 1
     assert n_cases == 2

@@ -28,6 +28,12 @@ struct Args {
     fp2* h;
     fp2* chal_out;
     fp2* proof;
+    const fp2* z2;
+    const fp2* w3;
+    long long w3_frame_stride, w3_round_stride;
+    fp2* closing;
+    fp2* point;
+    fp2* tag;
     late::Shape sh;
 };
 
@@ -65,6 +71,13 @@ __global__ void __launch_bounds__(kThreads) late_kernel(const Args a, const __gr
     f.h = a.h + i * (n + 1);
     f.chal_out = a.chal_out + i * 2 * n;
     f.proof = a.proof ? a.proof + i * 8 * n : nullptr;
+    const int nb = a.sh.round0;
+    f.z2 = a.closing ? a.z2 + i * nb : nullptr;
+    f.w3 = a.closing ? a.w3 + i * a.w3_frame_stride : nullptr;
+    f.w3_stride = a.w3_round_stride;
+    f.closing = a.closing ? a.closing + i * (n + 10) : nullptr;
+    f.point = a.closing ? a.point + i * (n + nb) : nullptr;
+    f.tag = a.closing ? a.tag + i : nullptr;
     late::run_frame(w, f, a.sh, G.g, DevPar{});
 }
 
@@ -76,15 +89,19 @@ int tp_late_rounds_dev(int n_frames, int n_in_bits, int n_gates, const int* gate
                        const int* in1, const void* d_wires, const void* d_beta, const void* d_gate_weights,
                        int weights_per_frame, const void* d_challenges, void* d_fs_states, void* d_vole_states,
                        const void* d_u, const void* d_v, long long count, int layer, int round0, void* d_coefs,
-                       void* d_line, void* d_challenges_out, void* d_proof, void* stream)
+                       void* d_line, void* d_challenges_out, void* d_proof, const void* d_z2, const void* d_w3,
+                       long long w3_frame_stride, long long w3_round_stride, void* d_closing, void* d_point,
+                       void* d_tag, void* stream)
 {
     tp::clear_error();
     if (!tp::ctx()) return -1;
     const bool given = d_challenges != nullptr;
     const bool vole_mode = d_fs_states && d_vole_states && d_u && d_v && count >= 3;
+    const bool closing = d_closing != nullptr;
     if (n_frames < 1 || n_in_bits < 1 || n_in_bits > late::kMaxInBits || n_gates < 1 || n_gates > late::kMaxGates ||
         !gate_type || !in0 || !in1 || !d_wires || !d_beta || !d_gate_weights || !d_coefs || !d_line ||
-        !d_challenges_out || given == vole_mode || (d_proof && !vole_mode)) {
+        !d_challenges_out || given == vole_mode || (d_proof && !vole_mode) || round0 < 0 || round0 > 64 ||
+        (closing && (!vole_mode || !d_point || !d_tag || (round0 > 0 && (!d_z2 || !d_w3))))) {
         tp::set_error(tp::TP_ERR_ARG, "tp_late_rounds_dev: bad arguments");
         return -1;
     }
@@ -111,6 +128,13 @@ int tp_late_rounds_dev(int n_frames, int n_in_bits, int n_gates, const int* gate
     a.h = static_cast<fp2*>(d_line);
     a.chal_out = static_cast<fp2*>(d_challenges_out);
     a.proof = static_cast<fp2*>(d_proof);
+    a.z2 = static_cast<const fp2*>(d_z2);
+    a.w3 = static_cast<const fp2*>(d_w3);
+    a.w3_frame_stride = w3_frame_stride;
+    a.w3_round_stride = w3_round_stride;
+    a.closing = static_cast<fp2*>(d_closing);
+    a.point = static_cast<fp2*>(d_point);
+    a.tag = static_cast<fp2*>(d_tag);
     a.sh.n = n_in_bits;
     a.sh.n_gates = n_gates;
     a.sh.count = given ? 0 : count;

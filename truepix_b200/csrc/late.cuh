@@ -65,6 +65,28 @@ TP_HD fp2 gatefn(unsigned t, fp2 x, fp2 y)
     }
 }
 
+// gateprover_vole.py p_com_gatefn_ (GateFunctionsPC, :706-720): a gate's value on
+// committed x, y and x*y, by the native type index
+TP_HD fp2 pc_gatefn(unsigned t, fp2 x, fp2 y, fp2 xy)
+{
+    const fp2 one = mk(1, 0);
+    switch (t) {
+    case 0: return xy;
+    case 1: return f2add(x, y);
+    case 2: return f2sub(x, y);
+    case 3: return x;
+    case 4: return y;
+    case 5: return f2sub(f2add(x, y), xy);
+    case 6: return f2sub(f2add(x, y), f2dbl(xy));
+    case 7: return f2sub(one, x);
+    case 8: return f2sub(one, xy);
+    case 9: return f2sub(f2add(one, xy), f2add(x, y));
+    case 10: return f2sub(f2add(one, f2dbl(xy)), f2add(x, y));
+    case 11: return f2sub(y, xy);
+    default: return x;
+    }
+}
+
 // one frame's inputs and outputs (pointers already at the frame)
 struct Frame {
     const fp2* wires;      // 2^n
@@ -79,6 +101,13 @@ struct Frame {
     fp2* h;                // n + 1
     fp2* chal_out;         // 2n
     fp2* proof;            // VOLE mode, optional: 2n x 4 (three d, the equality value)
+    // the layer's closing proofs (VOLE mode, optional)
+    const fp2* z2;         // nb: the copy part of the layer's point
+    const fp2* w3;         // the early challenges: w3[k * w3_stride], k < nb
+    long long w3_stride;
+    fp2* closing;          // n + 10 values in the order they are put
+    fp2* point;            // n + nb: the input point
+    fp2* tag;              // 1: its tag
 };
 
 struct Shape {
@@ -86,7 +115,7 @@ struct Shape {
     int n_gates;
     long long count; // correlations per frame
     int layer;       // labels "sc-<layer>-<round0 + round>"
-    int round0;
+    int round0;      // the early rounds before (their count: nb)
 };
 
 // the CTA's workspace (shared memory on the device)
@@ -99,11 +128,16 @@ struct Work {
     fp2 w[2 * kMaxInBits];     // the challenges
     fp2 pt[kMaxInBits];        // a point on the line
     fp2 h[kMaxInBits + 1];     // the line's values
+    fp2 hc[kMaxInBits + 1];    // its coefficients
+    fp2 vv[kMaxInBits + 1];    // closing: the coefficients' tags
+    fp2 pr[3];                 // closing: tags of x, of the line's sum, of the product
     fp2 beta, v1, r;
     fs::State st;
     vole::State vs;
     int bad;
 };
+
+static_assert(sizeof(Work) <= 48 * 1024, "the workspace fits the static shared memory of a CTA");
 
 // ---- steps -------------------------------------------------------------------
 
@@ -247,7 +281,132 @@ TP_HD void step_interpolate(Work& w, const Frame& f, const Shape& sh)
         c[0] = f2add(f2sub(f2zero(), f2scale(c[0], (u64)i)), d[i]);
         ++deg;
     }
-    for (int i = 0; i <= n; ++i) f.h[i] = c[i];
+    for (int i = 0; i <= n; ++i) f.h[i] = w.hc[i] = c[i];
+}
+
+// ---- the layer's closing proofs (circuitnizkvec_vole.py:433-500, one layer) ----
+
+// thread 0: create_final_prod_pok (:175-218) on the line's coefficients
+TP_HD void step_close_commit(Work& w, const Frame& f, const Shape& sh)
+{
+    const int n = sh.n;
+    if (w.vs.bad || w.vs.idx + (unsigned long long)(n + 2) > (unsigned long long)sh.count) {
+        w.vs.bad = 1;
+        w.bad = 1;
+        return;
+    }
+    fp2* out = f.closing;
+    fp2 sval = f2zero();
+    for (int k = 0; k <= n; ++k) sval = f2add(sval, w.hc[k]);
+    const fp2 prod = f2mul(w.hc[0], sval);
+    fp2 v1, v3;
+    out[0] = vole::commit(w.vs, w.hc[0], f.u, f.v, &v1);
+    out[1] = vole::commit(w.vs, prod, f.u, f.v, &v3);
+    fs::put_fp2(w.st, out[0].re, out[0].im);
+    fs::put_fp2(w.st, out[1].re, out[1].im);
+    fp2 rest_sum = f2zero(), rest_v = f2zero();
+    w.vv[0] = v1;
+    for (int k = 1; k <= n; ++k) {
+        out[1 + k] = vole::commit(w.vs, w.hc[k], f.u, f.v, &w.vv[k]);
+        fs::put_fp2(w.st, out[1 + k].re, out[1 + k].im);
+        rest_sum = f2add(rest_sum, w.hc[k]);
+        rest_v = f2add(rest_v, w.vv[k]);
+    }
+    const uint8_t pv[7] = {'p', 'o', 'k', '-', 'v', 'e', 'c'};
+    fp2 c;
+    fs::rand_ext(w.st, pv, 7, reinterpret_cast<uint64_t*>(&c.re), reinterpret_cast<uint64_t*>(&c.im));
+    out[n + 2] = f2mul(rest_sum, c);
+    out[n + 3] = f2mul(rest_v, c);
+    fp2 vsum = f2zero();
+    for (int k = 0; k <= n; ++k) vsum = f2add(vsum, w.vv[k]);
+    // prod_finish on (x, sum, x * sum) with tags (v1, sum of tags, v3)
+    out[n + 4] = f2mul(v1, vsum);
+    out[n + 5] = f2sub(f2add(f2mul(w.hc[0], vsum), f2mul(sval, v1)), v3);
+    for (int k = 2; k <= 5; ++k) fs::put_fp2(w.st, out[n + k].re, out[n + k].im);
+    w.pr[0] = v1;
+    w.pr[1] = vsum;
+    w.pr[2] = v3;
+}
+
+// per-thread partial sums of the wiring predicates' multilinear extensions times
+// the committed gate values (CircuitVerifier.eval_mlext, circuitverifier.py:224-290,
+// with GateFunctionsPC): sum over gates of z1eq_g * eq(w1, in0_g) * eq(w2, in1_g)
+// * pc_gate(v1, sum, v3)
+TP_HD void step_close_sums(Work& w, const Frame& f, const uint32_t* gates, const Shape& sh, int tid)
+{
+    const int n = sh.n;
+    fp2 s = f2zero();
+    const fp2 one = mk(1, 0);
+    for (int g = tid; g < sh.n_gates; g += kThreads) {
+        const uint32_t t = gates[g];
+        const int in0 = (int)((t >> 14) & 0x3FFFu), in1 = (int)(t & 0x3FFFu);
+        fp2 e = f.zg[g];
+        for (int j = 0; j < n; ++j) {
+            e = f2mul(e, ((in0 >> j) & 1) ? w.w[j] : f2sub(one, w.w[j]));
+            e = f2mul(e, ((in1 >> j) & 1) ? w.w[n + j] : f2sub(one, w.w[n + j]));
+        }
+        s = f2add(s, f2mul(e, pc_gatefn(t >> 28, w.pr[0], w.pr[1], w.pr[2])));
+    }
+    w.red[0][tid] = s;
+    w.red[1][tid] = f2zero();
+    w.red[2][tid] = f2zero();
+}
+
+// thread 0: the equality proof against the last round's value, tau, the proof of
+// knowledge of all round coefficients, the input point and its value proof
+TP_HD void step_close_tail(Work& w, const Frame& f, const Shape& sh)
+{
+    const int n = sh.n, nb = sh.round0;
+    fp2* out = f.closing;
+    // beta's factor: prod over the early challenges of 2 w z + 1 - (w + z)
+    fp2 mz = mk(1, 0);
+    for (int k = 0; k < nb; ++k) {
+        const fp2 wk = f.w3[k * f.w3_stride], zk = f.z2[k];
+        mz = f2mul(mz, f2sub(f2add(f2dbl(f2mul(wk, zk)), mk(1, 0)), f2add(wk, zk)));
+    }
+    const fp2 tv = f2mul(w.red[0][0], mz);
+    const uint8_t eq[2] = {'e', 'q'};
+    fp2 e;
+    fs::rand_ext(w.st, eq, 2, reinterpret_cast<uint64_t*>(&e.re), reinterpret_cast<uint64_t*>(&e.im));
+    out[n + 6] = f2mul(f2sub(w.vs.prev, tv), e);
+    fs::put_fp2(w.st, out[n + 6].re, out[n + 6].im);
+    uint8_t label[32];
+    const uint32_t len = vole::tau_label(label, sh.layer);
+    fp2 tau;
+    fs::rand_ext(w.st, label, len, reinterpret_cast<uint64_t*>(&tau.re), reinterpret_cast<uint64_t*>(&tau.im));
+    fp2 tag = w.vv[n];
+    for (int k = n - 1; k >= 0; --k) tag = f2add(f2mul(tag, tau), w.vv[k]);
+    for (int j = 0; j < n; ++j) f.point[j] = f2add(w.w[j], f2mul(f2sub(w.w[n + j], w.w[j]), tau));
+    for (int k = 0; k < nb; ++k) f.point[n + k] = f.w3[k * f.w3_stride];
+    // create_pok_final
+    fp2 osum = f2zero(), vsum = f2zero();
+    for (int k = 0; k < 4; ++k) {
+        osum = f2add(osum, w.vs.out_elem[k]);
+        vsum = f2add(vsum, w.vs.v_elem[k]);
+    }
+    const uint8_t pf[9] = {'p', 'o', 'k', '-', 'f', 'i', 'n', 'a', 'l'};
+    fp2 c;
+    fs::rand_ext(w.st, pf, 9, reinterpret_cast<uint64_t*>(&c.re), reinterpret_cast<uint64_t*>(&c.im));
+    out[n + 7] = f2mul(osum, c);
+    out[n + 8] = f2mul(vsum, c);
+    fs::put_fp2(w.st, out[n + 7].re, out[n + 7].im);
+    fs::put_fp2(w.st, out[n + 8].re, out[n + 8].im);
+    // put(["gkr_input_point", [[re, im], ...]]): a string, then every coordinate's two ints
+    const uint8_t gp[15] = {'g', 'k', 'r', '_', 'i', 'n', 'p', 'u', 't', '_', 'p', 'o', 'i', 'n', 't'};
+    fs::put_str(w.st, gp, 15);
+    for (int k = 0; k < n + nb; ++k) {
+        fs::absorb_byte(w.st, 0x02);
+        fs::absorb_le(w.st, f.point[k].re, 8);
+        fs::absorb_byte(w.st, 0x02);
+        fs::absorb_le(w.st, f.point[k].im, 8);
+    }
+    // create_input_value_proof
+    const uint8_t iv[9] = {'i', 'n', 'p', 'u', 't', '-', 'v', 'a', 'l'};
+    fs::rand_ext(w.st, iv, 9, reinterpret_cast<uint64_t*>(&c.re), reinterpret_cast<uint64_t*>(&c.im));
+    out[n + 9] = f2mul(tag, c);
+    fs::put_fp2(w.st, out[n + 9].re, out[n + 9].im);
+    w.vs.prev = tag;
+    *f.tag = tag;
 }
 
 // thread 0: the VOLE state and transcript back to the frame
@@ -294,6 +453,15 @@ TP_HD void run_frame(Work& w, const Frame& f, const Shape& sh, const uint32_t* g
             par.one([&] { w.h[t] = w.T[0]; });
         }
         par.one([&] { step_interpolate(w, f, sh); });
+        if (f.closing) {
+            par.one([&] { step_close_commit(w, f, sh); });
+            if (!w.bad) {
+                par.all([&](int tid) { step_close_sums(w, f, gates, sh, tid); });
+                for (int half = kThreads / 2; half > 0; half >>= 1)
+                    par.all([&](int tid) { step_reduce(w, half, tid); });
+                par.one([&] { step_close_tail(w, f, sh); });
+            }
+        }
     }
     par.one([&] { step_store(w, f); });
 }

@@ -56,6 +56,23 @@ TP_HD void interpolate_quadratic(fp2 f0, fp2 f1, fp2 fm1, fp2 c[3])
     c[2] = c2;
 }
 
+// the decimal digits of v at out + n; returns the new length
+TP_HD uint32_t put_decimal(uint8_t* out, uint32_t n, long long v)
+{
+    if (v < 0) {
+        out[n++] = '-';
+        v = -v;
+    }
+    uint8_t dig[20];
+    int k = 0;
+    do {
+        dig[k++] = (uint8_t)('0' + v % 10);
+        v /= 10;
+    } while (v);
+    while (k) out[n++] = dig[--k];
+    return n;
+}
+
 // "sc-<layer>-<round>" into out (at most 3 + 2 * 11 bytes); returns the length
 TP_HD uint32_t sc_label(uint8_t* out, int layer, int round)
 {
@@ -63,22 +80,29 @@ TP_HD uint32_t sc_label(uint8_t* out, int layer, int round)
     out[n++] = 's';
     out[n++] = 'c';
     out[n++] = '-';
-    for (int part = 0; part < 2; ++part) {
-        long long v = part == 0 ? layer : round;
-        if (v < 0) {
-            out[n++] = '-';
-            v = -v;
-        }
-        uint8_t dig[20];
-        int k = 0;
-        do {
-            dig[k++] = (uint8_t)('0' + v % 10);
-            v /= 10;
-        } while (v);
-        while (k) out[n++] = dig[--k];
-        if (part == 0) out[n++] = '-';
-    }
-    return n;
+    n = put_decimal(out, n, layer);
+    out[n++] = '-';
+    return put_decimal(out, n, round);
+}
+
+// "tau-<layer>" into out; returns the length
+TP_HD uint32_t tau_label(uint8_t* out, int layer)
+{
+    out[0] = 't';
+    out[1] = 'a';
+    out[2] = 'u';
+    out[3] = '-';
+    return put_decimal(out, 4, layer);
+}
+
+// ExtVOLECommit.commit with one repetition: the tag v and d = m - u of the next
+// correlation (the caller checks that one remains)
+TP_HD fp2 commit(State& w, fp2 m, const fp2* u, const fp2* v, fp2* tag)
+{
+    *tag = v[w.idx];
+    const fp2 d = f2sub(m, u[w.idx]);
+    ++w.idx;
+    return d;
 }
 
 // One committed round on the coefficients c[0..n_coef) (n_coef <= 4) with the

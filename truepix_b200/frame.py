@@ -272,6 +272,7 @@ class BatchFrameProver:
             assert len(self.groups) == 1
             C = next(iter(self.groups))
             z2s_dev, points_dev = {C: z2s_dev}, {C: points_dev}
+        self._z2s_dev = z2s_dev      # the layer's closing proofs read the copy part of the point
         launches = 0
         beta_of = {}
         for C, fs in self.groups.items():
@@ -355,8 +356,10 @@ class BatchFrameProver:
         in prove() (the states continue from the early rounds; round labels
         continue at the frame's copy-bit count). Results in self.late_coefs
         [B][2 log2 W][3], self.line [B][log2 W + 1], self.late_challenges
-        [B][2 log2 W] and, with vole, self.late_proof [B][2 log2 W][4] (packed
-        Fp2, int64 device tensors)."""
+        [B][2 log2 W] and, with vole, self.late_proof [B][2 log2 W][4] and the
+        layer's closing proofs: self.closing [B][log2 W + 10] (the values put, in
+        order), self.input_point [B][log2 W + copy bits] and self.input_tag [B]
+        (packed Fp2, int64 device tensors)."""
         torch, lib, s = self.torch, self.lib, self._s()
         n = int(math.log2(self.W))
         G = self.gt.size
@@ -386,19 +389,27 @@ class BatchFrameProver:
             rc = lib.tp_late_rounds_dev(self.B, n, G, gt, i0, i1, self.wires.data_ptr(), self.fin_beta.data_ptr(),
                                         d_zg.data_ptr(), 1, d_ch.data_ptr(), None, None, None, None, 0, layer, 0,
                                         self.late_coefs.data_ptr(), self.line.data_ptr(),
-                                        self.late_challenges.data_ptr(), None, s)
+                                        self.late_challenges.data_ptr(), None, None, None, 0, 0, None, None, None, s)
         else:
             if vole is None:
                 raise ValueError("the late rounds on device transcripts are the VOLE-committed rounds: pass vole")
             if any(L.n_copy_bits != self.max_rounds for L in self.layouts):
                 raise ValueError("device transcripts need frames with the same number of rounds")
+            nb = self.max_rounds
             with on_stream():
                 self.late_proof = torch.zeros(self.B * 2 * n * 4 * 2, dtype=i64, device=self.dev)
+                self.closing = torch.zeros(self.B * (n + 10) * 2, dtype=i64, device=self.dev)
+                self.input_point = torch.zeros(self.B * (n + nb) * 2, dtype=i64, device=self.dev)
+                self.input_tag = torch.zeros(self.B * 2, dtype=i64, device=self.dev)
+            z2 = next(iter(self._z2s_dev.values()))
+            # early challenges: self.device_challenges [round][frame]
             rc = lib.tp_late_rounds_dev(self.B, n, G, gt, i0, i1, self.wires.data_ptr(), self.fin_beta.data_ptr(),
                                         d_zg.data_ptr(), 1, None, transcripts.data_ptr(), vole["states"].data_ptr(),
-                                        vole["u"].data_ptr(), vole["v"].data_ptr(), vole["count"], layer,
-                                        self.max_rounds, self.late_coefs.data_ptr(), self.line.data_ptr(),
-                                        self.late_challenges.data_ptr(), self.late_proof.data_ptr(), s)
+                                        vole["u"].data_ptr(), vole["v"].data_ptr(), vole["count"], layer, nb,
+                                        self.late_coefs.data_ptr(), self.line.data_ptr(),
+                                        self.late_challenges.data_ptr(), self.late_proof.data_ptr(), z2.data_ptr(),
+                                        self.device_challenges.data_ptr(), 1, self.B, self.closing.data_ptr(),
+                                        self.input_point.data_ptr(), self.input_tag.data_ptr(), s)
         native.check(lib, rc, "tp_late_rounds_dev")
         self._late_keep = keep     # inputs stay alive until the stream has used them
 
