@@ -1,0 +1,66 @@
+"""truepix_b200.prover against proofs made by the reference prover itself
+(CircuitProverNIZK.run, tests/golden/prover_golden.npz: gray, inv and crop
+frames with fixed pids, VOLE correlations and commitment manifests): the proof
+container assembled from the restated values is byte-identical to the
+reference's proof, and prove_frames, with every step after the IO prefix on the
+device, produces the same bytes."""
+import numpy as np
+import pytest
+
+from proverlib import cases, circuit, fp2_type, restated_proof
+
+pytestmark = pytest.mark.gpu
+
+
+def test_container_from_restated_values_matches_reference_proof():
+    from truepix_b200.prover import LayerTranscript
+    F = fp2_type()
+    n = 0
+    for c in cases():
+        t = LayerTranscript(c["pid"], fp2_type=F)
+        digest = restated_proof(c, t)
+        assert t.proof_bytes() == c["proof"].tobytes(), c["name"]
+        assert digest == c["digest"].tobytes()
+        assert [(x.real, x.imag) for x in t.final_input_point] == [tuple(int(v) for v in p) for p in c["point"]]
+        n += 1
+    assert n == 3
+
+
+def test_device_proofs_match_reference_proofs():
+    import torch
+    from truepix_b200.frame import FrameLayout
+    from truepix_b200.prover import prove_frames
+    F = fp2_type()
+    n = 0
+    for c in cases():
+        gt, i0, i1 = circuit(c["circ"])
+        layout = FrameLayout(copies=c["copies"], copy_size=c["cs"], const_idx=c["ci"], const_val=c["cv"])
+        pix = torch.from_numpy(c["pix"].copy()).cuda()
+        tr = prove_frames([pix], layout, gt, i0, i1, [c["pid"]], [(c["u"], c["v"])], [c["manifest"]], fp2_type=F)
+        t = tr[0]
+        assert t.proof_bytes() == c["proof"].tobytes(), c["name"]
+        assert t.fs.digest() == c["digest"].tobytes()
+        assert (t.final_input_tag.real, t.final_input_tag.imag) == tuple(int(v) for v in c["tag"][0])
+        n += 1
+    assert n == 3
+    # a batch of the same frame twice under two pids: the first proof is the reference's
+    c = next(cases())
+    gt, i0, i1 = circuit(c["circ"])
+    layout = FrameLayout(copies=c["copies"], copy_size=c["cs"], const_idx=c["ci"], const_val=c["cv"])
+    pix = torch.from_numpy(c["pix"].copy()).cuda()
+    tr = prove_frames([pix, pix], layout, gt, i0, i1, [c["pid"], c["pid"] + 1], [(c["u"], c["v"])] * 2,
+                      [c["manifest"]] * 2, fp2_type=F)
+    assert tr[0].proof_bytes() == c["proof"].tobytes()
+    assert tr[1].proof_bytes() != c["proof"].tobytes()
+
+
+def test_too_few_correlations_raise():
+    import torch
+    from truepix_b200.frame import FrameLayout
+    from truepix_b200.prover import prove_frames
+    c = next(cases())
+    gt, i0, i1 = circuit(c["circ"])
+    layout = FrameLayout(copies=c["copies"], copy_size=c["cs"], const_idx=c["ci"], const_val=c["cv"])
+    pix = torch.from_numpy(c["pix"].copy()).cuda()
+    with pytest.raises(IndexError):
+        prove_frames([pix], layout, gt, i0, i1, [c["pid"]], [(c["u"][:40], c["v"][:40])], [c["manifest"]])
