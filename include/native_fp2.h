@@ -262,14 +262,18 @@ int tp_timer_read(float* ms, int* tags, int max_pairs);
  * two product-proof values, the equality value, the two final proof-of-knowledge
  * values, the input value proof), d_point [n_frames][n_in_bits + round0] (the
  * input point: the line at tau, then the early challenges), d_tag [n_frames] (its
- * tag). round0 is the number of early rounds (<= 64). Asynchronous on `stream`. */
+ * tag). zk != 0: the zero-knowledge prover's closing (circuitnizkvec_vole_ZK.py
+ * :188-247, TruePix's default), whose product proof adds three mask commitments
+ * of 1 after the proof-of-knowledge values and the masks' product proof after its
+ * own: d_closing then holds n_in_bits + 15 values per frame. round0 is the number
+ * of early rounds (<= 64). Asynchronous on `stream`. */
 int tp_late_rounds_dev(int n_frames, int n_in_bits, int n_gates, const int* gate_type, const int* in0,
                        const int* in1, const void* d_wires, const void* d_beta, const void* d_gate_weights,
                        int weights_per_frame, const void* d_challenges, void* d_fs_states, void* d_vole_states,
                        const void* d_u, const void* d_v, long long count, int layer, int round0, void* d_coefs,
                        void* d_line, void* d_challenges_out, void* d_proof, const void* d_z2, const void* d_w3,
                        long long w3_frame_stride, long long w3_round_stride, void* d_closing, void* d_point,
-                       void* d_tag, void* stream);
+                       void* d_tag, int zk, void* stream);
 
 /* ---- circuit evaluation: the prover's output vector ----
  * Replaces ArithCircuitIncrementalBuilder.run (libTruePix/arithcircuitbuilder.py:71-108,

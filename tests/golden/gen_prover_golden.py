@@ -1,6 +1,7 @@
 """Golden proofs of the reference prover itself: CircuitProverNIZK.run
-(TruePix-main/libTruePix/circuitnizkvec_vole.py:265-500) on small frames of the
-gray, inv and crop circuits, with a fixed process id, a VOLE prover file in the
+(TruePix-main/libTruePix/circuitnizkvec_vole.py:265-500, and its
+zero-knowledge variant circuitnizkvec_vole_ZK.py:293-520, TruePix's default) on
+small frames of the gray, inv and crop circuits, with a fixed process id, a VOLE prover file in the
 reference's binary format (ExtVOLEGen.py:25-50, 130-186) holding seeded
 correlations, and an Orion commitment manifest (fp2_link.py:426-504) with fixed
 roots.
@@ -29,16 +30,21 @@ REF = os.path.join(os.environ.get("TRUEPIX_REF", "/root/reference"), "TruePix-ma
 P61 = (1 << 61) - 1
 LAYOUT_ID = "copy-major-384-const128-pad512-v1"
 
-# name, circuit, copies, copy_size, const_idx, const_val, pid, zk
-CASES = [("gray4", "gray", 4, 384, 384, 128, 4242, True),
-         ("inv7", "inv", 7, 384, 384, 255, 777, False),
-         ("crop3", "Crop", 3, 385, 385, 128, 31337, True)]
+# name, circuit, copies, copy_size, const_idx, const_val, pid, zk manifest, zero-knowledge prover
+CASES = [("gray4", "gray", 4, 384, 384, 128, 4242, True, False),
+         ("inv7", "inv", 7, 384, 384, 255, 777, False, False),
+         ("crop3", "Crop", 3, 385, 385, 128, 31337, True, False),
+         ("gray4zk", "gray", 4, 384, 384, 128, 5151, True, True),
+         ("crop5zk", "Crop", 5, 385, 385, 128, 2718, True, True)]
 
 
-def run_case(rng, circ, copies, cs, ci, cv, pid, zk, workdir):
+def run_case(rng, circ, copies, cs, ci, cv, pid, zk, zk_prover, workdir):
     sys.path.insert(0, REF)
     warnings.simplefilter("ignore", SyntaxWarning)
-    import libTruePix.circuitnizkvec_vole as cnv
+    if zk_prover:      # TruePix's default mode: circuitnizkvec_vole_ZK.py
+        import libTruePix.circuitnizkvec_vole_ZK as cnv
+    else:
+        import libTruePix.circuitnizkvec_vole as cnv
     import libTruePix.gateprover as gp
     import libTruePix.util as util
     from libTruePix.extfield import Fp2
@@ -83,7 +89,7 @@ def run_case(rng, circ, copies, cs, ci, cv, pid, zk, workdir):
         fp2s += vals
         lens.append(len(vals))
     pk = lambda xs: np.array([[int(x.real), int(x.imag)] for x in xs], np.uint64).reshape(-1, 2)
-    return dict(pix=pix, layout=np.array(json.dumps([circ, copies, cs, ci, cv, pid]).encode(), "S"),
+    return dict(pix=pix, layout=np.array(json.dumps([circ, copies, cs, ci, cv, pid, int(zk_prover)]).encode(), "S"),
                 u=u, v=v, manifest=np.array(json.dumps(manifest).encode(), "S"),
                 proof=np.frombuffer(proof, np.uint8), trans_fp2=pk(fp2s), trans_lens=np.array(lens, np.int32),
                 point=pk(prv.final_input_point), tag=pk([prv.final_input_tag]),
@@ -94,8 +100,8 @@ def main():
     rng = np.random.default_rng(20261204)
     arrays = {}
     with tempfile.TemporaryDirectory() as workdir:
-        for (name, circ, copies, cs, ci, cv, pid, zk) in CASES:
-            for k, val in run_case(rng, circ, copies, cs, ci, cv, pid, zk, workdir).items():
+        for (name, circ, copies, cs, ci, cv, pid, zk, zk_prover) in CASES:
+            for k, val in run_case(rng, circ, copies, cs, ci, cv, pid, zk, zk_prover, workdir).items():
                 arrays[name + "_" + k] = val
     np.savez_compressed(os.path.join(HERE, "prover_golden.npz"), **arrays)
     print("wrote", len(CASES), "cases")

@@ -64,12 +64,14 @@ def vole_state_fields(b):
                 out_elem=[f(96 + 16 * k) for k in range(4)])
 
 
-def closing_python(T, line, prev, idx, v_elem, out_elem, u, v, w1, w2, w3, z2, zg, gates, layer=0):
+def closing_python(T, line, prev, idx, v_elem, out_elem, u, v, w1, w2, w3, z2, zg, gates, layer=0, zk=False):
     """The layer's closing proofs (circuitnizkvec_vole.py:433-500, one layer)
     restated on the hashlib transcript T: create_final_prod_pok on the line's
     coefficients, eval_mlext with GateFunctionsPC, the equality proof, tau, the
     input point and its tag, create_pok_final, the point put, the input value
-    proof. Returns (closing values in put order, point, tag, correlations used)."""
+    proof. zk: the zero-knowledge prover's product proof (circuitnizkvec_vole_ZK.py
+    :188-247), with three mask commitments of 1 and their product proof.
+    Returns (closing values in put order, point, tag, correlations used)."""
     from fslib import f2add, f2mul, f2sub
     import struct as _st
     n = len(line) - 1
@@ -104,8 +106,16 @@ def closing_python(T, line, prev, idx, v_elem, out_elem, u, v, w1, w2, w3, z2, z
     vsum = (0, 0)
     for t in tags:
         vsum = f2add(vsum, t)
+    if zk:
+        mask = [commit((1, 0)) for _ in range(3)]
+        for _, d in mask:
+            put(d)
     put(f2mul(v1, vsum))
     put(f2sub(f2add(f2mul(line[0], vsum), f2mul(sval, v1)), v3))
+    if zk:
+        (m1, _), (m2, _), (m3, _) = mask
+        put(f2mul(m1, m2))
+        put(f2sub(f2add(m2, m1), m3))
     pr = (v1, vsum, v3)
     one = (1, 0)
 

@@ -54,9 +54,9 @@ def fp2_type():
 def cases():
     g = np.load(os.path.join(ROOT, "tests", "golden", "prover_golden.npz"))
     for n in sorted(k[:-4] for k in g.files if k.endswith("_pix")):
-        circ, copies, cs, ci, cv, pid = json.loads(g[n + "_layout"].tobytes().decode())
+        circ, copies, cs, ci, cv, pid, zk = json.loads(g[n + "_layout"].tobytes().decode())
         d = {k[len(n) + 1:]: g[k] for k in g.files if k.startswith(n + "_")}
-        d.update(name=n, circ=circ, copies=copies, cs=cs, ci=ci, cv=cv, pid=pid,
+        d.update(name=n, circ=circ, copies=copies, cs=cs, ci=ci, cv=cv, pid=pid, zk=bool(zk),
                  manifest=json.loads(g[n + "_manifest"].tobytes().decode()))
         yield d
 
@@ -160,6 +160,6 @@ def restated_proof(c, lib_transcript):
             late_vals.append(row)
     w3, w1, w2 = chals[:nb], chals[nb:nb + n], chals[nb + n:]
     closing, point, tag, _ = closing_python(T, late.line(), prev, idx, v_elem, out_elem, u, v, w1, w2, w3, z2, zg,
-                                            tuple([int(x) for x in a] for a in (gt, i0, i1)))
-    t.record(early, late_vals, closing, point, tag)
+                                            tuple([int(x) for x in a] for a in (gt, i0, i1)), zk=c["zk"])
+    t.record(early, late_vals, closing, point, tag, zk=c["zk"])
     return T.h.digest()

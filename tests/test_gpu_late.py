@@ -48,7 +48,7 @@ def run_given(lib, n, gates, wires, beta, zg, chal, n_frames=1, per_frame=1):
     rc = lib.tp_late_rounds_dev(n_frames, n, gt.size, gt.ctypes.data_as(I32P), i0.ctypes.data_as(I32P),
                                 i1.ctypes.data_as(I32P), d_w.data_ptr(), d_b.data_ptr(), d_z.data_ptr(), per_frame,
                                 d_c.data_ptr(), None, None, None, None, 0, 0, 0, coefs.data_ptr(), line.data_ptr(),
-                                cho.data_ptr(), None, None, None, 0, 0, None, None, None, None)
+                                cho.data_ptr(), None, None, None, 0, 0, None, None, None, 0, None)
     assert rc == 0, lib.tp_last_error()
     torch.cuda.synchronize()
     return (host(coefs, (n_frames, 6 * n, 2)), host(line, (n_frames, n + 1, 2)), host(cho, (n_frames, 2 * n, 2)))
@@ -96,7 +96,7 @@ def test_vole_rounds_match_reference_chain(lib):
                                         None, d_st.data_ptr(), d_vs.data_ptr(), d_u.data_ptr(), d_v.data_ptr(),
                                         len(c["u"]), 0, nb, coefs.data_ptr(), line.data_ptr(), cho.data_ptr(),
                                         proof.data_ptr(), d_z2.data_ptr(), d_w3.data_ptr(), 0, 1,
-                                        closing.data_ptr() if close else None, point.data_ptr(), tag.data_ptr(),
+                                        closing.data_ptr() if close else None, point.data_ptr(), tag.data_ptr(), 0,
                                         None)
             assert rc == 0, lib.tp_last_error()
             torch.cuda.synchronize()
@@ -158,7 +158,7 @@ def test_running_out_of_correlations_stops_the_frame(lib):
                                 i1.ctypes.data_as(I32P), d_w.data_ptr(), d_b.data_ptr(), d_z.data_ptr(), 0, None,
                                 d_st.data_ptr(), d_vs.data_ptr(), d_u.data_ptr(), d_v.data_ptr(), count, 0, nb,
                                 coefs.data_ptr(), line.data_ptr(), cho.data_ptr(), None, None, None, 0, 0, None, None,
-                                None, None)
+                                None, 0, None)
     assert rc == 0, lib.tp_last_error()
     torch.cuda.synchronize()
     raw = d_vs.cpu().numpy().tobytes()
@@ -259,7 +259,7 @@ def test_bad_arguments_are_rejected(lib):
                                       np.ascontiguousarray(i0, np.int32).ctypes.data_as(I32P),
                                       np.ascontiguousarray(i1, np.int32).ctypes.data_as(I32P), wires, beta, zg, 1,
                                       ch, None, None, None, None, 0, 0, 0, coefs, line, cho, proof, None, None, 0, 0,
-                                      closing, line, cho, None)
+                                      closing, line, cho, 0, None)
 
     assert call() == 0
     assert call(n=10) == -1

@@ -1,6 +1,7 @@
 """truepix_b200.prover against proofs made by the reference prover itself
-(CircuitProverNIZK.run, tests/golden/prover_golden.npz: gray, inv and crop
-frames with fixed pids, VOLE correlations and commitment manifests): the proof
+(CircuitProverNIZK.run of circuitnizkvec_vole.py and of its zero-knowledge
+variant, tests/golden/prover_golden.npz: gray, inv and crop frames with fixed
+pids, VOLE correlations and commitment manifests): the proof
 container assembled from the restated values is byte-identical to the
 reference's proof, and prove_frames, with every step after the IO prefix on the
 device, produces the same bytes."""
@@ -23,7 +24,7 @@ def test_container_from_restated_values_matches_reference_proof():
         assert digest == c["digest"].tobytes()
         assert [(x.real, x.imag) for x in t.final_input_point] == [tuple(int(v) for v in p) for p in c["point"]]
         n += 1
-    assert n == 3
+    assert n == 5
 
 
 def test_device_proofs_match_reference_proofs():
@@ -36,20 +37,21 @@ def test_device_proofs_match_reference_proofs():
         gt, i0, i1 = circuit(c["circ"])
         layout = FrameLayout(copies=c["copies"], copy_size=c["cs"], const_idx=c["ci"], const_val=c["cv"])
         pix = torch.from_numpy(c["pix"].copy()).cuda()
-        tr = prove_frames([pix], layout, gt, i0, i1, [c["pid"]], [(c["u"], c["v"])], [c["manifest"]], fp2_type=F)
+        tr = prove_frames([pix], layout, gt, i0, i1, [c["pid"]], [(c["u"], c["v"])], [c["manifest"]], fp2_type=F,
+                          zk=c["zk"])
         t = tr[0]
         assert t.proof_bytes() == c["proof"].tobytes(), c["name"]
         assert t.fs.digest() == c["digest"].tobytes()
         assert (t.final_input_tag.real, t.final_input_tag.imag) == tuple(int(v) for v in c["tag"][0])
         n += 1
-    assert n == 3
+    assert n == 5
     # a batch of the same frame twice under two pids: the first proof is the reference's
     c = next(cases())
     gt, i0, i1 = circuit(c["circ"])
     layout = FrameLayout(copies=c["copies"], copy_size=c["cs"], const_idx=c["ci"], const_val=c["cv"])
     pix = torch.from_numpy(c["pix"].copy()).cuda()
     tr = prove_frames([pix, pix], layout, gt, i0, i1, [c["pid"], c["pid"] + 1], [(c["u"], c["v"])] * 2,
-                      [c["manifest"]] * 2, fp2_type=F)
+                      [c["manifest"]] * 2, fp2_type=F, zk=c["zk"])
     assert tr[0].proof_bytes() == c["proof"].tobytes()
     assert tr[1].proof_bytes() != c["proof"].tobytes()
 

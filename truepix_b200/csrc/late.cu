@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kThreads) late_kernel(const Args a, const __gr
     f.z2 = a.closing ? a.z2 + i * nb : nullptr;
     f.w3 = a.closing ? a.w3 + i * a.w3_frame_stride : nullptr;
     f.w3_stride = a.w3_round_stride;
-    f.closing = a.closing ? a.closing + i * (n + 10) : nullptr;
+    f.closing = a.closing ? a.closing + i * (n + 10 + 5 * (a.sh.zk != 0)) : nullptr;
     f.point = a.closing ? a.point + i * (n + nb) : nullptr;
     f.tag = a.closing ? a.tag + i : nullptr;
     late::run_frame(w, f, a.sh, G.g, DevPar{});
@@ -91,7 +91,7 @@ int tp_late_rounds_dev(int n_frames, int n_in_bits, int n_gates, const int* gate
                        const void* d_u, const void* d_v, long long count, int layer, int round0, void* d_coefs,
                        void* d_line, void* d_challenges_out, void* d_proof, const void* d_z2, const void* d_w3,
                        long long w3_frame_stride, long long w3_round_stride, void* d_closing, void* d_point,
-                       void* d_tag, void* stream)
+                       void* d_tag, int zk, void* stream)
 {
     tp::clear_error();
     if (!tp::ctx()) return -1;
@@ -140,6 +140,7 @@ int tp_late_rounds_dev(int n_frames, int n_in_bits, int n_gates, const int* gate
     a.sh.count = given ? 0 : count;
     a.sh.layer = layer;
     a.sh.round0 = round0;
+    a.sh.zk = zk ? 1 : 0;
     late_kernel<<<n_frames, kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(a, G);
     return tp::cuda_failed(cudaGetLastError(), "late rounds") ? -1 : 0;
 }

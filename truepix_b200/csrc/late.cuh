@@ -105,7 +105,7 @@ struct Frame {
     const fp2* z2;         // nb: the copy part of the layer's point
     const fp2* w3;         // the early challenges: w3[k * w3_stride], k < nb
     long long w3_stride;
-    fp2* closing;          // n + 10 values in the order they are put
+    fp2* closing;          // n + 10 (zero-knowledge prover: n + 15) values in the order they are put
     fp2* point;            // n + nb: the input point
     fp2* tag;              // 1: its tag
 };
@@ -116,6 +116,7 @@ struct Shape {
     long long count; // correlations per frame
     int layer;       // labels "sc-<layer>-<round0 + round>"
     int round0;      // the early rounds before (their count: nb)
+    int zk;          // closing proofs of the zero-knowledge prover (circuitnizkvec_vole_ZK.py)
 };
 
 // the CTA's workspace (shared memory on the device)
@@ -286,11 +287,19 @@ TP_HD void step_interpolate(Work& w, const Frame& f, const Shape& sh)
 
 // ---- the layer's closing proofs (circuitnizkvec_vole.py:433-500, one layer) ----
 
-// thread 0: create_final_prod_pok (:175-218) on the line's coefficients
+// index of the equality value among the closing values (before it: two
+// commitments, n commitments, two proof-of-knowledge values, with zk three mask
+// commitments, the product proof's two values and with zk the masks' two)
+TP_HD int close_eq_index(const Shape& sh) { return sh.n + 6 + 5 * (sh.zk != 0); }
+
+// thread 0: create_final_prod_pok (:175-218; the zero-knowledge prover's,
+// circuitnizkvec_vole_ZK.py:188-247, adds three mask commitments of 1 and their
+// product proof) on the line's coefficients
 TP_HD void step_close_commit(Work& w, const Frame& f, const Shape& sh)
 {
     const int n = sh.n;
-    if (w.vs.bad || w.vs.idx + (unsigned long long)(n + 2) > (unsigned long long)sh.count) {
+    const int zk = sh.zk != 0;
+    if (w.vs.bad || w.vs.idx + (unsigned long long)(n + 2 + 3 * zk) > (unsigned long long)sh.count) {
         w.vs.bad = 1;
         w.bad = 1;
         return;
@@ -317,12 +326,30 @@ TP_HD void step_close_commit(Work& w, const Frame& f, const Shape& sh)
     fs::rand_ext(w.st, pv, 7, reinterpret_cast<uint64_t*>(&c.re), reinterpret_cast<uint64_t*>(&c.im));
     out[n + 2] = f2mul(rest_sum, c);
     out[n + 3] = f2mul(rest_v, c);
+    fs::put_fp2(w.st, out[n + 2].re, out[n + 2].im);
+    fs::put_fp2(w.st, out[n + 3].re, out[n + 3].im);
+    int k = n + 4;
+    fp2 mtag[3];
+    if (zk) {
+        for (int q = 0; q < 3; ++q) {
+            out[k] = vole::commit(w.vs, mk(1, 0), f.u, f.v, &mtag[q]);
+            fs::put_fp2(w.st, out[k].re, out[k].im);
+            ++k;
+        }
+    }
     fp2 vsum = f2zero();
-    for (int k = 0; k <= n; ++k) vsum = f2add(vsum, w.vv[k]);
+    for (int q = 0; q <= n; ++q) vsum = f2add(vsum, w.vv[q]);
     // prod_finish on (x, sum, x * sum) with tags (v1, sum of tags, v3)
-    out[n + 4] = f2mul(v1, vsum);
-    out[n + 5] = f2sub(f2add(f2mul(w.hc[0], vsum), f2mul(sval, v1)), v3);
-    for (int k = 2; k <= 5; ++k) fs::put_fp2(w.st, out[n + k].re, out[n + k].im);
+    out[k] = f2mul(v1, vsum);
+    out[k + 1] = f2sub(f2add(f2mul(w.hc[0], vsum), f2mul(sval, v1)), v3);
+    fs::put_fp2(w.st, out[k].re, out[k].im);
+    fs::put_fp2(w.st, out[k + 1].re, out[k + 1].im);
+    if (zk) {   // prod_finish on (1, 1, 1) with the masks' tags
+        out[k + 2] = f2mul(mtag[0], mtag[1]);
+        out[k + 3] = f2sub(f2add(mtag[1], mtag[0]), mtag[2]);
+        fs::put_fp2(w.st, out[k + 2].re, out[k + 2].im);
+        fs::put_fp2(w.st, out[k + 3].re, out[k + 3].im);
+    }
     w.pr[0] = v1;
     w.pr[1] = vsum;
     w.pr[2] = v3;
@@ -357,7 +384,7 @@ TP_HD void step_close_sums(Work& w, const Frame& f, const uint32_t* gates, const
 TP_HD void step_close_tail(Work& w, const Frame& f, const Shape& sh)
 {
     const int n = sh.n, nb = sh.round0;
-    fp2* out = f.closing;
+    fp2* out = f.closing + (close_eq_index(sh) - (n + 6));   // out[n + 6]: the equality value
     // beta's factor: prod over the early challenges of 2 w z + 1 - (w + z)
     fp2 mz = mk(1, 0);
     for (int k = 0; k < nb; ++k) {

@@ -348,7 +348,7 @@ class BatchFrameProver:
                     self.mle[2 * f:2 * f + 2].copy_(out[2 * q:2 * q + 2])
         self.launches_last = launches
 
-    def prove_late(self, z1s, challenges=None, transcripts=None, vole=None, layer: int = 0) -> None:
+    def prove_late(self, z1s, challenges=None, transcripts=None, vole=None, layer: int = 0, zk: bool = False) -> None:
         """The late rounds and the line projection of every frame, after prove():
         one launch (tp_late_rounds_dev) from the batch's wires and beta. z1s: the
         per-gate weights given to prove() (uint64 [2, n_gates] per frame).
@@ -358,8 +358,9 @@ class BatchFrameProver:
         [B][2 log2 W][3], self.line [B][log2 W + 1], self.late_challenges
         [B][2 log2 W] and, with vole, self.late_proof [B][2 log2 W][4] and the
         layer's closing proofs: self.closing [B][log2 W + 10] (the values put, in
-        order), self.input_point [B][log2 W + copy bits] and self.input_tag [B]
-        (packed Fp2, int64 device tensors)."""
+        order; log2 W + 15 with zk, the zero-knowledge prover's product proof),
+        self.input_point [B][log2 W + copy bits] and self.input_tag [B] (packed
+        Fp2, int64 device tensors)."""
         torch, lib, s = self.torch, self.lib, self._s()
         n = int(math.log2(self.W))
         G = self.gt.size
@@ -389,7 +390,8 @@ class BatchFrameProver:
             rc = lib.tp_late_rounds_dev(self.B, n, G, gt, i0, i1, self.wires.data_ptr(), self.fin_beta.data_ptr(),
                                         d_zg.data_ptr(), 1, d_ch.data_ptr(), None, None, None, None, 0, layer, 0,
                                         self.late_coefs.data_ptr(), self.line.data_ptr(),
-                                        self.late_challenges.data_ptr(), None, None, None, 0, 0, None, None, None, s)
+                                        self.late_challenges.data_ptr(), None, None, None, 0, 0, None, None, None, 0,
+                                        s)
         else:
             if vole is None:
                 raise ValueError("the late rounds on device transcripts are the VOLE-committed rounds: pass vole")
@@ -398,7 +400,7 @@ class BatchFrameProver:
             nb = self.max_rounds
             with on_stream():
                 self.late_proof = torch.zeros(self.B * 2 * n * 4 * 2, dtype=i64, device=self.dev)
-                self.closing = torch.zeros(self.B * (n + 10) * 2, dtype=i64, device=self.dev)
+                self.closing = torch.zeros(self.B * (n + (15 if zk else 10)) * 2, dtype=i64, device=self.dev)
                 self.input_point = torch.zeros(self.B * (n + nb) * 2, dtype=i64, device=self.dev)
                 self.input_tag = torch.zeros(self.B * 2, dtype=i64, device=self.dev)
             z2 = next(iter(self._z2s_dev.values()))
@@ -409,7 +411,7 @@ class BatchFrameProver:
                                         self.late_coefs.data_ptr(), self.line.data_ptr(),
                                         self.late_challenges.data_ptr(), self.late_proof.data_ptr(), z2.data_ptr(),
                                         self.device_challenges.data_ptr(), 1, self.B, self.closing.data_ptr(),
-                                        self.input_point.data_ptr(), self.input_tag.data_ptr(), s)
+                                        self.input_point.data_ptr(), self.input_tag.data_ptr(), int(zk), s)
         native.check(lib, rc, "tp_late_rounds_dev")
         self._late_keep = keep     # inputs stay alive until the stream has used them
 

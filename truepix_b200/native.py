@@ -102,7 +102,7 @@ GKR_SIGNATURES = {
     "tp_fs_rand_ext_dev": (_I32, [_VP, _I32, ctypes.c_char_p, _VP, _VP]),
     "tp_late_rounds_dev": (_I32, [_I32, _I32, _I32, _PI32, _PI32, _PI32, _VP, _VP, _VP, _I32, _VP, _VP, _VP, _VP,
                                   _VP, ctypes.c_longlong, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP,
-                                  ctypes.c_longlong, ctypes.c_longlong, _VP, _VP, _VP, _VP]),
+                                  ctypes.c_longlong, ctypes.c_longlong, _VP, _VP, _VP, _I32, _VP]),
     "tp_circuit_out_bits": (_I32, [_I32]),
     "tp_circuit_outputs_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _I32, _PI32, _PI32, _PI32,
                                             _VP, _VP]),

@@ -1,6 +1,7 @@
 """The reference prover's proof of a frame (TruePix-main/libTruePix/
-circuitnizkvec_vole.py:265-500, CircuitProverNIZK.run) for the one-layer TruePix
-circuits, with every step after the transcript's IO prefix on the device:
+circuitnizkvec_vole.py:265-500, CircuitProverNIZK.run, and the zero-knowledge
+variant circuitnizkvec_vole_ZK.py:293-520, TruePix's default) for the one-layer
+TruePix circuits, with every step after the transcript's IO prefix on the device:
 
   host    put(pid), put(muxbits = None, io), put(["private_input_omitted", n], io),
           put(outputs, io), put(commit_binding(manifest)), z1 / z2 = rand_ext(...)
@@ -108,25 +109,34 @@ class LayerTranscript:
         z2 = [pair(fs.rand_ext("z2-%d" % i)) for i in range(n_copy_bits)]
         return z1, z2
 
-    def record(self, early, late, closing, point, tag) -> None:
+    def record(self, early, late, closing, point, tag, zk: bool = False) -> None:
         """Append the values the device put to the trans queue in the reference's
         order (early: [rounds][5] = four d, the equality value; late: [rounds][4];
-        closing: the n + 10 closing values; point, tag: the input point and tag)."""
+        closing: the closing values, n + 10, or n + 15 for the zero-knowledge
+        prover; point, tag: the input point and tag)."""
         t = self.fs.trans
         for rnd in list(early) + list(late):
             for x in rnd:
                 t.append([self._f(x)])
-        n = len(closing) - 10
+        n = len(closing) - (15 if zk else 10)
         cl = [self._f(x) for x in closing]
         t.append([(cl[0], cl[1])])
         for k in range(n):
             t.append([cl[2 + k]])
         t.append([(cl[n + 2], cl[n + 3])])
-        t.append([(cl[n + 4], cl[n + 5])])
-        t.append([cl[n + 6]])
-        t.append([(cl[n + 7], cl[n + 8])])
+        k = n + 4
+        if zk:       # circuitnizkvec_vole_ZK.py:224-240: the masks' commitments, then both product proofs
+            t.append([(cl[k], cl[k + 1], cl[k + 2])])
+            k += 3
+        t.append([(cl[k], cl[k + 1])])
+        k += 2
+        if zk:
+            t.append([(cl[k], cl[k + 1])])
+            k += 2
+        t.append([cl[k]])
+        t.append([(cl[k + 1], cl[k + 2])])
         t.append(["gkr_input_point", [[int(a), int(b)] for a, b in point]])
-        t.append([cl[n + 9]])
+        t.append([cl[k + 3]])
         self.final_input_point = [self._f(x) for x in point]
         self.final_input_tag = self._f(tag)
 
@@ -152,14 +162,16 @@ def gate_weights(lib, z1, n_gates: int) -> np.ndarray:
 
 
 def prove_frames(frames, layout, gate_type, in0, in1, pids, correlations, manifests, fp2_type=None,
-                 stream=None):
+                 stream=None, zk: bool = True):
     """Proofs of a batch of frames of one size and circuit.
 
     frames: uint8 device tensors (layout.copies * layout.copy_size bytes each);
     layout: truepix_b200.frame.FrameLayout; gate tables of the circuit; pids,
     correlations [(u, v) uint64 [count, 2]] (the same count for every frame) and
-    commitment manifests per frame. Returns one LayerTranscript per frame
-    (proof_bytes() is the reference's proof)."""
+    commitment manifests per frame. zk: the zero-knowledge prover
+    (circuitnizkvec_vole_ZK.py, TruePix's default), else circuitnizkvec_vole.py.
+    Returns one LayerTranscript per frame (proof_bytes() is the reference's
+    proof)."""
     import torch
     from .frame import BatchFrameProver, circuit_outputs, pack_fp2
     lib = native.gkr()
@@ -202,7 +214,7 @@ def prove_frames(frames, layout, gate_type, in0, in1, pids, correlations, manife
                 v=torch.from_numpy(v.view(np.int64).reshape(-1).copy()).to(dev), count=count)
     bp = BatchFrameProver([layout] * B, gt, i0, i1, device=dev.index or 0, stream=stream)
     bp.prove(frames, z1s, d_z2, d_pt, None, transcripts=states, vole=vole)
-    bp.prove_late(z1s, transcripts=states, vole=vole)
+    bp.prove_late(z1s, transcripts=states, vole=vole, zk=zk)
     if stream is not None:
         stream.synchronize()
     torch.cuda.synchronize(dev)
@@ -212,12 +224,12 @@ def prove_frames(frames, layout, gate_type, in0, in1, pids, correlations, manife
     n = int(math.log2(layout.n_wires))
     early = bp.device_proof.cpu().numpy().view(np.uint64).reshape(nb, B, 5, 2)
     late = bp.late_proof.cpu().numpy().view(np.uint64).reshape(B, 2 * n, 4, 2)
-    closing = bp.closing.cpu().numpy().view(np.uint64).reshape(B, n + 10, 2)
+    closing = bp.closing.cpu().numpy().view(np.uint64).reshape(B, n + (15 if zk else 10), 2)
     point = bp.input_point.cpu().numpy().view(np.uint64).reshape(B, n + nb, 2)
     tag = bp.input_tag.cpu().numpy().view(np.uint64).reshape(B, 2)
     for f in range(B):
         if struct.unpack_from("<I", raw_vs, f * nvs + 12)[0]:
             raise IndexError("frame %d: VOLE correlations ran out (%d given)" % (f, count))
-        tr[f].record(early[:, f], late[f], closing[f], point[f], tag[f])
+        tr[f].record(early[:, f], late[f], closing[f], point[f], tag[f], zk=zk)
         tr[f].fs.set_state(raw_st[f * nst:(f + 1) * nst])
     return tr
