@@ -66,3 +66,29 @@ def test_too_few_correlations_raise():
     pix = torch.from_numpy(c["pix"].copy()).cuda()
     with pytest.raises(IndexError):
         prove_frames([pix], layout, gt, i0, i1, [c["pid"]], [(c["u"][:40], c["v"][:40])], [c["manifest"]])
+
+
+def test_commit_then_prove():
+    """The commit phase and the proof in one process: the frame committed on the
+    device (zero-knowledge commit pair), its manifest built from the roots
+    (manifests_of), the proof bound to it equal to the restated proof of the same
+    frame under the same manifest."""
+    import torch
+    from truepix_b200.frame import FrameLayout
+    from truepix_b200.orion import FrameCommitter
+    from truepix_b200.prover import LayerTranscript, manifests_of, prove_frames
+    F = fp2_type()
+    c = [x for x in cases() if x["name"] == "gray4zk"][0]
+    gt, i0, i1 = circuit(c["circ"])
+    layout = FrameLayout(copies=c["copies"], copy_size=c["cs"], const_idx=c["ci"], const_val=c["cv"])
+    pix = torch.from_numpy(c["pix"].copy()).cuda()
+    fc = FrameCommitter([layout], zk=True)
+    fc.commit([pix], mask_seeds=[0x5EED])
+    torch.cuda.synchronize()
+    [m] = manifests_of(fc)
+    assert m["masked_root"] == fc.root_hex(0) and len(m["mask_root"]) == 64 and m["zk"]
+    [t] = prove_frames([pix], layout, gt, i0, i1, [c["pid"]], [(c["u"], c["v"])], [m], fp2_type=F, zk=True)
+    c2 = dict(c, manifest=m)
+    t2 = LayerTranscript(c["pid"], fp2_type=F)
+    restated_proof(c2, t2)
+    assert t.proof_bytes() == t2.proof_bytes()

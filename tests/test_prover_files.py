@@ -44,3 +44,25 @@ def test_commit_binding_fields():
                                                "const_idx", "const_val", "n", "lg_n")]
         assert b[12:] == [m["masked_root"], m["mask_root"] or ""]
         json.dumps(b)
+
+
+def test_commit_manifest_of_a_layout():
+    """the manifest of the commit phase for a frame layout: the fields of
+    make_layout (padded copies, 512-entry copies, n, lg_n) and the roots as
+    root_hex strings (pinned to the reference's hex of its own roots)"""
+    import os
+    from proverlib import ROOT
+    from truepix_b200.frame import FrameLayout
+    from truepix_b200.orion import FrameCommitter
+    from truepix_b200.prover import commit_manifest
+    g = np.load(os.path.join(ROOT, "tests", "golden", "orion_zk_golden.npz"))
+    root = g["zkmasked_gray40"].tobytes()
+    hx = FrameCommitter.hex(root)
+    assert hx == g["zkmaskedhex_gray40"].tobytes().decode()
+    L = FrameLayout.for_frame(1080, 1920)
+    m = commit_manifest(L, hx, "00" * 32, zk=True)
+    assert (m["copies"], m["padded_copies"], m["copy_size"], m["padded_copy_size"]) == (16200, 16384, 384, 512)
+    assert (m["const_idx"], m["const_val"], m["n"], m["lg_n"]) == (384, 128, 1 << 23, 23)
+    assert m["masked_root"] == hx and m["mask_root"] == "00" * 32 and m["zk"] is True
+    m = commit_manifest(FrameLayout(copies=5, copy_size=384, const_idx=-1, const_val=0), hx, zk=False)
+    assert m["mask_root"] == "" and m["zk"] is False and m["padded_copies"] == 8 and m["const_idx"] == -1

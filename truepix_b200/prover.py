@@ -62,6 +62,28 @@ def commit_binding(manifest: dict) -> list:
             + [manifest["masked_root"], manifest.get("mask_root") or ""])
 
 
+def commit_manifest(layout, masked_root: str, mask_root: str = "", zk: bool = True) -> dict:
+    """The manifest the reference's commit phase writes (truepix_gkr.h:391-418,
+    with the layout of make_layout :106-150) for a frame committed in `layout`
+    (truepix_b200.frame.FrameLayout); roots as root_hex strings
+    (FrameCommitter.root_hex)."""
+    n = layout.padded_copies * layout.n_wires
+    return dict(protocol=PROTOCOL_ID, layout=LAYOUT_ID, zk=bool(zk), copies=layout.copies,
+                padded_copies=layout.padded_copies, copy_size=layout.copy_size, padded_copy_size=layout.n_wires,
+                const_idx=layout.const_idx, const_val=layout.const_val, n=n, lg_n=n.bit_length() - 1,
+                masked_root=masked_root, mask_root=mask_root if zk else (mask_root or ""))
+
+
+def manifests_of(committer) -> list:
+    """commit_manifest of every frame of a truepix_b200.orion.FrameCommitter whose
+    commits have completed"""
+    out = []
+    for f, L in enumerate(committer.layouts):
+        mask = committer.hex(committer.mask_root(f)) if committer.zk else ""
+        out.append(commit_manifest(L, committer.root_hex(f), mask, committer.zk))
+    return out
+
+
 def read_vole_prover_file(path: str):
     """The reference's binary VOLE prover file ("EVOL", version 1, role 1): the
     correlations u, v as uint64 [n, 2] (real, imag). One repetition."""
