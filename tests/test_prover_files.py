@@ -66,3 +66,16 @@ def test_commit_manifest_of_a_layout():
     assert m["masked_root"] == hx and m["mask_root"] == "00" * 32 and m["zk"] is True
     m = commit_manifest(FrameLayout(copies=5, copy_size=384, const_idx=-1, const_val=0), hx, zk=False)
     assert m["mask_root"] == "" and m["zk"] is False and m["padded_copies"] == 8 and m["const_idx"] == -1
+
+
+def test_point_file_for_the_open_phase(tmp_path):
+    """the input point in fp2_link.write_point_file's two forms"""
+    from truepix_b200.prover import write_point_file
+    c = next(cases())
+    pts = [(int(a), int(b)) for a, b in c["point"]]
+    j, t = write_point_file(str(tmp_path / "gkr_point_prover.json"), pts)
+    d = json.load(open(j))
+    assert d == {"protocol": "truepix", "field": "fp2-mersenne61", "layout": "copy-major-384-const128-pad512-v1",
+                 "point": [list(p) for p in pts]}
+    lines = open(t).read().splitlines()
+    assert lines[0] == str(len(pts)) and lines[1:] == ["%d %d" % p for p in pts]

@@ -84,6 +84,25 @@ def manifests_of(committer) -> list:
     return out
 
 
+def write_point_file(path: str, point) -> tuple:
+    """fp2_link.write_point_file: the input point for the Orion open phase, as JSON
+    and as the plain-text companion the Orion binaries read ("<count>" then one
+    "<real> <imag>" line per coordinate). point: Fp2 values or (real, imag) pairs.
+    Returns (json path, text path)."""
+    import json
+    import os
+    pairs = [[int(x.real), int(x.imag)] if hasattr(x, "real") else [int(x[0]), int(x[1])] for x in point]
+    with open(path, "w") as fh:
+        json.dump({"protocol": PROTOCOL_ID, "field": "fp2-mersenne61", "layout": LAYOUT_ID, "point": pairs}, fh,
+                  indent=2)
+    txt = path if path.endswith(".txt") else os.path.splitext(path)[0] + ".txt"
+    with open(txt, "w") as fh:
+        fh.write("%d\n" % len(pairs))
+        for re, im in pairs:
+            fh.write("%d %d\n" % (re, im))
+    return path, txt
+
+
 def read_vole_prover_file(path: str):
     """The reference's binary VOLE prover file ("EVOL", version 1, role 1): the
     correlations u, v as uint64 [n, 2] (real, imag). One repetition."""
