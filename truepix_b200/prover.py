@@ -22,8 +22,11 @@ ExtVOLEGen.py:25-50, 130-186) and the Orion commitment manifest
 """
 from __future__ import annotations
 
+import concurrent.futures
 import ctypes
+import json
 import math
+import os
 import pickle
 import struct
 
@@ -89,8 +92,6 @@ def write_point_file(path: str, point) -> tuple:
     and as the plain-text companion the Orion binaries read ("<count>" then one
     "<real> <imag>" line per coordinate). point: Fp2 values or (real, imag) pairs.
     Returns (json path, text path)."""
-    import json
-    import os
     pairs = [[int(x.real), int(x.imag)] if hasattr(x, "real") else [int(x[0]), int(x[1])] for x in point]
     with open(path, "w") as fh:
         json.dump({"protocol": PROTOCOL_ID, "field": "fp2-mersenne61", "layout": LAYOUT_ID, "point": pairs}, fh,
@@ -203,7 +204,7 @@ def gate_weights(lib, z1, n_gates: int) -> np.ndarray:
 
 
 def prove_frames(frames, layout, gate_type, in0, in1, pids, correlations, manifests, fp2_type=None,
-                 stream=None, zk: bool = True):
+                 stream=None, zk: bool = True, io_threads: int = 0):
     """Proofs of a batch of frames of one size and circuit.
 
     frames: uint8 device tensors (layout.copies * layout.copy_size bytes each);
@@ -211,8 +212,9 @@ def prove_frames(frames, layout, gate_type, in0, in1, pids, correlations, manife
     correlations [(u, v) uint64 [count, 2]] (the same count for every frame) and
     commitment manifests per frame. zk: the zero-knowledge prover
     (circuitnizkvec_vole_ZK.py, TruePix's default), else circuitnizkvec_vole.py.
-    Returns one LayerTranscript per frame (proof_bytes() is the reference's
-    proof)."""
+    io_threads: host threads absorbing the frames' output vectors (0: one per
+    CPU). Returns one LayerTranscript per frame (proof_bytes() is the
+    reference's proof)."""
     import torch
     from .frame import BatchFrameProver, circuit_outputs, pack_fp2
     lib = native.gkr()
@@ -231,14 +233,23 @@ def prove_frames(frames, layout, gate_type, in0, in1, pids, correlations, manife
     bufs = [circuit_outputs(f, layout, gt, i0, i1, stream=stream) for f in frames]
     if stream is not None:
         stream.synchronize()
-    tr, z1s, z2s = [], [], []
-    for f in range(B):
-        t = LayerTranscript(pids[f], fp2_type)
-        outs = bufs[f].cpu().numpy().view(np.uint64)
-        z1, z2 = t.io_prefix(outs, n_inputs, commit_binding(manifests[f]), n_out_bits, nb)
-        tr.append(t)
-        z1s.append(gate_weights(lib, z1, G))
-        z2s.append(z2)
+    # each frame's output vector (64 MiB at 1080p) is one sequential SHA-256
+    # chain; the frames' chains run on host threads (the library's transcript
+    # calls release the interpreter lock)
+    outs = [b.cpu().numpy().view(np.uint64) for b in bufs]
+    tr = [LayerTranscript(pids[f], fp2_type) for f in range(B)]
+
+    def prefix(f):
+        return tr[f].io_prefix(outs[f], n_inputs, commit_binding(manifests[f]), n_out_bits, nb)
+
+    workers = max(1, min(B, io_threads or os.cpu_count() or 1))
+    if workers > 1:
+        with concurrent.futures.ThreadPoolExecutor(workers) as pool:
+            points = list(pool.map(prefix, range(B)))
+    else:
+        points = [prefix(f) for f in range(B)]
+    z1s = [gate_weights(lib, z1, G) for z1, _ in points]
+    z2s = [z2 for _, z2 in points]
     z2 = np.array(z2s, np.uint64).reshape(B, nb, 2)
     d_z2 = torch.from_numpy(pack_fp2(z2[..., 0].reshape(-1), z2[..., 1].reshape(-1))).to(dev)
     d_pt = torch.zeros(B * (nb + int(math.log2(layout.n_wires))) * 2, dtype=torch.int64, device=dev)
