@@ -1,0 +1,196 @@
+"""The Orion opening proof of a committed frame (non-ZK NIZK mode), as the
+reference's linearPC_multi_prove writes it (TruePix-main/Orion/Orion_nonzk:
+examples/multivariate_PC_test_prove.cpp:127-190, src/VPD/linearPC.cpp:426-640
+tensor_product_protocol, src/truepix/orion_proof.cpp:67-95 file format), with the
+passes over the codeword on the device.
+
+  host    the GKR input point reversed (truepix_gkr.h:233-239) and split into the
+          column weights r0 (its top 7 coordinates) and the row weights r1 (the
+          rest) as eq tables (linearPC.cpp:693-731 dfs); the Orion transcript
+          (src/truepix/orion_fs.cpp) absorbs "tensor-open", the commitment's
+          root, N, 1, r0 and r1 and draws the 1222 queried columns
+  device  combined codeword and its Merkle tree (tp_orion_combine_dev), the
+          answer sum r1[i] * combined[i] (tp_orion_answer_dev), the queried
+          columns (tp_orion_query_columns_dev), all over the codeword the commit
+          left in HBM (truepix_b200.orion.FrameCommitter)
+  host    the Merkle siblings of the queried leaves in both trees
+          (orion_proof.cpp:153-174) and the proof file's bytes.
+
+The reference also runs an in-process self-check of the combined codeword
+(its EC(y1) GKR, linearPC.cpp:585-620) whose results do not enter the file; the
+verifier repeats it on its side.
+"""
+from __future__ import annotations
+
+import hashlib
+import math
+import struct
+
+import numpy as np
+
+from . import native
+
+COLUMN_SIZE = 128
+TARGET_DISTANCE = 0.07          # linear_code/parameter.h:4
+P61 = (1 << 61) - 1
+
+
+def query_count() -> int:
+    """linearPC.cpp:440: -128 / log2(1 - target_distance), truncated"""
+    return int(-128 / math.log2(1 - TARGET_DISTANCE))
+
+
+class OrionTranscript:
+    """truepix_orion::FsTranscript (orion_fs.cpp:20-105): a 32-byte state; every
+    absorb of up to 32 bytes replaces it by SHA-256(state || bytes, zero-padded
+    to 64); draws come 8 bytes at a time from a pool SHA-256(state || 0x01 ||
+    0^31), after which the state becomes SHA-256(state || 0x02 || 0^31)."""
+
+    DOMAIN = b"truepix/orion-fs/v1"
+
+    def __init__(self):
+        self.state = bytes(32)
+        self.pool = bytes(32)
+        self.absorb(self.DOMAIN)
+        self.used = 32
+
+    def absorb(self, data: bytes) -> None:
+        for off in range(0, len(data), 32):
+            chunk = data[off:off + 32]
+            self.state = hashlib.sha256(self.state + chunk + bytes(32 - len(chunk))).digest()
+        self.used = 32
+
+    def absorb_u64(self, x: int) -> None:
+        self.absorb(struct.pack("<Q", x))
+
+    def absorb_label(self, label: str) -> None:
+        self.absorb(label.encode())
+
+    def absorb_field(self, real: int, imag: int) -> None:
+        self.absorb(struct.pack("<Q", real))
+        self.absorb(struct.pack("<Q", imag))
+
+    def _refill(self) -> None:
+        self.pool = hashlib.sha256(self.state + b"\x01" + bytes(31)).digest()
+        self.state = hashlib.sha256(self.state + b"\x02" + bytes(31)).digest()
+        self.used = 0
+
+    def squeeze_u64(self) -> int:
+        if self.used + 8 > 32:
+            self._refill()
+        v = struct.unpack_from("<Q", self.pool, self.used)[0]
+        self.used += 8
+        return v
+
+    def squeeze_index(self, bound: int) -> int:
+        return 0 if bound <= 0 else self.squeeze_u64() % bound
+
+
+def split_point(point):
+    """The eq-table coordinates of the column weights r0 and the row weights r1
+    (LSB first): open_and_verify reverses the GKR point and builds both tables
+    MSB-first over the reversed halves, which is the LSB-first table over the
+    point's own top 7 coordinates (r0) and its other ones (r1)."""
+    lg = len(point)
+    return list(point[lg - 7:]), list(point[:lg - 7])
+
+
+def eq_table(lib, coords) -> np.ndarray:
+    """eq(coords, i) for i < 2^len, LSB first, as (real, imag) uint64 [2^k, 2]
+    (native_fp2_compute_beta, on the device)"""
+    import ctypes
+    k = len(coords)
+    zr = np.ascontiguousarray([int(c[0]) for c in coords], np.uint64)
+    zi = np.ascontiguousarray([int(c[1]) for c in coords], np.uint64)
+    out_r = np.zeros(1 << k, np.uint64)
+    out_i = np.zeros(1 << k, np.uint64)
+    P = ctypes.POINTER(ctypes.c_uint64)
+    lib.native_fp2_compute_beta(zr.ctypes.data_as(P), zi.ctypes.data_as(P), k, 1, 0, out_r.ctypes.data_as(P),
+                                out_i.ctypes.data_as(P))
+    native.check(lib, None, "native_fp2_compute_beta")
+    return np.stack([out_r, out_i], axis=1)
+
+
+def merkle_siblings(tree: np.ndarray, n_leaves: int, positions) -> tuple:
+    """collect_merkle_siblings (orion_proof.cpp:153-174): for each position in
+    order, the siblings on its path not taken before (heap order, root at 1)"""
+    seen = set()
+    idxs, digs = [], []
+    for p in positions:
+        node = int(p) + n_leaves
+        while node != 1:
+            sib = node ^ 1
+            if sib not in seen:
+                seen.add(sib)
+                idxs.append(sib)
+                digs.append(tree[sib].tobytes())
+            node //= 2
+    return idxs, digs
+
+
+def opening_bytes(N, msg_len, cw_len, answer, com_root, comb_root, col_q, cols, combined, com_sparse, comb_sparse):
+    """OpeningProof::write_file (orion_proof.cpp:67-95); elements as (img, real) uint64 pairs"""
+    out = [b"ORIONPV1", struct.pack("<IIQQQQI", 2, 1, N, COLUMN_SIZE, msg_len, cw_len, len(col_q)),
+           np.ascontiguousarray(answer, np.uint64).tobytes(), com_root, comb_root,
+           np.asarray(col_q, np.int64).tobytes(), np.ascontiguousarray(cols, np.uint64).tobytes(),
+           np.ascontiguousarray(combined, np.uint64).tobytes(),
+           np.ascontiguousarray(combined[:msg_len], np.uint64).tobytes()]
+    for idxs, digs in (com_sparse, comb_sparse):
+        out.append(struct.pack("<Q", len(idxs)))
+        out += [struct.pack("<I", i) + d for i, d in zip(idxs, digs)]
+    return b"".join(out)
+
+
+def opening_proof(committer, f: int, point, stream=None) -> bytes:
+    """The NIZK opening proof of frame f of a non-ZK truepix_b200.orion.FrameCommitter
+    whose commit has completed, at the GKR input point (the prover's order:
+    (real, imag) pairs or Fp2 values)."""
+    import torch
+    lib = native.gkr()
+    if committer.zk:
+        raise ValueError("the non-ZK opening needs a non-ZK commitment")
+    L = committer.layouts[f]
+    N = L.padded_copies * L.n_wires
+    msg_len, cw_len, leaves = N // COLUMN_SIZE, committer.cw_len[f], committer.leaves[f]
+    pt = [(int(x.real), int(x.imag)) if hasattr(x, "real") else (int(x[0]), int(x[1])) for x in point]
+    if len(pt) != N.bit_length() - 1:
+        raise ValueError("the point has %d coordinates, the frame %d" % (len(pt), N.bit_length() - 1))
+    c0, c1 = split_point(pt)
+    r0, r1 = eq_table(lib, c0), eq_table(lib, c1)
+    com_root = committer.root(f)
+    T = OrionTranscript()
+    T.absorb_label("tensor-open")
+    T.absorb(com_root)
+    T.absorb_u64(N)
+    T.absorb_u64(1)
+    for re, im in r0.tolist():
+        T.absorb_field(re, im)
+    for re, im in r1.tolist():
+        T.absorb_field(re, im)
+    qc = query_count()
+    col_q = [T.squeeze_index(cw_len) for _ in range(qc)]
+    dev = committer.dev
+    s = stream.cuda_stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    as_dev = lambda a: torch.from_numpy(np.ascontiguousarray(a[:, ::-1]).view(np.int64).reshape(-1).copy()).to(dev)
+    d_r0, d_r1 = as_dev(r0), as_dev(r1)          # (img, real), the codeword's element order
+    comb = torch.empty(2 * cw_len, dtype=torch.int64, device=dev)
+    ctree = torch.empty(64 * leaves, dtype=torch.uint8, device=dev)
+    ans = torch.empty(2, dtype=torch.int64, device=dev)
+    q = torch.tensor(col_q, dtype=torch.int64, device=dev)
+    cols = torch.empty(2 * COLUMN_SIZE * qc, dtype=torch.int64, device=dev)
+    rows = committer.rows[f].data_ptr()
+    native.check(lib, lib.tp_orion_combine_dev(rows, N, d_r0.data_ptr(), comb.data_ptr(), ctree.data_ptr(), s),
+                 "tp_orion_combine_dev")
+    native.check(lib, lib.tp_orion_answer_dev(comb.data_ptr(), msg_len, d_r1.data_ptr(), ans.data_ptr(), s),
+                 "tp_orion_answer_dev")
+    native.check(lib, lib.tp_orion_query_columns_dev(rows, N, q.data_ptr(), qc, cols.data_ptr(), s),
+                 "tp_orion_query_columns_dev")
+    if stream is not None:
+        stream.synchronize()
+    torch.cuda.synchronize(dev)
+    combined = comb.cpu().numpy().view(np.uint64).reshape(cw_len, 2)
+    tree = committer.trees[f].cpu().numpy().reshape(-1, 32)
+    ct = ctree.cpu().numpy().reshape(-1, 32)
+    return opening_bytes(N, msg_len, cw_len, ans.cpu().numpy().view(np.uint64), com_root, ct[1].tobytes(), col_q,
+                         cols.cpu().numpy().view(np.uint64), combined, merkle_siblings(tree, leaves, col_q),
+                         merkle_siblings(ct, leaves, col_q))
