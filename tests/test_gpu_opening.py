@@ -1,8 +1,10 @@
-"""truepix_b200.opening on the device: the NIZK opening proof of a frame
-committed by FrameCommitter is byte-identical (SHA-256 of the whole file) to the
-orion_proof.bin that the reference's own linearPC_multi_prove writes for the same
-frame and point (tests/golden/opening_golden.npz), for a gray frame of 64 copies
-and a crop frame of 100."""
+"""truepix_b200.opening on the device: the NIZK opening proofs of a frame
+committed by FrameCommitter are byte-identical (SHA-256 of the whole file) to
+the files the reference's own linearPC_multi_prove programs write for the same
+frame and point (tests/golden/opening_golden.npz): orion_proof.bin for plain
+commits of a gray frame of 64 copies and a crop frame of 100, and for the
+zero-knowledge commit pair of a gray frame of 80 copies (TruePix's default)
+orion_proof_masked.bin and orion_proof_mask.bin."""
 import hashlib
 import json
 
@@ -21,29 +23,33 @@ def test_opening_proofs_match_reference_program():
     from truepix_b200.orion import FrameCommitter
     n = 0
     for c in cases():
-        copies, cs, ci, cv = json.loads(c["layout"].tobytes().decode())
+        copies, cs, ci, cv, seed = json.loads(c["layout"].tobytes().decode())
         layout = FrameLayout(copies=copies, copy_size=cs, const_idx=ci, const_val=cv)
         pix = torch.from_numpy(c["pix"].copy()).cuda()
-        fc = FrameCommitter([layout])
-        fc.commit([pix])
+        fc = FrameCommitter([layout], zk=seed is not None)
+        fc.commit([pix], mask_seeds=None if seed is None else [seed])
         torch.cuda.synchronize()
-        assert fc.root(0) == c["com_root"].tobytes(), c["name"]
-        proof = opening_proof(fc, 0, [(int(a), int(b)) for a, b in c["point"]])
-        assert len(proof) == int(c["size"][0]), c["name"]
-        assert hashlib.sha256(proof).digest() == c["sha256"].tobytes(), c["name"]
-        n += 1
-    assert n == 2
+        point = [(int(a), int(b)) for a, b in c["point"]]
+        for tag, poly in ([("", "masked"), ("mask_", "mask")] if seed is not None else [("", None)]):
+            root = fc.mask_root(0) if poly == "mask" else fc.root(0)
+            assert root == c[tag + "com_root"].tobytes(), c["name"] + tag
+            proof = opening_proof(fc, 0, point, poly)
+            assert len(proof) == int(c[tag + "size"][0]), c["name"] + tag
+            assert hashlib.sha256(proof).digest() == c[tag + "sha256"].tobytes(), c["name"] + tag
+            n += 1
+    assert n == 4
 
 
-def test_zk_committer_is_refused():
+def test_polynomial_must_match_the_commit():
     import torch
     from truepix_b200.frame import FrameLayout
     from truepix_b200.opening import opening_proof
     from truepix_b200.orion import FrameCommitter
     c = next(cases())
-    copies, cs, ci, cv = json.loads(c["layout"].tobytes().decode())
+    copies, cs, ci, cv, _ = json.loads(c["layout"].tobytes().decode())
     layout = FrameLayout(copies=copies, copy_size=cs, const_idx=ci, const_val=cv)
-    fc = FrameCommitter([layout], zk=True)
-    with pytest.raises(ValueError):
-        opening_proof(fc, 0, [(0, 0)] * 15)
+    for zk, poly in ((True, None), (False, "mask"), (True, "other")):
+        fc = FrameCommitter([layout], zk=zk)
+        with pytest.raises(ValueError):
+            opening_proof(fc, 0, [(0, 0)] * 15, poly)
     torch.cuda.synchronize()

@@ -27,7 +27,7 @@ def eq(coords):
 
 def cases():
     g = np.load(os.path.join(ROOT, "tests", "golden", "opening_golden.npz"))
-    for n in sorted(k[:-7] for k in g.files if k.endswith("_header")):
+    for n in sorted(k[:-4] for k in g.files if k.endswith("_pix")):
         d = {k[len(n) + 1:]: g[k] for k in g.files if k.startswith(n + "_")}
         d["name"] = n
         yield d
@@ -43,31 +43,35 @@ def dot(ws, els):
 
 
 def test_transcript_and_tables_match_reference_openings():
-    from truepix_b200.opening import OrionTranscript, query_count, split_point
+    """plain openings and both openings of the zero-knowledge pair (the masked
+    polynomial's over the even columns, the mask's over the odd ones)"""
+    from truepix_b200.opening import OrionTranscript, query_columns, query_count, split_point
     n = 0
     for c in cases():
-        version, group1, N, cs, msg_len, cw_len, qc = (int(x) for x in c["header"])
-        assert (version, group1, cs, qc) == (2, 1, 128, query_count())
-        pt = [(int(a), int(b)) for a, b in c["point"]]
-        c0, c1 = split_point(pt)
-        r0, r1 = eq(c0), eq(c1)
-        assert len(r0) == 128 and len(r1) == msg_len
-        T = OrionTranscript()
-        T.absorb_label("tensor-open")
-        T.absorb(c["com_root"].tobytes())
-        T.absorb_u64(N)
-        T.absorb_u64(1)
-        for re, im in r0 + r1:
-            T.absorb_field(re, im)
-        col_q = [T.squeeze_index(cw_len) for _ in range(qc)]
-        np.testing.assert_array_equal(np.array(col_q), c["col_q"], err_msg=c["name"])
-        im, re = (int(x) for x in c["answer"][0])
-        assert dot(r1, c["message"]) == (re, im)
-        for k in range(3):
-            im, re = (int(x) for x in c["combined3"][k])
-            assert dot(r0, c["cols3"][k]) == (re, im)
-        n += 1
-    assert n == 2
+        zk = json.loads(c["layout"].tobytes().decode())[4] is not None
+        for tag in (["", "mask_"] if zk else [""]):
+            version, group1, N, cs, msg_len, cw_len, qc = (int(x) for x in c[tag + "header"])
+            assert (version, group1, cs, qc) == (2, 0 if tag else 1, 128, query_count())
+            pt = [(int(a), int(b)) for a, b in c["point"]]
+            c0, c1 = split_point(pt)
+            r0, r1 = eq(c0), eq(c1)
+            assert len(r0) == 128 and len(r1) == msg_len
+            T = OrionTranscript()
+            T.absorb_label("tensor-open")
+            T.absorb(c[tag + "com_root"].tobytes())
+            T.absorb_u64(N)
+            T.absorb_u64(group1)
+            for re, im in r0 + r1:
+                T.absorb_field(re, im)
+            col_q = query_columns(T, cw_len, -1 if not zk else (1 if tag else 0))
+            np.testing.assert_array_equal(np.array(col_q), c[tag + "col_q"], err_msg=c["name"] + tag)
+            im, re = (int(x) for x in c[tag + "answer"][0])
+            assert dot(r1, c[tag + "message"]) == (re, im)
+            for k in range(3):
+                im, re = (int(x) for x in c[tag + "combined3"][k])
+                assert dot(r0, c[tag + "cols3"][k]) == (re, im)
+            n += 1
+    assert n == 4
 
 
 def test_proof_file_layout_round_trip():

@@ -1,5 +1,7 @@
-"""The Orion opening proof of a committed frame (non-ZK NIZK mode), as the
-reference's linearPC_multi_prove writes it (TruePix-main/Orion/Orion_nonzk:
+"""The Orion opening proof of a committed frame (NIZK mode; the plain commit's
+and, for TruePix's default zero-knowledge commit pair, the masked polynomial's
+and the mask's), as the reference's linearPC_multi_prove writes it
+(TruePix-main/Orion/Orion_nonzk and Orion_zk:
 examples/multivariate_PC_test_prove.cpp:127-190, src/VPD/linearPC.cpp:426-640
 tensor_product_protocol, src/truepix/orion_proof.cpp:67-95 file format), with the
 passes over the codeword on the device.
@@ -128,9 +130,10 @@ def merkle_siblings(tree: np.ndarray, n_leaves: int, positions) -> tuple:
     return idxs, digs
 
 
-def opening_bytes(N, msg_len, cw_len, answer, com_root, comb_root, col_q, cols, combined, com_sparse, comb_sparse):
+def opening_bytes(N, msg_len, cw_len, answer, com_root, comb_root, col_q, cols, combined, com_sparse, comb_sparse,
+                  use_group1: int = 1):
     """OpeningProof::write_file (orion_proof.cpp:67-95); elements as (img, real) uint64 pairs"""
-    out = [b"ORIONPV1", struct.pack("<IIQQQQI", 2, 1, N, COLUMN_SIZE, msg_len, cw_len, len(col_q)),
+    out = [b"ORIONPV1", struct.pack("<IIQQQQI", 2, use_group1, N, COLUMN_SIZE, msg_len, cw_len, len(col_q)),
            np.ascontiguousarray(answer, np.uint64).tobytes(), com_root, comb_root,
            np.asarray(col_q, np.int64).tobytes(), np.ascontiguousarray(cols, np.uint64).tobytes(),
            np.ascontiguousarray(combined, np.uint64).tobytes(),
@@ -141,14 +144,30 @@ def opening_bytes(N, msg_len, cw_len, answer, com_root, comb_root, col_q, cols, 
     return b"".join(out)
 
 
-def opening_proof(committer, f: int, point, stream=None) -> bytes:
-    """The NIZK opening proof of frame f of a non-ZK truepix_b200.orion.FrameCommitter
+def query_columns(T: OrionTranscript, cw_len: int, group: int):
+    """the queried columns: any of the cw_len (group -1, the non-ZK opening), or
+    the even ones (0: the masked polynomial, use_group1) or the odd ones (1: the
+    mask) of the zero-knowledge opening (Orion_zk linearPC.cpp:739-756)"""
+    qc = query_count()
+    if group < 0:
+        return [T.squeeze_index(cw_len) for _ in range(qc)]
+    size = (cw_len + 1) // 2 if group == 0 else cw_len // 2
+    return [2 * T.squeeze_index(size) + group for _ in range(qc)]
+
+
+def opening_proof(committer, f: int, point, polynomial: str = None, stream=None) -> bytes:
+    """The NIZK opening proof of frame f of a truepix_b200.orion.FrameCommitter
     whose commit has completed, at the GKR input point (the prover's order:
-    (real, imag) pairs or Fp2 values)."""
+    (real, imag) pairs or Fp2 values). For a zero-knowledge commit pair,
+    polynomial is "masked" (orion_proof_masked.bin) or "mask"
+    (orion_proof_mask.bin): TruePix's default (Orion_zk
+    examples/multivariate_PC_test_prove.cpp:252-300, linearPC.cpp:701-930); for
+    a plain commit it is None (orion_proof.bin)."""
     import torch
     lib = native.gkr()
-    if committer.zk:
-        raise ValueError("the non-ZK opening needs a non-ZK commitment")
+    if committer.zk != (polynomial is not None) or polynomial not in (None, "masked", "mask"):
+        raise ValueError("polynomial: 'masked' or 'mask' for a zero-knowledge commit pair, None otherwise")
+    group = -1 if polynomial is None else (0 if polynomial == "masked" else 1)
     L = committer.layouts[f]
     N = L.padded_copies * L.n_wires
     msg_len, cw_len, leaves = N // COLUMN_SIZE, committer.cw_len[f], committer.leaves[f]
@@ -157,18 +176,19 @@ def opening_proof(committer, f: int, point, stream=None) -> bytes:
         raise ValueError("the point has %d coordinates, the frame %d" % (len(pt), N.bit_length() - 1))
     c0, c1 = split_point(pt)
     r0, r1 = eq_table(lib, c0), eq_table(lib, c1)
-    com_root = committer.root(f)
+    mask = polynomial == "mask"
+    com_root = committer.mask_root(f) if mask else committer.root(f)
     T = OrionTranscript()
     T.absorb_label("tensor-open")
     T.absorb(com_root)
     T.absorb_u64(N)
-    T.absorb_u64(1)
+    T.absorb_u64(0 if mask else 1)       # use_group1
     for re, im in r0.tolist():
         T.absorb_field(re, im)
     for re, im in r1.tolist():
         T.absorb_field(re, im)
-    qc = query_count()
-    col_q = [T.squeeze_index(cw_len) for _ in range(qc)]
+    col_q = query_columns(T, cw_len, group)
+    qc = len(col_q)
     dev = committer.dev
     s = stream.cuda_stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
     as_dev = lambda a: torch.from_numpy(np.ascontiguousarray(a[:, ::-1]).view(np.int64).reshape(-1).copy()).to(dev)
@@ -178,7 +198,7 @@ def opening_proof(committer, f: int, point, stream=None) -> bytes:
     ans = torch.empty(2, dtype=torch.int64, device=dev)
     q = torch.tensor(col_q, dtype=torch.int64, device=dev)
     cols = torch.empty(2 * COLUMN_SIZE * qc, dtype=torch.int64, device=dev)
-    rows = committer.rows[f].data_ptr()
+    rows = (committer.mask_rows[f] if mask else committer.rows[f]).data_ptr()
     native.check(lib, lib.tp_orion_combine_dev(rows, N, d_r0.data_ptr(), comb.data_ptr(), ctree.data_ptr(), s),
                  "tp_orion_combine_dev")
     native.check(lib, lib.tp_orion_answer_dev(comb.data_ptr(), msg_len, d_r1.data_ptr(), ans.data_ptr(), s),
@@ -189,8 +209,8 @@ def opening_proof(committer, f: int, point, stream=None) -> bytes:
         stream.synchronize()
     torch.cuda.synchronize(dev)
     combined = comb.cpu().numpy().view(np.uint64).reshape(cw_len, 2)
-    tree = committer.trees[f].cpu().numpy().reshape(-1, 32)
+    tree = (committer.mask_trees[f] if mask else committer.trees[f]).cpu().numpy().reshape(-1, 32)
     ct = ctree.cpu().numpy().reshape(-1, 32)
     return opening_bytes(N, msg_len, cw_len, ans.cpu().numpy().view(np.uint64), com_root, ct[1].tobytes(), col_q,
                          cols.cpu().numpy().view(np.uint64), combined, merkle_siblings(tree, leaves, col_q),
-                         merkle_siblings(ct, leaves, col_q))
+                         merkle_siblings(ct, leaves, col_q), use_group1=0 if mask else 1)
