@@ -275,6 +275,19 @@ int tp_late_rounds_dev(int n_frames, int n_in_bits, int n_gates, const int* gate
                        long long w3_frame_stride, long long w3_round_stride, void* d_closing, void* d_point,
                        void* d_tag, int zk, void* stream);
 
+/* ---- the Orion opening's transcript ----
+ * The queried columns of the Orion NIZK opening (Orion_nonzk / Orion_zk
+ * src/VPD/linearPC.cpp tensor_product_protocol with the transcript of
+ * src/truepix/orion_fs.cpp): a fresh transcript absorbs "tensor-open", the
+ * commitment's root (32 bytes), N and use_group1 (u64), then r0 and r1 field by
+ * field (each element's real, then its imaginary part, 8 bytes each); then count
+ * indices are drawn: uniform in [0, cw_len) (group -1, the plain opening), or
+ * the even (group 0, the masked polynomial) or odd (group 1, the mask) columns of
+ * the zero-knowledge opening. r0, r1: (real, imag) u64 pairs. Host only. */
+int tp_orion_open_queries(const unsigned char* root32, uint64_t N, int use_group1, const uint64_t* r0, int n_r0,
+                          const uint64_t* r1, long long n_r1, long long cw_len, int group, int count,
+                          long long* col_q);
+
 /* ---- circuit evaluation: the prover's output vector ----
  * Replaces ArithCircuitIncrementalBuilder.run (libTruePix/arithcircuitbuilder.py:71-108,
  * arithcircuit.py:121-131, 172-181) as called by CircuitProver.set_inputs

@@ -40,6 +40,26 @@ def test_opening_proofs_match_reference_program():
     assert n == 4
 
 
+def test_library_transcript_draws_the_reference_queries():
+    """tp_orion_open_queries (host code of the library) against every golden proof's queries"""
+    import numpy as np
+    from test_opening_host import eq
+    from truepix_b200 import native
+    from truepix_b200.opening import query_columns, split_point
+    lib = native.gkr(require_device=False)
+    n = 0
+    for c in cases():
+        seed = json.loads(c["layout"].tobytes().decode())[4]
+        for tag, group in ([("", 0), ("mask_", 1)] if seed is not None else [("", -1)]):
+            N, cw = int(c[tag + "header"][2]), int(c[tag + "header"][5])
+            c0, c1 = split_point([(int(a), int(b)) for a, b in c["point"]])
+            q = query_columns(lib, c[tag + "com_root"].tobytes(), N, 0 if tag else 1, np.array(eq(c0), np.uint64),
+                              np.array(eq(c1), np.uint64), cw, group)
+            assert q == [int(x) for x in c[tag + "col_q"]], c["name"] + tag
+            n += 1
+    assert n == 4
+
+
 def test_polynomial_must_match_the_commit():
     import torch
     from truepix_b200.frame import FrameLayout

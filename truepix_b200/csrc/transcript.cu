@@ -145,6 +145,65 @@ void host_absorb_header(State& s, uint8_t tag, uint32_t n)
     host_absorb(s, b, 5);
 }
 
+// ---- the Orion opening's transcript (truepix_orion::FsTranscript, orion_fs.cpp) --
+// state' = SHA-256(state || chunk || zero pad) for each chunk of <= 32 bytes
+struct OrionFs {
+    uint8_t state[32];
+    uint8_t pool[32];
+    int used;
+};
+
+void sha256_64(const uint8_t in[64], uint8_t out[32])
+{
+    static const uint8_t kPad[64] = {0x80, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
+                                     0,    0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
+                                     0,    0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0x02, 0};
+    uint32_t h[8];
+    tp::sha::init(h);
+    host_blocks(h, in, 1);
+    host_blocks(h, kPad, 1);
+    for (int i = 0; i < 8; ++i) {
+        out[4 * i] = (uint8_t)(h[i] >> 24);
+        out[4 * i + 1] = (uint8_t)(h[i] >> 16);
+        out[4 * i + 2] = (uint8_t)(h[i] >> 8);
+        out[4 * i + 3] = (uint8_t)h[i];
+    }
+}
+
+void orion_absorb(OrionFs& t, const void* data, size_t n)
+{
+    const uint8_t* p = static_cast<const uint8_t*>(data);
+    while (n > 0) {
+        uint8_t block[64];
+        memset(block, 0, sizeof(block));
+        memcpy(block, t.state, 32);
+        const size_t take = n < 32 ? n : 32;
+        memcpy(block + 32, p, take);
+        sha256_64(block, t.state);
+        p += take;
+        n -= take;
+    }
+    t.used = 32;
+}
+
+uint64_t orion_squeeze(OrionFs& t)
+{
+    if (t.used + 8 > 32) {
+        uint8_t block[64];
+        memset(block, 0, sizeof(block));
+        memcpy(block, t.state, 32);
+        block[32] = 0x01;
+        sha256_64(block, t.pool);
+        block[32] = 0x02;
+        sha256_64(block, t.state);
+        t.used = 0;
+    }
+    uint64_t v;
+    memcpy(&v, t.pool + t.used, 8);
+    t.used += 8;
+    return v;
+}
+
 bool state_ok(const void* state, const char* who)
 {
     if (!state) {
@@ -299,6 +358,42 @@ int tp_fs_rand_ext_dev(void* d_states, int n, const char* label, void* d_out, vo
     rand_ext_kernel<<<(n + 127) / 128, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         static_cast<State*>(d_states), n, L, static_cast<ulonglong2*>(d_out));
     return tp::cuda_failed(cudaGetLastError(), "transcript rand_ext") ? -1 : 0;
+}
+
+int tp_orion_open_queries(const unsigned char* root32, uint64_t N, int use_group1, const uint64_t* r0, int n_r0,
+                          const uint64_t* r1, long long n_r1, long long cw_len, int group, int count,
+                          long long* col_q)
+{
+    tp::clear_error();
+    if (!root32 || !r0 || !r1 || !col_q || n_r0 < 1 || n_r1 < 1 || cw_len < 2 || group < -1 || group > 1 ||
+        count < 0) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_open_queries: bad arguments");
+        return -1;
+    }
+    OrionFs t;
+    memset(&t, 0, sizeof(t));
+    static const char kDom[] = "truepix/orion-fs/v1";
+    orion_absorb(t, kDom, sizeof(kDom) - 1);
+    static const char kLabel[] = "tensor-open";
+    orion_absorb(t, kLabel, sizeof(kLabel) - 1);
+    orion_absorb(t, root32, 32);
+    orion_absorb(t, &N, 8);
+    const uint64_t g1 = use_group1 ? 1 : 0;
+    orion_absorb(t, &g1, 8);
+    for (int i = 0; i < n_r0; ++i) {
+        orion_absorb(t, r0 + 2 * i, 8);
+        orion_absorb(t, r0 + 2 * i + 1, 8);
+    }
+    for (long long i = 0; i < n_r1; ++i) {
+        orion_absorb(t, r1 + 2 * i, 8);
+        orion_absorb(t, r1 + 2 * i + 1, 8);
+    }
+    const uint64_t size = group < 0 ? (uint64_t)cw_len : group == 0 ? (uint64_t)(cw_len + 1) / 2 : (uint64_t)cw_len / 2;
+    for (int i = 0; i < count; ++i) {
+        const uint64_t k = orion_squeeze(t) % size;
+        col_q[i] = group < 0 ? (long long)k : 2 * (long long)k + group;
+    }
+    return 0;
 }
 
 int tp_vole_state_bytes(void) { return (int)sizeof(VoleState); }

@@ -103,6 +103,8 @@ GKR_SIGNATURES = {
     "tp_late_rounds_dev": (_I32, [_I32, _I32, _I32, _PI32, _PI32, _PI32, _VP, _VP, _VP, _I32, _VP, _VP, _VP, _VP,
                                   _VP, ctypes.c_longlong, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP,
                                   ctypes.c_longlong, ctypes.c_longlong, _VP, _VP, _VP, _I32, _VP]),
+    "tp_orion_open_queries": (_I32, [_VP, _U64, _I32, _VP, _I32, _VP, ctypes.c_longlong, ctypes.c_longlong, _I32,
+                                     _I32, _VP]),
     "tp_circuit_out_bits": (_I32, [_I32]),
     "tp_circuit_outputs_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _I32, _PI32, _PI32, _PI32,
                                             _VP, _VP]),

@@ -9,8 +9,9 @@ passes over the codeword on the device.
   host    the GKR input point reversed (truepix_gkr.h:233-239) and split into the
           column weights r0 (its top 7 coordinates) and the row weights r1 (the
           rest) as eq tables (linearPC.cpp:693-731 dfs); the Orion transcript
-          (src/truepix/orion_fs.cpp) absorbs "tensor-open", the commitment's
-          root, N, 1, r0 and r1 and draws the 1222 queried columns
+          (src/truepix/orion_fs.cpp, tp_orion_open_queries) absorbs
+          "tensor-open", the commitment's root, N, use_group1, r0 and r1 and
+          draws the 1222 queried columns
   device  combined codeword and its Merkle tree (tp_orion_combine_dev), the
           answer sum r1[i] * combined[i] (tp_orion_answer_dev), the queried
           columns (tp_orion_query_columns_dev), all over the codeword the commit
@@ -24,7 +25,6 @@ verifier repeats it on its side.
 """
 from __future__ import annotations
 
-import hashlib
 import math
 import struct
 
@@ -40,52 +40,6 @@ P61 = (1 << 61) - 1
 def query_count() -> int:
     """linearPC.cpp:440: -128 / log2(1 - target_distance), truncated"""
     return int(-128 / math.log2(1 - TARGET_DISTANCE))
-
-
-class OrionTranscript:
-    """truepix_orion::FsTranscript (orion_fs.cpp:20-105): a 32-byte state; every
-    absorb of up to 32 bytes replaces it by SHA-256(state || bytes, zero-padded
-    to 64); draws come 8 bytes at a time from a pool SHA-256(state || 0x01 ||
-    0^31), after which the state becomes SHA-256(state || 0x02 || 0^31)."""
-
-    DOMAIN = b"truepix/orion-fs/v1"
-
-    def __init__(self):
-        self.state = bytes(32)
-        self.pool = bytes(32)
-        self.absorb(self.DOMAIN)
-        self.used = 32
-
-    def absorb(self, data: bytes) -> None:
-        for off in range(0, len(data), 32):
-            chunk = data[off:off + 32]
-            self.state = hashlib.sha256(self.state + chunk + bytes(32 - len(chunk))).digest()
-        self.used = 32
-
-    def absorb_u64(self, x: int) -> None:
-        self.absorb(struct.pack("<Q", x))
-
-    def absorb_label(self, label: str) -> None:
-        self.absorb(label.encode())
-
-    def absorb_field(self, real: int, imag: int) -> None:
-        self.absorb(struct.pack("<Q", real))
-        self.absorb(struct.pack("<Q", imag))
-
-    def _refill(self) -> None:
-        self.pool = hashlib.sha256(self.state + b"\x01" + bytes(31)).digest()
-        self.state = hashlib.sha256(self.state + b"\x02" + bytes(31)).digest()
-        self.used = 0
-
-    def squeeze_u64(self) -> int:
-        if self.used + 8 > 32:
-            self._refill()
-        v = struct.unpack_from("<Q", self.pool, self.used)[0]
-        self.used += 8
-        return v
-
-    def squeeze_index(self, bound: int) -> int:
-        return 0 if bound <= 0 else self.squeeze_u64() % bound
 
 
 def split_point(point):
@@ -144,15 +98,19 @@ def opening_bytes(N, msg_len, cw_len, answer, com_root, comb_root, col_q, cols, 
     return b"".join(out)
 
 
-def query_columns(T: OrionTranscript, cw_len: int, group: int):
-    """the queried columns: any of the cw_len (group -1, the non-ZK opening), or
-    the even ones (0: the masked polynomial, use_group1) or the odd ones (1: the
-    mask) of the zero-knowledge opening (Orion_zk linearPC.cpp:739-756)"""
-    qc = query_count()
-    if group < 0:
-        return [T.squeeze_index(cw_len) for _ in range(qc)]
-    size = (cw_len + 1) // 2 if group == 0 else cw_len // 2
-    return [2 * T.squeeze_index(size) + group for _ in range(qc)]
+def query_columns(lib, root: bytes, N: int, use_group1: int, r0: np.ndarray, r1: np.ndarray, cw_len: int,
+                  group: int):
+    """the queried columns drawn by the opening's transcript (tp_orion_open_queries):
+    any of the cw_len (group -1, the plain opening), or the even (0: the masked
+    polynomial) or odd (1: the mask) columns of the zero-knowledge opening
+    (Orion_zk linearPC.cpp:739-756)"""
+    out = np.zeros(query_count(), np.int64)
+    r0 = np.ascontiguousarray(r0, np.uint64)
+    r1 = np.ascontiguousarray(r1, np.uint64)
+    native.check(lib, lib.tp_orion_open_queries(root, N, use_group1, r0.ctypes.data, len(r0), r1.ctypes.data,
+                                                len(r1), cw_len, group, out.size, out.ctypes.data),
+                 "tp_orion_open_queries")
+    return out.tolist()
 
 
 def opening_proof(committer, f: int, point, polynomial: str = None, stream=None) -> bytes:
@@ -178,16 +136,7 @@ def opening_proof(committer, f: int, point, polynomial: str = None, stream=None)
     r0, r1 = eq_table(lib, c0), eq_table(lib, c1)
     mask = polynomial == "mask"
     com_root = committer.mask_root(f) if mask else committer.root(f)
-    T = OrionTranscript()
-    T.absorb_label("tensor-open")
-    T.absorb(com_root)
-    T.absorb_u64(N)
-    T.absorb_u64(0 if mask else 1)       # use_group1
-    for re, im in r0.tolist():
-        T.absorb_field(re, im)
-    for re, im in r1.tolist():
-        T.absorb_field(re, im)
-    col_q = query_columns(T, cw_len, group)
+    col_q = query_columns(lib, com_root, N, 0 if mask else 1, r0, r1, cw_len, group)
     qc = len(col_q)
     dev = committer.dev
     s = stream.cuda_stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
