@@ -689,7 +689,7 @@ def ours_arm(args, rank, world, local_rank):
         c, w, b, m = bprover.results(B - 1)
         res_ok = bool(c.any() and w.any() and m != (0, 0) and any(committer.root(B - 1)))
 
-    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = ref_gpu = fs_rounds = None
+    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = ref_gpu = fs_rounds = full = None
     # The side measurements run once, at N = 1 (a scaling run holds every GPU
     # while rank 0 works; it only needs the step's value).
     extras = rank == 0 and world == 1
@@ -706,6 +706,8 @@ def ours_arm(args, rank, world, local_rank):
         e2e_ref = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
         ref_gpu = reference_gpu_lib(frames[0], layout, gt, i0, i1, z1, z2, point, chal)
         fs_rounds = transcript_rounds(bprover, pix, z1s, z2s, pts, stream)
+    if extras and args.full_proof:
+        full = full_proof(pix, layout, gt, i0, i1, stream)
     if extras and not args.skip_serving:
         del bprover
         committer.rows = committer.trees = None
@@ -757,10 +759,58 @@ def ours_arm(args, rank, world, local_rank):
                             "every launch), whose shares match the serialised ncu launch list"
                             % len(committer.side),
             "ntt": ntt, "opening": opening, "zk": zk, "batched_uneven": uneven, "serving": serving, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
-            "reference_gpu_library": ref_gpu, "transcript_rounds": fs_rounds,
+            "reference_gpu_library": ref_gpu, "transcript_rounds": fs_rounds, "full_proof": full,
             "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
         }
         print(json.dumps(line), flush=True)
+
+
+def full_proof(pix, layout, gt, i0, i1, stream, n_frames=16):
+    """The reference prover's whole proof of frames in TruePix's default mode, on
+    the device path (wall clock, synchronised): per frame the zero-knowledge
+    commit pair, the manifest from its roots, the zero-knowledge prover's proof
+    (truepix_b200.prover.prove_frames: circuit outputs, the IO transcript on host
+    threads, the VOLE-committed early rounds, late rounds and closing proofs) and
+    both Orion openings (truepix_b200.opening.opening_proof). The proof
+    containers' pickling (the reference's format) is left out of the timing."""
+    import time
+    import numpy as np
+    import torch
+    from truepix_b200.opening import opening_proof
+    from truepix_b200.orion import FrameCommitter
+    from truepix_b200.prover import manifests_of, prove_frames
+    frames = pix[:n_frames]
+    B = len(frames)
+    rng = np.random.default_rng(5)
+    count = 4 * layout.n_copy_bits + 6 * 9 + 9 + 2 + 3 + 8
+    corr = [(rng.integers(0, (1 << 61) - 1, size=(count, 2), dtype=np.uint64),
+             rng.integers(0, (1 << 61) - 1, size=(count, 2), dtype=np.uint64)) for _ in range(B)]
+    fc = FrameCommitter([layout] * B, stream=stream, zk=True)
+    seeds = [0x5EED + f for f in range(B)]
+    out = {}
+    for rep in range(2):     # the first pass warms up (allocations, graphs, caches)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fc.commit(frames, mask_seeds=seeds)
+        stream.synchronize()
+        t1 = time.perf_counter()
+        tr = prove_frames(frames, layout, gt, i0, i1, [1000 + f for f in range(B)], corr, manifests_of(fc),
+                          stream=stream, zk=True)
+        t2 = time.perf_counter()
+        sizes = 0
+        for f in range(B):
+            pt = [(int(x.real), int(x.imag)) for x in tr[f].final_input_point]
+            sizes += len(opening_proof(fc, f, pt, "masked", stream=stream))
+            sizes += len(opening_proof(fc, f, pt, "mask", stream=stream))
+        t3 = time.perf_counter()
+        out = {"frames": B, "frames_per_s": B / (t3 - t0), "commit_ms": (t1 - t0) * 1e3,
+               "prove_ms": (t2 - t1) * 1e3, "open_ms": (t3 - t2) * 1e3, "opening_bytes_per_frame": sizes / B,
+               "note": "wall clock per batch: ZK commit pairs, the whole GKR input-layer proof of the zero-"
+                       "knowledge prover (IO transcript on host threads, everything after it on the device), "
+                       "both Orion openings; proof containers not pickled"}
+    del fc
+    torch.cuda.empty_cache()
+    return out
 
 
 def zk_step(args, bprover, pix, z1s, z2s, pts, chal_b, layout, stream, local_rank):
@@ -1402,6 +1452,9 @@ def main():
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--skip-zk", action="store_true")
     ap.add_argument("--skip-opening", action="store_true")
+    ap.add_argument("--full-proof", action="store_true",
+                    help="also time the whole proof of frames in TruePix's default mode (commit pairs, "
+                         "proof, openings)")
     ap.add_argument("--leaf-chunks", type=int, default=1,
                     help="launches the commits' SHA-256 leaf chains are split into (tp_orion_set_leaf_chunks)")
     ap.add_argument("--commit-streams", type=int, default=8,
