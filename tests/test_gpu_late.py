@@ -102,13 +102,6 @@ def test_vole_rounds_match_reference_chain(lib):
             torch.cuda.synchronize()
             if not close:
                 st_late, vs_late = d_st.cpu().numpy().tobytes(), d_vs.cpu().numpy().tobytes()
-        np.testing.assert_array_equal(host(closing, (n + 10, 2)), c["closing"])
-        np.testing.assert_array_equal(host(point, (n + nb, 2)), c["point"])
-        np.testing.assert_array_equal(host(tag, (1, 2)), c["tag"])
-        assert vole_state_fields(d_vs.cpu().numpy().tobytes())["idx"] == int(c["used_closed"][0])
-        d = ctypes.create_string_buffer(32)
-        assert lib.tp_fs_digest(d_st.cpu().numpy().tobytes(), d) == 0
-        assert d.raw == c["digest_closed"].tobytes()
         np.testing.assert_array_equal(host(coefs, (6 * n, 2)), c["coefs"][4 * nb:])
         np.testing.assert_array_equal(host(cho, (2 * n, 2)), c["chal"][nb:])
         pr = host(proof, (2 * n, 4, 2))
@@ -120,8 +113,18 @@ def test_vole_rounds_match_reference_chain(lib):
         assert f["prev"] == tuple(int(x) for x in c["prev"][0])
         assert f["v_elem"] == [tuple(int(x) for x in r) for r in c["v_elem"]]
         assert f["out_elem"] == [tuple(int(x) for x in r) for r in c["out_elem"]]
+        d = ctypes.create_string_buffer(32)
         assert lib.tp_fs_digest(st_late, d) == 0
         assert d.raw == c["digest"].tobytes()
+        # the closing proofs, row by row (their values go into the transcript in this order)
+        got = host(closing, (n + 10, 2))
+        rows = [k for k in range(n + 10) if not np.array_equal(got[k], c["closing"][k])]
+        assert not rows, f"{c['name']}: closing rows {rows} differ from the reference chain"
+        np.testing.assert_array_equal(host(point, (n + nb, 2)), c["point"])
+        np.testing.assert_array_equal(host(tag, (1, 2)), c["tag"])
+        assert vole_state_fields(d_vs.cpu().numpy().tobytes())["idx"] == int(c["used_closed"][0])
+        assert lib.tp_fs_digest(d_st.cpu().numpy().tobytes(), d) == 0
+        assert d.raw == c["digest_closed"].tobytes()
         n_cases += 1
     assert n_cases == 2
 

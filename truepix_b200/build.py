@@ -35,24 +35,44 @@ def nvcc() -> str:
     return exe
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> list[str]:
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(verbose: bool = False, ptxas_info: bool = False, jobs: int | None = None) -> list[str]:
+    """Compile every source of each library to an object in parallel (one nvcc
+    per source, objects under lib/_build/), then link the shared library."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(LIBDIR, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers += [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
+    compile_flags = [f for f in FLAGS if f != "-shared"]
     out = []
     for name, srcs in LIBS.items():
         target = os.path.join(LIBDIR, name)
-        paths = [os.path.join(CSRC, s) for s in srcs]
-        deps = paths + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-        deps.append(os.path.join(ROOT, "include", "native_fp2.h"))
-        if os.path.exists(target) and not ptxas_info:
-            t = os.path.getmtime(target)
-            if all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d)):
-                out.append(target)
-                continue
-        cmd = [nvcc()] + ARCH + FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + \
-            ["-o", target] + paths
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        objs, todo = [], []
+        for s in srcs:
+            src = os.path.join(CSRC, s)
+            obj = os.path.join(objdir, os.path.splitext(s)[0] + ".o")
+            objs.append(obj)
+            if ptxas_info or _stale(obj, [src] + headers):
+                todo.append([nvcc()] + ARCH + compile_flags + (["-Xptxas", "-v"] if ptxas_info else []) +
+                            ["-c", "-o", obj, src])
+
+        def run(cmd):
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+
+        with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+            list(ex.map(run, todo))
+        if todo or _stale(target, objs):
+            run([nvcc()] + ARCH + ["-shared", "-o", target] + objs)
         out.append(target)
     return out
 

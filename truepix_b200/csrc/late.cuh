@@ -322,8 +322,7 @@ TP_HD void step_close_commit(Work& w, const Frame& f, const Shape& sh)
         rest_v = f2add(rest_v, w.vv[k]);
     }
     const uint8_t pv[7] = {'p', 'o', 'k', '-', 'v', 'e', 'c'};
-    fp2 c;
-    fs::rand_ext(w.st, pv, 7, reinterpret_cast<uint64_t*>(&c.re), reinterpret_cast<uint64_t*>(&c.im));
+    const fp2 c = fs::rand_fp2(w.st, pv, 7);
     out[n + 2] = f2mul(rest_sum, c);
     out[n + 3] = f2mul(rest_v, c);
     fs::put_fp2(w.st, out[n + 2].re, out[n + 2].im);
@@ -393,14 +392,12 @@ TP_HD void step_close_tail(Work& w, const Frame& f, const Shape& sh)
     }
     const fp2 tv = f2mul(w.red[0][0], mz);
     const uint8_t eq[2] = {'e', 'q'};
-    fp2 e;
-    fs::rand_ext(w.st, eq, 2, reinterpret_cast<uint64_t*>(&e.re), reinterpret_cast<uint64_t*>(&e.im));
+    const fp2 e = fs::rand_fp2(w.st, eq, 2);
     out[n + 6] = f2mul(f2sub(w.vs.prev, tv), e);
     fs::put_fp2(w.st, out[n + 6].re, out[n + 6].im);
     uint8_t label[32];
     const uint32_t len = vole::tau_label(label, sh.layer);
-    fp2 tau;
-    fs::rand_ext(w.st, label, len, reinterpret_cast<uint64_t*>(&tau.re), reinterpret_cast<uint64_t*>(&tau.im));
+    const fp2 tau = fs::rand_fp2(w.st, label, len);
     fp2 tag = w.vv[n];
     for (int k = n - 1; k >= 0; --k) tag = f2add(f2mul(tag, tau), w.vv[k]);
     for (int j = 0; j < n; ++j) f.point[j] = f2add(w.w[j], f2mul(f2sub(w.w[n + j], w.w[j]), tau));
@@ -412,8 +409,7 @@ TP_HD void step_close_tail(Work& w, const Frame& f, const Shape& sh)
         vsum = f2add(vsum, w.vs.v_elem[k]);
     }
     const uint8_t pf[9] = {'p', 'o', 'k', '-', 'f', 'i', 'n', 'a', 'l'};
-    fp2 c;
-    fs::rand_ext(w.st, pf, 9, reinterpret_cast<uint64_t*>(&c.re), reinterpret_cast<uint64_t*>(&c.im));
+    const fp2 c = fs::rand_fp2(w.st, pf, 9);
     out[n + 7] = f2mul(osum, c);
     out[n + 8] = f2mul(vsum, c);
     fs::put_fp2(w.st, out[n + 7].re, out[n + 7].im);
@@ -429,8 +425,8 @@ TP_HD void step_close_tail(Work& w, const Frame& f, const Shape& sh)
     }
     // create_input_value_proof
     const uint8_t iv[9] = {'i', 'n', 'p', 'u', 't', '-', 'v', 'a', 'l'};
-    fs::rand_ext(w.st, iv, 9, reinterpret_cast<uint64_t*>(&c.re), reinterpret_cast<uint64_t*>(&c.im));
-    out[n + 9] = f2mul(tag, c);
+    const fp2 civ = fs::rand_fp2(w.st, iv, 9);
+    out[n + 9] = f2mul(tag, civ);
     fs::put_fp2(w.st, out[n + 9].re, out[n + 9].im);
     w.vs.prev = tag;
     *f.tag = tag;

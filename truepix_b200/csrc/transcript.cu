@@ -60,10 +60,9 @@ __global__ void rand_ext_kernel(State* __restrict__ st, int n, Label L, ulonglon
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     State s = st[i];
-    unsigned long long re, im;
-    tp::fs::rand_ext(s, L.b, L.len, (uint64_t*)&re, (uint64_t*)&im);
+    const tp::fp2 r = tp::fs::rand_fp2(s, L.b, L.len);
     st[i] = s;
-    out[i] = make_ulonglong2(re, im);
+    out[i] = make_ulonglong2(r.re, r.im);
 }
 
 // ---- VOLE-committed early round (vole.cuh), one thread per frame ----------------

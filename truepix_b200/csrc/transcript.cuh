@@ -159,5 +159,16 @@ TP_HD void rand_ext(State& s, const uint8_t* label, uint32_t len, uint64_t* re, 
     *im = rand_scalar(s);
 }
 
+// rand_ext returned by value as an Fp2. The draw is written to uint64_t
+// (unsigned long) locals and converted; writing it through a uint64_t pointer
+// into an fp2's unsigned long long limbs would be a strict-aliasing violation,
+// which the device compiler may exploit by reading the limbs as never written.
+TP_HD fp2 rand_fp2(State& s, const uint8_t* label, uint32_t len)
+{
+    uint64_t re, im;
+    rand_ext(s, label, len, &re, &im);
+    return mk(re, im);
+}
+
 }  // namespace fs
 }  // namespace tp

@@ -130,13 +130,11 @@ TP_HD bool round(fs::State& s, State& w, const fp2* c, int n_coef, const fp2* u,
     fp2 now = tag[0];
     for (int k = 0; k < n_coef; ++k) now = f2add(now, tag[k]);
     const uint8_t eq[2] = {'e', 'q'};
-    fp2 e;
-    fs::rand_ext(s, eq, 2, reinterpret_cast<uint64_t*>(&e.re), reinterpret_cast<uint64_t*>(&e.im));
+    const fp2 e = fs::rand_fp2(s, eq, 2);
     const fp2 vz = w.has_prev ? f2mul(f2sub(w.prev, now), e) : f2mul(now, e);
     fs::put_fp2(s, vz.re, vz.im);
     if (proof) proof[n_coef] = vz;
-    fp2 r;
-    fs::rand_ext(s, label, len, reinterpret_cast<uint64_t*>(&r.re), reinterpret_cast<uint64_t*>(&r.im));
+    const fp2 r = fs::rand_fp2(s, label, len);
     fp2 p = tag[n_coef - 1];
     for (int k = n_coef - 2; k >= 0; --k) p = f2add(f2mul(p, r), tag[k]);
     w.prev = p;
