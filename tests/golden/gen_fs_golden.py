@@ -16,7 +16,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/TruePix-main"
+REF = os.path.join(os.environ.get("TRUEPIX_REF", "/root/reference"), "TruePix-main")
 P61 = (1 << 61) - 1
 
 

@@ -25,7 +25,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/TruePix-main"
+REF = os.path.join(os.environ.get("TRUEPIX_REF", "/root/reference"), "TruePix-main")
 P61 = (1 << 61) - 1
 CASES = [("r3", 3, 1, False), ("r14", 14, 2, False), ("r11_prev", 11, 3, True)]   # (name, rounds, seed, has_prev)
 

@@ -164,17 +164,24 @@ def test_gate_form_rejects_bad_wire_index():
                             u64p(lin), 1, i32p(ab), u64p(cc)) == 0
 
 
-def test_bridge_without_device_fails_loudly():
-    import importlib
-    import truepix_b200.native_fp2_bridge as br
-    importlib.reload(br)
-    if br.GPU_ACTIVE:
+def test_library_without_device_fails_loudly():
+    """With no usable device the library's loader raises instead of falling back
+    to a CPU path, and a reference-facing session call returns NULL."""
+    from truepix_b200 import native
+    lib = native.gkr(require_device=False)
+    lib.native_fp2_init()
+    if lib.native_fp2_cuda_available():
         pytest.skip("a device is present")
-    assert not br.AVAILABLE and br.GPU_FAIL_REASON
+    native._cache.pop("gkr", None)
     with pytest.raises(RuntimeError):
-        br.compute_beta([1, 2, 3])
-    with pytest.raises(RuntimeError):
-        br.early_session_create([12], [0], [0], [1], 2, 1, [[1, 2]], [1, 1])
+        native.gkr()
+    lib = native.gkr(require_device=False)
+    gt = np.array([12], np.int32)
+    z = np.array([1], np.uint64)
+    v = np.array([1, 2], np.uint64)
+    h = lib.native_fp2_early_create(1, i32p(gt), i32p(gt * 0), i32p(gt * 0), u64p(z), u64p(z * 0), 2, 1,
+                                    u64p(v), u64p(v * 0), u64p(v), u64p(v * 0))
+    assert not h
 
 
 def test_orion_sizes_without_device():

@@ -187,55 +187,6 @@ def test_error_paths(gpu_lib):
                                b[:C // 2].copy())
 
 
-def test_bridge_api_vs_oracle(oracle_lib, circuits):
-    """The Python mirror of native_fp2_bridge, with Fp2 objects, against the oracle."""
-    import truepix_b200.native_fp2_bridge as br
-    assert br.GPU_ACTIVE, br.GPU_FAIL_REASON
-    rng = np.random.default_rng(17)
-    W, C = 512, 64
-    gt, i0, i1 = (circuits["Crop_" + k].tolist() for k in ("type", "in0", "in1"))
-    zr, zi = rand_fp(rng, len(gt)), rand_fp(rng, len(gt))
-    z1 = [br.Fp2(int(a), int(b)) for a, b in zip(zr, zi)]
-    vals = rng.integers(0, 256, size=(W, C), dtype=np.uint64)
-    rows = [[int(x) for x in row] for row in vals]
-    beta = br.compute_beta([br.Fp2(int(a), int(b)) for a, b in zip(rand_fp(rng, 6), rand_fp(rng, 6))])
-    sess = br.early_session_create(gt, i0, i1, z1, C, W, rows, beta)
-    o = oracle_lib.early_create(np.array(gt, np.int32), np.array(i0, np.int32),
-                                np.array(i1, np.int32), zr, zi, C, W, vals.reshape(-1).copy(),
-                                np.zeros(W * C, np.uint64),
-                                np.array([x.real for x in beta], np.uint64),
-                                np.array([x.imag for x in beta], np.uint64))
-    for k in range(6):
-        got = sess.claim()
-        want = oracle_lib.early_claim(o)[1]
-        assert [(x.real, x.imag) for x in got] == [(int(want[2 * t]), int(want[2 * t + 1]))
-                                                    for t in range(4)]
-        r = br.Fp2(int(rng.integers(0, P61)), int(rng.integers(0, P61)))
-        sess.fold(r)
-        oracle_lib.early_fold(o, (r.real, r.imag))
-    wires, bprev = sess.finish()
-    rc, wre, wim, ob = oracle_lib.early_finish(o, W)
-    assert [(w.real, w.imag) for w in wires] == list(zip(wre.tolist(), wim.tolist()))
-    assert (bprev.real, bprev.imag) == ob
-    sess.destroy()
-    oracle_lib.early_destroy(o)
-    # fold_values with expansion, compute_beta and mle_eval_base
-    vals = [br.Fp2(int(a), int(b)) for a, b in zip(rand_fp(rng, 64), rand_fp(rng, 64))]
-    out, scratch = br.fold_values(vals, 12345, expand_ncopies=3)
-    ore, oim = oracle_lib.fold(np.array([v.real for v in vals], np.uint64),
-                               np.array([v.imag for v in vals], np.uint64), (12345, 0))
-    assert [(x.real, x.imag) for x in scratch] == list(zip(ore.tolist(), oim.tolist()))
-    assert len(out) == 96 and out[5] == scratch[1]
-    x = [int(v) for v in rng.integers(0, P61, size=1000)]
-    zz = [br.Fp2(int(a), int(b)) for a, b in zip(rand_fp(rng, 10), rand_fp(rng, 10))]
-    got = br.mle_eval_base(x, zz)
-    xp = np.zeros(1024, np.uint64)
-    xp[:1000] = x
-    want = oracle_lib.mle_eval_base(xp, np.array([v.real for v in zz], np.uint64),
-                                    np.array([v.imag for v in zz], np.uint64))
-    assert (got.real, got.imag) == want
-
-
 def test_device_buffer_api(gpu_lib, oracle_lib, circuits):
     """tp_early_create_dev / tp_early_claim_dev / tp_early_finish_dev on torch buffers."""
     import torch
