@@ -211,9 +211,8 @@ TP_HD void step_head(Work& w, const Frame& f, const Shape& sh, int rd)
     if (f.chal) {
         r = f.chal[rd];
     } else {
-        uint8_t label[32];
-        const uint32_t len = vole::sc_label(label, sh.layer, sh.round0 + rd);
-        if (!vole::round(w.st, w.vs, c, 3, f.u, f.v, sh.count, label, len, f.proof ? f.proof + 4 * rd : nullptr,
+        const fs::Label label = vole::sc_label(sh.layer, sh.round0 + rd);
+        if (!vole::round(w.st, w.vs, c, 3, f.u, f.v, sh.count, label, f.proof ? f.proof + 4 * rd : nullptr,
                          &r))
             w.bad = 1;
     }
@@ -321,8 +320,7 @@ TP_HD void step_close_commit(Work& w, const Frame& f, const Shape& sh)
         rest_sum = f2add(rest_sum, w.hc[k]);
         rest_v = f2add(rest_v, w.vv[k]);
     }
-    const uint8_t pv[7] = {'p', 'o', 'k', '-', 'v', 'e', 'c'};
-    const fp2 c = fs::rand_fp2(w.st, pv, 7);
+    const fp2 c = fs::rand_fp2(w.st, fs::label_lit("pok-vec"));
     out[n + 2] = f2mul(rest_sum, c);
     out[n + 3] = f2mul(rest_v, c);
     fs::put_fp2(w.st, out[n + 2].re, out[n + 2].im);
@@ -391,13 +389,10 @@ TP_HD void step_close_tail(Work& w, const Frame& f, const Shape& sh)
         mz = f2mul(mz, f2sub(f2add(f2dbl(f2mul(wk, zk)), mk(1, 0)), f2add(wk, zk)));
     }
     const fp2 tv = f2mul(w.red[0][0], mz);
-    const uint8_t eq[2] = {'e', 'q'};
-    const fp2 e = fs::rand_fp2(w.st, eq, 2);
+    const fp2 e = fs::rand_fp2(w.st, fs::label_lit("eq"));
     out[n + 6] = f2mul(f2sub(w.vs.prev, tv), e);
     fs::put_fp2(w.st, out[n + 6].re, out[n + 6].im);
-    uint8_t label[32];
-    const uint32_t len = vole::tau_label(label, sh.layer);
-    const fp2 tau = fs::rand_fp2(w.st, label, len);
+    const fp2 tau = fs::rand_fp2(w.st, vole::tau_label(sh.layer));
     fp2 tag = w.vv[n];
     for (int k = n - 1; k >= 0; --k) tag = f2add(f2mul(tag, tau), w.vv[k]);
     for (int j = 0; j < n; ++j) f.point[j] = f2add(w.w[j], f2mul(f2sub(w.w[n + j], w.w[j]), tau));
@@ -408,15 +403,13 @@ TP_HD void step_close_tail(Work& w, const Frame& f, const Shape& sh)
         osum = f2add(osum, w.vs.out_elem[k]);
         vsum = f2add(vsum, w.vs.v_elem[k]);
     }
-    const uint8_t pf[9] = {'p', 'o', 'k', '-', 'f', 'i', 'n', 'a', 'l'};
-    const fp2 c = fs::rand_fp2(w.st, pf, 9);
+    const fp2 c = fs::rand_fp2(w.st, fs::label_lit("pok-final"));
     out[n + 7] = f2mul(osum, c);
     out[n + 8] = f2mul(vsum, c);
     fs::put_fp2(w.st, out[n + 7].re, out[n + 7].im);
     fs::put_fp2(w.st, out[n + 8].re, out[n + 8].im);
     // put(["gkr_input_point", [[re, im], ...]]): a string, then every coordinate's two ints
-    const uint8_t gp[15] = {'g', 'k', 'r', '_', 'i', 'n', 'p', 'u', 't', '_', 'p', 'o', 'i', 'n', 't'};
-    fs::put_str(w.st, gp, 15);
+    fs::put_label(w.st, fs::label_lit("gkr_input_point"));
     for (int k = 0; k < n + nb; ++k) {
         fs::absorb_byte(w.st, 0x02);
         fs::absorb_le(w.st, f.point[k].re, 8);
@@ -424,8 +417,7 @@ TP_HD void step_close_tail(Work& w, const Frame& f, const Shape& sh)
         fs::absorb_le(w.st, f.point[k].im, 8);
     }
     // create_input_value_proof
-    const uint8_t iv[9] = {'i', 'n', 'p', 'u', 't', '-', 'v', 'a', 'l'};
-    const fp2 civ = fs::rand_fp2(w.st, iv, 9);
+    const fp2 civ = fs::rand_fp2(w.st, fs::label_lit("input-val"));
     out[n + 9] = f2mul(tag, civ);
     fs::put_fp2(w.st, out[n + 9].re, out[n + 9].im);
     w.vs.prev = tag;

@@ -43,6 +43,23 @@ bool make_label(const char* label, Label* L, const char* who)
     return true;
 }
 
+// a label for device code, held by value (at most 32 bytes)
+bool make_device_label(const char* label, tp::fs::Label* L, const char* who)
+{
+    if (!label) {
+        tp::set_error(tp::TP_ERR_ARG, "%s: null label", who);
+        return false;
+    }
+    const size_t n = strlen(label);
+    if (n > 32) {
+        tp::set_error(tp::TP_ERR_ARG, "%s: a device label holds at most 32 bytes", who);
+        return false;
+    }
+    *L = tp::fs::label_empty();
+    for (size_t i = 0; i < n; ++i) tp::fs::label_push(*L, (uint8_t)label[i]);
+    return true;
+}
+
 __global__ void put_fp2s_kernel(State* __restrict__ st, int n, const ulonglong2* __restrict__ vals, int k)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -55,12 +72,12 @@ __global__ void put_fp2s_kernel(State* __restrict__ st, int n, const ulonglong2*
     st[i] = s;
 }
 
-__global__ void rand_ext_kernel(State* __restrict__ st, int n, Label L, ulonglong2* __restrict__ out)
+__global__ void rand_ext_kernel(State* __restrict__ st, int n, tp::fs::Label L, ulonglong2* __restrict__ out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     State s = st[i];
-    const tp::fp2 r = tp::fs::rand_fp2(s, L.b, L.len);
+    const tp::fp2 r = tp::fs::rand_fp2(s, L);
     st[i] = s;
     out[i] = make_ulonglong2(r.re, r.im);
 }
@@ -70,7 +87,7 @@ using VoleState = tp::vole::State;
 
 __global__ void vole_round_kernel(State* __restrict__ st, VoleState* __restrict__ vs, int n,
                                   const tp::fp2* __restrict__ claims, const tp::fp2* __restrict__ u,
-                                  const tp::fp2* __restrict__ v, long long count, Label L,
+                                  const tp::fp2* __restrict__ v, long long count, tp::fs::Label L,
                                   tp::fp2* __restrict__ chal, tp::fp2* __restrict__ proof)
 {
     using namespace tp;
@@ -82,7 +99,7 @@ __global__ void vole_round_kernel(State* __restrict__ st, VoleState* __restrict_
     vole::interpolate_cubic(claims[4 * i], claims[4 * i + 1], claims[4 * i + 2], claims[4 * i + 3], coef);
     const long long base = (long long)i * count;
     fp2 r;
-    vole::round(s, w, coef, 4, u + base, v + base, count, L.b, L.len, proof ? proof + 5 * i : nullptr, &r);
+    vole::round(s, w, coef, 4, u + base, v + base, count, L, proof ? proof + 5 * i : nullptr, &r);
     st[i] = s;
     vs[i] = w;
     chal[i] = r;
@@ -348,8 +365,8 @@ int tp_fs_rand_ext_dev(void* d_states, int n, const char* label, void* d_out, vo
 {
     tp::clear_error();
     if (!tp::ctx()) return -1;
-    Label L;
-    if (!make_label(label, &L, "tp_fs_rand_ext_dev")) return -1;
+    tp::fs::Label L;
+    if (!make_device_label(label, &L, "tp_fs_rand_ext_dev")) return -1;
     if (!d_states || n < 1 || !d_out) {
         tp::set_error(tp::TP_ERR_ARG, "tp_fs_rand_ext_dev: bad arguments");
         return -1;
@@ -422,8 +439,8 @@ int tp_vole_round_dev(void* d_fs_states, void* d_vole_states, int n, const void*
 {
     tp::clear_error();
     if (!tp::ctx()) return -1;
-    Label L;
-    if (!make_label(label, &L, "tp_vole_round_dev")) return -1;
+    tp::fs::Label L;
+    if (!make_device_label(label, &L, "tp_vole_round_dev")) return -1;
     if (!d_fs_states || !d_vole_states || n < 1 || !d_claims || !d_u || !d_v || count < 4 || !d_chal) {
         tp::set_error(tp::TP_ERR_ARG, "tp_vole_round_dev: bad arguments");
         return -1;

@@ -49,25 +49,88 @@ TP_HD void block(State& s)
 #endif
 }
 
-TP_HD void absorb(State& s, const uint8_t* p, uint64_t n)
+// one byte into the running hash
+TP_HD void absorb_byte(State& s, uint8_t b)
 {
-    for (uint64_t i = 0; i < n; ++i) {
-        s.buf[s.nbuf++] = p[i];
-        if (s.nbuf == 64) {
-            block(s);
-            s.nbuf = 0;
-        }
+    s.buf[s.nbuf++] = b;
+    if (s.nbuf == 64) {
+        block(s);
+        s.nbuf = 0;
     }
-    s.total += n;
+    s.total += 1;
 }
 
-TP_HD void absorb_byte(State& s, uint8_t b) { absorb(s, &b, 1); }
+// bytes from memory (the host entry points' caller-owned data)
+TP_HD void absorb(State& s, const uint8_t* p, uint64_t n)
+{
+    for (uint64_t i = 0; i < n; ++i) absorb_byte(s, p[i]);
+}
 
+// the low `bytes` bytes of v, least significant first
 TP_HD void absorb_le(State& s, uint64_t v, int bytes)
 {
-    uint8_t b[8];
-    for (int i = 0; i < bytes; ++i) b[i] = (uint8_t)(v >> (8 * i));
-    absorb(s, b, (uint64_t)bytes);
+    for (int i = 0; i < bytes; ++i) absorb_byte(s, (uint8_t)(v >> (8 * i)));
+}
+
+// A label of at most 32 bytes held by value in four 64-bit words (byte i in
+// bits 8 (i mod 8) of word i / 8). Device code builds, passes and absorbs labels
+// only in this form: no pointer to a local byte array is handed to the inlined
+// hash code (on sm_100a such a pointer, passed down through the fully inlined
+// draw, was observed to read the wrong bytes).
+struct Label {
+    uint64_t w0, w1, w2, w3;
+    uint32_t len;
+};
+
+TP_HD Label label_empty()
+{
+    Label L;
+    L.w0 = L.w1 = L.w2 = L.w3 = 0;
+    L.len = 0;
+    return L;
+}
+
+// append one byte (ignored past 32)
+TP_HD void label_push(Label& L, uint8_t b)
+{
+    const uint64_t v = (uint64_t)b << (8 * (L.len & 7));
+    const uint32_t q = L.len >> 3;
+    L.w0 |= q == 0 ? v : 0;
+    L.w1 |= q == 1 ? v : 0;
+    L.w2 |= q == 2 ? v : 0;
+    L.w3 |= q == 3 ? v : 0;
+    L.len += q < 4 ? 1 : 0;
+}
+
+// a label from a string literal of at most 32 characters
+template <int N>
+TP_HD Label label_lit(const char (&str)[N])
+{
+    static_assert(N - 1 <= 32, "labels hold at most 32 bytes");
+    Label L = label_empty();
+#pragma unroll
+    for (int i = 0; i < N - 1; ++i) label_push(L, (uint8_t)str[i]);
+    return L;
+}
+
+// the decimal digits of v (|v| < 2^31) appended, as Python's str(int) writes them
+TP_HD void label_decimal(Label& L, long long v)
+{
+    if (v < 0) {
+        label_push(L, '-');
+        v = -v;
+    }
+    long long p = 1;
+    while (p <= v / 10) p *= 10;
+    for (; p > 0; p /= 10) {
+        label_push(L, (uint8_t)('0' + (v / p) % 10));
+    }
+}
+
+TP_HD uint8_t label_byte(const Label& L, int i)
+{
+    const uint64_t w = i < 8 ? L.w0 : i < 16 ? L.w1 : i < 24 ? L.w2 : L.w3;
+    return (uint8_t)(w >> (8 * (i & 7)));
 }
 
 TP_HD void init(State& s)
@@ -101,14 +164,24 @@ TP_HD void put_str(State& s, const uint8_t* p, uint32_t len)
     absorb(s, p, len);
 }
 
-// the digest of everything absorbed so far (the running state is unchanged)
-TP_HD void digest(const State& s, uint8_t out[32])
+// put(str) of a label held by value
+TP_HD void put_label(State& s, const Label& L)
+{
+    absorb_byte(s, 0x04);
+    absorb_le(s, L.len, 4);
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+        if (i < (int)L.len) absorb_byte(s, label_byte(L, i));
+}
+
+// the running state with the SHA-256 padding absorbed: its words are the digest
+// of everything absorbed so far (the running state itself is unchanged)
+TP_HD State padded(const State& s)
 {
     State t = s;
     const uint64_t bits = t.total * 8;
-    uint8_t pad = 0x80;
     // pad without counting the padding in `total`
-    t.buf[t.nbuf++] = pad;
+    t.buf[t.nbuf++] = 0x80;
     if (t.nbuf > 56) {
         while (t.nbuf < 64) t.buf[t.nbuf++] = 0;
         block(t);
@@ -117,6 +190,13 @@ TP_HD void digest(const State& s, uint8_t out[32])
     while (t.nbuf < 56) t.buf[t.nbuf++] = 0;
     for (int i = 0; i < 8; ++i) t.buf[56 + i] = (uint8_t)(bits >> (56 - 8 * i));
     block(t);
+    return t;
+}
+
+// the digest bytes (big-endian words)
+TP_HD void digest(const State& s, uint8_t out[32])
+{
+    const State t = padded(s);
     for (int i = 0; i < 8; ++i) {
         out[4 * i] = (uint8_t)(t.h[i] >> 24);
         out[4 * i + 1] = (uint8_t)(t.h[i] >> 16);
@@ -127,47 +207,51 @@ TP_HD void digest(const State& s, uint8_t out[32])
 
 // A draw is redrawn only when its 61 bits are all ones (probability 2^-61); the
 // loop is bounded all the same, and past the bound returns the value reduced.
+// The low 64 bits of the big-endian digest are its last two words.
 TP_HD uint64_t rand_scalar(State& s)
 {
     uint64_t v = 0;
     for (int it = 0; it < 1000; ++it) {
-        const uint64_t r = s.rnum;
-        put_u64s(s, &r, 1);
+        // put([rnum]): a one-int list
+        absorb_byte(s, 0x01);
+        absorb_le(s, 1, 4);
+        absorb_le(s, s.rnum, 8);
         s.rnum += 1;
-        uint8_t d[32];
-        digest(s, d);
-        v = 0;
-        for (int i = 24; i < 32; ++i) v = (v << 8) | d[i];
-        v &= P61;
+        const State t = padded(s);
+        v = (((uint64_t)t.h[6] << 32) | t.h[7]) & P61;
         if (v < P61) return v;
     }
     return v % P61;
 }
 
-TP_HD void rand_ext(State& s, const uint8_t* label, uint32_t len, uint64_t* re, uint64_t* im)
+// rand_ext(label) as an Fp2: "ext", label, "real" -> the real limb; "ext",
+// label, "imag" -> the imaginary limb
+TP_HD fp2 rand_fp2(State& s, const Label& L)
 {
-    const uint8_t ext[3] = {'e', 'x', 't'};
-    const uint8_t real[4] = {'r', 'e', 'a', 'l'};
-    const uint8_t imag[4] = {'i', 'm', 'a', 'g'};
-    put_str(s, ext, 3);
-    put_str(s, label, len);
-    put_str(s, real, 4);
-    *re = rand_scalar(s);
-    put_str(s, ext, 3);
-    put_str(s, label, len);
-    put_str(s, imag, 4);
-    *im = rand_scalar(s);
+    const Label ext = label_lit("ext"), real = label_lit("real"), imag = label_lit("imag");
+    put_label(s, ext);
+    put_label(s, L);
+    put_label(s, real);
+    const uint64_t re = rand_scalar(s);
+    put_label(s, ext);
+    put_label(s, L);
+    put_label(s, imag);
+    const uint64_t im = rand_scalar(s);
+    return mk(re, im);
 }
 
-// rand_ext returned by value as an Fp2. The draw is written to uint64_t
-// (unsigned long) locals and converted; writing it through a uint64_t pointer
-// into an fp2's unsigned long long limbs would be a strict-aliasing violation,
-// which the device compiler may exploit by reading the limbs as never written.
-TP_HD fp2 rand_fp2(State& s, const uint8_t* label, uint32_t len)
+// the same draw with a label in memory (host entry points: labels of any length)
+TP_HD void rand_ext(State& s, const uint8_t* label, uint32_t len, uint64_t* re, uint64_t* im)
 {
-    uint64_t re, im;
-    rand_ext(s, label, len, &re, &im);
-    return mk(re, im);
+    const Label ext = label_lit("ext"), real = label_lit("real"), imag = label_lit("imag");
+    put_label(s, ext);
+    put_str(s, label, len);
+    put_label(s, real);
+    *re = rand_scalar(s);
+    put_label(s, ext);
+    put_str(s, label, len);
+    put_label(s, imag);
+    *im = rand_scalar(s);
 }
 
 }  // namespace fs

@@ -56,43 +56,22 @@ TP_HD void interpolate_quadratic(fp2 f0, fp2 f1, fp2 fm1, fp2 c[3])
     c[2] = c2;
 }
 
-// the decimal digits of v at out + n; returns the new length
-TP_HD uint32_t put_decimal(uint8_t* out, uint32_t n, long long v)
+// "sc-<layer>-<round>"
+TP_HD fs::Label sc_label(int layer, int round)
 {
-    if (v < 0) {
-        out[n++] = '-';
-        v = -v;
-    }
-    uint8_t dig[20];
-    int k = 0;
-    do {
-        dig[k++] = (uint8_t)('0' + v % 10);
-        v /= 10;
-    } while (v);
-    while (k) out[n++] = dig[--k];
-    return n;
+    fs::Label L = fs::label_lit("sc-");
+    fs::label_decimal(L, layer);
+    fs::label_push(L, '-');
+    fs::label_decimal(L, round);
+    return L;
 }
 
-// "sc-<layer>-<round>" into out (at most 3 + 2 * 11 bytes); returns the length
-TP_HD uint32_t sc_label(uint8_t* out, int layer, int round)
+// "tau-<layer>"
+TP_HD fs::Label tau_label(int layer)
 {
-    uint32_t n = 0;
-    out[n++] = 's';
-    out[n++] = 'c';
-    out[n++] = '-';
-    n = put_decimal(out, n, layer);
-    out[n++] = '-';
-    return put_decimal(out, n, round);
-}
-
-// "tau-<layer>" into out; returns the length
-TP_HD uint32_t tau_label(uint8_t* out, int layer)
-{
-    out[0] = 't';
-    out[1] = 'a';
-    out[2] = 'u';
-    out[3] = '-';
-    return put_decimal(out, 4, layer);
+    fs::Label L = fs::label_lit("tau-");
+    fs::label_decimal(L, layer);
+    return L;
 }
 
 // ExtVOLECommit.commit with one repetition: the tag v and d = m - u of the next
@@ -110,7 +89,7 @@ TP_HD fp2 commit(State& w, fp2 m, const fp2* u, const fp2* v, fp2* tag)
 // leaves the transcript untouched when fewer than n_coef correlations remain.
 // proof (optional): the n_coef values d, then the equality value.
 TP_HD bool round(fs::State& s, State& w, const fp2* c, int n_coef, const fp2* u, const fp2* v, long long count,
-                 const uint8_t* label, uint32_t len, fp2* proof, fp2* r_out)
+                 const fs::Label& label, fp2* proof, fp2* r_out)
 {
     if (w.bad || w.idx + (unsigned long long)n_coef > (unsigned long long)count) {
         w.bad = 1;
@@ -129,12 +108,11 @@ TP_HD bool round(fs::State& s, State& w, const fp2* c, int n_coef, const fp2* u,
     }
     fp2 now = tag[0];
     for (int k = 0; k < n_coef; ++k) now = f2add(now, tag[k]);
-    const uint8_t eq[2] = {'e', 'q'};
-    const fp2 e = fs::rand_fp2(s, eq, 2);
+    const fp2 e = fs::rand_fp2(s, fs::label_lit("eq"));
     const fp2 vz = w.has_prev ? f2mul(f2sub(w.prev, now), e) : f2mul(now, e);
     fs::put_fp2(s, vz.re, vz.im);
     if (proof) proof[n_coef] = vz;
-    const fp2 r = fs::rand_fp2(s, label, len);
+    const fp2 r = fs::rand_fp2(s, label);
     fp2 p = tag[n_coef - 1];
     for (int k = n_coef - 2; k >= 0; --k) p = f2add(f2mul(p, r), tag[k]);
     w.prev = p;
