@@ -337,6 +337,18 @@ int tp_fs_init(void* state, const char* protocol);
 int tp_fs_absorb(void* state, const void* bytes, size_t n);
 /* put(list of ints < 2^64): the array('Q') path (fiatshamir.py:112-120) */
 int tp_fs_put_u64s(void* state, const uint64_t* values, size_t n);
+/* For each of n_frames transcripts (host memory): put(the frame's circuit output
+ * vector) as a list of ints, the bytes tp_fs_put_u64s absorbs for the vector
+ * tp_circuit_outputs_pixels_dev writes (circuitnizkvec_vole.py:351-355), computed
+ * on the host copy by copy from the frame's bytes (pixels[f]: n_copies *
+ * copy_size bytes in host memory) and hashed as it is made; frames whose
+ * transcripts stand at the same offset are hashed two at a time in lockstep. The
+ * vector itself (2^23 values at 1080p) is never stored. Arguments as for
+ * tp_circuit_outputs_pixels_dev; n_gates <= 4096. */
+int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pixels, int n_frames, int n_copies,
+                                     int n_copies_padded, int copy_size, int n_wires, int const_idx,
+                                     uint64_t const_val, int n_gates, const int* gate_type, const int* in0,
+                                     const int* in1);
 /* put(Fp2) for each (re[i], im[i]) in turn (fiatshamir.py:129-131) */
 int tp_fs_put_fp2s(void* state, const uint64_t* re, const uint64_t* im, size_t n);
 /* put(str) (fiatshamir.py:132-136) */

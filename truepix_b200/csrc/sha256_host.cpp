@@ -59,9 +59,76 @@ extern "C" __attribute__((target("sha,sse4.1,ssse3"))) void tp_host_sha_ext_bloc
     _mm_storeu_si128(reinterpret_cast<__m128i*>(h + 4), _mm_alignr_epi8(dchg, feba, 8));  // e f g h
 }
 
+// N independent chains compressed in lockstep: chain c's state h[c], its blocks
+// at p[c]. One chain is bound by the latency of SHA256RNDS2 (each round pair
+// needs the previous one's result); interleaving the round pairs of N chains
+// keeps the SHA unit busy. The 16 XMM registers the SHA instructions can name
+// hold two chains' state and schedules without spilling.
+template <int N>
+__attribute__((target("sha,sse4.1,ssse3"), always_inline)) inline void sha_ext_lockstep(uint32_t* const* h,
+                                                                                        const uint8_t* const* p,
+                                                                                        size_t nblocks,
+                                                                                        const uint32_t K[64])
+{
+    const __m128i bswap = _mm_set_epi64x(0x0c0d0e0f08090a0bULL, 0x0405060700010203ULL);
+    __m128i abef[N], cdgh[N];
+    for (int c = 0; c < N; ++c) {
+        const __m128i abcd = _mm_shuffle_epi32(_mm_loadu_si128(reinterpret_cast<const __m128i*>(h[c])), 0xB1);
+        const __m128i efgh = _mm_shuffle_epi32(_mm_loadu_si128(reinterpret_cast<const __m128i*>(h[c] + 4)), 0x1B);
+        abef[c] = _mm_alignr_epi8(abcd, efgh, 8);
+        cdgh[c] = _mm_blend_epi16(efgh, abcd, 0xF0);
+    }
+    for (size_t blk = 0; blk < nblocks; ++blk) {
+        __m128i abef0[N], cdgh0[N], m[N][4];
+        for (int c = 0; c < N; ++c) {
+            abef0[c] = abef[c];
+            cdgh0[c] = cdgh[c];
+            const uint8_t* q = p[c] + 64 * blk;
+            for (int i = 0; i < 4; ++i)
+                m[c][i] = _mm_shuffle_epi8(_mm_loadu_si128(reinterpret_cast<const __m128i*>(q + 16 * i)), bswap);
+        }
+#pragma GCC unroll 16
+        for (int g = 0; g < 16; ++g) {
+            const __m128i k = _mm_loadu_si128(reinterpret_cast<const __m128i*>(K + 4 * g));
+            for (int c = 0; c < N; ++c) {
+                if (g >= 4) {
+                    const __m128i w7 = _mm_alignr_epi8(m[c][(g + 3) & 3], m[c][(g + 2) & 3], 4);
+                    m[c][g & 3] = _mm_sha256msg2_epu32(
+                        _mm_add_epi32(_mm_sha256msg1_epu32(m[c][g & 3], m[c][(g + 1) & 3]), w7), m[c][(g + 3) & 3]);
+                }
+                const __m128i wk = _mm_add_epi32(m[c][g & 3], k);
+                cdgh[c] = _mm_sha256rnds2_epu32(cdgh[c], abef[c], wk);
+                abef[c] = _mm_sha256rnds2_epu32(abef[c], cdgh[c], _mm_shuffle_epi32(wk, 0x0E));
+            }
+        }
+        for (int c = 0; c < N; ++c) {
+            abef[c] = _mm_add_epi32(abef[c], abef0[c]);
+            cdgh[c] = _mm_add_epi32(cdgh[c], cdgh0[c]);
+        }
+    }
+    for (int c = 0; c < N; ++c) {
+        const __m128i feba = _mm_shuffle_epi32(abef[c], 0x1B);
+        const __m128i dchg = _mm_shuffle_epi32(cdgh[c], 0xB1);
+        _mm_storeu_si128(reinterpret_cast<__m128i*>(h[c]), _mm_blend_epi16(feba, dchg, 0xF0));
+        _mm_storeu_si128(reinterpret_cast<__m128i*>(h[c] + 4), _mm_alignr_epi8(dchg, feba, 8));
+    }
+}
+
+// n chains (any n >= 1) of nblocks blocks each, in lockstep pairs
+extern "C" __attribute__((target("sha,sse4.1,ssse3"))) void tp_host_sha_ext_multi(uint32_t* const* h,
+                                                                                  const uint8_t* const* p, int n,
+                                                                                  size_t nblocks,
+                                                                                  const uint32_t K[64])
+{
+    int c = 0;
+    for (; c + 2 <= n; c += 2) sha_ext_lockstep<2>(h + c, p + c, nblocks, K);
+    if (c < n) sha_ext_lockstep<1>(h + c, p + c, nblocks, K);
+}
+
 #else
 
 extern "C" int tp_host_sha_ext_available(void) { return 0; }
 extern "C" void tp_host_sha_ext_blocks(uint32_t*, const uint8_t*, size_t, const uint32_t*) {}
+extern "C" void tp_host_sha_ext_multi(uint32_t* const*, const uint8_t* const*, int, size_t, const uint32_t*) {}
 
 #endif

@@ -7,6 +7,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <vector>
+
 #include "runtime.h"
 #include "transcript.cuh"
 #include "vole.cuh"
@@ -14,6 +16,8 @@
 
 extern "C" int tp_host_sha_ext_available(void);
 extern "C" void tp_host_sha_ext_blocks(uint32_t h[8], const uint8_t* p, size_t nblocks, const uint32_t K[64]);
+extern "C" void tp_host_sha_ext_multi(uint32_t* const* h, const uint8_t* const* p, int n, size_t nblocks,
+                                      const uint32_t K[64]);
 
 namespace {
 
@@ -161,6 +165,107 @@ void host_absorb_header(State& s, uint8_t tag, uint32_t n)
     host_absorb(s, b, 5);
 }
 
+// n chains of nblocks whole blocks each (with the SHA extensions: in lockstep pairs)
+void host_blocks_multi(uint32_t* const* h, const uint8_t* const* p, int n, size_t nblocks)
+{
+    if (host_sha_ext()) {
+        tp_host_sha_ext_multi(h, p, n, nblocks, kHostTables.k);
+        return;
+    }
+    for (int c = 0; c < n; ++c) host_blocks(h[c], p[c], nblocks);
+}
+
+// ---- a frame's circuit outputs put into its transcript, computed on the host --
+// The output vector (tp_circuit_outputs_pixels_dev's, 64 MiB at 1080p) is
+// generated copy by copy from the frame's bytes into a small staging buffer per
+// frame and hashed from there: nothing of the size of the vector is written or
+// copied. Frames whose transcripts stand at the same offset in their pending
+// block hash in lockstep pairs.
+
+// native_fp2_core.hpp:32-51 on canonical base-field values (as the device kernel)
+uint64_t host_gate_value(unsigned type, uint64_t x, uint64_t y)
+{
+    using tp::fadd;
+    using tp::fsub;
+    auto mul = [](uint64_t a, uint64_t b) { return tp::fmul(a, b); };
+    switch (type) {
+    case 0: return mul(x, y);
+    case 1: return fadd(x, y);
+    case 2: return fsub(x, y);
+    case 3: return x;
+    case 4: return y;
+    case 5: return fsub(fadd(x, y), mul(x, y));
+    case 6: return fsub(fadd(x, y), fadd(mul(x, y), mul(x, y)));
+    case 7: return fsub(1, x);
+    case 8: return fsub(1, mul(x, y));
+    case 9: return fsub(fadd(1, mul(x, y)), fadd(x, y));
+    case 10: return fsub(fadd(1, fadd(mul(x, y), mul(x, y))), fadd(x, y));
+    case 11: return mul(fsub(1, x), y);
+    default: return x;
+    }
+}
+
+struct OutputCircuit {
+    int n_copies, n_copies_padded, cs, n_wires, const_idx, n_gates, out_bits;
+    uint64_t const_val;
+    std::vector<uint32_t> type, src0, src1;   // src: the wire, or n_wires for "zero", n_wires + 1 for the constant
+    std::vector<uint8_t> direct;              // the gate's value is one of its inputs (pass, multiplexer)
+};
+
+// copy c's outputs (2^out_bits LE64 values) at out
+void copy_outputs(const OutputCircuit& C, const uint8_t* pix, long long c, uint64_t* out)
+{
+    const int G = 1 << C.out_bits;
+    if (c >= C.n_copies) {
+        memset(out, 0, 8 * (size_t)G);
+        return;
+    }
+    const uint8_t* row = pix + c * C.cs;
+    const uint32_t cs = (uint32_t)C.cs, konst = (uint32_t)C.n_wires + 1;
+    auto val = [&](uint32_t a) -> uint64_t { return a < cs ? row[a] : a == konst ? C.const_val : 0; };
+    for (int g = 0; g < C.n_gates; ++g) {
+        const uint64_t va = val(C.src0[g]);
+        out[g] = C.direct[g] ? va : host_gate_value(C.type[g], va, val(C.src1[g]));
+    }
+    if (G > C.n_gates) memset(out + C.n_gates, 0, 8 * (size_t)(G - C.n_gates));
+}
+
+// the values of copies [c0, c0 + nc) of every frame of a group, hashed in lockstep
+void put_outputs_group(State* const* st, const uint8_t* const* pix, int k, const OutputCircuit& C)
+{
+    constexpr long long kCopiesPerChunk = 16;
+    const size_t copy_bytes = (size_t)8 << C.out_bits;
+    const size_t cap = 64 + kCopiesPerChunk * copy_bytes;
+    std::vector<uint8_t> stage((size_t)k * cap);
+    uint32_t* h[2];
+    const uint8_t* p[2];
+    size_t fill = st[0]->nbuf;   // equal for every frame of the group
+    for (int c = 0; c < k; ++c) memcpy(&stage[(size_t)c * cap], st[c]->buf, fill);
+    const uint64_t n_values = (uint64_t)C.n_copies_padded << C.out_bits;
+    for (long long c0 = 0; c0 < C.n_copies_padded; c0 += kCopiesPerChunk) {
+        const long long nc = C.n_copies_padded - c0 < kCopiesPerChunk ? C.n_copies_padded - c0 : kCopiesPerChunk;
+        for (int c = 0; c < k; ++c) {
+            uint8_t* base = &stage[(size_t)c * cap] + fill;
+            for (long long q = 0; q < nc; ++q)
+                copy_outputs(C, pix[c], c0 + q, reinterpret_cast<uint64_t*>(base + q * copy_bytes));
+        }
+        const size_t total = fill + (size_t)nc * copy_bytes;
+        const size_t nblk = total / 64;
+        for (int c = 0; c < k; ++c) {
+            h[c] = st[c]->h;
+            p[c] = &stage[(size_t)c * cap];
+        }
+        host_blocks_multi(h, p, k, nblk);
+        fill = total - 64 * nblk;
+        for (int c = 0; c < k; ++c) memmove(&stage[(size_t)c * cap], &stage[(size_t)c * cap] + 64 * nblk, fill);
+    }
+    for (int c = 0; c < k; ++c) {
+        memcpy(st[c]->buf, &stage[(size_t)c * cap], fill);
+        st[c]->nbuf = (uint32_t)fill;
+        st[c]->total += 8 * n_values;
+    }
+}
+
 // ---- the Orion opening's transcript (truepix_orion::FsTranscript, orion_fs.cpp) --
 // state' = SHA-256(state || chunk || zero pad) for each chunk of <= 32 bytes
 struct OrionFs {
@@ -276,6 +381,76 @@ int tp_fs_put_u64s(void* state, const uint64_t* v, size_t n)
     State& s = *static_cast<State*>(state);
     host_absorb_header(s, 0x01, (uint32_t)n);
     host_absorb(s, reinterpret_cast<const uint8_t*>(v), 8 * (uint64_t)n);
+    return 0;
+}
+
+int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pixels, int n_frames, int n_copies,
+                                     int n_copies_padded, int copy_size, int n_wires, int const_idx,
+                                     uint64_t const_val, int n_gates, const int* gate_type, const int* in0,
+                                     const int* in1)
+{
+    tp::clear_error();
+    const long long values = n_copies_padded >= 1 && n_gates >= 1
+                                 ? ((long long)n_copies_padded << tp_circuit_out_bits(n_gates)) : 0;
+    if (!states || !pixels || n_frames < 1 || n_copies < 1 || n_copies_padded < n_copies ||
+        (n_copies_padded & (n_copies_padded - 1)) != 0 || copy_size < 1 || n_wires < copy_size ||
+        n_wires > (1 << 14) || const_idx >= n_wires || (const_idx >= 0 && const_idx < copy_size) ||
+        const_val >= tp::P61 || n_gates < 1 || n_gates > 4096 || !gate_type || !in0 || !in1 ||
+        values >= (1ll << 32)) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_fs_put_circuit_outputs_pixels: bad arguments");
+        return -1;
+    }
+    OutputCircuit C;
+    C.n_copies = n_copies;
+    C.n_copies_padded = n_copies_padded;
+    C.cs = copy_size;
+    C.n_wires = n_wires;
+    C.const_idx = const_idx;
+    C.const_val = const_val;
+    C.n_gates = n_gates;
+    C.out_bits = tp_circuit_out_bits(n_gates);
+    // sources: a byte of the copy (wire < copy_size), the constant (n_wires + 1), else zero (n_wires)
+    auto src = [&](int w) -> uint32_t {
+        return w < copy_size ? (uint32_t)w : w == const_idx ? (uint32_t)n_wires + 1 : (uint32_t)n_wires;
+    };
+    for (int g = 0; g < n_gates; ++g) {
+        if (gate_type[g] < 0 || gate_type[g] > 12 || in0[g] < 0 || in0[g] >= n_wires || in1[g] < 0 ||
+            in1[g] >= n_wires) {
+            tp::set_error(tp::TP_ERR_ARG, "tp_fs_put_circuit_outputs_pixels: gate %d out of range", g);
+            return -1;
+        }
+        const int t = gate_type[g];
+        const bool right = t == 4;
+        C.type.push_back((uint32_t)t);
+        C.src0.push_back(src(right ? in1[g] : in0[g]));
+        C.src1.push_back(src(in1[g]));
+        C.direct.push_back(t == 3 || t == 4 || t == 12);
+    }
+    for (int f = 0; f < n_frames; ++f) {
+        if (!states[f] || !pixels[f]) {
+            tp::set_error(tp::TP_ERR_ARG, "tp_fs_put_circuit_outputs_pixels: null state or frame %d", f);
+            return -1;
+        }
+        State& s = *static_cast<State*>(states[f]);
+        host_absorb_header(s, 0x01, (uint32_t)values);
+    }
+    // pairs of frames at the same offset hash in lockstep, the rest alone
+    std::vector<int> done(n_frames, 0);
+    for (int f = 0; f < n_frames; ++f) {
+        if (done[f]) continue;
+        done[f] = 1;
+        State* st[2] = {static_cast<State*>(states[f]), nullptr};
+        const uint8_t* px[2] = {static_cast<const uint8_t*>(pixels[f]), nullptr};
+        int k = 1;
+        for (int g = f + 1; g < n_frames && k < 2; ++g)
+            if (!done[g] && static_cast<State*>(states[g])->nbuf == st[0]->nbuf) {
+                done[g] = 1;
+                st[1] = static_cast<State*>(states[g]);
+                px[1] = static_cast<const uint8_t*>(pixels[g]);
+                k = 2;
+            }
+        put_outputs_group(st, px, k, C);
+    }
     return 0;
 }
 

@@ -93,6 +93,8 @@ GKR_SIGNATURES = {
     "tp_fs_init": (_I32, [_VP, ctypes.c_char_p]),
     "tp_fs_absorb": (_I32, [_VP, _VP, ctypes.c_size_t]),
     "tp_fs_put_u64s": (_I32, [_VP, _VP, ctypes.c_size_t]),
+    "tp_fs_put_circuit_outputs_pixels": (_I32, [_VP, _VP, _I32, _I32, _I32, _I32, _I32, _I32, _U64, _I32, _PI32,
+                                                _PI32, _PI32]),
     "tp_fs_put_fp2s": (_I32, [_VP, _VP, _VP, ctypes.c_size_t]),
     "tp_fs_put_str": (_I32, [_VP, ctypes.c_char_p]),
     "tp_fs_rand_scalar": (_I32, [_VP, _VP]),
