@@ -110,6 +110,11 @@ int tp_orion_combine_dev(const void* d_rows, long long N, const void* d_r0, void
  * Synchronises the stream. */
 int tp_orion_query_columns_dev(const void* d_rows, long long N, const void* d_q, int count, void* d_out,
                                void* stream);
+/* tp_orion_query_columns_dev without waiting for the device: an index outside
+ * the codeword gives a zero column and sets *d_bad (device int, optional; the
+ * caller clears it and reads it back later). Async on `stream`. */
+int tp_orion_query_columns_async_dev(const void* d_rows, long long N, const void* d_q, int count, void* d_out,
+                                     int* d_bad, void* stream);
 
 /* answer = sum_{i < msg_len} r1[i] * combined_message[i] (linearPC.cpp:569-571);
  * d_answer: one element. */
@@ -222,6 +227,22 @@ int tp_virgo_phase1_init_dev(void* layer, const void* d_values, const uint64_t* 
 int tp_virgo_phase2_init_dev(void* layer, const void* d_values, const uint64_t* r0, const uint64_t* r1,
                              const uint64_t* alpha, const uint64_t* beta, const void* d_vma0, const uint64_t* prev_r,
                              const uint64_t* r_u, void* d_vma, void* d_addv, void* d_ams, void* stream);
+
+/* ---- opening helpers for a prover of many frames ----
+ * eq(z, i) for i < 2^k, bit j of i <-> z_j (LSB first), as native_fp2_compute_beta
+ * with init 1 (native_fp2_core.hpp:139-161) but on the host: z: k (re, im)
+ * pairs, canonical; out: 2^k (re, im) pairs. The opening's column and row
+ * weights (linearPC.cpp:693-731 dfs over the reversed point halves). k <= 26. */
+int tp_eq_table_host(const uint64_t* z, int k, uint64_t* out);
+/* collect_merkle_siblings (orion_proof.cpp:153-174): for each position in order,
+ * the siblings on its path to the root (heap order, root 1) not listed before;
+ * writes their node indices to out_nodes (cap entries) and returns how many
+ * (-1 on bad arguments or when more than cap). */
+int tp_orion_path_nodes(long long n_leaves, const long long* positions, int count, int* out_nodes, int cap);
+/* d_out[i] = the 32-byte node d_nodes[i] of a heap-ordered tree of n_nodes_tree
+ * digests (device; a node index outside the tree gives 32 zero bytes). Async. */
+int tp_orion_gather_nodes_dev(const void* d_tree, long long n_nodes_tree, const void* d_nodes, int n, void* d_out,
+                              void* stream);
 
 #ifdef __cplusplus
 }

@@ -24,7 +24,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
 LIBS = {
     "libnative_fp2_gpu.so": ["runtime.cu", "gkr.cu", "gkr_pixels.cu", "gkr_batch.cu", "gkr_session.cu",
                              "native_fp2_abi.cu", "mle_noalloc.cu", "orion.cu", "orion_open.cu", "orion_abi.cu", "ntt.cu", "rs_commit.cu", "virgo.cu", "ntt_abi.cu",
-                             "transcript.cu", "sha256_host.cpp", "circuit.cu", "late.cu"],
+                             "transcript.cu", "sha256_host.cpp", "circuit.cu", "late.cu", "open_host.cu"],
 }
 
 

@@ -111,6 +111,9 @@ bool combine(const ulonglong2* rows, long long col_len, long long cw_len, const 
 // to report indices outside [0, cw_len)
 bool query_rows(const ulonglong2* rows, long long cw_len, const long long* q, int count, ulonglong2* out,
                 cudaStream_t s);
+// query_rows without the host round trip: bad rows give zeros and raise *bad
+bool query_rows_async(const ulonglong2* rows, long long cw_len, const long long* q, int count, ulonglong2* out,
+                      int* bad, cudaStream_t s);
 // *out = sum_{i < n} r1[i] combined[i]
 bool answer(const ulonglong2* combined, const ulonglong2* r1, long long n, ulonglong2* out, cudaStream_t s);
 

@@ -279,6 +279,24 @@ int tp_orion_query_columns_dev(const void* d_rows, long long N, const void* d_q,
                : -1;
 }
 
+int tp_orion_query_columns_async_dev(const void* d_rows, long long N, const void* d_q, int count, void* d_out,
+                                     int* d_bad, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!check_n(N, "tp_orion_query_columns_async_dev")) return -1;
+    if (!d_rows || !d_q || !d_out || count <= 0) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_query_columns_async_dev: bad arguments");
+        return -1;
+    }
+    const long long col_len = N / tp::orion::kColumns;
+    return tp::orion::query_rows_async(static_cast<const ulonglong2*>(d_rows), tp::orion::codeword_len(col_len),
+                                       static_cast<const long long*>(d_q), count, static_cast<ulonglong2*>(d_out),
+                                       d_bad, reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
 int tp_orion_answer_dev(const void* d_combined, long long msg_len, const void* d_r1, void* d_answer, void* stream)
 {
     tp::clear_error();

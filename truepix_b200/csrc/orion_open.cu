@@ -94,6 +94,20 @@ __global__ void __launch_bounds__(128) query_kernel(const ulonglong2* __restrict
     out[(long long)i * kColumns + threadIdx.x] = __ldg(rows + r * kColumns + threadIdx.x);
 }
 
+// the same without a host round trip: a row index outside [0, cw_len) gives a
+// zero row and raises *bad (when given), which the caller reads later
+__global__ void __launch_bounds__(128) query_async_kernel(const ulonglong2* __restrict__ rows, long long cw_len,
+                                                          const long long* __restrict__ q, int count,
+                                                          ulonglong2* __restrict__ out, int* __restrict__ bad)
+{
+    const int i = blockIdx.x;
+    if (i >= count) return;
+    const long long r = q[i];
+    const bool in = r >= 0 && r < cw_len;
+    if (!in && bad && threadIdx.x == 0) atomicExch(bad, 1);
+    out[(long long)i * kColumns + threadIdx.x] = in ? __ldg(rows + r * kColumns + threadIdx.x) : make_ulonglong2(0, 0);
+}
+
 // answer = sum_i r1[i] * combined[i], i < n: one CTA per 4096 entries, partial
 // sums to `part`, the last CTA (ticket) adds them up
 __global__ void __launch_bounds__(256) answer_kernel(const ulonglong2* __restrict__ combined,
@@ -171,6 +185,13 @@ bool query_rows(const ulonglong2* rows, long long cw_len, const long long* q, in
         return false;
     }
     return good;
+}
+
+bool query_rows_async(const ulonglong2* rows, long long cw_len, const long long* q, int count, ulonglong2* out,
+                      int* bad, cudaStream_t s)
+{
+    query_async_kernel<<<count, 128, 0, s>>>(rows, cw_len, q, count, out, bad);
+    return ok("orion query");
 }
 
 bool answer(const ulonglong2* combined, const ulonglong2* r1, long long n, ulonglong2* out, cudaStream_t s)

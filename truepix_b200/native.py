@@ -93,6 +93,9 @@ GKR_SIGNATURES = {
     "tp_fs_init": (_I32, [_VP, ctypes.c_char_p]),
     "tp_fs_absorb": (_I32, [_VP, _VP, ctypes.c_size_t]),
     "tp_fs_put_u64s": (_I32, [_VP, _VP, ctypes.c_size_t]),
+    "tp_eq_table_host": (_I32, [_VP, _I32, _VP]),
+    "tp_orion_path_nodes": (_I32, [ctypes.c_longlong, _VP, _I32, _VP, _I32]),
+    "tp_orion_gather_nodes_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _I32, _VP, _VP]),
     "tp_fs_put_circuit_outputs_pixels": (_I32, [_VP, _VP, _I32, _I32, _I32, _I32, _I32, _I32, _U64, _I32, _PI32,
                                                 _PI32, _PI32]),
     "tp_fs_put_fp2s": (_I32, [_VP, _VP, _VP, ctypes.c_size_t]),
@@ -121,6 +124,7 @@ GKR_SIGNATURES = {
     "tp_orion_last_launches": (_I32, []),
     "tp_orion_combine_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP, _VP, _VP]),
     "tp_orion_query_columns_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _I32, _VP, _VP]),
+    "tp_orion_query_columns_async_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _I32, _VP, _VP, _VP]),
     "tp_orion_answer_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP, _VP]),
     "tp_sha256_peak_dev": (_I32, [_I32, _I32, _VP, _VP]),
     "tp_fft": (_I32, [_VP, _I32, _I32, _VP]),

@@ -93,8 +93,13 @@ def opening_bytes(N, msg_len, cw_len, answer, com_root, comb_root, col_q, cols, 
            np.ascontiguousarray(combined, np.uint64).tobytes(),
            np.ascontiguousarray(combined[:msg_len], np.uint64).tobytes()]
     for idxs, digs in (com_sparse, comb_sparse):
-        out.append(struct.pack("<Q", len(idxs)))
-        out += [struct.pack("<I", i) + d for i, d in zip(idxs, digs)]
+        # u32 node index then its 32-byte digest, per node
+        rec = np.empty(len(idxs), dtype=[("i", "<u4"), ("d", "u1", 32)])
+        rec["i"] = np.asarray(idxs, np.uint32)
+        if len(idxs):
+            rec["d"] = np.frombuffer(b"".join(digs), np.uint8).reshape(-1, 32) if isinstance(digs, list) \
+                else np.asarray(digs, np.uint8).reshape(-1, 32)
+        out += [struct.pack("<Q", len(idxs)), rec.tobytes()]
     return b"".join(out)
 
 
