@@ -1,41 +1,42 @@
-"""Benchmark: proved 1080p frames/s on one B200 (device prover core of TruePix).
+"""Benchmark: proved 1080p frames/s on one B200.
 
 Workload: seeded 1920x1080x3 uint8 frames; each frame is 16,200 copies of 384
-bytes padded to 16,384 x 512 input wires (2^23). One frame's device work:
+bytes padded to 16,384 x 512 input wires (2^23), proved with TruePix's gray
+circuit. A proved frame is what TruePix's prover phase writes for it
+(run_truepix_prover.py:218-421, plain prover -z 2): the GKR input layer's NIZK
+proof (the IO transcript over the circuit's 2^23 outputs, 14 early and 18 late
+VOLE-committed sumcheck rounds, the layer's closing proofs) and the Orion
+opening proof (orion_proof.bin) of the frame's input commitment, which is made
+in the same run.
 
-  GKR input layer (truepix_b200.frame): beta over the 14 copy challenges, 14
-    early sumcheck rounds (claim + fold; rounds 0 and 1 read the frame's bytes),
-    finish, and the MLE of the 2^23-entry input vector at the final point;
-  Orion input commitment (truepix_b200.orion): expander encode of the 128
-    columns and the SHA-256 Merkle tree over the 2^17 codeword rows, read from
-    the bytes; codeword and tree stay in HBM for the opening.
+One step = one batch of B frames (default 64) through truepix_b200.pipeline:
+commits on side streams and IO transcripts on host threads for one batch while
+the GKR rounds and openings of the previous batch run on the main stream.
 
-One step = one batch of B frames (default 64): one kernel launch per sumcheck
-round for the whole batch (BatchFrameProver), then the B commits. Inputs stay
-in HBM: B frames (400 MB of bytes), their folded tables (~4.8 GB) and
-codewords (14.8 GB) are far larger than the 126 MB L2, so no flush is needed.
+  value         proved frames/s, frames resident in HBM (and in host memory,
+                where the IO transcript hashes them); CUDA events on the main
+                stream around all steps, the last event recorded after every
+                proof of the last step is assembled on the host
+  e2e           the same from pinned host frames only: their upload is inside
+                the timed region, every proof comes back to host memory
+  proof_check   one frame of the timed run against the step-by-step path
+                (prove_frames + opening_proof, pinned to the reference's proofs
+                and opening files by the GPU tests): byte-identical or the line
+                is marked invalid
+  breakdown     the single-instance prover (one frame at a time, every stage
+                synchronous), batched over plain
+  device_core   the device part alone (batched GKR input layer + MLE + Orion
+                commit per frame from resident bytes, challenges given): its
+                kernels with their time shares and the roofline of the dominant
+                ones (the SHA-256 leaf kernel against the integer-ALU pipe, the
+                fold kernel against HBM)
+  cpu_baseline  the reference implementation's proved frame on one host core
+                (oracle/reference_proof.py: the reference's compiled commit,
+                native_fp2.cpp and linearPC_multi_prove + fft_gkr programs, its
+                Python steps restated)
 
-  value         frames/s over all ranks, device time (CUDA events)
-  breakdown     the step split into its GKR part and its commit part, and the
-                GKR part alone batched vs one frame at a time (`plain`)
-  kernels       every kernel kind of the step: launches, time share, algorithmic
-                bytes, achieved GB/s (the library's kernel timer, CUDA events)
-  roofline      the kernel with the largest share, against MEASURED_PEAKS.json;
-                for the SHA-256 leaf kernel also compressions/s against the
-                register-only throughput of the same SHA-256 code
-  ntt           the Fp2 NTT / IFFT / rate-2^-5 RS commit microbenchmark at
-                2^16, 2^20, 2^24 points
-  e2e           the batched path from pinned host frames: H2D of the bytes, a
-                D2H of all claims after every round with a synchronise (the host
-                transcript needs them), D2H of wires, MLEs and commitment roots
-  e2e_reference_abi  one frame through the reference-facing C ABI with host
-                buffers (native_fp2_* and tp_orion_commit)
-  cpu_baseline  the reference CPU implementation (native_fp2.cpp and the Orion
-                sources, built from the reference by oracle/Makefile) proving one
-                frame of the same workload on one host core
-
-`--impl reference` times that reference CPU implementation on all host cores
-instead (one frame per worker process per step) and prints the same metric.
+`--impl reference` runs that reference proved frame on all host cores (one
+process per core, one frame per process per step) and prints the same metric.
 """
 from __future__ import annotations
 
@@ -52,8 +53,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 from truepix_b200 import native  # noqa: E402
 
-METRIC = "1080p proved frames/s (GKR input-layer sumcheck + input MLE + Orion input commitment, gray circuit)"
-WORKLOAD = "prover_core_gray_1080p"
+METRIC = ("1080p proved frames/s (whole proof per frame: GKR input-layer NIZK proof with VOLE commitments "
+          "+ Orion commitment and opening proof, gray circuit)")
+WORKLOAD = "proved_frame_gray_1080p"
 UNIT = "frames/s"
 H, Wd = 1080, 1920
 P61 = (1 << 61) - 1
@@ -94,71 +96,12 @@ def host_tables(pix, layout):
 # sources: native_fp2.cpp and the Orion commit) or the oracle ports when those
 # builds are absent.
 
-def cpu_lib():
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from fp2lib import Fp2Lib, REF_LIB, ORACLE_LIB
-    if os.path.exists(REF_LIB):
-        return Fp2Lib(REF_LIB, "native_fp2_"), "reference"
-    if not os.path.exists(ORACLE_LIB):
-        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"])
-    return Fp2Lib(ORACLE_LIB, "oracle_fp2_"), "port"
-
-
-def cpu_commit_fn():
-    """fn(elements) -> 32-byte root: the reference's commit() (ref_commit of
-    oracle/_ref/liborion_ref.so) or the oracle's restatement."""
-    import ctypes
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from orionlib import ORION_REF_LIB, ORION_ORACLE_LIB, OrionOracle
-    V = ctypes.c_void_p
-    if os.path.exists(ORION_REF_LIB):
-        lib = ctypes.CDLL(ORION_REF_LIB)
-        lib.ref_commit.argtypes = [V, ctypes.c_longlong, V, V]
-
-        def fn(src):
-            root, hx = ctypes.create_string_buffer(32), ctypes.create_string_buffer(80)
-            lib.ref_commit(V(src.ctypes.data), src.size // 2, root, hx)
-            return root.raw
-        return fn, "reference"
-    if not os.path.exists(ORION_ORACLE_LIB):
-        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"])
-    orc = OrionOracle()
-    return orc.commit, "port"
-
-
-def cpu_prove_frame(lib, commit, gt, i0, i1, z1, z2, point, chal, table, inputs, elems, layout):
-    from fp2lib import run_session
-    C, W = layout.padded_copies, layout.n_wires
-    bre, bim = lib.compute_beta(np.ascontiguousarray(z2[:, 0]), np.ascontiguousarray(z2[:, 1]),
-                                (1, 0))
-    run_session(lib, gt, i0, i1, z1[0], z1[1], C, W, table, np.zeros_like(table), bre, bim, chal)
-    lib.mle_eval_base(inputs, np.ascontiguousarray(point[:, 0]), np.ascontiguousarray(point[:, 1]))
-    return commit(elems)
-
-
 def frame_elements(pix, layout):
     """The commit input of a frame: element copy * W + wire (img 0, real value)."""
     _, inputs = host_tables(pix, layout)
     out = np.zeros(2 * inputs.size, np.uint64)
     out[1::2] = inputs
     return out
-
-
-def _cpu_worker(args):
-    idx, n_frames = args
-    from truepix_b200.frame import FrameLayout
-    layout = FrameLayout.for_frame(H, Wd)
-    rng = np.random.default_rng(SEED + idx)
-    frames, z1, z2, point, chal = make_inputs(rng, layout, 1)
-    table, inputs = host_tables(frames[0], layout)
-    elems = frame_elements(frames[0], layout)
-    lib, kind = cpu_lib()
-    commit, ckind = cpu_commit_fn()
-    gt, i0, i1 = circuit()
-    t0 = time.perf_counter()
-    for _ in range(n_frames):
-        cpu_prove_frame(lib, commit, gt, i0, i1, z1, z2, point, chal, table, inputs, elems, layout)
-    return time.perf_counter() - t0, kind if kind == ckind else kind + "+" + ckind
 
 
 def _cpu_zk_commit(_):
@@ -188,42 +131,80 @@ def _cpu_zk_commit(_):
     return time.perf_counter() - t0, "reference"
 
 
+def _cpu_proved_worker(args):
+    """(seconds for n_frames proved frames, stage seconds of the last) of the
+    reference implementation on this process's core (oracle/reference_proof.py)"""
+    idx, n_frames = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference_proof
+    from truepix_b200.frame import FrameLayout
+    os.environ["OMP_NUM_THREADS"] = "1"
+    layout = FrameLayout.for_frame(H, Wd)
+    rng = np.random.default_rng(SEED + idx)
+    pix = rng.integers(0, 256, size=layout.copies * layout.copy_size, dtype=np.uint8)
+    count = 4 * layout.n_copy_bits + 7 * layout.n_in_bits + 2
+    u = rng.integers(0, P61, size=(count, 2), dtype=np.uint64)
+    v = rng.integers(0, P61, size=(count, 2), dtype=np.uint64)
+    gt, i0, i1 = circuit()
+    t0 = time.perf_counter()
+    stages = None
+    for k in range(n_frames):
+        stages = reference_proof.prove_frame(pix, layout.copies, layout.copy_size, layout.const_idx,
+                                             layout.const_val, gt, i0, i1, 1000 + idx * 100 + k, u, v)["times"]
+    return time.perf_counter() - t0, stages
+
+
+REFERENCE_SAMPLE = ("per frame: the reference's commit() of the 2^23 inputs (commit phase); circuit outputs and "
+                    "the IO transcript (hashlib, as fiatshamir.py); compute_beta, 14 early rounds and finish in "
+                    "the reference's native_fp2.cpp; the VOLE-committed round loop, 18 late rounds and the "
+                    "closing proofs restated in Python as the reference prover runs them; the reference's "
+                    "linearPC_multi_prove program (recommit, tensor-product opening, EC(y1) self-check with "
+                    "its ./fft_gkr) writing orion_proof.bin")
+
+
 def reference_arm(args, rank, world):
-    """The reference CPU implementation on all host cores (rank 0 only). One step
-    = one frame per worker process; at most 6 timed frames per worker (a frame
-    takes ~7 s on one core), so the run ends within a few minutes."""
+    """The reference implementation's proved frames on all host cores (rank 0
+    only): one process per core, each step one frame per process. A proved frame
+    takes ~14 s on one core, so at most two timed steps run after one warm-up
+    step; the line reports the steps run."""
     if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference_proof
+    why = reference_proof.available()
+    if why:
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
         return
     import multiprocessing as mp
     workers = max(1, min(os.cpu_count() or 1, 64))
     try:
         import psutil
-        workers = max(1, min(workers, int(psutil.virtual_memory().available / 1.2e9)))
+        workers = max(1, min(workers, int(psutil.virtual_memory().available / 3e9)))
     except Exception:
         pass
-    per_worker = max(1, min(args.steps, 6))
+    steps = max(1, min(args.steps, 2))
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers) as pool:
-        pool.map(_cpu_worker, [(i, 1) for i in range(workers)])     # warm-up frame
+        pool.map(_cpu_proved_worker, [(i, 1) for i in range(workers)])     # warm-up step
         t0 = time.perf_counter()
-        res = pool.map(_cpu_worker, [(i, per_worker) for i in range(workers)])
+        res = pool.map(_cpu_proved_worker, [(i, steps) for i in range(workers)])
         wall = time.perf_counter() - t0
-    kind = res[0][1]
-    frames = workers * per_worker
+    frames = workers * steps
     value = frames / wall
+    stages = {k: sum(r[1][k] for r in res) / len(res) for k in res[0][1]}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / per_worker,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Fp2)",
+        "steps": steps, "warmup": 1, "ms_per_step": 1e3 * wall / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Fp2 over 2^61-1)",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "frame": [H, Wd, 3],
-                   "copies": 16200, "wires": 1 << 23, "circuit": "gray.pws",
-                   "per_frame": "compute_beta + 14 early rounds + finish + MLE over 2^23 inputs "
-                                "(native_fp2.cpp) + Orion commit of the 2^23 inputs (commit(), "
-                                "expander_init in the same process)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": kind,
-                         "sample": f"{per_worker} timed frames per worker process x {workers} "
-                                   f"processes after one warm-up frame each"},
+        "config": {"workload": WORKLOAD, "frame": [H, Wd, 3], "copies": 16200, "wires": 1 << 23,
+                   "circuit": "gray.pws", "prover": "plain (-z 2)",
+                   "step": f"one proved frame per worker process x {workers} processes",
+                   "steps_requested": args.steps, "warmup_requested": args.warmup},
+        "stage_seconds_per_frame": stages,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "reference",
+                         "sample": f"{steps} timed proved frames per process x {workers} processes after one "
+                                   f"warm-up frame each; " + REFERENCE_SAMPLE},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
     }
@@ -513,6 +494,26 @@ def ours_arm(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    extras = rank == 0 and world == 1
+    # ---- the headline: pipelined proved frames (needs the most memory: runs first)
+    proved, proved_e2e, pctx = proved_bench(args, rank, world, local_rank)
+    check = plain_pf = zk_proved = None
+    if rank == 0:
+        check = proof_check(pctx)
+        if world == 1 and not args.no_plain:
+            plain_pf = plain_proved(pctx)
+    del pctx
+    torch.cuda.empty_cache()
+    if extras and not args.skip_zk:
+        # TruePix's default: the zero-knowledge prover with commit pairs and two openings per frame
+        zres, ze2e, zctx = proved_bench(args, rank, world, local_rank, zk=True, steps=max(2, min(args.steps, 6)),
+                                        warmup=2)
+        zk_proved = {"frames_per_s": zres["value"], "steps": zres["steps"], "frames_per_step": args.batch,
+                     "e2e_frames_per_s": ze2e["value"], "proof_check": proof_check(zctx, zk=True),
+                     "what": "the zero-knowledge prover (circuitnizkvec_vole_ZK.py) with the Orion_zk commit pair "
+                             "(masked polynomial and mask) and both openings per frame, same pipeline"}
+        del zctx
+        torch.cuda.empty_cache()
     layout = FrameLayout.for_frame(H, Wd)
     gt, i0, i1 = circuit()
     B = args.batch
@@ -689,10 +690,9 @@ def ours_arm(args, rank, world, local_rank):
         c, w, b, m = bprover.results(B - 1)
         res_ok = bool(c.any() and w.any() and m != (0, 0) and any(committer.root(B - 1)))
 
-    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = ref_gpu = fs_rounds = full = None
+    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = ref_gpu = fs_rounds = None
     # The side measurements run once, at N = 1 (a scaling run holds every GPU
     # while rank 0 works; it only needs the step's value).
-    extras = rank == 0 and world == 1
     if extras and not args.skip_ntt:
         ntt = ntt_bench(lib, dev, stream)
     if extras and not args.skip_opening:
@@ -706,111 +706,247 @@ def ours_arm(args, rank, world, local_rank):
         e2e_ref = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
         ref_gpu = reference_gpu_lib(frames[0], layout, gt, i0, i1, z1, z2, point, chal)
         fs_rounds = transcript_rounds(bprover, pix, z1s, z2s, pts, stream)
-    if extras and args.full_proof:
-        full = full_proof(pix, layout, gt, i0, i1, stream)
     if extras and not args.skip_serving:
         del bprover
         committer.rows = committer.trees = None
         torch.cuda.empty_cache()
         uneven, serving = serving_in_own_process(local_rank)
     if rank == 0 and world == 1 and not args.skip_cpu:
-        secs, kind = _cpu_worker((0, 1))
-        cpu = {"value": 1.0 / secs, "unit": UNIT, "cores": 1, "kind": kind,
-               "sample": "1 frame of the same workload (compute_beta + 14 early rounds + finish "
-                         "+ MLE over 2^23 inputs + Orion commit of the 2^23 inputs), library "
-                         "calls only, one process"}
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import reference_proof
+        if reference_proof.available():
+            cpu = {"unavailable": reference_proof.available()}
+        else:
+            import multiprocessing as mp
+            with mp.get_context("spawn").Pool(1, maxtasksperchild=1) as pool:
+                secs, stages = pool.apply(_cpu_proved_worker, ((0, 1),))
+            cpu = {"value": 1.0 / secs, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "1 proved frame of the same workload, one process; " + REFERENCE_SAMPLE,
+                   "stage_seconds": stages}
     if rank == 0:
+        core = {
+            "what": "the device part alone: batched GKR input layer (beta, 14 early rounds, finish, MLE) and the "
+                    "Orion commit of every frame from its resident bytes, challenges given, commits on %d side "
+                    "streams under the rounds" % len(committer.side),
+            "frames_per_s": value, "ms_per_step": ms / args.steps, "steps": args.steps, "frames_per_step": B,
+            "fp2_elem_per_s": folded / (ms / 1e3),
+            "breakdown": {
+                "serialised_step": "GKR part, then the commits, on one stream",
+                "gkr_ms_per_step": gkr_ms, "commit_ms_per_step": commit_ms,
+                "gkr_frames_per_s": B / (gkr_ms / 1e3) if gkr_ms else None,
+                "commit_frames_per_s": B / (commit_ms / 1e3) if commit_ms else None,
+                "plain_frames_per_s": plain_fps, "plain_gkr_frames_per_s": plain_gkr_fps,
+                "gkr_batched_over_plain": (B / (gkr_ms / 1e3) / plain_gkr_fps) if plain_gkr_fps and gkr_ms
+                else None},
+            "kernels": kernels_iso or kernels, "roofline_fold_kernel": roof_fold,
+            "kernels_timed_region": kernels,
+            "kernels_note": "kernels (and the line's roofline) come from one step with the commits serialised "
+                            "on the step's stream (CUDA events around every launch), whose shares match the "
+                            "serialised ncu launch list; the timed steps overlap them (kernels_timed_region)",
+            "e2e_from_pinned_frames": e2e, "outputs_nonzero": res_ok}
+        valid = bool(check and check["ok"])
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "metric": METRIC, "value": proved["value"], "unit": UNIT, "n_gpus": world,
+            "steps": proved["steps"], "warmup": args.warmup, "ms_per_step": proved["ms"] / proved["steps"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u64 (Fp2 over 2^61-1)", "data": "synthetic",
             "config": {"workload": WORKLOAD, "frame": [H, Wd, 3],
                        "copies": layout.copies, "padded_copies": layout.padded_copies,
-                       "wires": layout.padded_copies * layout.n_wires, "rounds": nb,
-                       "circuit": "gray.pws", "batch": B, "step": f"one batch of {B} frames",
-                       "path": "bytes -> batched rounds (tp_batch_*) -> Orion commits from bytes",
-                       "orion": {"columns": 128, "codeword_rows": cw_len, "tree_leaves": leaves},
-                       "l2": "inputs > L2: B distinct frames (0.4 GB), their folded tables "
-                             "(~4.8 GB) and codewords (14.8 GB) per step",
+                       "wires": layout.padded_copies * layout.n_wires, "early_rounds": nb, "late_rounds": 18,
+                       "circuit": "gray.pws", "prover": "plain (-z 2)", "batch": B,
+                       "step": f"one batch of {B} frames through the whole proof (truepix_b200.pipeline)",
+                       "orion": {"columns": 128, "codeword_rows": cw_len, "tree_leaves": leaves,
+                                 "queried_columns": 1222},
+                       "l2": "inputs > L2: B distinct frames (0.4 GB) and their codewords (14.8 GB) per step",
+                       "host_threads": os.cpu_count(),
                        "parallelism": f"replicas x{world}"},
+            "proof_check": check,
             "breakdown": {
-                "serialised_step": "GKR part, then the commits, on one stream (the timed steps "
-                                   "overlap them)",
-                "gkr_ms_per_step": gkr_ms, "commit_ms_per_step": commit_ms,
-                "gkr_frames_per_s": B / (gkr_ms / 1e3),
-                "commit_frames_per_s": B / (commit_ms / 1e3),
-                "plain_frames_per_s": plain_fps, "plain_gkr_frames_per_s": plain_gkr_fps,
-                "batched_over_plain": (value / world / plain_fps) if plain_fps else None,
-                "gkr_batched_over_plain": (B / (gkr_ms / 1e3) / plain_gkr_fps)
-                if plain_gkr_fps else None,
-                "plain": f"{n_plain} single-frame sessions (GKR, then GKR + commit) back to back"},
-            "fp2_elem_per_s": folded / (ms / 1e3),
-            "latency_ms_per_batch": {"p50": per_batch[len(per_batch) // 2],
-                                     "p99": per_batch[min(len(per_batch) - 1,
-                                                          int(0.99 * len(per_batch)))]},
-            "roofline": roof_iso or roof, "roofline_fold_kernel": roof_fold,
-            "kernels": kernels_iso or kernels,
-            "roofline_timed_region": roof, "kernels_timed_region": kernels,
-            "kernels_note": "the timed steps run the commits on %d side streams under the GKR "
-                            "rounds, so their per-kernel durations overlap (kernels_timed_region, "
-                            "roofline_timed_region); roofline and kernels come from one more step "
-                            "with the commits serialised on the step's stream (CUDA events around "
-                            "every launch), whose shares match the serialised ncu launch list"
-                            % len(committer.side),
-            "ntt": ntt, "opening": opening, "zk": zk, "batched_uneven": uneven, "serving": serving, "cpu_baseline": cpu, "e2e": e2e, "e2e_reference_abi": e2e_ref,
-            "reference_gpu_library": ref_gpu, "transcript_rounds": fs_rounds, "full_proof": full,
-            "gpu_launches": launches, "clocks": clk.summary(), "outputs_nonzero": res_ok,
+                "plain": plain_pf,
+                "batched_over_plain": (proved["value"] / world / plain_pf["frames_per_s"]) if plain_pf else None,
+                "latency_ms_per_batch": proved["latency_ms_per_batch"],
+                "bound": "host: the IO transcript hashes each frame's 64 MiB output vector with SHA-256, a "
+                         "sequential chain per frame, on the host cores"},
+            "e2e": proved_e2e,
+            "roofline": roof_iso or roof,
+            "roofline_note": "the dominant device kernel of the step (the commits' SHA-256 leaf chains), timed in "
+                             "the device-core measurement below",
+            "device_core": core,
+            "zk": zk_proved, "zk_device_core": zk,
+            "ntt": ntt, "opening": opening, "batched_uneven": uneven, "serving": serving,
+            "cpu_baseline": cpu, "e2e_reference_abi": e2e_ref,
+            "reference_gpu_library": ref_gpu, "transcript_rounds": fs_rounds,
+            "gpu_launches": proved["launches"], "clocks": proved["clocks"],
         }
+        if not valid:
+            line["invalid"] = "proof check failed: the timed proofs differ from the step-by-step path"
         print(json.dumps(line), flush=True)
 
 
-def full_proof(pix, layout, gt, i0, i1, stream, n_frames=16):
-    """The reference prover's whole proof of frames in TruePix's default mode, on
-    the device path (wall clock, synchronised): per frame the zero-knowledge
-    commit pair, the manifest from its roots, the zero-knowledge prover's proof
-    (truepix_b200.prover.prove_frames: circuit outputs, the IO transcript on host
-    threads, the VOLE-committed early rounds, late rounds and closing proofs) and
-    both Orion openings (truepix_b200.opening.opening_proof). The proof
-    containers' pickling (the reference's format) is left out of the timing."""
-    import time
-    import numpy as np
+def proved_inputs(rng, layout, B, zk=False):
+    """B seeded frames (pinned host tensors), VOLE correlations per frame"""
+    import torch
+    from truepix_b200.pipeline import correlations_needed
+    count = correlations_needed(layout, zk)
+    frames = [torch.from_numpy(rng.integers(0, 256, size=layout.copies * layout.copy_size, dtype=np.uint8))
+              .pin_memory() for _ in range(B)]
+    corr = [(rng.integers(0, P61, size=(count, 2), dtype=np.uint64),
+             rng.integers(0, P61, size=(count, 2), dtype=np.uint64)) for _ in range(B)]
+    return frames, corr
+
+
+def proved_bench(args, rank, world, local_rank, zk=False, steps=None, warmup=None):
+    """The headline: proved frames/s of the pipelined prover (truepix_b200.pipeline),
+    frames resident in HBM, then (`e2e`) from pinned host frames. CUDA events on
+    the pipeline's main stream; the end event is recorded once every proof of the
+    last step is assembled on the host. Max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from truepix_b200.frame import FrameLayout
+    from truepix_b200.pipeline import ProofPipeline
+    dev = torch.device("cuda", local_rank)
+    layout = FrameLayout.for_frame(H, Wd)
+    gt, i0, i1 = circuit()
+    B = args.batch
+    K = steps or args.steps
+    Wm = warmup or args.warmup
+    rng = np.random.default_rng(replica_seed(rank) + 100)
+    frames, corr = proved_inputs(rng, layout, B, zk)
+    frames_dev = [f.to(dev) for f in frames]
+    pipe = ProofPipeline(layout, gt, i0, i1, batch=B, device=local_rank, zk=zk, commit_streams=args.commit_streams)
+
+    def batches(k, resident, base):
+        for b in range(k):
+            yield dict(frames_host=frames, frames_dev=frames_dev if resident else None,
+                       pids=[base + b * B + f for f in range(B)], correlations=corr,
+                       mask_seeds=[base + b * B + f for f in range(B)] if zk else None)
+
+    out = {}
+    for mode in ("resident", "host"):
+        for _ in pipe.run(batches(Wm, mode == "resident", 1 << 20)):
+            pass
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        clk = ClockSampler(local_rank)
+        if mode == "resident":
+            clk.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        clk.t0 = time.time()
+        pipe.launches_last = 0
+        e0.record(pipe.stream)
+        last = None
+        marks = []
+        t0 = time.perf_counter()
+        for proofs in pipe.run(batches(K, mode == "resident", 0)):
+            last = proofs
+            marks.append(time.perf_counter() - t0)
+        e1.record(pipe.stream)
+        torch.cuda.synchronize(dev)
+        clk.t1 = time.time()
+        launches = pipe.launches_last
+        if mode == "resident":
+            clk.stop()
+        if world > 1:
+            dist.barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
+        value = job_throughput(K * B, ms, world)
+        gaps = sorted(b - a for a, b in zip([0.0] + marks[:-1], marks))
+        res = {"value": value, "ms": ms, "launches": launches, "steps": K,
+               "latency_ms_per_batch": {"p50": 1e3 * gaps[len(gaps) // 2],
+                                        "p99": 1e3 * gaps[min(len(gaps) - 1, int(0.99 * len(gaps)))]}}
+        if mode == "resident":
+            res["clocks"] = clk.summary()
+            res["last"] = last
+        out[mode] = res
+    frame_bytes = layout.copies * layout.copy_size
+    cw, qc, lv = pipe.cw_len, pipe.qc, pipe.leaves
+    # host -> device per step: frames (e2e only), z2, transcript and VOLE states, correlations, the opening's
+    # r0 / r1 / queried indices / node lists; device -> host: roots, the GKR proof values and final states,
+    # per opened polynomial the combined codeword, its root, the answer, the queried columns and the nodes
+    n_poly = 2 if zk else 1
+    small_h2d = B * (16 * layout.n_copy_bits + 120 + 160 + 2 * 16 * pipe.count)
+    open_h2d = B * n_poly * (16 * 128 + 16 * (pipe.N // 128) + 8 * qc + 4 * qc * 17)
+    d2h = B * (32 * n_poly + 16 * (5 * layout.n_copy_bits + 8 * layout.n_in_bits + 20 + layout.n_in_bits +
+                                   layout.n_copy_bits + 1) + 120 + 160) + \
+        B * n_poly * (16 * cw + 32 + 16 + 16 * 128 * qc + 2 * 32 * qc * 17)
+    res_e2e = {"value": out["host"]["value"], "unit": UNIT, "h2d_bytes_per_step": B * frame_bytes + small_h2d + open_h2d,
+               "d2h_bytes_per_step": d2h, "steps": K, "frames_per_step": B,
+               "timer": "CUDA events on the main stream, the end event after the last proofs are assembled",
+               "path": "pinned host frames uploaded on a copy stream inside the timed region; every proof "
+                       "(GKR proof values, opening file bytes) assembled in host memory"}
+    pipe.close()
+    last = out["resident"].pop("last")
+    del pipe, frames_dev
+    torch.cuda.empty_cache()
+    return out["resident"], res_e2e, (frames, corr, last, layout, gt, i0, i1)
+
+
+def proof_check(ctx, zk=False):
+    """One frame of the timed run against the step-by-step path (commit,
+    prove_frames, opening_proof; pinned to the reference prover's proofs and to
+    the reference program's opening files by the GPU tests)."""
     import torch
     from truepix_b200.opening import opening_proof
     from truepix_b200.orion import FrameCommitter
     from truepix_b200.prover import manifests_of, prove_frames
-    frames = pix[:n_frames]
-    B = len(frames)
-    rng = np.random.default_rng(5)
-    count = 4 * layout.n_copy_bits + 6 * 9 + 9 + 2 + 3 + 8
-    corr = [(rng.integers(0, (1 << 61) - 1, size=(count, 2), dtype=np.uint64),
-             rng.integers(0, (1 << 61) - 1, size=(count, 2), dtype=np.uint64)) for _ in range(B)]
-    fc = FrameCommitter([layout] * B, stream=stream, zk=True)
-    seeds = [0x5EED + f for f in range(B)]
-    out = {}
-    for rep in range(2):     # the first pass warms up (allocations, graphs, caches)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        fc.commit(frames, mask_seeds=seeds)
-        stream.synchronize()
-        t1 = time.perf_counter()
-        tr = prove_frames(frames, layout, gt, i0, i1, [1000 + f for f in range(B)], corr, manifests_of(fc),
-                          stream=stream, zk=True)
-        t2 = time.perf_counter()
-        sizes = 0
-        for f in range(B):
-            pt = [(int(x.real), int(x.imag)) for x in tr[f].final_input_point]
-            sizes += len(opening_proof(fc, f, pt, "masked", stream=stream))
-            sizes += len(opening_proof(fc, f, pt, "mask", stream=stream))
-        t3 = time.perf_counter()
-        out = {"frames": B, "frames_per_s": B / (t3 - t0), "commit_ms": (t1 - t0) * 1e3,
-               "prove_ms": (t2 - t1) * 1e3, "open_ms": (t3 - t2) * 1e3, "opening_bytes_per_frame": sizes / B,
-               "note": "wall clock per batch: ZK commit pairs, the whole GKR input-layer proof of the zero-"
-                       "knowledge prover (IO transcript on host threads, everything after it on the device), "
-                       "both Orion openings; proof containers not pickled"}
+    frames, corr, last, layout, gt, i0, i1 = ctx
+    f = len(last) - 1
+    p = last[f]
+    pix = frames[f].cuda()
+    fc = FrameCommitter([layout], zk=zk)
+    fc.commit([pix], mask_seeds=[p.pid] if zk else None)
+    torch.cuda.synchronize()
+    [m] = manifests_of(fc)
+    [t] = prove_frames([pix], layout, gt, i0, i1, [p.pid], [corr[f]], [m], zk=zk)
+    pt = [(int(x[0]), int(x[1])) if not hasattr(x, "real") else (int(x.real), int(x.imag))
+          for x in t.final_input_point]
+    ok = p.manifest == m and p.proof_bytes() == t.proof_bytes()
+    if zk:
+        ok = ok and p.opening["masked"] == opening_proof(fc, 0, pt, "masked") and \
+            p.opening["mask"] == opening_proof(fc, 0, pt, "mask")
+    else:
+        ok = ok and p.opening == opening_proof(fc, 0, pt)
     del fc
     torch.cuda.empty_cache()
-    return out
+    return {"ok": bool(ok), "frame": "the last frame of the last timed step",
+            "against": "truepix_b200.prover.prove_frames + truepix_b200.opening.opening_proof on the same frame, "
+                       "pid and correlations (the step-by-step path the GPU tests pin to the reference)",
+            "proof_bytes": len(p.proof_bytes()),
+            "opening_bytes": sum(map(len, p.opening.values())) if zk else len(p.opening)}
+
+
+def plain_proved(ctx, n=6):
+    """The single-instance prover: one frame at a time, every stage synchronous
+    (commit, IO transcript, GKR rounds and closing proofs, opening) on the same
+    device code, no batching and no overlap. Wall clock."""
+    import torch
+    from truepix_b200.opening import opening_proof
+    from truepix_b200.orion import FrameCommitter
+    from truepix_b200.prover import manifests_of, prove_frames
+    frames, corr, _, layout, gt, i0, i1 = ctx
+    fc = FrameCommitter([layout])
+
+    def one(f):
+        pix = frames[f % len(frames)].cuda()
+        fc.commit([pix])
+        torch.cuda.synchronize()
+        [t] = prove_frames([pix], layout, gt, i0, i1, [f], [corr[f % len(corr)]], manifests_of(fc), zk=False)
+        pt = [(int(x[0]), int(x[1])) if not hasattr(x, "real") else (int(x.real), int(x.imag))
+              for x in t.final_input_point]
+        opening_proof(fc, 0, pt)
+
+    one(0)
+    t0 = time.perf_counter()
+    for f in range(n):
+        one(f)
+    secs = (time.perf_counter() - t0) / n
+    del fc
+    torch.cuda.empty_cache()
+    return {"frames_per_s": 1.0 / secs, "ms_per_frame": 1e3 * secs, "frames": n,
+            "what": "one frame at a time through the same device code, each stage synchronous: commit "
+                    "(FrameCommitter), prove_frames (IO transcript, VOLE rounds, closing proofs), opening_proof"}
 
 
 def zk_step(args, bprover, pix, z1s, z2s, pts, chal_b, layout, stream, local_rank):
@@ -1452,9 +1588,6 @@ def main():
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--skip-zk", action="store_true")
     ap.add_argument("--skip-opening", action="store_true")
-    ap.add_argument("--full-proof", action="store_true",
-                    help="also time the whole proof of frames in TruePix's default mode (commit pairs, "
-                         "proof, openings)")
     ap.add_argument("--leaf-chunks", type=int, default=1,
                     help="launches the commits' SHA-256 leaf chains are split into (tp_orion_set_leaf_chunks)")
     ap.add_argument("--commit-streams", type=int, default=8,
