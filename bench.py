@@ -275,6 +275,42 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def leaf_int_profile():
+    """ALU-pipe instructions per launch of the commits' SHA-256 leaf kernel and the
+    pipe's hardware peak per SM per cycle, from the committed ncu summary
+    (profiles/leaf_kernel_alu_1080p.json: one 1080p launch)"""
+    p = os.path.join(ROOT, "profiles", "leaf_kernel_alu_1080p.json")
+    try:
+        return json.load(open(p))["leaf_kernel"]
+    except (OSError, ValueError, KeyError):
+        return None
+
+
+def int_alu_roof(ms_per_launch, rows_per_launch, sm_mhz, n_sm):
+    """the leaf kernel against the integer ALU pipe: ALU warp instructions per
+    launch (ncu, scaled by codeword rows) over the live launch duration, against
+    the pipe's peak x SMs x the sampled SM clock"""
+    prof = leaf_int_profile()
+    if not prof or not ms_per_launch or not sm_mhz:
+        return None
+    inst = prof["alu_warp_inst"] * rows_per_launch / prof["codeword_rows"]
+    achieved = inst / (ms_per_launch / 1e3) / 1e9
+    peak = prof["alu_peak_warp_inst_per_cycle_per_sm"] * n_sm * sm_mhz * 1e6 / 1e9
+    return {"kernel": "leaf_kernel", "bound": "int_alu", "unit": "G ALU warp instructions/s",
+            "achieved": achieved, "peak": peak, "frac": achieved / peak,
+            "peak_source": "ALU pipe peak_sustained = %d warp instructions per cycle per SM (ncu) x %d SMs x %d MHz "
+                           "(SM clock sampled during the run)" % (prof["alu_peak_warp_inst_per_cycle_per_sm"], n_sm,
+                                                                  sm_mhz),
+            "work_per_launch": {"alu_warp_inst": inst, "compressions": 128 * rows_per_launch,
+                                "alu_inst_per_compression": 32 * prof["alu_warp_inst"] / prof["compressions"]},
+            "avg_launch_us": 1e3 * ms_per_launch,
+            "fmaheavy": {"achieved": prof["fmaheavy_warp_inst"] * rows_per_launch / prof["codeword_rows"] /
+                         (ms_per_launch / 1e3) / 1e9,
+                         "peak": prof["fmaheavy_peak_warp_inst_per_cycle_per_sm"] * n_sm * sm_mhz * 1e6 / 1e9},
+            "traffic": prof["dram_bytes"] * rows_per_launch / prof["codeword_rows"],
+            "profile": "profiles/leaf_kernel_int_pipes_1080p.md"}
+
+
 def profiled_traffic():
     """DRAM bytes (read + write) per launch of each round kernel of the 64-frame
     1080p step, from the committed ncu summary (profiles/gkr_batch_1080p_traffic.json;
@@ -636,8 +672,23 @@ def ours_arm(args, rank, world, local_rank):
             out.append(k)
         return out
 
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    core_mhz = clk.summary()["sm_mhz"] or 1965     # sampled during the timed steps (else the B200's max clock)
+
     def roof_of(k, grp):
         g = grp[k["kernel"]]
+        if k["kernel"] == "leaf_kernel":
+            # integer-ALU bound: the hardware ALU pipe is the roof (the HBM and the register-only
+            # figures stay beside it)
+            # a launch hashes every row over 1 / leaf_chunks of the column pairs
+            r = int_alu_roof(g["ms"] / g["launches"], cw_len / args.leaf_chunks, core_mhz, n_sm)
+            if r is not None:
+                r["hbm"] = {"achieved_gbs": k["achieved_gbs"], "peak_gbs": peak,
+                            "frac": k["achieved_gbs"] / peak if k["achieved_gbs"] else None}
+                if k.get("g_compressions_per_s"):
+                    r["sha256_register_only"] = {"achieved_g_compressions_per_s": k["g_compressions_per_s"],
+                                                 "same_code_register_only": sha_gcs}
+                return r
         r = {"kernel": k["kernel"], "bound": "hbm", "achieved": k["achieved_gbs"], "peak": peak,
              "unit": "GB/s",
              "frac": k["achieved_gbs"] / peak if k["achieved_gbs"] else None,
@@ -1543,11 +1594,26 @@ def serving_sweep(rates=(100, 250, 500, 1000), n_req=192, seed=5):
 def profile_case(name):
     """A short fixed workload for `ncu` captures (no timing, no JSON line):
     orion = one 1080p Orion commit from bytes, one RS commit of 2^20 elements and
-    one 2^24-point forward NTT, through include/orion_gpu.h."""
+    one 2^24-point forward NTT, through include/orion_gpu.h; proved = two batches of
+    16 1080p frames through the pipelined whole proof."""
     import torch
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from orionlib import elements
     from truepix_b200.frame import FrameLayout
+    if name == "proved":
+        # two batches of 16 1080p frames through the pipelined whole proof (truepix_b200.pipeline)
+        from truepix_b200.frame import FrameLayout
+        from truepix_b200.pipeline import ProofPipeline
+        L = FrameLayout.for_frame(H, Wd)
+        gt, i0, i1 = circuit()
+        frames, corr = proved_inputs(np.random.default_rng(SEED), L, 16)
+        pipe = ProofPipeline(L, gt, i0, i1, batch=16)
+        batch = dict(frames_host=frames, pids=list(range(16)), correlations=corr)
+        for _ in pipe.run([batch, batch]):
+            pass
+        pipe.close()
+        torch.cuda.synchronize()
+        return
     assert name == "orion", name
     lib = native.gkr()
     dev = torch.device("cuda", 0)
@@ -1592,7 +1658,7 @@ def main():
                     help="launches the commits' SHA-256 leaf chains are split into (tp_orion_set_leaf_chunks)")
     ap.add_argument("--commit-streams", type=int, default=8,
                     help="streams the step's commits are spread over (0: the step's stream)")
-    ap.add_argument("--profile-case", choices=["orion"], help="run a fixed short workload for ncu and exit")
+    ap.add_argument("--profile-case", choices=["orion", "proved"], help="run a fixed short workload for ncu and exit")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)
