@@ -614,10 +614,13 @@ def ours_arm(args, rank, world, local_rank):
     # ---- compute roof of the SHA-256 leaf kernels
     sha_gcs = sha_peak(lib, dev, stream)
 
-    # ---- batched: the timed region
+    # ---- batched: the timed region (the first warm-up step measures the round launches' splits)
+    from truepix_b200.frame import autotune_rounds, round_tuning
     with torch.cuda.stream(stream):
         for i in range(args.warmup):
+            autotune_rounds(i == 0)
             run_batch()
+    autotune_rounds(False)
     torch.cuda.synchronize()
     per_step_pairs = nb * 2 + 24 * B + 16
     npairs = args.steps * per_step_pairs
@@ -794,7 +797,11 @@ def ours_arm(args, rank, world, local_rank):
             "kernels_note": "kernels (and the line's roofline) come from one step with the commits serialised "
                             "on the step's stream (CUDA events around every launch), whose shares match the "
                             "serialised ncu launch list; the timed steps overlap them (kernels_timed_region)",
-            "e2e_from_pinned_frames": e2e, "outputs_nonzero": res_ok}
+            "e2e_from_pinned_frames": e2e, "outputs_nonzero": res_ok,
+            "round_tuning": [{"kind": k, "bucket": b, "ctas_per_sm": m} for k, b, m in round_tuning()],
+            "round_tuning_note": "the round autotuner's measured CTA split per (kind: 0 table claim, 1 table fold + "
+                                 "claim, 2 byte claim, 3 byte fold + claim; bucket: log2 of pairs x rows), "
+                                 "measured in the first warm-up step (tp_batch_autotune)"}
         valid = bool(check and check["ok"])
         line = {
             "metric": METRIC, "value": proved["value"], "unit": UNIT, "n_gpus": world,

@@ -192,6 +192,33 @@ int tp_batch_n_copies(void* batch, int i);
 /* d_wires: frame i at d_wires + 16 * (sum of n_wires of frames < i) bytes -- with equal
  * n_wires simply [n_frames][n_wires] packed Fp2; d_beta: [n_frames] packed Fp2 */
 int tp_batch_finish(void* batch, void* d_wires, void* d_beta);
+/* Every early round of the batch on device transcripts, as one CUDA graph
+ * (north_star's graph-captured round launches; no counterpart in the reference,
+ * whose session returns to the host every round, native_fp2.cu:676-812): per
+ * round k the claims of all frames (d_claims + 64 B k bytes, 8 u64 per frame),
+ * tp_vole_round_dev's VOLE-committed round on the frames' transcripts and VOLE
+ * states (label "sc-<layer>-<k>", challenges d_challenges + 16 B k bytes, proof
+ * elements d_proof + 80 B k bytes or NULL), the fold by the drawn challenge;
+ * then tp_batch_finish into d_wires / d_beta. All frames need the same number of
+ * rounds; the batch's stream must be a stream of the caller's (capture). The
+ * rounds' jobs are planned on the host and uploaded in one copy; the graph is
+ * captured on the first call and replayed while the shape and the buffers stay
+ * the same (tp_batch_graph_replays counts the launches of a graph). */
+int tp_batch_vole_rounds_graph(void* batch, void* d_claims, void* d_fs_states, void* d_vole_states, const void* d_u,
+                               const void* d_v, long long count, int layer, void* d_challenges, void* d_proof,
+                               void* d_wires, void* d_beta);
+int tp_batch_graph_replays(void* batch);
+/* Autotuner of the round launches (no counterpart in the reference): with it on,
+ * the first immediate claim launch of each (round kind, work bucket) is timed
+ * under several splits of its CTAs over the frames' pair tiles and row groups
+ * (2 to 16 CTAs per SM) and the fastest is kept for this device; launches of a
+ * bucket not yet measured use 4 per SM. tp_batch_tune_table lists the measured
+ * entries (returns their count), tp_batch_tune_set installs one (e.g. from a
+ * saved table). Kinds: 0 table claim, 1 table fold + claim, 2 byte claim, 3 byte
+ * fold + claim; bucket = floor(log2 of the launch's pairs x rows). */
+int tp_batch_autotune(int on);
+int tp_batch_tune_table(int* kind, int* bucket, int* ctas_per_sm, int max);
+int tp_batch_tune_set(int kind, int bucket, int ctas_per_sm);
 /* Serving: frames join and leave a running batch between rounds. Finish frame i
  * alone (its n_wires wires into d_wires, its beta into d_beta; NULL = the frame's
  * staging buffer), then free its slot for tp_batch_set_* of a new frame while the

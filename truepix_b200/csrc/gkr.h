@@ -86,6 +86,19 @@ struct Batch {
     void* d_patch = nullptr;   // (job, device challenge) pairs patched into the job array
     size_t cap_patch = 0;
     int launches = 0;
+    // the graph path (batch_vole_rounds_graph): every round's jobs in one device
+    // table, uploaded from a pinned stage, and the captured graph of the rounds
+    Job* d_table = nullptr;
+    size_t cap_table = 0;
+    void* d_ptable = nullptr;
+    size_t cap_ptable = 0;
+    void* h_stage = nullptr;
+    size_t cap_stage = 0;
+    cudaEvent_t staged = nullptr;     // the last upload from h_stage has completed
+    cudaGraphExec_t graph = nullptr;
+    std::vector<long long> graph_key;
+    int graph_kernels = 0;
+    int graph_replays = 0;
 };
 
 Batch* batch_create(int n_frames, cudaStream_t s);
@@ -105,6 +118,21 @@ bool batch_fold_dev(Batch* B, int i, const fp2* d_r);
 // wires / beta of every frame into d_wires[i] (n_wires packed) / d_beta[i] (1 packed);
 // nullptr destinations use the frame's own staging buffer
 bool batch_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta);
+// Every early round of a batch on device transcripts, as one CUDA graph: per
+// round the claims (d_claims + 8 B k u64), the VOLE-committed round
+// (tp_vole_round_dev: challenge d_chal + B k, proof d_proof + 5 B k, labels
+// "sc-<layer>-<k>"), the fold by the drawn challenge; then the finish. All
+// frames must have the same number of rounds. The jobs of all rounds are planned
+// on the host and uploaded in one copy; the graph is captured on the first call
+// of a shape and replayed while the shape and the buffers stay the same.
+bool batch_vole_rounds_graph(Batch* B, u64* d_claims, void* d_states, void* d_vole_states, const fp2* d_u,
+                             const fp2* d_v, long long count, int layer, fp2* d_chal, fp2* d_proof,
+                             fp2* const* d_wires, fp2* const* d_beta);
+// measure the claim / fold launch split per (round kind, work bucket) on the next
+// immediate rounds (autotuner on / off), and the table of measured splits
+void batch_tune_enable(bool on);
+int batch_tune_table(int* kind, int* bucket, int* ctas_per_sm, int max);
+bool batch_tune_set(int kind, int bucket, int ctas_per_sm);
 // one frame: its wires / beta (nullptr: the frame's staging buffer), then its slot
 // is free for a new frame (serving: frames join and leave between rounds)
 bool batch_finish_frame(Batch* B, int i, fp2* d_wires, fp2* d_beta);

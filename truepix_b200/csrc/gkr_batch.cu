@@ -702,6 +702,8 @@ void plan_job(Job& j, int target_ctas)
     j.vec = (j.kind >= 2 && (j.cs & 15) == 0 && (reinterpret_cast<size_t>(j.pix) & 15) == 0) ? 1 : 0;
 }
 
+bool prepare_round_kernels() { return set_attrs(); }
+
 bool launch_round(const Job* d_jobs, const std::vector<Job>& jobs, int kind, cudaStream_t s,
                   int* launches)
 {

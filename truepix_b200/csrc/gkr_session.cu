@@ -12,7 +12,10 @@
 #include "runtime.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace tp {
 
@@ -281,12 +284,111 @@ bool batch_load_pixels(Batch* B, int i, const PixSrc& px, const fp2* d_beta)
     return true;
 }
 
-bool batch_claim(Batch* B, u64* const* d_claims)
+namespace {
+
+// ---- round planning ----------------------------------------------------------
+// A round launch is planned on the host from the frames' state (which it then
+// advances as the launch will), before anything is uploaded: the immediate path
+// uploads and launches it at once, the graph path plans every round of a proof
+// first and replays them from one device job table.
+
+// work of a launch, for the autotuner's size buckets
+int work_bucket(const std::vector<Job>& jobs, int kind)
+{
+    double total = 0;
+    for (const Job& j : jobs) total += (double)j.n_pairs * (kind < 2 ? j.W_rows : j.cs);
+    int b = 0;
+    while (b < 62 && (double)(1ull << (b + 1)) <= total) ++b;
+    return b;
+}
+
+// The claim/fold launch split: a round launch of one kind spreads `target` CTAs
+// over its jobs in proportion to their work (pair tiles x row groups,
+// plan_job). The autotuner measures the target, as CTAs per SM, per (kind, work
+// bucket) on the device and keeps the fastest; 4 per SM until it has.
+constexpr int kTuneMults[] = {2, 3, 4, 6, 8, 12, 16};
+
+// one planned launch: a round kind (0..3) or the finish (kind 4)
+struct RoundLaunch {
+    int kind = 0;
+    std::vector<Job> jobs;
+    std::vector<const fp2*> rdev;   // per job: the device challenge patched into it, or null
+    int bucket = 0;
+    int timer_tag = 0;
+    int max_w = 0;                  // finish: the widest frame
+};
+
+struct TuneKey {
+    int device, kind, bucket;
+    bool operator<(const TuneKey& o) const
+    {
+        return device != o.device ? device < o.device : kind != o.kind ? kind < o.kind : bucket < o.bucket;
+    }
+};
+std::map<TuneKey, int>& tune_table()
+{
+    static std::map<TuneKey, int> t;
+    return t;
+}
+std::mutex& tune_mutex()
+{
+    static std::mutex m;
+    return m;
+}
+bool g_tune_on = false;
+
+bool tune_known(int kind, int bucket)
+{
+    Ctx* c = ctx();
+    std::lock_guard<std::mutex> lk(tune_mutex());
+    return tune_table().count(TuneKey{c ? c->device : 0, kind, bucket}) != 0;
+}
+
+int tuned_mult(int kind, int bucket)
+{
+    Ctx* c = ctx();
+    std::lock_guard<std::mutex> lk(tune_mutex());
+    auto it = tune_table().find(TuneKey{c ? c->device : 0, kind, bucket});
+    return it == tune_table().end() ? 4 : it->second;
+}
+
+void plan_jobs(std::vector<Job>& jobs, int kind, int target)
+{
+    double total = 0;
+    for (const Job& j : jobs) total += (double)j.n_pairs * (kind < 2 ? j.W_rows : j.cs);
+    int cta = 0;
+    for (Job& j : jobs) {
+        const double w = (double)j.n_pairs * (kind < 2 ? j.W_rows : j.cs);
+        plan_job(j, std::max(1, (int)(target * w / total + 0.5)));
+        j.cta0 = cta;
+        cta += j.tiles * j.groups;
+    }
+}
+
+size_t launch_ctas(const std::vector<Job>& jobs)
+{
+    size_t n = 0;
+    for (const Job& j : jobs) n += (size_t)j.tiles * j.groups;
+    return n;
+}
+
+void set_workspace_ptrs(Batch* B, std::vector<Job>& jobs)
+{
+    for (size_t q = 0; q < jobs.size(); ++q) {
+        jobs[q].partials = B->partials + 4 * (size_t)jobs[q].cta0;
+        jobs[q].ticket = B->tickets + q;
+    }
+}
+
+// the claim launches of one round: per kind, its jobs and the device challenges
+// of their pending folds; advances the frames past the round's folds
+bool plan_claims(Batch* B, u64* const* d_claims, std::vector<RoundLaunch>& out)
 {
     Ctx* c = ctx();
     if (!c) return false;
-    std::vector<Job> by_kind[4];
+    RoundLaunch by_kind[4];
     std::vector<Frame*> fr[4];
+    for (int k = 0; k < 4; ++k) by_kind[k].kind = k;
     for (size_t i = 0; i < B->frames.size(); ++i) {
         Frame* f = B->frames[i];
         if (!f->configured) continue;
@@ -304,43 +406,23 @@ bool batch_claim(Batch* B, u64* const* d_claims)
         }
         j.n_pairs = f->n_copies / 2;
         j.out8 = (d_claims && d_claims[i]) ? d_claims[i] : f->out8;
-        by_kind[j.kind].push_back(j);
+        by_kind[j.kind].jobs.push_back(j);
+        by_kind[j.kind].rdev.push_back(f->pending ? f->r_dev : nullptr);
         fr[j.kind].push_back(f);
     }
-    if (B->frames.size() == 1 && by_kind[0].empty() && by_kind[1].empty() && by_kind[2].empty() &&
-        by_kind[3].empty()) {
+    if (B->frames.size() == 1 && by_kind[0].jobs.empty() && by_kind[1].jobs.empty() && by_kind[2].jobs.empty() &&
+        by_kind[3].jobs.empty()) {
         set_error(TP_ERR_ARG, "claim needs at least 2 copies (have %d)", B->frames[0]->n_copies);
         return false;
     }
-    const int target = 4 * c->n_sm;
     for (int k = 0; k < 4; ++k) {
-        std::vector<Job>& jobs = by_kind[k];
-        if (jobs.empty()) continue;
-        double total = 0;
-        for (const Job& j : jobs) total += (double)j.n_pairs * (k < 2 ? j.W_rows : j.cs);
-        int cta = 0;
-        for (size_t q = 0; q < jobs.size(); ++q) {
-            Job& j = jobs[q];
-            const double w = (double)j.n_pairs * (k < 2 ? j.W_rows : j.cs);
-            plan_job(j, std::max(1, (int)(target * w / total + 0.5)));
-            j.cta0 = cta;
-            cta += j.tiles * j.groups;
-        }
-        if (!ensure_workspace(B, jobs.size(), (size_t)cta)) return false;
-        for (size_t q = 0; q < jobs.size(); ++q) {
-            jobs[q].partials = B->partials + 4 * (size_t)jobs[q].cta0;
-            jobs[q].ticket = B->tickets + q;
-        }
-        std::vector<const fp2*> rdev(jobs.size(), nullptr);
-        for (size_t q = 0; q < jobs.size(); ++q)
-            if (fr[k][q]->pending) rdev[q] = fr[k][q]->r_dev;
-        if (!upload_jobs(B, jobs.data(), jobs.size(), rdev)) return false;
+        RoundLaunch& L = by_kind[k];
+        if (L.jobs.empty()) continue;
+        L.bucket = work_bucket(L.jobs, k);
+        plan_jobs(L.jobs, k, tuned_mult(k, L.bucket) * c->n_sm);
         int lg = 0;
-        while ((1 << lg) < 2 * jobs[0].n_pairs) ++lg;
-        timer_begin(B->stream, 1000 * (k >> 1) + 100 * (k & 1) + lg);
-        const bool ok = launch_round(B->d_jobs, jobs, k, B->stream, &B->launches);
-        timer_end(B->stream);
-        if (!ok) return false;
+        while ((1 << lg) < 2 * L.jobs[0].n_pairs) ++lg;
+        L.timer_tag = 1000 * (k >> 1) + 100 * (k & 1) + lg;
         for (Frame* f : fr[k]) {
             if (f->pending) {
                 f->cur = f->pix_cur ? 1 : (f->cur ^ 1);
@@ -350,7 +432,81 @@ bool batch_claim(Batch* B, u64* const* d_claims)
                 f->r_dev = nullptr;
             }
         }
+        out.push_back(std::move(L));
     }
+    return true;
+}
+
+// time one round launch under each candidate split, keep the fastest for its
+// (kind, bucket); the launches rerun the same jobs (a claim or fold + claim
+// reads its source and rewrites the same outputs)
+bool tune_launch(Batch* B, RoundLaunch& L)
+{
+    Ctx* c = ctx();
+    cudaStream_t s = B->stream;
+    float best_ms = 0;
+    int best = 4;
+    cudaEvent_t e0, e1;
+    TP_CUDA_OK(cudaEventCreate(&e0), "tune event");
+    TP_CUDA_OK(cudaEventCreate(&e1), "tune event");
+    bool ok = true;
+    for (int mult : kTuneMults) {
+        std::vector<Job> jobs = L.jobs;
+        plan_jobs(jobs, L.kind, mult * c->n_sm);
+        if (!ensure_workspace(B, jobs.size(), launch_ctas(jobs))) {
+            ok = false;
+            break;
+        }
+        set_workspace_ptrs(B, jobs);
+        if (!upload_jobs(B, jobs.data(), jobs.size(), L.rdev)) {
+            ok = false;
+            break;
+        }
+        int dummy = 0;
+        ok = launch_round(B->d_jobs, jobs, L.kind, s, &dummy);   // warm
+        ok = ok && !cuda_failed(cudaEventRecord(e0, s), "tune event");
+        for (int rep = 0; ok && rep < 3; ++rep) ok = launch_round(B->d_jobs, jobs, L.kind, s, &dummy);
+        ok = ok && !cuda_failed(cudaEventRecord(e1, s), "tune event") &&
+             !cuda_failed(cudaEventSynchronize(e1), "tune sync");
+        if (!ok) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (best_ms == 0 || ms < best_ms) {
+            best_ms = ms;
+            best = mult;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!ok) return false;
+    {
+        std::lock_guard<std::mutex> lk(tune_mutex());
+        tune_table()[TuneKey{c->device, L.kind, L.bucket}] = best;
+    }
+    plan_jobs(L.jobs, L.kind, best * c->n_sm);
+    return true;
+}
+
+bool launch_planned(Batch* B, RoundLaunch& L)
+{
+    if (g_tune_on && !tune_known(L.kind, L.bucket) && !tune_launch(B, L)) return false;
+    if (!ensure_workspace(B, L.jobs.size(), launch_ctas(L.jobs))) return false;
+    set_workspace_ptrs(B, L.jobs);
+    if (!upload_jobs(B, L.jobs.data(), L.jobs.size(), L.rdev)) return false;
+    timer_begin(B->stream, L.timer_tag);
+    const bool ok = launch_round(B->d_jobs, L.jobs, L.kind, B->stream, &B->launches);
+    timer_end(B->stream);
+    return ok;
+}
+
+}  // namespace
+
+bool batch_claim(Batch* B, u64* const* d_claims)
+{
+    std::vector<RoundLaunch> plan;
+    if (!plan_claims(B, d_claims, plan)) return false;
+    for (RoundLaunch& L : plan)
+        if (!launch_planned(B, L)) return false;
     return true;
 }
 
@@ -404,11 +560,15 @@ bool batch_fold_dev(Batch* B, int i, const fp2* d_r)
     return true;
 }
 
-bool batch_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta)
+namespace {
+
+// the finish launch: wires and beta of every configured frame (a pending fold of
+// the last two copies applied by it); a pending fold of more copies is applied
+// first (host challenges only)
+bool plan_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta, RoundLaunch& L)
 {
-    std::vector<Job> jobs;
-    std::vector<const fp2*> rdev;
-    int max_w = 0;
+    L.kind = 4;
+    L.max_w = 0;
     for (size_t i = 0; i < B->frames.size(); ++i) {
         Frame* f = B->frames[i];
         if (!f->configured) continue;
@@ -422,13 +582,257 @@ bool batch_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta)
         j.kind = f->pending ? 1 : 0;  // a pending fold of the last two copies
         j.fin = (d_wires && d_wires[i]) ? d_wires[i] : f->fin;
         j.fin_beta = (d_beta && d_beta[i]) ? d_beta[i] : f->fin + f->n_wires;
-        max_w = std::max(max_w, f->n_wires);
-        jobs.push_back(j);
-        rdev.push_back(f->pending ? f->r_dev : nullptr);
+        L.max_w = std::max(L.max_w, f->n_wires);
+        L.jobs.push_back(j);
+        L.rdev.push_back(f->pending ? f->r_dev : nullptr);
     }
-    if (!ensure_workspace(B, jobs.size(), 1)) return false;
-    if (!upload_jobs(B, jobs.data(), jobs.size(), rdev)) return false;
-    return launch_finish(B->d_jobs, (int)jobs.size(), max_w, B->stream, &B->launches);
+    return true;
+}
+
+}  // namespace
+
+bool batch_finish(Batch* B, fp2* const* d_wires, fp2* const* d_beta)
+{
+    RoundLaunch L;
+    if (!plan_finish(B, d_wires, d_beta, L)) return false;
+    if (!ensure_workspace(B, L.jobs.size(), 1)) return false;
+    if (!upload_jobs(B, L.jobs.data(), L.jobs.size(), L.rdev)) return false;
+    return launch_finish(B->d_jobs, (int)L.jobs.size(), L.max_w, B->stream, &B->launches);
+}
+
+namespace {
+
+struct GraphOp {
+    int type = 0;          // 0 round launch, 1 VOLE round, 2 finish
+    RoundLaunch L;
+    size_t job_off = 0, patch_off = 0, n_patch = 0;
+    int round = 0;
+};
+
+template <class T>
+bool grow_dev(T*& p, size_t& cap, size_t n, cudaStream_t s)
+{
+    if (n <= cap) return true;
+    dev_free(p, s);
+    cap = std::max(n, cap * 2);
+    p = static_cast<T*>(dev_alloc(sizeof(T) * cap, s));
+    if (!p) cap = 0;
+    return p != nullptr;
+}
+
+}  // namespace
+
+bool batch_vole_rounds_graph(Batch* B, u64* d_claims, void* d_states, void* d_vole_states, const fp2* d_u,
+                             const fp2* d_v, long long count, int layer, fp2* d_chal, fp2* d_proof,
+                             fp2* const* d_wires, fp2* const* d_beta)
+{
+    Ctx* c = ctx();
+    if (!c) return false;
+    cudaStream_t s = B->stream;
+    if (!s) {
+        set_error(TP_ERR_ARG, "the graph path needs a stream of the caller's (the legacy stream cannot capture)");
+        return false;
+    }
+    const int nB = (int)B->frames.size();
+    int rounds = -1;
+    for (Frame* f : B->frames) {
+        if (!f->configured || f->n_copies < 2) {
+            set_error(TP_ERR_ARG, "every frame of the batch needs at least one round");
+            return false;
+        }
+        int r = 0;
+        while ((2 << r) <= f->n_copies) ++r;
+        if (rounds >= 0 && r != rounds) {
+            set_error(TP_ERR_ARG, "the graph path needs frames with the same number of rounds");
+            return false;
+        }
+        rounds = r;
+    }
+    // ---- plan every launch (advances the frames as the launches will)
+    std::vector<GraphOp> ops;
+    std::vector<u64*> claim_ptrs((size_t)nB);
+    for (int k = 0; k < rounds; ++k) {
+        for (int i = 0; i < nB; ++i) claim_ptrs[(size_t)i] = d_claims + 8 * ((size_t)nB * k + i);
+        std::vector<RoundLaunch> plan;
+        if (!plan_claims(B, claim_ptrs.data(), plan)) return false;
+        for (RoundLaunch& L : plan) {
+            GraphOp op;
+            op.type = 0;
+            op.L = std::move(L);
+            ops.push_back(std::move(op));
+        }
+        GraphOp v;
+        v.type = 1;
+        v.round = k;
+        ops.push_back(v);
+        for (int i = 0; i < nB; ++i)
+            if (!batch_fold_dev(B, i, d_chal + (size_t)nB * k + i)) return false;
+    }
+    {
+        GraphOp fin;
+        fin.type = 2;
+        if (!plan_finish(B, d_wires, d_beta, fin.L)) return false;
+        ops.push_back(std::move(fin));
+    }
+    // ---- workspace, one job table and one patch table
+    size_t max_jobs = 1, max_ctas = 1, n_jobs = 0, n_patch = 0;
+    for (GraphOp& op : ops) {
+        if (op.type == 1) continue;
+        max_jobs = std::max(max_jobs, op.L.jobs.size());
+        if (op.type == 0) max_ctas = std::max(max_ctas, launch_ctas(op.L.jobs));
+    }
+    if (!ensure_workspace(B, max_jobs, max_ctas)) return false;
+    for (GraphOp& op : ops) {
+        if (op.type == 1) continue;
+        if (op.type == 0) set_workspace_ptrs(B, op.L.jobs);
+        op.job_off = n_jobs;
+        op.patch_off = n_patch;
+        for (const fp2* r : op.L.rdev) op.n_patch += r ? 1 : 0;
+        n_jobs += op.L.jobs.size();
+        n_patch += op.n_patch;
+    }
+    struct Patch {
+        const fp2* r;
+        long long job;
+    };
+    static_assert(sizeof(Patch) == 16, "patch layout (patch_r_kernel's RPatch)");
+    const size_t bytes_jobs = sizeof(Job) * n_jobs, bytes_patch = sizeof(Patch) * std::max<size_t>(1, n_patch);
+    if (!grow_dev(B->d_table, B->cap_table, n_jobs, s)) return false;
+    {
+        unsigned char* pt = static_cast<unsigned char*>(B->d_ptable);
+        size_t cap = B->cap_ptable;
+        if (!grow_dev(pt, cap, bytes_patch, s)) return false;
+        B->d_ptable = pt;
+        B->cap_ptable = cap;
+    }
+    if (!B->staged) TP_CUDA_OK(cudaEventCreateWithFlags(&B->staged, cudaEventDisableTiming), "stage event");
+    TP_CUDA_OK(cudaEventSynchronize(B->staged), "stage reuse");   // the previous upload has read the stage
+    if (bytes_jobs + bytes_patch > B->cap_stage) {
+        if (B->h_stage) cudaFreeHost(B->h_stage);
+        B->cap_stage = std::max(bytes_jobs + bytes_patch, 2 * B->cap_stage);
+        if (cuda_failed(cudaMallocHost(&B->h_stage, B->cap_stage), "pinned stage")) {
+            B->h_stage = nullptr;
+            B->cap_stage = 0;
+            return false;
+        }
+    }
+    Job* hj = static_cast<Job*>(B->h_stage);
+    Patch* hp = reinterpret_cast<Patch*>(static_cast<unsigned char*>(B->h_stage) + bytes_jobs);
+    for (const GraphOp& op : ops) {
+        if (op.type == 1) continue;
+        std::memcpy(hj + op.job_off, op.L.jobs.data(), sizeof(Job) * op.L.jobs.size());
+        size_t q = op.patch_off;
+        for (size_t j = 0; j < op.L.rdev.size(); ++j)
+            if (op.L.rdev[j]) hp[q++] = Patch{op.L.rdev[j], (long long)(op.job_off + j)};
+    }
+    TP_CUDA_OK(cudaMemcpyAsync(B->d_table, hj, bytes_jobs, cudaMemcpyHostToDevice, s), "job table");
+    if (n_patch)
+        TP_CUDA_OK(cudaMemcpyAsync(B->d_ptable, hp, sizeof(Patch) * n_patch, cudaMemcpyHostToDevice, s),
+                   "patch table");
+    TP_CUDA_OK(cudaEventRecord(B->staged, s), "stage event");
+    // ---- the graph: captured once per shape, replayed after
+    std::vector<long long> key = {(long long)(size_t)s, (long long)(size_t)B->d_table, (long long)(size_t)B->d_ptable,
+                                  (long long)(size_t)d_states, (long long)(size_t)d_vole_states,
+                                  (long long)(size_t)d_u, (long long)(size_t)d_v, count, layer,
+                                  (long long)(size_t)d_chal, (long long)(size_t)d_proof, (long long)nB};
+    int kernels = 0;
+    for (const GraphOp& op : ops) {
+        key.push_back(op.type);
+        key.push_back(op.L.kind);
+        key.push_back((long long)op.job_off);
+        key.push_back((long long)op.L.jobs.size());
+        key.push_back((long long)op.patch_off);
+        key.push_back((long long)op.n_patch);
+        key.push_back(op.L.max_w);
+        for (const Job& j : op.L.jobs) {
+            key.push_back(j.tiles);
+            key.push_back(j.groups);
+            key.push_back(j.wpg);
+            key.push_back(j.pw);
+        }
+        kernels += (op.type == 1) ? 1 : 1 + (op.n_patch ? 1 : 0);
+    }
+    if (!B->graph || key != B->graph_key) {
+        if (B->graph) {
+            cudaGraphExecDestroy(B->graph);
+            B->graph = nullptr;
+        }
+        if (!prepare_round_kernels()) return false;
+        TP_CUDA_OK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+        bool ok = true;
+        int dummy = 0;
+        for (const GraphOp& op : ops) {
+            if (!ok) break;
+            if (op.type == 1) {
+                char label[40];
+                std::snprintf(label, sizeof(label), "sc-%d-%d", layer, op.round);
+                ok = launch_vole_round_batch(d_states, d_vole_states, nB, d_claims + 8 * (size_t)nB * op.round,
+                                             d_u, d_v, count, label, d_chal + (size_t)nB * op.round,
+                                             d_proof ? d_proof + 5 * (size_t)nB * op.round : nullptr, s);
+                continue;
+            }
+            if (op.n_patch) {
+                patch_r_kernel<<<(unsigned)((op.n_patch + 127) / 128), 128, 0, s>>>(
+                    B->d_table, static_cast<const RPatch*>(B->d_ptable) + op.patch_off, (int)op.n_patch);
+                ok = !cuda_failed(cudaGetLastError(), "challenge patch");
+            }
+            if (!ok) break;
+            if (op.type == 0)
+                ok = launch_round(B->d_table + op.job_off, op.L.jobs, op.L.kind, s, &dummy);
+            else
+                ok = launch_finish(B->d_table + op.job_off, (int)op.L.jobs.size(), op.L.max_w, s, &dummy);
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (!ok || cuda_failed(e, "end capture")) {
+            if (g) cudaGraphDestroy(g);
+            return false;
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&B->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (cuda_failed(ie, "graph instantiate")) {
+            B->graph = nullptr;
+            return false;
+        }
+        B->graph_key = key;
+        B->graph_kernels = kernels;
+    }
+    TP_CUDA_OK(cudaGraphLaunch(B->graph, s), "graph launch");
+    B->launches += B->graph_kernels;
+    ++B->graph_replays;
+    return true;
+}
+
+void batch_tune_enable(bool on) { g_tune_on = on; }
+
+int batch_tune_table(int* kind, int* bucket, int* ctas_per_sm, int max)
+{
+    Ctx* c = ctx();
+    std::lock_guard<std::mutex> lk(tune_mutex());
+    int n = 0;
+    for (const auto& kv : tune_table()) {
+        if (c && kv.first.device != c->device) continue;
+        if (n < max) {
+            kind[n] = kv.first.kind;
+            bucket[n] = kv.first.bucket;
+            ctas_per_sm[n] = kv.second;
+        }
+        ++n;
+    }
+    return n;
+}
+
+bool batch_tune_set(int kind, int bucket, int ctas_per_sm)
+{
+    Ctx* c = ctx();
+    if (!c) return false;
+    if (kind < 0 || kind > 3 || bucket < 0 || bucket > 62 || ctas_per_sm < 1 || ctas_per_sm > 64) {
+        set_error(TP_ERR_ARG, "tune entry (%d, %d, %d) out of range", kind, bucket, ctas_per_sm);
+        return false;
+    }
+    std::lock_guard<std::mutex> lk(tune_mutex());
+    tune_table()[TuneKey{c->device, kind, bucket}] = ctas_per_sm;
+    return true;
 }
 
 bool batch_finish_frame(Batch* B, int i, fp2* d_wires, fp2* d_beta)
@@ -501,6 +905,14 @@ void batch_destroy(Batch* B)
     dev_free(B->partials, s);
     dev_free(B->tickets, s);
     dev_free(B->d_patch, s);
+    dev_free(B->d_table, s);
+    dev_free(B->d_ptable, s);
+    if (B->graph) cudaGraphExecDestroy(B->graph);
+    if (B->staged) {
+        cudaEventSynchronize(B->staged);
+        cudaEventDestroy(B->staged);
+    }
+    if (B->h_stage) cudaFreeHost(B->h_stage);
     delete B;
 }
 

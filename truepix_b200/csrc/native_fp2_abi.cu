@@ -571,6 +571,60 @@ int tp_batch_finish(void* batch, void* d_wires, void* d_beta)
     return tp::batch_finish(B, w.data(), b.data()) ? 0 : -1;
 }
 
+int tp_batch_vole_rounds_graph(void* batch, void* d_claims, void* d_fs_states, void* d_vole_states, const void* d_u,
+                               const void* d_v, long long count, int layer, void* d_challenges, void* d_proof,
+                               void* d_wires, void* d_beta)
+{
+    tp::clear_error();
+    if (!batch || !d_claims || !d_fs_states || !d_vole_states || !d_u || !d_v || count < 4 || !d_challenges ||
+        !d_wires || !d_beta) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_batch_vole_rounds_graph: bad arguments");
+        return -1;
+    }
+    tp::Batch* B = static_cast<tp::Batch*>(batch);
+    const size_t n = B->frames.size();
+    std::vector<fp2*> w(n, nullptr), b(n, nullptr);
+    for (size_t i = 0; i < n; ++i) {
+        w[i] = static_cast<fp2*>(d_wires) + i * (size_t)B->frames[i]->n_wires;
+        b[i] = static_cast<fp2*>(d_beta) + i;
+    }
+    return tp::batch_vole_rounds_graph(B, static_cast<u64*>(d_claims), d_fs_states, d_vole_states,
+                                       static_cast<const fp2*>(d_u), static_cast<const fp2*>(d_v), count, layer,
+                                       static_cast<fp2*>(d_challenges), static_cast<fp2*>(d_proof), w.data(),
+                                       b.data())
+               ? 0
+               : -1;
+}
+
+int tp_batch_graph_replays(void* batch)
+{
+    return batch ? static_cast<tp::Batch*>(batch)->graph_replays : 0;
+}
+
+int tp_batch_autotune(int on)
+{
+    tp::clear_error();
+    tp::batch_tune_enable(on != 0);
+    return 0;
+}
+
+int tp_batch_tune_table(int* kind, int* bucket, int* ctas_per_sm, int max)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (max > 0 && (!kind || !bucket || !ctas_per_sm)) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_batch_tune_table: null outputs");
+        return -1;
+    }
+    return tp::batch_tune_table(kind, bucket, ctas_per_sm, max);
+}
+
+int tp_batch_tune_set(int kind, int bucket, int ctas_per_sm)
+{
+    tp::clear_error();
+    return tp::batch_tune_set(kind, bucket, ctas_per_sm) ? 0 : -1;
+}
+
 int tp_batch_finish_frame(void* batch, int i, void* d_wires, void* d_beta)
 {
     tp::clear_error();

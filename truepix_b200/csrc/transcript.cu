@@ -9,6 +9,7 @@
 
 #include <vector>
 
+#include "gkr_internal.cuh"
 #include "runtime.h"
 #include "transcript.cuh"
 #include "vole.cuh"
@@ -335,6 +336,23 @@ bool state_ok(const void* state, const char* who)
 }
 
 }  // namespace
+
+namespace tp {
+
+bool launch_vole_round_batch(void* d_states, void* d_vole_states, int n, const void* d_claims, const void* d_u,
+                             const void* d_v, long long count, const char* label, void* d_chal, void* d_proof,
+                             cudaStream_t s)
+{
+    fs::Label L;
+    if (!make_device_label(label, &L, "vole round")) return false;
+    vole_round_kernel<<<(n + 127) / 128, 128, 0, s>>>(
+        static_cast<State*>(d_states), static_cast<VoleState*>(d_vole_states), n, static_cast<const fp2*>(d_claims),
+        static_cast<const fp2*>(d_u), static_cast<const fp2*>(d_v), count, L, static_cast<fp2*>(d_chal),
+        static_cast<fp2*>(d_proof));
+    return !cuda_failed(cudaGetLastError(), "vole round");
+}
+
+}  // namespace tp
 
 extern "C" {
 

@@ -249,7 +249,7 @@ class BatchFrameProver:
             self.torch.cuda.current_stream(self.dev).cuda_stream
 
     def prove(self, pixels, z1s, z2s_dev, points_dev, challenges: np.ndarray,
-              round_hook=None, transcripts=None, layer: int = 0, vole=None) -> None:
+              round_hook=None, transcripts=None, layer: int = 0, vole=None, graph: bool = False) -> None:
         """pixels: one uint8 device tensor per frame; z1s: uint64 [2, n_gates] per
         frame; z2s_dev / points_dev: per padded size C, a packed Fp2 device tensor
         [frames of size C][log2 C] / [..][log2 W + log2 C], frames in batch order
@@ -266,7 +266,10 @@ class BatchFrameProver:
         round (tp_vole_round_dev): a dict of `states` (uint8 [B * 160], device),
         `u`, `v` (int64 [B * count * 2], device: each frame's correlations) and
         `count`; the round's proof elements (four commitments and the equality
-        value per frame) are left in self.device_proof [rounds][B][5] Fp2."""
+        value per frame) are left in self.device_proof [rounds][B][5] Fp2.
+        graph: with transcripts and vole on a stream of the caller's, every round
+        and the finish run as one CUDA graph (tp_batch_vole_rounds_graph), captured
+        on the first call and replayed after."""
         lib, s, b = self.lib, self._s(), self.handle
         if not isinstance(z2s_dev, dict):
             assert len(self.groups) == 1
@@ -307,7 +310,14 @@ class BatchFrameProver:
         else:
             ch = np.ascontiguousarray(challenges, np.uint64)
         l0 = lib.tp_batch_launches(b)
-        for k in range(self.max_rounds):
+        use_graph = graph and transcripts is not None and vole is not None and self.stream is not None
+        if use_graph:
+            native.check(lib, lib.tp_batch_vole_rounds_graph(
+                b, base, transcripts.data_ptr(), vole["states"].data_ptr(), vole["u"].data_ptr(),
+                vole["v"].data_ptr(), vole["count"], layer, self.device_challenges.data_ptr(),
+                self.device_proof.data_ptr(), self.wires.data_ptr(), self.fin_beta.data_ptr()),
+                "tp_batch_vole_rounds_graph")
+        for k in range(0 if use_graph else self.max_rounds):
             native.check(lib, lib.tp_batch_claim(b, base + 64 * self.B * k), "batch_claim")
             if round_hook is not None:
                 round_hook(k)
@@ -329,8 +339,9 @@ class BatchFrameProver:
                 continue
             native.check(lib, lib.tp_batch_fold(
                 b, ch[k].reshape(-1).ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))), "batch_fold")
-        native.check(lib, lib.tp_batch_finish(b, self.wires.data_ptr(), self.fin_beta.data_ptr()),
-                     "batch_finish")
+        if not use_graph:
+            native.check(lib, lib.tp_batch_finish(b, self.wires.data_ptr(), self.fin_beta.data_ptr()),
+                         "batch_finish")
         launches += lib.tp_batch_launches(b) - l0
         L0 = self.layouts[0]
         for C, fs in self.groups.items():
@@ -423,3 +434,45 @@ class BatchFrameProver:
         b = self.fin_beta.cpu().numpy().view(np.uint64).reshape(self.B, 2)[f]
         m = self.mle.cpu().numpy().view(np.uint64).reshape(self.B, 2)[f]
         return c, w, (int(b[0]), int(b[1])), (int(m[0]), int(m[1]))
+
+
+# ---- the round launches' autotuner (tp_batch_autotune) ----------------------------
+
+def autotune_rounds(on: bool = True) -> None:
+    """Measure the claim / fold launch split of each (round kind, work bucket) the
+    next immediate batched rounds meet, and keep the fastest for this device."""
+    lib = native.gkr()
+    native.check(lib, lib.tp_batch_autotune(1 if on else 0), "tp_batch_autotune")
+
+
+def round_tuning() -> list:
+    """The measured splits on this device: [(kind, bucket, CTAs per SM)]"""
+    lib = native.gkr()
+    n = lib.tp_batch_tune_table(None, None, None, 0)
+    native.check(lib, 0 if n >= 0 else -1, "tp_batch_tune_table")
+    k, b, m = (np.zeros(max(1, n), np.int32) for _ in range(3))
+    n = lib.tp_batch_tune_table(k.ctypes.data, b.ctypes.data, m.ctypes.data, n)
+    return [(int(k[i]), int(b[i]), int(m[i])) for i in range(n)]
+
+
+def save_round_tuning(path: str) -> None:
+    """round_tuning() to a JSON file, keyed by the device's name"""
+    import json
+    import torch
+    with open(path, "w") as fh:
+        json.dump({"device": torch.cuda.get_device_name(), "entries": round_tuning()}, fh)
+
+
+def load_round_tuning(path: str) -> int:
+    """install the splits a JSON file of save_round_tuning holds for this device's
+    name; returns how many"""
+    import json
+    import torch
+    lib = native.gkr()
+    with open(path) as fh:
+        d = json.load(fh)
+    if d.get("device") != torch.cuda.get_device_name():
+        return 0
+    for kind, bucket, mult in d.get("entries", []):
+        native.check(lib, lib.tp_batch_tune_set(int(kind), int(bucket), int(mult)), "tp_batch_tune_set")
+    return len(d.get("entries", []))

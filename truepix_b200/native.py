@@ -93,6 +93,11 @@ GKR_SIGNATURES = {
     "tp_fs_init": (_I32, [_VP, ctypes.c_char_p]),
     "tp_fs_absorb": (_I32, [_VP, _VP, ctypes.c_size_t]),
     "tp_fs_put_u64s": (_I32, [_VP, _VP, ctypes.c_size_t]),
+    "tp_batch_vole_rounds_graph": (_I32, [_VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_longlong, _I32, _VP, _VP, _VP, _VP]),
+    "tp_batch_graph_replays": (_I32, [_VP]),
+    "tp_batch_autotune": (_I32, [_I32]),
+    "tp_batch_tune_table": (_I32, [_VP, _VP, _VP, _I32]),
+    "tp_batch_tune_set": (_I32, [_I32, _I32, _I32]),
     "tp_eq_table_host": (_I32, [_VP, _I32, _VP]),
     "tp_orion_path_nodes": (_I32, [ctypes.c_longlong, _VP, _I32, _VP, _I32]),
     "tp_orion_gather_nodes_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _I32, _VP, _VP]),

@@ -20,7 +20,9 @@ Stages of a batch, and where they run:
   GKR       device, main stream: gate weights and beta, the VOLE-committed
             early rounds, late rounds and closing proofs of all frames, each
             frame's transcript and VOLE state resident on the device
-            (truepix_b200.frame.BatchFrameProver.prove / prove_late)
+            (truepix_b200.frame.BatchFrameProver.prove / prove_late); the
+            first batch's rounds run launch by launch with the round autotuner
+            on, every later batch replays them as one CUDA graph
   opening   host threads: the point's eq tables and the Orion transcript's
             queried columns and Merkle node lists; device: the combined codeword,
             its tree and the answer, the queried columns and the Merkle nodes
@@ -162,7 +164,7 @@ class ProofPipeline:
     and yields, per batch, the list of FrameProof."""
 
     def __init__(self, layout, gate_type, in0, in1, batch: int, device: int = 0, zk: bool = False,
-                 host_threads: int = 0, commit_streams: int = 8, fp2_type=None):
+                 host_threads: int = 0, commit_streams: int = 8, fp2_type=None, graph: bool = True):
         import torch
         from .frame import BatchFrameProver
         self.torch = torch
@@ -214,6 +216,10 @@ class ProofPipeline:
         self.vs0 = vs0.raw
         self.pool = concurrent.futures.ThreadPoolExecutor(host_threads or os.cpu_count() or 4)
         self.launches_last = 0
+        # the first batch's rounds run launch by launch with the round autotuner on;
+        # later batches replay them as one CUDA graph (BatchFrameProver.prove(graph=True))
+        self.graph = graph
+        self.tuned = False
 
     def close(self):
         self.pool.shutdown(wait=True)
@@ -332,7 +338,17 @@ class ProofPipeline:
             self.d_v.copy_(h["v"], non_blocking=True)
         vole = dict(states=self.d_vs, u=self.d_u, v=self.d_v, count=self.count)
         bp = self.prover
-        bp.prove(slot.frames_dev, zg, self.d_z2, self.d_pt, None, transcripts=self.d_states, vole=vole)
+        from .frame import autotune_rounds
+        if not self.tuned:
+            autotune_rounds(True)
+            try:
+                bp.prove(slot.frames_dev, zg, self.d_z2, self.d_pt, None, transcripts=self.d_states, vole=vole)
+            finally:
+                autotune_rounds(False)
+            self.tuned = True
+        else:
+            bp.prove(slot.frames_dev, zg, self.d_z2, self.d_pt, None, transcripts=self.d_states, vole=vole,
+                     graph=self.graph)
         bp.prove_late(zg, transcripts=self.d_states, vole=vole, zk=self.zk)
         self.launches_last += bp.launches_last + 1
         o = self.h_out
