@@ -1530,10 +1530,21 @@ def serving_circuits():
             "crop": Circuit("crop", *g("Crop"), 385, -1, 0)}
 
 
+def _correlations(rng, circuit, h, w):
+    from truepix_b200.pipeline import correlations_needed
+    from truepix_b200.serving import layout_for
+    count = correlations_needed(layout_for(circuit, h, w))
+    return (rng.integers(0, P61, size=(count, 2), dtype=np.uint64),
+            rng.integers(0, P61, size=(count, 2), dtype=np.uint64))
+
+
 def batched_uneven(seed=4):
-    """64 crop-then-gray frames of uneven size proven as one batch: sources 240p to
+    """64 crop-then-gray frames of uneven size proven together: sources 240p to
     1080p (16:9), crop fractions x1 < x2, y1 < y2 uniform in [0, 1] (seeded); the
-    cropped region goes through the gray circuit (2^14 .. 2^23 input wires)."""
+    cropped region goes through the gray circuit (2^14 .. 2^23 input wires). All 64
+    queued at once into the serving loop: one claim launch and one VOLE-round
+    launch per tick for every frame in its early rounds, each at its own round;
+    every frame leaves with its whole proof."""
     from truepix_b200.serving import ProofServer, Request, latency_stats
     rng = np.random.default_rng(seed)
     gray = serving_circuits()["gray"]
@@ -1546,25 +1557,27 @@ def batched_uneven(seed=4):
         y = np.sort(rng.random(2))
         cw, ch = max(1, int(round((x[1] - x[0]) * w))), max(1, int(round((y[1] - y[0]) * h)))
         reqs.append(Request(i, gray, ch, cw, pinned_frame(rng.integers(0, 256, size=ch * cw * 3, dtype=np.uint8)),
-                            seed=9000 + i, arrival=0.0))
-    srv = ProofServer(slots=64, hbm_budget=80e9)
+                            pid=9000 + i, correlations=_correlations(rng, gray, ch, cw), arrival=0.0))
+    srv = ProofServer(slots=64, hbm_budget=80e9, max_height=1080, max_width=1920)
     srv.run(reqs, realtime=False)                  # warm-up: every size's expander graphs, pools
+    t0 = srv.ticks
     res = srv.run(reqs, realtime=False)
     st = latency_stats(res)
-    ticks = srv.ticks
+    ticks = srv.ticks - t0
     release(srv)
     wires = sorted(1 << (9 + int(np.log2(max(2, 1 << int(np.ceil(np.log2(max(2, -(-r.height * r.width * 3 // 384)))))))))
                    for r in reqs)
     return {"workload": "64 crop-then-gray frames, sources 240p-1080p, seeded crops", "frames": len(res),
             "frames_per_s": st.get("frames_per_s"), "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"),
             "input_wires_min": wires[0], "input_wires_max": wires[-1], "ticks": ticks,
-            "what": "GKR early rounds + MLE + Orion commit per frame, continuous batch of 64 slots"}
+            "what": "whole proofs (proof container + Orion opening file) of 64 uneven frames, continuous batch "
+                    "of 64 slots on device transcripts"}
 
 
 def serving_sweep(rates=(100, 250, 500, 1000), n_req=192, seed=5):
     """Poisson arrivals of gray / crop / mask proofs of 360p .. 2160p frames at rate
     lambda (frames/s), real time, admission by HBM footprint (60 GB budget); frames
-    in pinned host memory."""
+    in pinned host memory; every request leaves with its whole proof."""
     from truepix_b200.serving import ProofServer, Request, latency_stats
     cs = serving_circuits()
     sizes = [(360, 640), (480, 854), (720, 1280), (1080, 1920), (1440, 2560), (2160, 3840)]
@@ -1574,6 +1587,7 @@ def serving_sweep(rates=(100, 250, 500, 1000), n_req=192, seed=5):
     srv = ProofServer(slots=64, hbm_budget=60e9)
     out = []
     runs = []
+    corr = {}
     for lam in rates:
         t = 0.0
         reqs = []
@@ -1581,7 +1595,10 @@ def serving_sweep(rates=(100, 250, 500, 1000), n_req=192, seed=5):
             t += rng.exponential(1.0 / lam)
             hw = sizes[int(rng.integers(len(sizes)))]
             op = ["gray", "crop", "mask"][int(rng.integers(3))]
-            reqs.append(Request(i, cs[op], hw[0], hw[1], frames[hw][i % 2], seed=77 + i, arrival=t))
+            if (op, hw) not in corr:
+                corr[(op, hw)] = _correlations(rng, cs[op], hw[0], hw[1])
+            reqs.append(Request(i, cs[op], hw[0], hw[1], frames[hw][i % 2], pid=77 + i, correlations=corr[(op, hw)],
+                                arrival=t))
         runs.append((lam, reqs))
     # warm-up: one rate's requests all at once (every size's graphs, the pools
     # grown to a full batch's footprint)
@@ -1594,7 +1611,7 @@ def serving_sweep(rates=(100, 250, 500, 1000), n_req=192, seed=5):
         out.append(st)
     release(srv)
     return {"workload": "Poisson requests, ops gray/crop/mask uniform, 360p-2160p uniform, %d per rate, "
-                        "frames in pinned host memory" % n_req,
+                        "frames in pinned host memory, whole proofs" % n_req,
             "slots": 64, "hbm_budget_gb": 60, "by_rate": out}
 
 

@@ -368,12 +368,14 @@ int tp_fs_put_u64s(void* state, const uint64_t* values, size_t n);
  * vector) as a list of ints, the bytes tp_fs_put_u64s absorbs for the vector
  * tp_circuit_outputs_pixels_dev writes (circuitnizkvec_vole.py:351-355), computed
  * on the host copy by copy from the frame's bytes (pixels[f]: n_copies *
- * copy_size bytes in host memory) and hashed as it is made; frames whose
+ * copy_size bytes in host memory, of which the first n_bytes are read: past them
+ * the inputs are zero, as in a frame whose last copy is not full) and hashed as
+ * it is made; frames whose
  * transcripts stand at the same offset are hashed two at a time in lockstep. The
  * vector itself (2^23 values at 1080p) is never stored. Arguments as for
  * tp_circuit_outputs_pixels_dev; n_gates <= 4096. */
-int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pixels, int n_frames, int n_copies,
-                                     int n_copies_padded, int copy_size, int n_wires, int const_idx,
+int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pixels, long long n_bytes, int n_frames,
+                                     int n_copies, int n_copies_padded, int copy_size, int n_wires, int const_idx,
                                      uint64_t const_val, int n_gates, const int* gate_type, const int* in0,
                                      const int* in1);
 /* put(Fp2) for each (re[i], im[i]) in turn (fiatshamir.py:129-131) */
@@ -413,6 +415,16 @@ int tp_vole_state_init(void* state, uint64_t first_correlation, const uint64_t* 
 int tp_vole_round_dev(void* d_fs_states, void* d_vole_states, int n, const void* d_claims, const void* d_u,
                       const void* d_v, long long count, const char* label, void* d_chal, void* d_proof,
                       void* stream);
+/* The same round for frames each at its own round (a serving loop's slots; no
+ * counterpart in the reference, which proves one frame per process): d_meta[i]
+ * = {round, rounds} as two ints (round < 0: slot idle); slot i's claims at
+ * d_claims + 64 i bytes, correlations u / v at + 16 count i, label
+ * "sc-<layer>-<round>"; its challenge to d_chal_cur[i] and d_chal_hist[i *
+ * max_rounds + round], proof elements (optional) at d_proof + 80 (i * max_rounds
+ * + round) bytes; then round + 1, or -1 after the last round. Async. */
+int tp_vole_round_slots_dev(void* d_fs_states, void* d_vole_states, int n_slots, void* d_meta, const void* d_claims,
+                            const void* d_u, const void* d_v, long long count, int layer, void* d_chal_cur,
+                            void* d_chal_hist, void* d_proof, int max_rounds, void* stream);
 
 #ifdef __cplusplus
 }

@@ -239,6 +239,22 @@ int tp_eq_table_host(const uint64_t* z, int k, uint64_t* out);
  * writes their node indices to out_nodes (cap entries) and returns how many
  * (-1 on bad arguments or when more than cap). */
 int tp_orion_path_nodes(long long n_leaves, const long long* positions, int count, int* out_nodes, int cap);
+/* The bytes of an opening proof file (OpeningProof::write_file, orion_proof.cpp:67-95):
+ * "ORIONPV1", version 2, use_group1, N, the column size 128, msg_len, cw_len, the
+ * query count; the answer; both roots; the queried column indices; the queried
+ * columns (n_queries x 128 elements); the combined codeword (cw_len elements) and
+ * its first msg_len again (the combined message); then per tree the node count and
+ * (u32 index, 32-byte digest) per node. Elements are (img, real) u64 pairs. Writes
+ * into out (cap bytes; tp_orion_opening_file_size tells how many) on the host and
+ * returns the size, or -1. */
+long long tp_orion_opening_file_size(long long msg_len, long long cw_len, int n_queries, int n_com_nodes,
+                                     int n_comb_nodes);
+long long tp_orion_opening_file(long long N, long long msg_len, long long cw_len, const uint64_t* answer,
+                                const unsigned char* com_root, const unsigned char* comb_root, const long long* col_q,
+                                int n_queries, const uint64_t* cols, const uint64_t* combined, const int* com_idx,
+                                const unsigned char* com_nodes, int n_com_nodes, const int* comb_idx,
+                                const unsigned char* comb_nodes, int n_comb_nodes, int use_group1, unsigned char* out,
+                                long long cap);
 /* d_out[i] = the 32-byte node d_nodes[i] of a heap-ordered tree of n_nodes_tree
  * digests (device; a node index outside the tree gives 32 zero bytes). Async. */
 int tp_orion_gather_nodes_dev(const void* d_tree, long long n_nodes_tree, const void* d_nodes, int n, void* d_out,

@@ -1,7 +1,11 @@
-"""Continuous batching (truepix_b200.serving): frames of mixed operations and
-resolutions join and leave one running batch between rounds; every result must
-be bit-identical to the same request proven alone, and to the single-frame path
-(truepix_b200.frame.GkrInputLayerProver + truepix_b200.orion.FrameCommitter)."""
+"""The serving loop (truepix_b200.serving): requests of mixed operations and
+resolutions join and leave one running batch, each on its own device
+transcript; every request leaves with its whole proof (the proof container and
+the Orion opening file). A proof made in the mix is byte-identical to the same
+request served alone and to the step-by-step path (commit, prove_frames,
+opening_proof: pinned to the reference prover's proofs and the reference
+program's opening files by tests/test_gpu_prover.py and test_gpu_opening.py);
+admission keeps the HBM footprint within the budget."""
 import os
 
 import numpy as np
@@ -10,6 +14,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+P61 = (1 << 61) - 1
 
 
 def circuits():
@@ -23,102 +28,79 @@ def circuits():
 
 
 def requests():
-    from truepix_b200.serving import Request
+    from truepix_b200.pipeline import correlations_needed
+    from truepix_b200.serving import Request, layout_for
     cs = circuits()
     sizes = [(120, 160), (360, 640), (240, 426), (480, 854), (720, 1280), (120, 160), (360, 640),
              (1080, 1920), (240, 426), (480, 854)]
     ops = ["gray", "crop", "mask", "inv", "gray", "crop", "gray", "gray", "mask", "crop"]
-    arrivals = [0, 0, 1, 2, 3, 5, 8, 9, 12, 13]
     out = []
-    for i, ((h, w), op, t) in enumerate(zip(sizes, ops, arrivals)):
+    for i, ((h, w), op) in enumerate(zip(sizes, ops)):
         rng = np.random.default_rng(100 + i)
-        out.append(Request(i, cs[op], h, w, rng.integers(0, 256, size=h * w * 3, dtype=np.uint8),
-                           seed=500 + i, arrival=float(t)))
+        count = correlations_needed(layout_for(cs[op], h, w)) + i
+        corr = (rng.integers(0, P61, size=(count, 2), dtype=np.uint64),
+                rng.integers(0, P61, size=(count, 2), dtype=np.uint64))
+        out.append(Request(i, cs[op], h, w, rng.integers(0, 256, size=h * w * 3, dtype=np.uint8), pid=500 + i,
+                           correlations=corr, arrival=0.0))
     return out
 
 
-def by_rid(results):
-    return {r.rid: r for r in results}
-
-
-def same(a, b):
-    return (np.array_equal(a.claims, b.claims) and np.array_equal(a.wires, b.wires) and a.beta == b.beta
-            and a.mle == b.mle and a.root == b.root)
-
-
-def test_results_in_the_mix_equal_results_alone():
+def test_proofs_in_the_mix_equal_proofs_alone():
     from truepix_b200.serving import ProofServer
-    reqs = requests()
-    srv = ProofServer(slots=6, hbm_budget=8e9)
-    mixed = by_rid(srv.run(reqs, realtime=False))
-    assert sorted(mixed) == list(range(len(reqs)))
-    alone_srv = ProofServer(slots=2)
-    for r in requests():
-        alone = alone_srv.run([r], realtime=False)
-        assert len(alone) == 1
-        assert same(mixed[r.rid], alone[0]), r.rid
-        from truepix_b200.serving import layout_for
-        assert mixed[r.rid].claims.shape == (layout_for(r.circuit, r.height, r.width).n_copy_bits, 8)
-
-
-def test_serving_matches_the_single_frame_path():
-    import torch
-    from truepix_b200.frame import GkrInputLayerProver, pack_fp2
-    from truepix_b200.orion import FrameCommitter
-    from truepix_b200.serving import ProofServer, layout_for, transcript_values
-    r = requests()[4]                     # gray 720p, 13 rounds
-    res = ProofServer(slots=2).run([r], realtime=False)[0]
-    L = layout_for(r.circuit, r.height, r.width)
-    z1, z2, point, chal = transcript_values(r.seed, r.circuit.gate_type.size, L.n_copy_bits, L.n_in_bits)
-    dev = torch.device("cuda", 0)
-    pix = torch.from_numpy(np.ascontiguousarray(r.pixels[:L.copies * L.copy_size])).to(dev)
-    plain = GkrInputLayerProver(L, r.circuit.gate_type, r.circuit.in0, r.circuit.in1)
-    plain.prove(pix, z1, torch.from_numpy(pack_fp2(z2[:, 0], z2[:, 1])).to(dev),
-                torch.from_numpy(pack_fp2(point[:, 0], point[:, 1])).to(dev), chal)
-    fc = FrameCommitter([L])
-    fc.commit([pix])
-    torch.cuda.synchronize()
-    c, w, b, m = plain.results()
-    assert np.array_equal(c, res.claims) and np.array_equal(w, res.wires)
-    assert b == res.beta and m == res.mle
-    assert fc.root(0) == res.root
-
-
-def test_admission_respects_the_hbm_budget():
-    from truepix_b200.serving import ProofServer
-    reqs = requests()
-    from truepix_b200.serving import layout_for
-    budget = 2 * max(ProofServer.footprint(layout_for(q.circuit, q.height, q.width)) for q in reqs)
-    srv = ProofServer(slots=8, hbm_budget=budget)
+    srv = ProofServer(slots=6, hbm_budget=8e9, max_height=1080, max_width=1920, host_threads=4, commit_streams=3)
     peak = [0.0]
-    orig = srv._start
+    admit = srv._admit
 
-    def start(req):
-        orig(req)
+    def watch(req):
+        admit(req)
         peak[0] = max(peak[0], srv.used)
-    srv._start = start
-    out = srv.run(reqs, realtime=False)
-    assert len(out) == len(reqs)
-    assert peak[0] <= budget
+    srv._admit = watch
+    mixed = {r.rid: r for r in srv.run(requests(), realtime=False)}
+    srv.close()
+    assert sorted(mixed) == list(range(10))
+    assert peak[0] <= 8e9 or len(mixed) == 1
+    alone_srv = ProofServer(slots=2, max_height=1080, max_width=1920, host_threads=2, commit_streams=1)
+    for r in requests():
+        [alone] = alone_srv.run([r], realtime=False)
+        assert alone.proof.proof_bytes() == mixed[r.rid].proof.proof_bytes(), r.rid
+        assert alone.proof.opening == mixed[r.rid].proof.opening, r.rid
+        assert alone.latency > 0
+    alone_srv.close()
 
 
-def test_pinned_tensor_frames_equal_numpy_frames():
-    """Frames handed over in pinned host memory (copied straight to the device)
-    and as numpy arrays (through the staging buffers), in one realtime run with
-    small commit and slot pools: identical results."""
+def test_serving_matches_the_step_by_step_path():
     import torch
+    from truepix_b200.opening import opening_proof
+    from truepix_b200.orion import FrameCommitter
+    from truepix_b200.prover import manifests_of, prove_frames
+    from truepix_b200.serving import ProofServer, layout_for
+    for k in (4, 1):                       # gray 720p, crop 360p
+        r = requests()[k]
+        srv = ProofServer(slots=2, max_height=1080, max_width=1920, host_threads=2, commit_streams=1)
+        [res] = srv.run([r], realtime=False)
+        srv.close()
+        L = layout_for(r.circuit, r.height, r.width)
+        padded = np.zeros(L.copies * L.copy_size, np.uint8)     # the last copy zero-padded
+        padded[:min(padded.size, r.pixels.size)] = r.pixels[:padded.size]
+        pix = torch.from_numpy(padded).cuda()
+        fc = FrameCommitter([L])
+        fc.commit([pix])
+        torch.cuda.synchronize()
+        [m] = manifests_of(fc)
+        assert res.proof.manifest == m
+        c = r.circuit
+        [t] = prove_frames([pix], L, c.gate_type, c.in0, c.in1, [r.pid], [r.correlations], [m], zk=False)
+        assert res.proof.proof_bytes() == t.proof_bytes(), k
+        pt = [(int(x.real), int(x.imag)) if hasattr(x, "real") else (int(x[0]), int(x[1]))
+              for x in t.final_input_point]
+        assert res.proof.opening == opening_proof(fc, 0, pt), k
+
+
+def test_too_few_correlations_are_refused():
     from truepix_b200.serving import ProofServer
-    base = by_rid(ProofServer(slots=4).run(requests(), realtime=False))
-    reqs = requests()
-    for k, r in enumerate(reqs):
-        if k % 2 == 0:
-            r.pixels = torch.from_numpy(r.pixels).pin_memory()
-        r.arrival = 0.002 * k
-    srv = ProofServer(slots=3, commit_buffers=2)
-    got = by_rid(srv.run(reqs, realtime=True))
-    assert sorted(got) == sorted(base)
-    for rid in base:
-        assert same(got[rid], base[rid]), rid
-    with pytest.raises(ValueError):
-        srv.run([type(reqs[0])(99, reqs[0].circuit, 120, 160, torch.zeros(120 * 160 * 3, dtype=torch.uint8),
-                               seed=1)], realtime=False)
+    r = requests()[0]
+    r.correlations = (r.correlations[0][:10], r.correlations[1][:10])
+    srv = ProofServer(slots=1, max_height=240, max_width=320, host_threads=1, commit_streams=1)
+    with pytest.raises(IndexError):
+        srv.run([r], realtime=False)
+    srv.close()

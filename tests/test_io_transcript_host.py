@@ -37,7 +37,8 @@ def _put_fused(lib, states, frames, c):
     st_arr = (ctypes.c_void_p * len(states))(*[ctypes.cast(s, ctypes.c_void_p) for s in states])
     px_arr = (ctypes.c_void_p * len(pix))(*[p.ctypes.data for p in pix])
     ip = ctypes.POINTER(ctypes.c_int)
-    return lib.tp_fs_put_circuit_outputs_pixels(st_arr, px_arr, len(states), c["copies"], c["padded"], c["cs"],
+    n_bytes = min(f.size for f in pix)
+    return lib.tp_fs_put_circuit_outputs_pixels(st_arr, px_arr, n_bytes, len(states), c["copies"], c["padded"], c["cs"],
                                                 c["n_wires"], c["const_idx"], c["const_val"], gt.size,
                                                 gt.ctypes.data_as(ip), i0.ctypes.data_as(ip), i1.ctypes.data_as(ip))
 
@@ -109,6 +110,22 @@ def test_unequal_offsets_and_three_frames():
         _put_vector(lib, want, oracle_outputs(frames[f], c["copies"], c["padded"], c["cs"], c["n_wires"],
                                               c["const_idx"], c["const_val"], c["gt"], c["i0"], c["i1"]))
         assert _key(sts[f]) == _key(want), f
+
+
+def test_short_frames_read_as_zero_padded():
+    """a frame whose bytes end inside its last copy (a crop of 385-byte copies)
+    hashes as the same frame zero-padded to whole copies"""
+    lib = _lib()
+    c = _frame_case("Crop", 50, 64, 385, 512, -1, 0, 21)
+    short = c["pix"][:50 * 385 - 200].copy()
+    padded = np.zeros(50 * 385, np.uint8)
+    padded[:short.size] = short
+    st = _state(lib, b"p")
+    assert _put_fused(lib, [st], [short], c) == 0
+    want = _state(lib, b"p")
+    _put_vector(lib, want, oracle_outputs(padded, c["copies"], c["padded"], c["cs"], c["n_wires"], c["const_idx"],
+                                          c["const_val"], c["gt"], c["i0"], c["i1"]))
+    assert _key(st) == _key(want)
 
 
 def test_bad_arguments_are_rejected():

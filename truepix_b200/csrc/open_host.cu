@@ -88,6 +88,67 @@ int tp_orion_path_nodes(long long n_leaves, const long long* positions, int coun
     return n;
 }
 
+long long tp_orion_opening_file_size(long long msg_len, long long cw_len, int n_queries, int n_com_nodes,
+                                     int n_comb_nodes)
+{
+    if (msg_len < 0 || cw_len < 0 || n_queries < 0 || n_com_nodes < 0 || n_comb_nodes < 0) return -1;
+    return 8 + 44 + 16 + 32 + 32 + 8ll * n_queries + 16ll * 128 * n_queries + 16 * cw_len + 16 * msg_len +
+           8 + 36ll * n_com_nodes + 8 + 36ll * n_comb_nodes;
+}
+
+long long tp_orion_opening_file(long long N, long long msg_len, long long cw_len, const uint64_t* answer,
+                                const unsigned char* com_root, const unsigned char* comb_root, const long long* col_q,
+                                int n_queries, const uint64_t* cols, const uint64_t* combined, const int* com_idx,
+                                const unsigned char* com_nodes, int n_com_nodes, const int* comb_idx,
+                                const unsigned char* comb_nodes, int n_comb_nodes, int use_group1, unsigned char* out,
+                                long long cap)
+{
+    tp::clear_error();
+    const long long size = tp_orion_opening_file_size(msg_len, cw_len, n_queries, n_com_nodes, n_comb_nodes);
+    if (size < 0 || !answer || !com_root || !comb_root || (n_queries && (!col_q || !cols)) || !combined || !out ||
+        msg_len > cw_len || (n_com_nodes && (!com_idx || !com_nodes)) || (n_comb_nodes && (!comb_idx || !comb_nodes))) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_opening_file: bad arguments");
+        return -1;
+    }
+    if (cap < size) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_opening_file: %lld bytes needed, %lld given", size, cap);
+        return -1;
+    }
+    unsigned char* o = out;
+    auto put = [&](const void* p, size_t n) {
+        memcpy(o, p, n);
+        o += n;
+    };
+    auto u32 = [&](uint32_t v) { put(&v, 4); };
+    auto u64 = [&](uint64_t v) { put(&v, 8); };
+    put("ORIONPV1", 8);
+    u32(2);
+    u32((uint32_t)use_group1);
+    u64((uint64_t)N);
+    u64(128);
+    u64((uint64_t)msg_len);
+    u64((uint64_t)cw_len);
+    u32((uint32_t)n_queries);
+    put(answer, 16);
+    put(com_root, 32);
+    put(comb_root, 32);
+    put(col_q, 8 * (size_t)n_queries);
+    put(cols, 16 * 128 * (size_t)n_queries);
+    put(combined, 16 * (size_t)cw_len);
+    put(combined, 16 * (size_t)msg_len);
+    for (int t = 0; t < 2; ++t) {
+        const int n = t ? n_comb_nodes : n_com_nodes;
+        const int* idx = t ? comb_idx : com_idx;
+        const unsigned char* dig = t ? comb_nodes : com_nodes;
+        u64((uint64_t)n);
+        for (int i = 0; i < n; ++i) {
+            u32((uint32_t)idx[i]);
+            put(dig + 32 * (size_t)i, 32);
+        }
+    }
+    return (long long)(o - out);
+}
+
 int tp_orion_gather_nodes_dev(const void* d_tree, long long n_nodes_tree, const void* d_nodes, int n, void* d_out,
                               void* stream)
 {

@@ -7,6 +7,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "gkr_internal.cuh"
@@ -110,6 +111,36 @@ __global__ void vole_round_kernel(State* __restrict__ st, VoleState* __restrict_
     chal[i] = r;
 }
 
+// ---- VOLE-committed rounds of frames each at its own round (the serving loop) ----
+// meta[slot] = {round, rounds}: round < 0 means the slot is idle; after its round
+// the slot moves to round + 1, or to -1 after its last round.
+__global__ void vole_round_slots_kernel(State* __restrict__ st, VoleState* __restrict__ vs, int n,
+                                        int2* __restrict__ meta, const tp::fp2* __restrict__ claims,
+                                        const tp::fp2* __restrict__ u, const tp::fp2* __restrict__ v,
+                                        long long count, int layer, tp::fp2* __restrict__ chal_cur,
+                                        tp::fp2* __restrict__ chal_hist, tp::fp2* __restrict__ proof, int max_rounds)
+{
+    using namespace tp;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int2 m = meta[i];
+    if (m.x < 0 || m.x >= m.y || m.x >= max_rounds) return;
+    VoleState w = vs[i];
+    State s = st[i];
+    fp2 coef[4];
+    vole::interpolate_cubic(claims[4 * i], claims[4 * i + 1], claims[4 * i + 2], claims[4 * i + 3], coef);
+    const long long base = (long long)i * count;
+    fp2 r;
+    const long long at = (long long)i * max_rounds + m.x;
+    vole::round(s, w, coef, 4, u + base, v + base, count, vole::sc_label(layer, m.x), proof ? proof + 5 * at : nullptr,
+                &r);
+    st[i] = s;
+    vs[i] = w;
+    chal_cur[i] = r;
+    chal_hist[at] = r;
+    meta[i] = make_int2(m.x + 1 < m.y ? m.x + 1 : -1, m.y);
+}
+
 // ---- host absorbs: whole blocks compressed straight from the caller's bytes,
 // with the x86 SHA extensions where the CPU has them (sha256_host.cpp) ----------
 constexpr tp::sha::Tables kHostTables = tp::sha::make_tables();
@@ -209,6 +240,7 @@ uint64_t host_gate_value(unsigned type, uint64_t x, uint64_t y)
 struct OutputCircuit {
     int n_copies, n_copies_padded, cs, n_wires, const_idx, n_gates, out_bits;
     uint64_t const_val;
+    long long n_bytes;                        // the frame's bytes; past them a copy's inputs are zero
     std::vector<uint32_t> type, src0, src1;   // src: the wire, or n_wires for "zero", n_wires + 1 for the constant
     std::vector<uint8_t> direct;              // the gate's value is one of its inputs (pass, multiplexer)
 };
@@ -222,8 +254,12 @@ void copy_outputs(const OutputCircuit& C, const uint8_t* pix, long long c, uint6
         return;
     }
     const uint8_t* row = pix + c * C.cs;
+    const long long left = C.n_bytes - c * (long long)C.cs;
+    const uint32_t avail = left >= C.cs ? (uint32_t)C.cs : left > 0 ? (uint32_t)left : 0u;
     const uint32_t cs = (uint32_t)C.cs, konst = (uint32_t)C.n_wires + 1;
-    auto val = [&](uint32_t a) -> uint64_t { return a < cs ? row[a] : a == konst ? C.const_val : 0; };
+    auto val = [&](uint32_t a) -> uint64_t {
+        return a < cs ? (a < avail ? row[a] : 0) : a == konst ? C.const_val : 0;
+    };
     for (int g = 0; g < C.n_gates; ++g) {
         const uint64_t va = val(C.src0[g]);
         out[g] = C.direct[g] ? va : host_gate_value(C.type[g], va, val(C.src1[g]));
@@ -402,8 +438,8 @@ int tp_fs_put_u64s(void* state, const uint64_t* v, size_t n)
     return 0;
 }
 
-int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pixels, int n_frames, int n_copies,
-                                     int n_copies_padded, int copy_size, int n_wires, int const_idx,
+int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pixels, long long n_bytes, int n_frames,
+                                     int n_copies, int n_copies_padded, int copy_size, int n_wires, int const_idx,
                                      uint64_t const_val, int n_gates, const int* gate_type, const int* in0,
                                      const int* in1)
 {
@@ -414,7 +450,7 @@ int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pix
         (n_copies_padded & (n_copies_padded - 1)) != 0 || copy_size < 1 || n_wires < copy_size ||
         n_wires > (1 << 14) || const_idx >= n_wires || (const_idx >= 0 && const_idx < copy_size) ||
         const_val >= tp::P61 || n_gates < 1 || n_gates > 4096 || !gate_type || !in0 || !in1 ||
-        values >= (1ll << 32)) {
+        values >= (1ll << 32) || n_bytes < 0) {
         tp::set_error(tp::TP_ERR_ARG, "tp_fs_put_circuit_outputs_pixels: bad arguments");
         return -1;
     }
@@ -427,6 +463,7 @@ int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pix
     C.const_val = const_val;
     C.n_gates = n_gates;
     C.out_bits = tp_circuit_out_bits(n_gates);
+    C.n_bytes = std::min<long long>(n_bytes, (long long)n_copies * copy_size);
     // sources: a byte of the copy (wire < copy_size), the constant (n_wires + 1), else zero (n_wires)
     auto src = [&](int w) -> uint32_t {
         return w < copy_size ? (uint32_t)w : w == const_idx ? (uint32_t)n_wires + 1 : (uint32_t)n_wires;
@@ -624,6 +661,25 @@ int tp_vole_state_init(void* state, uint64_t first_correlation, const uint64_t* 
     }
     memcpy(state, &w, sizeof(w));
     return 0;
+}
+
+int tp_vole_round_slots_dev(void* d_fs_states, void* d_vole_states, int n_slots, void* d_meta, const void* d_claims,
+                            const void* d_u, const void* d_v, long long count, int layer, void* d_chal_cur,
+                            void* d_chal_hist, void* d_proof, int max_rounds, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!d_fs_states || !d_vole_states || n_slots < 1 || !d_meta || !d_claims || !d_u || !d_v || count < 4 ||
+        !d_chal_cur || !d_chal_hist || max_rounds < 1 || max_rounds > 64 || layer < 0) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_vole_round_slots_dev: bad arguments");
+        return -1;
+    }
+    vole_round_slots_kernel<<<(n_slots + 127) / 128, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        static_cast<State*>(d_fs_states), static_cast<VoleState*>(d_vole_states), n_slots, static_cast<int2*>(d_meta),
+        static_cast<const tp::fp2*>(d_claims), static_cast<const tp::fp2*>(d_u), static_cast<const tp::fp2*>(d_v),
+        count, layer, static_cast<tp::fp2*>(d_chal_cur), static_cast<tp::fp2*>(d_chal_hist),
+        static_cast<tp::fp2*>(d_proof), max_rounds);
+    return tp::cuda_failed(cudaGetLastError(), "vole round slots") ? -1 : 0;
 }
 
 int tp_vole_round_dev(void* d_fs_states, void* d_vole_states, int n, const void* d_claims, const void* d_u,

@@ -95,14 +95,20 @@ GKR_SIGNATURES = {
     "tp_fs_put_u64s": (_I32, [_VP, _VP, ctypes.c_size_t]),
     "tp_batch_vole_rounds_graph": (_I32, [_VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_longlong, _I32, _VP, _VP, _VP, _VP]),
     "tp_batch_graph_replays": (_I32, [_VP]),
+    "tp_vole_round_slots_dev": (_I32, [_VP, _VP, _I32, _VP, _VP, _VP, _VP, ctypes.c_longlong, _I32, _VP, _VP, _VP, _I32,
+                                       _VP]),
     "tp_batch_autotune": (_I32, [_I32]),
     "tp_batch_tune_table": (_I32, [_VP, _VP, _VP, _I32]),
     "tp_batch_tune_set": (_I32, [_I32, _I32, _I32]),
     "tp_eq_table_host": (_I32, [_VP, _I32, _VP]),
+    "tp_orion_opening_file_size": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_longlong, _I32, _I32, _I32]),
+    "tp_orion_opening_file": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, _VP, _VP,
+                                                  _VP, _VP, _I32, _VP, _VP, _VP, _VP, _I32, _VP, _VP, _I32, _I32,
+                                                  _VP, ctypes.c_longlong]),
     "tp_orion_path_nodes": (_I32, [ctypes.c_longlong, _VP, _I32, _VP, _I32]),
     "tp_orion_gather_nodes_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _I32, _VP, _VP]),
-    "tp_fs_put_circuit_outputs_pixels": (_I32, [_VP, _VP, _I32, _I32, _I32, _I32, _I32, _I32, _U64, _I32, _PI32,
-                                                _PI32, _PI32]),
+    "tp_fs_put_circuit_outputs_pixels": (_I32, [_VP, _VP, ctypes.c_longlong, _I32, _I32, _I32, _I32, _I32, _I32, _U64,
+                                                _I32, _PI32, _PI32, _PI32]),
     "tp_fs_put_fp2s": (_I32, [_VP, _VP, _VP, ctypes.c_size_t]),
     "tp_fs_put_str": (_I32, [_VP, ctypes.c_char_p]),
     "tp_fs_rand_scalar": (_I32, [_VP, _VP]),

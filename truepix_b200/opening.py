@@ -25,6 +25,7 @@ verifier repeats it on its side.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 import struct
 
@@ -85,22 +86,30 @@ def merkle_siblings(tree: np.ndarray, n_leaves: int, positions) -> tuple:
 
 
 def opening_bytes(N, msg_len, cw_len, answer, com_root, comb_root, col_q, cols, combined, com_sparse, comb_sparse,
-                  use_group1: int = 1):
-    """OpeningProof::write_file (orion_proof.cpp:67-95); elements as (img, real) uint64 pairs"""
-    out = [b"ORIONPV1", struct.pack("<IIQQQQI", 2, use_group1, N, COLUMN_SIZE, msg_len, cw_len, len(col_q)),
-           np.ascontiguousarray(answer, np.uint64).tobytes(), com_root, comb_root,
-           np.asarray(col_q, np.int64).tobytes(), np.ascontiguousarray(cols, np.uint64).tobytes(),
-           np.ascontiguousarray(combined, np.uint64).tobytes(),
-           np.ascontiguousarray(combined[:msg_len], np.uint64).tobytes()]
-    for idxs, digs in (com_sparse, comb_sparse):
-        # u32 node index then its 32-byte digest, per node
-        rec = np.empty(len(idxs), dtype=[("i", "<u4"), ("d", "u1", 32)])
-        rec["i"] = np.asarray(idxs, np.uint32)
-        if len(idxs):
-            rec["d"] = np.frombuffer(b"".join(digs), np.uint8).reshape(-1, 32) if isinstance(digs, list) \
-                else np.asarray(digs, np.uint8).reshape(-1, 32)
-        out += [struct.pack("<Q", len(idxs)), rec.tobytes()]
-    return b"".join(out)
+                  use_group1: int = 1) -> bytearray:
+    """OpeningProof::write_file (orion_proof.cpp:67-95); elements as (img, real)
+    uint64 pairs; com_sparse / comb_sparse: (node indices, their 32-byte digests as
+    a list of bytes or an [n, 32] uint8 array). The bytes are written by the
+    library (tp_orion_opening_file) into a bytearray."""
+    lib = native.gkr(require_device=False)
+    arr = lambda a, t: np.ascontiguousarray(a, t)
+
+    def sparse(sp):
+        idxs, digs = sp
+        d = np.frombuffer(b"".join(digs), np.uint8) if isinstance(digs, list) else np.asarray(digs, np.uint8)
+        return arr(idxs, np.int32), arr(d.reshape(-1), np.uint8)
+    ans, q = arr(answer, np.uint64), arr(col_q, np.int64)
+    cl, cb = arr(cols, np.uint64), arr(combined, np.uint64)
+    (ci, cd), (bi, bd) = sparse(com_sparse), sparse(comb_sparse)
+    size = lib.tp_orion_opening_file_size(msg_len, cw_len, q.size, ci.size, bi.size)
+    out = bytearray(size)
+    buf = (ctypes.c_char * size).from_buffer(out)
+    got = lib.tp_orion_opening_file(N, msg_len, cw_len, ans.ctypes.data, bytes(com_root), bytes(comb_root),
+                                    q.ctypes.data, q.size, cl.ctypes.data, cb.ctypes.data, ci.ctypes.data,
+                                    cd.ctypes.data, ci.size, bi.ctypes.data, bd.ctypes.data, bi.size, use_group1,
+                                    ctypes.addressof(buf), size)
+    native.check(lib, 0 if got == size else -1, "tp_orion_opening_file")
+    return out
 
 
 def query_columns(lib, root: bytes, N: int, use_group1: int, r0: np.ndarray, r1: np.ndarray, cw_len: int,

@@ -72,7 +72,11 @@ class CircuitOutputs:
     def values(self) -> np.ndarray:
         import torch
         from .frame import circuit_outputs
-        pix = torch.from_numpy(np.ascontiguousarray(self.pixels)).to(self.device)
+        L = self.layout
+        full = np.zeros(L.copies * L.copy_size, np.uint8)        # a short last copy is zero-padded
+        n = min(full.size, self.pixels.size)
+        full[:n] = np.asarray(self.pixels).reshape(-1)[:n]
+        pix = torch.from_numpy(full).to(self.device)
         out = circuit_outputs(pix, self.layout, *self.gates)
         torch.cuda.synchronize(self.device)
         return out.cpu().numpy().view(np.uint64)
@@ -278,8 +282,9 @@ class ProofPipeline:
             t.fs.io.append(CircuitOutputs(slot.frames_host[f], L, self.gt, self.i0, self.i1, self.dev))
         states = (ctypes.c_void_p * len(fs))(*[ctypes.addressof(t.fs._st) for t in trs])
         pix = (ctypes.c_void_p * len(fs))(*[slot.frames_host[f].ctypes.data for f in fs])
+        n_bytes = min(slot.frames_host[f].size for f in fs)
         native.check(self.lib, self.lib.tp_fs_put_circuit_outputs_pixels(
-            states, pix, len(fs), L.copies, L.padded_copies, L.copy_size, L.n_wires, L.const_idx, L.const_val,
+            states, pix, n_bytes, len(fs), L.copies, L.padded_copies, L.copy_size, L.n_wires, L.const_idx, L.const_val,
             self.G, self.gt.ctypes.data_as(_I32P), self.i0.ctypes.data_as(_I32P), self.i1.ctypes.data_as(_I32P)),
             "tp_fs_put_circuit_outputs_pixels")
         for ev in slot.root_events:
@@ -474,6 +479,18 @@ class ProofPipeline:
     def run(self, batches):
         """Prove every batch (see the class docstring); yields each batch's list of
         FrameProof in order."""
+        import sys
+        # the host threads hold the interpreter lock in short stretches (numpy
+        # assembly, transcript puts): a short switch interval lets the launching
+        # thread take it back soon
+        switch = sys.getswitchinterval()
+        sys.setswitchinterval(2e-4)
+        try:
+            yield from self._run(batches)
+        finally:
+            sys.setswitchinterval(switch)
+
+    def _run(self, batches):
         prev = None
         for i, batch in enumerate(batches):
             slot = self.slots[i % 2]
