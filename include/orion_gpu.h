@@ -121,6 +121,33 @@ int tp_orion_query_columns_async_dev(const void* d_rows, long long N, const void
 int tp_orion_answer_dev(const void* d_combined, long long msg_len, const void* d_r1, void* d_answer,
                         void* stream);
 
+/* Replaces encode(src, dst, n) of one message (include/linear_code/linear_code_encode.h:17-72)
+ * with the graphs of expander_init(col_len): d_out (tp_orion_codeword_len(col_len)
+ * elements) receives the codeword of d_msg (col_len elements). The EC(y1) step of
+ * the opening (linearPC.cpp:585-605: the GKR circuit generate_circuit builds
+ * computes this code at the queried positions). Async. */
+int tp_orion_encode_dev(const void* d_msg, long long col_len, void* d_out, void* stream);
+
+/* The per-query checks of verify_opening_proof (src/VPD/linearPC.cpp:733-879) on
+ * the device, all queries at once: for i < count,
+ *   d_flags[i] bit 0  sum_j r0[j] cols[i][j] != combined[q[i]]   (column linear combo)
+ *              bit 1  the column's leaf chain does not reach com_root along the
+ *                     commitment's sparse siblings (verify_claim_sparse,
+ *                     src/truepix/orion_proof.cpp:176-200)
+ *              bit 2  SHA256(combined[q[i]] || 0^48) does not reach comb_root
+ *              bit 3  enc[q2[i]] != combined[q2[i]] (EC(y1); d_q2 may be NULL)
+ *              16     an index outside [0, cw_len)
+ * d_r0: 128 elements; d_q, d_q2: count int64; d_cols: count x 128 elements;
+ * d_combined, d_enc: cw_len elements; sibling lists: n node indices (uint32,
+ * ascending) and n 32-byte digests on the device; roots: 32 host bytes. msg_len a
+ * power of two, cw_len = tp_orion_codeword_len(msg_len). Async. */
+int tp_orion_verify_opening_dev(long long msg_len, long long cw_len, const void* d_r0, const void* d_q,
+                                const void* d_q2, int count, const void* d_cols, const void* d_combined,
+                                const void* d_enc, const void* d_com_idx, const void* d_com_nodes, int n_com,
+                                const void* d_cmb_idx, const void* d_cmb_nodes, int n_cmb,
+                                const unsigned char* com_root, const unsigned char* comb_root, int* d_flags,
+                                void* stream);
+
 /* Kernels launched by the calling thread's last commit (any of the three forms). */
 int tp_orion_last_launches(void);
 
@@ -186,6 +213,22 @@ int tp_rs_commit_dev(const void* d_src, int log_len, void* d_l_eval, void* d_tre
  * (merkle[step], root at 1). r canonical (real, imag). */
 int tp_fri_commit_step_dev(const void* d_witness, int log_m, uint64_t r_real, uint64_t r_imag, void* d_next,
                            void* d_tree, void* stream);
+
+/* ---- ./fft_gkr (src/VPD/fft_circuit_GKR.cpp) ---------------------------------
+ * Replaces the program that poly_commit_verifier::verify_poly_commitment runs as
+ * system("./fft_gkr <lg> log_fftgkr.txt") (src/VPD/vpd_verifier.cpp:80-89): the
+ * GKR proof, with its verifier's checks, of the circuit build_circuit(lg)
+ * (:22-112: tensor expansion of lg points, inverse FFT of size 2^lg, scaling,
+ * 64 polynomial evaluations and their sums) over the sumcheck of engage_gkr
+ * (:770-825). The prover runs on the device; the verifier's randomness is the
+ * reference's (glibc rand() in its unseeded state, drawn in its order), so the
+ * claims are the reference's. Outputs what main (:827-845) writes: v_time
+ * (seconds of the closed-form layer checks), proof_size (bytes, the reference's
+ * count) and p_time (seconds of the whole proof, checks included); *accepted = 1
+ * when every check passed. trace_path: NULL, or a file receiving the layers (lg
+ * <= 6), the claim after each layer group, the last sumcheck tables and the
+ * result (the fixture format of tests/golden/gen_fft_gkr_golden.py). 0 <= lg <= 20. */
+int tp_fft_gkr(int lg, double* v_time, long long* proof_size, double* p_time, int* accepted, const char* trace_path);
 
 /* ---- Virgo (linear GKR) sumcheck (src/linear_gkr/prover.cpp) --------------- */
 

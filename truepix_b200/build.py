@@ -24,7 +24,19 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
 LIBS = {
     "libnative_fp2_gpu.so": ["runtime.cu", "gkr.cu", "gkr_pixels.cu", "gkr_batch.cu", "gkr_session.cu",
                              "native_fp2_abi.cu", "mle_noalloc.cu", "orion.cu", "orion_open.cu", "orion_abi.cu", "ntt.cu", "rs_commit.cu", "virgo.cu", "ntt_abi.cu",
-                             "transcript.cu", "sha256_host.cpp", "circuit.cu", "late.cu", "open_host.cu"],
+                             "transcript.cu", "sha256_host.cpp", "circuit.cu", "late.cu", "open_host.cu", "fft_gkr.cu", "orion_verify.cu"],
+}
+
+
+# Programs over the library (host code), in truepix_b200/bin/: the process
+# boundaries the reference's Python front end runs (./fft_gkr and the
+# linearPC_multi_* Orion programs), each linked to libnative_fp2_gpu.so.
+BINDIR = os.path.join(PKG, "bin")
+PROGRAMS = {
+    "fft_gkr": ("fft_gkr_main.cpp", []),
+    "linearPC_multi_commit": ("orion_cli.cpp", ["-DTP_CLI_PHASE=1"]),
+    "linearPC_multi_prove": ("orion_cli.cpp", ["-DTP_CLI_PHASE=2"]),
+    "linearPC_multi_open": ("orion_cli.cpp", ["-DTP_CLI_PHASE=3"]),
 }
 
 
@@ -74,6 +86,19 @@ def build(verbose: bool = False, ptxas_info: bool = False, jobs: int | None = No
         if todo or _stale(target, objs):
             run([nvcc()] + ARCH + ["-shared", "-o", target] + objs)
         out.append(target)
+    os.makedirs(BINDIR, exist_ok=True)
+    lib = os.path.join(LIBDIR, "libnative_fp2_gpu.so")
+    progs = []
+    for name, (src, defs) in PROGRAMS.items():
+        target = os.path.join(BINDIR, name)
+        srcp = os.path.join(CSRC, src)
+        if _stale(target, [srcp, lib] + headers):
+            progs.append([nvcc()] + ARCH + ["-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include")] + defs +
+                         ["-o", target, srcp, "-L" + LIBDIR, "-lnative_fp2_gpu", "-Xlinker", "-rpath",
+                          "-Xlinker", "$ORIGIN/../lib"])
+        out.append(target)
+    with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+        list(ex.map(run, progs))
     return out
 
 

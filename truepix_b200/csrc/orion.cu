@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "fp2.cuh"
+#include "glibc_rand.h"
 #include "orion.h"
 #include "runtime.h"
 #include "sha256.cuh"
@@ -22,40 +23,6 @@ std::atomic<int> g_leaf_chunks{1};   // launches the row-leaf chains are split i
 
 // kernel-timer tags (runtime.h timer_*): commit kernels are 9100 + kind
 constexpr int kTagLoad = 9100, kTagGatherBytes = 9101, kTagGather = 9102, kTagLeaf = 9103, kTagTree = 9104;
-
-// glibc rand(): the TYPE_3 additive generator (degree 31, separation 3) that
-// glibc uses by default. Seeded like srand(seed): r[0] = seed, r[i] = 16807 *
-// r[i-1] mod (2^31 - 1) for i < 31, r[31..33] = r[0..2], then 310 outputs are
-// discarded; each output is o[i] = o[i-31] + o[i-3] (mod 2^32), returned >> 1.
-// The reference never seeds it, so its stream is that of seed 1.
-class GlibcRand {
-public:
-    explicit GlibcRand(uint32_t seed)
-    {
-        int64_t v = seed;
-        s_[0] = (uint32_t)v;
-        for (int i = 1; i < 31; ++i) {
-            v = (16807 * v) % 2147483647;
-            if (v < 0) v += 2147483647;
-            s_[i] = (uint32_t)v;
-        }
-        for (int i = 31; i < 34; ++i) s_[i] = s_[i - 31];
-        pos_ = 34;
-        for (int i = 0; i < 310; ++i) step();
-    }
-    int next() { return (int)(step() >> 1); }
-
-private:
-    uint32_t step()
-    {
-        const uint32_t o = s_[(pos_ - 31) % 34] + s_[(pos_ - 3) % 34];
-        s_[pos_ % 34] = o;
-        ++pos_;
-        return o;
-    }
-    uint32_t s_[34];
-    long long pos_;
-};
 
 long long c_targets(long long n) { return (long long)(0.238 * (double)n); }
 long long d_targets(long long n, long long L) { return (long long)((double)n * (1.72 - 1) - (double)L); }
@@ -753,6 +720,14 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
     }
     // 5. the tree
     return build_tree(tree, size, s);
+}
+
+bool leaf_digests(const ulonglong2* rows, long long count, unsigned char* digests, cudaStream_t s)
+{
+    if (count <= 0) return true;
+    leaf_kernel<<<(unsigned)((count + kLeafRows - 1) / kLeafRows), kLeafRows, 0, s>>>(rows, count, digests, 0, 1u, 0,
+                                                                                       kColumns / 2);
+    return launch_ok("orion column leaves");
 }
 
 bool build_tree(unsigned char* tree, long long leaves, cudaStream_t s)

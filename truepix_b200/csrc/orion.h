@@ -117,6 +117,24 @@ bool query_rows_async(const ulonglong2* rows, long long cw_len, const long long*
 // *out = sum_{i < n} r1[i] combined[i]
 bool answer(const ulonglong2* combined, const ulonglong2* r1, long long n, ulonglong2* out, cudaStream_t s);
 
+// The row-leaf chains of `count` rows of 128 elements (the commit's leaves)
+// into digests[0 .. count) (32 bytes each).
+bool leaf_digests(const ulonglong2* rows, long long count, unsigned char* digests, cudaStream_t s);
+
+// Enc(msg) of one column (orion_verify.cu): out[0, cw_len) from msg[0, col_len)
+// with the encoder's graphs, level by level as commit() does for 128 columns.
+bool encode_vector(const Encoder& enc, const ulonglong2* msg, ulonglong2* out, cudaStream_t s);
+
+// The verifier's per-query checks of an opening proof (orion_verify.cu): flags[i]
+// bit 0 column sum != combined[q[i]], bit 1 commitment path, bit 2 combined
+// path, bit 3 enc[q2[i]] != combined[q2[i]] (q2 may be null), 16 an index
+// outside the codeword. Sibling lists sorted by node index.
+bool verify_opening(long long msg_len, long long cw_len, const ulonglong2* r0, const long long* q,
+                    const long long* q2, int count, const ulonglong2* cols, const ulonglong2* combined,
+                    const ulonglong2* enc, const unsigned* com_idx, const unsigned char* com_dig, int n_com,
+                    const unsigned* cmb_idx, const unsigned char* cmb_dig, int n_cmb, const unsigned char* com_root,
+                    const unsigned char* cmb_root, int* flags, cudaStream_t s);
+
 // `blocks` CTAs of 128 threads, each thread chaining `iters` SHA-256 of 64 bytes
 // in registers (2 compressions each); XORs its last digest into *out
 bool sha_peak(int blocks, int iters, uint32_t* out, cudaStream_t s);

@@ -311,6 +311,49 @@ int tp_orion_answer_dev(const void* d_combined, long long msg_len, const void* d
                : -1;
 }
 
+int tp_orion_encode_dev(const void* d_msg, long long col_len, void* d_out, void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (!d_msg || !d_out || col_len <= 0 || col_len > (1LL << 22)) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_encode_dev: bad arguments");
+        return -1;
+    }
+    const tp::orion::Encoder* e = tp::orion::encoder(col_len);
+    if (!e) return -1;
+    return tp::orion::encode_vector(*e, static_cast<const ulonglong2*>(d_msg), static_cast<ulonglong2*>(d_out),
+                                    reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
+int tp_orion_verify_opening_dev(long long msg_len, long long cw_len, const void* d_r0, const void* d_q,
+                                const void* d_q2, int count, const void* d_cols, const void* d_combined,
+                                const void* d_enc, const void* d_com_idx, const void* d_com_nodes, int n_com,
+                                const void* d_cmb_idx, const void* d_cmb_nodes, int n_cmb,
+                                const unsigned char* com_root, const unsigned char* comb_root, int* d_flags,
+                                void* stream)
+{
+    tp::clear_error();
+    if (!tp::ctx()) return -1;
+    if (msg_len <= 0 || (msg_len & (msg_len - 1)) || cw_len != tp::orion::codeword_len(msg_len) || !d_r0 || !d_q ||
+        count <= 0 || !d_cols || !d_combined || (d_q2 && !d_enc) || !d_com_idx || !d_com_nodes || n_com <= 0 ||
+        !d_cmb_idx || !d_cmb_nodes || n_cmb <= 0 || !com_root || !comb_root || !d_flags) {
+        tp::set_error(tp::TP_ERR_ARG, "tp_orion_verify_opening_dev: bad arguments");
+        return -1;
+    }
+    return tp::orion::verify_opening(msg_len, cw_len, static_cast<const ulonglong2*>(d_r0),
+                                     static_cast<const long long*>(d_q), static_cast<const long long*>(d_q2), count,
+                                     static_cast<const ulonglong2*>(d_cols), static_cast<const ulonglong2*>(d_combined),
+                                     static_cast<const ulonglong2*>(d_enc), static_cast<const unsigned*>(d_com_idx),
+                                     static_cast<const unsigned char*>(d_com_nodes), n_com,
+                                     static_cast<const unsigned*>(d_cmb_idx),
+                                     static_cast<const unsigned char*>(d_cmb_nodes), n_cmb, com_root, comb_root,
+                                     d_flags, reinterpret_cast<cudaStream_t>(stream))
+               ? 0
+               : -1;
+}
+
 int tp_sha256_peak_dev(int blocks, int iters, void* d_out, void* stream)
 {
     tp::clear_error();
