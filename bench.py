@@ -1379,7 +1379,7 @@ def reference_gpu_lib(frame, layout, gt, i0, i1, z1, z2, point, chal, reps=3):
     z1r, z1i = np.ascontiguousarray(z1[0]), np.ascontiguousarray(z1[1])
     z2r, z2i = np.ascontiguousarray(z2[:, 0]), np.ascontiguousarray(z2[:, 1])
     pr, pim = np.ascontiguousarray(point[:, 0]), np.ascontiguousarray(point[:, 1])
-    out, res = {}, {}
+    out, res, loop = {}, {}, {}
     for name, path in (("reference", REF_GPU_LIB), ("ours", GPU_LIB)):
         lib = Fp2Lib(path)
         lib.init()
@@ -1396,10 +1396,29 @@ def reference_gpu_lib(frame, layout, gt, i0, i1, z1, z2, point, chal, reps=3):
         for _ in range(reps):
             one()
         out[name + "_frames_per_s"] = reps / (time.perf_counter() - t0)
+        # the round loop alone on the resident session: the tables are on the
+        # device after early_create (untimed); nb x (claim, fold), each call
+        # returning when its kernels are done (both libraries' API is synchronous)
+        bre, bim = lib.compute_beta(z2r, z2i, (1, 0))
+        best = None
+        for _ in range(reps):
+            h = lib.early_create(gti, i0i, i1i, z1r, z1i, C, W, table, zero, bre, bim)
+            t0 = time.perf_counter()
+            for k in range(nb):
+                lib.early_claim(h)
+                lib.early_fold(h, chal[k])
+            dt = time.perf_counter() - t0
+            lib.early_destroy(h)
+            best = dt if best is None else min(best, dt)
+        loop[name] = 1e3 * best
     a, b = res["reference"], res["ours"]
     out["identical_outputs"] = bool(np.array_equal(a[0][0], b[0][0]) and np.array_equal(a[0][1], b[0][1])
                                     and np.array_equal(a[0][2], b[0][2]) and a[0][3] == b[0][3] and a[1] == b[1])
     out["ours_over_reference"] = out["ours_frames_per_s"] / out["reference_frames_per_s"]
+    out["round_loop_ms"] = {"reference": loop["reference"], "ours": loop["ours"],
+                            "reference_over_ours": loop["reference"] / loop["ours"],
+                            "what": "%d x (claim, fold) on the session resident on the device (best of %d), "
+                                    "host wall clock around the calls" % (nb, reps)}
     out["what"] = ("GKR input layer of one 1080p frame through the native_fp2 C ABI (host buffers, %d rounds): "
                    "the reference's native_fp2.cu (its build.sh recipe, -arch=sm_100a) vs ours" % nb)
     return out
@@ -1624,6 +1643,30 @@ def profile_case(name):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from orionlib import elements
     from truepix_b200.frame import FrameLayout
+    if name == "refgpu":
+        # one 1080p frame's GKR session through the native_fp2 C ABI: the
+        # reference's CUDA library, then ours (kernel-against-kernel launch lists)
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from fp2lib import GPU_LIB, REF_GPU_LIB, Fp2Lib, run_session
+        L = FrameLayout.for_frame(H, Wd)
+        gt, i0, i1 = circuit()
+        rng = np.random.default_rng(SEED)
+        frame = rng.integers(0, 256, size=L.copies * L.copy_size, dtype=np.uint8)
+        table, _ = host_tables(frame, L)
+        zero = np.zeros_like(table)
+        nb = L.n_copy_bits
+        z1 = rng.integers(0, P61, size=(2, 9), dtype=np.uint64)
+        z2 = rng.integers(0, P61, size=(nb, 2), dtype=np.uint64)
+        chal = [(int(a), int(b)) for a, b in rng.integers(0, P61, size=(nb, 2), dtype=np.uint64)]
+        g = [np.ascontiguousarray(x, np.int32) for x in (gt, i0, i1)]
+        for path in (REF_GPU_LIB, GPU_LIB):
+            lib = Fp2Lib(path)
+            lib.init()
+            bre, bim = lib.compute_beta(np.ascontiguousarray(z2[:, 0]), np.ascontiguousarray(z2[:, 1]), (1, 0))
+            run_session(lib, *g, np.ascontiguousarray(z1[0]), np.ascontiguousarray(z1[1]), L.padded_copies,
+                        L.n_wires, table, zero, bre, bim, chal)
+        torch.cuda.synchronize()
+        return
     if name == "proved":
         # two batches of 16 1080p frames through the pipelined whole proof (truepix_b200.pipeline)
         from truepix_b200.frame import FrameLayout
@@ -1682,7 +1725,8 @@ def main():
                     help="launches the commits' SHA-256 leaf chains are split into (tp_orion_set_leaf_chunks)")
     ap.add_argument("--commit-streams", type=int, default=8,
                     help="streams the step's commits are spread over (0: the step's stream)")
-    ap.add_argument("--profile-case", choices=["orion", "proved"], help="run a fixed short workload for ncu and exit")
+    ap.add_argument("--profile-case", choices=["orion", "proved", "refgpu"],
+                    help="run a fixed short workload for ncu and exit")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)

@@ -314,6 +314,13 @@ int tp_late_rounds_dev(int n_frames, int n_in_bits, int n_gates, const int* gate
 int tp_orion_open_queries(const unsigned char* root32, uint64_t N, int use_group1, const uint64_t* r0, int n_r0,
                           const uint64_t* r1, long long n_r1, long long cw_len, int group, int count,
                           long long* col_q);
+/* The same draws followed by the opening's second batch: ec_q receives the next
+ * count indices, uniform in [0, cw_len) in both modes (the positions at which
+ * the EC(y1) step checks the code of the combined message, linearPC.cpp:573-575
+ * in Orion_nonzk, :879-880 in Orion_zk). ec_q may be NULL. Host only. */
+int tp_orion_open_queries2(const unsigned char* root32, uint64_t N, int use_group1, const uint64_t* r0, int n_r0,
+                           const uint64_t* r1, long long n_r1, long long cw_len, int group, int count,
+                           long long* col_q, long long* ec_q);
 
 /* ---- circuit evaluation: the prover's output vector ----
  * Replaces ArithCircuitIncrementalBuilder.run (libTruePix/arithcircuitbuilder.py:71-108,

@@ -65,6 +65,13 @@ int tp_orion_commit_pixels_dev(const void* d_pixels, int n_copies, int n_copies_
  * digests do not depend on n. 0, or -1 for another n. */
 int tp_orion_set_leaf_chunks(int n);
 
+/* No counterpart in the reference. The expander gathers of later commits
+ * multiply 61 x 31 bits when every weight limb is below 2^31 (the reference's
+ * weights are rand() % p per limb); for graphs of 8192 targets or more each
+ * lane handles 1, 2 (default) or 4 of the 128 columns (4, 2 or 1 warps per
+ * target). Process-wide; the codewords do not depend on it. 0, or -1 otherwise. */
+int tp_orion_set_gather_lanes(int columns_per_lane);
+
 /* Zero-knowledge commits (TruePix-main/Orion/Orion_zk). Replaces
  * commit_pair(masked, mask, N) of src/VPD/linearPC.cpp:253-460: two Orion
  * commits, each byte-identical to commit() of its polynomial, trees returned

@@ -14,12 +14,13 @@ import pytest
 from clilib import env_for, first_error, lay_out, manifest, ours, reference, run
 
 PROGS = ("linearPC_multi_commit", "linearPC_multi_prove", "linearPC_multi_open")
+ZK = tuple(p + "_zk" for p in PROGS)
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def test_programs_are_built_against_the_in_tree_library():
     lib = os.path.realpath(os.path.join(HERE, "..", "truepix_b200", "lib", "libnative_fp2_gpu.so"))
-    for name in PROGS + ("fft_gkr",):
+    for name in PROGS + ZK + ("fft_gkr",):
         path = ours(name)
         assert os.access(path, os.X_OK), path
         out = subprocess.run(["ldd", path], capture_output=True, text=True).stdout
@@ -49,7 +50,13 @@ CASES = [
     (1, ["4", "0"], {}, "no_point"),
     (2, ["4", "0"], {}, "bad_point"),
     (1, ["4", "0"], {"TRUEPIX_GKR_POINT_FILE": "/nonexistent/p.json"}, "manifest"),
+    (4, ["4", "0"], {}, "manifest"),              # zero-knowledge program, plain manifest
+    (5, ["4", "0"], {}, "zk_manifest"),           # no mask seed file
+    (4, ["4", "0"], {}, "zk_seed_no_point"),
+    (5, ["4", "0"], {"TRUEPIX_CONST_IDX": "5"}, "input"),
+    (4, ["4", "1"], {}, "input"),
 ]
+ALL = PROGS + ZK
 
 
 def _files(d, kind):
@@ -72,13 +79,15 @@ def _files(d, kind):
     m = None
     if kind in ("manifest", "no_point", "bad_point"):
         m = manifest(4, 384, 384, 128, "00" * 32)
-    elif kind == "zk_manifest":
+    elif kind in ("zk_manifest", "zk_seed_no_point"):
         m = manifest(4, 384, 384, 128, "00" * 32, zk=True)
+        if kind == "zk_seed_no_point":
+            open(os.path.join(d, "orion_mask_seed.txt"), "w").write("12345\n")
     elif kind == "other_layout":
         m = manifest(8, 384, 384, 128, "00" * 32)
     if kind == "bad_point":
         point = [(3, 4)] * (lg - 1)
-    lay_out(d, pix, 4, 384, None if kind == "no_point" else point, m)
+    lay_out(d, pix, 4, 384, None if kind in ("no_point", "zk_seed_no_point") else point, m)
 
 
 @pytest.mark.parametrize("k", range(len(CASES)))
@@ -87,17 +96,17 @@ def test_refusals_match_the_reference_programs(k, tmp_path):
     if not os.path.exists(reference(PROGS[1])):
         pytest.skip("oracle/_ref reference programs not built")
     got = {}
-    for who, path in (("ours", ours(PROGS[idx])), ("ref", reference(PROGS[idx]))):
+    if not os.path.exists(reference(ALL[idx])):
+        pytest.skip("reference program missing")
+    for who, path in (("ours", ours(ALL[idx])), ("ref", reference(ALL[idx]))):
         d = tmp_path / who
         d.mkdir()
         _files(str(d), kind)
         env = env_for(str(d), 384, 384, 128, **extra)
-        if kind == "no_point":
+        if kind in ("no_point", "zk_seed_no_point"):
             env.pop("TRUEPIX_GKR_POINT_FILE")
         r = run(path, str(d), env, *argv, timeout=60)
         got[who] = (r.returncode != 0, first_error(r).replace(path, "PROG"))
-    if not os.path.exists(reference(PROGS[idx])):
-        pytest.skip("reference program missing")
     assert got["ours"] == got["ref"], got
 
 
@@ -106,13 +115,18 @@ def test_no_device_fails_loudly(tmp_path):
     import torch
     if torch.cuda.is_available():
         pytest.skip("a device is present")
+    for names, zk in ((PROGS, False), (ZK, True)):
+        d = str(tmp_path / str(zk))
+        os.makedirs(d)
+        lay_out(d, _frame(), 4, 384, [(3, 4)] * 11, manifest(4, 384, 384, 128, "00" * 32, zk=zk))
+        open(os.path.join(d, "orion_mask_seed.txt"), "w").write("12345\n")
+        env = env_for(d, 384, 384, 128)
+        for name in names:
+            r = run(ours(name), d, env, 4, 0, timeout=60)
+            assert r.returncode == 1 and "no CUDA device" in r.stderr, (name, r.stdout, r.stderr)
+            assert not [f for f in os.listdir(d) if f.endswith(".bin")]
     d = str(tmp_path)
-    lay_out(d, _frame(), 4, 384, [(3, 4)] * 11, manifest(4, 384, 384, 128, "00" * 32))
     env = env_for(d, 384, 384, 128)
-    for name in PROGS:
-        r = run(ours(name), d, env, 4, 0, timeout=60)
-        assert r.returncode == 1 and "no CUDA device" in r.stderr, (name, r.stdout, r.stderr)
-        assert not os.path.exists(os.path.join(d, "orion_proof.bin"))
     r = run(ours("fft_gkr"), d, env, 4, os.path.join(d, "out.txt"), timeout=60)
     assert r.returncode == 1 and r.stderr.startswith("fft_gkr: ") and not os.path.exists(os.path.join(d, "out.txt"))
 

@@ -165,3 +165,68 @@ def test_open_rejects_tampered_proofs_like_the_reference(tmp_path, kind):
         rr = run(reference("linearPC_multi_open"), d, env, copies, 0)
         assert rr.returncode == 1
         assert first_error(r) == first_error(rr), (kind, r.stderr, rr.stderr)
+
+
+def _zk_case():
+    for c in cases():
+        copies, cs, ci, cv, seed = json.loads(c["layout"].tobytes().decode())
+        if seed is not None:
+            return c, copies, cs, ci, cv, seed
+    raise AssertionError("no zero-knowledge case")
+
+
+def test_zk_programs_match_the_reference(tmp_path):
+    """the Orion_zk programs (TruePix's default): with the fixture's mask seed the
+    two opening files are byte-identical to the reference program's; our open
+    accepts them and reports masked - mask = the plaintext MLE; the reference's
+    open accepts our files"""
+    c, copies, cs, ci, cv, seed = _zk_case()
+    d = str(tmp_path)
+    m = manifest(copies, cs, ci, cv, _root_hex(c["com_root"].tobytes()), zk=True)
+    m["mask_root"] = _root_hex(c["mask_com_root"].tobytes())
+    lay_out(d, c["pix"], copies, cs, [(int(a), int(b)) for a, b in c["point"]], m)
+    with open(os.path.join(d, "orion_mask_seed.txt"), "w") as fh:
+        fh.write("%d\n" % seed)
+    env = env_for(d, cs, ci, cv, TRUEPIX_ORION_RESULT_FILE=os.path.join(d, "result.json"))
+    r = run(ours("linearPC_multi_prove_zk"), d, env, copies, 0)
+    assert r.returncode == 0 and "check pass" in r.stdout and "Commit time(mask)" in r.stdout, r.stdout + r.stderr
+    for tag, name in (("", "orion_proof_masked.bin"), ("mask_", "orion_proof_mask.bin")):
+        assert sha256_file(os.path.join(d, name)) == c[tag + "sha256"].tobytes(), name
+    r = run(ours("linearPC_multi_open_zk"), d, env, copies, 0)
+    assert r.returncode == 0 and "check pass" in r.stdout, r.stdout + r.stderr
+    ours_res = json.load(open(os.path.join(d, "result.json")))
+    assert ours_res["ok"] is True
+    if os.path.exists(reference("linearPC_multi_open_zk")):
+        os.remove(os.path.join(d, "result.json"))
+        os.symlink(ours("fft_gkr"), os.path.join(d, "fft_gkr"))
+        rr = run(reference("linearPC_multi_open_zk"), d, env, copies, 0)
+        assert rr.returncode == 0 and "check pass" in rr.stdout, rr.stdout[-2000:] + rr.stderr[-2000:]
+        assert json.load(open(os.path.join(d, "result.json"))) == ours_res
+
+
+def test_zk_commit_prove_open_round_trip(tmp_path):
+    """a fresh commit (seed from /dev/urandom, written to the seed file), then
+    prove and open; the reference's prove with the same seed writes the same files"""
+    c, copies, cs, ci, cv, _ = _zk_case()
+    d = str(tmp_path / "ours")
+    os.makedirs(d)
+    lay_out(d, c["pix"], copies, cs, [(int(a), int(b)) for a, b in c["point"]])
+    env = env_for(d, cs, ci, cv)
+    r = run(ours("linearPC_multi_commit_zk"), d, env, copies, 0)
+    assert r.returncode == 0 and "Commit time(mask)" in r.stdout, r.stderr
+    m = json.load(open(os.path.join(d, "orion_commit.json")))
+    assert m["zk"] is True and len(m["masked_root"]) == 64 and len(m["mask_root"]) == 64
+    assert run(ours("linearPC_multi_prove_zk"), d, env, copies, 0).returncode == 0
+    r = run(ours("linearPC_multi_open_zk"), d, env, copies, 0)
+    assert r.returncode == 0 and "check pass" in r.stdout, r.stdout + r.stderr
+    if os.path.exists(reference("linearPC_multi_prove_zk")):
+        e = str(tmp_path / "ref")
+        os.makedirs(e)
+        for f in ("input.txt", "gkr_point_prover.txt", "orion_commit.json", "orion_mask_seed.txt"):
+            with open(os.path.join(d, f)) as src, open(os.path.join(e, f), "w") as dst:
+                dst.write(src.read())
+        os.symlink(ours("fft_gkr"), os.path.join(e, "fft_gkr"))
+        rr = run(reference("linearPC_multi_prove_zk"), e, env_for(e, cs, ci, cv), copies, 0)
+        assert rr.returncode == 0 and "check pass" in rr.stdout, rr.stdout[-2000:] + rr.stderr[-2000:]
+        for name in ("orion_proof_masked.bin", "orion_proof_mask.bin"):
+            assert sha256_file(os.path.join(d, name)) == sha256_file(os.path.join(e, name)), name

@@ -37,6 +37,9 @@ PROGRAMS = {
     "linearPC_multi_commit": ("orion_cli.cpp", ["-DTP_CLI_PHASE=1"]),
     "linearPC_multi_prove": ("orion_cli.cpp", ["-DTP_CLI_PHASE=2"]),
     "linearPC_multi_open": ("orion_cli.cpp", ["-DTP_CLI_PHASE=3"]),
+    "linearPC_multi_commit_zk": ("orion_cli.cpp", ["-DTP_CLI_PHASE=1", "-DTP_CLI_ZK=1"]),
+    "linearPC_multi_prove_zk": ("orion_cli.cpp", ["-DTP_CLI_PHASE=2", "-DTP_CLI_ZK=1"]),
+    "linearPC_multi_open_zk": ("orion_cli.cpp", ["-DTP_CLI_PHASE=3", "-DTP_CLI_ZK=1"]),
 }
 
 

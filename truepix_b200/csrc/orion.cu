@@ -20,6 +20,7 @@ namespace {
 
 thread_local int g_launches = 0;
 std::atomic<int> g_leaf_chunks{1};   // launches the row-leaf chains are split into
+std::atomic<int> g_gather_cpl{2};    // columns per lane of the 61 x 31-bit gathers of large graphs
 
 // kernel-timer tags (runtime.h timer_*): commit kernels are 9100 + kind
 constexpr int kTagLoad = 9100, kTagGatherBytes = 9101, kTagGather = 9102, kTagLeaf = 9103, kTagTree = 9104;
@@ -472,12 +473,143 @@ __global__ void __launch_bounds__(kLeafRows) sha_peak_kernel(int iters, uint32_t
     atomicXor(out, st[0] ^ st[1] ^ st[2] ^ st[3] ^ st[4] ^ st[5] ^ st[6] ^ st[7]);
 }
 
+// The same gather for weights whose limbs are below 2^31 (Encoder::d_w32). With
+// x = x1 2^32 + x0 canonical (< 2^61) and w < 2^31, x w < 2^92 is accumulated
+// exactly, by multiply-add with carry, into three 32-bit words per partial
+// product (re c, im d, re d, im c for the weight c + d i); every 16 edges each
+// accumulator is folded mod 2^61 - 1 back below 2^62 (16 products of < 2^92 and
+// the fold stay below 2^96). Two 32 x 32 products per 61 x 31 product instead of
+// the four of a full one, and no fold per product.
+struct Acc3 {
+    u32 w0, w1, w2;
+};
+
+__device__ __forceinline__ void mac31(Acc3& a, u64 x, u32 w)
+{
+    const u32 x0 = (u32)x, x1 = (u32)(x >> 32);
+    asm("mad.lo.cc.u32 %0, %3, %5, %0;\n\t"
+        "madc.hi.cc.u32 %1, %3, %5, %1;\n\t"
+        "addc.u32 %2, %2, 0;\n\t"
+        "mad.lo.cc.u32 %1, %4, %5, %1;\n\t"
+        "madc.hi.u32 %2, %4, %5, %2;"
+        : "+r"(a.w0), "+r"(a.w1), "+r"(a.w2)
+        : "r"(x0), "r"(x1), "r"(w));
+}
+
+// the accumulator's value mod p, below 2^61 + 8 (2^64 == 8), stored back into it
+__device__ __forceinline__ u64 settle(Acc3& a)
+{
+    const u64 lo = ((u64)a.w1 << 32) | a.w0;
+    const u64 v = fold61(fold61(lo) + 8ull * a.w2);
+    a.w0 = (u32)v;
+    a.w1 = (u32)(v >> 32);
+    a.w2 = 0;
+    return v;
+}
+
+template <int CPL>
+__global__ void __launch_bounds__(256) gather31_kernel(ulonglong2* __restrict__ rows, long long src_row,
+                                                       long long dst_row, long long n_targets,
+                                                       const unsigned* __restrict__ ptr,
+                                                       const unsigned* __restrict__ esrc,
+                                                       const uint2* __restrict__ ew)
+{
+    constexpr int kWarpsPerTarget = 4 / CPL;
+    const long long gw = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const long long t = gw / kWarpsPerTarget;
+    const int sub = (int)(gw % kWarpsPerTarget);
+    if (t >= n_targets) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned e0 = ptr[t], e1 = ptr[t + 1];
+    const ulonglong2* src = rows + src_row * kColumns + lane + 32 * sub * CPL;
+    Acc3 A[CPL], B[CPL], C[CPL], D[CPL];   // re c, im d, re d, im c
+#pragma unroll
+    for (int k = 0; k < CPL; ++k) A[k] = B[k] = C[k] = D[k] = Acc3{0, 0, 0};
+    for (unsigned eb = e0; eb < e1; eb += 32) {
+        const int cnt = (int)min(32u, e1 - eb);
+        unsigned my_s = 0;
+        uint2 my_w = make_uint2(0, 0);
+        if (lane < cnt) {
+            my_s = esrc[eb + lane];
+            my_w = ew[eb + lane];
+        }
+        for (int h = 0; h < cnt; h += 16) {
+            const int end = min(cnt, h + 16);
+            int j = h;
+            for (; j + 2 <= end; j += 2) {
+                const unsigned s0 = __shfl_sync(0xffffffffu, my_s, j), s1 = __shfl_sync(0xffffffffu, my_s, j + 1);
+                const u32 c0 = __shfl_sync(0xffffffffu, my_w.x, j), d0 = __shfl_sync(0xffffffffu, my_w.y, j);
+                const u32 c1 = __shfl_sync(0xffffffffu, my_w.x, j + 1), d1 = __shfl_sync(0xffffffffu, my_w.y, j + 1);
+                const ulonglong2* p0 = src + (long long)s0 * kColumns;
+                const ulonglong2* p1 = src + (long long)s1 * kColumns;
+                ulonglong2 v0[CPL], v1[CPL];
+#pragma unroll
+                for (int k = 0; k < CPL; ++k) {
+                    v0[k] = ldg16(p0 + 32 * k);
+                    v1[k] = ldg16(p1 + 32 * k);
+                }
+#pragma unroll
+                for (int k = 0; k < CPL; ++k) {
+                    mac31(A[k], v0[k].y, c0);
+                    mac31(B[k], v0[k].x, d0);
+                    mac31(C[k], v0[k].y, d0);
+                    mac31(D[k], v0[k].x, c0);
+                    mac31(A[k], v1[k].y, c1);
+                    mac31(B[k], v1[k].x, d1);
+                    mac31(C[k], v1[k].y, d1);
+                    mac31(D[k], v1[k].x, c1);
+                }
+            }
+            if (j < end) {
+                const unsigned s0 = __shfl_sync(0xffffffffu, my_s, j);
+                const u32 c0 = __shfl_sync(0xffffffffu, my_w.x, j), d0 = __shfl_sync(0xffffffffu, my_w.y, j);
+                const ulonglong2* p0 = src + (long long)s0 * kColumns;
+#pragma unroll
+                for (int k = 0; k < CPL; ++k) {
+                    const ulonglong2 v = ldg16(p0 + 32 * k);
+                    mac31(A[k], v.y, c0);
+                    mac31(B[k], v.x, d0);
+                    mac31(C[k], v.y, d0);
+                    mac31(D[k], v.x, c0);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < CPL; ++k) {
+                settle(A[k]);
+                settle(B[k]);
+                settle(C[k]);
+                settle(D[k]);
+            }
+        }
+    }
+    ulonglong2* dst = rows + (dst_row + t) * kColumns + lane + 32 * sub * CPL;
+#pragma unroll
+    for (int k = 0; k < CPL; ++k) {
+        const u64 a = settle(A[k]), b = settle(B[k]), c = settle(C[k]), d = settle(D[k]);
+        dst[32 * k] = make_ulonglong2(canon61(fold61(c + d)), canon61(fold61(a + (2 * P61 - b))));
+    }
+}
+
 // graphs with fewer targets than this get four warps per target
 constexpr long long kSmallGraph = 8192;
 
 void launch_gather(ulonglong2* rows, long long src_row, long long dst_row, long long n_targets,
-                   const unsigned* ptr, const unsigned* esrc, const ulonglong2* ew, cudaStream_t s)
+                   const unsigned* ptr, const unsigned* esrc, const ulonglong2* ew, const uint2* ew32,
+                   cudaStream_t s)
 {
+    if (ew32) {
+        const int cpl = n_targets < kSmallGraph ? 1 : g_gather_cpl.load();
+        if (cpl == 1)
+            gather31_kernel<1><<<(unsigned)((4 * n_targets + 7) / 8), 256, 0, s>>>(rows, src_row, dst_row,
+                                                                                   n_targets, ptr, esrc, ew32);
+        else if (cpl == 2)
+            gather31_kernel<2><<<(unsigned)((2 * n_targets + 7) / 8), 256, 0, s>>>(rows, src_row, dst_row,
+                                                                                   n_targets, ptr, esrc, ew32);
+        else
+            gather31_kernel<4><<<(unsigned)((n_targets + 7) / 8), 256, 0, s>>>(rows, src_row, dst_row, n_targets,
+                                                                               ptr, esrc, ew32);
+        return;
+    }
     if (n_targets < kSmallGraph)
         gather_kernel<1><<<(unsigned)((4 * n_targets + 7) / 8), 256, 0, s>>>(rows, src_row, dst_row, n_targets,
                                                                              ptr, esrc, ew);
@@ -587,10 +719,20 @@ const Encoder* encoder(long long col_len)
                           "orion graph upload") &&
              !cuda_failed(cudaMemcpy(e->d_w, w.data(), sizeof(ulonglong2) * w.size(), cudaMemcpyHostToDevice),
                           "orion graph upload");
+    bool small = ok && e->n_edges > 0;
+    for (size_t i = 0; small && i < w.size(); ++i) small = w[i].x < (1ull << 31) && w[i].y < (1ull << 31);
+    if (small) {
+        std::vector<uint2> w32(w.size());
+        for (size_t i = 0; i < w.size(); ++i) w32[i] = make_uint2((unsigned)w[i].y, (unsigned)w[i].x);
+        ok = !cuda_failed(cudaMalloc(&e->d_w32, sizeof(uint2) * w32.size()), "orion graph alloc") &&
+             !cuda_failed(cudaMemcpy(e->d_w32, w32.data(), sizeof(uint2) * w32.size(), cudaMemcpyHostToDevice),
+                          "orion graph upload");
+    }
     if (!ok) {
         cudaFree(e->d_ptr);
         cudaFree(e->d_src);
         cudaFree(e->d_w);
+        cudaFree(e->d_w32);
         delete e;
         return nullptr;
     }
@@ -599,6 +741,16 @@ const Encoder* encoder(long long col_len)
 }
 
 int last_launches() { return g_launches; }
+
+bool set_gather_lanes(int columns_per_lane)
+{
+    if (columns_per_lane != 1 && columns_per_lane != 2 && columns_per_lane != 4) {
+        set_error(TP_ERR_ARG, "orion: columns per lane %d not in {1, 2, 4}", columns_per_lane);
+        return false;
+    }
+    g_gather_cpl.store(columns_per_lane);
+    return true;
+}
 
 bool set_leaf_chunks(int n)
 {
@@ -681,7 +833,7 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
         }
         timer_begin(s, kTagGather);
         launch_gather(rows, lv.off, lv.off + lv.n, lv.R, enc.d_ptr + lv.c_ptr, enc.d_src + lv.c_edge,
-                      enc.d_w + lv.c_edge, s);
+                      enc.d_w + lv.c_edge, enc.d_w32 ? enc.d_w32 + lv.c_edge : nullptr, s);
         timer_end(s);
         if (!launch_ok("orion C gather")) return false;
     }
@@ -693,7 +845,7 @@ bool commit(const Encoder& enc, const ulonglong2* src, const PixelInput* px, ulo
         const long long next = lv.off + lv.n;
         timer_begin(s, kTagGather);
         launch_gather(rows, next, next + lv.L, lv.RD, enc.d_ptr + lv.d_ptr, enc.d_src + lv.d_edge,
-                      enc.d_w + lv.d_edge, s);
+                      enc.d_w + lv.d_edge, enc.d_w32 ? enc.d_w32 + lv.d_edge : nullptr, s);
         timer_end(s);
         if (!launch_ok("orion D gather")) return false;
     }

@@ -49,6 +49,11 @@ struct Encoder {
     unsigned* d_ptr = nullptr;         // [n_ptr] first edge of each target (per graph, + 1 end)
     unsigned* d_src = nullptr;         // [n_edges] source row within the graph's source range
     ulonglong2* d_w = nullptr;         // [n_edges] weights {img, real}, canonical
+    // The reference draws each weight limb as rand() % p (prime_field::random,
+    // src/linear_gkr/prime_field.cpp:35-40), so both limbs are below 2^31; when
+    // every weight is, they are also kept as {real, img} 32-bit pairs and the
+    // gathers multiply 61 x 31 bits (d_w32 non-null).
+    uint2* d_w32 = nullptr;            // [n_edges]
 };
 
 // cached per (device, col_len); nullptr and the error set on failure
@@ -144,6 +149,10 @@ bool sha_peak(int blocks, int iters, uint32_t* out, cudaStream_t s);
 // kernels of other streams (latency of a serving loop's rounds), at the cost of
 // n - 1 launches and 64 bytes per row of extra traffic. Same digests for any n.
 bool set_leaf_chunks(int n);
+
+// columns per lane (1, 2, 4; default 2) of the 61 x 31-bit gathers of graphs
+// with 8192 targets or more: 4 warps, 2 or 1 per target; same codewords
+bool set_gather_lanes(int columns_per_lane);
 
 // launches issued by commit() / build_tree() on this thread since the last commit()
 int last_launches();

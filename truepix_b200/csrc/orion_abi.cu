@@ -243,6 +243,12 @@ int tp_orion_set_leaf_chunks(int n)
     return tp::orion::set_leaf_chunks(n) ? 0 : -1;
 }
 
+int tp_orion_set_gather_lanes(int columns_per_lane)
+{
+    tp::clear_error();
+    return tp::orion::set_gather_lanes(columns_per_lane) ? 0 : -1;
+}
+
 int tp_orion_combine_dev(const void* d_rows, long long N, const void* d_r0, void* d_combined, void* d_ctree,
                          void* stream)
 {

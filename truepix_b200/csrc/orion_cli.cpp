@@ -1,27 +1,33 @@
-// linearPC_multi_commit / linearPC_multi_prove / linearPC_multi_open <copies> <userandom>
+// linearPC_multi_{commit,prove,open}[_zk] <copies> <userandom>
 //
-// The three Orion programs TruePix runs as subprocesses
-// (TruePix-main/Orion/Orion_nonzk/examples/multivariate_PC_test_{commit,prove,open}.cpp,
-// called through libTruePix/fp2_link.py:639-651 and run_truepix_prover.py:379-398),
-// over this library: the commit, the opening and the opening's checks run on
-// the device. One source, built once per phase (TP_CLI_PHASE 1 commit, 2
-// prove, 3 open). The process contract is the reference's:
+// The six Orion programs TruePix runs as subprocesses
+// (TruePix-main/Orion/Orion_nonzk/examples/multivariate_PC_test_{commit,prove,open}.cpp
+// and the zero-knowledge Orion_zk ones, called through
+// libTruePix/fp2_link.py:639-651 and run_truepix_prover.py:379-398), over this
+// library: the commits, the openings and the openings' checks run on the
+// device. One source, built once per program (TP_CLI_PHASE 1 commit, 2 prove,
+// 3 open; TP_CLI_ZK 1 for the zero-knowledge commit pair: the masked polynomial
+// and the mask from a seed file, opened over the even and the odd columns). The
+// process contract is the reference's:
 //
 //   arguments    <copies> <userandom>; userandom must be 0 (input.txt)
 //   environment  TRUEPIX_PROTOCOL (fp2-linked-v1 or truepix), TRUEPIX_COPY_SIZE,
 //                TRUEPIX_CONST_IDX, TRUEPIX_CONST_VAL, TRUEPIX_ORION_COMMIT_FILE,
-//                TRUEPIX_GKR_POINT_FILE, TRUEPIX_ORION_MODE, TRUEPIX_ORION_RESULT_FILE
+//                TRUEPIX_GKR_POINT_FILE, TRUEPIX_ORION_MODE, TRUEPIX_ORION_RESULT_FILE,
+//                TRUEPIX_MASK_SEED_FILE
 //   files        input.txt (one copy per line), orion_commit.json (the manifest,
 //                include/truepix/truepix_gkr.h:391-418), the GKR point file
 //                ("<count>" then "<real> <imag>" per coordinate), orion_proof.bin
-//                (src/truepix/orion_proof.cpp:67-95)
+//                or orion_proof_masked.bin + orion_proof_mask.bin
+//                (src/truepix/orion_proof.cpp:67-95), orion_mask_seed.txt
 //   stdout       the lines fp2_link.py parses: "Commit time", "Open time",
 //                "Proof size for tensor IOP ... bytes", "Verification time"
 //   exit status  0 when every check passed
 //
-// Only the TruePix protocol's plain (non-ZK) NIZK path is served: the legacy
-// Y/Cb/Cr benchmark packing (TRUEPIX_PROTOCOL unset) and the interactive Orion
-// mode are refused with a message.
+// Only the TruePix protocol's NIZK path is served: the legacy Y/Cb/Cr benchmark
+// packing (TRUEPIX_PROTOCOL unset) and the interactive Orion mode are refused
+// with a message, and so are zero-knowledge commits of input values above 255
+// (TruePix frames are bytes).
 //
 // EC(y1): the reference's prover and verifier both re-run a GKR proof of the
 // code of the combined message (generate_circuit + zk_verifier::verify,
@@ -47,6 +53,9 @@
 
 #ifndef TP_CLI_PHASE
 #error "TP_CLI_PHASE must be 1 (commit), 2 (prove) or 3 (open)"
+#endif
+#ifndef TP_CLI_ZK
+#define TP_CLI_ZK 0
 #endif
 
 namespace {
@@ -249,7 +258,7 @@ bool root_from_hex(const std::string& hex, unsigned char* d)
 
 std::string manifest_path() { return env_or("TRUEPIX_ORION_COMMIT_FILE", "orion_commit.json"); }
 
-bool write_manifest(const Layout& L, const std::string& root)
+bool write_manifest(const Layout& L, const std::string& root, const std::string& mask_root, bool zk)
 {
     const std::string path = manifest_path();
     FILE* f = fopen(path.c_str(), "w");
@@ -258,14 +267,53 @@ bool write_manifest(const Layout& L, const std::string& root)
         return false;
     }
     const char* e = getenv("TRUEPIX_PROTOCOL");
-    fprintf(f, "{\n  \"protocol\": \"%s\",\n  \"layout\": \"%s\",\n  \"zk\": false,\n  \"copies\": %d,\n"
+    fprintf(f, "{\n  \"protocol\": \"%s\",\n  \"layout\": \"%s\",\n  \"zk\": %s,\n  \"copies\": %d,\n"
                "  \"padded_copies\": %d,\n  \"copy_size\": %d,\n  \"padded_copy_size\": %d,\n  \"const_idx\": %d,\n"
                "  \"const_val\": %d,\n  \"n\": %lld,\n  \"lg_n\": %d,\n  \"masked_root\": \"%s\",\n"
-               "  \"mask_root\": \"\"\n}\n",
-            (e && protocol_ok(e)) ? e : kProtocol, kLayoutId, L.copies, L.padded_copies, L.copy_size,
-            L.padded_copy_size, L.const_idx, L.const_val, L.n, L.lg_n, root.c_str());
+               "  \"mask_root\": \"%s\"\n}\n",
+            (e && protocol_ok(e)) ? e : kProtocol, kLayoutId, zk ? "true" : "false", L.copies, L.padded_copies,
+            L.copy_size, L.padded_copy_size, L.const_idx, L.const_val, L.n, L.lg_n, root.c_str(), mask_root.c_str());
     fclose(f);
-    printf("TruePix: wrote commit manifest %s (zk=false masked_root=%s mask_root=)\n", path.c_str(), root.c_str());
+    printf("TruePix: wrote commit manifest %s (zk=%s masked_root=%s mask_root=%s)\n", path.c_str(),
+           zk ? "true" : "false", root.c_str(), mask_root.c_str());
+    return true;
+}
+
+// ---- the mask seed (Orion_zk include/truepix/truepix_gkr.h:294-329) ---------------
+std::string mask_seed_path() { return env_or("TRUEPIX_MASK_SEED_FILE", "orion_mask_seed.txt"); }
+
+bool mask_seed_read(u64& seed)
+{
+    std::ifstream in(mask_seed_path());
+    if (!in) {
+        fprintf(stderr, "TruePix: cannot open mask seed file %s; run the commit phase (run_fennel_signer.py) first\n",
+                mask_seed_path().c_str());
+        return false;
+    }
+    unsigned long long v = 0;
+    if (!(in >> v)) {
+        fprintf(stderr, "TruePix: malformed mask seed file %s\n", mask_seed_path().c_str());
+        return false;
+    }
+    seed = v;
+    return true;
+}
+
+bool mask_seed_create(u64& seed)
+{
+    std::ifstream urandom("/dev/urandom", std::ios::binary);
+    unsigned long long v = 0;
+    if (!urandom || !urandom.read(reinterpret_cast<char*>(&v), sizeof(v))) {
+        fprintf(stderr, "TruePix: cannot read /dev/urandom for the mask seed\n");
+        return false;
+    }
+    std::ofstream out(mask_seed_path(), std::ios::trunc);
+    if (!out) {
+        fprintf(stderr, "TruePix: cannot write mask seed file %s\n", mask_seed_path().c_str());
+        return false;
+    }
+    out << v << "\n";
+    seed = v;
     return true;
 }
 
@@ -364,29 +412,51 @@ bool upload(Dev& d, const void* h, size_t bytes)
 {
     return alloc(d, bytes) && cuda_ok(cudaMemcpy(d.p, h, bytes, cudaMemcpyHostToDevice), "upload");
 }
+bool download(void* h, const void* d, size_t bytes)
+{
+    return cuda_ok(cudaMemcpy(h, d, bytes, cudaMemcpyDeviceToHost), "download");
+}
 
-// the frame on the device and its commit: rows (cw_len x 128 elements), tree
-struct Frame {
-    Dev pixels, src;   // bytes (small inputs) or the N-element vector {img, real}
+// one committed polynomial: its row-major codeword and Merkle tree on the device
+struct Poly {
     Dev rows, tree;
-    long long msg_len = 0, cw_len = 0, leaves = 0;
     unsigned char root[32];
 };
 
-bool commit_frame(const Layout& L, const Input& in, Frame& F)
+struct Frame {
+    Dev pixels, src;   // the frame's bytes, or (values above 255) its N-element vector {img, real}
+    long long msg_len = 0, cw_len = 0, leaves = 0;
+    Poly plain, masked, mask;
+};
+
+bool sizes(const Layout& L, Frame& F)
 {
     F.msg_len = L.n / kColumns;
     F.cw_len = tp_orion_codeword_len(F.msg_len);
     F.leaves = tp_orion_tree_leaves(L.n);
-    if (F.cw_len <= 0 || F.leaves <= 0) return lib_ok(-1, "codeword size");
-    if (!alloc(F.rows, 16 * (size_t)F.cw_len * kColumns) || !alloc(F.tree, 64 * (size_t)F.leaves)) return false;
+    return (F.cw_len > 0 && F.leaves > 0) || lib_ok(-1, "codeword size");
+}
+bool alloc_poly(const Frame& F, Poly& P)
+{
+    return alloc(P.rows, 16 * (size_t)F.cw_len * kColumns) && alloc(P.tree, 64 * (size_t)F.leaves);
+}
+bool fetch_root(Poly& P) { return download(P.root, P.tree.as<unsigned char>() + 32, 32); }
+bool upload_bytes(const Input& in, Frame& F)
+{
+    std::vector<unsigned char> b(in.vals.size());
+    for (size_t i = 0; i < b.size(); ++i) b[i] = (unsigned char)in.vals[i];
+    return upload(F.pixels, b.data(), b.size());
+}
+
+// commit(): the plain polynomial (truepix_gkr.h layout)
+bool commit_frame(const Layout& L, const Input& in, Frame& F)
+{
+    if (!sizes(L, F) || !alloc_poly(F, F.plain)) return false;
     if (in.small) {
-        std::vector<unsigned char> b(in.vals.size());
-        for (size_t i = 0; i < b.size(); ++i) b[i] = (unsigned char)in.vals[i];
-        if (!upload(F.pixels, b.data(), b.size())) return false;
-        if (!lib_ok(tp_orion_commit_pixels_dev(F.pixels.p, L.copies, L.padded_copies, L.copy_size,
-                                               L.padded_copy_size, L.const_idx, (uint64_t)L.const_val, F.rows.p,
-                                               F.tree.p, nullptr), "commit"))
+        if (!upload_bytes(in, F) ||
+            !lib_ok(tp_orion_commit_pixels_dev(F.pixels.p, L.copies, L.padded_copies, L.copy_size,
+                                               L.padded_copy_size, L.const_idx, (uint64_t)L.const_val,
+                                               F.plain.rows.p, F.plain.tree.p, nullptr), "commit"))
             return false;
     } else {
         std::vector<u64> v(2 * (size_t)L.n, 0);   // {img, real} per element
@@ -395,19 +465,36 @@ bool commit_frame(const Layout& L, const Input& in, Frame& F)
                 v[2 * ((size_t)c * L.padded_copy_size + w) + 1] = in.vals[(size_t)c * L.copy_size + w];
             if (L.const_idx >= 0) v[2 * ((size_t)c * L.padded_copy_size + L.const_idx) + 1] = (u64)L.const_val % P61;
         }
-        if (!upload(F.src, v.data(), 8 * v.size())) return false;
-        if (!lib_ok(tp_orion_commit_dev(F.src.p, L.n, F.rows.p, F.tree.p, nullptr), "commit")) return false;
+        if (!upload(F.src, v.data(), 8 * v.size()) ||
+            !lib_ok(tp_orion_commit_dev(F.src.p, L.n, F.plain.rows.p, F.plain.tree.p, nullptr), "commit"))
+            return false;
     }
-    return cuda_ok(cudaMemcpy(F.root, F.tree.as<unsigned char>() + 32, 32, cudaMemcpyDeviceToHost), "commit root");
+    return fetch_root(F.plain);
 }
 
-// the MLE of the frame's polynomial at the GKR point, LSB first (truepix::mle_gkr,
-// truepix_gkr.h:210-229): out (real, imag)
+// commit_pair(): the masked polynomial and the mask from the seed (Orion_zk)
+bool commit_frame_zk(const Layout& L, const Input& in, u64 seed, Frame& F)
+{
+    if (!in.small) {
+        fprintf(stderr, "TruePix: zero-knowledge commits here take byte inputs (values 0..255)\n");
+        return false;
+    }
+    if (!sizes(L, F) || !alloc_poly(F, F.masked) || !alloc_poly(F, F.mask) || !upload_bytes(in, F)) return false;
+    return lib_ok(tp_orion_commit_zk_pixels_dev(F.pixels.p, L.copies, L.padded_copies, L.copy_size,
+                                                L.padded_copy_size, L.const_idx, (uint64_t)L.const_val, seed,
+                                                F.masked.rows.p, F.masked.tree.p, F.mask.rows.p, F.mask.tree.p,
+                                                nullptr), "commit pair") &&
+           fetch_root(F.masked) && fetch_root(F.mask);
+}
+
+// the MLE of the frame's (plain) polynomial at the GKR point, LSB first
+// (truepix::mle_gkr, truepix_gkr.h:210-229): out (real, imag)
 bool frame_mle(const Layout& L, const Input& in, Frame& F, const std::vector<u64>& pt, u64 out[2])
 {
     Dev z, o;
     if (!upload(z, pt.data(), 8 * pt.size()) || !alloc(o, 16)) return false;
     if (in.small) {
+        if (!F.pixels.p && !upload_bytes(in, F)) return false;
         if (!lib_ok(tp_mle_eval_pixels(F.pixels.p, L.copies, L.padded_copies, L.copy_size, L.padded_copy_size,
                                        L.const_idx, (uint64_t)L.const_val, z.p, o.p, nullptr), "MLE"))
             return false;
@@ -423,7 +510,7 @@ bool frame_mle(const Layout& L, const Input& in, Frame& F, const std::vector<u64
             !lib_ok(tp_mle_eval_base_dev(dx.p, z.p, L.lg_n, o.p, nullptr), "MLE"))
             return false;
     }
-    return cuda_ok(cudaMemcpy(out, o.p, 16, cudaMemcpyDeviceToHost), "MLE");
+    return download(out, o.p, 16);
 }
 
 // r0 (column weights: the point's top 7 coordinates) and r1 (the rest) as LSB-first
@@ -446,11 +533,7 @@ std::vector<u64> swapped(const std::vector<u64>& v)
     }
     return o;
 }
-
-bool same_fe(const u64* a_img_real, const u64 b_real_imag[2])
-{
-    return a_img_real[1] == b_real_imag[0] && a_img_real[0] == b_real_imag[1];
-}
+u64 fsub(u64 a, u64 b) { return a >= b ? a - b : a + P61 - b; }
 
 void write_result(bool ok, const u64 value[2])
 {
@@ -473,32 +556,34 @@ bool nizk_mode()
     return !(m && (!strcmp(m, "interactive") || !strcmp(m, "INTERACTIVE") || !strcmp(m, "interact")));
 }
 
-// ---- the opening (tensor_product_protocol, linearPC.cpp:426-662) -----------------
-// Writes orion_proof.bin; returns the EC(y1) outcome (false also on errors);
-// answer: (real, imag).
-bool open_frame(const Layout& L, Frame& F, const std::vector<u64>& pt, u64 answer[2], double& verify_time)
+// ---- an opening (tensor_product_protocol, linearPC.cpp:426-662; Orion_zk :701-960) ----
+// use_group1 1 and group -1: the plain opening; ZK: the masked polynomial over the
+// even columns (use_group1 1, group 0) or the mask over the odd ones (0, 1).
+// Writes `path`; returns the EC(y1) outcome (false also on errors). answer: (real, imag).
+bool open_poly(const Layout& L, const Frame& F, const Poly& P, int use_group1, int group, const char* path,
+               const std::vector<u64>& pt, u64 answer[2])
 {
     const int qc = query_count();
     const long long msg_len = F.msg_len, cw_len = F.cw_len;
-    printf("Query count %d\nColumn size %d\nNumber of merkle pathes %d\nNumber of field elements %d\n", qc, kColumns,
-           qc, qc * kColumns);
+    if (group < 0)
+        printf("Query count %d\nColumn size %d\nNumber of merkle pathes %d\nNumber of field elements %d\n", qc,
+               kColumns, qc, qc * kColumns);
     std::vector<u64> r0, r1;
     weights(pt, L.lg_n, r0, r1);
-    // the column queries, then the EC(y1) positions: consecutive transcript draws
-    std::vector<long long> q(2 * (size_t)qc);
-    if (!lib_ok(tp_orion_open_queries(F.root, (uint64_t)L.n, 1, r0.data(), kColumns, r1.data(), msg_len, cw_len, -1,
-                                      2 * qc, q.data()), "opening transcript"))
+    std::vector<long long> q(2 * (size_t)qc);   // the column queries, then the EC(y1) positions
+    if (!lib_ok(tp_orion_open_queries2(P.root, (uint64_t)L.n, use_group1, r0.data(), kColumns, r1.data(), msg_len,
+                                       cw_len, group, qc, q.data(), q.data() + qc), "opening transcript"))
         return false;
     Dev d_r0, d_r1, d_q, comb, ctree, ans, cols;
     if (!upload(d_r0, swapped(r0).data(), 8 * r0.size()) || !upload(d_r1, swapped(r1).data(), 8 * r1.size()) ||
         !upload(d_q, q.data(), 8 * q.size()) || !alloc(comb, 16 * (size_t)cw_len) ||
         !alloc(ctree, 64 * (size_t)F.leaves) || !alloc(ans, 16) || !alloc(cols, 16 * (size_t)qc * kColumns))
         return false;
-    if (!lib_ok(tp_orion_combine_dev(F.rows.p, L.n, d_r0.p, comb.p, ctree.p, nullptr), "combine") ||
+    if (!lib_ok(tp_orion_combine_dev(P.rows.p, L.n, d_r0.p, comb.p, ctree.p, nullptr), "combine") ||
         !lib_ok(tp_orion_answer_dev(comb.p, msg_len, d_r1.p, ans.p, nullptr), "answer") ||
-        !lib_ok(tp_orion_query_columns_dev(F.rows.p, L.n, d_q.p, qc, cols.p, nullptr), "queried columns"))
+        !lib_ok(tp_orion_query_columns_dev(P.rows.p, L.n, d_q.p, qc, cols.p, nullptr), "queried columns"))
         return false;
-    // the Merkle nodes of both openings
+    // the Merkle nodes of both trees at the queried leaves
     const int cap = qc * 64;
     std::vector<int> nodes(cap);
     const int nn = tp_orion_path_nodes(F.leaves, q.data(), qc, nodes.data(), cap);
@@ -506,7 +591,7 @@ bool open_frame(const Layout& L, Frame& F, const std::vector<u64>& pt, u64 answe
     Dev d_nodes, com_dig, cmb_dig;
     if (!upload(d_nodes, nodes.data(), 4 * (size_t)nn) || !alloc(com_dig, 32 * (size_t)nn) ||
         !alloc(cmb_dig, 32 * (size_t)nn) ||
-        !lib_ok(tp_orion_gather_nodes_dev(F.tree.p, 2 * F.leaves, d_nodes.p, nn, com_dig.p, nullptr), "Merkle nodes") ||
+        !lib_ok(tp_orion_gather_nodes_dev(P.tree.p, 2 * F.leaves, d_nodes.p, nn, com_dig.p, nullptr), "Merkle nodes") ||
         !lib_ok(tp_orion_gather_nodes_dev(ctree.p, 2 * F.leaves, d_nodes.p, nn, cmb_dig.p, nullptr), "Merkle nodes"))
         return false;
     // EC(y1): the code of the combined message at the second batch of positions
@@ -517,13 +602,10 @@ bool open_frame(const Layout& L, Frame& F, const std::vector<u64>& pt, u64 answe
     std::vector<u64> h_comb(2 * (size_t)cw_len), h_enc(2 * (size_t)cw_len), h_cols(2 * (size_t)qc * kColumns);
     std::vector<unsigned char> h_com(32 * (size_t)nn), h_cmb(32 * (size_t)nn), croot(32);
     u64 h_ans[2];
-    if (!cuda_ok(cudaMemcpy(h_comb.data(), comb.p, 8 * h_comb.size(), cudaMemcpyDeviceToHost), "download") ||
-        !cuda_ok(cudaMemcpy(h_enc.data(), enc.p, 8 * h_enc.size(), cudaMemcpyDeviceToHost), "download") ||
-        !cuda_ok(cudaMemcpy(h_cols.data(), cols.p, 8 * h_cols.size(), cudaMemcpyDeviceToHost), "download") ||
-        !cuda_ok(cudaMemcpy(h_com.data(), com_dig.p, h_com.size(), cudaMemcpyDeviceToHost), "download") ||
-        !cuda_ok(cudaMemcpy(h_cmb.data(), cmb_dig.p, h_cmb.size(), cudaMemcpyDeviceToHost), "download") ||
-        !cuda_ok(cudaMemcpy(croot.data(), ctree.as<unsigned char>() + 32, 32, cudaMemcpyDeviceToHost), "download") ||
-        !cuda_ok(cudaMemcpy(h_ans, ans.p, 16, cudaMemcpyDeviceToHost), "download"))
+    if (!download(h_comb.data(), comb.p, 8 * h_comb.size()) || !download(h_enc.data(), enc.p, 8 * h_enc.size()) ||
+        !download(h_cols.data(), cols.p, 8 * h_cols.size()) || !download(h_com.data(), com_dig.p, h_com.size()) ||
+        !download(h_cmb.data(), cmb_dig.p, h_cmb.size()) ||
+        !download(croot.data(), ctree.as<unsigned char>() + 32, 32) || !download(h_ans, ans.p, 16))
         return false;
     bool result = true;
     for (int i = qc; i < 2 * qc; ++i) {
@@ -537,27 +619,26 @@ bool open_frame(const Layout& L, Frame& F, const std::vector<u64>& pt, u64 answe
     printf("EC(y1) code-switching time %lf\n", ec);
     printf("Proof size for tensor IOP %lld bytes\n", proof_size);
     printf("Proof size for P %lld bytes\n", proof_size);
-    printf("Verification time %lf\n", verify_time + ec);
+    printf("Verification time %lf\n", ec);
     if (!result) return false;
     const long long size = tp_orion_opening_file_size(msg_len, cw_len, qc, nn, nn);
     std::vector<unsigned char> file((size_t)size);
-    if (tp_orion_opening_file(L.n, msg_len, cw_len, h_ans, F.root, croot.data(), q.data(), qc, h_cols.data(),
-                              h_comb.data(), nodes.data(), h_com.data(), nn, nodes.data(), h_cmb.data(), nn, 1,
-                              file.data(), size) != size)
+    if (tp_orion_opening_file(L.n, msg_len, cw_len, h_ans, P.root, croot.data(), q.data(), qc, h_cols.data(),
+                              h_comb.data(), nodes.data(), h_com.data(), nn, nodes.data(), h_cmb.data(), nn,
+                              use_group1, file.data(), size) != size)
         return lib_ok(-1, "opening file");
-    const std::string path = "orion_proof.bin";
-    FILE* f = fopen(path.c_str(), "wb");
+    FILE* f = fopen(path, "wb");
     if (!f || fwrite(file.data(), 1, file.size(), f) != file.size()) {
         if (f) fclose(f);
-        fprintf(stderr, "TruePix: failed to write NIZK proof %s\n", path.c_str());
+        fprintf(stderr, "TruePix: failed to write NIZK proof %s\n", path);
         return false;
     }
     fclose(f);
-    printf("ORION_NIZK_PROOF_BYTES %lld\nORION_NIZK_PROOF_FILE %s\n", size, path.c_str());
+    printf("ORION_NIZK_PROOF_BYTES %lld\nORION_NIZK_PROOF_FILE %s\n", size, path);
     return true;
 }
 
-// ---- the opening's checks (verify_opening_proof, linearPC.cpp:733-879) -------------
+// ---- an opening's checks (verify_opening_proof, linearPC.cpp:733-879; Orion_zk :1037-1200) ----
 struct Reader {
     const std::vector<unsigned char>& b;
     size_t at = 0;
@@ -579,14 +660,14 @@ struct Reader {
     }
 };
 
-// (answer (real, imag), accepted)
-bool verify_frame(const Layout& L, const unsigned char* expected_root, const std::vector<u64>& pt, u64 answer[2],
-                  double& vt, long long& proof_size)
+// accepted?; answer (real, imag); vt: seconds of the checks
+bool verify_poly(const Layout& L, const unsigned char* expected_root, int use_group1, int group, const char* path,
+                 const std::vector<u64>& pt, u64 answer[2], double& vt)
 {
     answer[0] = answer[1] = 0;
     std::vector<unsigned char> b;
     {
-        std::ifstream f("orion_proof.bin", std::ios::binary);
+        std::ifstream f(path, std::ios::binary);
         if (!f) {
             fprintf(stderr, "TruePix: cannot read NIZK proof\n");
             return false;
@@ -599,24 +680,18 @@ bool verify_frame(const Layout& L, const unsigned char* expected_root, const std
     const uint32_t version = R.get<uint32_t>(), group1 = R.get<uint32_t>();
     const u64 N = R.get<u64>(), csize = R.get<u64>(), msg_len = R.get<u64>(), cw_len = R.get<u64>();
     const uint32_t qc = R.get<uint32_t>();
-    (void)group1;
-    const bool head_ok = R.ok && magic && !memcmp(magic, "ORIONPV1", 8) && version == 2 && csize == kColumns &&
-                         msg_len > 0 && msg_len <= (1ULL << 24) && cw_len > 0 && cw_len <= (1ULL << 26) &&
-                         qc <= (1u << 16);
-    if (!head_ok) {
-        fprintf(stderr, "TruePix: cannot read NIZK proof\n");
-        return false;
-    }
     const unsigned char* ans = R.take(16);
     const unsigned char* com_root = R.take(32);
     const unsigned char* cmb_root = R.take(32);
-    const unsigned char* col_q = R.take(8 * (size_t)qc);
-    const unsigned char* cols = R.take(16 * (size_t)qc * kColumns);
-    const unsigned char* combined = R.take(16 * (size_t)cw_len);
-    const unsigned char* message = R.take(16 * (size_t)msg_len);
+    const bool sane = R.ok && !memcmp(magic, "ORIONPV1", 8) && version == 2 && msg_len <= (1ULL << 24) &&
+                      cw_len <= (1ULL << 26) && qc <= (1u << 16);
+    const unsigned char* col_q = sane ? R.take(8 * (size_t)qc) : nullptr;
+    const unsigned char* cols = sane ? R.take(16 * (size_t)qc * kColumns) : nullptr;
+    const unsigned char* combined = sane ? R.take(16 * (size_t)cw_len) : nullptr;
+    const unsigned char* message = sane ? R.take(16 * (size_t)msg_len) : nullptr;
     std::vector<std::pair<uint32_t, const unsigned char*>> com, cmb;
     for (auto* list : {&com, &cmb}) {
-        const u64 n = R.get<u64>();
+        const u64 n = sane ? R.get<u64>() : 0;
         if (!R.ok || n > (1ULL << 24)) { R.ok = false; break; }
         for (u64 i = 0; i < n && R.ok; ++i) {
             const uint32_t idx = R.get<uint32_t>();
@@ -624,11 +699,11 @@ bool verify_frame(const Layout& L, const unsigned char* expected_root, const std
             list->emplace_back(idx, d);
         }
     }
-    if (!R.ok) {
+    if (!sane || !R.ok) {
         fprintf(stderr, "TruePix: cannot read NIZK proof\n");
         return false;
     }
-    if (N != (u64)L.n) {
+    if (N != (u64)L.n || csize != kColumns || (TP_CLI_ZK && group1 != (uint32_t)use_group1)) {
         fprintf(stderr, "TruePix: proof layout mismatch\n");
         return false;
     }
@@ -641,8 +716,13 @@ bool verify_frame(const Layout& L, const unsigned char* expected_root, const std
     std::vector<u64> r0, r1;
     weights(pt, L.lg_n, r0, r1);
     std::vector<long long> q(2 * (size_t)qc);
-    if (!lib_ok(tp_orion_open_queries(com_root, N, 1, r0.data(), kColumns, r1.data(), (long long)msg_len,
-                                      (long long)cw_len, -1, 2 * (int)qc, q.data()), "opening transcript"))
+    if (cw_len < 2 || msg_len != (u64)L.n / kColumns) {
+        fprintf(stderr, "TruePix: proof layout mismatch\n");
+        return false;
+    }
+    if (!lib_ok(tp_orion_open_queries2(com_root, N, use_group1, r0.data(), kColumns, r1.data(), (long long)msg_len,
+                                       (long long)cw_len, group, (int)qc, q.data(), q.data() + qc),
+                "opening transcript"))
         return false;
     for (uint32_t i = 0; i < qc; ++i) {
         long long got;
@@ -653,7 +733,7 @@ bool verify_frame(const Layout& L, const unsigned char* expected_root, const std
         }
     }
     const double t0 = now();
-    // sibling lists sorted by node index; the first entry of an index wins
+    // sibling lists sorted by node index; the first entry of an index wins (as a map would)
     auto sorted = [](std::vector<std::pair<uint32_t, const unsigned char*>>& v, std::vector<uint32_t>& idx,
                      std::vector<unsigned char>& dig) {
         std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
@@ -667,7 +747,7 @@ bool verify_frame(const Layout& L, const unsigned char* expected_root, const std
     std::vector<unsigned char> com_dig, cmb_dig;
     sorted(com, com_idx, com_dig);
     sorted(cmb, cmb_idx, cmb_dig);
-    if (com_idx.empty() || cmb_idx.empty()) {
+    if (qc == 0 || com_idx.empty() || cmb_idx.empty()) {
         fprintf(stderr, "TruePix: NIZK Merkle verify failed\n");
         return false;
     }
@@ -680,7 +760,7 @@ bool verify_frame(const Layout& L, const unsigned char* expected_root, const std
         !upload(d_bi, cmb_idx.data(), 4 * cmb_idx.size()) || !upload(d_bd, cmb_dig.data(), cmb_dig.size()) ||
         !alloc(d_flags, 4 * (size_t)qc))
         return false;
-    // the answer from the proof's combined message, and EC(y1): its code
+    // the answer from the proof's combined message; EC(y1): its code at the second batch
     if (!lib_ok(tp_orion_answer_dev(d_msg.p, (long long)msg_len, d_r1.p, d_ans.p, nullptr), "answer") ||
         !lib_ok(tp_orion_encode_dev(d_msg.p, (long long)msg_len, d_enc.p, nullptr), "EC(y1)") ||
         !lib_ok(tp_orion_verify_opening_dev((long long)msg_len, (long long)cw_len, d_r0.p, d_q.p,
@@ -691,9 +771,7 @@ bool verify_frame(const Layout& L, const unsigned char* expected_root, const std
         return false;
     std::vector<int> flags(qc);
     u64 re_ans[2];
-    if (!cuda_ok(cudaMemcpy(flags.data(), d_flags.p, 4 * (size_t)qc, cudaMemcpyDeviceToHost), "download") ||
-        !cuda_ok(cudaMemcpy(re_ans, d_ans.p, 16, cudaMemcpyDeviceToHost), "download"))
-        return false;
+    if (!download(flags.data(), d_flags.p, 4 * (size_t)qc) || !download(re_ans, d_ans.p, 16)) return false;
     vt = now() - t0;
     // the reference's order: per query the column, then both paths; then the answer
     for (uint32_t i = 0; i < qc; ++i) {
@@ -713,7 +791,8 @@ bool verify_frame(const Layout& L, const unsigned char* expected_root, const std
     bool ec_ok = true;
     for (uint32_t i = 0; i < qc; ++i) ec_ok &= !(flags[i] & 8);
     if (!ec_ok) fprintf(stderr, "TruePix: EC(y1) code check failed\n");
-    proof_size = 32LL * (long long)(com.size() + cmb.size()) + (long long)qc * kColumns * 16 + (long long)qc * 16;
+    const long long proof_size =
+        32LL * (long long)(com_idx.size() + cmb_idx.size()) + (long long)qc * kColumns * 16 + (long long)qc * 16;
     printf("EC(y1) code-switching time %lf\n", vt);
     printf("Proof size for tensor IOP %lld bytes\n", proof_size);
     printf("Verification time %lf\n", vt);
@@ -728,6 +807,186 @@ bool device_ready()
         return false;
     }
     return true;
+}
+
+bool root_matches(const Poly& P, const std::string& want, const char* label)
+{
+    const std::string got = root_hex(P.root);
+    if (got == want) return true;
+    if (label)
+        fprintf(stderr, "TruePix: %s Merkle root mismatch\n  committed: %s\n  manifest:  %s\n", label, got.c_str(),
+                want.c_str());
+    else
+        fprintf(stderr, "TruePix: Merkle root mismatch\n  committed: %s\n  manifest:  %s\n", got.c_str(), want.c_str());
+    return false;
+}
+
+// ---- the phases -------------------------------------------------------------------
+int run_commit(const Layout& lay)
+{
+    Input in;
+    if (!load_input("input.txt", lay, in)) return 1;
+    Frame F;
+    if (TP_CLI_ZK) {
+        u64 seed = 0;
+        if (!mask_seed_create(seed) || !device_ready()) return 1;
+        printf("Running fused mask commit...\n");
+        const double t0 = now();
+        if (!commit_frame_zk(lay, in, seed, F)) return 1;
+        printf("Commit time(mask): %lf\n", now() - t0);
+        return write_manifest(lay, root_hex(F.masked.root), root_hex(F.mask.root), true) ? 0 : 1;
+    }
+    if (!device_ready()) return 1;
+    const double t0 = now();
+    if (!commit_frame(lay, in, F)) return 1;
+    printf("Commit time %lf\n", now() - t0);
+    return write_manifest(lay, root_hex(F.plain.root), "", false) ? 0 : 1;
+}
+
+// manifest, input, (seed), point: the common front of prove and open
+bool front(int phase, const Layout& lay, Manifest& man, Input& in, u64& seed, std::vector<u64>& pt)
+{
+    if (!read_manifest(man)) return false;
+    if (TP_CLI_ZK && !man.zk) {
+        fprintf(stderr, "TruePix: ZK Orion cannot open a non-ZK commitment\n");
+        return false;
+    }
+    if (!TP_CLI_ZK && man.zk) {
+        fprintf(stderr, "TruePix: non-ZK Orion cannot open a ZK commitment\n");
+        return false;
+    }
+    if (!(lay == man.lay)) {
+        fprintf(stderr, "TruePix: layout does not match the commit manifest\n");
+        return false;
+    }
+    if (!load_input("input.txt", lay, in)) return false;
+    if (TP_CLI_ZK && !mask_seed_read(seed)) return false;
+    if (!load_point(lay.lg_n, pt)) {
+        if (phase == 3) fprintf(stderr, "TruePix: refusing to open at a point unrelated to the GKR claim\n");
+        return false;
+    }
+    if (!nizk_mode()) {
+        fprintf(stderr, "TruePix: only the NIZK Orion mode is served (TRUEPIX_ORION_MODE=%s)\n",
+                getenv("TRUEPIX_ORION_MODE"));
+        return false;
+    }
+    return device_ready();
+}
+
+int run_prove(const Layout& lay)
+{
+    Manifest man;
+    Input in;
+    u64 seed = 0, mle[2] = {0, 0};
+    std::vector<u64> pt;
+    if (!front(2, lay, man, in, seed, pt)) return 1;
+    Frame F;
+    if (TP_CLI_ZK) {
+        printf("Running fused mask commit...\n");
+        const double t0 = now();
+        if (!commit_frame_zk(lay, in, seed, F)) return 1;
+        printf("Commit time(mask): %lf\n", now() - t0);
+        if (!frame_mle(lay, in, F, pt, mle)) return 1;
+        const bool root_masked = root_matches(F.masked, man.masked_root, "masked");
+        u64 v_masked[2], v_mask[2];
+        double t1 = now();
+        const bool open_masked = open_poly(lay, F, F.masked, 1, 0, "orion_proof_masked.bin", pt, v_masked);
+        printf("Open time(masked): %lf\nResult: %s\n", now() - t1, open_masked ? "succ" : "fail");
+        const bool root_mask = root_matches(F.mask, man.mask_root, "mask");
+        t1 = now();
+        const bool open_mask = open_poly(lay, F, F.mask, 0, 1, "orion_proof_mask.bin", pt, v_mask);
+        printf("Open time(mask): %lf\nResult: %s\n", now() - t1, open_mask ? "succ" : "fail");
+        const bool consistent = fsub(v_masked[0], v_mask[0]) == mle[0] && fsub(v_masked[1], v_mask[1]) == mle[1];
+        const bool ok = open_masked && open_mask && root_masked && root_mask && consistent;
+        printf("TruePix prove: open_masked=%d open_mask=%d root_masked=%d root_mask=%d mle_consistent=%d -> ok=%d\n",
+               (int)open_masked, (int)open_mask, (int)root_masked, (int)root_mask, (int)consistent, (int)ok);
+        printf(ok ? "check pass\n" : "check notpass\n");
+        return ok ? 0 : 1;
+    }
+    const double t0 = now();
+    if (!commit_frame(lay, in, F)) return 1;
+    printf("Commit time %lf\n", now() - t0);
+    if (!frame_mle(lay, in, F, pt, mle)) return 1;
+    const bool root_ok = root_matches(F.plain, man.masked_root, nullptr);
+    const double t1 = now();
+    u64 value[2] = {0, 0};
+    const bool opened = open_poly(lay, F, F.plain, 1, -1, "orion_proof.bin", pt, value);
+    printf("Open time %lf\n", now() - t1);
+    printf("%s\n", opened ? "succ" : "fail");
+    const bool consistent = value[0] == mle[0] && value[1] == mle[1];
+    const bool ok = opened && root_ok && consistent;
+    printf("TruePix prove: open=%d root=%d mle_consistent=%d -> ok=%d\n", (int)opened, (int)root_ok,
+           (int)consistent, (int)ok);
+    printf(ok ? "check pass\n" : "check notpass\n");
+    return ok ? 0 : 1;
+}
+
+int run_open(const Layout& lay)
+{
+    Manifest man;
+    Input in;
+    u64 seed = 0, mle[2] = {0, 0}, value[2] = {0, 0};
+    std::vector<u64> pt;
+    if (!front(3, lay, man, in, seed, pt)) return 1;
+    Frame F;   // the plaintext MLE only; nothing is committed here
+    const double tm = now();
+    if (!frame_mle(lay, in, F, pt, mle)) return 1;
+    const double mle_seconds = now() - tm;
+    bool ok;
+    if (TP_CLI_ZK) {
+        u64 v[2][2] = {{0, 0}, {0, 0}};
+        bool opened[2] = {false, false}, root_ok[2] = {false, false};
+        const char* labels[2] = {"masked", "mask"};
+        const char* files[2] = {"orion_proof_masked.bin", "orion_proof_mask.bin"};
+        const std::string* roots[2] = {&man.masked_root, &man.mask_root};
+        for (int k = 0; k < 2; ++k) {
+            printf(k == 0 ? "Running with mask...\n" : "Running without mask...\n");
+            unsigned char expected[32];
+            if (!root_from_hex(*roots[k], expected)) {
+                fprintf(stderr, "TruePix: %s invalid root hex in manifest\n", labels[k]);
+                continue;
+            }
+            root_ok[k] = true;
+            double vt = 0;
+            const double t1 = now();
+            opened[k] = verify_poly(lay, expected, k == 0 ? 1 : 0, k, files[k], pt, v[k], vt);
+            printf("Open time(%s): %lf\nResult: %s\n", labels[k], now() - t1, opened[k] ? "succ" : "fail");
+        }
+        value[0] = fsub(v[0][0], v[1][0]);
+        value[1] = fsub(v[0][1], v[1][1]);
+        const bool consistent = value[0] == mle[0] && value[1] == mle[1];
+        if (!consistent)
+            fprintf(stderr, "TruePix: verified opening %llu+%llui disagrees with the plaintext MLE %llu+%llui\n",
+                    (unsigned long long)value[0], (unsigned long long)value[1], (unsigned long long)mle[0],
+                    (unsigned long long)mle[1]);
+        printf("MLE evaluation time %f\n", mle_seconds);
+        ok = opened[0] && opened[1] && root_ok[0] && root_ok[1] && consistent;
+        printf("TruePix open: children=1 open_masked=%d open_mask=%d root_masked=%d root_mask=%d mle_consistent=%d "
+               "-> ok=%d\n", (int)opened[0], (int)opened[1], (int)root_ok[0], (int)root_ok[1], (int)consistent,
+               (int)ok);
+    } else {
+        unsigned char expected[32];
+        if (!root_from_hex(man.masked_root, expected)) {
+            fprintf(stderr, "TruePix: invalid root hex in manifest\n");
+            return 1;
+        }
+        const double t1 = now();
+        double vt = 0;
+        const bool opened = verify_poly(lay, expected, 1, -1, "orion_proof.bin", pt, value, vt);
+        printf("Open time %lf\n", now() - t1);
+        printf("%s\n", opened ? "succ" : "fail");
+        const bool consistent = value[0] == mle[0] && value[1] == mle[1];
+        if (!consistent)
+            fprintf(stderr, "TruePix: verified opening %llu+%llui disagrees with the plaintext MLE %llu+%llui\n",
+                    (unsigned long long)value[0], (unsigned long long)value[1], (unsigned long long)mle[0],
+                    (unsigned long long)mle[1]);
+        ok = opened && consistent;
+        printf("TruePix open: open=%d root=%d mle_consistent=%d -> ok=%d\n", (int)opened, 1, (int)consistent,
+               (int)ok);
+    }
+    printf(ok ? "check pass\n" : "check notpass\n");
+    write_result(ok, value);
+    return ok ? 0 : 1;
 }
 
 }  // namespace
@@ -747,93 +1006,7 @@ int main(int argc, char** argv)
     }
     Layout lay;
     if (!make_layout(copies, lay)) return 1;
-#if TP_CLI_PHASE == 1
-    Input in;
-    if (!load_input("input.txt", lay, in) || !device_ready()) return 1;
-    Frame F;
-    const double t0 = now();
-    if (!commit_frame(lay, in, F)) return 1;
-    printf("Commit time %lf\n", now() - t0);
-    return write_manifest(lay, root_hex(F.root)) ? 0 : 1;
-#else
-    Manifest man;
-    if (!read_manifest(man)) return 1;
-    if (man.zk) {
-        fprintf(stderr, "TruePix: non-ZK Orion cannot open a ZK commitment\n");
-        return 1;
-    }
-    if (!(lay == man.lay)) {
-        fprintf(stderr, "TruePix: layout does not match the commit manifest\n");
-        return 1;
-    }
-    Input in;
-    if (!load_input("input.txt", lay, in)) return 1;
-    std::vector<u64> pt;
-    if (!load_point(lay.lg_n, pt)) {
-#if TP_CLI_PHASE == 3
-        fprintf(stderr, "TruePix: refusing to open at a point unrelated to the GKR claim\n");
-#endif
-        return 1;
-    }
-    if (!nizk_mode()) {
-        fprintf(stderr, "TruePix: only the NIZK Orion mode is served (TRUEPIX_ORION_MODE=%s)\n",
-                getenv("TRUEPIX_ORION_MODE"));
-        return 1;
-    }
-    if (!device_ready()) return 1;
-    Frame F;
-    u64 mle[2] = {0, 0}, value[2] = {0, 0};
-#if TP_CLI_PHASE == 2
-    const double t0 = now();
-    if (!commit_frame(lay, in, F)) return 1;
-    printf("Commit time %lf\n", now() - t0);
-    if (!frame_mle(lay, in, F, pt, mle)) return 1;
-    const std::string root = root_hex(F.root);
-    const bool root_ok = root == man.masked_root;
-    if (!root_ok)
-        fprintf(stderr, "TruePix: Merkle root mismatch\n  committed: %s\n  manifest:  %s\n", root.c_str(),
-                man.masked_root.c_str());
-    const double t1 = now();
-    double vt = 0;
-    const bool opened = open_frame(lay, F, pt, value, vt);
-    printf("Open time %lf\n", now() - t1);
-    printf("%s\n", opened ? "succ" : "fail");
-    const bool consistent = value[0] == mle[0] && value[1] == mle[1];
-    const bool ok = opened && root_ok && consistent;
-    printf("TruePix prove: open=%d root=%d mle_consistent=%d -> ok=%d\n", (int)opened, (int)root_ok,
-           (int)consistent, (int)ok);
-    printf(ok ? "check pass\n" : "check notpass\n");
-    return ok ? 0 : 1;
-#else
-    // the plaintext MLE needs the frame on the device; nothing is committed here
-    Frame G;
-    if (in.small) {
-        std::vector<unsigned char> b(in.vals.size());
-        for (size_t i = 0; i < b.size(); ++i) b[i] = (unsigned char)in.vals[i];
-        if (!upload(G.pixels, b.data(), b.size())) return 1;
-    }
-    if (!frame_mle(lay, in, G, pt, mle)) return 1;
-    unsigned char expected[32];
-    if (!root_from_hex(man.masked_root, expected)) {
-        fprintf(stderr, "TruePix: invalid root hex in manifest\n");
-        return 1;
-    }
-    const double t1 = now();
-    double vt = 0;
-    long long proof_size = 0;
-    const bool opened = verify_frame(lay, expected, pt, value, vt, proof_size);
-    printf("Open time %lf\n", now() - t1);
-    printf("%s\n", opened ? "succ" : "fail");
-    const bool consistent = value[0] == mle[0] && value[1] == mle[1];
-    if (!consistent)
-        fprintf(stderr, "TruePix: verified opening %llu+%llui disagrees with the plaintext MLE %llu+%llui\n",
-                (unsigned long long)value[0], (unsigned long long)value[1], (unsigned long long)mle[0],
-                (unsigned long long)mle[1]);
-    const bool ok = opened && consistent;
-    printf("TruePix open: open=%d root=%d mle_consistent=%d -> ok=%d\n", (int)opened, 1, (int)consistent, (int)ok);
-    printf(ok ? "check pass\n" : "check notpass\n");
-    write_result(ok, value);
-    return ok ? 0 : 1;
-#endif
-#endif
+    const int rc = TP_CLI_PHASE == 1 ? run_commit(lay) : TP_CLI_PHASE == 2 ? run_prove(lay) : run_open(lay);
+    fflush(stdout);
+    return rc;
 }

@@ -610,6 +610,13 @@ int tp_orion_open_queries(const unsigned char* root32, uint64_t N, int use_group
                           const uint64_t* r1, long long n_r1, long long cw_len, int group, int count,
                           long long* col_q)
 {
+    return tp_orion_open_queries2(root32, N, use_group1, r0, n_r0, r1, n_r1, cw_len, group, count, col_q, nullptr);
+}
+
+int tp_orion_open_queries2(const unsigned char* root32, uint64_t N, int use_group1, const uint64_t* r0, int n_r0,
+                           const uint64_t* r1, long long n_r1, long long cw_len, int group, int count,
+                           long long* col_q, long long* ec_q)
+{
     tp::clear_error();
     if (!root32 || !r0 || !r1 || !col_q || n_r0 < 1 || n_r1 < 1 || cw_len < 2 || group < -1 || group > 1 ||
         count < 0) {
@@ -639,6 +646,10 @@ int tp_orion_open_queries(const unsigned char* root32, uint64_t N, int use_group
         const uint64_t k = orion_squeeze(t) % size;
         col_q[i] = group < 0 ? (long long)k : 2 * (long long)k + group;
     }
+    // the EC(y1) positions: the next draws, over the whole codeword
+    // (linearPC.cpp:573-575; Orion_zk linearPC.cpp:879-880)
+    if (ec_q)
+        for (int i = 0; i < count; ++i) ec_q[i] = (long long)(orion_squeeze(t) % (uint64_t)cw_len);
     return 0;
 }
 

@@ -84,6 +84,7 @@ GKR_SIGNATURES = {
     "tp_orion_commit_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _VP, _VP, _VP]),
     "tp_orion_commit_pair": (_I32, [_VP, _VP, ctypes.c_longlong, _VP, _VP]),
     "tp_orion_set_leaf_chunks": (_I32, [_I32]),
+    "tp_orion_set_gather_lanes": (_I32, [_I32]),
     "tp_batch_fold_dev": (_I32, [_VP, _VP]),
     "tp_fs_state_bytes": (_I32, []),
     "tp_vole_state_bytes": (_I32, []),
@@ -121,6 +122,12 @@ GKR_SIGNATURES = {
                                   ctypes.c_longlong, ctypes.c_longlong, _VP, _VP, _VP, _I32, _VP]),
     "tp_orion_open_queries": (_I32, [_VP, _U64, _I32, _VP, _I32, _VP, ctypes.c_longlong, ctypes.c_longlong, _I32,
                                      _I32, _VP]),
+    "tp_orion_open_queries2": (_I32, [_VP, _U64, _I32, _VP, _I32, _VP, ctypes.c_longlong, ctypes.c_longlong, _I32,
+                                      _I32, _VP, _VP]),
+    "tp_orion_encode_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP]),
+    "tp_orion_verify_opening_dev": (_I32, [ctypes.c_longlong, ctypes.c_longlong, _VP, _VP, _VP, _I32, _VP, _VP, _VP,
+                                           _VP, _VP, _I32, _VP, _VP, _I32, _VP, _VP, _VP, _VP]),
+    "tp_fft_gkr": (_I32, [_I32, _VP, _VP, _VP, _VP, ctypes.c_char_p]),
     "tp_circuit_out_bits": (_I32, [_I32]),
     "tp_circuit_outputs_pixels_dev": (_I32, [_VP, _I32, _I32, _I32, _I32, _I32, _U64, _I32, _PI32, _PI32, _PI32,
                                             _VP, _VP]),
