@@ -1650,14 +1650,9 @@ def profile_case(name):
         from fp2lib import GPU_LIB, REF_GPU_LIB, Fp2Lib, run_session
         L = FrameLayout.for_frame(H, Wd)
         gt, i0, i1 = circuit()
-        rng = np.random.default_rng(SEED)
-        frame = rng.integers(0, 256, size=L.copies * L.copy_size, dtype=np.uint8)
-        table, _ = host_tables(frame, L)
+        frames, z1, z2, _, chal = make_inputs(np.random.default_rng(SEED), L, 1)
+        table, _ = host_tables(frames[0], L)
         zero = np.zeros_like(table)
-        nb = L.n_copy_bits
-        z1 = rng.integers(0, P61, size=(2, 9), dtype=np.uint64)
-        z2 = rng.integers(0, P61, size=(nb, 2), dtype=np.uint64)
-        chal = [(int(a), int(b)) for a, b in rng.integers(0, P61, size=(nb, 2), dtype=np.uint64)]
         g = [np.ascontiguousarray(x, np.int32) for x in (gt, i0, i1)]
         for path in (REF_GPU_LIB, GPU_LIB):
             lib = Fp2Lib(path)
