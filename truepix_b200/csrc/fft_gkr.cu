@@ -601,7 +601,7 @@ int run(int L, double* v_time, long long* proof_size, double* p_time, int* accep
         rounds_ok(claim, L, rv);
         const fp2 v_v = last_eval(3 + 2 * d, rv[L - 1]);
         const double t = wall();
-        // the closed form of :713-760
+        // the closed form of :709-753
         const int lj = d, lk = L - d - 1;
         const fp2 base = f2mul(omr(ru[lj]), rv[lj]);
         fp2 A0u = f2mul(f2mul(omr(r0[L - 1]), base), alpha), A1u = f2mul(f2mul(omr(r1[L - 1]), base), beta);
