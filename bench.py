@@ -744,7 +744,7 @@ def ours_arm(args, rank, world, local_rank):
         c, w, b, m = bprover.results(B - 1)
         res_ok = bool(c.any() and w.any() and m != (0, 0) and any(committer.root(B - 1)))
 
-    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = ref_gpu = fs_rounds = None
+    ntt = e2e = e2e_ref = cpu = uneven = serving = zk = opening = ref_gpu = fs_rounds = programs = None
     # The side measurements run once, at N = 1 (a scaling run holds every GPU
     # while rank 0 works; it only needs the step's value).
     if extras and not args.skip_ntt:
@@ -760,6 +760,7 @@ def ours_arm(args, rank, world, local_rank):
         e2e_ref = e2e_c_abi(args, lib, frames[0], layout, gt, i0, i1, z1, z2, point, chal)
         ref_gpu = reference_gpu_lib(frames[0], layout, gt, i0, i1, z1, z2, point, chal)
         fs_rounds = transcript_rounds(bprover, pix, z1s, z2s, pts, stream)
+        programs = process_boundaries(frames[0], layout)
     if extras and not args.skip_serving:
         del bprover
         committer.rows = committer.trees = None
@@ -833,7 +834,7 @@ def ours_arm(args, rank, world, local_rank):
             "zk": zk_proved, "zk_device_core": zk,
             "ntt": ntt, "opening": opening, "batched_uneven": uneven, "serving": serving,
             "cpu_baseline": cpu, "e2e_reference_abi": e2e_ref,
-            "reference_gpu_library": ref_gpu, "transcript_rounds": fs_rounds,
+            "reference_gpu_library": ref_gpu, "transcript_rounds": fs_rounds, "process_boundaries": programs,
             "gpu_launches": proved["launches"], "clocks": proved["clocks"],
         }
         if not valid:
@@ -1424,10 +1425,53 @@ def reference_gpu_lib(frame, layout, gt, i0, i1, z1, z2, point, chal, reps=3):
     return out
 
 
+def process_boundaries(frame, layout):
+    """The Orion programs TruePix runs as subprocesses, on one 1080p frame: the
+    reference's linearPC_multi_{commit,prove,open} (built from its sources in
+    oracle/_ref, with its own ./fft_gkr) and ours (truepix_b200/bin), each a fresh
+    process in a scratch directory with input.txt and the point file; wall clock
+    per process, manifest roots and orion_proof.bin bytes compared."""
+    import shutil
+    import tempfile
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from clilib import env_for, lay_out, ours, reference, run, sha256_file
+    if not os.path.exists(reference("linearPC_multi_prove")) or not os.path.exists(reference("linearPC_multi_open")):
+        return {"unavailable": "oracle/_ref reference programs not built"}
+    copies, cs, ci, cv = layout.copies, layout.copy_size, layout.const_idx, layout.const_val
+    rng = np.random.default_rng(SEED + 7)
+    point = rng.integers(0, P61, size=(layout.n_in_bits + layout.n_copy_bits, 2), dtype=np.uint64)
+    out = {"workload": "one 1080p frame (%d copies of %d bytes), gray layout; fresh process per phase" % (copies, cs)}
+    files = {}
+    for who, prog, fft in (("reference", reference, reference("fft_gkr")), ("ours", ours, ours("fft_gkr"))):
+        d = tempfile.mkdtemp(prefix="tp_programs_")
+        try:
+            lay_out(d, frame, copies, cs, [(int(a), int(b)) for a, b in point])
+            os.symlink(fft, os.path.join(d, "fft_gkr"))
+            env = env_for(d, cs, ci, cv, TRUEPIX_ORION_RESULT_FILE=os.path.join(d, "result.json"))
+            t = {}
+            for phase in ("commit", "prove", "open"):
+                t0 = time.perf_counter()
+                r = run(prog("linearPC_multi_" + phase), d, env, copies, 0, timeout=1800)
+                t[phase + "_s"] = time.perf_counter() - t0
+                if r.returncode != 0 or "check pass" not in r.stdout and phase != "commit":
+                    return {"unavailable": "%s %s failed: %s" % (who, phase, (r.stdout + r.stderr)[-300:])}
+            files[who] = (json.load(open(os.path.join(d, "orion_commit.json")))["masked_root"],
+                          sha256_file(os.path.join(d, "orion_proof.bin")),
+                          json.load(open(os.path.join(d, "result.json"))))
+            out[who] = t
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+    out["same_root_proof_and_result"] = files["reference"] == files["ours"]
+    out["reference_over_ours"] = {k: out["reference"][k] / out["ours"][k] for k in out["ours"]}
+    return out
+
+
 def _serving_job(device):
     import torch
     torch.cuda.set_device(device)
-    return batched_uneven(), serving_sweep()
+    uneven = batched_uneven()
+    uneven["graph_early_rounds"] = uneven_graph()
+    return uneven, serving_sweep()
 
 
 def serving_in_own_process(device):
@@ -1591,6 +1635,93 @@ def batched_uneven(seed=4):
             "input_wires_min": wires[0], "input_wires_max": wires[-1], "ticks": ticks,
             "what": "whole proofs (proof container + Orion opening file) of 64 uneven frames, continuous batch "
                     "of 64 slots on device transcripts"}
+
+
+def uneven_graph(seed=4, reps=10):
+    """The early rounds of the same 64 uneven crop-then-gray frames as one CUDA
+    graph per batch (tp_batch_vole_rounds_graph): per round one claim launch per
+    source kind for every frame still in its rounds, one VOLE-committed round on
+    the frames' device transcripts (frames past their last round skip it) and the
+    folds by the drawn challenges; then the finish, beta and MLE. Captured on the
+    first call, replayed after (transcripts and VOLE states reset before each
+    replay, inside the timed region); CUDA events on the batch's stream."""
+    import ctypes
+    import torch
+    from truepix_b200.frame import BatchFrameProver, pack_fp2
+    from truepix_b200.pipeline import correlations_needed
+    from truepix_b200.serving import layout_for
+    rng = np.random.default_rng(seed)
+    gray = serving_circuits()["gray"]
+    heights = [240, 360, 480, 720, 1080]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    layouts, frames = [], []
+    for i in range(64):                 # the draws of batched_uneven: same crops, same bytes
+        h = int(rng.choice(heights))
+        w = (h * 16 + 8) // 9
+        x = np.sort(rng.random(2))
+        y = np.sort(rng.random(2))
+        cw, ch = max(1, int(round((x[1] - x[0]) * w))), max(1, int(round((y[1] - y[0]) * h)))
+        L = layout_for(gray, ch, cw)
+        t = torch.zeros(L.copies * L.copy_size, dtype=torch.uint8, device=dev)
+        t[:ch * cw * 3] = torch.from_numpy(rng.integers(0, 256, size=ch * cw * 3, dtype=np.uint8)).to(dev)
+        _correlations(rng, gray, ch, cw)
+        layouts.append(L)
+        frames.append(t)
+    B = len(layouts)
+    gt, i0, i1 = (np.ascontiguousarray(a, np.int32) for a in (gray.gate_type, gray.in0, gray.in1))
+    zg = [np.stack([rng.integers(0, P61, size=gt.size, dtype=np.uint64),
+                    rng.integers(0, P61, size=gt.size, dtype=np.uint64)]) for _ in range(B)]
+    z2d, ptd = {}, {}
+    for C in sorted({L.padded_copies for L in layouts}):
+        n = sum(1 for L in layouts if L.padded_copies == C)
+        nb = int(np.log2(C))
+        z2d[C] = torch.from_numpy(pack_fp2(rng.integers(0, P61, size=n * nb, dtype=np.uint64),
+                                           rng.integers(0, P61, size=n * nb, dtype=np.uint64))).to(dev)
+        ptd[C] = torch.zeros(2 * n * (9 + nb), dtype=torch.int64, device=dev)
+    stream = torch.cuda.Stream(dev)
+    bp = BatchFrameProver(layouts, gt, i0, i1, stream=stream)
+    lib = bp.lib
+    count = max(correlations_needed(L) for L in layouts)
+    st0 = []
+    for f in range(B):
+        st = ctypes.create_string_buffer(lib.tp_fs_state_bytes())
+        lib.tp_fs_init(st, b"truepix")
+        lib.tp_fs_put_u64s(st, np.array([f], np.uint64).ctypes.data, 1)
+        st0.append(st.raw)
+    vs = ctypes.create_string_buffer(lib.tp_vole_state_bytes())
+    lib.tp_vole_state_init(vs, 0, None)
+    init_st = torch.from_numpy(np.frombuffer(b"".join(st0), np.uint8).copy()).to(dev)
+    init_vs = torch.from_numpy(np.frombuffer(vs.raw * B, np.uint8).copy()).to(dev)
+    d_st, d_vs = init_st.clone(), init_vs.clone()
+    vole = dict(states=d_vs, u=torch.from_numpy(rng.integers(0, P61, size=B * count * 2, dtype=np.uint64).view(
+        np.int64)).to(dev), v=torch.from_numpy(rng.integers(0, P61, size=B * count * 2, dtype=np.uint64).view(
+            np.int64)).to(dev), count=count)
+
+    def once():
+        with torch.cuda.stream(stream):
+            d_st.copy_(init_st, non_blocking=True)
+            d_vs.copy_(init_vs, non_blocking=True)
+            bp.prove(frames, zg, z2d, ptd, None, transcripts=d_st, vole=vole, graph=True)
+
+    for _ in range(3):
+        once()
+    stream.synchronize()
+    l0 = lib.tp_batch_launches(bp.handle)
+    r0 = lib.tp_batch_graph_replays(bp.handle)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        once()
+    e1.record(stream)
+    stream.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    rounds = sorted({L.n_copy_bits for L in layouts})
+    return {"frames_per_s": B / (ms / 1e3), "ms_per_batch": ms, "reps": reps,
+            "graph_replays": lib.tp_batch_graph_replays(bp.handle) - r0,
+            "kernels_per_replay": (lib.tp_batch_launches(bp.handle) - l0) / reps,
+            "rounds_min": rounds[0], "rounds_max": rounds[-1],
+            "what": "the early rounds (VOLE-committed, device transcripts) of the same 64 uneven frames as one "
+                    "CUDA graph per batch, replayed; plus beta and MLE"}
 
 
 def serving_sweep(rates=(100, 250, 500, 1000), n_req=192, seed=5):

@@ -192,15 +192,17 @@ int tp_batch_n_copies(void* batch, int i);
 /* d_wires: frame i at d_wires + 16 * (sum of n_wires of frames < i) bytes -- with equal
  * n_wires simply [n_frames][n_wires] packed Fp2; d_beta: [n_frames] packed Fp2 */
 int tp_batch_finish(void* batch, void* d_wires, void* d_beta);
-/* Every early round of the batch on device transcripts, as one CUDA graph
- * (north_star's graph-captured round launches; no counterpart in the reference,
- * whose session returns to the host every round, native_fp2.cu:676-812): per
+/* Every early round of the batch on device transcripts, as one CUDA graph (no
+ * counterpart in the reference, whose session returns to the host every round,
+ * native_fp2.cu:676-812): per
  * round k the claims of all frames (d_claims + 64 B k bytes, 8 u64 per frame),
  * tp_vole_round_dev's VOLE-committed round on the frames' transcripts and VOLE
  * states (label "sc-<layer>-<k>", challenges d_challenges + 16 B k bytes, proof
  * elements d_proof + 80 B k bytes or NULL), the fold by the drawn challenge;
- * then tp_batch_finish into d_wires / d_beta. All frames need the same number of
- * rounds; the batch's stream must be a stream of the caller's (capture). The
+ * then tp_batch_finish into d_wires / d_beta. Frames of different sizes leave
+ * the loop after their own last round (their claims, challenges and proof
+ * elements of later rounds are not written); the batch's stream must be a
+ * stream of the caller's (capture). The
  * rounds' jobs are planned on the host and uploaded in one copy; the graph is
  * captured on the first call and replayed while the shape and the buffers stay
  * the same (tp_batch_graph_replays counts the launches of a graph). */

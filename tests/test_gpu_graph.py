@@ -1,8 +1,9 @@
 """The batched early rounds on device transcripts as one CUDA graph
 (tp_batch_vole_rounds_graph) against the same rounds launch by launch: the same
 claims, challenges, VOLE proof elements, wires, beta, transcripts and VOLE
-states, on the first call (capture) and on replays with other frames; and the
-round autotuner: measured splits change no value."""
+states, on the first call (capture) and on replays with other frames; an uneven
+batch (frames of different sizes in one graph) against each frame alone; and
+the round autotuner: measured splits change no value."""
 import numpy as np
 import pytest
 
@@ -100,7 +101,7 @@ def test_autotuned_rounds_give_the_same_values():
         np.testing.assert_array_equal(got_g[k], want[k], err_msg=k)
 
 
-def test_graph_needs_a_stream_of_the_callers_and_equal_rounds():
+def test_graph_needs_configured_frames():
     import torch
     from truepix_b200 import native
     from truepix_b200.frame import BatchFrameProver, FrameLayout
@@ -110,6 +111,80 @@ def test_graph_needs_a_stream_of_the_callers_and_equal_rounds():
     bp = BatchFrameProver([FrameLayout(copies=64), FrameLayout(copies=200)], *gates, stream=torch.cuda.Stream())
     buf = torch.zeros(4096, dtype=torch.int64, device="cuda")
     p = buf.data_ptr()
-    # the frames are not configured yet (and would have unequal rounds): rejected before any launch
+    # the frames are not configured yet: rejected before any launch
     assert lib.tp_batch_vole_rounds_graph(bp.handle, p, p, p, p, p, 10, 0, p, None, p, p) == -1
     assert b"round" in lib.tp_last_error()
+
+
+def test_uneven_batch_graph_matches_frames_alone():
+    """frames of different sizes in one graph (each leaves the round loop after its
+    own last round) against each frame proved alone launch by launch: its claims,
+    challenges, VOLE proof elements, wires, beta, transcript and VOLE state"""
+    import ctypes
+    import torch
+    from truepix_b200 import native
+    from truepix_b200.frame import BatchFrameProver, FrameLayout, pack_fp2
+    from truepix_b200.pipeline import correlations_needed
+    from proverlib import circuit
+    lib = native.gkr()
+    gt, i0, i1 = circuit("gray")
+    P = (1 << 61) - 1
+    copies = [300, 70, 1000, 9, 300, 2]
+    layouts = [FrameLayout(copies=c) for c in copies]
+    B = len(layouts)
+    rng = np.random.default_rng(11)
+    frames = [torch.from_numpy(rng.integers(0, 256, size=c * 384, dtype=np.uint8)).cuda() for c in copies]
+    zg = [np.stack([rng.integers(0, P, size=gt.size, dtype=np.uint64),
+                    rng.integers(0, P, size=gt.size, dtype=np.uint64)]) for _ in range(B)]
+    z2 = [rng.integers(0, P, size=(L.n_copy_bits, 2), dtype=np.uint64) for L in layouts]
+    count = max(correlations_needed(L) for L in layouts)
+    u = rng.integers(0, P, size=(B, count, 2), dtype=np.uint64)
+    v = rng.integers(0, P, size=(B, count, 2), dtype=np.uint64)
+    states = []
+    for f in range(B):
+        st = ctypes.create_string_buffer(lib.tp_fs_state_bytes())
+        assert lib.tp_fs_init(st, b"truepix") == 0
+        pre = np.array([f + 3, 5], np.uint64)
+        assert lib.tp_fs_put_u64s(st, pre.ctypes.data, 2) == 0
+        states.append(st.raw)
+    vs0 = ctypes.create_string_buffer(lib.tp_vole_state_bytes())
+    assert lib.tp_vole_state_init(vs0, 0, None) == 0
+
+    def dev_fp2(rows):
+        a = np.concatenate(rows) if rows else np.zeros((0, 2), np.uint64)
+        return torch.from_numpy(pack_fp2(a[:, 0].copy(), a[:, 1].copy())).cuda()
+
+    def run(idx, graph):
+        Ls = [layouts[f] for f in idx]
+        s = torch.cuda.Stream()
+        bp = BatchFrameProver(Ls, gt, i0, i1, stream=s)
+        z2d, ptd = {}, {}
+        for C in sorted({L.padded_copies for L in Ls}):
+            fs = [f for f in idx if layouts[f].padded_copies == C]
+            z2d[C] = dev_fp2([z2[f] for f in fs])
+            ptd[C] = torch.zeros(2 * len(fs) * (9 + int(np.log2(C))), dtype=torch.int64, device="cuda")
+        d_st = torch.from_numpy(np.frombuffer(b"".join(states[f] for f in idx), np.uint8).copy()).cuda()
+        vole = dict(states=torch.from_numpy(np.frombuffer(vs0.raw * len(idx), np.uint8).copy()).cuda(),
+                    u=torch.from_numpy(u[idx].view(np.int64).reshape(-1).copy()).cuda(),
+                    v=torch.from_numpy(v[idx].view(np.int64).reshape(-1).copy()).cuda(), count=count)
+        bp.prove([frames[f] for f in idx], [zg[f] for f in idx], z2d, ptd, None, transcripts=d_st, vole=vole,
+                 graph=graph)
+        s.synchronize()
+        R, n = bp.max_rounds, len(idx)
+        return dict(claims=bp.claims.cpu().numpy().view(np.uint64).reshape(R, n, 8),
+                    chal=bp.device_challenges.cpu().numpy().view(np.uint64).reshape(R, n, 2),
+                    proof=bp.device_proof.cpu().numpy().view(np.uint64).reshape(R, n, 10),
+                    wires=bp.wires.cpu().numpy().view(np.uint64).reshape(n, -1),
+                    beta=bp.fin_beta.cpu().numpy().view(np.uint64).reshape(n, 2),
+                    st=d_st.cpu().numpy().reshape(n, -1), vs=vole["states"].cpu().numpy().reshape(n, -1)), bp
+
+    got, bp = run(list(range(B)), graph=True)
+    assert lib.tp_batch_graph_replays(bp.handle) == 1
+    for f in range(B):
+        want, _ = run([f], graph=False)
+        r = layouts[f].n_copy_bits
+        np.testing.assert_array_equal(got["claims"][:r, f], want["claims"][:r, 0], err_msg="claims %d" % f)
+        np.testing.assert_array_equal(got["chal"][:r, f], want["chal"][:r, 0], err_msg="chal %d" % f)
+        np.testing.assert_array_equal(got["proof"][:r, f], want["proof"][:r, 0], err_msg="proof %d" % f)
+        for k in ("wires", "beta", "st", "vs"):
+            np.testing.assert_array_equal(got[k][f], want[k][0], err_msg="%s %d" % (k, f))

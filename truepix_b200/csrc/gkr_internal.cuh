@@ -147,10 +147,11 @@ bool launch_finish(const Job* d_jobs, int n_jobs, int max_w, cudaStream_t s, int
 // the round kernels' attributes, set once (before a stream capture)
 bool prepare_round_kernels();
 // one VOLE-committed round of n frames on device transcripts (transcript.cu,
-// tp_vole_round_dev's kernel): label at most 32 bytes
+// tp_vole_round_dev's kernel): label at most 32 bytes. d_rounds (device, n
+// ints, optional): frame i takes part only while round k < d_rounds[i]
 bool launch_vole_round_batch(void* d_states, void* d_vole_states, int n, const void* d_claims, const void* d_u,
                              const void* d_v, long long count, const char* label, void* d_chal, void* d_proof,
-                             cudaStream_t s);
+                             cudaStream_t s, const int* d_rounds = nullptr, int k = 0);
 
 // host-side launchers implemented in gkr_pixels.cu / gkr.cu
 bool pixsrc_valid(const PixSrc& px, int n_pad, int W);

@@ -634,19 +634,23 @@ bool batch_vole_rounds_graph(Batch* B, u64* d_claims, void* d_states, void* d_vo
         return false;
     }
     const int nB = (int)B->frames.size();
-    int rounds = -1;
-    for (Frame* f : B->frames) {
+    // rounds per frame; frames of different sizes (uneven batches) leave the
+    // round loop after their own last round: their VOLE round is skipped (the
+    // frame's entry in a device array of rounds) and they get no more claims
+    int rounds = 0;
+    bool uneven = false;
+    std::vector<int> fr_rounds((size_t)nB);
+    for (int i = 0; i < nB; ++i) {
+        Frame* f = B->frames[(size_t)i];
         if (!f->configured || f->n_copies < 2) {
             set_error(TP_ERR_ARG, "every frame of the batch needs at least one round");
             return false;
         }
         int r = 0;
         while ((2 << r) <= f->n_copies) ++r;
-        if (rounds >= 0 && r != rounds) {
-            set_error(TP_ERR_ARG, "the graph path needs frames with the same number of rounds");
-            return false;
-        }
-        rounds = r;
+        fr_rounds[(size_t)i] = r;
+        if (i && r != rounds) uneven = true;
+        rounds = std::max(rounds, r);
     }
     // ---- plan every launch (advances the frames as the launches will)
     std::vector<GraphOp> ops;
@@ -666,7 +670,7 @@ bool batch_vole_rounds_graph(Batch* B, u64* d_claims, void* d_states, void* d_vo
         v.round = k;
         ops.push_back(v);
         for (int i = 0; i < nB; ++i)
-            if (!batch_fold_dev(B, i, d_chal + (size_t)nB * k + i)) return false;
+            if (k < fr_rounds[(size_t)i] && !batch_fold_dev(B, i, d_chal + (size_t)nB * k + i)) return false;
     }
     {
         GraphOp fin;
@@ -696,7 +700,9 @@ bool batch_vole_rounds_graph(Batch* B, u64* d_claims, void* d_states, void* d_vo
         long long job;
     };
     static_assert(sizeof(Patch) == 16, "patch layout (patch_r_kernel's RPatch)");
-    const size_t bytes_jobs = sizeof(Job) * n_jobs, bytes_patch = sizeof(Patch) * std::max<size_t>(1, n_patch);
+    // the patch table, then (uneven batches) the rounds of each frame
+    const size_t bytes_jobs = sizeof(Job) * n_jobs, bytes_patch_only = sizeof(Patch) * std::max<size_t>(1, n_patch);
+    const size_t bytes_patch = bytes_patch_only + (uneven ? sizeof(int) * (size_t)nB : 0);
     if (!grow_dev(B->d_table, B->cap_table, n_jobs, s)) return false;
     {
         unsigned char* pt = static_cast<unsigned char*>(B->d_ptable);
@@ -725,16 +731,21 @@ bool batch_vole_rounds_graph(Batch* B, u64* d_claims, void* d_states, void* d_vo
         for (size_t j = 0; j < op.L.rdev.size(); ++j)
             if (op.L.rdev[j]) hp[q++] = Patch{op.L.rdev[j], (long long)(op.job_off + j)};
     }
+    int* d_rounds = nullptr;
+    if (uneven) {
+        std::memcpy(reinterpret_cast<unsigned char*>(hp) + bytes_patch_only, fr_rounds.data(), sizeof(int) * (size_t)nB);
+        d_rounds = reinterpret_cast<int*>(static_cast<unsigned char*>(B->d_ptable) + bytes_patch_only);
+    }
     TP_CUDA_OK(cudaMemcpyAsync(B->d_table, hj, bytes_jobs, cudaMemcpyHostToDevice, s), "job table");
-    if (n_patch)
-        TP_CUDA_OK(cudaMemcpyAsync(B->d_ptable, hp, sizeof(Patch) * n_patch, cudaMemcpyHostToDevice, s),
-                   "patch table");
+    if (n_patch || uneven)
+        TP_CUDA_OK(cudaMemcpyAsync(B->d_ptable, hp, bytes_patch, cudaMemcpyHostToDevice, s), "patch table");
     TP_CUDA_OK(cudaEventRecord(B->staged, s), "stage event");
     // ---- the graph: captured once per shape, replayed after
     std::vector<long long> key = {(long long)(size_t)s, (long long)(size_t)B->d_table, (long long)(size_t)B->d_ptable,
                                   (long long)(size_t)d_states, (long long)(size_t)d_vole_states,
                                   (long long)(size_t)d_u, (long long)(size_t)d_v, count, layer,
-                                  (long long)(size_t)d_chal, (long long)(size_t)d_proof, (long long)nB};
+                                  (long long)(size_t)d_chal, (long long)(size_t)d_proof, (long long)nB,
+                                  (long long)uneven};
     int kernels = 0;
     for (const GraphOp& op : ops) {
         key.push_back(op.type);
@@ -768,7 +779,8 @@ bool batch_vole_rounds_graph(Batch* B, u64* d_claims, void* d_states, void* d_vo
                 std::snprintf(label, sizeof(label), "sc-%d-%d", layer, op.round);
                 ok = launch_vole_round_batch(d_states, d_vole_states, nB, d_claims + 8 * (size_t)nB * op.round,
                                              d_u, d_v, count, label, d_chal + (size_t)nB * op.round,
-                                             d_proof ? d_proof + 5 * (size_t)nB * op.round : nullptr, s);
+                                             d_proof ? d_proof + 5 * (size_t)nB * op.round : nullptr, s, d_rounds,
+                                             op.round);
                 continue;
             }
             if (op.n_patch) {

@@ -91,14 +91,16 @@ __global__ void rand_ext_kernel(State* __restrict__ st, int n, tp::fs::Label L, 
 // ---- VOLE-committed early round (vole.cuh), one thread per frame ----------------
 using VoleState = tp::vole::State;
 
+// rounds (optional): frame i takes part only while this round k < rounds[i]
 __global__ void vole_round_kernel(State* __restrict__ st, VoleState* __restrict__ vs, int n,
                                   const tp::fp2* __restrict__ claims, const tp::fp2* __restrict__ u,
                                   const tp::fp2* __restrict__ v, long long count, tp::fs::Label L,
-                                  tp::fp2* __restrict__ chal, tp::fp2* __restrict__ proof)
+                                  tp::fp2* __restrict__ chal, tp::fp2* __restrict__ proof,
+                                  const int* __restrict__ rounds, int k)
 {
     using namespace tp;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (rounds && k >= rounds[i])) return;
     VoleState w = vs[i];
     State s = st[i];
     fp2 coef[4];
@@ -377,14 +379,14 @@ namespace tp {
 
 bool launch_vole_round_batch(void* d_states, void* d_vole_states, int n, const void* d_claims, const void* d_u,
                              const void* d_v, long long count, const char* label, void* d_chal, void* d_proof,
-                             cudaStream_t s)
+                             cudaStream_t s, const int* d_rounds, int k)
 {
     fs::Label L;
     if (!make_device_label(label, &L, "vole round")) return false;
     vole_round_kernel<<<(n + 127) / 128, 128, 0, s>>>(
         static_cast<State*>(d_states), static_cast<VoleState*>(d_vole_states), n, static_cast<const fp2*>(d_claims),
         static_cast<const fp2*>(d_u), static_cast<const fp2*>(d_v), count, L, static_cast<fp2*>(d_chal),
-        static_cast<fp2*>(d_proof));
+        static_cast<fp2*>(d_proof), d_rounds, k);
     return !cuda_failed(cudaGetLastError(), "vole round");
 }
 
@@ -708,7 +710,7 @@ int tp_vole_round_dev(void* d_fs_states, void* d_vole_states, int n, const void*
     vole_round_kernel<<<(n + 127) / 128, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         static_cast<State*>(d_fs_states), static_cast<VoleState*>(d_vole_states), n,
         static_cast<const tp::fp2*>(d_claims), static_cast<const tp::fp2*>(d_u), static_cast<const tp::fp2*>(d_v),
-        count, L, static_cast<tp::fp2*>(d_chal), static_cast<tp::fp2*>(d_proof));
+        count, L, static_cast<tp::fp2*>(d_chal), static_cast<tp::fp2*>(d_proof), nullptr, 0);
     return tp::cuda_failed(cudaGetLastError(), "vole round") ? -1 : 0;
 }
 

@@ -260,8 +260,10 @@ class BatchFrameProver:
         device memory (uint8 tensor [B * tp_fs_state_bytes()]): every round, each
         frame's transcript puts its four claims and draws the fold challenge
         rand_ext("sc-<layer>-<round>") on the device (tp_fs_*_dev, tp_batch_fold_dev),
-        with no host round trip; all frames must then have the same number of
-        rounds. The drawn challenges are left in self.device_challenges.
+        with no host round trip; launch by launch all frames must then have the
+        same number of rounds (the graph path below takes uneven batches: a frame
+        leaves after its own last round). The drawn challenges are left in
+        self.device_challenges [round][frame].
         vole: with transcripts, run each round as the reference's VOLE-committed
         round (tp_vole_round_dev): a dict of `states` (uint8 [B * 160], device),
         `u`, `v` (int64 [B * count * 2], device: each frame's correlations) and
@@ -296,9 +298,11 @@ class BatchFrameProver:
                 z1r.ctypes.data, z1i.ctypes.data, pixels[f].data_ptr(), L.copies, L.padded_copies,
                 L.copy_size, L.n_wires, L.const_idx, L.const_val, beta_of[f]), "batch_set_pixels")
         base = self.claims.data_ptr()
+        use_graph = graph and transcripts is not None and vole is not None and self.stream is not None
         if transcripts is not None:
-            if any(L.n_copy_bits != self.max_rounds for L in self.layouts):
-                raise ValueError("device transcripts need frames with the same number of rounds")
+            if not use_graph and any(L.n_copy_bits != self.max_rounds for L in self.layouts):
+                raise ValueError("device transcripts launch by launch need frames with the same number of rounds "
+                                 "(the graph path takes uneven batches)")
             if transcripts.numel() != self.B * lib.tp_fs_state_bytes():
                 raise ValueError("one transcript state per frame")
             if getattr(self, "device_challenges", None) is None:
@@ -310,7 +314,6 @@ class BatchFrameProver:
         else:
             ch = np.ascontiguousarray(challenges, np.uint64)
         l0 = lib.tp_batch_launches(b)
-        use_graph = graph and transcripts is not None and vole is not None and self.stream is not None
         if use_graph:
             native.check(lib, lib.tp_batch_vole_rounds_graph(
                 b, base, transcripts.data_ptr(), vole["states"].data_ptr(), vole["u"].data_ptr(),
