@@ -1769,7 +1769,10 @@ def profile_case(name):
     """A short fixed workload for `ncu` captures (no timing, no JSON line):
     orion = one 1080p Orion commit from bytes, one RS commit of 2^20 elements and
     one 2^24-point forward NTT, through include/orion_gpu.h; proved = two batches of
-    16 1080p frames through the pipelined whole proof."""
+    16 1080p frames through the pipelined whole proof after two warm-up batches
+    (the profiler API brackets the measured two: ncu --profile-from-start off);
+    refgpu = one 1080p frame's GKR session through the native_fp2 C ABI, the
+    reference's CUDA library, then ours."""
     import torch
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from orionlib import elements
@@ -1802,10 +1805,15 @@ def profile_case(name):
         frames, corr = proved_inputs(np.random.default_rng(SEED), L, 16)
         pipe = ProofPipeline(L, gt, i0, i1, batch=16)
         batch = dict(frames_host=frames, pids=list(range(16)), correlations=corr)
+        for _ in pipe.run([batch, batch]):          # the round autotuner and the graph capture
+            pass
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()                 # ncu --profile-from-start off: the steady state only
         for _ in pipe.run([batch, batch]):
             pass
-        pipe.close()
         torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        pipe.close()
         return
     assert name == "orion", name
     lib = native.gkr()

@@ -473,18 +473,19 @@ __global__ void __launch_bounds__(kLeafRows) sha_peak_kernel(int iters, uint32_t
     atomicXor(out, st[0] ^ st[1] ^ st[2] ^ st[3] ^ st[4] ^ st[5] ^ st[6] ^ st[7]);
 }
 
-// The same gather for weights whose limbs are below 2^31 (Encoder::d_w32). With
-// x = x1 2^32 + x0 canonical (< 2^61) and w < 2^31, x w < 2^92 is accumulated
-// exactly, by multiply-add with carry, into three 32-bit words per partial
-// product (re c, im d, re d, im c for the weight c + d i); every 16 edges each
-// accumulator is folded mod 2^61 - 1 back below 2^62 (16 products of < 2^92 and
-// the fold stay below 2^96). Two 32 x 32 products per 61 x 31 product instead of
-// the four of a full one, and no fold per product.
+// The same gather for weights whose limbs are below 2^31 (Encoder::d_w32). For an
+// element x = a + b i (canonical) and a weight c + d i, Karatsuba's three products
+// a c, b d and s (c + d) with s = a + b reduced below p: each is a 61 x 32-bit
+// product (< 2^93), accumulated exactly, by multiply-add with carry, into three
+// 32-bit words (two 32 x 32 multiply-adds per product, no fold per product);
+// every 8 edges each accumulator is folded mod 2^61 - 1 back below 2^61 + 8 (8
+// products below 2^93 and the fold stay below 2^96). The result is
+// (a c - b d) + (s (c + d) - a c - b d) i.
 struct Acc3 {
     u32 w0, w1, w2;
 };
 
-__device__ __forceinline__ void mac31(Acc3& a, u64 x, u32 w)
+__device__ __forceinline__ void mac32(Acc3& a, u64 x, u32 w)
 {
     const u32 x0 = (u32)x, x1 = (u32)(x >> 32);
     asm("mad.lo.cc.u32 %0, %3, %5, %0;\n\t"
@@ -507,6 +508,16 @@ __device__ __forceinline__ u64 settle(Acc3& a)
     return v;
 }
 
+// one edge into the column's accumulators: element v {img, real}, weight c + d i, w = c + d
+__device__ __forceinline__ void edge31(Acc3& A, Acc3& Bd, Acc3& S, ulonglong2 v, u32 c, u32 d, u32 w)
+{
+    u64 sum = v.y + v.x;
+    sum = sum >= P61 ? sum - P61 : sum;
+    mac32(A, v.y, c);
+    mac32(Bd, v.x, d);
+    mac32(S, sum, w);
+}
+
 template <int CPL>
 __global__ void __launch_bounds__(256) gather31_kernel(ulonglong2* __restrict__ rows, long long src_row,
                                                        long long dst_row, long long n_targets,
@@ -522,9 +533,9 @@ __global__ void __launch_bounds__(256) gather31_kernel(ulonglong2* __restrict__ 
     const int lane = threadIdx.x & 31;
     const unsigned e0 = ptr[t], e1 = ptr[t + 1];
     const ulonglong2* src = rows + src_row * kColumns + lane + 32 * sub * CPL;
-    Acc3 A[CPL], B[CPL], C[CPL], D[CPL];   // re c, im d, re d, im c
+    Acc3 A[CPL], Bd[CPL], S[CPL];   // a c, b d, s (c + d)
 #pragma unroll
-    for (int k = 0; k < CPL; ++k) A[k] = B[k] = C[k] = D[k] = Acc3{0, 0, 0};
+    for (int k = 0; k < CPL; ++k) A[k] = Bd[k] = S[k] = Acc3{0, 0, 0};
     for (unsigned eb = e0; eb < e1; eb += 32) {
         const int cnt = (int)min(32u, e1 - eb);
         unsigned my_s = 0;
@@ -533,8 +544,8 @@ __global__ void __launch_bounds__(256) gather31_kernel(ulonglong2* __restrict__ 
             my_s = esrc[eb + lane];
             my_w = ew[eb + lane];
         }
-        for (int h = 0; h < cnt; h += 16) {
-            const int end = min(cnt, h + 16);
+        for (int h = 0; h < cnt; h += 8) {
+            const int end = min(cnt, h + 8);
             int j = h;
             for (; j + 2 <= end; j += 2) {
                 const unsigned s0 = __shfl_sync(0xffffffffu, my_s, j), s1 = __shfl_sync(0xffffffffu, my_s, j + 1);
@@ -550,14 +561,8 @@ __global__ void __launch_bounds__(256) gather31_kernel(ulonglong2* __restrict__ 
                 }
 #pragma unroll
                 for (int k = 0; k < CPL; ++k) {
-                    mac31(A[k], v0[k].y, c0);
-                    mac31(B[k], v0[k].x, d0);
-                    mac31(C[k], v0[k].y, d0);
-                    mac31(D[k], v0[k].x, c0);
-                    mac31(A[k], v1[k].y, c1);
-                    mac31(B[k], v1[k].x, d1);
-                    mac31(C[k], v1[k].y, d1);
-                    mac31(D[k], v1[k].x, c1);
+                    edge31(A[k], Bd[k], S[k], v0[k], c0, d0, c0 + d0);
+                    edge31(A[k], Bd[k], S[k], v1[k], c1, d1, c1 + d1);
                 }
             }
             if (j < end) {
@@ -565,28 +570,21 @@ __global__ void __launch_bounds__(256) gather31_kernel(ulonglong2* __restrict__ 
                 const u32 c0 = __shfl_sync(0xffffffffu, my_w.x, j), d0 = __shfl_sync(0xffffffffu, my_w.y, j);
                 const ulonglong2* p0 = src + (long long)s0 * kColumns;
 #pragma unroll
-                for (int k = 0; k < CPL; ++k) {
-                    const ulonglong2 v = ldg16(p0 + 32 * k);
-                    mac31(A[k], v.y, c0);
-                    mac31(B[k], v.x, d0);
-                    mac31(C[k], v.y, d0);
-                    mac31(D[k], v.x, c0);
-                }
+                for (int k = 0; k < CPL; ++k) edge31(A[k], Bd[k], S[k], ldg16(p0 + 32 * k), c0, d0, c0 + d0);
             }
 #pragma unroll
             for (int k = 0; k < CPL; ++k) {
                 settle(A[k]);
-                settle(B[k]);
-                settle(C[k]);
-                settle(D[k]);
+                settle(Bd[k]);
+                settle(S[k]);
             }
         }
     }
     ulonglong2* dst = rows + (dst_row + t) * kColumns + lane + 32 * sub * CPL;
 #pragma unroll
     for (int k = 0; k < CPL; ++k) {
-        const u64 a = settle(A[k]), b = settle(B[k]), c = settle(C[k]), d = settle(D[k]);
-        dst[32 * k] = make_ulonglong2(canon61(fold61(c + d)), canon61(fold61(a + (2 * P61 - b))));
+        const u64 ac = settle(A[k]), bd = settle(Bd[k]), sw = settle(S[k]);
+        dst[32 * k] = make_ulonglong2(canon61(fold61(sw + (4 * P61 - ac - bd))), canon61(fold61(ac + (2 * P61 - bd))));
     }
 }
 
