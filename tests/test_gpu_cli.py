@@ -12,7 +12,9 @@ root is the reference program's, orion_proof.bin is byte-identical to the one
 the reference's linearPC_multi_prove wrote, our open accepts it and reports the
 opening value, the reference's own linearPC_multi_open (oracle/_ref, where
 present) accepts our file, and both reject the same tampered files with the same
-first message."""
+first message. The zero-knowledge programs (TruePix's default) against the
+reference's prove_zk and open_zk, and inputs beyond a byte against the reference's
+prove programs."""
 import json
 import os
 import struct
@@ -230,3 +232,37 @@ def test_zk_commit_prove_open_round_trip(tmp_path):
         assert rr.returncode == 0 and "check pass" in rr.stdout, rr.stdout[-2000:] + rr.stderr[-2000:]
         for name in ("orion_proof_masked.bin", "orion_proof_mask.bin"):
             assert sha256_file(os.path.join(d, name)) == sha256_file(os.path.join(e, name)), name
+
+
+@pytest.mark.parametrize("zk", [False, True])
+def test_programs_take_values_above_255(tmp_path, zk):
+    """input.txt values beyond a byte (the element-vector path of the commits):
+    our commit, prove and open agree with each other, and the reference's prove
+    program, given our manifest (and seed), passes its root check and writes the
+    same opening files"""
+    if not os.path.exists(reference("linearPC_multi_prove" + ("_zk" if zk else ""))):
+        pytest.skip("oracle/_ref reference programs not built")
+    rng = np.random.default_rng(21)
+    copies, cs, ci, cv = 64, 384, 384, 128
+    vals = rng.integers(0, 5000, size=copies * cs, dtype=np.int64)
+    point = [(int(a), int(b)) for a, b in rng.integers(0, (1 << 61) - 1, size=(15, 2), dtype=np.uint64)]
+    sfx = "_zk" if zk else ""
+    d, e = str(tmp_path / "ours"), str(tmp_path / "ref")
+    os.makedirs(d)
+    os.makedirs(e)
+    lay_out(d, vals, copies, cs, point)
+    env = env_for(d, cs, ci, cv)
+    r = run(ours("linearPC_multi_commit" + sfx), d, env, copies, 0)
+    assert r.returncode == 0, r.stderr
+    r = run(ours("linearPC_multi_prove" + sfx), d, env, copies, 0)
+    assert r.returncode == 0 and "check pass" in r.stdout, r.stdout + r.stderr
+    r = run(ours("linearPC_multi_open" + sfx), d, env, copies, 0)
+    assert r.returncode == 0 and "check pass" in r.stdout, r.stdout + r.stderr
+    for f in ("input.txt", "gkr_point_prover.txt", "orion_commit.json") + (("orion_mask_seed.txt",) if zk else ()):
+        with open(os.path.join(d, f)) as src, open(os.path.join(e, f), "w") as dst:
+            dst.write(src.read())
+    os.symlink(ours("fft_gkr"), os.path.join(e, "fft_gkr"))
+    rr = run(reference("linearPC_multi_prove" + sfx), e, env_for(e, cs, ci, cv), copies, 0)
+    assert rr.returncode == 0 and "check pass" in rr.stdout, rr.stdout[-2000:] + rr.stderr[-2000:]
+    for name in (("orion_proof_masked.bin", "orion_proof_mask.bin") if zk else ("orion_proof.bin",)):
+        assert sha256_file(os.path.join(d, name)) == sha256_file(os.path.join(e, name)), name

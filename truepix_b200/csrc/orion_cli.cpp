@@ -26,8 +26,7 @@
 //
 // Only the TruePix protocol's NIZK path is served: the legacy Y/Cb/Cr benchmark
 // packing (TRUEPIX_PROTOCOL unset) and the interactive Orion mode are refused
-// with a message, and so are zero-knowledge commits of input values above 255
-// (TruePix frames are bytes).
+// with a message.
 //
 // EC(y1): the reference's prover and verifier both re-run a GKR proof of the
 // code of the combined message (generate_circuit + zk_verifier::verify,
@@ -473,17 +472,49 @@ bool commit_frame(const Layout& L, const Input& in, Frame& F)
 }
 
 // commit_pair(): the masked polynomial and the mask from the seed (Orion_zk)
+// splitmix64 (Steele, Lea and Flood's SplitMix generator, 64-bit output)
+u64 splitmix64(u64& state)
+{
+    state += 0x9E3779B97F4A7C15ull;
+    u64 z = state;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// commit_pair(): the masked polynomial and the mask from the seed (Orion_zk). Byte
+// inputs are committed from their bytes (the library draws the mask on the
+// device); other inputs from the two element vectors built here: the mask is zero
+// except at the private wires (copy < copies, wire < copy_size), which take the
+// seed's splitmix64 outputs mod p in flat order (real parts; Orion_zk
+// include/truepix/truepix_gkr.h:339-362), and masked = frame + mask.
 bool commit_frame_zk(const Layout& L, const Input& in, u64 seed, Frame& F)
 {
-    if (!in.small) {
-        fprintf(stderr, "TruePix: zero-knowledge commits here take byte inputs (values 0..255)\n");
-        return false;
+    if (!sizes(L, F) || !alloc_poly(F, F.masked) || !alloc_poly(F, F.mask)) return false;
+    if (in.small) {
+        if (!upload_bytes(in, F)) return false;
+        return lib_ok(tp_orion_commit_zk_pixels_dev(F.pixels.p, L.copies, L.padded_copies, L.copy_size,
+                                                    L.padded_copy_size, L.const_idx, (uint64_t)L.const_val, seed,
+                                                    F.masked.rows.p, F.masked.tree.p, F.mask.rows.p, F.mask.tree.p,
+                                                    nullptr), "commit pair") &&
+               fetch_root(F.masked) && fetch_root(F.mask);
     }
-    if (!sizes(L, F) || !alloc_poly(F, F.masked) || !alloc_poly(F, F.mask) || !upload_bytes(in, F)) return false;
-    return lib_ok(tp_orion_commit_zk_pixels_dev(F.pixels.p, L.copies, L.padded_copies, L.copy_size,
-                                                L.padded_copy_size, L.const_idx, (uint64_t)L.const_val, seed,
-                                                F.masked.rows.p, F.masked.tree.p, F.mask.rows.p, F.mask.tree.p,
-                                                nullptr), "commit pair") &&
+    std::vector<u64> masked(2 * (size_t)L.n, 0), mask(2 * (size_t)L.n, 0);   // {img, real} per element
+    u64 state = seed;
+    for (int c = 0; c < L.copies; ++c) {
+        const size_t base = (size_t)c * L.padded_copy_size;
+        for (int w = 0; w < L.copy_size; ++w) {
+            const u64 m = splitmix64(state) % P61;
+            const u64 x = in.vals[(size_t)c * L.copy_size + w];
+            mask[2 * (base + w) + 1] = m;
+            masked[2 * (base + w) + 1] = x + m >= P61 ? x + m - P61 : x + m;
+        }
+        if (L.const_idx >= 0) masked[2 * (base + L.const_idx) + 1] = (u64)L.const_val % P61;
+    }
+    Dev d_masked, d_mask;
+    return upload(d_masked, masked.data(), 8 * masked.size()) && upload(d_mask, mask.data(), 8 * mask.size()) &&
+           lib_ok(tp_orion_commit_dev(d_masked.p, L.n, F.masked.rows.p, F.masked.tree.p, nullptr), "commit") &&
+           lib_ok(tp_orion_commit_dev(d_mask.p, L.n, F.mask.rows.p, F.mask.tree.p, nullptr), "commit") &&
            fetch_root(F.masked) && fetch_root(F.mask);
 }
 
