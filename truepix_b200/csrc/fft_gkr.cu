@@ -302,6 +302,20 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+// a pair of timing events, destroyed with the scope
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~EventPair()
+    {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+    bool create()
+    {
+        return !cuda_failed(cudaEventCreate(&a), "fft_gkr event") && !cuda_failed(cudaEventCreate(&b), "fft_gkr event");
+    }
+};
+
 bool dalloc(DevBuf& b, size_t bytes, const char* what)
 {
     if (cuda_failed(cudaMalloc(&b.p, bytes), what)) return false;
@@ -444,11 +458,10 @@ int run(int L, double* v_time, long long* proof_size, double* p_time, int* accep
     }
 
     // ---- the prover: every phase's init and rounds, no host round trip
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    EventPair ev;
+    if (!ev.create()) return -1;
     const double t0 = wall();
-    cudaEventRecord(e0, s);
+    cudaEventRecord(ev.a, s);
     ulonglong2 *A = tabA.as<ulonglong2>(), *B = tabB.as<ulonglong2>();
     long long round = 0, phase = 0;
     // runs the rounds of one phase over tables of `len` entries starting in set A;
@@ -508,16 +521,14 @@ int run(int L, double* v_time, long long* proof_size, double* p_time, int* accep
         if (d == L - 1 && cuda_failed(cudaMemcpyAsync(finals, fin2, 6 * fe, cudaMemcpyDeviceToDevice, s), "fft_gkr record"))
             return -1;
     }
-    cudaEventRecord(e1, s);
+    cudaEventRecord(ev.b, s);
     std::vector<ulonglong2> h_rec(rec_elems), h_out(kPolys);
     if (cuda_failed(cudaMemcpyAsync(h_rec.data(), rec.p, fe * rec_elems, cudaMemcpyDeviceToHost, s), "fft_gkr record") ||
         cuda_failed(cudaMemcpyAsync(h_out.data(), outs.p, fe * kPolys, cudaMemcpyDeviceToHost, s), "fft_gkr outputs") ||
         cuda_failed(cudaStreamSynchronize(s), "fft_gkr prover"))
         return -1;
     float dev_ms = 0;
-    cudaEventElapsedTime(&dev_ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    cudaEventElapsedTime(&dev_ms, ev.a, ev.b);
 
     // ---- the verifier's side (host)
     auto el = [&](long long i) { return mk(h_rec[i].y, h_rec[i].x); };
