@@ -59,14 +59,17 @@ class FrameCommitter:
         return self.stream.cuda_stream if self.stream is not None else \
             self.torch.cuda.current_stream(self.dev).cuda_stream
 
-    def commit(self, pixels, join: bool = True, mask_seeds=None, ready=None) -> None:
+    def commit(self, pixels, join: bool = True, mask_seeds=None, ready=None, after=None) -> None:
         """Queue the commits of all frames (pixels: one uint8 device tensor each).
         With side streams and join=False the step's stream does not wait for them
         here (work queued on it next overlaps the commits); call join() later.
         mask_seeds: one 64-bit seed per frame, required (only) for zk.
         ready: optional CUDA events, one per frame, recorded when that frame's
         bytes are in place (e.g. after its host-to-device copy on a copy stream):
-        each frame's commit waits for its own event only."""
+        each frame's commit waits for its own event only.
+        after: optional callable after(f), called with frame f's commit stream
+        current right after that commit is queued (work it queues follows the
+        frame's commit, not the stream's later frames)."""
         if self.zk != (mask_seeds is not None):
             raise ValueError("mask_seeds are given exactly for a zk committer")
         torch, lib, s = self.torch, self.lib, self._s()
@@ -93,6 +96,9 @@ class FrameCommitter:
                     L.const_idx, L.const_val, self.rows[f].data_ptr(), self.trees[f].data_ptr(), fs),
                     "orion commit")
             launches += lib.tp_orion_last_launches()
+            if after is not None:
+                with torch.cuda.stream(self.side[f % len(self.side)] if self.side else main):
+                    after(f)
         self._pending = []
         for q in self.side:
             done = torch.cuda.Event()

@@ -252,19 +252,20 @@ class ProofPipeline:
         slot.frames_dev = frames_dev
         slot.upload_ready = ready
         c = slot.committer
-        c.commit(frames_dev, join=False, mask_seeds=batch.get("mask_seeds") if self.zk else None, ready=ready)
-        # roots back to pinned memory behind each side stream's commits
-        side = c.side or [self.stream]
-        slot.root_events = []
-        for k, q in enumerate(side):
-            with torch.cuda.stream(q):
-                for f in range(k, B, len(side)):
-                    slot.roots[0, f].copy_(c.trees[f][32:64], non_blocking=True)
-                    if self.zk:
-                        slot.roots[1, f].copy_(c.mask_trees[f][32:64], non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(q)
-                slot.root_events.append(ev)
+        # each frame's roots back to pinned memory right behind its own commit, with
+        # an event per frame: a frame's IO task waits for that commit only
+        slot.root_events = [None] * B
+
+        def roots_of(f):
+            slot.roots[0, f].copy_(c.trees[f][32:64], non_blocking=True)
+            if self.zk:
+                slot.roots[1, f].copy_(c.mask_trees[f][32:64], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record()
+            slot.root_events[f] = ev
+
+        c.commit(frames_dev, join=False, mask_seeds=batch.get("mask_seeds") if self.zk else None, ready=ready,
+                 after=roots_of)
         # the main stream joins the commits only when it proves this batch (_finish)
         self.launches_last += c.launches_last
         # IO transcripts on the host threads, two frames per task
@@ -287,8 +288,8 @@ class ProofPipeline:
             states, pix, n_bytes, len(fs), L.copies, L.padded_copies, L.copy_size, L.n_wires, L.const_idx, L.const_val,
             self.G, self.gt.ctypes.data_as(_I32P), self.i0.ctypes.data_as(_I32P), self.i1.ctypes.data_as(_I32P)),
             "tp_fs_put_circuit_outputs_pixels")
-        for ev in slot.root_events:
-            ev.synchronize()
+        for f in fs:
+            slot.root_events[f].synchronize()
         given = slot.batch.get("manifests")
         for f, t in zip(fs, trs):
             if given is not None:
