@@ -809,6 +809,7 @@ def ours_arm(args, rank, world, local_rank):
             "steps": proved["steps"], "warmup": args.warmup, "ms_per_step": proved["ms"] / proved["steps"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u64 (Fp2 over 2^61-1)", "data": "synthetic",
+            "batched_over_plain": (proved["value"] / world / plain_pf["frames_per_s"]) if plain_pf else None,
             "config": {"workload": WORKLOAD, "frame": [H, Wd, 3],
                        "copies": layout.copies, "padded_copies": layout.padded_copies,
                        "wires": layout.padded_copies * layout.n_wires, "early_rounds": nb, "late_rounds": 18,
