@@ -323,6 +323,16 @@ int tp_orion_open_queries(const unsigned char* root32, uint64_t N, int use_group
 int tp_orion_open_queries2(const unsigned char* root32, uint64_t N, int use_group1, const uint64_t* r0, int n_r0,
                            const uint64_t* r1, long long n_r1, long long cw_len, int group, int count,
                            long long* col_q, long long* ec_q);
+/* No counterpart in the reference (its prover opens one polynomial per
+ * process). n (<= 64) independent opening transcripts, each as
+ * tp_orion_open_queries2 with its own root, use_group1, r0, r1, group and
+ * outputs (arrays of n pointers; the sizes are shared), hashed in lockstep pairs:
+ * two SHA-256 chains interleaved keep the x86 SHA unit busier than one. The draws
+ * of each equal tp_orion_open_queries2's for the same arguments. Host only. */
+int tp_orion_open_queries_multi(int n, const unsigned char* const* roots, uint64_t N, const int* use_group1,
+                                const uint64_t* const* r0, int n_r0, const uint64_t* const* r1, long long n_r1,
+                                long long cw_len, const int* groups, int count, long long* const* col_q,
+                                long long* const* ec_q);
 
 /* ---- circuit evaluation: the prover's output vector ----
  * Replaces ArithCircuitIncrementalBuilder.run (libTruePix/arithcircuitbuilder.py:71-108,

@@ -135,3 +135,85 @@ def test_proof_file_layout_round_trip():
     assert list(f["col_q"]) == [1, 2, 3, 4, 39] and list(f["sparse"]) == [2, 1]
     np.testing.assert_array_equal(f["message"], comb[:msg])
     np.testing.assert_array_equal(f["cols"].reshape(-1, 2), cols)
+
+
+def _addrs(arrays):
+    return np.array([a.ctypes.data for a in arrays], np.uint64)
+
+
+def test_library_transcript_draws_single_and_lockstep():
+    """the library's opening transcript (tp_orion_open_queries2 and its lockstep
+    form tp_orion_open_queries_multi: SHA-256 chains hashed in pairs, an odd one
+    alone) against the restatement above: the queried columns of every group and
+    the second batch of draws (the EC(y1) positions), for n = 1..5 transcripts in
+    one call, and
+    the reference's own openings drawn as a lockstep pair"""
+    from truepix_b200 import native
+    lib = native.gkr(require_device=False)
+    rng = np.random.default_rng(11)
+    N, n_r0, n_r1, cw_len, count = 128 * 16, 128, 16, 41, 37
+    specs = []
+    for i in range(5):
+        root = rng.integers(0, 256, 32, dtype=np.uint8)
+        r0 = rng.integers(0, P61, (n_r0, 2), dtype=np.uint64)
+        r1 = rng.integers(0, P61, (n_r1, 2), dtype=np.uint64)
+        specs.append((root, i % 2, r0, r1, (-1, 0, 1)[i % 3]))
+    expect = []
+    for root, g1, r0, r1, group in specs:
+        T = OrionTranscript()
+        T.absorb(b"tensor-open")
+        T.absorb(root.tobytes())
+        T.absorb_u64(N)
+        T.absorb_u64(g1)
+        for re, im in np.concatenate([r0, r1]).tolist():
+            T.absorb_field(re, im)
+        col = query_columns(T, cw_len, group, count)
+        ec = [T.squeeze_index(cw_len) for _ in range(count)]
+        expect.append((col, ec))
+    for (root, g1, r0, r1, group), (col, ec) in zip(specs, expect):
+        q, q2 = np.zeros(count, np.int64), np.zeros(count, np.int64)
+        native.check(lib, lib.tp_orion_open_queries2(root.tobytes(), N, g1, r0.ctypes.data, n_r0, r1.ctypes.data,
+                                                     n_r1, cw_len, group, count, q.ctypes.data, q2.ctypes.data),
+                     "tp_orion_open_queries2")
+        assert q.tolist() == col and q2.tolist() == ec
+    for n in range(1, 6):
+        sp = specs[:n]
+        qs = [np.zeros(count, np.int64) for _ in range(n)]
+        q2s = [np.zeros(count, np.int64) for _ in range(n)]
+        g1s = np.array([s[1] for s in sp], np.int32)
+        groups = np.array([s[4] for s in sp], np.int32)
+        # the pointer arrays stay referenced until the call returns
+        a_root, a_r0, a_r1 = _addrs([s[0] for s in sp]), _addrs([s[2] for s in sp]), _addrs([s[3] for s in sp])
+        a_q, a_q2 = _addrs(qs), _addrs(q2s)
+        native.check(lib, lib.tp_orion_open_queries_multi(n, a_root.ctypes.data, N, g1s.ctypes.data, a_r0.ctypes.data,
+                                                          n_r0, a_r1.ctypes.data, n_r1, cw_len, groups.ctypes.data,
+                                                          count, a_q.ctypes.data, a_q2.ctypes.data),
+                     "tp_orion_open_queries_multi")
+        for (col, ec), q, q2 in zip(expect, qs, q2s):
+            assert q.tolist() == col and q2.tolist() == ec
+    # the zero-knowledge golden openings: the masked polynomial's and the mask's
+    # transcripts of one proof drawn as a pair
+    from truepix_b200.opening import split_point
+    pairs = 0
+    for c in cases():
+        if json.loads(c["layout"].tobytes().decode())[4] is None:
+            continue
+        pt = [(int(a), int(b)) for a, b in c["point"]]
+        c0, c1 = split_point(pt)
+        r0 = np.array(eq(c0), np.uint64)
+        r1 = np.array(eq(c1), np.uint64)
+        hdr = [[int(x) for x in c[tag + "header"]] for tag in ("", "mask_")]
+        assert hdr[0][2] == hdr[1][2] and hdr[0][5] == hdr[1][5]
+        N, cw_len, qc = hdr[0][2], hdr[0][5], hdr[0][6]
+        roots = [np.frombuffer(c[tag + "com_root"].tobytes(), np.uint8).copy() for tag in ("", "mask_")]
+        qs = [np.zeros(qc, np.int64) for _ in range(2)]
+        a_root, a_r0, a_r1, a_q = _addrs(roots), _addrs([r0, r0]), _addrs([r1, r1]), _addrs(qs)
+        g1s, groups = np.array([1, 0], np.int32), np.array([0, 1], np.int32)
+        native.check(lib, lib.tp_orion_open_queries_multi(2, a_root.ctypes.data, N, g1s.ctypes.data, a_r0.ctypes.data,
+                                                          len(r0), a_r1.ctypes.data, len(r1), cw_len,
+                                                          groups.ctypes.data, qc, a_q.ctypes.data, None),
+                     "tp_orion_open_queries_multi")
+        np.testing.assert_array_equal(qs[0], c["col_q"], err_msg=c["name"])
+        np.testing.assert_array_equal(qs[1], c["mask_col_q"], err_msg=c["name"])
+        pairs += 1
+    assert pairs >= 1

@@ -125,10 +125,102 @@ extern "C" __attribute__((target("sha,sse4.1,ssse3"))) void tp_host_sha_ext_mult
     if (c < n) sha_ext_lockstep<1>(h + c, p + c, nblocks, K);
 }
 
+// SHA-256 of N independent 64-byte messages (the Orion transcript's absorbs and
+// draws: each hashes its 32-byte state with up to 32 bytes), digests written as
+// bytes. The second block of a 64-byte message is the constant padding block
+// (0x80, zeros, bit length 512), so its message schedule plus the round
+// constants (pad_wk) is computed once and its rounds need no schedule work; the
+// state stays in registers between the two blocks.
+namespace {
+inline uint32_t rotr32(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+
+struct PadWk {
+    uint32_t wk[64];
+    explicit PadWk(const uint32_t K[64])
+    {
+        uint32_t w[64] = {0x80000000u};
+        w[15] = 512;
+        for (int t = 16; t < 64; ++t) {
+            const uint32_t s0 = rotr32(w[t - 15], 7) ^ rotr32(w[t - 15], 18) ^ (w[t - 15] >> 3);
+            const uint32_t s1 = rotr32(w[t - 2], 17) ^ rotr32(w[t - 2], 19) ^ (w[t - 2] >> 10);
+            w[t] = w[t - 16] + s0 + w[t - 7] + s1;
+        }
+        for (int t = 0; t < 64; ++t) wk[t] = w[t] + K[t];
+    }
+};
+}  // namespace
+
+template <int N>
+__attribute__((target("sha,sse4.1,ssse3"), always_inline)) inline void sha_ext_hash64(const uint8_t* const* in,
+                                                                                      uint8_t* const* out,
+                                                                                      const uint32_t K[64],
+                                                                                      const uint32_t PWK[64])
+{
+    const __m128i bswap = _mm_set_epi64x(0x0c0d0e0f08090a0bULL, 0x0405060700010203ULL);
+    // the initial hash value in the round instruction's lanes: {F E B A}, {H G D C}
+    const __m128i abef_iv = _mm_set_epi32(0x6a09e667, 0xbb67ae85, 0x510e527f, 0x9b05688c);
+    const __m128i cdgh_iv = _mm_set_epi32(0x3c6ef372, 0xa54ff53a, 0x1f83d9ab, 0x5be0cd19);
+    __m128i abef[N], cdgh[N], m[N][4];
+    for (int c = 0; c < N; ++c) {
+        abef[c] = abef_iv;
+        cdgh[c] = cdgh_iv;
+        for (int i = 0; i < 4; ++i)
+            m[c][i] = _mm_shuffle_epi8(_mm_loadu_si128(reinterpret_cast<const __m128i*>(in[c] + 16 * i)), bswap);
+    }
+#pragma GCC unroll 16
+    for (int g = 0; g < 16; ++g) {
+        const __m128i k = _mm_loadu_si128(reinterpret_cast<const __m128i*>(K + 4 * g));
+        for (int c = 0; c < N; ++c) {
+            if (g >= 4) {
+                const __m128i w7 = _mm_alignr_epi8(m[c][(g + 3) & 3], m[c][(g + 2) & 3], 4);
+                m[c][g & 3] = _mm_sha256msg2_epu32(_mm_add_epi32(_mm_sha256msg1_epu32(m[c][g & 3], m[c][(g + 1) & 3]), w7),
+                                                   m[c][(g + 3) & 3]);
+            }
+            const __m128i wk = _mm_add_epi32(m[c][g & 3], k);
+            cdgh[c] = _mm_sha256rnds2_epu32(cdgh[c], abef[c], wk);
+            abef[c] = _mm_sha256rnds2_epu32(abef[c], cdgh[c], _mm_shuffle_epi32(wk, 0x0E));
+        }
+    }
+    __m128i abef1[N], cdgh1[N];
+    for (int c = 0; c < N; ++c) {
+        abef[c] = abef1[c] = _mm_add_epi32(abef[c], abef_iv);
+        cdgh[c] = cdgh1[c] = _mm_add_epi32(cdgh[c], cdgh_iv);
+    }
+#pragma GCC unroll 16
+    for (int g = 0; g < 16; ++g) {
+        const __m128i wk = _mm_loadu_si128(reinterpret_cast<const __m128i*>(PWK + 4 * g));
+        for (int c = 0; c < N; ++c) {
+            cdgh[c] = _mm_sha256rnds2_epu32(cdgh[c], abef[c], wk);
+            abef[c] = _mm_sha256rnds2_epu32(abef[c], cdgh[c], _mm_shuffle_epi32(wk, 0x0E));
+        }
+    }
+    for (int c = 0; c < N; ++c) {
+        abef[c] = _mm_add_epi32(abef[c], abef1[c]);
+        cdgh[c] = _mm_add_epi32(cdgh[c], cdgh1[c]);
+        const __m128i feba = _mm_shuffle_epi32(abef[c], 0x1B);
+        const __m128i dchg = _mm_shuffle_epi32(cdgh[c], 0xB1);
+        const __m128i abcd = _mm_blend_epi16(feba, dchg, 0xF0), efgh = _mm_alignr_epi8(dchg, feba, 8);
+        _mm_storeu_si128(reinterpret_cast<__m128i*>(out[c]), _mm_shuffle_epi8(abcd, bswap));
+        _mm_storeu_si128(reinterpret_cast<__m128i*>(out[c] + 16), _mm_shuffle_epi8(efgh, bswap));
+    }
+}
+
+// n messages of 64 bytes (any n >= 1), in lockstep pairs; out[c]: 32 digest bytes
+extern "C" __attribute__((target("sha,sse4.1,ssse3"))) void tp_host_sha_ext_hash64(const uint8_t* const* in,
+                                                                                   uint8_t* const* out, int n,
+                                                                                   const uint32_t K[64])
+{
+    static const PadWk pad(K);
+    int c = 0;
+    for (; c + 2 <= n; c += 2) sha_ext_hash64<2>(in + c, out + c, K, pad.wk);
+    if (c < n) sha_ext_hash64<1>(in + c, out + c, K, pad.wk);
+}
+
 #else
 
 extern "C" int tp_host_sha_ext_available(void) { return 0; }
 extern "C" void tp_host_sha_ext_blocks(uint32_t*, const uint8_t*, size_t, const uint32_t*) {}
 extern "C" void tp_host_sha_ext_multi(uint32_t* const*, const uint8_t* const*, int, size_t, const uint32_t*) {}
+extern "C" void tp_host_sha_ext_hash64(const uint8_t* const*, uint8_t* const*, int, const uint32_t*) {}
 
 #endif

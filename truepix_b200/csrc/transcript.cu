@@ -8,9 +8,11 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <vector>
 
 #include "gkr_internal.cuh"
+#include "native_fp2.h"
 #include "runtime.h"
 #include "transcript.cuh"
 #include "vole.cuh"
@@ -18,6 +20,7 @@
 
 extern "C" int tp_host_sha_ext_available(void);
 extern "C" void tp_host_sha_ext_blocks(uint32_t h[8], const uint8_t* p, size_t nblocks, const uint32_t K[64]);
+extern "C" void tp_host_sha_ext_hash64(const uint8_t* const* in, uint8_t* const* out, int n, const uint32_t K[64]);
 extern "C" void tp_host_sha_ext_multi(uint32_t* const* h, const uint8_t* const* p, int n, size_t nblocks,
                                       const uint32_t K[64]);
 
@@ -315,6 +318,12 @@ struct OrionFs {
 
 void sha256_64(const uint8_t in[64], uint8_t out[32])
 {
+    if (host_sha_ext()) {       // both blocks in registers, the padding block's schedule precomputed
+        const uint8_t* ip = in;
+        uint8_t* op = out;
+        tp_host_sha_ext_hash64(&ip, &op, 1, kHostTables.k);
+        return;
+    }
     static const uint8_t kPad[64] = {0x80, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
                                      0,    0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
                                      0,    0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0x02, 0};
@@ -328,40 +337,6 @@ void sha256_64(const uint8_t in[64], uint8_t out[32])
         out[4 * i + 2] = (uint8_t)(h[i] >> 8);
         out[4 * i + 3] = (uint8_t)h[i];
     }
-}
-
-void orion_absorb(OrionFs& t, const void* data, size_t n)
-{
-    const uint8_t* p = static_cast<const uint8_t*>(data);
-    while (n > 0) {
-        uint8_t block[64];
-        memset(block, 0, sizeof(block));
-        memcpy(block, t.state, 32);
-        const size_t take = n < 32 ? n : 32;
-        memcpy(block + 32, p, take);
-        sha256_64(block, t.state);
-        p += take;
-        n -= take;
-    }
-    t.used = 32;
-}
-
-uint64_t orion_squeeze(OrionFs& t)
-{
-    if (t.used + 8 > 32) {
-        uint8_t block[64];
-        memset(block, 0, sizeof(block));
-        memcpy(block, t.state, 32);
-        block[32] = 0x01;
-        sha256_64(block, t.pool);
-        block[32] = 0x02;
-        sha256_64(block, t.state);
-        t.used = 0;
-    }
-    uint64_t v;
-    memcpy(&v, t.pool + t.used, 8);
-    t.used += 8;
-    return v;
 }
 
 bool state_ok(const void* state, const char* who)
@@ -619,39 +594,108 @@ int tp_orion_open_queries2(const unsigned char* root32, uint64_t N, int use_grou
                            const uint64_t* r1, long long n_r1, long long cw_len, int group, int count,
                            long long* col_q, long long* ec_q)
 {
+    return tp_orion_open_queries_multi(1, &root32, N, &use_group1, &r0, n_r0, &r1, n_r1, cw_len, &group, count, &col_q,
+                                       ec_q ? &ec_q : nullptr);
+}
+
+int tp_orion_open_queries_multi(int n, const unsigned char* const* roots, uint64_t N, const int* use_group1,
+                                const uint64_t* const* r0, int n_r0, const uint64_t* const* r1, long long n_r1,
+                                long long cw_len, const int* groups, int count, long long* const* col_q,
+                                long long* const* ec_q)
+{
     tp::clear_error();
-    if (!root32 || !r0 || !r1 || !col_q || n_r0 < 1 || n_r1 < 1 || cw_len < 2 || group < -1 || group > 1 ||
-        count < 0) {
+    bool ok = n >= 1 && n <= 64 && roots && use_group1 && r0 && r1 && groups && col_q && n_r0 >= 1 && n_r1 >= 1 &&
+              cw_len >= 2 && count >= 0;
+    for (int c = 0; ok && c < n; ++c)
+        ok = roots[c] && r0[c] && r1[c] && col_q[c] && groups[c] >= -1 && groups[c] <= 1 && (!ec_q || ec_q[c]);
+    if (!ok) {
         tp::set_error(tp::TP_ERR_ARG, "tp_orion_open_queries: bad arguments");
         return -1;
     }
-    OrionFs t;
-    memset(&t, 0, sizeof(t));
+    // the n transcripts take the same steps on their own bytes, their hashes in
+    // lockstep (two SHA-256 chains interleaved keep the SHA unit busier than one)
+    std::vector<OrionFs> t((size_t)n);
+    std::vector<std::array<uint8_t, 64>> blocks((size_t)n);
+    std::vector<const uint8_t*> in((size_t)n);
+    std::vector<uint8_t*> out((size_t)n);
+    for (OrionFs& x : t) memset(&x, 0, sizeof(x));
+    auto hash_all = [&]() {
+        if (host_sha_ext()) {
+            tp_host_sha_ext_hash64(in.data(), out.data(), n, kHostTables.k);
+        } else {
+            for (int c = 0; c < n; ++c) sha256_64(in[(size_t)c], out[(size_t)c]);
+        }
+    };
+    // absorb of `len` <= 32 bytes, chain c's bytes at src(c)
+    auto absorb = [&](auto src, size_t len) {
+        for (int c = 0; c < n; ++c) {
+            uint8_t* b = blocks[(size_t)c].data();
+            memcpy(b, t[(size_t)c].state, 32);
+            memcpy(b + 32, src(c), len);
+            memset(b + 32 + len, 0, 32 - len);
+            in[(size_t)c] = b;
+            out[(size_t)c] = t[(size_t)c].state;
+        }
+        hash_all();
+        for (OrionFs& x : t) x.used = 32;
+    };
     static const char kDom[] = "truepix/orion-fs/v1";
-    orion_absorb(t, kDom, sizeof(kDom) - 1);
     static const char kLabel[] = "tensor-open";
-    orion_absorb(t, kLabel, sizeof(kLabel) - 1);
-    orion_absorb(t, root32, 32);
-    orion_absorb(t, &N, 8);
-    const uint64_t g1 = use_group1 ? 1 : 0;
-    orion_absorb(t, &g1, 8);
+    absorb([&](int) { return (const void*)kDom; }, sizeof(kDom) - 1);
+    absorb([&](int) { return (const void*)kLabel; }, sizeof(kLabel) - 1);
+    absorb([&](int c) { return (const void*)roots[c]; }, 32);
+    absorb([&](int) { return (const void*)&N; }, 8);
+    std::vector<uint64_t> g1((size_t)n);
+    for (int c = 0; c < n; ++c) g1[(size_t)c] = use_group1[c] ? 1 : 0;
+    absorb([&](int c) { return (const void*)&g1[(size_t)c]; }, 8);
     for (int i = 0; i < n_r0; ++i) {
-        orion_absorb(t, r0 + 2 * i, 8);
-        orion_absorb(t, r0 + 2 * i + 1, 8);
+        absorb([&](int c) { return (const void*)(r0[c] + 2 * i); }, 8);
+        absorb([&](int c) { return (const void*)(r0[c] + 2 * i + 1); }, 8);
     }
     for (long long i = 0; i < n_r1; ++i) {
-        orion_absorb(t, r1 + 2 * i, 8);
-        orion_absorb(t, r1 + 2 * i + 1, 8);
+        absorb([&](int c) { return (const void*)(r1[c] + 2 * i); }, 8);
+        absorb([&](int c) { return (const void*)(r1[c] + 2 * i + 1); }, 8);
     }
-    const uint64_t size = group < 0 ? (uint64_t)cw_len : group == 0 ? (uint64_t)(cw_len + 1) / 2 : (uint64_t)cw_len / 2;
+    // draws: every 4th refills each chain's pool (SHA256(state || 0x01 || 0)) and
+    // moves its state on (SHA256(state || 0x02 || 0)), as orion_squeeze
+    auto squeeze = [&](std::vector<uint64_t>& v) {
+        if (t[0].used + 8 > 32) {
+            for (int tag = 1; tag <= 2; ++tag) {
+                for (int c = 0; c < n; ++c) {
+                    uint8_t* b = blocks[(size_t)c].data();
+                    memset(b, 0, 64);
+                    memcpy(b, t[(size_t)c].state, 32);
+                    b[32] = (uint8_t)tag;
+                    in[(size_t)c] = b;
+                    out[(size_t)c] = tag == 1 ? t[(size_t)c].pool : t[(size_t)c].state;
+                }
+                hash_all();
+            }
+            for (OrionFs& x : t) x.used = 0;
+        }
+        for (int c = 0; c < n; ++c) {
+            memcpy(&v[(size_t)c], t[(size_t)c].pool + t[(size_t)c].used, 8);
+            t[(size_t)c].used += 8;
+        }
+    };
+    std::vector<uint64_t> v((size_t)n);
     for (int i = 0; i < count; ++i) {
-        const uint64_t k = orion_squeeze(t) % size;
-        col_q[i] = group < 0 ? (long long)k : 2 * (long long)k + group;
+        squeeze(v);
+        for (int c = 0; c < n; ++c) {
+            const int group = groups[c];
+            const uint64_t size =
+                group < 0 ? (uint64_t)cw_len : group == 0 ? (uint64_t)(cw_len + 1) / 2 : (uint64_t)cw_len / 2;
+            const uint64_t k = v[(size_t)c] % size;
+            col_q[c][i] = group < 0 ? (long long)k : 2 * (long long)k + group;
+        }
     }
     // the EC(y1) positions: the next draws, over the whole codeword
     // (linearPC.cpp:573-575; Orion_zk linearPC.cpp:879-880)
     if (ec_q)
-        for (int i = 0; i < count; ++i) ec_q[i] = (long long)(orion_squeeze(t) % (uint64_t)cw_len);
+        for (int i = 0; i < count; ++i) {
+            squeeze(v);
+            for (int c = 0; c < n; ++c) ec_q[c][i] = (long long)(v[(size_t)c] % (uint64_t)cw_len);
+        }
     return 0;
 }
 

@@ -124,6 +124,8 @@ GKR_SIGNATURES = {
                                      _I32, _VP]),
     "tp_orion_open_queries2": (_I32, [_VP, _U64, _I32, _VP, _I32, _VP, ctypes.c_longlong, ctypes.c_longlong, _I32,
                                       _I32, _VP, _VP]),
+    "tp_orion_open_queries_multi": (_I32, [_I32, _VP, _U64, _VP, _VP, _I32, _VP, ctypes.c_longlong,
+                                           ctypes.c_longlong, _VP, _I32, _VP, _VP]),
     "tp_orion_encode_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _VP]),
     "tp_orion_verify_opening_dev": (_I32, [ctypes.c_longlong, ctypes.c_longlong, _VP, _VP, _VP, _I32, _VP, _VP, _VP,
                                            _VP, _VP, _I32, _VP, _VP, _I32, _VP, _VP, _VP, _VP]),

@@ -383,34 +383,51 @@ class ProofPipeline:
             t.point = [(int(a), int(b)) for a, b in point[f]]
 
     # ---- stage: openings ------------------------------------------------------
-    def _open_host(self, slot: _Slot, f: int, k: int) -> None:
-        """the opening's host part for frame f, polynomial k (0: the commit / the
-        masked polynomial, 1: the mask): eq tables, queried columns, node lists"""
-        lib, L = self.lib, self.layout
-        hb = slot.open_host[f][k]
-        pt = slot.tr[f].point
-        lg = len(pt)
-        c0, c1 = pt[lg - 7:], pt[:lg - 7]
-        r0 = np.empty((COLUMN_SIZE, 2), np.uint64)
-        r1 = np.empty((self.N // COLUMN_SIZE, 2), np.uint64)
-        z0 = np.ascontiguousarray(c0, np.uint64).reshape(-1)
-        z1 = np.ascontiguousarray(c1, np.uint64).reshape(-1)
-        native.check(lib, lib.tp_eq_table_host(z0.ctypes.data, len(c0), r0.ctypes.data), "eq table")
-        native.check(lib, lib.tp_eq_table_host(z1.ctypes.data, len(c1), r1.ctypes.data), "eq table")
-        root = slot.roots[k, f].numpy().tobytes()
-        group = -1 if not self.zk else k
-        q = hb["q"].numpy()
-        native.check(lib, lib.tp_orion_open_queries(root, self.N, 0 if k == 1 else 1, r0.ctypes.data, len(r0),
-                                                    r1.ctypes.data, len(r1), self.cw_len, group, self.qc,
-                                                    q.ctypes.data), "tp_orion_open_queries")
-        hb["r0"].numpy().view(np.uint64).reshape(-1, 2)[:] = r0[:, ::-1]     # (img, real): the codeword's order
-        hb["r1"].numpy().view(np.uint64).reshape(-1, 2)[:] = r1[:, ::-1]
-        if self.qc and (q.min() < 0 or q.max() >= self.cw_len):
-            raise IndexError("queried column outside the codeword")
-        # the same positions open both trees: one node list
-        hb["n_nodes"] = lib.tp_orion_path_nodes(self.leaves, q.ctypes.data, self.qc, hb["idx"].numpy().ctypes.data,
-                                                slot.max_nodes)
-        native.check(lib, 0 if hb["n_nodes"] >= 0 else -1, "tp_orion_path_nodes")
+    def _open_host(self, slot: _Slot, items) -> None:
+        """the opening's host part for the (frame, polynomial) pairs `items`
+        (polynomial 0: the commit / the masked polynomial, 1: the mask): eq tables
+        (once per frame), queried columns, node lists. The items' opening
+        transcripts are hashed in lockstep (tp_orion_open_queries_multi)."""
+        lib = self.lib
+        eq = {}
+        for f, _ in items:
+            if f in eq:
+                continue
+            pt = slot.tr[f].point
+            lg = len(pt)
+            c0, c1 = pt[lg - 7:], pt[:lg - 7]
+            r0 = np.empty((COLUMN_SIZE, 2), np.uint64)
+            r1 = np.empty((self.N // COLUMN_SIZE, 2), np.uint64)
+            z0 = np.ascontiguousarray(c0, np.uint64).reshape(-1)
+            z1 = np.ascontiguousarray(c1, np.uint64).reshape(-1)
+            native.check(lib, lib.tp_eq_table_host(z0.ctypes.data, len(c0), r0.ctypes.data), "eq table")
+            native.check(lib, lib.tp_eq_table_host(z1.ctypes.data, len(c1), r1.ctypes.data), "eq table")
+            eq[f] = (r0, r1)
+        n = len(items)
+        hbs = [slot.open_host[f][k] for f, k in items]
+        qs = [hb["q"].numpy() for hb in hbs]
+        addrs = lambda xs: np.array(xs, np.uint64)
+        roots = addrs([slot.roots[k, f].data_ptr() for f, k in items])
+        use_g1 = np.array([0 if k == 1 else 1 for _, k in items], np.int32)
+        groups = np.array([-1 if not self.zk else k for _, k in items], np.int32)
+        r0s = addrs([eq[f][0].ctypes.data for f, _ in items])
+        r1s = addrs([eq[f][1].ctypes.data for f, _ in items])
+        qp = addrs([q.ctypes.data for q in qs])
+        native.check(lib, lib.tp_orion_open_queries_multi(n, roots.ctypes.data, self.N, use_g1.ctypes.data,
+                                                          r0s.ctypes.data, COLUMN_SIZE, r1s.ctypes.data,
+                                                          self.N // COLUMN_SIZE, self.cw_len, groups.ctypes.data,
+                                                          self.qc, qp.ctypes.data, None),
+                     "tp_orion_open_queries_multi")
+        for (f, _), hb, q in zip(items, hbs, qs):
+            r0, r1 = eq[f]
+            hb["r0"].numpy().view(np.uint64).reshape(-1, 2)[:] = r0[:, ::-1]     # (img, real): the codeword's order
+            hb["r1"].numpy().view(np.uint64).reshape(-1, 2)[:] = r1[:, ::-1]
+            if self.qc and (q.min() < 0 or q.max() >= self.cw_len):
+                raise IndexError("queried column outside the codeword")
+            # the same positions open both trees: one node list
+            hb["n_nodes"] = lib.tp_orion_path_nodes(self.leaves, q.ctypes.data, self.qc,
+                                                    hb["idx"].numpy().ctypes.data, slot.max_nodes)
+            native.check(lib, 0 if hb["n_nodes"] >= 0 else -1, "tp_orion_path_nodes")
 
     def _open_device(self, slot: _Slot, f: int, k: int) -> None:
         torch, lib = self.torch, self.lib
@@ -467,11 +484,16 @@ class ProofPipeline:
     def _finish(self, slot: _Slot) -> list:
         """GKR and openings of a started batch; returns futures of its FrameProofs"""
         self._gkr(slot)
-        kinds = 2 if self.zk else 1
-        host = [[self.pool.submit(self._open_host, slot, f, k) for k in range(kinds)] for f in range(self.B)]
-        for f in range(self.B):
-            for k in range(kinds):
-                host[f][k].result()
+        # host tasks of two openings each (a frame's two polynomials in the
+        # zero-knowledge mode, two frames' commits in the plain one), hashed in lockstep
+        if self.zk:
+            groups = [[(f, 0), (f, 1)] for f in range(self.B)]
+        else:
+            groups = [[(f, 0) for f in range(g, min(g + 2, self.B))] for g in range(0, self.B, 2)]
+        host = [self.pool.submit(self._open_host, slot, g) for g in groups]
+        for g, fut in zip(groups, host):
+            fut.result()
+            for f, k in g:
                 self._open_device(slot, f, k)
         slot.opened.record(self.stream)
         slot.assembly = [self.pool.submit(self._assemble, slot, f) for f in range(self.B)]
