@@ -390,13 +390,20 @@ int tp_fs_put_u64s(void* state, const uint64_t* values, size_t n);
  * copy_size bytes in host memory, of which the first n_bytes are read: past them
  * the inputs are zero, as in a frame whose last copy is not full) and hashed as
  * it is made; frames whose
- * transcripts stand at the same offset are hashed two at a time in lockstep. The
- * vector itself (2^23 values at 1080p) is never stored. Arguments as for
+ * transcripts stand at the same offset are hashed together, up to 16 at a time
+ * (the lanes of an AVX-512 multi-buffer SHA-256 where the host has AVX-512, else
+ * lockstep pairs on the SHA extensions): pass 16 frames per call for the best
+ * host throughput, 2 for the lowest latency. The vector itself (2^23 values at
+ * 1080p) is never stored. Arguments as for
  * tp_circuit_outputs_pixels_dev; n_gates <= 4096. */
 int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pixels, long long n_bytes, int n_frames,
                                      int n_copies, int n_copies_padded, int copy_size, int n_wires, int const_idx,
                                      uint64_t const_val, int n_gates, const int* gate_type, const int* in0,
                                      const int* in1);
+/* No counterpart in the reference: 1 when this host hashes groups of frames
+ * with the AVX-512 multi-buffer SHA-256 (CPU and OS support AVX-512 F/BW/VL),
+ * else 0. Host only. */
+int tp_host_sha_mb_available(void);
 /* put(Fp2) for each (re[i], im[i]) in turn (fiatshamir.py:129-131) */
 int tp_fs_put_fp2s(void* state, const uint64_t* re, const uint64_t* im, size_t n);
 /* put(str) (fiatshamir.py:132-136) */

@@ -4,7 +4,8 @@ state after it equals the state after put(output vector) of the vector the
 reference's circuit evaluator writes (the golden vectors of tests/golden/
 circuit_outputs_golden.npz, and the oracle's restatement for larger frames),
 for several frames at once, at equal and unequal offsets in the pending block,
-with the x86 SHA extensions and with the portable compression."""
+in groups of up to 16, with the AVX-512 multi-buffer compression, the x86 SHA
+extensions and the portable compression."""
 import ctypes
 import os
 import subprocess
@@ -112,6 +113,24 @@ def test_unequal_offsets_and_three_frames():
         assert _key(sts[f]) == _key(want), f
 
 
+def test_groups_of_sixteen_and_eight_lanes():
+    """29 frames in one call: 25 at one offset (a group of 16 lanes, one of 8 and
+    a single frame), 4 at another (lockstep pairs), each frame's state equal to
+    the put of its own output vector"""
+    lib = _lib()
+    c = _frame_case("inv", 40, 64, 384, 512, 384, 255, 13)
+    rng = np.random.default_rng(14)
+    frames = [rng.integers(0, 256, size=c["pix"].size, dtype=np.uint8) for _ in range(29)]
+    prefixes = [b"q" if f % 7 else b"rr" * 20 for f in range(29)]
+    sts = [_state(lib, p) for p in prefixes]
+    assert _put_fused(lib, sts, frames, c) == 0
+    for f in range(29):
+        want = _state(lib, prefixes[f])
+        _put_vector(lib, want, oracle_outputs(frames[f], c["copies"], c["padded"], c["cs"], c["n_wires"],
+                                              c["const_idx"], c["const_val"], c["gt"], c["i0"], c["i1"]))
+        assert _key(sts[f]) == _key(want), f
+
+
 def test_short_frames_read_as_zero_padded():
     """a frame whose bytes end inside its last copy (a crop of 385-byte copies)
     hashes as the same frame zero-padded to whole copies"""
@@ -140,13 +159,17 @@ def test_bad_arguments_are_rejected():
     assert b"out of range" in lib.tp_last_error()
 
 
-def test_portable_compression_gives_the_same_state():
-    """TRUEPIX_HOST_SHA_PORTABLE=1 (read once per process): a child process
-    hashes with the portable compression"""
+@pytest.mark.parametrize("setting", ["TRUEPIX_HOST_SHA_PORTABLE", "TRUEPIX_HOST_SHA_NO_MULTIBUFFER"])
+def test_other_compressions_give_the_same_state(setting):
+    """TRUEPIX_HOST_SHA_PORTABLE=1 (the portable compression for every chain) and
+    TRUEPIX_HOST_SHA_NO_MULTIBUFFER=1 (groups on the SHA extensions' lockstep
+    pairs instead of the AVX-512 lanes), each read once per process: a child
+    process per setting"""
     code = ("import sys; sys.path[:0] = [%r, %r]\n"
             "import test_io_transcript_host as t\n"
             "t.test_fused_put_matches_put_of_the_output_vector()\n"
-            "t.test_unequal_offsets_and_three_frames()\n" % (ROOT, os.path.join(ROOT, "tests")))
-    env = dict(os.environ, TRUEPIX_HOST_SHA_PORTABLE="1")
+            "t.test_unequal_offsets_and_three_frames()\n"
+            "t.test_groups_of_sixteen_and_eight_lanes()\n" % (ROOT, os.path.join(ROOT, "tests")))
+    env = dict(os.environ, **{setting: "1"})
     r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr

@@ -772,22 +772,15 @@ bool launch_mle_base(const u64* d_in, const fp2* d_z, int n_z, fp2* d_out, cudaS
     if (!c) return false;
     const int h = std::min(n_z, 12), hb = n_z - h;
     const size_t nt = ((size_t)1 << h) + ((size_t)1 << hb);
+    // eq tables, up to 2048 blocks' partials (four words each), the ticket
     fp2* tabs = (fp2*)dev_alloc(sizeof(fp2) * nt + 4 * sizeof(fp2) * 2048 + 256, s);
     if (!tabs) return false;
-    fp2* lo = tabs;
-    fp2* hi = tabs + ((size_t)1 << h);
     fp2* partials = tabs + nt;
     unsigned* ticket = reinterpret_cast<unsigned*>(partials + 4 * 2048);
-    bool ok = !cuda_failed(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s), "mle ticket");
-    eq_tables_kernel<<<blocks_for(nt, kThreads), kThreads, 0, s>>>(d_z, h, hb, mk(1, 0), lo, hi);
-    const size_t n = (size_t)1 << n_z;
-    const size_t work = h >= 3 ? (n >> 3) : n;
-    const unsigned blocks = (unsigned)std::max<size_t>(
-        1, std::min<size_t>(std::min<size_t>(blocks_for(work, kThreads), (size_t)c->n_sm * 8), 2048));
-    mle_kernel<<<blocks, kThreads, 0, s>>>(d_in, n, h, lo, hi, partials, ticket,
-                                           reinterpret_cast<u64*>(d_out));
-    t_launches = 2;
-    ok = ok && !cuda_failed(cudaGetLastError(), "mle launch");
+    bool ok = !cuda_failed(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s), "mle ticket") &&
+              launch_mle_base_into(d_in, d_z, n_z, d_out, tabs, partials, ticket,
+                                   (unsigned)std::min(c->n_sm * 8, 2048), s);
+    if (ok) t_launches = 2;
     dev_free(tabs, s);
     return ok;
 }

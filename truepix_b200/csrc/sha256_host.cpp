@@ -5,6 +5,8 @@
 // the message schedule in four registers of four words that roll every four
 // rounds (Intel, "Intel SHA Extensions", 2013). Used only when CPUID reports the
 // extensions; the portable compression in sha256.cuh serves every other host.
+// Many chains at once (a group of frames' transcripts) go through the AVX-512
+// multi-buffer compression below, where the CPU and OS support it.
 #include <stddef.h>
 #include <stdint.h>
 
@@ -216,11 +218,197 @@ extern "C" __attribute__((target("sha,sse4.1,ssse3"))) void tp_host_sha_ext_hash
     if (c < n) sha_ext_hash64<1>(in + c, out + c, K, pad.wk);
 }
 
+// ---- multi-buffer SHA-256 with AVX-512 ----
+// 16 independent chains in the 32-bit lanes of zmm registers (8 in ymm): each
+// vector instruction does one step of the same round for every chain (Intel,
+// "Fast Multi-buffer IPsec Implementations on Intel Architecture Processors",
+// 2010). A round is 17 vector operations: the sigma functions as three rotates
+// and one three-way XOR (VPTERNLOGD), choice and majority one VPTERNLOGD each.
+// Each chain's next 64-byte block is loaded as one vector (two for 8 lanes) and
+// the 16 x 16 word matrix transposed by four rounds of pairwise interleaves
+// (register k with register k + L/2), so lane c of W[i] holds word i of chain c.
+// One chain alone is slower than with SHA256RNDS2, 16 together are faster.
+#define TP_MB_TARGET __attribute__((target("avx512f,avx512vl,avx512bw")))
+
+extern "C" int tp_host_sha_mb_available(void)
+{
+    unsigned a, b, c, d;
+    if (!__get_cpuid(1, &a, &b, &c, &d)) return 0;
+    if (!((c >> 27) & 1)) return 0;   // OSXSAVE
+    unsigned lo, hi;
+    __asm__ volatile("xgetbv" : "=a"(lo), "=d"(hi) : "c"(0));
+    if ((lo & 0xE6) != 0xE6) return 0;   // XMM, YMM, opmask and ZMM state enabled by the OS
+    if (!__get_cpuid_count(7, 0, &a, &b, &c, &d)) return 0;
+    const bool f = (b >> 16) & 1, bw = (b >> 30) & 1, vl = (b >> 31) & 1;
+    return f && bw && vl;
+}
+
+namespace {
+
+struct Lanes16 {
+    using V = __m512i;
+    static constexpr int L = 16;
+    TP_MB_TARGET static V add(V a, V b) { return _mm512_add_epi32(a, b); }
+    template <int n> TP_MB_TARGET static V ror(V a) { return _mm512_ror_epi32(a, n); }
+    template <int n> TP_MB_TARGET static V shr(V a) { return _mm512_srli_epi32(a, n); }
+    template <int imm> TP_MB_TARGET static V tern(V a, V b, V c) { return _mm512_ternarylogic_epi32(a, b, c, imm); }
+    TP_MB_TARGET static V set1(uint32_t k) { return _mm512_set1_epi32((int)k); }
+    TP_MB_TARGET static V load(const void* p) { return _mm512_loadu_si512(p); }
+    TP_MB_TARGET static void store(void* p, V v) { _mm512_storeu_si512(p, v); }
+    TP_MB_TARGET static V bswap(V v)
+    {
+        return _mm512_shuffle_epi8(v, _mm512_set4_epi32(0x0c0d0e0f, 0x08090a0b, 0x04050607, 0x00010203));
+    }
+    // lo = a0 b0 a1 b1 ... a7 b7, hi = a8 b8 ... a15 b15
+    TP_MB_TARGET static void interleave(V a, V b, V& lo, V& hi)
+    {
+        lo = _mm512_permutex2var_epi32(a, _mm512_set_epi32(23, 7, 22, 6, 21, 5, 20, 4, 19, 3, 18, 2, 17, 1, 16, 0), b);
+        hi = _mm512_permutex2var_epi32(a, _mm512_set_epi32(31, 15, 30, 14, 29, 13, 28, 12, 27, 11, 26, 10, 25, 9, 24, 8),
+                                       b);
+    }
+};
+
+struct Lanes8 {
+    using V = __m256i;
+    static constexpr int L = 8;
+    TP_MB_TARGET static V add(V a, V b) { return _mm256_add_epi32(a, b); }
+    template <int n> TP_MB_TARGET static V ror(V a) { return _mm256_ror_epi32(a, n); }
+    template <int n> TP_MB_TARGET static V shr(V a) { return _mm256_srli_epi32(a, n); }
+    template <int imm> TP_MB_TARGET static V tern(V a, V b, V c) { return _mm256_ternarylogic_epi32(a, b, c, imm); }
+    TP_MB_TARGET static V set1(uint32_t k) { return _mm256_set1_epi32((int)k); }
+    TP_MB_TARGET static V load(const void* p) { return _mm256_loadu_si256(reinterpret_cast<const __m256i*>(p)); }
+    TP_MB_TARGET static void store(void* p, V v) { _mm256_storeu_si256(reinterpret_cast<__m256i*>(p), v); }
+    TP_MB_TARGET static V bswap(V v)
+    {
+        const V m = _mm256_set_epi32(0x0c0d0e0f, 0x08090a0b, 0x04050607, 0x00010203, 0x0c0d0e0f, 0x08090a0b,
+                                     0x04050607, 0x00010203);
+        return _mm256_shuffle_epi8(v, m);
+    }
+    TP_MB_TARGET static void interleave(V a, V b, V& lo, V& hi)
+    {
+        lo = _mm256_permutex2var_epi32(a, _mm256_set_epi32(11, 3, 10, 2, 9, 1, 8, 0), b);
+        hi = _mm256_permutex2var_epi32(a, _mm256_set_epi32(15, 7, 14, 6, 13, 5, 12, 4), b);
+    }
+};
+
+// x[c] lane i -> x[i] lane c for an L x L matrix of words: log2(L) rounds of
+// interleaving register k with register k + L/2 (a perfect shuffle of the rows)
+template <class T>
+TP_MB_TARGET inline void transpose(typename T::V* x)
+{
+    using V = typename T::V;
+    constexpr int L = T::L;
+    for (int r = 0; (1 << r) < L; ++r) {
+        V y[L];
+        for (int k = 0; k < L / 2; ++k) T::interleave(x[k], x[k + L / 2], y[2 * k], y[2 * k + 1]);
+        for (int k = 0; k < L; ++k) x[k] = y[k];
+    }
+}
+
+// one SHA-256 round for every lane: T1 = h + S1(e) + Ch(e, f, g) + K[t] + W[t];
+// d += T1; h = T1 + S0(a) + Maj(a, b, c) (the other words are renamed by the caller)
+#define TP_MB_ROUND(a, b, c, d, e, f, g, h, t, w)                                                                 \
+    {                                                                                                          \
+        const V t1 = T::add(T::add(h, T::template tern<0x96>(T::template ror<6>(e), T::template ror<11>(e),     \
+                                                             T::template ror<25>(e))),                          \
+                            T::add(T::template tern<0xCA>(e, f, g), T::add(T::set1(K[t]), w)));                \
+        d = T::add(d, t1);                                                                                     \
+        h = T::add(t1, T::add(T::template tern<0x96>(T::template ror<2>(a), T::template ror<13>(a),            \
+                                                     T::template ror<22>(a)),                                  \
+                              T::template tern<0xE8>(a, b, c)));                                               \
+    }
+
+// T::L chains of nblocks blocks: chain c's state h[c], its blocks at p[c]
+template <class T>
+TP_MB_TARGET void mb_blocks(uint32_t* const* h, const uint8_t* const* p, size_t nblocks, const uint32_t K[64])
+{
+    using V = typename T::V;
+    constexpr int L = T::L;
+    alignas(64) uint32_t tmp[8][L];
+    for (int w = 0; w < 8; ++w)
+        for (int c = 0; c < L; ++c) tmp[w][c] = h[c][w];
+    V s[8];
+    for (int w = 0; w < 8; ++w) s[w] = T::load(tmp[w]);
+    for (size_t blk = 0; blk < nblocks; ++blk) {
+        V W[16];
+        if constexpr (L == 16) {
+            for (int c = 0; c < 16; ++c) W[c] = T::bswap(T::load(p[c] + 64 * blk));
+            transpose<T>(W);
+        } else {   // words 0-7 and 8-15 of the 8 chains, transposed separately
+            for (int c = 0; c < 8; ++c) W[c] = T::bswap(T::load(p[c] + 64 * blk));
+            for (int c = 0; c < 8; ++c) W[8 + c] = T::bswap(T::load(p[c] + 64 * blk + 32));
+            transpose<T>(W);
+            transpose<T>(W + 8);
+        }
+        V a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], hh = s[7];
+#pragma GCC unroll 4
+        for (int t0 = 0; t0 < 64; t0 += 16) {
+            if (t0) {   // W[t] = s1(W[t-2]) + W[t-7] + s0(W[t-15]) + W[t-16], 16 at a time in place
+                for (int i = 0; i < 16; ++i) {
+                    const V w2 = W[(i + 14) & 15], w15 = W[(i + 1) & 15];
+                    const V s1 = T::template tern<0x96>(T::template ror<17>(w2), T::template ror<19>(w2),
+                                                        T::template shr<10>(w2));
+                    const V s0 = T::template tern<0x96>(T::template ror<7>(w15), T::template ror<18>(w15),
+                                                        T::template shr<3>(w15));
+                    W[i] = T::add(T::add(W[i], s0), T::add(W[(i + 9) & 15], s1));
+                }
+            }
+            TP_MB_ROUND(a, b, c, d, e, f, g, hh, t0 + 0, W[0]);
+            TP_MB_ROUND(hh, a, b, c, d, e, f, g, t0 + 1, W[1]);
+            TP_MB_ROUND(g, hh, a, b, c, d, e, f, t0 + 2, W[2]);
+            TP_MB_ROUND(f, g, hh, a, b, c, d, e, t0 + 3, W[3]);
+            TP_MB_ROUND(e, f, g, hh, a, b, c, d, t0 + 4, W[4]);
+            TP_MB_ROUND(d, e, f, g, hh, a, b, c, t0 + 5, W[5]);
+            TP_MB_ROUND(c, d, e, f, g, hh, a, b, t0 + 6, W[6]);
+            TP_MB_ROUND(b, c, d, e, f, g, hh, a, t0 + 7, W[7]);
+            TP_MB_ROUND(a, b, c, d, e, f, g, hh, t0 + 8, W[8]);
+            TP_MB_ROUND(hh, a, b, c, d, e, f, g, t0 + 9, W[9]);
+            TP_MB_ROUND(g, hh, a, b, c, d, e, f, t0 + 10, W[10]);
+            TP_MB_ROUND(f, g, hh, a, b, c, d, e, t0 + 11, W[11]);
+            TP_MB_ROUND(e, f, g, hh, a, b, c, d, t0 + 12, W[12]);
+            TP_MB_ROUND(d, e, f, g, hh, a, b, c, t0 + 13, W[13]);
+            TP_MB_ROUND(c, d, e, f, g, hh, a, b, t0 + 14, W[14]);
+            TP_MB_ROUND(b, c, d, e, f, g, hh, a, t0 + 15, W[15]);
+        }
+        s[0] = T::add(s[0], a);
+        s[1] = T::add(s[1], b);
+        s[2] = T::add(s[2], c);
+        s[3] = T::add(s[3], d);
+        s[4] = T::add(s[4], e);
+        s[5] = T::add(s[5], f);
+        s[6] = T::add(s[6], g);
+        s[7] = T::add(s[7], hh);
+    }
+    for (int w = 0; w < 8; ++w) T::store(tmp[w], s[w]);
+    for (int w = 0; w < 8; ++w)
+        for (int c = 0; c < L; ++c) h[c][w] = tmp[w][c];
+}
+#undef TP_MB_ROUND
+
+}  // namespace
+
+// the first n chains, in groups of 16 lanes and then one of 8 where n allows;
+// returns how many chains were hashed (the caller hashes the rest another way)
+extern "C" TP_MB_TARGET int tp_host_sha_mb_blocks(uint32_t* const* h, const uint8_t* const* p, int n,
+                                                  size_t nblocks, const uint32_t K[64])
+{
+    int c = 0;
+    for (; c + 16 <= n; c += 16) mb_blocks<Lanes16>(h + c, p + c, nblocks, K);
+    if (c + 8 <= n) {
+        mb_blocks<Lanes8>(h + c, p + c, nblocks, K);
+        c += 8;
+    }
+    return c;
+}
+#undef TP_MB_TARGET
+
 #else
 
 extern "C" int tp_host_sha_ext_available(void) { return 0; }
 extern "C" void tp_host_sha_ext_blocks(uint32_t*, const uint8_t*, size_t, const uint32_t*) {}
 extern "C" void tp_host_sha_ext_multi(uint32_t* const*, const uint8_t* const*, int, size_t, const uint32_t*) {}
 extern "C" void tp_host_sha_ext_hash64(const uint8_t* const*, uint8_t* const*, int, const uint32_t*) {}
+extern "C" int tp_host_sha_mb_available(void) { return 0; }
+extern "C" int tp_host_sha_mb_blocks(uint32_t* const*, const uint8_t* const*, int, size_t, const uint32_t*) { return 0; }
 
 #endif

@@ -21,6 +21,9 @@
 extern "C" int tp_host_sha_ext_available(void);
 extern "C" void tp_host_sha_ext_blocks(uint32_t h[8], const uint8_t* p, size_t nblocks, const uint32_t K[64]);
 extern "C" void tp_host_sha_ext_hash64(const uint8_t* const* in, uint8_t* const* out, int n, const uint32_t K[64]);
+extern "C" int tp_host_sha_mb_available(void);
+extern "C" int tp_host_sha_mb_blocks(uint32_t* const* h, const uint8_t* const* p, int n, size_t nblocks,
+                                     const uint32_t K[64]);
 extern "C" void tp_host_sha_ext_multi(uint32_t* const* h, const uint8_t* const* p, int n, size_t nblocks,
                                       const uint32_t K[64]);
 
@@ -157,6 +160,15 @@ bool host_sha_ext()
     return ok;
 }
 
+// TRUEPIX_HOST_SHA_NO_MULTIBUFFER=1 keeps groups of chains off the AVX-512
+// multi-buffer compression (the portable setting does too)
+bool host_sha_mb()
+{
+    static const bool ok = tp_host_sha_mb_available() != 0 && !getenv("TRUEPIX_HOST_SHA_PORTABLE") &&
+                           !getenv("TRUEPIX_HOST_SHA_NO_MULTIBUFFER");
+    return ok;
+}
+
 void host_blocks(uint32_t h[8], const uint8_t* p, size_t nblocks)
 {
     if (host_sha_ext()) {
@@ -202,9 +214,16 @@ void host_absorb_header(State& s, uint8_t tag, uint32_t n)
     host_absorb(s, b, 5);
 }
 
-// n chains of nblocks whole blocks each (with the SHA extensions: in lockstep pairs)
+// n chains of nblocks whole blocks each: groups of 16 (then 8) in the lanes of
+// the AVX-512 multi-buffer compression, the rest with the SHA extensions in
+// lockstep pairs
 void host_blocks_multi(uint32_t* const* h, const uint8_t* const* p, int n, size_t nblocks)
 {
+    const int done = host_sha_mb() ? tp_host_sha_mb_blocks(h, p, n, nblocks, kHostTables.k) : 0;
+    h += done;
+    p += done;
+    n -= done;
+    if (n == 0) return;
     if (host_sha_ext()) {
         tp_host_sha_ext_multi(h, p, n, nblocks, kHostTables.k);
         return;
@@ -217,7 +236,9 @@ void host_blocks_multi(uint32_t* const* h, const uint8_t* const* p, int n, size_
 // generated copy by copy from the frame's bytes into a small staging buffer per
 // frame and hashed from there: nothing of the size of the vector is written or
 // copied. Frames whose transcripts stand at the same offset in their pending
-// block hash in lockstep pairs.
+// block hash together, up to kGroup at a time (host_blocks_multi: the lanes of
+// the multi-buffer compression, else lockstep pairs).
+constexpr int kGroup = 16;
 
 // native_fp2_core.hpp:32-51 on canonical base-field values (as the device kernel)
 uint64_t host_gate_value(unsigned type, uint64_t x, uint64_t y)
@@ -246,12 +267,13 @@ struct OutputCircuit {
     int n_copies, n_copies_padded, cs, n_wires, const_idx, n_gates, out_bits;
     uint64_t const_val;
     long long n_bytes;                        // the frame's bytes; past them a copy's inputs are zero
-    std::vector<uint32_t> type, src0, src1;   // src: the wire, or n_wires for "zero", n_wires + 1 for the constant
+    std::vector<uint32_t> type, src0, src1;   // src: the byte's index, or cs for "zero", cs + 1 for the constant
     std::vector<uint8_t> direct;              // the gate's value is one of its inputs (pass, multiplexer)
 };
 
-// copy c's outputs (2^out_bits LE64 values) at out
-void copy_outputs(const OutputCircuit& C, const uint8_t* pix, long long c, uint64_t* out)
+// copy c's outputs (2^out_bits LE64 values) at out; ext: cs + 2 words of scratch
+// (the copy's inputs widened, then zero and the constant, indexed by src)
+void copy_outputs(const OutputCircuit& C, const uint8_t* pix, long long c, uint64_t* ext, uint64_t* out)
 {
     const int G = 1 << C.out_bits;
     if (c >= C.n_copies) {
@@ -260,14 +282,14 @@ void copy_outputs(const OutputCircuit& C, const uint8_t* pix, long long c, uint6
     }
     const uint8_t* row = pix + c * C.cs;
     const long long left = C.n_bytes - c * (long long)C.cs;
-    const uint32_t avail = left >= C.cs ? (uint32_t)C.cs : left > 0 ? (uint32_t)left : 0u;
-    const uint32_t cs = (uint32_t)C.cs, konst = (uint32_t)C.n_wires + 1;
-    auto val = [&](uint32_t a) -> uint64_t {
-        return a < cs ? (a < avail ? row[a] : 0) : a == konst ? C.const_val : 0;
-    };
+    const int cs = C.cs, avail = left >= cs ? cs : left > 0 ? (int)left : 0;
+    for (int a = 0; a < avail; ++a) ext[a] = row[a];
+    for (int a = avail; a < cs; ++a) ext[a] = 0;
+    ext[cs] = 0;
+    ext[cs + 1] = C.const_val;
     for (int g = 0; g < C.n_gates; ++g) {
-        const uint64_t va = val(C.src0[g]);
-        out[g] = C.direct[g] ? va : host_gate_value(C.type[g], va, val(C.src1[g]));
+        const uint64_t va = ext[C.src0[g]];
+        out[g] = C.direct[g] ? va : host_gate_value(C.type[g], va, ext[C.src1[g]]);
     }
     if (G > C.n_gates) memset(out + C.n_gates, 0, 8 * (size_t)(G - C.n_gates));
 }
@@ -279,8 +301,9 @@ void put_outputs_group(State* const* st, const uint8_t* const* pix, int k, const
     const size_t copy_bytes = (size_t)8 << C.out_bits;
     const size_t cap = 64 + kCopiesPerChunk * copy_bytes;
     std::vector<uint8_t> stage((size_t)k * cap);
-    uint32_t* h[2];
-    const uint8_t* p[2];
+    std::vector<uint64_t> ext((size_t)C.cs + 2);
+    uint32_t* h[kGroup];
+    const uint8_t* p[kGroup];
     size_t fill = st[0]->nbuf;   // equal for every frame of the group
     for (int c = 0; c < k; ++c) memcpy(&stage[(size_t)c * cap], st[c]->buf, fill);
     const uint64_t n_values = (uint64_t)C.n_copies_padded << C.out_bits;
@@ -289,7 +312,7 @@ void put_outputs_group(State* const* st, const uint8_t* const* pix, int k, const
         for (int c = 0; c < k; ++c) {
             uint8_t* base = &stage[(size_t)c * cap] + fill;
             for (long long q = 0; q < nc; ++q)
-                copy_outputs(C, pix[c], c0 + q, reinterpret_cast<uint64_t*>(base + q * copy_bytes));
+                copy_outputs(C, pix[c], c0 + q, ext.data(), reinterpret_cast<uint64_t*>(base + q * copy_bytes));
         }
         const size_t total = fill + (size_t)nc * copy_bytes;
         const size_t nblk = total / 64;
@@ -441,9 +464,9 @@ int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pix
     C.n_gates = n_gates;
     C.out_bits = tp_circuit_out_bits(n_gates);
     C.n_bytes = std::min<long long>(n_bytes, (long long)n_copies * copy_size);
-    // sources: a byte of the copy (wire < copy_size), the constant (n_wires + 1), else zero (n_wires)
+    // sources: a byte of the copy (wire < copy_size), the constant (copy_size + 1), else zero (copy_size)
     auto src = [&](int w) -> uint32_t {
-        return w < copy_size ? (uint32_t)w : w == const_idx ? (uint32_t)n_wires + 1 : (uint32_t)n_wires;
+        return w < copy_size ? (uint32_t)w : w == const_idx ? (uint32_t)copy_size + 1 : (uint32_t)copy_size;
     };
     for (int g = 0; g < n_gates; ++g) {
         if (gate_type[g] < 0 || gate_type[g] > 12 || in0[g] < 0 || in0[g] >= n_wires || in1[g] < 0 ||
@@ -466,20 +489,20 @@ int tp_fs_put_circuit_outputs_pixels(void* const* states, const void* const* pix
         State& s = *static_cast<State*>(states[f]);
         host_absorb_header(s, 0x01, (uint32_t)values);
     }
-    // pairs of frames at the same offset hash in lockstep, the rest alone
+    // frames at the same offset hash together, up to kGroup at a time
     std::vector<int> done(n_frames, 0);
     for (int f = 0; f < n_frames; ++f) {
         if (done[f]) continue;
         done[f] = 1;
-        State* st[2] = {static_cast<State*>(states[f]), nullptr};
-        const uint8_t* px[2] = {static_cast<const uint8_t*>(pixels[f]), nullptr};
+        State* st[kGroup] = {static_cast<State*>(states[f])};
+        const uint8_t* px[kGroup] = {static_cast<const uint8_t*>(pixels[f])};
         int k = 1;
-        for (int g = f + 1; g < n_frames && k < 2; ++g)
+        for (int g = f + 1; g < n_frames && k < kGroup; ++g)
             if (!done[g] && static_cast<State*>(states[g])->nbuf == st[0]->nbuf) {
                 done[g] = 1;
-                st[1] = static_cast<State*>(states[g]);
-                px[1] = static_cast<const uint8_t*>(pixels[g]);
-                k = 2;
+                st[k] = static_cast<State*>(states[g]);
+                px[k] = static_cast<const uint8_t*>(pixels[g]);
+                ++k;
             }
         put_outputs_group(st, px, k, C);
     }

@@ -110,6 +110,7 @@ GKR_SIGNATURES = {
     "tp_orion_gather_nodes_dev": (_I32, [_VP, ctypes.c_longlong, _VP, _I32, _VP, _VP]),
     "tp_fs_put_circuit_outputs_pixels": (_I32, [_VP, _VP, ctypes.c_longlong, _I32, _I32, _I32, _I32, _I32, _I32, _U64,
                                                 _I32, _PI32, _PI32, _PI32]),
+    "tp_host_sha_mb_available": (_I32, []),
     "tp_fs_put_fp2s": (_I32, [_VP, _VP, _VP, ctypes.c_size_t]),
     "tp_fs_put_str": (_I32, [_VP, ctypes.c_char_p]),
     "tp_fs_rand_scalar": (_I32, [_VP, _VP]),
