@@ -46,8 +46,9 @@ def _frames(rng, layout, k):
 @pytest.mark.parametrize("zk", [False, True])
 @pytest.mark.parametrize("resident", [True, False])
 def test_pipeline_matches_step_by_step_proofs_and_openings(zk, resident):
-    """three batches of three 90-copy gray frames through the pipeline, against
-    commit + prove_frames + opening_proof of each frame on its own"""
+    """four batches of two 90-copy gray frames through the pipeline (device slots
+    reused, IO hashed ahead: the first batch in pairs, the rest in one group per
+    batch), against commit + prove_frames + opening_proof of each frame on its own"""
     import torch
     from truepix_b200.frame import FrameLayout
     from truepix_b200.opening import opening_proof
@@ -59,9 +60,9 @@ def test_pipeline_matches_step_by_step_proofs_and_openings(zk, resident):
     layout = FrameLayout(copies=90)
     rng = np.random.default_rng(5 + zk + 2 * resident)
     count = correlations_needed(layout, zk) + 3
-    B = 3
+    B = 2
     batches, want = [], []
-    for b in range(3):
+    for b in range(4):
         frames = _frames(rng, layout, B)
         corr = [(rng.integers(0, (1 << 61) - 1, size=(count, 2), dtype=np.uint64),
                  rng.integers(0, (1 << 61) - 1, size=(count, 2), dtype=np.uint64)) for _ in range(B)]
@@ -71,10 +72,11 @@ def test_pipeline_matches_step_by_step_proofs_and_openings(zk, resident):
         if resident:
             batch["frames_dev"] = [torch.from_numpy(f).cuda() for f in frames]
         batches.append(batch)
-    pipe = ProofPipeline(layout, gt, i0, i1, batch=B, zk=zk, fp2_type=F, host_threads=4, commit_streams=2)
+    pipe = ProofPipeline(layout, gt, i0, i1, batch=B, zk=zk, fp2_type=F, host_threads=4, commit_streams=2,
+                         slots=3 if resident else 2, io_ahead=2)
     got = list(pipe.run(batches))
     pipe.close()
-    assert len(got) == 3
+    assert len(got) == 4
     for b, batch in enumerate(batches):
         frames = [np.asarray(x) if not hasattr(x, "numpy") else x.numpy() for x in batch["frames_host"]]
         for f in range(B):

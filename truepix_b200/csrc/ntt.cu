@@ -23,6 +23,7 @@ struct Tables {
     fp2* lo = nullptr;
     fp2* hi = nullptr;
     int h = 0;
+    int quarter = 0;   // w^(n/4) = +i (1) or -i (-1); 0 for n < 4
 };
 
 std::mutex g_mu;
@@ -38,6 +39,7 @@ struct Pass {
     int n_dig;                        // last pass: the earlier digits
     int dig_bits[3];
     int dig_shift[3];
+    int quarter;                      // w_R^(R/4) = +i (1) or -i (-1)
 };
 
 __device__ __forceinline__ fp2 ld_fe(const ulonglong2* p) { const ulonglong2 v = *p; return mk(v.y, v.x); }
@@ -58,13 +60,20 @@ __device__ __forceinline__ int bitrev(int j, int bits) { return bits ? (int)(__b
 // distinct banks.
 __device__ __forceinline__ int at(int r, int c, int log_g) { return (r << log_g) + c + (r >> 3); }
 
+// y * (+i) or y * (-i): the 4th root of unity of the pass, by a swap and a negation
+__device__ __forceinline__ fp2 times_quarter(fp2 y, int quarter)
+{
+    return quarter > 0 ? mk(lsub(0, y.im), y.re) : mk(y.im, lsub(0, y.re));
+}
+
 // K consecutive radix-2 stages lh0 .. lh0 + K - 1 in registers: a work item is one
 // column and the 2^K rows base + m 2^lh0 (m < 2^K) that these stages combine.
 // The butterfly of stage lh on rows (u, u + 2^lh) uses w_R^(pin R / 2^(lh+1)),
 // pin = u mod 2^lh; FIRST (lh0 = 0) makes every pin a compile-time constant, so
-// the multiplications by w^0 = 1 vanish.
+// the multiplications by w^0 = 1 vanish and those by w_R^(R/4) = +-i become a
+// swap and a negation.
 template <int K, bool FIRST>
-__device__ __forceinline__ void stage_group(fp2* sm, const fp2* tws, int log_r, int log_g, int lh0)
+__device__ __forceinline__ void stage_group(fp2* sm, const fp2* tws, int log_r, int log_g, int lh0, int quarter)
 {
     const int G = 1 << log_g;
     const int items = ((1 << log_r) >> K) << log_g;
@@ -85,7 +94,8 @@ __device__ __forceinline__ void stage_group(fp2* sm, const fp2* tws, int log_r, 
                 if (m & (1 << j)) continue;
                 const int pin = ((m & ((1 << j) - 1)) << sh) + lo;
                 fp2 y = x[m + (1 << j)];
-                if (pin) y = l2mul(tws[pin << (log_r - 1 - lh)], y);
+                if (FIRST && lh >= 1 && pin == (1 << (lh - 1)) && quarter) y = times_quarter(y, quarter);
+                else if (pin) y = l2mul(tws[pin << (log_r - 1 - lh)], y);
                 const fp2 a = x[m];
                 x[m] = l2add(a, y);
                 x[m + (1 << j)] = l2sub(a, y);
@@ -134,7 +144,15 @@ __global__ void __launch_bounds__(kThreads, 3) pass_kernel(const ulonglong2* src
             j = idx >> p.log_g;
             pos = col_base + c + (long long)j * S;
         } else {
-            j = idx & (R - 1);
+            // the element of the column: for R >= 2^6, the three lowest lane bits
+            // become bits log_r - 6 .. log_r - 4 of j, so that the eight threads of
+            // a quarter warp write rows bitrev(j) whose bits 3..5 differ (eight
+            // distinct bank groups of the padded tile) while every 64 bytes of
+            // the row are still read by four neighbouring lanes
+            const int u = idx & (R - 1);
+            const int at_bit = p.log_r - 6;
+            const int hi = u >> 3;
+            j = at_bit < 0 ? u : (hi & ((1 << at_bit) - 1)) | ((u & 7) << at_bit) | ((hi >> at_bit) << (at_bit + 3));
             c = idx >> p.log_r;
             const long long cc = c0 + c;
             long long base = 0;
@@ -158,13 +176,13 @@ __global__ void __launch_bounds__(kThreads, 3) pass_kernel(const ulonglong2* src
     for (int lh0 = 0; lh0 < p.log_r; lh0 += 3) {
         const int k = min(3, p.log_r - lh0);
         if (lh0 == 0) {
-            if (k == 3) stage_group<3, true>(sm, tws, p.log_r, p.log_g, 0);
-            else if (k == 2) stage_group<2, true>(sm, tws, p.log_r, p.log_g, 0);
-            else stage_group<1, true>(sm, tws, p.log_r, p.log_g, 0);
+            if (k == 3) stage_group<3, true>(sm, tws, p.log_r, p.log_g, 0, p.quarter);
+            else if (k == 2) stage_group<2, true>(sm, tws, p.log_r, p.log_g, 0, p.quarter);
+            else stage_group<1, true>(sm, tws, p.log_r, p.log_g, 0, p.quarter);
         } else {
-            if (k == 3) stage_group<3, false>(sm, tws, p.log_r, p.log_g, lh0);
-            else if (k == 2) stage_group<2, false>(sm, tws, p.log_r, p.log_g, lh0);
-            else stage_group<1, false>(sm, tws, p.log_r, p.log_g, lh0);
+            if (k == 3) stage_group<3, false>(sm, tws, p.log_r, p.log_g, lh0, p.quarter);
+            else if (k == 2) stage_group<2, false>(sm, tws, p.log_r, p.log_g, lh0, p.quarter);
+            else stage_group<1, false>(sm, tws, p.log_r, p.log_g, lh0, p.quarter);
         }
         __syncthreads();
     }
@@ -227,6 +245,10 @@ const Tables* tables(int logn, bool inv)
     const fp2 step = nlo < ((size_t)1 << logn) ? f2mul(lo[nlo - 1], w) : mk(1, 0);   // w^(2^h)
     hi[0] = mk(1, 0);
     for (size_t i = 1; i < nhi; ++i) hi[i] = f2mul(hi[i - 1], step);
+    if (logn >= 2) {
+        const fp2 q = f2pow(w, 1ull << (logn - 2));
+        t.quarter = (q.re == 0 && q.im == 1) ? 1 : (q.re == 0 && q.im == P61 - 1) ? -1 : 0;
+    }
     if (cuda_failed(cudaMalloc(&t.lo, sizeof(fp2) * nlo), "ntt twiddle alloc") ||
         cuda_failed(cudaMalloc(&t.hi, sizeof(fp2) * nhi), "ntt twiddle alloc") ||
         cuda_failed(cudaMemcpy(t.lo, lo.data(), sizeof(fp2) * nlo, cudaMemcpyHostToDevice), "ntt twiddle upload") ||
@@ -314,6 +336,7 @@ bool run(const ulonglong2* in, long long in_len, long long in_step, int logn, bo
         p.in_len = in_len;
         p.in_step = in_step;
         p.scale = p.last ? scale : 0;
+        p.quarter = tb->quarter;
         const ulonglong2* src = t == 0 ? in : tmp;
         ulonglong2* dst = p.last ? out : tmp;
         p.src_batch = t == 0 ? in_batch : n;

@@ -383,8 +383,8 @@ class BatchFrameProver:
         # uploads on the launch stream, so that the kernel is ordered after them
         def on_stream():
             return torch.cuda.stream(self.stream) if self.stream is not None else contextlib.nullcontext()
-        with on_stream():
-            d_zg = torch.from_numpy(zg.view(np.int64).copy()).to(self.dev)
+        with on_stream():    # from pinned memory, asynchronously: no wait for the launch stream to drain
+            d_zg = torch.from_numpy(zg.view(np.int64)).pin_memory().to(self.dev, non_blocking=True)
         i64 = torch.int64
         with on_stream():
             self.late_coefs = torch.zeros(self.B * 2 * n * 3 * 2, dtype=i64, device=self.dev)

@@ -12,11 +12,13 @@ Stages of a batch, and where they run:
   commit    device, side streams: the Orion commitment of every frame from its
             bytes (truepix_b200.orion.FrameCommitter); codewords and trees stay
             in HBM for the opening, the roots come back to pinned memory
-  IO        host threads: each frame's transcript puts its pid, the IO values
-            and the circuit's output vector, computed from the frame's bytes and
-            hashed as it is made, two frames per thread in lockstep
-            (tp_fs_put_circuit_outputs_pixels); then the commitment binding
-            (once the root is back) and the GKR point's draws z1, z2
+  IO        host threads (a pool of their own): each frame's transcript puts
+            its pid, the IO values and the circuit's output vector, computed from
+            the frame's bytes and hashed as it is made, 16 frames per task in the
+            lanes of the multi-buffer SHA-256 (tp_fs_put_circuit_outputs_pixels;
+            the first batch of a run in pairs, for latency); this runs io_ahead
+            batches ahead of the commits. Then, once a frame's root is back, the
+            commitment binding and the GKR point's draws z1, z2
   GKR       device, main stream: gate weights and beta, the VOLE-committed
             early rounds, late rounds and closing proofs of all frames, each
             frame's transcript and VOLE state resident on the device
@@ -29,14 +31,17 @@ Stages of a batch, and where they run:
             gathered over the HBM-resident codeword and trees; host threads:
             the opening file's bytes
 
-Two batches are in flight: while the device commits batch b on the side streams
-and the host threads hash its IO, the main stream proves and opens batch b - 1.
+Batches overlap: while the device commits batch b on the side streams, the main
+stream proves and opens batch b - 1, the host threads assemble batch b - 2's
+proofs (handed out once batch b - 1 is proved) and hash the IO of batches
+b .. b + io_ahead.
 Every value is the reference's: truepix_b200.prover.prove_frames and
 truepix_b200.opening.opening_proof produce the same proofs one step at a time
 and are pinned to proofs and files made by the reference itself.
 """
 from __future__ import annotations
 
+import collections
 import concurrent.futures
 import ctypes
 import math
@@ -105,6 +110,17 @@ class FrameProof:
             io.extend(saved)
 
 
+class _Pending:
+    """A batch taken from the input whose IO hashing is under way: its frames'
+    host views, transcripts and hashing futures (one per group of frames)."""
+    batch: dict
+    host_t: list
+    frames_host: list
+    tr: list
+    groups: list
+    hashed: list
+
+
 class _Slot:
     """Device and pinned host buffers of one batch in flight."""
 
@@ -146,6 +162,25 @@ class _Slot:
                                 idx=torch.empty(self.max_nodes, dtype=torch.int32).pin_memory())
                            for _ in range(n_trees)] for _ in range(p.B)]
         self.opened = torch.cuda.Event()
+        # the GKR's inputs and results in pinned memory: per slot, since a batch's
+        # results are read (opener thread) while the next batch's GKR is launched
+        B, nb, n, i64 = p.B, p.nb, p.n, torch.int64
+        nst, nvs = p.lib.tp_fs_state_bytes(), p.lib.tp_vole_state_bytes()
+        self.h_in = dict(z2=torch.empty(2 * B * nb, dtype=i64).pin_memory(),
+                         states=torch.empty(B * nst, dtype=torch.uint8).pin_memory(),
+                         vs=torch.empty(B * nvs, dtype=torch.uint8).pin_memory(),
+                         u=torch.empty(2 * B * p.count, dtype=i64).pin_memory(),
+                         v=torch.empty(2 * B * p.count, dtype=i64).pin_memory())
+        ncl = n + (15 if p.zk else 10)
+        self.h_out = dict(early=torch.empty(nb * B * 10, dtype=i64).pin_memory(),
+                          late=torch.empty(B * 2 * n * 4 * 2, dtype=i64).pin_memory(),
+                          closing=torch.empty(B * ncl * 2, dtype=i64).pin_memory(),
+                          point=torch.empty(B * (n + nb) * 2, dtype=i64).pin_memory(),
+                          tag=torch.empty(B * 2, dtype=i64).pin_memory(),
+                          states=torch.empty(B * nst, dtype=torch.uint8).pin_memory(),
+                          vs=torch.empty(B * nvs, dtype=torch.uint8).pin_memory())
+        self.inputs_sent = torch.cuda.Event()   # h_in copied to the device: free to refill
+        self.gkr_done = torch.cuda.Event()
 
 
 class ProofPipeline:
@@ -165,10 +200,17 @@ class ProofPipeline:
       manifests    optional: the commitment manifests the transcripts bind
                    (truepix_b200.prover.commit_manifest); by default each frame's
                    manifest is made from its device commit's roots
-    and yields, per batch, the list of FrameProof."""
+    and yields, per batch, the list of FrameProof. io_group frames are hashed per
+    IO task (0: 16 where the host has the multi-buffer SHA-256, else 2), on
+    io_threads threads (0: one per CPU but four), io_ahead batches ahead of the
+    commits; host_threads run the bindings, openings and assembly. `slots` batches
+    hold device buffers at once (each frame's codewords and trees, 231 MB per
+    committed 1080p polynomial): with three, a batch's commits never wait for the
+    assembly of the batch two before it."""
 
     def __init__(self, layout, gate_type, in0, in1, batch: int, device: int = 0, zk: bool = False,
-                 host_threads: int = 0, commit_streams: int = 8, fp2_type=None, graph: bool = True):
+                 host_threads: int = 0, commit_streams: int = 8, fp2_type=None, graph: bool = True,
+                 io_group: int = 0, io_ahead: int = 3, io_threads: int = 0, slots: int = 3):
         import torch
         from .frame import BatchFrameProver
         self.torch = torch
@@ -192,7 +234,7 @@ class ProofPipeline:
         self.qc = query_count()
         self.count = correlations_needed(layout, zk)
         self.prover = BatchFrameProver([layout] * batch, self.gt, self.i0, self.i1, device=device, stream=self.stream)
-        self.slots = [_Slot(self), _Slot(self)]
+        self.slots = [_Slot(self) for _ in range(max(2, slots))]
         B, nb, n = batch, self.nb, self.n
         i64 = torch.int64
         self.d_z2 = torch.empty(2 * B * nb, dtype=i64, device=self.dev)
@@ -201,50 +243,58 @@ class ProofPipeline:
         self.d_vs = torch.empty(B * self.lib.tp_vole_state_bytes(), dtype=torch.uint8, device=self.dev)
         self.d_u = torch.empty(2 * B * self.count, dtype=i64, device=self.dev)
         self.d_v = torch.empty(2 * B * self.count, dtype=i64, device=self.dev)
-        self.h_in = dict(z2=torch.empty(2 * B * nb, dtype=i64).pin_memory(),
-                         states=torch.empty(B * self.lib.tp_fs_state_bytes(), dtype=torch.uint8).pin_memory(),
-                         vs=torch.empty(B * self.lib.tp_vole_state_bytes(), dtype=torch.uint8).pin_memory(),
-                         u=torch.empty(2 * B * self.count, dtype=i64).pin_memory(),
-                         v=torch.empty(2 * B * self.count, dtype=i64).pin_memory())
-        ncl = n + (15 if zk else 10)
-        self.h_out = dict(early=torch.empty(nb * B * 10, dtype=i64).pin_memory(),
-                          late=torch.empty(B * 2 * n * 4 * 2, dtype=i64).pin_memory(),
-                          closing=torch.empty(B * ncl * 2, dtype=i64).pin_memory(),
-                          point=torch.empty(B * (n + nb) * 2, dtype=i64).pin_memory(),
-                          tag=torch.empty(B * 2, dtype=i64).pin_memory(),
-                          states=torch.empty(B * self.lib.tp_fs_state_bytes(), dtype=torch.uint8).pin_memory(),
-                          vs=torch.empty(B * self.lib.tp_vole_state_bytes(), dtype=torch.uint8).pin_memory())
-        self.gkr_done = torch.cuda.Event()
         vs0 = ctypes.create_string_buffer(self.lib.tp_vole_state_bytes())
         native.check(self.lib, self.lib.tp_vole_state_init(vs0, 0, None), "tp_vole_state_init")
         self.vs0 = vs0.raw
         self.pool = concurrent.futures.ThreadPoolExecutor(host_threads or os.cpu_count() or 4)
+        # the IO hashing on a pool of its own, so that the long hashing tasks of
+        # the batches ahead never queue in front of the current batch's openings
+        self.io_pool = concurrent.futures.ThreadPoolExecutor(io_threads or max(1, (os.cpu_count() or 4) - 4))
+        self.io_group = io_group or (16 if self.lib.tp_host_sha_mb_available() else 2)
+        self.io_ahead = io_ahead
+        # waits on device events and hashing that would otherwise hold host pool threads
+        self.waiter = concurrent.futures.ThreadPoolExecutor(1)
+        self.binder = concurrent.futures.ThreadPoolExecutor(1)
+        # a batch's GKR results are read, and its openings run, on a thread and a
+        # stream of their own while the main thread launches the next batch's GKR
+        self.opener = concurrent.futures.ThreadPoolExecutor(1)
+        self.open_stream = torch.cuda.Stream(self.dev)
+        self._count_lock = __import__("threading").Lock()
         self.launches_last = 0
         # the first batch's rounds run launch by launch with the round autotuner on;
         # later batches replay them as one CUDA graph (BatchFrameProver.prove(graph=True))
         self.graph = graph
         self.tuned = False
 
+    def _count(self, k: int) -> None:
+        with self._count_lock:
+            self.launches_last += k
+
     def close(self):
+        self.opener.shutdown(wait=True)
+        self.binder.shutdown(wait=True)
+        self.waiter.shutdown(wait=True)
+        self.io_pool.shutdown(wait=True)
         self.pool.shutdown(wait=True)
 
-    # ---- stage: commits and IO ------------------------------------------------
-    def _start(self, slot: _Slot, batch: dict) -> None:
+    # ---- stage: commits ---------------------------------------------------------
+    def _start(self, slot: _Slot, pend: "_Pending") -> None:
         torch, B = self.torch, self.B
         for f in slot.assembly:          # the slot's previous batch is assembled
             f.result()
         slot.assembly = []
+        batch = pend.batch
+        slot.pending = pend
         slot.batch = batch
-        host_t = [a if torch.is_tensor(a) else torch.from_numpy(np.ascontiguousarray(a, np.uint8).reshape(-1))
-                  for a in batch["frames_host"]]
-        slot.frames_host = [a.numpy() for a in host_t]
+        slot.frames_host = pend.frames_host
+        slot.tr = pend.tr
         if batch.get("frames_dev") is not None:
             frames_dev = list(batch["frames_dev"])
             ready = None
         else:   # uploads on their own stream (pinned frames: asynchronous), each commit waits for its frame
             frames_dev, ready = [], []
             with torch.cuda.stream(self.upload):
-                for a in host_t:
+                for a in pend.host_t:
                     frames_dev.append(a.to(self.dev, non_blocking=True))
                     ev = torch.cuda.Event()
                     ev.record(self.upload)
@@ -253,7 +303,7 @@ class ProofPipeline:
         slot.upload_ready = ready
         c = slot.committer
         # each frame's roots back to pinned memory right behind its own commit, with
-        # an event per frame: a frame's IO task waits for that commit only
+        # an event per frame: a frame's binding waits for that commit only
         slot.root_events = [None] * B
 
         def roots_of(f):
@@ -267,31 +317,76 @@ class ProofPipeline:
         c.commit(frames_dev, join=False, mask_seeds=batch.get("mask_seeds") if self.zk else None, ready=ready,
                  after=roots_of)
         # the main stream joins the commits only when it proves this batch (_finish)
-        self.launches_last += c.launches_last
-        # IO transcripts on the host threads, two frames per task
-        slot.tr = [LayerTranscript(batch["pids"][f], self.fp2_type) for f in range(B)]
-        slot.io = [self.pool.submit(self._io_pair, slot, list(range(f, min(f + 2, B)))) for f in range(0, B, 2)]
+        self._count(c.launches_last)
+        # the commitment bindings, two frames per host task, each once its
+        # frames are hashed and their roots are back (the bind thread waits)
+        pairs = [list(range(f, min(f + 2, B))) for f in range(0, B, 2)]
+        slot.io = [concurrent.futures.Future() for _ in pairs]
+        self.binder.submit(self._bind_when_ready, slot, pairs, slot.io)
 
-    def _io_pair(self, slot: _Slot, fs) -> None:
+    # ---- stage: IO hashing (runs ahead of the commits) ------------------------
+    def _prehash(self, batch: dict, group: int) -> "_Pending":
+        """the batch's IO hashing, started on the IO pool before the batch has a slot"""
+        torch, B = self.torch, self.B
+        pend = _Pending()
+        pend.batch = batch
+        pend.host_t = [a if torch.is_tensor(a) else torch.from_numpy(np.ascontiguousarray(a, np.uint8).reshape(-1))
+                       for a in batch["frames_host"]]
+        pend.frames_host = [a.numpy() for a in pend.host_t]
+        pend.tr = [LayerTranscript(batch["pids"][f], self.fp2_type) for f in range(B)]
+        pend.groups = [list(range(f, min(f + group, B))) for f in range(0, B, group)]
+        pend.hashed = [self.io_pool.submit(self._io_hash, pend, fs) for fs in pend.groups]
+        return pend
+
+    def _io_hash(self, pend: "_Pending", fs) -> None:
+        """the IO transcript of frames fs up to the circuit's output vector, the
+        vectors hashed together (tp_fs_put_circuit_outputs_pixels)"""
         L = self.layout
         n_inputs = L.padded_copies * L.n_wires
-        trs = [slot.tr[f] for f in fs]
+        trs = [pend.tr[f] for f in fs]
         for f, t in zip(fs, trs):
             t.fs.put(t.pid)
             t.fs.put(None, True)
             t.fs.put(["private_input_omitted", int(n_inputs)], True)
-            t.fs.io.append(CircuitOutputs(slot.frames_host[f], L, self.gt, self.i0, self.i1, self.dev))
+            t.fs.io.append(CircuitOutputs(pend.frames_host[f], L, self.gt, self.i0, self.i1, self.dev))
         states = (ctypes.c_void_p * len(fs))(*[ctypes.addressof(t.fs._st) for t in trs])
-        pix = (ctypes.c_void_p * len(fs))(*[slot.frames_host[f].ctypes.data for f in fs])
-        n_bytes = min(slot.frames_host[f].size for f in fs)
+        pix = (ctypes.c_void_p * len(fs))(*[pend.frames_host[f].ctypes.data for f in fs])
+        n_bytes = min(pend.frames_host[f].size for f in fs)
         native.check(self.lib, self.lib.tp_fs_put_circuit_outputs_pixels(
             states, pix, n_bytes, len(fs), L.copies, L.padded_copies, L.copy_size, L.n_wires, L.const_idx, L.const_val,
             self.G, self.gt.ctypes.data_as(_I32P), self.i0.ctypes.data_as(_I32P), self.i1.ctypes.data_as(_I32P)),
             "tp_fs_put_circuit_outputs_pixels")
-        for f in fs:
-            slot.root_events[f].synchronize()
+
+    def _bind_when_ready(self, slot: _Slot, pairs, futs) -> None:
+        """(bind thread) hands each pair of frames' commitment binding to the host
+        pool once their hashing is done and their roots are on the host"""
+        pend = slot.pending
+        group_of = {f: g for g, fs in enumerate(pend.groups) for f in fs}
+        for fs, fut in zip(pairs, futs):
+            try:
+                for g in sorted({group_of[f] for f in fs}):
+                    pend.hashed[g].result()
+                for f in fs:
+                    slot.root_events[f].synchronize()
+            except BaseException as e:      # handed to the pair's future
+                fut.set_exception(e)
+                continue
+            self.pool.submit(self._io_bind_into, slot, fs, fut)
+
+    def _io_bind_into(self, slot: _Slot, fs, fut) -> None:
+        try:
+            self._io_bind(slot, fs)
+            fut.set_result(None)
+        except BaseException as e:      # handed to the pair's future
+            fut.set_exception(e)
+
+    def _io_bind(self, slot: _Slot, fs) -> None:
+        """the commitment binding of frames fs (their roots are on the host) and
+        the GKR point's draws z1, z2"""
+        L = self.layout
         given = slot.batch.get("manifests")
-        for f, t in zip(fs, trs):
+        for f in fs:
+            t = slot.tr[f]
             if given is not None:
                 t.manifest = given[f]
             else:
@@ -306,6 +401,8 @@ class ProofPipeline:
 
     # ---- stage: GKR -------------------------------------------------------------
     def _gkr(self, slot: _Slot) -> None:
+        """(main thread) the batch's GKR launched on the main stream, its results
+        copied back to the slot's pinned buffers behind it (slot.gkr_done)"""
         torch, lib, B, nb, n = self.torch, self.lib, self.B, self.nb, self.n
         slot.committer.join()      # the main stream waits for this batch's commits (and uploads)
         for f in slot.io:
@@ -319,7 +416,8 @@ class ProofPipeline:
             native.check(lib, lib.tp_eq_table_host(z.ctypes.data, self.n_out_bits, tab.ctypes.data), "eq table")
             w = tab.reshape(-1, 2)[:self.G]
             zg.append(np.stack([w[:, 0].copy(), w[:, 1].copy()]))
-        h = self.h_in
+        h = slot.h_in
+        slot.inputs_sent.synchronize()      # the slot's previous batch has sent them
         h["z2"].numpy().view(np.uint64)[:] = np.asarray([t.z2 for t in tr], np.uint64).reshape(-1)
         nst = lib.tp_fs_state_bytes()
         st = h["states"].numpy()
@@ -342,6 +440,7 @@ class ProofPipeline:
             self.d_vs.copy_(h["vs"], non_blocking=True)
             self.d_u.copy_(h["u"], non_blocking=True)
             self.d_v.copy_(h["v"], non_blocking=True)
+        slot.inputs_sent.record(s)
         vole = dict(states=self.d_vs, u=self.d_u, v=self.d_v, count=self.count)
         bp = self.prover
         from .frame import autotune_rounds
@@ -356,8 +455,8 @@ class ProofPipeline:
             bp.prove(slot.frames_dev, zg, self.d_z2, self.d_pt, None, transcripts=self.d_states, vole=vole,
                      graph=self.graph)
         bp.prove_late(zg, transcripts=self.d_states, vole=vole, zk=self.zk)
-        self.launches_last += bp.launches_last + 1
-        o = self.h_out
+        self._count(bp.launches_last + 1)
+        o = slot.h_out
         with torch.cuda.stream(s):
             o["early"].copy_(bp.device_proof, non_blocking=True)
             o["late"].copy_(bp.late_proof, non_blocking=True)
@@ -366,8 +465,15 @@ class ProofPipeline:
             o["tag"].copy_(bp.input_tag, non_blocking=True)
             o["states"].copy_(self.d_states, non_blocking=True)
             o["vs"].copy_(self.d_vs, non_blocking=True)
-        self.gkr_done.record(s)
-        self.gkr_done.synchronize()
+        slot.gkr_done.record(s)
+
+    def _read_gkr(self, slot: _Slot) -> None:
+        """(opener thread) the batch's GKR results into its frames' transcripts"""
+        lib, B, nb, n = self.lib, self.B, self.nb, self.n
+        tr = slot.tr
+        nst = lib.tp_fs_state_bytes()
+        o = slot.h_out
+        slot.gkr_done.synchronize()
         raw_st, raw_vs = o["states"].numpy().tobytes(), o["vs"].numpy().tobytes()
         nvs = lib.tp_vole_state_bytes()
         early = o["early"].numpy().view(np.uint64).reshape(nb, B, 5, 2)
@@ -435,7 +541,7 @@ class ProofPipeline:
         c = slot.committer
         rows = (c.mask_rows[f] if k == 1 else c.rows[f]).data_ptr()
         tree = c.mask_trees[f] if k == 1 else c.trees[f]
-        s = self.stream
+        s = self.open_stream
         sp = s.cuda_stream
         n_nodes = hb["n_nodes"]
         with torch.cuda.stream(s):
@@ -453,7 +559,7 @@ class ProofPipeline:
                                                         db["idx"].data_ptr(), n_nodes,
                                                         db["nodes_comb"].data_ptr(), sp), "gather")
         # combine, its leaves, its tree levels (nine per launch), answer, query, two gathers
-        self.launches_last += 6 + -(-int(math.log2(self.leaves)) // 9)
+        self._count(6 + -(-int(math.log2(self.leaves)) // 9))
         with torch.cuda.stream(s):
             hb["comb"].copy_(db["comb"], non_blocking=True)
             hb["ans"].copy_(db["ans"], non_blocking=True)
@@ -482,22 +588,55 @@ class ProofPipeline:
         return FrameProof(t.pid, t, t.manifest, opening)
 
     def _finish(self, slot: _Slot) -> list:
-        """GKR and openings of a started batch; returns futures of its FrameProofs"""
+        """(main thread) launches the batch's GKR and hands its openings to the
+        opener thread; returns futures of its FrameProofs"""
         self._gkr(slot)
-        # host tasks of two openings each (a frame's two polynomials in the
-        # zero-knowledge mode, two frames' commits in the plain one), hashed in lockstep
-        if self.zk:
-            groups = [[(f, 0), (f, 1)] for f in range(self.B)]
-        else:
-            groups = [[(f, 0) for f in range(g, min(g + 2, self.B))] for g in range(0, self.B, 2)]
-        host = [self.pool.submit(self._open_host, slot, g) for g in groups]
-        for g, fut in zip(groups, host):
-            fut.result()
-            for f, k in g:
-                self._open_device(slot, f, k)
-        slot.opened.record(self.stream)
-        slot.assembly = [self.pool.submit(self._assemble, slot, f) for f in range(self.B)]
+        slot.assembly = [concurrent.futures.Future() for _ in range(self.B)]
+        self.opener.submit(self._open_batch, slot, slot.assembly)
         return slot.assembly
+
+    def _open_batch(self, slot: _Slot, futs) -> None:
+        """(opener thread) the GKR results into the transcripts, then the openings:
+        host tasks of two openings each (a frame's two polynomials in the
+        zero-knowledge mode, two frames' commits in the plain one, hashed in
+        lockstep), each followed by its device passes on the opening stream"""
+        try:
+            self.torch.cuda.set_device(self.dev)     # this thread's launches go to the pipeline's device
+            self._read_gkr(slot)
+            self.open_stream.wait_event(slot.gkr_done)
+            if self.zk:
+                groups = [[(f, 0), (f, 1)] for f in range(self.B)]
+            else:
+                groups = [[(f, 0) for f in range(g, min(g + 2, self.B))] for g in range(0, self.B, 2)]
+            host = [self.pool.submit(self._open_host, slot, g) for g in groups]
+            for g, fut in zip(groups, host):
+                fut.result()
+                for f, k in g:
+                    self._open_device(slot, f, k)
+            slot.opened.record(self.open_stream)
+        except BaseException as e:      # handed to the frames' futures
+            for x in futs:
+                x.set_exception(e)
+            return
+        # the frames' assembly goes to the pool only once the openings are on the
+        # host: its threads keep hashing the next batch's IO meanwhile
+        self.waiter.submit(self._release_assembly, slot, futs)
+
+    def _release_assembly(self, slot: _Slot, futs) -> None:
+        try:
+            slot.opened.synchronize()
+        except BaseException as e:      # handed to the frames' futures
+            for x in futs:
+                x.set_exception(e)
+            return
+        for f, x in enumerate(futs):
+            self.pool.submit(self._assemble_into, slot, f, x)
+
+    def _assemble_into(self, slot: _Slot, f: int, fut) -> None:
+        try:
+            fut.set_result(self._assemble(slot, f))
+        except BaseException as e:      # handed to the frame's future
+            fut.set_exception(e)
 
     def run(self, batches):
         """Prove every batch (see the class docstring); yields each batch's list of
@@ -514,12 +653,37 @@ class ProofPipeline:
             sys.setswitchinterval(switch)
 
     def _run(self, batches):
+        it = iter(batches)
+        ahead = collections.deque()
+        first = [True]
+
+        def pull():
+            batch = next(it, None)
+            if batch is not None:
+                # the first batch of a run hashes in pairs (its proofs wait on it);
+                # the batches behind it in groups of io_group (host throughput)
+                ahead.append(self._prehash(batch, 2 if first[0] else self.io_group))
+                first[0] = False
+
+        for _ in range(1 + self.io_ahead):
+            pull()
+        # a batch's proofs are handed out once the batches behind it fill the other
+        # slots: the main thread launches the next GKR without waiting for them
         prev = None
-        for i, batch in enumerate(batches):
-            slot = self.slots[i % 2]
-            self._start(slot, batch)
+        done = collections.deque()
+        i = 0
+        while ahead:
+            pend = ahead.popleft()
+            pull()
+            slot = self.slots[i % len(self.slots)]
+            i += 1
+            self._start(slot, pend)
             if prev is not None:
-                yield [x.result() for x in self._finish(prev)]
+                done.append(self._finish(prev))
+                while len(done) > len(self.slots) - 1:
+                    yield [x.result() for x in done.popleft()]
             prev = slot
         if prev is not None:
-            yield [x.result() for x in self._finish(prev)]
+            done.append(self._finish(prev))
+        while done:
+            yield [x.result() for x in done.popleft()]
