@@ -326,9 +326,10 @@ int tp_orion_open_queries2(const unsigned char* root32, uint64_t N, int use_grou
 /* No counterpart in the reference (its prover opens one polynomial per
  * process). n (<= 64) independent opening transcripts, each as
  * tp_orion_open_queries2 with its own root, use_group1, r0, r1, group and
- * outputs (arrays of n pointers; the sizes are shared), hashed in lockstep pairs:
- * two SHA-256 chains interleaved keep the x86 SHA unit busier than one. The draws
- * of each equal tp_orion_open_queries2's for the same arguments. Host only. */
+ * outputs (arrays of n pointers; the sizes are shared), hashed in lockstep: 16
+ * (then 8) at a time in the lanes of an AVX-512 multi-buffer SHA-256 where the
+ * host has AVX-512, the rest in pairs on the x86 SHA extensions. The draws of
+ * each equal tp_orion_open_queries2's for the same arguments. Host only. */
 int tp_orion_open_queries_multi(int n, const unsigned char* const* roots, uint64_t N, const int* use_group1,
                                 const uint64_t* const* r0, int n_r0, const uint64_t* const* r1, long long n_r1,
                                 long long cw_len, const int* groups, int count, long long* const* col_q,

@@ -143,17 +143,17 @@ def _addrs(arrays):
 
 def test_library_transcript_draws_single_and_lockstep():
     """the library's opening transcript (tp_orion_open_queries2 and its lockstep
-    form tp_orion_open_queries_multi: SHA-256 chains hashed in pairs, an odd one
-    alone) against the restatement above: the queried columns of every group and
-    the second batch of draws (the EC(y1) positions), for n = 1..5 transcripts in
-    one call, and
+    form tp_orion_open_queries_multi: SHA-256 chains hashed in the 16 and 8 lanes
+    of the multi-buffer compression, in pairs, an odd one alone) against the
+    restatement above: the queried columns of every group and the second batch of
+    draws (the EC(y1) positions), for 1 to 25 transcripts in one call, and
     the reference's own openings drawn as a lockstep pair"""
     from truepix_b200 import native
     lib = native.gkr(require_device=False)
     rng = np.random.default_rng(11)
     N, n_r0, n_r1, cw_len, count = 128 * 16, 128, 16, 41, 37
     specs = []
-    for i in range(5):
+    for i in range(25):
         root = rng.integers(0, 256, 32, dtype=np.uint8)
         r0 = rng.integers(0, P61, (n_r0, 2), dtype=np.uint64)
         r1 = rng.integers(0, P61, (n_r1, 2), dtype=np.uint64)
@@ -176,7 +176,7 @@ def test_library_transcript_draws_single_and_lockstep():
                                                      n_r1, cw_len, group, count, q.ctypes.data, q2.ctypes.data),
                      "tp_orion_open_queries2")
         assert q.tolist() == col and q2.tolist() == ec
-    for n in range(1, 6):
+    for n in (1, 2, 3, 5, 8, 16, 17, 25):
         sp = specs[:n]
         qs = [np.zeros(count, np.int64) for _ in range(n)]
         q2s = [np.zeros(count, np.int64) for _ in range(n)]

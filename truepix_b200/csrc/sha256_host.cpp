@@ -305,18 +305,110 @@ TP_MB_TARGET inline void transpose(typename T::V* x)
     }
 }
 
-// one SHA-256 round for every lane: T1 = h + S1(e) + Ch(e, f, g) + K[t] + W[t];
-// d += T1; h = T1 + S0(a) + Maj(a, b, c) (the other words are renamed by the caller)
-#define TP_MB_ROUND(a, b, c, d, e, f, g, h, t, w)                                                                 \
+// one SHA-256 round for every lane: T1 = h + S1(e) + Ch(e, f, g) + wk (wk = K[t] +
+// W[t]); d += T1; h = T1 + S0(a) + Maj(a, b, c) (the other words are renamed by the caller)
+#define TP_MB_ROUND(a, b, c, d, e, f, g, h, wk)                                                                   \
     {                                                                                                          \
         const V t1 = T::add(T::add(h, T::template tern<0x96>(T::template ror<6>(e), T::template ror<11>(e),     \
                                                              T::template ror<25>(e))),                          \
-                            T::add(T::template tern<0xCA>(e, f, g), T::add(T::set1(K[t]), w)));                \
+                            T::add(T::template tern<0xCA>(e, f, g), wk));                                      \
         d = T::add(d, t1);                                                                                     \
         h = T::add(t1, T::add(T::template tern<0x96>(T::template ror<2>(a), T::template ror<13>(a),            \
                                                      T::template ror<22>(a)),                                  \
                               T::template tern<0xE8>(a, b, c)));                                               \
     }
+
+// 16 rounds t0 .. t0 + 15, round t's K[t] + W[t] given by WK(t, i) (i = t mod 16)
+#define TP_MB_16_ROUNDS(WK)                                                                                    \
+    TP_MB_ROUND(a, b, c, d, e, f, g, hh, WK(t0 + 0, 0));                                                       \
+    TP_MB_ROUND(hh, a, b, c, d, e, f, g, WK(t0 + 1, 1));                                                       \
+    TP_MB_ROUND(g, hh, a, b, c, d, e, f, WK(t0 + 2, 2));                                                       \
+    TP_MB_ROUND(f, g, hh, a, b, c, d, e, WK(t0 + 3, 3));                                                       \
+    TP_MB_ROUND(e, f, g, hh, a, b, c, d, WK(t0 + 4, 4));                                                       \
+    TP_MB_ROUND(d, e, f, g, hh, a, b, c, WK(t0 + 5, 5));                                                       \
+    TP_MB_ROUND(c, d, e, f, g, hh, a, b, WK(t0 + 6, 6));                                                       \
+    TP_MB_ROUND(b, c, d, e, f, g, hh, a, WK(t0 + 7, 7));                                                       \
+    TP_MB_ROUND(a, b, c, d, e, f, g, hh, WK(t0 + 8, 8));                                                       \
+    TP_MB_ROUND(hh, a, b, c, d, e, f, g, WK(t0 + 9, 9));                                                       \
+    TP_MB_ROUND(g, hh, a, b, c, d, e, f, WK(t0 + 10, 10));                                                     \
+    TP_MB_ROUND(f, g, hh, a, b, c, d, e, WK(t0 + 11, 11));                                                     \
+    TP_MB_ROUND(e, f, g, hh, a, b, c, d, WK(t0 + 12, 12));                                                     \
+    TP_MB_ROUND(d, e, f, g, hh, a, b, c, WK(t0 + 13, 13));                                                     \
+    TP_MB_ROUND(c, d, e, f, g, hh, a, b, WK(t0 + 14, 14));                                                     \
+    TP_MB_ROUND(b, c, d, e, f, g, hh, a, WK(t0 + 15, 15));
+
+// chain c's next block (64 bytes at p[c]) into the lanes of W: lane c of W[i] is
+// its big-endian word i
+template <class T>
+TP_MB_TARGET inline void load_block(typename T::V* W, const uint8_t* const* p, size_t off)
+{
+    if constexpr (T::L == 16) {
+        for (int c = 0; c < 16; ++c) W[c] = T::bswap(T::load(p[c] + off));
+        transpose<T>(W);
+    } else {   // words 0-7 and 8-15 of the 8 chains, transposed separately
+        for (int c = 0; c < 8; ++c) W[c] = T::bswap(T::load(p[c] + off));
+        for (int c = 0; c < 8; ++c) W[8 + c] = T::bswap(T::load(p[c] + off + 32));
+        transpose<T>(W);
+        transpose<T>(W + 8);
+    }
+}
+
+// one block for every lane: s += the compression of W (the schedule is built in W)
+template <class T>
+TP_MB_TARGET inline void compress(typename T::V* s, typename T::V* W, const uint32_t K[64])
+{
+    using V = typename T::V;
+    V a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], hh = s[7];
+#define TP_MB_WK(t, i) T::add(T::set1(K[t]), W[i])
+#pragma GCC unroll 4
+    for (int t0 = 0; t0 < 64; t0 += 16) {
+        if (t0) {   // W[t] = s1(W[t-2]) + W[t-7] + s0(W[t-15]) + W[t-16], 16 at a time in place
+            for (int i = 0; i < 16; ++i) {
+                const V w2 = W[(i + 14) & 15], w15 = W[(i + 1) & 15];
+                const V s1 = T::template tern<0x96>(T::template ror<17>(w2), T::template ror<19>(w2),
+                                                    T::template shr<10>(w2));
+                const V s0 = T::template tern<0x96>(T::template ror<7>(w15), T::template ror<18>(w15),
+                                                    T::template shr<3>(w15));
+                W[i] = T::add(T::add(W[i], s0), T::add(W[(i + 9) & 15], s1));
+            }
+        }
+        TP_MB_16_ROUNDS(TP_MB_WK)
+    }
+#undef TP_MB_WK
+    s[0] = T::add(s[0], a);
+    s[1] = T::add(s[1], b);
+    s[2] = T::add(s[2], c);
+    s[3] = T::add(s[3], d);
+    s[4] = T::add(s[4], e);
+    s[5] = T::add(s[5], f);
+    s[6] = T::add(s[6], g);
+    s[7] = T::add(s[7], hh);
+}
+
+// the padding block of a 64-byte message for every lane: its W[t] + K[t] are the
+// constants PWK[t], so there is no schedule
+template <class T>
+TP_MB_TARGET inline void compress_pad(typename T::V* s, const uint32_t PWK[64])
+{
+    using V = typename T::V;
+    V a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], hh = s[7];
+#define TP_MB_PWK(t, i) T::set1(PWK[t])
+#pragma GCC unroll 4
+    for (int t0 = 0; t0 < 64; t0 += 16) {
+        TP_MB_16_ROUNDS(TP_MB_PWK)
+    }
+#undef TP_MB_PWK
+    s[0] = T::add(s[0], a);
+    s[1] = T::add(s[1], b);
+    s[2] = T::add(s[2], c);
+    s[3] = T::add(s[3], d);
+    s[4] = T::add(s[4], e);
+    s[5] = T::add(s[5], f);
+    s[6] = T::add(s[6], g);
+    s[7] = T::add(s[7], hh);
+}
+#undef TP_MB_16_ROUNDS
+#undef TP_MB_ROUND
 
 // T::L chains of nblocks blocks: chain c's state h[c], its blocks at p[c]
 template <class T>
@@ -331,59 +423,39 @@ TP_MB_TARGET void mb_blocks(uint32_t* const* h, const uint8_t* const* p, size_t 
     for (int w = 0; w < 8; ++w) s[w] = T::load(tmp[w]);
     for (size_t blk = 0; blk < nblocks; ++blk) {
         V W[16];
-        if constexpr (L == 16) {
-            for (int c = 0; c < 16; ++c) W[c] = T::bswap(T::load(p[c] + 64 * blk));
-            transpose<T>(W);
-        } else {   // words 0-7 and 8-15 of the 8 chains, transposed separately
-            for (int c = 0; c < 8; ++c) W[c] = T::bswap(T::load(p[c] + 64 * blk));
-            for (int c = 0; c < 8; ++c) W[8 + c] = T::bswap(T::load(p[c] + 64 * blk + 32));
-            transpose<T>(W);
-            transpose<T>(W + 8);
-        }
-        V a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], hh = s[7];
-#pragma GCC unroll 4
-        for (int t0 = 0; t0 < 64; t0 += 16) {
-            if (t0) {   // W[t] = s1(W[t-2]) + W[t-7] + s0(W[t-15]) + W[t-16], 16 at a time in place
-                for (int i = 0; i < 16; ++i) {
-                    const V w2 = W[(i + 14) & 15], w15 = W[(i + 1) & 15];
-                    const V s1 = T::template tern<0x96>(T::template ror<17>(w2), T::template ror<19>(w2),
-                                                        T::template shr<10>(w2));
-                    const V s0 = T::template tern<0x96>(T::template ror<7>(w15), T::template ror<18>(w15),
-                                                        T::template shr<3>(w15));
-                    W[i] = T::add(T::add(W[i], s0), T::add(W[(i + 9) & 15], s1));
-                }
-            }
-            TP_MB_ROUND(a, b, c, d, e, f, g, hh, t0 + 0, W[0]);
-            TP_MB_ROUND(hh, a, b, c, d, e, f, g, t0 + 1, W[1]);
-            TP_MB_ROUND(g, hh, a, b, c, d, e, f, t0 + 2, W[2]);
-            TP_MB_ROUND(f, g, hh, a, b, c, d, e, t0 + 3, W[3]);
-            TP_MB_ROUND(e, f, g, hh, a, b, c, d, t0 + 4, W[4]);
-            TP_MB_ROUND(d, e, f, g, hh, a, b, c, t0 + 5, W[5]);
-            TP_MB_ROUND(c, d, e, f, g, hh, a, b, t0 + 6, W[6]);
-            TP_MB_ROUND(b, c, d, e, f, g, hh, a, t0 + 7, W[7]);
-            TP_MB_ROUND(a, b, c, d, e, f, g, hh, t0 + 8, W[8]);
-            TP_MB_ROUND(hh, a, b, c, d, e, f, g, t0 + 9, W[9]);
-            TP_MB_ROUND(g, hh, a, b, c, d, e, f, t0 + 10, W[10]);
-            TP_MB_ROUND(f, g, hh, a, b, c, d, e, t0 + 11, W[11]);
-            TP_MB_ROUND(e, f, g, hh, a, b, c, d, t0 + 12, W[12]);
-            TP_MB_ROUND(d, e, f, g, hh, a, b, c, t0 + 13, W[13]);
-            TP_MB_ROUND(c, d, e, f, g, hh, a, b, t0 + 14, W[14]);
-            TP_MB_ROUND(b, c, d, e, f, g, hh, a, t0 + 15, W[15]);
-        }
-        s[0] = T::add(s[0], a);
-        s[1] = T::add(s[1], b);
-        s[2] = T::add(s[2], c);
-        s[3] = T::add(s[3], d);
-        s[4] = T::add(s[4], e);
-        s[5] = T::add(s[5], f);
-        s[6] = T::add(s[6], g);
-        s[7] = T::add(s[7], hh);
+        load_block<T>(W, p, 64 * blk);
+        compress<T>(s, W, K);
     }
     for (int w = 0; w < 8; ++w) T::store(tmp[w], s[w]);
     for (int w = 0; w < 8; ++w)
         for (int c = 0; c < L; ++c) h[c][w] = tmp[w][c];
 }
-#undef TP_MB_ROUND
+
+// SHA-256 of T::L messages of 64 bytes each (in[c]), digests as bytes (out[c])
+template <class T>
+TP_MB_TARGET void mb_hash64(const uint8_t* const* in, uint8_t* const* out, const uint32_t K[64],
+                            const uint32_t PWK[64])
+{
+    using V = typename T::V;
+    constexpr int L = T::L;
+    static const uint32_t iv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
+                                   0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+    V s[8], W[16];
+    for (int w = 0; w < 8; ++w) s[w] = T::set1(iv[w]);
+    load_block<T>(W, in, 0);
+    compress<T>(s, W, K);
+    compress_pad<T>(s, PWK);
+    alignas(64) uint32_t tmp[8][L];
+    for (int w = 0; w < 8; ++w) T::store(tmp[w], s[w]);
+    for (int c = 0; c < L; ++c)
+        for (int w = 0; w < 8; ++w) {
+            const uint32_t x = tmp[w][c];
+            out[c][4 * w] = (uint8_t)(x >> 24);
+            out[c][4 * w + 1] = (uint8_t)(x >> 16);
+            out[c][4 * w + 2] = (uint8_t)(x >> 8);
+            out[c][4 * w + 3] = (uint8_t)x;
+        }
+}
 
 }  // namespace
 
@@ -400,6 +472,21 @@ extern "C" TP_MB_TARGET int tp_host_sha_mb_blocks(uint32_t* const* h, const uint
     }
     return c;
 }
+
+// SHA-256 of the first n 64-byte messages in groups of 16 lanes and then one of 8
+// where n allows; returns how many were hashed (the caller hashes the rest)
+extern "C" TP_MB_TARGET int tp_host_sha_mb_hash64(const uint8_t* const* in, uint8_t* const* out, int n,
+                                                  const uint32_t K[64])
+{
+    static const PadWk pad(K);
+    int c = 0;
+    for (; c + 16 <= n; c += 16) mb_hash64<Lanes16>(in + c, out + c, K, pad.wk);
+    if (c + 8 <= n) {
+        mb_hash64<Lanes8>(in + c, out + c, K, pad.wk);
+        c += 8;
+    }
+    return c;
+}
 #undef TP_MB_TARGET
 
 #else
@@ -410,5 +497,6 @@ extern "C" void tp_host_sha_ext_multi(uint32_t* const*, const uint8_t* const*, i
 extern "C" void tp_host_sha_ext_hash64(const uint8_t* const*, uint8_t* const*, int, const uint32_t*) {}
 extern "C" int tp_host_sha_mb_available(void) { return 0; }
 extern "C" int tp_host_sha_mb_blocks(uint32_t* const*, const uint8_t* const*, int, size_t, const uint32_t*) { return 0; }
+extern "C" int tp_host_sha_mb_hash64(const uint8_t* const*, uint8_t* const*, int, const uint32_t*) { return 0; }
 
 #endif

@@ -24,6 +24,7 @@ extern "C" void tp_host_sha_ext_hash64(const uint8_t* const* in, uint8_t* const*
 extern "C" int tp_host_sha_mb_available(void);
 extern "C" int tp_host_sha_mb_blocks(uint32_t* const* h, const uint8_t* const* p, int n, size_t nblocks,
                                      const uint32_t K[64]);
+extern "C" int tp_host_sha_mb_hash64(const uint8_t* const* in, uint8_t* const* out, int n, const uint32_t K[64]);
 extern "C" void tp_host_sha_ext_multi(uint32_t* const* h, const uint8_t* const* p, int n, size_t nblocks,
                                       const uint32_t K[64]);
 
@@ -636,17 +637,21 @@ int tp_orion_open_queries_multi(int n, const unsigned char* const* roots, uint64
         return -1;
     }
     // the n transcripts take the same steps on their own bytes, their hashes in
-    // lockstep (two SHA-256 chains interleaved keep the SHA unit busier than one)
+    // lockstep (multi-buffer lanes, else pairs of interleaved SHA-extension chains)
     std::vector<OrionFs> t((size_t)n);
     std::vector<std::array<uint8_t, 64>> blocks((size_t)n);
     std::vector<const uint8_t*> in((size_t)n);
     std::vector<uint8_t*> out((size_t)n);
     for (OrionFs& x : t) memset(&x, 0, sizeof(x));
     auto hash_all = [&]() {
+        // groups of 16 (then 8) in the lanes of the multi-buffer compression, the
+        // rest in lockstep pairs on the SHA extensions
+        const int done = host_sha_mb() ? tp_host_sha_mb_hash64(in.data(), out.data(), n, kHostTables.k) : 0;
+        if (done == n) return;
         if (host_sha_ext()) {
-            tp_host_sha_ext_hash64(in.data(), out.data(), n, kHostTables.k);
+            tp_host_sha_ext_hash64(in.data() + done, out.data() + done, n - done, kHostTables.k);
         } else {
-            for (int c = 0; c < n; ++c) sha256_64(in[(size_t)c], out[(size_t)c]);
+            for (int c = done; c < n; ++c) sha256_64(in[(size_t)c], out[(size_t)c]);
         }
     };
     // absorb of `len` <= 32 bytes, chain c's bytes at src(c)

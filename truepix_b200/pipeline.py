@@ -203,14 +203,16 @@ class ProofPipeline:
     and yields, per batch, the list of FrameProof. io_group frames are hashed per
     IO task (0: 16 where the host has the multi-buffer SHA-256, else 2), on
     io_threads threads (0: one per CPU but four), io_ahead batches ahead of the
-    commits; host_threads run the bindings, openings and assembly. `slots` batches
+    commits; host_threads run the bindings, openings (open_group per task, their
+    transcripts hashed in lockstep: 16 use the multi-buffer SHA-256's lanes, at a
+    longer latency per task than the default 2) and assembly. `slots` batches
     hold device buffers at once (each frame's codewords and trees, 231 MB per
     committed 1080p polynomial): with three, a batch's commits never wait for the
     assembly of the batch two before it."""
 
     def __init__(self, layout, gate_type, in0, in1, batch: int, device: int = 0, zk: bool = False,
                  host_threads: int = 0, commit_streams: int = 8, fp2_type=None, graph: bool = True,
-                 io_group: int = 0, io_ahead: int = 3, io_threads: int = 0, slots: int = 3):
+                 io_group: int = 0, io_ahead: int = 3, io_threads: int = 0, slots: int = 3, open_group: int = 0):
         import torch
         from .frame import BatchFrameProver
         self.torch = torch
@@ -250,7 +252,9 @@ class ProofPipeline:
         # the IO hashing on a pool of its own, so that the long hashing tasks of
         # the batches ahead never queue in front of the current batch's openings
         self.io_pool = concurrent.futures.ThreadPoolExecutor(io_threads or max(1, (os.cpu_count() or 4) - 4))
-        self.io_group = io_group or (16 if self.lib.tp_host_sha_mb_available() else 2)
+        mb = self.lib.tp_host_sha_mb_available()
+        self.io_group = io_group or (16 if mb else 2)
+        self.open_group = open_group or 2
         self.io_ahead = io_ahead
         # waits on device events and hashing that would otherwise hold host pool threads
         self.waiter = concurrent.futures.ThreadPoolExecutor(1)
@@ -597,17 +601,16 @@ class ProofPipeline:
 
     def _open_batch(self, slot: _Slot, futs) -> None:
         """(opener thread) the GKR results into the transcripts, then the openings:
-        host tasks of two openings each (a frame's two polynomials in the
-        zero-knowledge mode, two frames' commits in the plain one, hashed in
-        lockstep), each followed by its device passes on the opening stream"""
+        host tasks of open_group openings each (in the zero-knowledge mode a
+        frame's two polynomials side by side), their transcripts hashed in
+        lockstep, each task followed by its device passes on the opening stream"""
         try:
             self.torch.cuda.set_device(self.dev)     # this thread's launches go to the pipeline's device
             self._read_gkr(slot)
             self.open_stream.wait_event(slot.gkr_done)
-            if self.zk:
-                groups = [[(f, 0), (f, 1)] for f in range(self.B)]
-            else:
-                groups = [[(f, 0) for f in range(g, min(g + 2, self.B))] for g in range(0, self.B, 2)]
+            items = [(f, k) for f in range(self.B) for k in range(2 if self.zk else 1)]
+            per = self.open_group
+            groups = [items[g:g + per] for g in range(0, len(items), per)]
             host = [self.pool.submit(self._open_host, slot, g) for g in groups]
             for g, fut in zip(groups, host):
                 fut.result()
