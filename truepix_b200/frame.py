@@ -289,11 +289,12 @@ class BatchFrameProver:
                 beta_of[f] = self.betas[C].data_ptr() + 16 * C * q
         lib.tp_batch_reset(b)
         keep = []
+        quick = native.gkr_launcher()     # per-frame setup calls keep the interpreter lock
         for f, L in enumerate(self.layouts):
             z1r = np.ascontiguousarray(z1s[f][0], np.uint64)
             z1i = np.ascontiguousarray(z1s[f][1], np.uint64)
             keep += [z1r, z1i]
-            native.check(lib, lib.tp_batch_set_pixels(
+            native.check(lib, quick.tp_batch_set_pixels(
                 b, f, self.gt.size, self.gt.ctypes.data, self.i0.ctypes.data, self.i1.ctypes.data,
                 z1r.ctypes.data, z1i.ctypes.data, pixels[f].data_ptr(), L.copies, L.padded_copies,
                 L.copy_size, L.n_wires, L.const_idx, L.const_val, beta_of[f]), "batch_set_pixels")

@@ -165,8 +165,8 @@ GKR_SIGNATURES = {
 _cache = {}
 
 
-def _bind(path: str, sigs: dict):
-    lib = ctypes.CDLL(path)
+def _bind(path: str, sigs: dict, keep_lock: bool = False):
+    lib = (ctypes.PyDLL if keep_lock else ctypes.CDLL)(path)
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):
             fn = getattr(lib, name)
@@ -192,6 +192,18 @@ def gkr(require_device: bool = True):
         if not lib.native_fp2_cuda_available():
             raise RuntimeError("no usable CUDA device: " + lib.tp_last_error().decode())
     return lib
+
+
+def gkr_launcher():
+    """The same library bound so that its calls keep the interpreter lock, for
+    entry points that only queue device work (microseconds each): a launching
+    thread that gives the lock up for each of hundreds of such calls per batch
+    waits to take it back from the host threads every time."""
+    if "gkr_launcher" not in _cache:
+        gkr(require_device=False)
+        path = os.environ.get("TRUEPIX_NATIVE_FP2_GPU_LIB", lib_path("libnative_fp2_gpu.so"))
+        _cache["gkr_launcher"] = _bind(path, GKR_SIGNATURES, keep_lock=True)
+    return _cache["gkr_launcher"]
 
 
 def check(lib, rc=0, what="call"):

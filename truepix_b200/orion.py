@@ -72,7 +72,7 @@ class FrameCommitter:
         frame's commit, not the stream's later frames)."""
         if self.zk != (mask_seeds is not None):
             raise ValueError("mask_seeds are given exactly for a zk committer")
-        torch, lib, s = self.torch, self.lib, self._s()
+        torch, lib, s = self.torch, native.gkr_launcher(), self._s()
         launches = 0
         main = self.stream if self.stream is not None else torch.cuda.current_stream(self.dev)
         if self.side:

@@ -540,7 +540,7 @@ class ProofPipeline:
             native.check(lib, 0 if hb["n_nodes"] >= 0 else -1, "tp_orion_path_nodes")
 
     def _open_device(self, slot: _Slot, f: int, k: int) -> None:
-        torch, lib = self.torch, self.lib
+        torch, lib = self.torch, native.gkr_launcher()
         hb, db = slot.open_host[f][k], slot.open_dev[f][k]
         c = slot.committer
         rows = (c.mask_rows[f] if k == 1 else c.rows[f]).data_ptr()
@@ -649,7 +649,7 @@ class ProofPipeline:
         # assembly, transcript puts): a short switch interval lets the launching
         # thread take it back soon
         switch = sys.getswitchinterval()
-        sys.setswitchinterval(2e-4)
+        sys.setswitchinterval(5e-5)
         try:
             yield from self._run(batches)
         finally:
