@@ -107,44 +107,58 @@ void dev_free(void* p, cudaStream_t s)
 }
 
 namespace {
-constexpr int kRingSlots = 64;
-constexpr size_t kRingSlot = 256 * 1024;
+// Pinned staging rings for small uploads: a slot is reused once the copy that
+// last read it has run (its event). Uploads of a batch's per-frame tables (a few
+// KB each, three per frame) take the small ring, whose 1024 slots outlast several
+// batches: a ring that wrapped inside one batch would make the launching thread
+// wait for copies queued behind the device's earlier work.
+struct Ring {
+    int slots;
+    size_t slot_bytes;
+    unsigned char* mem = nullptr;
+    std::vector<cudaEvent_t> ev;
+    std::vector<bool> used;
+    int next = 0;
+};
+Ring g_small{1024, 16 * 1024};
+Ring g_large{64, 256 * 1024};
 std::mutex g_ring_mu;
-unsigned char* g_ring = nullptr;
-cudaEvent_t g_ring_ev[kRingSlots];
-bool g_ring_used[kRingSlots] = {false};
-int g_ring_next = 0;
+
+bool ring_upload(Ring& r, void* d_dst, const void* h_src, size_t bytes, cudaStream_t s)
+{
+    if (!r.mem) {
+        if (cuda_failed(cudaHostAlloc((void**)&r.mem, (size_t)r.slots * r.slot_bytes, cudaHostAllocDefault),
+                        "pinned staging"))
+            return false;
+        r.ev.assign((size_t)r.slots, nullptr);
+        r.used.assign((size_t)r.slots, false);
+        for (int i = 0; i < r.slots; ++i)
+            if (cuda_failed(cudaEventCreateWithFlags(&r.ev[(size_t)i], cudaEventDisableTiming), "staging event"))
+                return false;
+    }
+    const int slot = r.next;
+    r.next = (r.next + 1) % r.slots;
+    if (r.used[(size_t)slot] && cuda_failed(cudaEventSynchronize(r.ev[(size_t)slot]), "staging wait"))
+        return false;
+    unsigned char* h = r.mem + (size_t)slot * r.slot_bytes;
+    memcpy(h, h_src, bytes);
+    if (cuda_failed(cudaMemcpyAsync(d_dst, h, bytes, cudaMemcpyHostToDevice, s), "upload")) return false;
+    r.used[(size_t)slot] = true;
+    return !cuda_failed(cudaEventRecord(r.ev[(size_t)slot], s), "staging record");
+}
 }  // namespace
 
 bool upload_async(void* d_dst, const void* h_src, size_t bytes, cudaStream_t s)
 {
     if (bytes == 0) return true;
     if (!ctx()) return false;
-    if (bytes > kRingSlot) {
+    if (bytes > g_large.slot_bytes) {
         if (cuda_failed(cudaMemcpyAsync(d_dst, h_src, bytes, cudaMemcpyHostToDevice, s), "upload"))
             return false;
         return !cuda_failed(cudaStreamSynchronize(s), "upload");
     }
     std::lock_guard<std::mutex> lock(g_ring_mu);
-    if (!g_ring) {
-        if (cuda_failed(cudaHostAlloc((void**)&g_ring, kRingSlots * kRingSlot, cudaHostAllocDefault),
-                        "pinned staging"))
-            return false;
-        for (int i = 0; i < kRingSlots; ++i)
-            if (cuda_failed(cudaEventCreateWithFlags(&g_ring_ev[i], cudaEventDisableTiming),
-                            "staging event"))
-                return false;
-    }
-    const int slot = g_ring_next;
-    g_ring_next = (g_ring_next + 1) % kRingSlots;
-    if (g_ring_used[slot] && cuda_failed(cudaEventSynchronize(g_ring_ev[slot]), "staging wait"))
-        return false;
-    unsigned char* h = g_ring + (size_t)slot * kRingSlot;
-    memcpy(h, h_src, bytes);
-    if (cuda_failed(cudaMemcpyAsync(d_dst, h, bytes, cudaMemcpyHostToDevice, s), "upload"))
-        return false;
-    g_ring_used[slot] = true;
-    return !cuda_failed(cudaEventRecord(g_ring_ev[slot], s), "staging record");
+    return ring_upload(bytes <= g_small.slot_bytes ? g_small : g_large, d_dst, h_src, bytes, s);
 }
 
 namespace {
