@@ -157,11 +157,13 @@ class LayerTranscript:
         closing: the closing values, n + 10, or n + 15 for the zero-knowledge
         prover; point, tag: the input point and tag)."""
         t = self.fs.trans
+        F = self.F
+        tl = lambda a: a.tolist() if hasattr(a, "tolist") else [[int(v) for v in x] for x in a]
         for rnd in list(early) + list(late):
-            for x in rnd:
-                t.append([self._f(x)])
+            for a, b in tl(rnd):          # plain ints first: far cheaper than numpy scalars one by one
+                t.append([F(a, b, P61)])
         n = len(closing) - (15 if zk else 10)
-        cl = [self._f(x) for x in closing]
+        cl = [F(a, b, P61) for a, b in tl(closing)]
         t.append([(cl[0], cl[1])])
         for k in range(n):
             t.append([cl[2 + k]])
