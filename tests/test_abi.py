@@ -196,3 +196,16 @@ def test_orion_sizes_without_device():
     assert lib.tp_orion_tree_leaves(128 * 100) == 256
     assert lib.tp_orion_tree_leaves(1 << 23) == 1 << 17
     assert lib.tp_orion_tree_leaves(100) == 0
+
+
+def test_launcher_handle_keeps_the_lock_and_shares_the_library():
+    """native.gkr_launcher(): the same library bound as a PyDLL (calls keep the
+    interpreter lock), with the same signatures and the same error state"""
+    import ctypes
+    from truepix_b200 import native
+    lib, quick = native.gkr(require_device=False), native.gkr_launcher()
+    assert isinstance(quick, ctypes.PyDLL) and not isinstance(lib, ctypes.PyDLL)
+    assert quick.tp_host_sha_mb_available() == lib.tp_host_sha_mb_available()
+    bad = np.array([(1 << 61) - 1, 0], np.uint64)
+    assert quick.tp_eq_table_host(bad.ctypes.data, 1, np.empty(4, np.uint64).ctypes.data) == -1
+    assert lib.tp_last_error_code() != 0 and lib.tp_last_error()

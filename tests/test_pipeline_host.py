@@ -1,8 +1,9 @@
 """Host pieces of the pipelined prover (truepix_b200.pipeline) on the CPU: the
 host eq table (tp_eq_table_host) against the oracle's compute_beta, the Merkle
 node list of an opening (tp_orion_path_nodes) against the restatement of the
-reference's collect_merkle_siblings, and the VOLE correlation count of a frame's
-proof against the reference chain's fixture."""
+reference's collect_merkle_siblings, the VOLE correlation count of a frame's
+proof against the reference chain's fixture, and the run loop's ordering (IO
+hashed ahead, slots reused, batches handed out in order) with its stages stubbed."""
 import ctypes
 
 import numpy as np
@@ -64,3 +65,48 @@ def test_correlation_count_matches_reference_chain():
         assert correlations_needed(layout) == int(c["used_closed"][0]) - int(c["start"][0])
         n += 1
     assert n == 2
+
+
+def test_run_order_lookahead_and_slot_reuse():
+    """ProofPipeline._run with its stages stubbed (no device): every batch is
+    hashed ahead (the first in pairs, the rest in io_group), started on the slots
+    in turn, finished once, and handed out in input order; a slot is started again
+    only after the batch that last held it was finished (its proofs' futures exist:
+    the real _start waits on them)"""
+    import concurrent.futures
+    from truepix_b200.pipeline import ProofPipeline
+    for n_slots, ahead, n_batches in ((3, 3, 7), (2, 1, 5), (3, 0, 1), (4, 2, 0)):
+        pipe = object.__new__(ProofPipeline)
+        pipe.io_ahead, pipe.io_group = ahead, 16
+        pipe.slots = [dict(name=i, holds=None) for i in range(n_slots)]
+        log, out = [], []
+
+        def prehash(batch, group):
+            log.append(("hash", batch, group))
+            return batch
+
+        def start(slot, batch):
+            assert slot["holds"] is None or ("finish", slot["holds"]) in log, (slot, log)
+            slot["holds"] = batch
+            log.append(("start", batch))
+
+        def finish(slot):
+            log.append(("finish", slot["holds"]))
+            fut = concurrent.futures.Future()
+            fut.set_result(slot["holds"])
+            return [fut]
+
+        pipe._prehash, pipe._start, pipe._finish = prehash, start, finish
+        for got in pipe._run(iter(range(n_batches))):
+            out.extend(got)
+        assert out == list(range(n_batches))
+        hashes = [e for e in log if e[0] == "hash"]
+        assert [e[1] for e in hashes] == list(range(n_batches))
+        assert [e[2] for e in hashes] == [2] + [16] * (n_batches - 1) if n_batches else hashes == []
+        starts = [e[1] for e in log if e[0] == "start"]
+        assert starts == list(range(n_batches))
+        assert sorted(e[1] for e in log if e[0] == "finish") == list(range(n_batches))
+        for b in range(n_batches):     # hashing runs ahead of the commits by io_ahead + 1 batches at most
+            assert log.index(("hash", b, 2 if b == 0 else 16)) < log.index(("start", b))
+            if b > ahead + 1:
+                assert log.index(("start", b - ahead - 2)) < log.index(("hash", b, 16))

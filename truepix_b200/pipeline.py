@@ -47,6 +47,7 @@ import ctypes
 import math
 import os
 import struct
+import threading
 
 import numpy as np
 
@@ -263,7 +264,7 @@ class ProofPipeline:
         # stream of their own while the main thread launches the next batch's GKR
         self.opener = concurrent.futures.ThreadPoolExecutor(1)
         self.open_stream = torch.cuda.Stream(self.dev)
-        self._count_lock = __import__("threading").Lock()
+        self._count_lock = threading.Lock()
         self.launches_last = 0
         # the first batch's rounds run launch by launch with the round autotuner on;
         # later batches replay them as one CUDA graph (BatchFrameProver.prove(graph=True))
