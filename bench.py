@@ -818,7 +818,7 @@ def ours_arm(args, rank, world, local_rank):
                        "orion": {"columns": 128, "codeword_rows": cw_len, "tree_leaves": leaves,
                                  "queried_columns": 1222},
                        "l2": "inputs > L2: B distinct frames (0.4 GB) and their codewords (14.8 GB) per step",
-                       "host_threads": os.cpu_count(),
+                       "host_threads": os.cpu_count(), "pipeline": proved.get("pipeline"),
                        "parallelism": f"replicas x{world}"},
             "proof_check": check,
             "breakdown": {
@@ -936,6 +936,10 @@ def proved_bench(args, rank, world, local_rank, zk=False, steps=None, warmup=Non
                "timer": "CUDA events on the main stream, the end event after the last proofs are assembled",
                "path": "pinned host frames uploaded on a copy stream inside the timed region; every proof "
                        "(GKR proof values, opening file bytes) assembled in host memory"}
+    # the pipeline's shape: device slots, IO hashing groups and lookahead, opening groups, host threads
+    out["resident"]["pipeline"] = {"slots": len(pipe.slots), "io_group": pipe.io_group, "io_ahead": pipe.io_ahead,
+                                   "open_group": pipe.open_group, "io_threads": pipe.io_pool._max_workers,
+                                   "host_threads": pipe.pool._max_workers}
     pipe.close()
     last = out["resident"].pop("last")
     del pipe, frames_dev
